@@ -1,0 +1,441 @@
+"""Benchmark of the BETA assembly + PCG path on B200.
+
+Default workload (N=1): 3D hex8 linear elasticity on a structured
+100x100x100 cube (1,030,301 nodes, 3,090,903 dofs), 2x2x2 Gauss, per-element
+E = 1e4*exp(N(0,0.5^2)), nu ~ U[0.20,0.35], z=0 clamped, pressure 1.0 on z=1.
+One step = FP32 assembly + mixed-precision refinement solve (FP32 block-Jacobi
+inner PCG, FP64 matrix-free outer residual and update) to
+||b - A u||/||b|| <= tol, inputs resident in HBM.  The plain FP64 GPU
+Jacobi-PCG is measured on the same workload for the mixed/plain ratio.
+
+Multi-GPU (torchrun): every rank solves its own replica (the path does not
+shard: one system per GPU); value = total dofs solved / max-over-ranks time.
+
+--impl reference: the reference's CPU algorithm (the oracle restatement,
+all host cores) on a bounded sample of the same workload, extrapolated to
+the full solve (see cpu_baseline.sample in the output).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solved DOFs/s at <=1e-8 rel err, mixed vs plain FP64 GPU PCG; p50/p99 latency"
+UNIT = "DOF/s"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons in the background."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic():
+    p = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def make_model(cfg, n):
+    from betanoox_b200 import workloads as W
+    if cfg == "cube":
+        return W.cube_hex8(n)
+    raise SystemExit(f"unknown config {cfg}")
+
+
+def _pinned_copy(a):
+    import torch
+    t = torch.empty(a.shape, dtype={np.float64: torch.float64, np.int32: torch.int32,
+                                     np.uint8: torch.uint8}[a.dtype.type], pin_memory=True)
+    t.numpy()[...] = a
+    return t.numpy()
+
+
+def spmv_algorithmic_bytes(nblk, nnode, nd):
+    """Per launch of the FP32 node-block SpMV: every stored block once (nd*nd
+    FP32 values + one 4-byte column index), the input vector once and the
+    output vector once (nd FP32 per node)."""
+    return nblk * (nd * nd * 4 + 4) + 2 * nnode * nd * 4
+
+
+def run_ours(args):
+    import torch
+    from betanoox_b200 import Solver, _abi, opts
+
+    ws, rank, local = _dist()
+    dev = local
+    torch.cuda.set_device(dev)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
+
+    m = make_model(args.config, args.n)
+    stream = torch.cuda.Stream(device=dev)
+    g = Solver(dev)
+    g.lib.beta_gpu_set_stream(g.h, C.c_void_p(stream.cuda_stream))
+    t0 = time.perf_counter()
+    g.load_model(m)
+    g.build_pattern()
+    t_setup = time.perf_counter() - t0
+    lib, h = g.lib, g.h
+
+    tol = args.tol
+    o_mp = opts(mode=_abi.MODE_MPIR, precond=_abi.PRECOND_BLOCK_JACOBI, stop_rule=_abi.STOP_RB, tol=tol,
+                inner_tol=args.inner_tol, profile=True)
+    o_64 = opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=tol, profile=True)
+
+    def counters():
+        a = (C.c_longlong * 3)()
+        lib.beta_gpu_counters(h, a, 3)
+        return list(a)
+
+    def step_mp():
+        g.assemble(_abi.FP32)
+        rc, st = g.solve(o_mp)
+        return st
+
+    def step_64():
+        g.assemble(_abi.FP64)
+        rc, st = g.solve(o_64)
+        return st
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        c0 = counters()
+        stats = []
+        with torch.cuda.stream(stream):
+            for i in range(steps):
+                evs[i][0].record(stream)
+                stats.append(fn())
+                evs[i][1].record(stream)
+        barrier()
+        c1 = counters()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        return ms, stats, [c1[k] - c0[k] for k in range(3)]
+
+    # -- mixed precision (headline) --
+    with Clocks(dev) as clk:
+        ms_mp, st_mp, cnt_mp = timed(step_mp, args.steps, args.warmup)
+    u_mp = g.download()
+    # -- plain FP64 GPU PCG on the same workload --
+    fp64 = None
+    if not args.skip_fp64:
+        ms_64, st_64, _ = timed(step_64, max(1, min(args.steps, 2)), 1)
+        u_64 = g.download()
+        fp64 = {"ms": ms_64, "stats": [s.as_dict() for s in st_64], "u": u_64}
+    # accuracy: error of both against a tight FP64 reference solution
+    err = None
+    if not args.skip_accuracy:
+        g.assemble(_abi.FP64)
+        g.solve(opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=1e-13))
+        u_t = g.download()
+        nt = np.linalg.norm(u_t)
+        err = {"mixed": float(np.linalg.norm(u_mp - u_t) / nt)}
+        if fp64:
+            err["fp64"] = float(np.linalg.norm(fp64["u"] - u_t) / nt)
+
+    # -- end to end through the C ABI from pinned host buffers --
+    e2e = None
+    if not args.skip_e2e:
+        pm = type(m)(m.name, m.kind, m.ndim, _pinned_copy(m.xyz), _pinned_copy(m.conn), m.ndpn,
+                     _pinned_copy(m.params), _pinned_copy(m.restrained), _pinned_copy(m.prescribed),
+                     _pinned_copy(m.load), m.order, m.meta)
+        u_host = _pinned_copy(np.zeros(m.ndof))
+        ge = Solver(dev)
+        ge.lib.beta_gpu_set_stream(ge.h, C.c_void_p(stream.cuda_stream))
+
+        def e2e_step():
+            ge.load_model(pm)
+            ge.build_pattern()
+            ge.assemble(_abi.FP32)
+            ge.solve(o_mp)
+            ge.lib.beta_gpu_download(ge.h, u_host.ctypes.data_as(C.c_void_p))
+
+        def ecnt():
+            a = (C.c_longlong * 3)()
+            ge.lib.beta_gpu_counters(ge.h, a, 3)
+            return list(a)
+
+        e2e_step()
+        barrier()
+        c0 = ecnt()
+        tw = []
+        for _ in range(max(1, args.e2e_steps)):
+            t1 = time.perf_counter()
+            e2e_step()
+            torch.cuda.synchronize()
+            tw.append(time.perf_counter() - t1)
+        c1 = ecnt()
+        k = max(1, args.e2e_steps)
+        tmax = max(tw)
+        if ws > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([tmax], device=f"cuda:{dev}")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            tmax = float(tt.item())
+        e2e = {"value": ws * m.ndof / statistics.median(tw), "unit": UNIT,
+               "h2d_bytes_per_step": (c1[1] - c0[1]) // k, "d2h_bytes_per_step": (c1[2] - c0[2]) // k,
+               "ms_per_step": 1e3 * statistics.median(tw)}
+        ge.close()
+
+    # -- reduce timing over ranks --
+    tot_ms = sum(ms_mp)
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([tot_ms], device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot_ms = float(tt.item())
+    ms_step = tot_ms / args.steps
+    value = ws * m.ndof * args.steps / (tot_ms / 1e3)
+
+    out = None
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        nblk = int(g.nnz_blocks) if hasattr(g, "nnz_blocks") else None
+        spmv_ms = statistics.median([s.ms_spmv_avg for s in st_mp])
+        alg = spmv_algorithmic_bytes(_nblk(m), m.nnode, m.ndpn)
+        achieved = alg / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
+        tr = _traffic()
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": tr.get("bytes_per_launch") if tr else None,
+                "kernel": "k_spmv_dot_b<3> (FP32 node-block sliced-ELL SpMV + p.Ap)",
+                "algorithmic_bytes_per_launch": alg, "ms_per_launch": spmv_ms,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
+        lat = sorted(ms_mp)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32 inner / fp64 outer", "data": "synthetic (seeded generator)",
+            "config": {"workload": f"hex8 elasticity cube {m.meta['n']}^3, {m.ndof} dofs, lognormal E, "
+                                   f"2x2x2 Gauss, z=0 clamped, p=1 on z=1",
+                       "global_batch": ws, "ndof": m.ndof, "nelem": m.nelem, "parallelism": f"replicas x{ws}",
+                       "tol": tol, "stop_rule": "||b-Au||/||b||", "inner_tol": args.inner_tol,
+                       "l2": "inputs larger than L2 (FP32 matrix ~1 GB per replica)"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "mixed": {"iterations": [s.iterations for s in st_mp], "outer": [s.outer_iterations for s in st_mp],
+                      "true_rel_residual": [s.true_rel_residual for s in st_mp], "ms_steps": ms_mp},
+            "e2e": e2e, "gpu_launches": cnt_mp[0], "roofline": roof,
+            "clocks": clk.summary(), "setup_s": t_setup,
+        }
+        if fp64:
+            v64 = m.ndof / (statistics.median(fp64["ms"]) / 1e3)
+            out["fp64_plain"] = {"value": ws * v64, "ms_steps": fp64["ms"],
+                                 "iterations": [s["iterations"] for s in fp64["stats"]],
+                                 "ms_spmv_avg": [s["ms_spmv_avg"] for s in fp64["stats"]]}
+            out["mixed_over_fp64"] = value / (ws * v64)
+        if err:
+            out["rel_err_vs_fp64_reference"] = err
+        if not args.skip_cpu:
+            out["cpu_baseline"] = cpu_baseline(m, args, st_64_iters=out.get("fp64_plain", {}).get("iterations"))
+    g.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return out
+
+
+def _nblk(m):
+    """Stored node-pair blocks of the full symmetric matrix (node graph nnz)."""
+    from betanoox_b200 import _abi
+    import ctypes as C
+    lib = _abi.load()
+    # the node graph of a mesh equals the scalar pattern of its ndpn=1 view
+    conn = np.ascontiguousarray(m.conn, np.int32)
+    fd = np.arange(m.nnode, dtype=np.int32)
+    r = np.zeros(m.nnode, np.uint8)
+    nnz = C.c_longlong()
+    lib.beta_gpu_pattern_lower_host(m.nnode, m.nelem, m.nnpe, 1, conn.ctypes.data, fd.ctypes.data, r.ctypes.data,
+                                    C.byref(nnz), None, None)
+    return 2 * nnz.value - m.nnode
+
+
+# ---- CPU baseline (oracle restatement, test infrastructure) ---------------
+def cpu_baseline(m, args, st_64_iters=None, steps=1):
+    """Bounded sample of the workload on the host cores, extrapolated:
+      * element matrices: a contiguous slice of the mesh, all host threads
+        (the compute half of ESA_Assembler::assembleK);
+      * PCG: a fixed number of iterations of the threaded CSR Jacobi-PCG on
+        the same generator at a smaller size, scaled per stored entry;
+      * iteration count of the full solve: the plain FP64 GPU PCG's (same
+        algorithm and stop rule) when measured, else estimated.
+    """
+    from oracle import beta_oracle as bo
+    from betanoox_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    ne_s = min(m.nelem, args.cpu_elems)
+    t0 = time.perf_counter()
+    st, _ = bo.element_matrices_threaded(m, m.params, m.order, 0, ne_s, threads)
+    t_el = (time.perf_counter() - t0) / ne_s
+    ms = W.cube_hex8(args.cpu_n)
+    s = bo.System(ms)
+    s.set_bc(ms.restrained, ms.prescribed, ms.load)
+    s.build_pattern()
+    s.assemble(ms.params, ms.order)
+    b = s.rhs()
+    nnz_s = 2 * bo.lib().oracle_sys_nnz(s.h) - ms.ndof
+    s.solve_threaded(b, 1e-30, maxit=2, threads=threads)  # builds the CSR copy
+    t0 = time.perf_counter()
+    rc, x, sst = s.solve_threaded(b, 1e-30, maxit=args.cpu_iters, threads=threads)
+    t_it = (time.perf_counter() - t0) / max(1, sst.iterations)
+    nnz_full = 2 * _lower_nnz(m) - m.ndof
+    t_it_full = t_it * nnz_full / nnz_s
+    iters = int(statistics.median(st_64_iters)) if st_64_iters else None
+    if iters is None:
+        iters = int(args.cpu_assumed_iters)
+    t_total = t_el * m.nelem + iters * t_it_full
+    return {"value": m.ndof / t_total, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"extrapolated: element matrices of {ne_s} of {m.nelem} elements "
+                       f"({t_el * 1e6:.2f} us/elem on {threads} threads) + {sst.iterations} threaded Jacobi-PCG "
+                       f"iterations on the {args.cpu_n}^3 cube ({t_it * 1e3:.2f} ms/iter, scaled by stored "
+                       f"entries {nnz_full}/{nnz_s}) x {iters} iterations (plain FP64 GPU PCG count, same stop rule)"),
+            "seconds_full_solve_est": t_total}
+
+
+def _lower_nnz(m):
+    from betanoox_b200 import _abi
+    lib = _abi.load()
+    conn = np.ascontiguousarray(m.conn, np.int32)
+    fd = np.ascontiguousarray(m.first_dof, np.int32)
+    r = np.ascontiguousarray(m.restrained, np.uint8)
+    nnz = C.c_longlong()
+    lib.beta_gpu_pattern_lower_host(m.nnode, m.nelem, m.nnpe, m.ndpn, conn.ctypes.data, fd.ctypes.data,
+                                    r.ctypes.data, C.byref(nnz), None, None)
+    return nnz.value
+
+
+def run_reference(args):
+    ws, rank, local = _dist()
+    if rank != 0:
+        return None
+    m = make_model(args.config, args.n)
+    iters = args.cpu_assumed_iters
+    vals = []
+    cb = None
+    for _ in range(args.warmup and 1):
+        cpu_baseline(m, args, None)
+    for _ in range(args.steps):
+        cb = cpu_baseline(m, args, None)
+        vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * m.ndof / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": {"workload": f"hex8 elasticity cube {m.meta['n']}^3, {m.ndof} dofs", "ndof": m.ndof,
+                       "assumed_iterations": iters},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cube")
+    ap.add_argument("--n", type=int, default=100)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--cpu-elems", type=int, default=100000)
+    ap.add_argument("--cpu-n", type=int, default=30)
+    ap.add_argument("--cpu-iters", type=int, default=30)
+    ap.add_argument("--cpu-assumed-iters", type=int, default=2000)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,153 @@
+"""B200-native element assembly + PCG path for BETA (kaushik-d/BetaNoOx).
+
+The compute path is the C ABI in include/beta_gpu.h, implemented by
+hand-written sm_100a kernels in csrc/ and built in-tree into
+_lib/libbeta_gpu.so.  This package adds a thin Python view of that ABI
+(:class:`Solver`) mirroring BETA's Equations / assembler calls, plus seeded
+workload generators.  Nothing here computes on the CPU in place of the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import BetaGpuError, SolveOpts, SolveStats
+
+__all__ = ["Solver", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
+
+
+def build(force: bool = False) -> str:
+    from .build import build as _b
+    return _b(force=force)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def opts(mode=_abi.MODE_MPIR, precond=_abi.PRECOND_BLOCK_JACOBI, stop_rule=_abi.STOP_RB, tol=1e-10,
+         maxit=100000, inner_tol=1e-5, max_outer=40, use_last_solution=0, check_every=0, profile=False):
+    return SolveOpts(mode, precond, stop_rule, maxit, tol, inner_tol, max_outer, use_last_solution, check_every,
+                     1 if profile else 0)
+
+
+class Solver:
+    """One device-resident finite-element system (a beta_gpu context).
+
+    Mirrors the BETA sequence: mesh/material/boundary upload (ReadMesh,
+    SetElementProperty, loads applyTo), build_pattern (allocateEquationsMatrix),
+    assemble (assembler->assembleK), solve (Equations::solve).
+    """
+
+    def __init__(self, device: int = 0):
+        self.lib = _abi.load()
+        h = C.c_void_p()
+        st = self.lib.beta_gpu_create(C.byref(h), device)
+        if st != _abi.OK:
+            raise BetaGpuError(st, "beta_gpu_create failed (no usable CUDA device?)")
+        self.h = h
+        self.model = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.beta_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what=""):
+        if st != _abi.OK:
+            msg = self.lib.beta_gpu_last_error(self.h)
+            raise BetaGpuError(st, f"{what}: {msg.decode() if msg else ''}")
+        return st
+
+    # -- upload -------------------------------------------------------------
+    def load_model(self, m, params=None, elem_group=None):
+        self.model = m
+        xyz = np.ascontiguousarray(m.xyz, dtype=np.float64)
+        conn = np.ascontiguousarray(m.conn, dtype=np.int32)
+        fd = np.ascontiguousarray(m.first_dof, dtype=np.int32)
+        self._check(self.lib.beta_gpu_mesh_upload(self.h, m.kind, m.ndim, m.nnode, _ptr(xyz), m.nelem, m.nnpe,
+                                                  _ptr(conn), _ptr(fd), m.ndpn, m.order), "mesh_upload")
+        p = np.ascontiguousarray(m.params if params is None else params, dtype=np.float64)
+        eg = None if elem_group is None else np.ascontiguousarray(elem_group, dtype=np.int32)
+        self._check(self.lib.beta_gpu_materials_upload(self.h, p.shape[0], p.shape[1], _ptr(p), _ptr(eg)),
+                    "materials_upload")
+        self.set_bc(m.restrained, m.prescribed, m.load)
+
+    def set_bc(self, restrained, prescribed, load):
+        r = np.ascontiguousarray(restrained, dtype=np.uint8)
+        p = np.ascontiguousarray(prescribed, dtype=np.float64)
+        ld = np.ascontiguousarray(load, dtype=np.float64)
+        self._check(self.lib.beta_gpu_bc_upload(self.h, _ptr(r), _ptr(p), _ptr(ld)), "bc_upload")
+
+    def build_pattern(self):
+        nnz = C.c_longlong(0)
+        self._check(self.lib.beta_gpu_build_pattern(self.h, C.byref(nnz)), "build_pattern")
+        self.nnz_lower = int(nnz.value)
+        return self.nnz_lower
+
+    def pattern_lower(self):
+        n = self.model.ndof
+        rp = np.zeros(n + 1, dtype=np.int64)
+        col = np.zeros(self.nnz_lower, dtype=np.int32)
+        self._check(self.lib.beta_gpu_pattern_lower(self.h, _ptr(rp), _ptr(col)), "pattern_lower")
+        return rp, col
+
+    def assemble(self, precision=_abi.FP32, what=_abi.ASM_K, dt=0.0, alpha=1.0):
+        self._check(self.lib.beta_gpu_assemble(self.h, what, precision, dt, alpha), "assemble")
+
+    def lower_values(self, precision):
+        vals = np.zeros(self.nnz_lower)
+        pl = np.zeros(self.model.ndof)
+        self._check(self.lib.beta_gpu_matrix_lower_values(self.h, precision, _ptr(vals), _ptr(pl)), "lower_values")
+        return vals, pl
+
+    def solve(self, o=None, raise_on_error=True):
+        o = o or opts()
+        st = SolveStats()
+        rc = self.lib.beta_gpu_solve(self.h, C.byref(o), C.byref(st))
+        if raise_on_error:
+            self._check(rc, "solve")
+        return rc, st
+
+    def download(self):
+        u = np.zeros(self.model.ndof)
+        self._check(self.lib.beta_gpu_download(self.h, _ptr(u)), "download")
+        return u
+
+    def matvec(self, x, precision=_abi.FP64):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        self._check(self.lib.beta_gpu_matvec(self.h, precision, _ptr(x), _ptr(y)), "matvec")
+        return y
+
+    def internal_force(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        f = np.zeros_like(u)
+        self._check(self.lib.beta_gpu_internal_force(self.h, _ptr(u), _ptr(f)), "internal_force")
+        return f
+
+    # -- transient diffusion -------------------------------------------------
+    def heat_set_state(self, u0):
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        self._check(self.lib.beta_gpu_heat_set_state(self.h, _ptr(u0)), "heat_set_state")
+
+    def heat_run(self, dt, nsteps, o=None, alpha=1.0):
+        o = o or opts()
+        st = SolveStats()
+        tot = C.c_int(0)
+        self._check(self.lib.beta_gpu_heat_run(self.h, dt, alpha, nsteps, C.byref(o), C.byref(st), C.byref(tot)),
+                    "heat_run")
+        return st, int(tot.value)
+
+    def heat_get_state(self):
+        u = np.zeros(self.model.ndof)
+        self._check(self.lib.beta_gpu_heat_get_state(self.h, _ptr(u)), "heat_get_state")
+        return u

@@ -1,0 +1,126 @@
+"""ctypes binding of the C ABI in include/beta_gpu.h.
+
+Loads the in-tree libbeta_gpu.so.  There is no fallback: if the library is
+missing or fails to load, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libbeta_gpu.so")
+
+# status codes
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_STATE = 3
+MAXIT = 4
+BREAKDOWN = 5
+ERR_NEGDIAG = 6
+ERR_ZERODIAG = 7
+ERR_OOM = 8
+REJECTED = 9
+TIMEOUT = 10
+ERR_NOT_FINITE = 11
+ERR_LOAD_ON_RESTRAINED = 12
+ERR_UNSUPPORTED = 13
+
+QUAD4_PSTRESS = 1
+HEX8_ELASTIC = 2
+HEX8_HEAT = 3
+
+ASM_K = 1
+ASM_MBAR = 2
+
+FP64 = 0
+FP32 = 1
+
+MODE_FP64 = 0
+MODE_MPIR = 1
+PRECOND_JACOBI = 0
+PRECOND_BLOCK_JACOBI = 1
+STOP_REF = 0
+STOP_RB = 1
+
+STATUS_NAMES = {
+    0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_STATE", 4: "MAXIT", 5: "BREAKDOWN",
+    6: "ERR_NEGDIAG", 7: "ERR_ZERODIAG", 8: "ERR_OOM", 9: "REJECTED", 10: "TIMEOUT",
+    11: "ERR_NOT_FINITE", 12: "ERR_LOAD_ON_RESTRAINED", 13: "ERR_UNSUPPORTED",
+}
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int), ("precond", C.c_int), ("stop_rule", C.c_int), ("maxit", C.c_int),
+        ("tol", C.c_double), ("inner_tol", C.c_double), ("max_outer", C.c_int),
+        ("use_last_solution", C.c_int), ("check_every", C.c_int), ("reserved", C.c_int),
+    ]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [
+        ("status", C.c_int), ("iterations", C.c_int), ("outer_iterations", C.c_int), ("reserved", C.c_int),
+        ("final_norm", C.c_double), ("true_rel_residual", C.c_double), ("ms_solve", C.c_double),
+        ("ms_spmv_avg", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
+# Every exported symbol with its signature (kept in step with include/beta_gpu.h).
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+SIGNATURES = {
+    "beta_gpu_create": (_I, [C.POINTER(_P), _I]),
+    "beta_gpu_destroy": (_I, [_P]),
+    "beta_gpu_last_error": (C.c_char_p, [_P]),
+    "beta_gpu_version": (_I, []),
+    "beta_gpu_set_stream": (_I, [_P, _P]),
+    "beta_gpu_counters": (_I, [_P, C.POINTER(C.c_longlong), _I]),
+    "beta_gpu_mesh_upload": (_I, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _I, _I]),
+    "beta_gpu_materials_upload": (_I, [_P, _I, _I, _P, _P]),
+    "beta_gpu_bc_upload": (_I, [_P, _P, _P, _P]),
+    "beta_gpu_build_pattern": (_I, [_P, C.POINTER(C.c_longlong)]),
+    "beta_gpu_pattern_lower": (_I, [_P, _P, _P]),
+    "beta_gpu_pattern_lower_host": (_I, [_I, _I, _I, _I, _P, _P, _P, C.POINTER(C.c_longlong), _P, _P]),
+    "beta_gpu_assemble": (_I, [_P, _I, _I, _D, _D]),
+    "beta_gpu_matrix_lower_values": (_I, [_P, _I, _P, _P]),
+    "beta_gpu_solve": (_I, [_P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "beta_gpu_download": (_I, [_P, _P]),
+    "beta_gpu_matvec": (_I, [_P, _I, _P, _P]),
+    "beta_gpu_internal_force": (_I, [_P, _P, _P]),
+    "beta_gpu_heat_set_state": (_I, [_P, _P]),
+    "beta_gpu_heat_run": (_I, [_P, _D, _D, _I, C.POINTER(SolveOpts), C.POINTER(SolveStats), C.POINTER(_I)]),
+    "beta_gpu_heat_get_state": (_I, [_P, _P]),
+    "beta_gpu_csr_pcg_device": (_I, [_I, _P, _P, _P, _P, _P, _I, _D, _I, _P, C.POINTER(SolveStats)]),
+}
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Loads (once) and returns the library; raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"CUDA extension not built: {p} is missing (run python -m betanoox_b200.build)")
+    lib = C.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class BetaGpuError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status

@@ -1,0 +1,1118 @@
+// beta_gpu.cu -- C ABI of the B200 assembly + PCG path (see include/beta_gpu.h).
+#include "../../include/beta_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "elem_kernels.cuh"
+#include "mf_kernels.cuh"
+#include "pattern.hpp"
+#include "pcg_kernels.cuh"
+
+using namespace betagpu;
+
+namespace {
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (count == n && p) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    else p = nullptr;
+    return e;
+  }
+};
+
+// Gauss-Legendre nodes and weights on [-1,1] by Newton iteration on the
+// three-term Legendre recurrence (the published Golub/Numerical-Recipes
+// construction BETA also uses in gauss.cpp:14-60).
+void gauss_legendre(int k, double* x, double* w) {
+  for (int i = 0; i < (k + 1) / 2; ++i) {
+    double z = std::cos(M_PI * (i + 0.75) / (k + 0.5)), dp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = 0.0;
+      for (int j = 0; j < k; ++j) {
+        double p2 = p1;
+        p1 = p0;
+        p0 = ((2.0 * j + 1.0) * z * p1 - j * p2) / (j + 1.0);
+      }
+      dp = k * (z * p0 - p1) / (z * z - 1.0);
+      double dz = p0 / dp;
+      z -= dz;
+      if (std::fabs(dz) <= 3e-15) break;
+    }
+    x[i] = -z;
+    x[k - 1 - i] = z;
+    w[i] = w[k - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+// BETA local node order (BasicElement.cpp:464-467, 518-525).
+const int kHex[8][3] = {{-1, -1, -1}, {-1, 1, -1}, {-1, 1, 1}, {-1, -1, 1},
+                        {1, -1, -1},  {1, 1, -1},  {1, 1, 1},  {1, -1, 1}};
+const int kQuad[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+
+void make_gauss_table(int ndim, int order, GaussTable& gt) {
+  std::memset(&gt, 0, sizeof(gt));
+  double g[8], gw[8];
+  gauss_legendre(order, g, gw);
+  int ip = 0;
+  if (ndim == 3) {
+    for (int i = 0; i < order; ++i)
+      for (int j = 0; j < order; ++j)
+        for (int k = 0; k < order; ++k, ++ip) {
+          double xi = g[i], et = g[j], ze = g[k];
+          gt.w[ip] = gw[i] * gw[j] * gw[k];
+          for (int a = 0; a < 8; ++a) {
+            double fx = 1 + kHex[a][0] * xi, fy = 1 + kHex[a][1] * et, fz = 1 + kHex[a][2] * ze;
+            gt.N[ip][a] = fx * fy * fz / 8;
+            gt.dN[ip][0][a] = kHex[a][0] * fy * fz / 8;
+            gt.dN[ip][1][a] = kHex[a][1] * fx * fz / 8;
+            gt.dN[ip][2][a] = kHex[a][2] * fx * fy / 8;
+          }
+        }
+  } else {
+    for (int i = 0; i < order; ++i)
+      for (int k = 0; k < order; ++k, ++ip) {
+        double xi = g[i], et = g[k];
+        gt.w[ip] = gw[i] * gw[k];
+        for (int a = 0; a < 4; ++a) {
+          double fx = 1 + kQuad[a][0] * xi, fy = 1 + kQuad[a][1] * et;
+          gt.N[ip][a] = fx * fy / 4;
+          gt.dN[ip][0][a] = kQuad[a][0] * fy / 4;
+          gt.dN[ip][1][a] = kQuad[a][1] * fx / 4;
+        }
+      }
+  }
+  gt.nip = ip;
+}
+
+}  // namespace
+
+struct beta_gpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  long long n_launch = 0, n_h2d = 0, n_d2h = 0;
+  int nsm = 148;
+  std::string err;
+
+  // mesh
+  int kind = 0, ndim = 0, nnode = 0, nelem = 0, nnpe = 0, ndpn = 0, ndof = 0, order = 0;
+  std::vector<int> h_conn, h_first_dof;
+  DBuf<double> xyz;
+  DBuf<int> conn;
+  GaussTable h_gt;
+  DBuf<GaussTable> gt;
+  // materials
+  int ngroups = 0, nparams = 0;
+  DBuf<double> gparams;
+  DBuf<int> egroup;
+  bool have_egroup = false, have_mat = false;
+  // boundary conditions
+  std::vector<unsigned char> h_rest;
+  DBuf<unsigned char> rest;
+  DBuf<double> presc, load;
+  bool have_bc = false;
+  // structure
+  bool have_pattern = false;
+  HostPattern P;
+  DBuf<int> elems, slot, nrp, bsoff, bcol, ndiag, soff, scol;
+  DBuf<long long> ssoff, sdiag;
+  // matrices
+  DBuf<double> sval, pseudo;
+  DBuf<float> bval;
+  bool have64 = false, have32 = false;
+  int what64 = 0, what32 = 0;
+  double kscale64 = 1, mscale64 = 0, kscale32 = 1, mscale32 = 0;
+  // solver workspace
+  DBuf<PcgState> st;
+  DBuf<double> partials, sums;
+  DBuf<unsigned> flags, ticket;
+  PcgState* h_st = nullptr;   // pinned
+  double* h_sums = nullptr;   // pinned
+  DBuf<double> b64, x64, r64, p64, q64, d64, y64, t64;
+  DBuf<float> v32[5];         // node-layout float vectors: x(d), r, p, q, spare
+  DBuf<float> minv;
+  int minv_kind = -1;
+  // solution / transient state
+  DBuf<double> u, us;
+  bool have_u = false, have_us = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> evs;
+  int max_grid = 0;
+};
+
+namespace {
+
+int fail(beta_gpu_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(beta_gpu_ctx* c, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();
+  return fail(c, e == cudaErrorMemoryAllocation ? BETA_GPU_ERR_OOM : BETA_GPU_ERR_CUDA, m);
+}
+
+#define CK(call)                                       \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+  } while (0)
+
+#define CKL(what)                                          \
+  do {                                                     \
+    cudaError_t e_ = cudaGetLastError();                   \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, what);  \
+  } while (0)
+
+// Kernel launch on the context stream, counted.
+template <typename... KArgs, typename... Args>
+void launch(beta_gpu_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, Args... args) {
+  k<<<grid, block, smem, c->stream>>>(args...);
+  ++c->n_launch;
+}
+
+cudaError_t h2d(beta_gpu_ctx* c, void* dst, const void* src, size_t bytes) {
+  c->n_h2d += (long long)bytes;
+  return h2d(c, dst, src, bytes);
+}
+
+cudaError_t d2h(beta_gpu_ctx* c, void* dst, const void* src, size_t bytes) {
+  c->n_d2h += (long long)bytes;
+  return d2h(c, dst, src, bytes);
+}
+
+int grid_for(beta_gpu_ctx* c, long long work_items, int per_block) {
+  long long g = (work_items + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > c->max_grid) g = c->max_grid;
+  return (int)g;
+}
+
+template <typename T>
+int upload(beta_gpu_ctx* c, DBuf<T>& d, const T* h, size_t n) {
+  CK(d.alloc(n));
+  if (n) CK(h2d(c, d.p, h, n * sizeof(T)));
+  return BETA_GPU_OK;
+}
+
+bool all_finite(const double* a, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(a[i])) return false;
+  return true;
+}
+
+void invalidate_matrices(beta_gpu_ctx* c) {
+  c->have64 = c->have32 = false;
+  c->minv_kind = -1;
+}
+
+// ---- element launches (colour by colour) ----------------------------------
+ElemArgs elem_args(beta_gpu_ctx* c) {
+  ElemArgs A;
+  A.xyz = c->xyz.p;
+  A.conn = c->conn.p;
+  A.gparams = c->gparams.p;
+  A.egroup = c->have_egroup ? c->egroup.p : nullptr;
+  A.nparams = c->nparams;
+  A.nip = c->h_gt.nip;
+  A.gt = c->gt.p;
+  A.slot = c->slot.p;
+  A.nrp = c->nrp.p;
+  A.rest = c->rest.p;
+  A.presc = c->presc.p;
+  A.bsoff = c->bsoff.p;
+  A.bval = c->bval.p;
+  A.soff = c->soff.p;
+  A.ssoff = c->ssoff.p;
+  A.sval = c->sval.p;
+  A.pseudo = c->pseudo.p;
+  A.kscale = 1.0;
+  A.mscale = 0.0;
+  A.flags = c->flags.p;
+  return A;
+}
+
+template <typename T>
+int launch_assembly(beta_gpu_ctx* c, const ElemArgs& A) {
+  const int nip = c->h_gt.nip;
+  for (int col = 0; col < c->P.ncolor; ++col) {
+    const int beg = c->P.color_ptr[col], nel = c->P.color_ptr[col + 1] - beg;
+    if (nel == 0) continue;
+    const int* el = c->elems.p + beg;
+    if (c->kind == BETA_GPU_HEX8_ELASTIC) {
+      size_t sm = (size_t)nip * 33 * sizeof(T);
+      launch(c, k_asm_hex8_elastic<T>, grid_for(c, nel, 8), 256, sm, A, el, nel);
+    } else if (c->kind == BETA_GPU_HEX8_HEAT) {
+      size_t sm = (size_t)nip * 33 * sizeof(T);
+      launch(c, k_asm_hex8_heat<T>, grid_for(c, nel, 8), 256, sm, A, el, nel);
+    } else {
+      size_t sm = (size_t)nip * 13 * sizeof(T);
+      launch(c, k_asm_quad4_pstress<T>, grid_for(c, nel, 16), 256, sm, A, el, nel);
+    }
+    CKL("element kernel launch");
+  }
+  return BETA_GPU_OK;
+}
+
+// y = K (c1 w1 + c2 w2) + cm M w1 (FP64, matrix-free), y zeroed first.
+int mf_apply(beta_gpu_ctx* c, double c1, const double* w1, double c2, const double* w2, double cm,
+             double* y) {
+  MfArgs A;
+  A.xyz = c->xyz.p;
+  A.conn = c->conn.p;
+  A.gparams = c->gparams.p;
+  A.egroup = c->have_egroup ? c->egroup.p : nullptr;
+  A.nparams = c->nparams;
+  A.nip = c->h_gt.nip;
+  A.gt = c->gt.p;
+  A.c1 = c1;
+  A.c2 = c2;
+  A.cm = cm;
+  CK(cudaMemsetAsync(y, 0, sizeof(double) * c->ndof, c->stream));
+  for (int col = 0; col < c->P.ncolor; ++col) {
+    const int beg = c->P.color_ptr[col], nel = c->P.color_ptr[col + 1] - beg;
+    if (nel == 0) continue;
+    const int* el = c->elems.p + beg;
+    if (c->kind == BETA_GPU_HEX8_ELASTIC)
+      launch(c, k_mf_hex8_elastic, grid_for(c, nel, 32), 256, 0, A, el, nel, w1, w2, y);
+    else if (c->kind == BETA_GPU_HEX8_HEAT)
+      launch(c, k_mf_hex8_heat, grid_for(c, nel, 32), 256, 0, A, el, nel, w1, w2, y);
+    else
+      launch(c, k_mf_quad4_pstress, grid_for(c, nel, 64), 256, 0, A, el, nel, w1, w2, y);
+    CKL("matrix-free kernel launch");
+  }
+  return BETA_GPU_OK;
+}
+
+int read_flags(beta_gpu_ctx* c, unsigned* out) {
+  CK(d2h(c, c->h_sums, c->flags.p, sizeof(unsigned)));
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(out, c->h_sums, sizeof(unsigned));
+  return BETA_GPU_OK;
+}
+
+int read_state(beta_gpu_ctx* c, PcgState* out) {
+  CK(d2h(c, c->h_st, c->st.p, sizeof(PcgState)));
+  CK(cudaStreamSynchronize(c->stream));
+  *out = *c->h_st;
+  return BETA_GPU_OK;
+}
+
+int read_sums(beta_gpu_ctx* c, int n, double* out) {
+  CK(d2h(c, c->h_sums, c->sums.p, sizeof(double) * n));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n; ++i) out[i] = c->h_sums[i];
+  return BETA_GPU_OK;
+}
+
+int init_state(beta_gpu_ctx* c, int rule, double tol, int maxit) {
+  PcgState s;
+  std::memset(&s, 0, sizeof(s));
+  s.rule = rule;
+  s.tol2 = tol * tol;
+  s.maxit = maxit;
+  *c->h_st = s;
+  CK(h2d(c, c->st.p, c->h_st, sizeof(PcgState)));
+  return BETA_GPU_OK;
+}
+
+int ensure_events(beta_gpu_ctx* c, int n) {
+  while ((int)c->evs.size() < n) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    c->evs.push_back(e);
+  }
+  return BETA_GPU_OK;
+}
+
+struct ProfAcc {
+  bool on = false;
+  double ms = 0.0;
+  long long launches = 0;
+};
+
+// Runs PCG iterations in chunks until the device state says done.  kind 0:
+// scalar FP64; kind ND (1..3): node-block FP32.
+template <int ND>
+int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
+  const int ce = std::max(1, check_every);
+  int rc;
+  if (prof && prof->on && (rc = ensure_events(c, 2 * ce)) != BETA_GPU_OK) return rc;
+  for (;;) {
+    for (int k = 0; k < ce; ++k) {
+      if (prof && prof->on) CK(cudaEventRecord(c->evs[2 * k], c->stream));
+      if constexpr (ND == 0) {
+        ScalarMat A{c->ndof, c->P.nsslice, c->ssoff.p, c->scol.p, c->sval.p};
+        launch(c, k_spmv_dot_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, 
+            A, c->p64.p, c->q64.p, c->st.p, c->partials.p);
+      } else {
+        using V = typename NV<ND>::T;
+        BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p};
+        launch(c, k_spmv_dot_b<ND>, grid_for(c, (long long)c->P.nslice * 32, 256), 256, 0, 
+            A, (const V*)c->v32[2].p, (V*)c->v32[3].p, c->st.p, c->partials.p);
+      }
+      if (prof && prof->on) CK(cudaEventRecord(c->evs[2 * k + 1], c->stream));
+      if constexpr (ND == 0) {
+        launch(c, k_update_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->x64.p, c->r64.p, c->p64.p,
+                                                                     c->q64.p, c->d64.p, c->st.p, c->partials.p);
+        launch(c, k_pupd_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->p64.p, c->r64.p, c->d64.p, c->st.p);
+      } else {
+        using V = typename NV<ND>::T;
+        launch(c, k_update_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
+            c->nnode, (V*)c->v32[0].p, (V*)c->v32[1].p, (const V*)c->v32[2].p, (const V*)c->v32[3].p,
+            (const V*)c->minv.p, c->st.p, c->partials.p);
+        launch(c, k_pupd_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
+            c->nnode, (V*)c->v32[2].p, (const V*)c->v32[1].p, (const V*)c->minv.p, c->st.p);
+      }
+    }
+    CKL("pcg launch");
+    int before = c->h_st->iter;
+    PcgState s;
+    if ((rc = read_state(c, &s)) != BETA_GPU_OK) return rc;
+    if (prof && prof->on) {
+      int real = std::min(ce, std::max(0, s.iter - before) + (s.done && s.status == kStatusBreakdown ? 1 : 0));
+      for (int k = 0; k < real; ++k) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->evs[2 * k], c->evs[2 * k + 1]));
+        prof->ms += ms;
+        prof->launches += 1;
+      }
+    }
+    if (s.done) {
+      *out = s;
+      return BETA_GPU_OK;
+    }
+  }
+}
+
+int ensure_workspace(beta_gpu_ctx* c) {
+  const size_t n = c->ndof;
+  for (DBuf<double>* b : {&c->b64, &c->x64, &c->r64, &c->p64, &c->q64, &c->d64, &c->y64, &c->t64})
+    CK(b->alloc(n));
+  const size_t nv = (size_t)c->nnode * (c->ndpn == 3 ? 4 : c->ndpn);
+  for (auto& v : c->v32) CK(v.alloc(nv));
+  CK(c->minv.alloc(nv * c->ndpn));
+  CK(c->u.alloc(n));
+  return BETA_GPU_OK;
+}
+
+template <int ND>
+int compute_minv(beta_gpu_ctx* c, int precond) {
+  if (c->minv_kind == precond) return BETA_GPU_OK;
+  CK(cudaMemsetAsync(c->flags.p, 0, sizeof(unsigned), c->stream));
+  launch(c, k_minv_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
+      c->nnode, c->bsoff.p, c->ndiag.p, c->bval.p, (typename NV<ND>::T*)c->minv.p,
+      precond == BETA_GPU_PRECOND_JACOBI ? 1 : 0, c->flags.p);
+  CKL("k_minv_b");
+  unsigned f = 0;
+  int rc = read_flags(c, &f);
+  if (rc) return rc;
+  if (f & 16u) return fail(c, BETA_GPU_ERR_NEGDIAG, "non-positive diagonal in the assembled matrix");
+  c->minv_kind = precond;
+  return BETA_GPU_OK;
+}
+
+// Mixed-precision refinement on A64 x = b with
+//   residual r = rest ? 0 : load - [K (c1 x + c2 w2) + cm M x]
+// (FP64 matrix-free) and inner FP32 node-block PCG on the assembled matrix.
+// x64 holds the initial iterate (prescribed values on restrained dofs) on
+// entry and the solution on exit.  bnorm is ||b||.
+template <int ND>
+int mpir_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c2, const double* w2,
+              double cm, const double* loadv, double bnorm, beta_gpu_solve_stats* stats, ProfAcc* prof) {
+  int rc;
+  using V = typename NV<ND>::T;
+  if ((rc = compute_minv<ND>(c, o->precond)) != BETA_GPU_OK) return rc;
+  const int maxit = o->maxit > 0 ? o->maxit : 10000;
+  const int max_outer = o->max_outer > 0 ? o->max_outer : 30;
+  const double itol = o->inner_tol > 0 ? o->inner_tol : 1e-5;
+  const int ce = o->check_every > 0 ? o->check_every : std::max(8, std::min(64, c->ndof / 20000));
+  int total = 0, outer = 0, status = BETA_GPU_OK;
+  double q = 1.0;
+  for (;;) {
+    if ((rc = mf_apply(c, c1, c->x64.p, c2, w2, cm, c->y64.p)) != BETA_GPU_OK) return rc;
+    launch(c, k_residual64, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->rest.p, loadv, c->y64.p,
+                                                                    c->x64.p, c->r64.p, c->sums.p,
+                                                                    c->partials.p, c->ticket.p);
+    CKL("k_residual64");
+    double s2[2];
+    if ((rc = read_sums(c, 2, s2)) != BETA_GPU_OK) return rc;
+    const double rn = std::sqrt(s2[0]);
+    if (o->stop_rule == BETA_GPU_STOP_REF) q = s2[1] > 0 ? rn / std::sqrt(s2[1]) : (rn == 0 ? 0 : 1e300);
+    else q = bnorm > 0 ? rn / bnorm : rn;
+    if (!std::isfinite(q)) { status = BETA_GPU_BREAKDOWN; break; }
+    if (q < o->tol || rn == 0.0) break;
+    if (outer >= max_outer || total >= maxit) { status = BETA_GPU_MAXIT; break; }
+    ++outer;
+    launch(c, k_to_node32<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->r64.p, 1.0 / rn,
+                                                                        (V*)c->v32[1].p);
+    if ((rc = init_state(c, kStopRel, itol, std::max(1, maxit - total))) != BETA_GPU_OK) return rc;
+    launch(c, k_start_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
+        c->nnode, (V*)c->v32[0].p, (const V*)c->v32[1].p, (V*)c->v32[2].p, (const V*)c->minv.p, c->st.p,
+        c->partials.p);
+    CKL("k_start_b");
+    PcgState s;
+    if ((rc = pcg_loop<ND>(c, ce, prof, &s)) != BETA_GPU_OK) return rc;
+    total += s.iter;
+    if (s.status == kStatusBreakdown && s.iter == 0) { status = BETA_GPU_BREAKDOWN; break; }
+    launch(c, k_axpy_from_node32<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->x64.p, rn,
+                                                                               (const V*)c->v32[0].p);
+    CKL("k_axpy_from_node32");
+  }
+  if (stats) {
+    stats->status = status;
+    stats->iterations = total;
+    stats->outer_iterations = outer;
+    stats->final_norm = q;
+  }
+  return status;
+}
+
+int mpir_dispatch(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c2, const double* w2,
+                  double cm, const double* loadv, double bnorm, beta_gpu_solve_stats* stats, ProfAcc* prof) {
+  switch (c->ndpn) {
+    case 1: return mpir_core<1>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof);
+    case 2: return mpir_core<2>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof);
+    default: return mpir_core<3>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof);
+  }
+}
+
+// Plain FP64 Jacobi-PCG on the assembled scalar matrix: b64 must hold the
+// right-hand side, x64 the initial guess.
+int fp64_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve_stats* stats, ProfAcc* prof) {
+  int rc;
+  const int n = c->ndof;
+  ScalarMat A{n, c->P.nsslice, c->ssoff.p, c->scol.p, c->sval.p};
+  CK(cudaMemsetAsync(c->flags.p, 0, sizeof(unsigned), c->stream));
+  launch(c, k_dinv_s, grid_for(c, n, 256), 256, 0, n, c->sdiag.p, c->sval.p, c->d64.p, c->flags.p);
+  CKL("k_dinv_s");
+  unsigned f = 0;
+  if ((rc = read_flags(c, &f)) != BETA_GPU_OK) return rc;
+  if (f & 8u) return fail(c, BETA_GPU_ERR_ZERODIAG, "zero diagonal (LargeMatrix::CheckAndFixZeroDiagonal)");
+  if (f & 16u) return fail(c, BETA_GPU_ERR_NEGDIAG, "negative diagonal (LargeMatrix::CheckAndFixZeroDiagonal)");
+  launch(c, k_spmv_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, A, c->x64.p, c->r64.p, c->b64.p);
+  const int rule = o->stop_rule == BETA_GPU_STOP_REF ? kStopRef : kStopRB;
+  if ((rc = init_state(c, rule, o->tol, o->maxit > 0 ? o->maxit : 10000)) != BETA_GPU_OK) return rc;
+  launch(c, k_start_s, grid_for(c, n, 256), 256, 0, n, c->x64.p, c->r64.p, c->b64.p, c->d64.p, c->p64.p,
+                                                        c->st.p, c->partials.p);
+  CKL("k_start_s");
+  const int ce = o->check_every > 0 ? o->check_every : std::max(8, std::min(64, n / 20000));
+  PcgState s;
+  if ((rc = pcg_loop<0>(c, ce, prof, &s)) != BETA_GPU_OK) return rc;
+  // true residual ||b - A x|| / ||b||
+  launch(c, k_spmv_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, A, c->x64.p, c->t64.p, c->b64.p);
+  launch(c, k_norm2_diff, grid_for(c, n, 256), 256, 0, n, c->t64.p, nullptr, c->sums.p, c->partials.p,
+                                                           c->ticket.p);
+  CKL("true residual");
+  double rr;
+  if ((rc = read_sums(c, 1, &rr)) != BETA_GPU_OK) return rc;
+  int status = s.status == kStatusOk ? BETA_GPU_OK : (s.status == kStatusMaxit ? BETA_GPU_MAXIT : BETA_GPU_BREAKDOWN);
+  if (stats) {
+    stats->status = status;
+    stats->iterations = s.iter;
+    stats->outer_iterations = 0;
+    stats->final_norm = s.last;
+    stats->true_rel_residual = s.bb > 0 ? std::sqrt(rr / s.bb) : std::sqrt(rr);
+  }
+  return status;
+}
+
+}  // namespace
+
+// =============================== C ABI ======================================
+extern "C" {
+
+int beta_gpu_version(void) { return 10000; }
+
+const char* beta_gpu_last_error(const beta_gpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int beta_gpu_create(beta_gpu_ctx** out, int device) {
+  if (!out) return BETA_GPU_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<beta_gpu_ctx> c(new beta_gpu_ctx());
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { cudaGetLastError(); return BETA_GPU_ERR_CUDA; }
+  beta_gpu_ctx* cp = c.get();
+  {
+    beta_gpu_ctx* c = cp;  // for CK
+    CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+    c->max_grid = c->nsm * 8;
+    CK(c->st.alloc(1));
+    CK(c->partials.alloc((size_t)c->max_grid * 4 + 64));
+    CK(c->sums.alloc(8));
+    CK(c->flags.alloc(1));
+    CK(c->ticket.alloc(1));
+    CK(cudaMemset(c->ticket.p, 0, sizeof(unsigned)));
+    CK(cudaMemset(c->flags.p, 0, sizeof(unsigned)));
+    CK(cudaMallocHost(&c->h_st, sizeof(PcgState)));
+    CK(cudaMallocHost(&c->h_sums, 8 * sizeof(double)));
+    std::memset(c->h_st, 0, sizeof(PcgState));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+  }
+  *out = c.release();
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_destroy(beta_gpu_ctx* c) {
+  if (!c) return BETA_GPU_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto e : c->evs) cudaEventDestroy(e);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->h_st) cudaFreeHost(c->h_st);
+  if (c->h_sums) cudaFreeHost(c->h_sums);
+  cudaStream_t s = c->own_stream;
+  delete c;  // DBuf destructors free device memory
+  if (s) cudaStreamDestroy(s);
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_set_stream(beta_gpu_ctx* c, void* stream) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->stream));
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_counters(const beta_gpu_ctx* c, long long* out, int n) {
+  if (!c || !out || n < 0 || n > 3) return BETA_GPU_ERR_ARG;
+  const long long v[3] = {c->n_launch, c->n_h2d, c->n_d2h};
+  for (int i = 0; i < n; ++i) out[i] = v[i];
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_mesh_upload(beta_gpu_ctx* c, int kind, int ndim, int nnode, const double* xyz, int nelem,
+                         int nnpe, const int* conn, const int* first_dof, int ndpn, int order) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  int want_nnpe = 0, want_ndim = 0, want_ndpn = 0;
+  switch (kind) {
+    case BETA_GPU_QUAD4_PSTRESS: want_nnpe = 4; want_ndim = 2; want_ndpn = 2; break;
+    case BETA_GPU_HEX8_ELASTIC: want_nnpe = 8; want_ndim = 3; want_ndpn = 3; break;
+    case BETA_GPU_HEX8_HEAT: want_nnpe = 8; want_ndim = 3; want_ndpn = 1; break;
+    default: return fail(c, BETA_GPU_ERR_UNSUPPORTED, "unknown element kind");
+  }
+  if (nnpe != want_nnpe || ndim != want_ndim || ndpn != want_ndpn)
+    return fail(c, BETA_GPU_ERR_ARG, "nnpe/ndim/ndof_per_node do not match the element kind");
+  if (nnode <= 0 || nelem <= 0 || !xyz || !conn || !first_dof)
+    return fail(c, BETA_GPU_ERR_ARG, "empty mesh");
+  if (order < 1 || order > 4) return fail(c, BETA_GPU_ERR_ARG, "integration order must be 1..4");
+  if ((long long)nnode * ndpn > 2000000000LL) return fail(c, BETA_GPU_ERR_ARG, "too many dofs");
+  if (!all_finite(xyz, (size_t)nnode * ndim)) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite coordinates");
+  for (long long k = 0; k < (long long)nelem * nnpe; ++k)
+    if (conn[k] < 0 || conn[k] >= nnode) return fail(c, BETA_GPU_ERR_ARG, "connectivity out of range");
+  c->kind = kind; c->ndim = ndim; c->nnode = nnode; c->nelem = nelem; c->nnpe = nnpe; c->ndpn = ndpn;
+  c->ndof = nnode * ndpn; c->order = order;
+  c->h_conn.assign(conn, conn + (size_t)nelem * nnpe);
+  c->h_first_dof.assign(first_dof, first_dof + nnode);
+  int rc;
+  if ((rc = upload(c, c->xyz, xyz, (size_t)nnode * ndim))) return rc;
+  if ((rc = upload(c, c->conn, conn, (size_t)nelem * nnpe))) return rc;
+  make_gauss_table(ndim, order, c->h_gt);
+  if ((rc = upload(c, c->gt, &c->h_gt, 1))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_pattern = false;
+  c->have_bc = false;
+  c->have_mat = false;
+  c->have_u = c->have_us = false;
+  invalidate_matrices(c);
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_materials_upload(beta_gpu_ctx* c, int ngroups, int nparams, const double* gp, const int* eg) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  if (!c->nelem) return fail(c, BETA_GPU_ERR_STATE, "upload the mesh first");
+  cudaSetDevice(c->device);
+  int want = c->kind == BETA_GPU_HEX8_ELASTIC ? 9 : 4;
+  if (nparams != want) return fail(c, BETA_GPU_ERR_ARG, "wrong number of material parameters for the element kind");
+  if (ngroups <= 0 || !gp) return fail(c, BETA_GPU_ERR_ARG, "no material groups");
+  if (!eg && ngroups != c->nelem) return fail(c, BETA_GPU_ERR_ARG, "without elem_group there must be one group per element");
+  if (!all_finite(gp, (size_t)ngroups * nparams)) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite material parameters");
+  if (eg)
+    for (int e = 0; e < c->nelem; ++e)
+      if (eg[e] < 0 || eg[e] >= ngroups) return fail(c, BETA_GPU_ERR_ARG, "elem_group out of range");
+  int rc;
+  if ((rc = upload(c, c->gparams, gp, (size_t)ngroups * nparams))) return rc;
+  c->have_egroup = eg != nullptr;
+  if (eg && (rc = upload(c, c->egroup, eg, (size_t)c->nelem))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->ngroups = ngroups;
+  c->nparams = nparams;
+  c->have_mat = true;
+  invalidate_matrices(c);
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_bc_upload(beta_gpu_ctx* c, const unsigned char* restrained, const double* prescribed,
+                       const double* load) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  if (!c->ndof) return fail(c, BETA_GPU_ERR_STATE, "upload the mesh first");
+  cudaSetDevice(c->device);
+  const size_t n = c->ndof;
+  std::vector<unsigned char> r(n, 0);
+  if (restrained)
+    for (size_t i = 0; i < n; ++i) r[i] = restrained[i] ? 1 : 0;
+  std::vector<double> pz(n, 0.0), lz(n, 0.0);
+  const double* p = prescribed ? prescribed : pz.data();
+  const double* l = load ? load : lz.data();
+  if (!all_finite(p, n) || !all_finite(l, n)) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite boundary data");
+  for (size_t i = 0; i < n; ++i)
+    if (r[i] && l[i] != 0.0)
+      return fail(c, BETA_GPU_ERR_LOAD_ON_RESTRAINED, "Cannot add load to a restrained degree of freedom.");
+  if (c->have_pattern && r != c->h_rest) {
+    c->have_pattern = false;
+    invalidate_matrices(c);
+  }
+  c->h_rest = r;
+  int rc;
+  if ((rc = upload(c, c->rest, r.data(), n))) return rc;
+  if ((rc = upload(c, c->presc, p, n))) return rc;
+  if ((rc = upload(c, c->load, l, n))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_bc = true;
+  if (c->have64 || c->have32) invalidate_matrices(c);  // pseudo load depends on prescribed values
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_build_pattern(beta_gpu_ctx* c, long long* nnz_lower) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  if (!c->ndof || !c->have_bc) return fail(c, BETA_GPU_ERR_STATE, "upload mesh and boundary conditions first");
+  cudaSetDevice(c->device);
+  std::string msg = build_pattern(c->nnode, c->nelem, c->nnpe, c->ndpn, c->h_conn.data(), c->h_first_dof.data(),
+                                  c->h_rest.data(), c->P);
+  if (!msg.empty()) return fail(c, BETA_GPU_ERR_UNSUPPORTED, msg);
+  const HostPattern& P = c->P;
+  int rc;
+  if ((rc = upload(c, c->elems, P.elem_by_color.data(), P.elem_by_color.size()))) return rc;
+  if ((rc = upload(c, c->slot, P.slot.data(), P.slot.size()))) return rc;
+  if ((rc = upload(c, c->nrp, P.nrp.data(), P.nrp.size()))) return rc;
+  if ((rc = upload(c, c->bsoff, P.bsoff.data(), P.bsoff.size()))) return rc;
+  if ((rc = upload(c, c->bcol, P.bcol.data(), P.bcol.size()))) return rc;
+  if ((rc = upload(c, c->ndiag, P.ndiag.data(), P.ndiag.size()))) return rc;
+  if ((rc = upload(c, c->soff, P.soff.data(), P.soff.size()))) return rc;
+  if ((rc = upload(c, c->ssoff, P.ssoff.data(), P.ssoff.size()))) return rc;
+  if ((rc = upload(c, c->scol, P.scol.data(), P.scol.size()))) return rc;
+  if ((rc = upload(c, c->sdiag, P.sdiag.data(), P.sdiag.size()))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_pattern = true;
+  invalidate_matrices(c);
+  if (nnz_lower) *nnz_lower = P.nnz_lower;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_pattern_lower(beta_gpu_ctx* c, long long* row_ptr, int* col) {
+  if (!c || !row_ptr || !col) return BETA_GPU_ERR_ARG;
+  if (!c->have_pattern) return fail(c, BETA_GPU_ERR_STATE, "build the pattern first");
+  export_lower_pattern(c->P, c->h_rest.data(), row_ptr, col);
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_pattern_lower_host(int nnode, int nelem, int nnpe, int ndpn, const int* conn, const int* first_dof,
+                                const unsigned char* restrained, long long* nnz_lower, long long* row_ptr, int* col) {
+  if (!conn || !first_dof || !restrained || !nnz_lower) return BETA_GPU_ERR_ARG;
+  HostPattern P;
+  std::vector<unsigned char> r((size_t)nnode * ndpn);
+  for (size_t i = 0; i < r.size(); ++i) r[i] = restrained[i] ? 1 : 0;
+  std::string msg = build_pattern(nnode, nelem, nnpe, ndpn, conn, first_dof, r.data(), P);
+  if (!msg.empty()) return BETA_GPU_ERR_UNSUPPORTED;
+  *nnz_lower = P.nnz_lower;
+  if (row_ptr && col) export_lower_pattern(P, r.data(), row_ptr, col);
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_assemble(beta_gpu_ctx* c, int what, int precision, double dt, double alpha) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  if (!c->have_pattern || !c->have_mat) return fail(c, BETA_GPU_ERR_STATE, "pattern and materials required");
+  cudaSetDevice(c->device);
+  double ks = 1.0, ms = 0.0;
+  if (what == BETA_GPU_ASM_MBAR) {
+    if (c->kind != BETA_GPU_HEX8_HEAT) return fail(c, BETA_GPU_ERR_UNSUPPORTED, "Mbar assembly is for diffusion elements");
+    if (!(dt > 0)) return fail(c, BETA_GPU_ERR_ARG, "dt must be positive");
+    ks = alpha * dt / dt;  // (a1 K + M)/dt with a1 = alpha*dt (formK_s, HeatTransferElement3DTransient.cpp:341)
+    ms = 1.0 / dt;
+  } else if (what != BETA_GPU_ASM_K) {
+    return fail(c, BETA_GPU_ERR_ARG, "unknown assembly action");
+  }
+  ElemArgs A = elem_args(c);
+  A.kscale = ks;
+  A.mscale = ms;
+  CK(cudaMemsetAsync(c->flags.p, 0, sizeof(unsigned), c->stream));
+  int rc;
+  if (precision == BETA_GPU_FP64) {
+    CK(c->sval.alloc(c->P.ssoff.back()));
+    CK(c->pseudo.alloc(c->ndof));
+    CK(cudaMemsetAsync(c->sval.p, 0, sizeof(double) * c->sval.n, c->stream));
+    CK(cudaMemsetAsync(c->pseudo.p, 0, sizeof(double) * c->ndof, c->stream));
+    A.sval = c->sval.p;
+    A.pseudo = c->pseudo.p;
+    if ((rc = launch_assembly<double>(c, A))) return rc;
+    launch(c, k_set_restrained_diag64, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->rest.p, c->sdiag.p,
+                                                                              c->sval.p);
+    CKL("k_set_restrained_diag64");
+    c->have64 = true;
+    c->what64 = what;
+    c->kscale64 = ks;
+    c->mscale64 = ms;
+  } else if (precision == BETA_GPU_FP32) {
+    const size_t nv = (size_t)c->P.nchunk * 32 * c->ndpn * c->ndpn;
+    CK(c->bval.alloc(nv));
+    CK(cudaMemsetAsync(c->bval.p, 0, sizeof(float) * nv, c->stream));
+    A.bval = c->bval.p;
+    if ((rc = launch_assembly<float>(c, A))) return rc;
+    const int g = grid_for(c, c->nnode, 256);
+    if (c->ndpn == 3) launch(c, k_set_restrained_diag32<3>, g, 256, 0, c->nnode, c->rest.p, c->bsoff.p, c->ndiag.p, c->bval.p);
+    else if (c->ndpn == 2) launch(c, k_set_restrained_diag32<2>, g, 256, 0, c->nnode, c->rest.p, c->bsoff.p, c->ndiag.p, c->bval.p);
+    else launch(c, k_set_restrained_diag32<1>, g, 256, 0, c->nnode, c->rest.p, c->bsoff.p, c->ndiag.p, c->bval.p);
+    CKL("k_set_restrained_diag32");
+    c->have32 = true;
+    c->what32 = what;
+    c->kscale32 = ks;
+    c->mscale32 = ms;
+    c->minv_kind = -1;
+  } else {
+    return fail(c, BETA_GPU_ERR_ARG, "unknown precision");
+  }
+  unsigned f = 0;
+  if ((rc = read_flags(c, &f))) return rc;
+  if (f & kFlagNegDiag) {
+    if (precision == BETA_GPU_FP64) c->have64 = false; else c->have32 = false;
+    return fail(c, BETA_GPU_ERR_NEGDIAG, "BasicElement::bad diagonal in K (element diagonal <= 0)");
+  }
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_matrix_lower_values(beta_gpu_ctx* c, int precision, double* vals, double* pseudo_load) {
+  if (!c || !vals) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (precision == BETA_GPU_FP64) {
+    if (!c->have64) return fail(c, BETA_GPU_ERR_STATE, "no FP64 matrix assembled");
+    std::vector<double> h(c->sval.n);
+    CK(d2h(c, h.data(), c->sval.p, sizeof(double) * h.size()));
+    if (pseudo_load)
+      CK(d2h(c, pseudo_load, c->pseudo.p, sizeof(double) * c->ndof));
+    CK(cudaStreamSynchronize(c->stream));
+    export_lower_values_scalar(c->P, c->h_rest.data(), h.data(), vals);
+  } else {
+    if (!c->have32) return fail(c, BETA_GPU_ERR_STATE, "no FP32 matrix assembled");
+    std::vector<float> h(c->bval.n);
+    CK(d2h(c, h.data(), c->bval.p, sizeof(float) * h.size()));
+    CK(cudaStreamSynchronize(c->stream));
+    export_lower_values_block(c->P, c->h_rest.data(), h.data(), vals);
+    if (pseudo_load) std::memset(pseudo_load, 0, sizeof(double) * c->ndof);
+  }
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_solve(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve_stats* stats) {
+  if (!c || !o) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  const int n = c->ndof;
+  const bool last = o->use_last_solution && c->have_u;
+  ProfAcc prof;
+  prof.on = o->reserved & 1;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int status;
+  if (o->mode == BETA_GPU_MODE_FP64) {
+    if (!c->have64) return fail(c, BETA_GPU_ERR_STATE, "assemble in FP64 before an FP64 solve");
+    if (c->what64 != BETA_GPU_ASM_K) return fail(c, BETA_GPU_ERR_STATE, "static solve needs the K assembly");
+    launch(c, k_rhs64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, c->load.p, c->pseudo.p, c->b64.p);
+    if (last) CK(cudaMemcpyAsync(c->x64.p, c->u.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    else CK(cudaMemsetAsync(c->x64.p, 0, sizeof(double) * n, c->stream));
+    CKL("k_rhs64");
+    status = fp64_core(c, o, stats, &prof);
+  } else if (o->mode == BETA_GPU_MODE_MPIR) {
+    if (!c->have32) return fail(c, BETA_GPU_ERR_STATE, "assemble in FP32 before a mixed-precision solve");
+    if (c->what32 != BETA_GPU_ASM_K) return fail(c, BETA_GPU_ERR_STATE, "static solve needs the K assembly");
+    // ||b|| with b = rest ? presc : load - K ubar_ext
+    launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, nullptr, c->t64.p);
+    if ((rc = mf_apply(c, 1.0, c->t64.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
+    launch(c, k_rhs_elim64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, c->load.p, c->y64.p,
+                                                            c->b64.p, c->sums.p, c->partials.p, c->ticket.p);
+    CKL("k_rhs_elim64");
+    double bb;
+    if ((rc = read_sums(c, 1, &bb))) return rc;
+    launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, last ? c->u.p : nullptr, c->x64.p);
+    CKL("k_ext64");
+    status = mpir_dispatch(c, o, 1.0, 0.0, nullptr, 0.0, c->load.p, std::sqrt(bb), stats, &prof);
+    if (stats && (status == BETA_GPU_OK || status == BETA_GPU_MAXIT)) {
+      // true FP64 residual of the returned iterate
+      if ((rc = mf_apply(c, 1.0, c->x64.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
+      launch(c, k_residual64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->load.p, c->y64.p, c->x64.p,
+                                                              c->r64.p, c->sums.p, c->partials.p, c->ticket.p);
+      double s2[2];
+      if ((rc = read_sums(c, 2, s2))) return rc;
+      stats->true_rel_residual = bb > 0 ? std::sqrt(s2[0] / bb) : std::sqrt(s2[0]);
+    }
+  } else {
+    return fail(c, BETA_GPU_ERR_ARG, "unknown solve mode");
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  if (status == BETA_GPU_OK || status == BETA_GPU_MAXIT) {
+    CK(cudaMemcpyAsync(c->u.p, c->x64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    c->have_u = true;
+  }
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    stats->ms_solve = ms;
+    stats->ms_spmv_avg = prof.launches ? prof.ms / prof.launches : 0.0;
+  }
+  if (status == BETA_GPU_MAXIT) c->err = "Solution not converged...";
+  if (status == BETA_GPU_BREAKDOWN) c->err = "PCG breakdown (p.Ap <= 0 or non-finite)";
+  return status;
+}
+
+int beta_gpu_download(beta_gpu_ctx* c, double* u) {
+  if (!c || !u) return BETA_GPU_ERR_ARG;
+  if (!c->have_u) return fail(c, BETA_GPU_ERR_STATE, "no solution");
+  cudaSetDevice(c->device);
+  CK(d2h(c, u, c->u.p, sizeof(double) * c->ndof));
+  CK(cudaStreamSynchronize(c->stream));
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_matvec(beta_gpu_ctx* c, int precision, const double* x, double* y) {
+  if (!c || !x || !y) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  const int n = c->ndof;
+  CK(h2d(c, c->t64.p, x, sizeof(double) * n));
+  if (precision == BETA_GPU_FP64) {
+    if (!c->have64) return fail(c, BETA_GPU_ERR_STATE, "no FP64 matrix");
+    ScalarMat A{n, c->P.nsslice, c->ssoff.p, c->scol.p, c->sval.p};
+    launch(c, k_spmv_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, A, c->t64.p, c->y64.p, nullptr);
+  } else {
+    if (!c->have32) return fail(c, BETA_GPU_ERR_STATE, "no FP32 matrix");
+    BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p};
+    const int g = grid_for(c, (long long)c->P.nslice * 32, 256), gn = grid_for(c, c->nnode, 256);
+    if (c->ndpn == 3) {
+      launch(c, k_to_node32<3>, gn, 256, 0, c->nnode, c->t64.p, 1.0, (float4*)c->v32[0].p);
+      launch(c, k_spmv_b<3>, g, 256, 0, A, (const float4*)c->v32[0].p, (float4*)c->v32[1].p);
+    } else if (c->ndpn == 2) {
+      launch(c, k_to_node32<2>, gn, 256, 0, c->nnode, c->t64.p, 1.0, (float2*)c->v32[0].p);
+      launch(c, k_spmv_b<2>, g, 256, 0, A, (const float2*)c->v32[0].p, (float2*)c->v32[1].p);
+    } else {
+      launch(c, k_to_node32<1>, gn, 256, 0, c->nnode, c->t64.p, 1.0, c->v32[0].p);
+      launch(c, k_spmv_b<1>, g, 256, 0, A, c->v32[0].p, c->v32[1].p);
+    }
+    CK(cudaMemsetAsync(c->y64.p, 0, sizeof(double) * n, c->stream));
+    if (c->ndpn == 3) launch(c, k_axpy_from_node32<3>, gn, 256, 0, c->nnode, c->y64.p, 1.0, (const float4*)c->v32[1].p);
+    else if (c->ndpn == 2) launch(c, k_axpy_from_node32<2>, gn, 256, 0, c->nnode, c->y64.p, 1.0, (const float2*)c->v32[1].p);
+    else launch(c, k_axpy_from_node32<1>, gn, 256, 0, c->nnode, c->y64.p, 1.0, c->v32[1].p);
+  }
+  CKL("matvec");
+  CK(d2h(c, y, c->y64.p, sizeof(double) * n));
+  CK(cudaStreamSynchronize(c->stream));
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_internal_force(beta_gpu_ctx* c, const double* u, double* f) {
+  if (!c || !u || !f) return BETA_GPU_ERR_ARG;
+  if (!c->have_pattern || !c->have_mat) return fail(c, BETA_GPU_ERR_STATE, "pattern and materials required");
+  cudaSetDevice(c->device);
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  CK(h2d(c, c->t64.p, u, sizeof(double) * c->ndof));
+  if ((rc = mf_apply(c, 1.0, c->t64.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
+  CK(d2h(c, f, c->y64.p, sizeof(double) * c->ndof));
+  CK(cudaStreamSynchronize(c->stream));
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_heat_set_state(beta_gpu_ctx* c, const double* u0) {
+  if (!c || !u0) return BETA_GPU_ERR_ARG;
+  if (c->kind != BETA_GPU_HEX8_HEAT) return fail(c, BETA_GPU_ERR_UNSUPPORTED, "transient state is for diffusion");
+  cudaSetDevice(c->device);
+  if (!all_finite(u0, c->ndof)) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite initial field");
+  int rc;
+  if ((rc = upload(c, c->us, u0, c->ndof))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_us = true;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_heat_get_state(beta_gpu_ctx* c, double* u) {
+  if (!c || !u) return BETA_GPU_ERR_ARG;
+  if (!c->have_us) return fail(c, BETA_GPU_ERR_STATE, "no transient state");
+  cudaSetDevice(c->device);
+  CK(d2h(c, u, c->us.p, sizeof(double) * c->ndof));
+  CK(cudaStreamSynchronize(c->stream));
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, const beta_gpu_solve_opts* o,
+                      beta_gpu_solve_stats* stats, int* total_iterations) {
+  if (!c || !o || nsteps < 0) return BETA_GPU_ERR_ARG;
+  if (c->kind != BETA_GPU_HEX8_HEAT || !c->have_us) return fail(c, BETA_GPU_ERR_STATE, "diffusion mesh and state required");
+  cudaSetDevice(c->device);
+  int rc;
+  const int prec = o->mode == BETA_GPU_MODE_MPIR ? BETA_GPU_FP32 : BETA_GPU_FP64;
+  const double a1 = alpha * dt, a2 = (1.0 - alpha) * dt;
+  const double ks = a1 / dt, ms = 1.0 / dt, kf = (a1 + a2) / dt;
+  bool have = prec == BETA_GPU_FP64 ? (c->have64 && c->what64 == BETA_GPU_ASM_MBAR && c->kscale64 == ks && c->mscale64 == ms)
+                                    : (c->have32 && c->what32 == BETA_GPU_ASM_MBAR && c->kscale32 == ks && c->mscale32 == ms);
+  if (!have && (rc = beta_gpu_assemble(c, BETA_GPU_ASM_MBAR, prec, dt, alpha))) return rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  const int n = c->ndof;
+  int total = 0;
+  beta_gpu_solve_stats s;
+  std::memset(&s, 0, sizeof(s));
+  ProfAcc prof;
+  prof.on = o->reserved & 1;
+  for (int step = 0; step < nsteps; ++step) {
+    if (prec == BETA_GPU_FP64) {
+      // F = -(a1+a2)/dt K u_s (formF_s_new) on free rows, + pseudo load
+      if ((rc = mf_apply(c, -kf, c->us.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
+      launch(c, k_rhs64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, c->y64.p, c->pseudo.p, c->b64.p);
+      CK(cudaMemsetAsync(c->x64.p, 0, sizeof(double) * n, c->stream));
+      CKL("k_rhs64");
+      rc = fp64_core(c, o, &s, &prof);
+    } else {
+      // b = rest ? presc : -(kf K u_s + Mbar ubar_ext) ; r = -(K(ks x + kf u_s) + ms M x)
+      launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, nullptr, c->t64.p);
+      if ((rc = mf_apply(c, ks, c->t64.p, kf, c->us.p, ms, c->y64.p))) return rc;
+      launch(c, k_rhs_elim64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, nullptr, c->y64.p,
+                                                              c->b64.p, c->sums.p, c->partials.p, c->ticket.p);
+      CKL("k_rhs_elim64");
+      double bb;
+      if ((rc = read_sums(c, 1, &bb))) return rc;
+      CK(cudaMemcpyAsync(c->x64.p, c->t64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+      rc = mpir_dispatch(c, o, ks, kf, c->us.p, ms, nullptr, std::sqrt(bb), &s, &prof);
+    }
+    if (rc != BETA_GPU_OK) {
+      if (stats) *stats = s;
+      return rc;
+    }
+    total += s.iterations;
+    // u_s <- u_s + delta (DiffusionModel.cpp:800-818)
+    launch(c, k_axpy64, grid_for(c, n, 256), 256, 0, n, c->us.p, 1.0, c->x64.p);
+    CKL("k_axpy64");
+  }
+  if (stats) *stats = s;
+  if (total_iterations) *total_iterations = total;
+  return BETA_GPU_OK;
+}
+
+// Jacobi-PCG on caller-owned device CSR; scratch from cudaMalloc, freed on return.
+int beta_gpu_csr_pcg_device(int n, const int* d_rp, const int* d_ci, const double* d_v, const double* d_b,
+                            double* d_x, int stop_rule, double tol, int maxit, void* stream_ptr,
+                            beta_gpu_solve_stats* stats) {
+  if (n <= 0 || !d_rp || !d_ci || !d_v || !d_b || !d_x || !(tol > 0)) return BETA_GPU_ERR_ARG;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  cudaStream_t s = (cudaStream_t)stream_ptr;
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return BETA_GPU_ERR_CUDA;
+  }
+  const int max_grid = nsm * 8;
+  auto grid = [&](long long items) { long long g = (items + 255) / 256; return (int)std::max(1LL, std::min<long long>(g, max_grid)); };
+  // scratch: r, p, q, dinv (n each), partials, state, counters
+  const size_t need = sizeof(double) * ((size_t)4 * n + (size_t)max_grid * 4 + 8) + sizeof(PcgState) + 64;
+  unsigned char* scratch = nullptr;
+  if (cudaMalloc(&scratch, need) != cudaSuccess) { cudaGetLastError(); return BETA_GPU_ERR_OOM; }
+  double* r = (double*)scratch;
+  double* p = r + n;
+  double* q = p + n;
+  double* dinv = q + n;
+  double* partials = dinv + n;
+  double* sums = partials + (size_t)max_grid * 4;
+  PcgState* st = (PcgState*)(sums + 8);
+  unsigned* flags = (unsigned*)(st + 1);
+  unsigned* ticket = flags + 1;
+  int status = BETA_GPU_OK;
+  PcgState h;
+  std::memset(&h, 0, sizeof(h));
+  h.rule = stop_rule == BETA_GPU_STOP_REF ? kStopRef : kStopRB;
+  h.tol2 = tol * tol;
+  h.maxit = maxit > 0 ? maxit : 10000;
+  CsrMat A{n, d_rp, d_ci, d_v};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, s);
+  cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned), s);
+  cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, s);
+  k_csr_dinv<<<grid(n), 256, 0, s>>>(A, dinv, flags);
+  k_csr_spmv<<<grid((long long)n * 8), 256, 0, s>>>(A, d_x, r, d_b);
+  k_start_s<<<grid(n), 256, 0, s>>>(n, d_x, r, d_b, dinv, p, st, partials);
+  unsigned hf[2] = {0, 0};
+  cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) status = BETA_GPU_ERR_CUDA;
+  else if (hf[0] & 8u) status = BETA_GPU_ERR_ZERODIAG;
+  else if (hf[0] & 16u) status = BETA_GPU_ERR_NEGDIAG;
+  while (status == BETA_GPU_OK) {
+    for (int k = 0; k < 16; ++k) {
+      k_csr_spmv_dot<<<grid((long long)n * 8), 256, 0, s>>>(A, p, q, st, partials);
+      k_update_s<<<grid(n), 256, 0, s>>>(n, d_x, r, p, q, dinv, st, partials);
+      k_pupd_s<<<grid(n), 256, 0, s>>>(n, p, r, dinv, st);
+    }
+    cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) { status = BETA_GPU_ERR_CUDA; break; }
+    if (h.done) {
+      status = h.status == kStatusOk ? BETA_GPU_OK : (h.status == kStatusMaxit ? BETA_GPU_MAXIT : BETA_GPU_BREAKDOWN);
+      break;
+    }
+  }
+  if (status == BETA_GPU_OK || status == BETA_GPU_MAXIT) {
+    k_csr_spmv<<<grid((long long)n * 8), 256, 0, s>>>(A, d_x, q, d_b);
+    k_norm2_diff<<<grid(n), 256, 0, s>>>(n, q, nullptr, sums, partials, ticket);
+    double rr = 0.0;
+    cudaMemcpyAsync(&rr, sums, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(e1, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) status = BETA_GPU_ERR_CUDA;
+    if (stats) {
+      stats->iterations = h.iter;
+      stats->final_norm = h.last;
+      stats->true_rel_residual = h.bb > 0 ? std::sqrt(rr / h.bb) : std::sqrt(rr);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      stats->ms_solve = ms;
+    }
+  }
+  if (stats) stats->status = status;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(scratch);
+  if (cudaGetLastError() != cudaSuccess && status == BETA_GPU_OK) status = BETA_GPU_ERR_CUDA;
+  return status;
+}
+
+}  // extern "C"

@@ -1,0 +1,195 @@
+// mf_kernels.cuh -- FP64 matrix-free element operators.
+//
+//   y += K (c1*w1 + c2*w2) + cm * M w1
+//
+// evaluated element by element from the mesh, in FP64 (the outer residual of
+// mixed-precision refinement and the internal force).  Per Gauss point:
+// displacement gradient, strain (engineering shear), stress = C strain, and
+// Fe += B^T stress * detJ * w -- ElasticityElement3D::derivativesOfFields /
+// calculateStrain / calculateFe / addToFe (ElasticityElement3D.cpp:162-207,
+// 124-134, 1053-1065, 41-55) with ElasticMaterial::calculateStress
+// (elastic.cpp:411-451); for diffusion flux = k grad T and the capacity term
+// (HeatTransferElement3DTransient.cpp:41-77).  One lane per element node, the
+// element-level sums by xor butterflies; colours make the scatter exclusive.
+#pragma once
+#include "common.cuh"
+
+namespace betagpu {
+
+struct MfArgs {
+  const double* xyz;
+  const int* conn;
+  const double* gparams;
+  const int* egroup;
+  int nparams;
+  int nip;
+  const GaussTable* gt;
+  double c1, c2, cm;
+};
+
+// hex8 elasticity: 8 lanes per element, 4 elements per warp.
+__global__ void __launch_bounds__(256) k_mf_hex8_elastic(MfArgs A, const int* __restrict__ elems,
+                                                         int nel, const double* __restrict__ w1,
+                                                         const double* __restrict__ w2,
+                                                         double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 24];
+  __shared__ double s_w[kMaxIP];
+  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
+    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
+  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, b = lane & 7;
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 4 * w < nel; w += gridDim.x * wpb) {
+    const int idx = 4 * w + (lane >> 3);
+    const bool valid = idx < nel;
+    const int e = elems[valid ? idx : nel - 1];
+    const int* ce = A.conn + (long long)e * 8;
+    const int J = ce[b], n0 = ce[0];
+    double xr[3], u[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      xr[c] = A.xyz[3LL * J + c] - A.xyz[3LL * n0 + c];
+      u[c] = A.c1 * w1[3LL * J + c] + (w2 ? A.c2 * w2[3LL * J + c] : 0.0);
+    }
+    double nn[6], gg[3];
+    ortho_c(A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams, nn, gg);
+    double f0 = 0, f1 = 0, f2 = 0;
+    for (int ip = 0; ip < A.nip; ++ip) {
+      const double d0 = s_dN[ip * 24 + b], d1 = s_dN[ip * 24 + 8 + b], d2 = s_dN[ip * 24 + 16 + b];
+      double M[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        M[c] = group_sum<8>(d0 * xr[c]);
+        M[3 + c] = group_sum<8>(d1 * xr[c]);
+        M[6 + c] = group_sum<8>(d2 * xr[c]);
+      }
+      double Mi[9];
+      const double det = inv3<double>(M, Mi);
+      const double g0 = Mi[0] * d0 + Mi[1] * d1 + Mi[2] * d2;
+      const double g1 = Mi[3] * d0 + Mi[4] * d1 + Mi[5] * d2;
+      const double g2 = Mi[6] * d0 + Mi[7] * d1 + Mi[8] * d2;
+      double G[9];  // du_i/dx_c
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        G[3 * i] = group_sum<8>(u[i] * g0);
+        G[3 * i + 1] = group_sum<8>(u[i] * g1);
+        G[3 * i + 2] = group_sum<8>(u[i] * g2);
+      }
+      const double e0 = G[0], e1 = G[4], e2 = G[8];
+      const double e3 = G[1] + G[3], e4 = G[5] + G[7], e5 = G[2] + G[6];
+      const double s0 = nn[0] * e0 + nn[1] * e1 + nn[2] * e2;
+      const double s1 = nn[1] * e0 + nn[3] * e1 + nn[4] * e2;
+      const double s2 = nn[2] * e0 + nn[4] * e1 + nn[5] * e2;
+      const double s3 = gg[0] * e3, s4 = gg[1] * e4, s5 = gg[2] * e5;
+      const double fw = det * s_w[ip];
+      f0 += fw * (g0 * s0 + g1 * s3 + g2 * s5);
+      f1 += fw * (g1 * s1 + g0 * s3 + g2 * s4);
+      f2 += fw * (g2 * s2 + g1 * s4 + g0 * s5);
+    }
+    if (valid) {
+      y[3LL * J] += f0;
+      y[3LL * J + 1] += f1;
+      y[3LL * J + 2] += f2;
+    }
+  }
+}
+
+// quad4 plane stress: 4 lanes per element, 8 elements per warp.
+__global__ void __launch_bounds__(256) k_mf_quad4_pstress(MfArgs A, const int* __restrict__ elems,
+                                                          int nel, const double* __restrict__ w1,
+                                                          const double* __restrict__ w2,
+                                                          double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 8];
+  __shared__ double s_w[kMaxIP];
+  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_dN[i] = A.gt->dN[i / 8][(i / 4) % 2][i % 4];
+  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, b = lane & 3;
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 8 * w < nel; w += gridDim.x * wpb) {
+    const int idx = 8 * w + (lane >> 2);
+    const bool valid = idx < nel;
+    const int e = elems[valid ? idx : nel - 1];
+    const int* ce = A.conn + (long long)e * 4;
+    const int J = ce[b], n0 = ce[0];
+    const double xr0 = A.xyz[2LL * J] - A.xyz[2LL * n0], xr1 = A.xyz[2LL * J + 1] - A.xyz[2LL * n0 + 1];
+    const double u0 = A.c1 * w1[2LL * J] + (w2 ? A.c2 * w2[2LL * J] : 0.0);
+    const double u1 = A.c1 * w1[2LL * J + 1] + (w2 ? A.c2 * w2[2LL * J + 1] : 0.0);
+    double cc[4];
+    pstress_c(A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams, cc);
+    double f0 = 0, f1 = 0;
+    for (int ip = 0; ip < A.nip; ++ip) {
+      const double d0 = s_dN[ip * 8 + b], d1 = s_dN[ip * 8 + 4 + b];
+      const double M00 = group_sum<4>(d0 * xr0), M01 = group_sum<4>(d0 * xr1);
+      const double M10 = group_sum<4>(d1 * xr0), M11 = group_sum<4>(d1 * xr1);
+      const double det = M00 * M11 - M01 * M10, id = 1.0 / det;
+      const double g0 = (M11 * d0 - M01 * d1) * id, g1 = (-M10 * d0 + M00 * d1) * id;
+      const double G00 = group_sum<4>(u0 * g0), G01 = group_sum<4>(u0 * g1);
+      const double G10 = group_sum<4>(u1 * g0), G11 = group_sum<4>(u1 * g1);
+      const double e0 = G00, e1 = G11, e2 = G01 + G10;
+      const double s0 = cc[0] * e0 + cc[1] * e1, s1 = cc[1] * e0 + cc[2] * e1, s2 = cc[3] * e2;
+      const double fw = det * s_w[ip];
+      f0 += fw * (g0 * s0 + g1 * s2);
+      f1 += fw * (g1 * s1 + g0 * s2);
+    }
+    if (valid) {
+      y[2LL * J] += f0;
+      y[2LL * J + 1] += f1;
+    }
+  }
+}
+
+// hex8 diffusion: y += K (c1 w1 + c2 w2) + cm M w1, 8 lanes per element.
+__global__ void __launch_bounds__(256) k_mf_hex8_heat(MfArgs A, const int* __restrict__ elems, int nel,
+                                                      const double* __restrict__ w1,
+                                                      const double* __restrict__ w2,
+                                                      double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 24];
+  __shared__ double s_N[kMaxIP * 8];
+  __shared__ double s_w[kMaxIP];
+  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
+    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
+  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_N[i] = A.gt->N[i / 8][i % 8];
+  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, b = lane & 7;
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 4 * w < nel; w += gridDim.x * wpb) {
+    const int idx = 4 * w + (lane >> 3);
+    const bool valid = idx < nel;
+    const int e = elems[valid ? idx : nel - 1];
+    const int* ce = A.conn + (long long)e * 8;
+    const int J = ce[b], n0 = ce[0];
+    double xr[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) xr[c] = A.xyz[3LL * J + c] - A.xyz[3LL * n0 + c];
+    const double vk = A.c1 * w1[J] + (w2 ? A.c2 * w2[J] : 0.0);
+    const double vm = w1[J];
+    const double* pm = A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams;
+    double f = 0;
+    for (int ip = 0; ip < A.nip; ++ip) {
+      const double d0 = s_dN[ip * 24 + b], d1 = s_dN[ip * 24 + 8 + b], d2 = s_dN[ip * 24 + 16 + b];
+      double M[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        M[c] = group_sum<8>(d0 * xr[c]);
+        M[3 + c] = group_sum<8>(d1 * xr[c]);
+        M[6 + c] = group_sum<8>(d2 * xr[c]);
+      }
+      double Mi[9];
+      const double det = inv3<double>(M, Mi);
+      const double g0 = Mi[0] * d0 + Mi[1] * d1 + Mi[2] * d2;
+      const double g1 = Mi[3] * d0 + Mi[4] * d1 + Mi[5] * d2;
+      const double g2 = Mi[6] * d0 + Mi[7] * d1 + Mi[8] * d2;
+      const double t0 = group_sum<8>(vk * g0), t1 = group_sum<8>(vk * g1), t2 = group_sum<8>(vk * g2);
+      const double Sb = s_N[ip * 8 + b];
+      const double tv = group_sum<8>(vm * Sb);
+      const double fw = det * s_w[ip];
+      f += fw * (g0 * pm[0] * t0 + g1 * pm[1] * t1 + g2 * pm[2] * t2 + A.cm * pm[3] * Sb * tv);
+    }
+    if (valid) y[J] += f;
+  }
+}
+
+}  // namespace betagpu

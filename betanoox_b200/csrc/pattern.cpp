@@ -1,0 +1,296 @@
+// pattern.cpp -- host-side integer structure (see pattern.hpp).
+#include "pattern.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <functional>
+#include <thread>
+
+namespace betagpu {
+
+static void parallel_for(long long n, const std::function<void(long long, long long)>& body) {
+  unsigned hw = std::thread::hardware_concurrency();
+  int t = (int)std::min<unsigned>(hw ? hw : 1, 64);
+  if (n < 20000 || t <= 1) { body(0, n); return; }
+  std::vector<std::thread> th;
+  for (int k = 0; k < t; ++k) {
+    long long lo = n * k / t, hi = n * (k + 1) / t;
+    th.emplace_back(body, lo, hi);
+  }
+  for (auto& x : th) x.join();
+}
+
+std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* conn,
+                          const int* first_dof, const unsigned char* rest, HostPattern& P) {
+  if (nnode <= 0 || nelem <= 0 || nnpe <= 0 || nnpe > 8 || ndpn < 1 || ndpn > 3)
+    return "build_pattern: bad sizes";
+  for (int i = 0; i < nnode; ++i)
+    if (first_dof[i] != ndpn * i)
+      return "build_pattern: first_dof must be the uniform node-major numbering ndpn*node";
+  for (long long k = 0; k < (long long)nelem * nnpe; ++k)
+    if (conn[k] < 0 || conn[k] >= nnode) return "build_pattern: connectivity out of range";
+  P = HostPattern();
+  P.nnode = nnode; P.nelem = nelem; P.nnpe = nnpe; P.ndpn = ndpn; P.ndof = nnode * ndpn;
+
+  // ---- node -> element incidence -------------------------------------
+  std::vector<int> icnt(nnode + 1, 0);
+  for (long long k = 0; k < (long long)nelem * nnpe; ++k) icnt[conn[k] + 1]++;
+  for (int i = 0; i < nnode; ++i) icnt[i + 1] += icnt[i];
+  std::vector<int> inc(icnt[nnode]);
+  {
+    std::vector<int> fill(icnt.begin(), icnt.end() - 1);
+    for (int e = 0; e < nelem; ++e)
+      for (int a = 0; a < nnpe; ++a) inc[fill[conn[(long long)e * nnpe + a]]++] = e;
+  }
+
+  // ---- node graph (two passes: count, then fill) ---------------------
+  auto collect = [&](int i, std::vector<int>& buf) {
+    buf.clear();
+    for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
+      const int* ce = conn + (long long)inc[k] * nnpe;
+      for (int a = 0; a < nnpe; ++a) buf.push_back(ce[a]);
+    }
+    if (buf.empty()) buf.push_back(i);  // a node in no element keeps its diagonal
+    std::sort(buf.begin(), buf.end());
+    buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+  };
+  P.nrp.assign(nnode + 1, 0);
+  parallel_for(nnode, [&](long long lo, long long hi) {
+    std::vector<int> buf;
+    for (long long i = lo; i < hi; ++i) { collect((int)i, buf); P.nrp[i + 1] = (int)buf.size(); }
+  });
+  for (int i = 0; i < nnode; ++i) {
+    if ((long long)P.nrp[i] + P.nrp[i + 1] > 2000000000LL) return "build_pattern: node graph too large";
+    P.nrp[i + 1] += P.nrp[i];
+  }
+  P.nblk = P.nrp[nnode];
+  P.ncol.resize(P.nblk);
+  P.ndiag.resize(nnode);
+  parallel_for(nnode, [&](long long lo, long long hi) {
+    std::vector<int> buf;
+    for (long long i = lo; i < hi; ++i) {
+      collect((int)i, buf);
+      std::copy(buf.begin(), buf.end(), P.ncol.begin() + P.nrp[i]);
+      P.ndiag[i] = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
+    }
+  });
+
+  // ---- greedy element colouring (one 64-bit colour mask per node) ----
+  {
+    std::vector<uint64_t> used(nnode, 0);
+    std::vector<int> color(nelem);
+    int maxc = 0;
+    for (int e = 0; e < nelem; ++e) {
+      const int* ce = conn + (long long)e * nnpe;
+      uint64_t m = 0;
+      for (int a = 0; a < nnpe; ++a) m |= used[ce[a]];
+      if (m == ~0ULL) return "build_pattern: more than 64 element colours";
+      int c = __builtin_ctzll(~m);
+      color[e] = c;
+      maxc = std::max(maxc, c + 1);
+      for (int a = 0; a < nnpe; ++a) used[ce[a]] |= (1ULL << c);
+    }
+    P.ncolor = maxc;
+    P.color_ptr.assign(maxc + 1, 0);
+    for (int e = 0; e < nelem; ++e) P.color_ptr[color[e] + 1]++;
+    for (int c = 0; c < maxc; ++c) P.color_ptr[c + 1] += P.color_ptr[c];
+    P.elem_by_color.resize(nelem);
+    std::vector<int> fill(P.color_ptr.begin(), P.color_ptr.end() - 1);
+    for (int e = 0; e < nelem; ++e) P.elem_by_color[fill[color[e]]++] = e;
+  }
+
+  // ---- element -> node-pair block map --------------------------------
+  const int npair = nnpe * nnpe;
+  P.slot.resize((size_t)nelem * npair);
+  parallel_for(nelem, [&](long long lo, long long hi) {
+    for (long long e = lo; e < hi; ++e) {
+      const int* ce = conn + e * nnpe;
+      for (int a = 0; a < nnpe; ++a) {
+        const int I = ce[a];
+        const int* rb = P.ncol.data() + P.nrp[I];
+        const int* re = P.ncol.data() + P.nrp[I + 1];
+        for (int b = 0; b < nnpe; ++b) {
+          const int* it = std::lower_bound(rb, re, ce[b]);
+          P.slot[e * npair + a * nnpe + b] = (int)(it - P.ncol.data());
+        }
+      }
+    }
+  });
+
+  // ---- node-block sliced ELL ------------------------------------------
+  P.nslice = (nnode + 31) / 32;
+  P.bsoff.assign(P.nslice + 1, 0);
+  for (int s = 0; s < P.nslice; ++s) {
+    int w = 0;
+    for (int i = s * 32; i < std::min(nnode, s * 32 + 32); ++i) w = std::max(w, P.nrp[i + 1] - P.nrp[i]);
+    P.bsoff[s + 1] = P.bsoff[s] + w;
+  }
+  P.nchunk = P.bsoff[P.nslice];
+  if (P.nchunk * 32LL * ndpn * ndpn > 2000000000LL) return "build_pattern: block layout exceeds 2^31 entries";
+  P.bcol.assign((size_t)P.nchunk * 32, 0);
+  parallel_for(P.nslice, [&](long long lo, long long hi) {
+    for (long long s = lo; s < hi; ++s) {
+      int w = P.bsoff[s + 1] - P.bsoff[s];
+      for (int lane = 0; lane < 32; ++lane) {
+        int i = (int)s * 32 + lane;
+        int len = i < nnode ? P.nrp[i + 1] - P.nrp[i] : 0;
+        for (int k = 0; k < w; ++k)
+          P.bcol[(size_t)(P.bsoff[s] + k) * 32 + lane] =
+              k < len ? P.ncol[P.nrp[i] + k] : (i < nnode ? i : 0);
+      }
+    }
+  });
+
+  // ---- scalar sliced ELL over dofs ------------------------------------
+  const int ndof = P.ndof;
+  std::vector<int> ufree(nnode, 0);
+  for (int i = 0; i < nnode; ++i)
+    for (int j = 0; j < ndpn; ++j) ufree[i] += rest[ndpn * i + j] ? 0 : 1;
+  P.soff.resize(P.nblk);
+  std::vector<int> nodelen(nnode);
+  parallel_for(nnode, [&](long long lo, long long hi) {
+    for (long long i = lo; i < hi; ++i) {
+      int acc = 0;
+      for (int k = P.nrp[i]; k < P.nrp[i + 1]; ++k) { P.soff[k] = acc; acc += ufree[P.ncol[k]]; }
+      nodelen[i] = acc;
+    }
+  });
+  P.srowlen.resize(ndof);
+  P.nnz_full = 0;
+  P.nnz_lower = 0;
+  for (int r = 0; r < ndof; ++r) {
+    P.srowlen[r] = rest[r] ? 1 : nodelen[r / ndpn];
+    P.nnz_full += P.srowlen[r];
+  }
+  // lower count per free row: free columns c <= r in the node's row
+  {
+    std::vector<long long> lower(ndof, 0);
+    parallel_for(nnode, [&](long long lo, long long hi) {
+      for (long long I = lo; I < hi; ++I)
+        for (int i = 0; i < ndpn; ++i) {
+          int r = (int)I * ndpn + i;
+          if (rest[r]) { lower[r] = 1; continue; }
+          long long cnt = 0;
+          for (int k = P.nrp[I]; k < P.nrp[I + 1]; ++k) {
+            int J = P.ncol[k];
+            for (int j = 0; j < ndpn; ++j) {
+              int c = J * ndpn + j;
+              if (!rest[c] && c <= r) ++cnt;
+            }
+          }
+          lower[r] = cnt ? cnt : 1;
+        }
+    });
+    for (int r = 0; r < ndof; ++r) P.nnz_lower += lower[r];
+  }
+  P.nsslice = (ndof + 31) / 32;
+  P.ssoff.assign(P.nsslice + 1, 0);
+  for (int s = 0; s < P.nsslice; ++s) {
+    int w = 0;
+    for (int r = s * 32; r < std::min(ndof, s * 32 + 32); ++r) w = std::max(w, P.srowlen[r]);
+    P.ssoff[s + 1] = P.ssoff[s] + (long long)w * 32;
+  }
+  if (P.ssoff[P.nsslice] > 2000000000LL) return "build_pattern: scalar layout exceeds 2^31 entries";
+  P.scol.assign(P.ssoff[P.nsslice], 0);
+  P.sdiag.assign(ndof, 0);
+  parallel_for(P.nsslice, [&](long long lo, long long hi) {
+    for (long long s = lo; s < hi; ++s) {
+      int w = (int)((P.ssoff[s + 1] - P.ssoff[s]) / 32);
+      for (int lane = 0; lane < 32; ++lane) {
+        int r = (int)s * 32 + lane;
+        long long base = P.ssoff[s] + lane;
+        int k = 0;
+        if (r < ndof) {
+          if (rest[r]) {
+            P.scol[base] = r;
+            P.sdiag[r] = base;
+            k = 1;
+          } else {
+            int I = r / ndpn;
+            for (int q = P.nrp[I]; q < P.nrp[I + 1]; ++q) {
+              int J = P.ncol[q];
+              for (int j = 0; j < ndpn; ++j) {
+                int c = J * ndpn + j;
+                if (rest[c]) continue;
+                if (c == r) P.sdiag[r] = base + (long long)k * 32;
+                P.scol[base + (long long)k * 32] = c;
+                ++k;
+              }
+            }
+          }
+        }
+        for (; k < w; ++k) P.scol[base + (long long)k * 32] = r < ndof ? r : 0;
+      }
+    }
+  });
+  return "";
+}
+
+void export_lower_pattern(const HostPattern& P, const unsigned char* rest, long long* row_ptr,
+                          int* col) {
+  long long p = 0;
+  const int nd = P.ndpn;
+  for (int r = 0; r < P.ndof; ++r) {
+    row_ptr[r] = p;
+    if (rest[r]) { col[p++] = r; continue; }
+    int I = r / nd;
+    long long start = p;
+    for (int k = P.nrp[I]; k < P.nrp[I + 1]; ++k) {
+      int J = P.ncol[k];
+      for (int j = 0; j < nd; ++j) {
+        int c = J * nd + j;
+        if (!rest[c] && c <= r) col[p++] = c;
+      }
+    }
+    if (p == start) col[p++] = r;
+  }
+  row_ptr[P.ndof] = p;
+}
+
+void export_lower_values_scalar(const HostPattern& P, const unsigned char* rest, const double* sval,
+                                double* out) {
+  long long p = 0;
+  const int nd = P.ndpn;
+  for (int r = 0; r < P.ndof; ++r) {
+    long long base = P.ssoff[r / 32] + (r % 32);
+    if (rest[r]) { out[p++] = sval[P.sdiag[r]]; continue; }
+    int I = r / nd;
+    int k = 0;
+    for (int q = P.nrp[I]; q < P.nrp[I + 1]; ++q) {
+      int J = P.ncol[q];
+      for (int j = 0; j < nd; ++j) {
+        int c = J * nd + j;
+        if (rest[c]) continue;
+        if (c <= r) out[p++] = sval[base + (long long)k * 32];
+        ++k;
+      }
+    }
+  }
+}
+
+void export_lower_values_block(const HostPattern& P, const unsigned char* rest, const float* bval,
+                               double* out) {
+  long long p = 0;
+  const int nd = P.ndpn, bb = nd * nd;
+  for (int r = 0; r < P.ndof; ++r) {
+    int I = r / nd, i = r % nd;
+    long long chunk0 = P.bsoff[I / 32];
+    int lane = I % 32;
+    if (rest[r]) {
+      long long ch = chunk0 + P.ndiag[I];
+      out[p++] = bval[ch * 32 * bb + (long long)(i * nd + i) * 32 + lane];
+      continue;
+    }
+    for (int q = P.nrp[I]; q < P.nrp[I + 1]; ++q) {
+      int J = P.ncol[q];
+      long long ch = chunk0 + (q - P.nrp[I]);
+      for (int j = 0; j < nd; ++j) {
+        int c = J * nd + j;
+        if (rest[c] || c > r) continue;
+        out[p++] = bval[ch * 32 * bb + (long long)(i * nd + j) * 32 + lane];
+      }
+    }
+  }
+}
+
+}  // namespace betagpu

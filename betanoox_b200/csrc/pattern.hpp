@@ -1,0 +1,79 @@
+// pattern.hpp -- host-side integer structure of one finite-element system.
+//
+// Everything here is integer work done once per mesh (BETA does it once per
+// analysis in BasicModel::allocateEquationsMatrix, BasicModel.cpp:1022-1033):
+//   * node graph: for every node the sorted set of nodes sharing an element;
+//   * element colouring: no two elements of one colour share a node, so the
+//     device scatter needs no atomics and sums in a fixed order;
+//   * element->slot map: for element e and local node pair (a,b) the index of
+//     the node-pair block (conn[e][a], conn[e][b]) in the node graph;
+//   * two sliced-ELL layouts of the global matrix (32 rows per slice, entry
+//     (row, k) stored at slice_base + k*32 + row%32 so a warp reads 128-byte
+//     lines): node-block rows for the FP32 inner solver and scalar DOF rows
+//     with restrained columns removed for the plain FP64 solver;
+//   * the reference's lower-triangle pattern (Equations::specifyNonZeroLocation,
+//     equation.cpp:1216-1267 + SymmetricSparseMatrix::allocate,
+//     sparse.cpp:482-495), exported for the bit-exact structure check.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace betagpu {
+
+struct HostPattern {
+  int nnode = 0, nelem = 0, nnpe = 0, ndpn = 0, ndof = 0;
+
+  // node graph (CSR over nodes, columns ascending, self included)
+  std::vector<int> nrp;       // nnode+1
+  std::vector<int> ncol;      // nblk
+  std::vector<int> ndiag;     // position of node i in its own row
+  long long nblk = 0;
+
+  // element colouring
+  int ncolor = 0;
+  std::vector<int> color_ptr;     // ncolor+1
+  std::vector<int> elem_by_color; // nelem
+
+  // element -> node-pair block index, nelem * nnpe * nnpe
+  std::vector<int> slot;
+
+  // node-block sliced ELL: slice s covers nodes [32s, 32s+32)
+  int nslice = 0;
+  std::vector<int> bsoff;     // nslice+1, in chunks (one chunk = 32 blocks)
+  std::vector<int> bcol;      // nchunk*32, padding points at the row's own node
+  long long nchunk = 0;
+
+  // scalar sliced ELL over dofs (restrained rows: diagonal only; restrained
+  // columns removed), slice s covers rows [32s, 32s+32)
+  int nsslice = 0;
+  std::vector<long long> ssoff;   // nsslice+1, in entries
+  std::vector<int> scol;          // ssoff.back()
+  std::vector<int> soff;          // per node-pair block: column offset of node J's
+                                  // first free dof within rows of node I
+  std::vector<int> srowlen;       // per dof
+  std::vector<long long> sdiag;   // per dof: index of the diagonal entry
+  long long nnz_full = 0;         // scalar nonzeros (without padding)
+
+  // reference lower-triangle pattern
+  long long nnz_lower = 0;
+};
+
+// Builds everything above.  conn: nelem*nnpe; restrained: ndof (0/1).
+// Returns an empty string on success, else an error message.
+std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* conn,
+                          const int* first_dof, const unsigned char* restrained, HostPattern& P);
+
+// Lower-triangle pattern export in SymmetricSparseMatrix order.
+void export_lower_pattern(const HostPattern& P, const unsigned char* restrained,
+                          long long* row_ptr, int* col);
+
+// Lower-triangle values export from the scalar FP64 sliced-ELL values.
+void export_lower_values_scalar(const HostPattern& P, const unsigned char* restrained,
+                                const double* sval, double* out);
+
+// Lower-triangle values export from the node-block FP32 sliced-ELL values.
+void export_lower_values_block(const HostPattern& P, const unsigned char* restrained,
+                               const float* bval, double* out);
+
+}  // namespace betagpu

@@ -1,0 +1,234 @@
+/*
+ * beta_gpu.h -- C ABI of the B200 element-assembly + PCG path for BETA.
+ *
+ * This library replaces, behind BETA's own interfaces, the hot path
+ *   SerialAssembler/ESA_Assembler::assembleK  (beta/assemblers/SerialAssembler.cpp:35-59,
+ *                                              beta/assemblers/ESA_Assembler.cpp:9-68)
+ *   Element::update("K"|"F"|"KM")             (beta/elements/3D/ElasticityElement3D.cpp:1032-1051,
+ *                                              beta_ext/diffusion/element/HeatTransferElement3DTransient.cpp:707-767)
+ *   Equations::addMatrix / specifyNonZeroLocation / solve
+ *                                             (beta/math/equation/equation.cpp:445-562, 1216-1267, 1288-1405)
+ *   SymmetricSparseMatrix::solve / vectorProduct (beta/math/equation/sparse.cpp:114-242, 452-478)
+ * with hand-written sm_100a kernels.  Every call is plain C: host pointers,
+ * sizes and opaque handles; no CUDA or framework types cross the boundary
+ * except in the explicitly device-pointer entry points, whose names say so.
+ *
+ * Conventions
+ *   - Every function returns an int status (BETA_GPU_OK == 0).  Nothing calls
+ *     exit(); beta_gpu_last_error() returns a message for the last failure.
+ *   - Host pointers are only read (or written) during the call.
+ *   - All device work of a context runs on the context's own stream, in order.
+ *   - DOF numbering is BETA's: dof(node, j) = first_dof[node] + j
+ *     (BasicElement::calculateDofList, beta/elements/BasicElement.cpp:49-68;
+ *     Node::setNumDofPerNode, beta/mesh/node.cpp:158-227).  The block
+ *     layouts require the uniform node-major numbering first_dof[i] = ndpn*i
+ *     that "SetNumDofPerNode <n> all" produces.
+ */
+#ifndef BETA_GPU_H
+#define BETA_GPU_H
+
+#if defined(__GNUC__)
+#define BETA_GPU_API __attribute__((visibility("default")))
+#else
+#define BETA_GPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  BETA_GPU_OK = 0,
+  BETA_GPU_ERR_ARG = 1,          /* bad argument / size                                  */
+  BETA_GPU_ERR_CUDA = 2,         /* CUDA runtime error (message in last_error)           */
+  BETA_GPU_ERR_STATE = 3,        /* call out of order (e.g. solve before assemble)       */
+  BETA_GPU_MAXIT = 4,            /* PCG hit max iterations (sparse.cpp:225-229)          */
+  BETA_GPU_BREAKDOWN = 5,        /* p.Ap <= 0 or non-finite scalar in PCG                */
+  BETA_GPU_ERR_NEGDIAG = 6,      /* element/global diagonal <= 0 (BasicElement.cpp:116-130) */
+  BETA_GPU_ERR_ZERODIAG = 7,     /* zero global diagonal (largeMatrix.cpp:43-79)         */
+  BETA_GPU_ERR_OOM = 8,          /* device allocation failed                             */
+  BETA_GPU_REJECTED = 9,         /* admission refused (HBM budget)                       */
+  BETA_GPU_TIMEOUT = 10,         /* bounded device wait expired                          */
+  BETA_GPU_ERR_NOT_FINITE = 11,  /* NaN/Inf in inputs                                    */
+  BETA_GPU_ERR_LOAD_ON_RESTRAINED = 12, /* equation.cpp:858-861                          */
+  BETA_GPU_ERR_UNSUPPORTED = 13  /* layout or element kind not supported                 */
+};
+
+/* ---- element / material kinds ------------------------------------------ */
+enum {
+  /* ElasticityElement2D quad4 + PlaneStress material: 4 params per group
+     (E11, E22, nu12, G12) as PlaneStress::read takes them (pStress.cpp:49-85). */
+  BETA_GPU_QUAD4_PSTRESS = 1,
+  /* ElasticityElement3D hex8 + ElasticMaterial "readModuli": 9 params per group
+     (E11, E22, E33, nu12, nu23, nu13, G12, G23, G13) (elastic.cpp:335-370). */
+  BETA_GPU_HEX8_ELASTIC = 2,
+  /* HeatTransferElement3Dtransient hex8 + HeatTransferMaterial: 4 params per
+     group (k11, k22, k33, capacity c) (heatTransferMaterial.cpp:89-92). */
+  BETA_GPU_HEX8_HEAT = 3
+};
+
+/* ---- what to assemble (Element::update action letters) ------------------ */
+enum {
+  BETA_GPU_ASM_K = 1,      /* "K": stiffness / conductivity                           */
+  BETA_GPU_ASM_MBAR = 2    /* "KM" + formK_s: Mbar = (a1*K + M)/dt (DiffusionModel.cpp:322-347) */
+};
+
+/* ---- precision of the assembled matrix ---------------------------------- */
+enum {
+  BETA_GPU_FP64 = 0,       /* scalar FP64 sliced-ELL (plain FP64 PCG)                  */
+  BETA_GPU_FP32 = 1        /* node-block FP32 sliced-ELL (mixed-precision inner PCG)   */
+};
+
+/* ---- solver options ------------------------------------------------------ */
+enum {
+  BETA_GPU_MODE_FP64 = 0,  /* plain FP64 Jacobi-PCG on the FP64 matrix                 */
+  BETA_GPU_MODE_MPIR = 1   /* FP32 inner PCG + FP64 matrix-free outer residual/update  */
+};
+enum {
+  BETA_GPU_PRECOND_JACOBI = 0,       /* z = r / diag (sparse.cpp:165, 192)            */
+  BETA_GPU_PRECOND_BLOCK_JACOBI = 1  /* z = inv(D_node) r, per-node ndpn x ndpn block */
+};
+enum {
+  BETA_GPU_STOP_REF = 0,   /* sqrt(r.r / x.x) < tol, the reference rule (sparse.cpp:202-223) */
+  BETA_GPU_STOP_RB = 1     /* ||b - A x|| / ||b|| < tol                                      */
+};
+
+typedef struct beta_gpu_solve_opts {
+  int mode;          /* BETA_GPU_MODE_*                                              */
+  int precond;       /* BETA_GPU_PRECOND_* (MPIR inner solve; FP64 mode uses JACOBI) */
+  int stop_rule;     /* BETA_GPU_STOP_*                                              */
+  int maxit;         /* max PCG iterations (FP64) / max total inner iterations (MPIR) */
+  double tol;        /* outer tolerance (FP64: PCG tolerance)                        */
+  double inner_tol;  /* MPIR: relative residual reduction of each inner solve         */
+  int max_outer;     /* MPIR: max refinement steps                                   */
+  int use_last_solution; /* start from the previous solution (Equations::lastSolution) */
+  int check_every;   /* host convergence poll interval in iterations (0 = default)   */
+  int reserved;
+} beta_gpu_solve_opts;
+
+typedef struct beta_gpu_solve_stats {
+  int status;             /* BETA_GPU_OK / MAXIT / BREAKDOWN ...                    */
+  int iterations;         /* total PCG iterations (MPIR: sum of inner iterations)   */
+  int outer_iterations;   /* MPIR refinement steps                                  */
+  int reserved;
+  double final_norm;      /* last value of the stop-rule quantity                   */
+  double true_rel_residual; /* ||b - A x|| / ||b|| in FP64 at exit                  */
+  double ms_solve;        /* device time of the solve (CUDA events)                 */
+  double ms_spmv_avg;     /* average device time of one SpMV launch (if measured)   */
+} beta_gpu_solve_stats;
+
+typedef struct beta_gpu_ctx beta_gpu_ctx;
+
+/* ---- lifetime ----------------------------------------------------------- */
+/* Creates a context bound to CUDA device `device` with its own stream. */
+BETA_GPU_API int beta_gpu_create(beta_gpu_ctx** ctx, int device);
+BETA_GPU_API int beta_gpu_destroy(beta_gpu_ctx* ctx);
+BETA_GPU_API const char* beta_gpu_last_error(const beta_gpu_ctx* ctx);
+/* Library/ABI version: major*10000 + minor*100 + patch. */
+BETA_GPU_API int beta_gpu_version(void);
+
+/* Runs the context's device work on a caller-owned cudaStream_t (passed as
+ * void*; NULL restores the context's own stream).  The caller keeps the
+ * stream alive while the context uses it. */
+BETA_GPU_API int beta_gpu_set_stream(beta_gpu_ctx* ctx, void* stream);
+/* Cumulative counters since creation: out[0] kernel launches, out[1] bytes
+ * copied host->device, out[2] bytes copied device->host.  n <= 3. */
+BETA_GPU_API int beta_gpu_counters(const beta_gpu_ctx* ctx, long long* out, int n);
+
+/* ---- model upload (BasicMesh::ReadMesh / SetElementProperty / loads) ----- */
+/* Mesh: ndim 2|3, xyz[nnode*ndim] (node-major), conn[nelem*nnpe] in BETA
+ * local node order (BasicElement.cpp:464-467, 518-525), first_dof[nnode].
+ * `kind` fixes the element formulation; `integration_order` is the Gauss order
+ * per direction (IsoElement::setIntegrationOrder, isoElement.cpp:463-478). */
+BETA_GPU_API int beta_gpu_mesh_upload(beta_gpu_ctx* ctx, int kind, int ndim, int nnode, const double* xyz,
+                         int nelem, int nnpe, const int* conn, const int* first_dof,
+                         int ndof_per_node, int integration_order);
+
+/* Materials as groups (BasicModel::SetElementProperty, BasicModel.cpp:682-748):
+ * group_params[ngroups*nparams] (nparams per kind, see above) and
+ * elem_group[nelem] (NULL: group index = element index). */
+BETA_GPU_API int beta_gpu_materials_upload(beta_gpu_ctx* ctx, int ngroups, int nparams,
+                              const double* group_params, const int* elem_group);
+
+/* Boundary conditions over ndof dofs (Equations::setRestraint/setSolution/
+ * addLoadToEqn, equation.cpp:306-341, 851-868): restrained[ndof] (0/1),
+ * prescribed[ndof] (used where restrained), load[ndof] (nodal loads). */
+BETA_GPU_API int beta_gpu_bc_upload(beta_gpu_ctx* ctx, const unsigned char* restrained,
+                       const double* prescribed, const double* load);
+
+/* ---- structure ---------------------------------------------------------- */
+/* Builds the node graph, element colouring, element->slot map and the
+ * sliced-ELL layouts (Equations::specifyNonZeroLocation + allocate,
+ * equation.cpp:1216-1280; sparse.cpp:479-495).  Returns the number of stored
+ * lower-triangle entries of the reference layout in *nnz_lower. */
+BETA_GPU_API int beta_gpu_build_pattern(beta_gpu_ctx* ctx, long long* nnz_lower);
+
+/* Exports the lower-triangle pattern exactly as SymmetricSparseMatrix stores
+ * it: row_ptr[ndof+1], col[nnz_lower], columns ascending, diagonal last. */
+BETA_GPU_API int beta_gpu_pattern_lower(beta_gpu_ctx* ctx, long long* row_ptr, int* col);
+
+/* Host-only form of the structure step (no device needed): the reference's
+ * lower-triangle pattern for a mesh and restraint mask.  Call with
+ * row_ptr == col == NULL to get *nnz_lower, then again with row_ptr[ndof+1]
+ * and col[*nnz_lower].  Same layout as beta_gpu_pattern_lower. */
+BETA_GPU_API int beta_gpu_pattern_lower_host(int nnode, int nelem, int nnpe, int ndof_per_node,
+                                             const int* conn, const int* first_dof,
+                                             const unsigned char* restrained, long long* nnz_lower,
+                                             long long* row_ptr, int* col);
+
+/* ---- assembly ------------------------------------------------------------ */
+/* Assembles the global matrix in `precision` (zeroMatrix + element loop +
+ * addMatrix).  what = BETA_GPU_ASM_K (static) or BETA_GPU_ASM_MBAR with
+ * a1 = alpha*dt (DiffusionModel.cpp:745-746).  In FP64 the pseudo-load of
+ * restrained columns is formed as Equations::addMatrix does. */
+BETA_GPU_API int beta_gpu_assemble(beta_gpu_ctx* ctx, int what, int precision, double dt, double alpha);
+
+/* Exports the assembled lower-triangle values in the pattern_lower order (FP32
+ * values are widened) and, for FP64 assembly, the pseudo-load vector. */
+BETA_GPU_API int beta_gpu_matrix_lower_values(beta_gpu_ctx* ctx, int precision, double* vals,
+                                 double* pseudo_load);
+
+/* ---- solve --------------------------------------------------------------- */
+/* Equations::solve: right-hand side = load + pseudo-load on free dofs,
+ * prescribed values on restrained dofs; then PCG per opts.  The solution stays
+ * on the device until beta_gpu_download. */
+BETA_GPU_API int beta_gpu_solve(beta_gpu_ctx* ctx, const beta_gpu_solve_opts* opts,
+                   beta_gpu_solve_stats* stats);
+BETA_GPU_API int beta_gpu_download(beta_gpu_ctx* ctx, double* u);
+
+/* y = A x with the assembled matrix of `precision` (SymmetricSparseMatrix::
+ * vectorProduct, sparse.cpp:452-478), host vectors of length ndof. */
+BETA_GPU_API int beta_gpu_matvec(beta_gpu_ctx* ctx, int precision, const double* x, double* y);
+
+/* Internal force f = K_e u summed over elements in FP64, matrix-free
+ * (BasicModel::CalculateResidual, BasicModel.cpp:1035-1061, without the
+ * restrained-row skip): host u[ndof] -> host f[ndof]. */
+BETA_GPU_API int beta_gpu_internal_force(beta_gpu_ctx* ctx, const double* u, double* f);
+
+/* ---- transient diffusion (DiffusionModel::DoTransientNonLinearAnalysis) -- */
+/* Sets u_s (host, ndof) as the current field. */
+BETA_GPU_API int beta_gpu_heat_set_state(beta_gpu_ctx* ctx, const double* u0);
+/* Runs nsteps steps of size dt with the generalized-alpha family (alpha=1:
+ * backward Euler), assembling Mbar = (a1 K + M)/dt once (linear conductivity)
+ * and solving Mbar du = -(a1+a2) K u_s / dt per step (DiffusionModel.cpp:743-818). */
+BETA_GPU_API int beta_gpu_heat_run(beta_gpu_ctx* ctx, double dt, double alpha, int nsteps,
+                      const beta_gpu_solve_opts* opts, beta_gpu_solve_stats* last_step_stats,
+                      int* total_iterations);
+BETA_GPU_API int beta_gpu_heat_get_state(beta_gpu_ctx* ctx, double* u);
+
+/* ---- device-pointer solver (LargeMatrix::solve on caller-owned storage) --- */
+/* Jacobi-PCG on a caller-provided full (both-triangle) CSR matrix in device
+ * memory: A x = b, x holds the initial guess on entry and the solution on
+ * exit.  Scratch (Krylov vectors and reduction partials) is allocated by the
+ * call with cudaMalloc and freed before return.  Stop rule and tolerance as in
+ * beta_gpu_solve_opts.  Runs on the legacy default stream when stream == 0,
+ * otherwise on the given cudaStream_t (passed as void*). */
+BETA_GPU_API int beta_gpu_csr_pcg_device(int n, const int* d_row_ptr, const int* d_col, const double* d_val,
+                            const double* d_b, double* d_x, int stop_rule, double tol, int maxit,
+                            void* stream, beta_gpu_solve_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BETA_GPU_H */

@@ -1,0 +1,349 @@
+"""ctypes view of the CPU oracle (test infrastructure only).
+
+The oracle is a C++ FP64 restatement of BETA's assembly + Jacobi-PCG path
+(``beta_oracle.cpp``).  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` import this module; the GPU product never
+does.  ``RefLeaf`` wraps the reference's own ``gauss.cpp``/``shape.cpp``
+compiled into ``_ref/`` (present only where the reference tree was available
+at build time).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libbeta_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libbeta_ref_leaf.so")
+
+KIND_QUAD4_PSTRESS = 1
+KIND_HEX8_ELASTIC = 2
+KIND_HEX8_HEAT = 3
+
+OK = 0
+ERR_MAXIT = 4
+ERR_NEG_DIAG = 6
+ERR_ZERO_DIAG = 7
+ERR_LOAD_ON_RESTRAINED = 12
+
+
+def build() -> None:
+    """Compile the oracle (and _ref when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_up = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("last_norm", C.c_double)]
+
+
+def _load():
+    if not os.path.exists(LIB):
+        build()
+    lib = C.CDLL(LIB)
+    V, I, D, P = C.c_void_p, C.c_int, C.c_double, C.c_void_p
+    sig = {
+        "oracle_gauss_1d": (I, [I, _dp, _dp]),
+        "oracle_hex_points": (I, [I, _dp, _dp, _dp, _dp]),
+        "oracle_quad_points": (I, [I, _dp, _dp, _dp]),
+        "oracle_shape_hex8": (None, [D, D, D, _dp, _dp, _dp, _dp]),
+        "oracle_shape_quad4": (None, [D, D, _dp, _dp, _dp]),
+        "oracle_invert": (I, [I, _dp]),
+        "oracle_cmat_ortho3d": (I, [_dp, _dp]),
+        "oracle_cmat_plane_stress": (None, [_dp, _dp]),
+        "oracle_ke_hex8": (I, [_dp, _dp, I, _dp]),
+        "oracle_ke_quad4": (I, [_dp, _dp, I, _dp]),
+        "oracle_km_hex8_heat": (I, [_dp, _dp, D, I, _dp, _dp]),
+        "oracle_fe_hex8": (I, [_dp, _dp, I, _dp, _dp]),
+        "oracle_sys_create": (V, [I]),
+        "oracle_sys_destroy": (None, [V]),
+        "oracle_sys_set_bc": (I, [V, _up, _dp, _dp]),
+        "oracle_sys_specify": (None, [V, _ip, I]),
+        "oracle_sys_allocate": (None, [V]),
+        "oracle_sys_zero": (None, [V]),
+        "oracle_sys_nnz": (C.c_longlong, [V]),
+        "oracle_sys_add_matrix": (I, [V, _dp, _ip, I, P]),
+        "oracle_sys_export_lower": (None, [V, _lp, _ip, _dp]),
+        "oracle_sys_pseudo_load": (None, [V, _dp]),
+        "oracle_sys_vector_product": (None, [V, _dp, _dp]),
+        "oracle_sys_solve": (I, [V, P, D, I, _dp, C.POINTER(SolveStats)]),
+        "oracle_sys_rhs": (None, [V, _dp]),
+        "oracle_sys_specify_mesh": (None, [V, I, I, I, _ip, _ip]),
+        "oracle_sys_assemble_mesh": (I, [V, I, I, I, I, I, _ip, _dp, _ip, _dp, I, I]),
+        "oracle_internal_force_hex8": (I, [I, _ip, _dp, _ip, _dp, I, P, _dp, _dp]),
+        "oracle_heat_step": (I, [V, I, _ip, _dp, _ip, _dp, I, D, D, _dp, D, I, C.POINTER(SolveStats)]),
+        "oracle_csr_from_sys": (V, [V]),
+        "oracle_csr_destroy": (None, [V]),
+        "oracle_csr_pcg_threaded": (I, [V, _dp, _dp, D, I, I, C.POINTER(SolveStats)]),
+        "oracle_element_matrices_threaded": (I, [I, I, I, I, I, _ip, _dp, _dp, I, I, I, _dp, I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = _load()
+    return _LIB
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+# -- element level ---------------------------------------------------------
+def gauss_1d(k):
+    x, w = np.zeros(k), np.zeros(k)
+    assert lib().oracle_gauss_1d(k, x, w) == 0
+    return x, w
+
+
+def hex_points(order):
+    n = order ** 3
+    a = [np.zeros(n) for _ in range(4)]
+    assert lib().oracle_hex_points(order, *a) == 0
+    return a
+
+
+def quad_points(order):
+    n = order ** 2
+    a = [np.zeros(n) for _ in range(3)]
+    assert lib().oracle_quad_points(order, *a) == 0
+    return a
+
+
+def shape_hex8(xi, eta, zeta):
+    S, d0, d1, d2 = (np.zeros(8) for _ in range(4))
+    lib().oracle_shape_hex8(xi, eta, zeta, S, d0, d1, d2)
+    return S, d0, d1, d2
+
+
+def shape_quad4(xi, eta):
+    S, d0, d1 = (np.zeros(4) for _ in range(3))
+    lib().oracle_shape_quad4(xi, eta, S, d0, d1)
+    return S, d0, d1
+
+
+def invert(A):
+    A = _f64(A).copy()
+    n = A.shape[0]
+    st = lib().oracle_invert(n, A.reshape(-1))
+    if st:
+        raise ArithmeticError(f"singular matrix (status {st})")
+    return A
+
+
+def cmat_ortho3d(m9):
+    C36 = np.zeros(36)
+    assert lib().oracle_cmat_ortho3d(_f64(m9), C36) == 0
+    return C36.reshape(6, 6)
+
+
+def cmat_plane_stress(m4):
+    C9 = np.zeros(9)
+    lib().oracle_cmat_plane_stress(_f64(m4), C9)
+    return C9.reshape(3, 3)
+
+
+def _full_from_upper(Ku):
+    return np.triu(Ku) + np.triu(Ku, 1).T
+
+
+def ke_hex8(xyz, C36, order=2):
+    Ke = np.zeros(24 * 24)
+    st = lib().oracle_ke_hex8(_f64(xyz).reshape(-1), _f64(C36).reshape(-1), order, Ke)
+    return st, _full_from_upper(Ke.reshape(24, 24))
+
+
+def ke_quad4(xy, C9, order=2):
+    Ke = np.zeros(64)
+    st = lib().oracle_ke_quad4(_f64(xy).reshape(-1), _f64(C9).reshape(-1), order, Ke)
+    return st, _full_from_upper(Ke.reshape(8, 8))
+
+
+def km_hex8_heat(xyz, k3, c, order=2):
+    K, M = np.zeros(64), np.zeros(64)
+    k9 = np.diag(np.asarray(k3, dtype=np.float64)).reshape(-1)
+    st = lib().oracle_km_hex8_heat(_f64(xyz).reshape(-1), _f64(k9), float(c), order, K, M)
+    return st, _full_from_upper(K.reshape(8, 8)), _full_from_upper(M.reshape(8, 8))
+
+
+def fe_hex8(xyz, C36, ue, order=2):
+    Fe = np.zeros(24)
+    assert lib().oracle_fe_hex8(_f64(xyz).reshape(-1), _f64(C36).reshape(-1), order, _f64(ue), Fe) == 0
+    return Fe
+
+
+# -- system level ----------------------------------------------------------
+class System:
+    """Equations + SymmetricSparseMatrix restated (default 'SPARSE' storage)."""
+
+    def __init__(self, mesh):
+        self.mesh = mesh
+        self.n = int(mesh.ndof)
+        self.h = lib().oracle_sys_create(self.n)
+        if not self.h:
+            raise ValueError("empty system")
+        self._csr = None
+
+    def __del__(self):
+        try:
+            if self._csr:
+                lib().oracle_csr_destroy(self._csr)
+            if self.h:
+                lib().oracle_sys_destroy(self.h)
+        except Exception:
+            pass
+
+    def set_bc(self, restrained, prescribed, load):
+        st = lib().oracle_sys_set_bc(self.h, np.ascontiguousarray(restrained, dtype=np.uint8),
+                                     _f64(prescribed), _f64(load))
+        return st
+
+    def build_pattern(self):
+        m = self.mesh
+        lib().oracle_sys_specify_mesh(self.h, m.nelem, m.nnpe, m.ndpn, _i32(m.conn).reshape(-1),
+                                      _i32(m.first_dof))
+        lib().oracle_sys_allocate(self.h)
+        return int(lib().oracle_sys_nnz(self.h))
+
+    def assemble(self, params, order):
+        m = self.mesh
+        params = _f64(params)
+        return lib().oracle_sys_assemble_mesh(
+            self.h, m.kind, m.nelem, m.nnpe, m.ndpn, m.ndim, _i32(m.conn).reshape(-1),
+            _f64(m.xyz).reshape(-1), _i32(m.first_dof), params.reshape(-1), params.shape[1], order)
+
+    def export_lower(self):
+        nnz = int(lib().oracle_sys_nnz(self.h))
+        rp = np.zeros(self.n + 1, dtype=np.int64)
+        col = np.zeros(nnz, dtype=np.int32)
+        val = np.zeros(nnz)
+        lib().oracle_sys_export_lower(self.h, rp, col, val)
+        return rp, col, val
+
+    def pseudo_load(self):
+        out = np.zeros(self.n)
+        lib().oracle_sys_pseudo_load(self.h, out)
+        return out
+
+    def rhs(self):
+        out = np.zeros(self.n)
+        lib().oracle_sys_rhs(self.h, out)
+        return out
+
+    def matvec(self, x):
+        y = np.zeros(self.n)
+        lib().oracle_sys_vector_product(self.h, _f64(x), y)
+        return y
+
+    def solve(self, eps=1e-4, maxit=10000, init_guess=None):
+        out = np.zeros(self.n)
+        st = SolveStats()
+        g = None if init_guess is None else _f64(init_guess)
+        rc = lib().oracle_sys_solve(self.h, None if g is None else g.ctypes.data, eps, maxit, out,
+                                    C.byref(st))
+        return rc, out, st
+
+    def solve_threaded(self, b, eps, maxit=10000, threads=0, x0=None):
+        if self._csr is None:
+            self._csr = lib().oracle_csr_from_sys(self.h)
+        x = np.zeros(self.n) if x0 is None else _f64(x0).copy()
+        st = SolveStats()
+        rc = lib().oracle_csr_pcg_threaded(self._csr, _f64(b), x, eps, maxit, threads, C.byref(st))
+        return rc, x, st
+
+    def heat_step(self, params, order, dt, u_s, alpha=1.0, eps=1e-10, maxit=10000):
+        m = self.mesh
+        st = SolveStats()
+        u = _f64(u_s).copy()
+        rc = lib().oracle_heat_step(self.h, m.nelem, _i32(m.conn).reshape(-1), _f64(m.xyz).reshape(-1),
+                                    _i32(m.first_dof), _f64(params).reshape(-1), order, dt, alpha, u,
+                                    eps, maxit, C.byref(st))
+        return rc, u, st
+
+
+def internal_force_hex8(mesh, params, order, u, restrained=None):
+    f = np.zeros(mesh.ndof)
+    r = None if restrained is None else np.ascontiguousarray(restrained, dtype=np.uint8)
+    st = lib().oracle_internal_force_hex8(mesh.nelem, _i32(mesh.conn).reshape(-1), _f64(mesh.xyz).reshape(-1),
+                                          _i32(mesh.first_dof), _f64(params).reshape(-1), order,
+                                          None if r is None else r.ctypes.data, _f64(u), f)
+    assert st == 0
+    return f
+
+
+def element_matrices_threaded(mesh, params, order, e0, e1, threads=0):
+    nd = mesh.nnpe * mesh.ndpn
+    out = np.zeros((e1 - e0) * nd * nd)
+    params = _f64(params)
+    st = lib().oracle_element_matrices_threaded(mesh.kind, e0, e1, mesh.nnpe, mesh.ndim,
+                                                _i32(mesh.conn).reshape(-1), _f64(mesh.xyz).reshape(-1),
+                                                params.reshape(-1), params.shape[1], order, nd, out, threads)
+    return st, out
+
+
+# -- the reference's own leaf code (oracle/_ref) -----------------------------
+class RefLeaf:
+    """The reference's gauss.cpp + shape.cpp, compiled unmodified."""
+
+    def __init__(self):
+        if not os.path.exists(REF_LIB):
+            raise FileNotFoundError(REF_LIB)
+        self.lib = C.CDLL(REF_LIB)
+        I, D = C.c_int, C.c_double
+        self.lib.ref_gauss_1d.argtypes = [I, _dp, _dp]
+        self.lib.ref_hex_points.argtypes = [I, _dp, _dp, _dp, _dp]
+        self.lib.ref_quad_points.argtypes = [I, _dp, _dp, _dp]
+        self.lib.ref_shape_hex8.argtypes = [D, D, D, _dp, _dp, _dp, _dp]
+        self.lib.ref_shape_quad4.argtypes = [D, D, _dp, _dp, _dp]
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_LIB)
+
+    def gauss_1d(self, k):
+        x, w = np.zeros(k), np.zeros(k)
+        self.lib.ref_gauss_1d(k, x, w)
+        return x, w
+
+    def hex_points(self, order):
+        n = order ** 3
+        a = [np.zeros(n) for _ in range(4)]
+        self.lib.ref_hex_points(order, *a)
+        return a
+
+    def quad_points(self, order):
+        n = order ** 2
+        a = [np.zeros(n) for _ in range(3)]
+        self.lib.ref_quad_points(order, *a)
+        return a
+
+    def shape_hex8(self, xi, eta, zeta):
+        S, d0, d1, d2 = (np.zeros(8) for _ in range(4))
+        self.lib.ref_shape_hex8(xi, eta, zeta, S, d0, d1, d2)
+        return S, d0, d1, d2
+
+    def shape_quad4(self, xi, eta):
+        S, d0, d1 = (np.zeros(4) for _ in range(3))
+        self.lib.ref_shape_quad4(xi, eta, S, d0, d1)
+        return S, d0, d1

@@ -1,0 +1,40 @@
+// C entry points over the reference's own gauss.cpp and shape.cpp, compiled
+// unmodified into oracle/_ref/libbeta_ref_leaf.so.  Test infrastructure: used
+// only to pin the oracle's restatement against the reference's code.
+#include "gauss.hpp"
+#include "hexQuadPoint.hpp"
+#include "quadQuadPoint.hpp"
+
+void shapeHex8(double* S, double xi, double eta, double zeta);
+void derivHex8(double* Sxi, double* Seta, double* Szeta, double xi, double eta, double zeta);
+void shapeQuad4(double* S, double zeta, double eta);
+void derivQuad4(double* Szeta, double* Seta, double zeta, double eta);
+
+extern "C" {
+int ref_gauss_1d(int k, double* x, double* w) {
+  GAUSS g(k);
+  for (int i = 0; i < k; ++i) { x[i] = g.getCoord(i); w[i] = g.getWeight(i); }
+  return 0;
+}
+int ref_hex_points(int order, double* xi, double* eta, double* zeta, double* w) {
+  double *a, *b, *c, *d;
+  HexQuadPoints::getQuadraturePointsForHex(order, &a, &b, &c, &d);
+  for (int i = 0; i < order * order * order; ++i) { xi[i] = a[i]; eta[i] = b[i]; zeta[i] = c[i]; w[i] = d[i]; }
+  return 0;
+}
+int ref_quad_points(int order, double* xi, double* eta, double* w) {
+  double *a, *b, *d;
+  QuadQuadPoints::getQuadraturePointsForQuad(order, &a, &b, &d);
+  for (int i = 0; i < order * order; ++i) { xi[i] = a[i]; eta[i] = b[i]; w[i] = d[i]; }
+  return 0;
+}
+void ref_shape_hex8(double xi, double eta, double zeta, double* S, double* dxi, double* deta,
+                    double* dzeta) {
+  shapeHex8(S, xi, eta, zeta);
+  derivHex8(dxi, deta, dzeta, xi, eta, zeta);
+}
+void ref_shape_quad4(double xi, double eta, double* S, double* dxi, double* deta) {
+  shapeQuad4(S, xi, eta);
+  derivQuad4(dxi, deta, xi, eta);
+}
+}

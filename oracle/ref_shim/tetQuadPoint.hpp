@@ -1,0 +1,11 @@
+// Shim declaration (definition in beta/math/gaussQuadrature/gauss.cpp).
+#pragma once
+class TetQuadPoints {
+ public:
+  static void getQuadraturePointsForTet(int order, double** xi, double** eta, double** zeta, double** w);
+  static void deleteAll();
+  static double* xi[5];
+  static double* eta[5];
+  static double* zeta[5];
+  static double* weight[5];
+};

@@ -1,0 +1,104 @@
+"""Generates tests/golden/*.json.
+
+Run from the repository root, in a checkout that has the reference tree and
+the compiled reference leaf library (``make -C oracle``):
+
+    python tests/golden/gen_golden.py
+
+* ``ref_quadrature.json`` -- Gauss-Legendre points/weights (orders 1-8) and the
+  hex/quad tensor lists (orders 1-4) produced by the reference's own
+  beta/math/gaussQuadrature/gauss.cpp, and hex8/quad4 shape functions and
+  local derivatives from beta/elements/shape.cpp, at a fixed set of points.
+  These are outputs of the reference code itself (oracle/_ref).
+* ``ref_matrix_kat.json`` -- the known answers written in the reference's
+  DEBUG_MATRIX_CLASS main (beta/math/matrix.cpp:679-696).
+* ``oracle_small.json`` -- small end-to-end cases from the oracle (element
+  matrices, assembled lower-triangle systems, PCG solutions) used as
+  regression fixtures by the GPU parity tests.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import beta_oracle as bo  # noqa: E402
+from betanoox_b200 import workloads as W  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+SAMPLE_HEX = [(-0.9, 0.1, 0.7), (0.3, -0.7, 0.1), (-0.57735, 0.57735, -0.57735), (0.0, 0.0, 0.0), (1.0, -1.0, 1.0)]
+SAMPLE_QUAD = [(-0.9, 0.1), (0.3, -0.7), (0.57735, -0.57735), (0.0, 0.0), (-1.0, 1.0)]
+
+
+def ref_quadrature():
+    r = bo.RefLeaf()
+    out = {"gauss": {}, "hex": {}, "quad": {}, "shape_hex8": [], "shape_quad4": []}
+    for k in range(1, 9):
+        x, w = r.gauss_1d(k)
+        out["gauss"][str(k)] = {"x": x.tolist(), "w": w.tolist()}
+    for o in range(1, 5):
+        a = r.hex_points(o)
+        out["hex"][str(o)] = {"xi": a[0].tolist(), "eta": a[1].tolist(), "zeta": a[2].tolist(), "w": a[3].tolist()}
+        b = r.quad_points(o)
+        out["quad"][str(o)] = {"xi": b[0].tolist(), "eta": b[1].tolist(), "w": b[2].tolist()}
+    for p in SAMPLE_HEX:
+        S, d0, d1, d2 = r.shape_hex8(*p)
+        out["shape_hex8"].append({"at": p, "S": S.tolist(), "dxi": d0.tolist(), "deta": d1.tolist(), "dzeta": d2.tolist()})
+    for p in SAMPLE_QUAD:
+        S, d0, d1 = r.shape_quad4(*p)
+        out["shape_quad4"].append({"at": p, "S": S.tolist(), "dxi": d0.tolist(), "deta": d1.tolist()})
+    out["source"] = "reference gauss.cpp + shape.cpp compiled unmodified (oracle/_ref)"
+    return out
+
+
+def matrix_kat():
+    return {
+        "source": "beta/math/matrix.cpp:679-696 (DEBUG_MATRIX_CLASS expected values)",
+        "A": [[1, 2], [3, 1]], "B": [[2, 4], [7, -3]],
+        "A_plus_B": [[3, 6], [10, -2]],
+        "A_times_B": [[16, -2], [13, 9]],
+        "B_inverse": [[0.088235, 0.11765], [0.20588, -0.058824]],
+        "B_inverse_digits": 5,
+    }
+
+
+def oracle_small():
+    out = {}
+    # element matrices on a distorted hex and quad
+    xyz = np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], float)
+    xyz = xyz * np.array([0.7, 1.1, 0.9]) + 0.05 * np.sin(np.arange(24).reshape(8, 3))
+    m9 = W.iso3d_params(np.array([2.0e4]), 0.27)[0]
+    C = bo.cmat_ortho3d(m9)
+    st, Ke = bo.ke_hex8(xyz, C, 2)
+    out["ke_hex8"] = {"xyz": xyz.tolist(), "params": m9.tolist(), "order": 2, "Ke": Ke.tolist()}
+    xy = np.array([[0, 0], [1.2, 0.1], [1.0, 0.9], [-0.1, 1.0]], float)
+    m4 = W.pstress_params(np.array([70e3]), 0.3)[0]
+    st, Kq = bo.ke_quad4(xy, bo.cmat_plane_stress(m4), 2)
+    out["ke_quad4"] = {"xy": xy.tolist(), "params": m4.tolist(), "order": 2, "Ke": Kq.tolist()}
+    st, Kh, Mh = bo.km_hex8_heat(xyz, [1.3, 0.8, 2.1], 1.7, 3)
+    out["km_hex8_heat"] = {"xyz": xyz.tolist(), "k": [1.3, 0.8, 2.1], "c": 1.7, "order": 3, "K": Kh.tolist(),
+                           "M": Mh.tolist()}
+    # a small static system
+    m = W.cube_hex8(3, seed=5)
+    s = bo.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    s.assemble(m.params, m.order)
+    rp, col, val = s.export_lower()
+    rc, u, sst = s.solve(eps=1e-12, maxit=10000)
+    out["cube3"] = {"rowptr": rp.tolist(), "col": col.tolist(), "val": val.tolist(), "u": u.tolist(),
+                    "iterations": sst.iterations, "eps": 1e-12}
+    return out
+
+
+if __name__ == "__main__":
+    with open(os.path.join(OUT, "ref_quadrature.json"), "w") as f:
+        json.dump(ref_quadrature(), f)
+    with open(os.path.join(OUT, "ref_matrix_kat.json"), "w") as f:
+        json.dump(matrix_kat(), f, indent=1)
+    with open(os.path.join(OUT, "oracle_small.json"), "w") as f:
+        json.dump(oracle_small(), f)
+    print("wrote golden fixtures to", OUT)

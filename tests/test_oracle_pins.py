@@ -1,0 +1,177 @@
+"""The oracle pinned against the reference's own code and known answers.
+
+* Gauss points/weights and shape functions vs the reference's gauss.cpp and
+  shape.cpp (golden vectors produced by those files, tests/golden).
+* Dense LU inverse vs the known answer in the reference's matrix.cpp debug main.
+* Analytic element properties the reference's elements must satisfy.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from betanoox_b200 import workloads as W
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _load(name):
+    with open(os.path.join(GOLD, name)) as f:
+        return json.load(f)
+
+
+def test_gauss_matches_reference_golden(oracle):
+    g = _load("ref_quadrature.json")
+    for k, d in g["gauss"].items():
+        x, w = oracle.gauss_1d(int(k))
+        np.testing.assert_array_equal(x, np.array(d["x"]))  # same Newton recurrence: bit-exact
+        np.testing.assert_array_equal(w, np.array(d["w"]))
+
+
+def test_tensor_points_match_reference_golden(oracle):
+    g = _load("ref_quadrature.json")
+    for o, d in g["hex"].items():
+        xi, eta, zeta, w = oracle.hex_points(int(o))
+        for a, key in ((xi, "xi"), (eta, "eta"), (zeta, "zeta"), (w, "w")):
+            np.testing.assert_array_equal(a, np.array(d[key]))
+    for o, d in g["quad"].items():
+        xi, eta, w = oracle.quad_points(int(o))
+        for a, key in ((xi, "xi"), (eta, "eta"), (w, "w")):
+            np.testing.assert_array_equal(a, np.array(d[key]))
+
+
+def test_shape_functions_match_reference_golden(oracle):
+    g = _load("ref_quadrature.json")
+    for d in g["shape_hex8"]:
+        S, d0, d1, d2 = oracle.shape_hex8(*d["at"])
+        for a, key in ((S, "S"), (d0, "dxi"), (d1, "deta"), (d2, "dzeta")):
+            np.testing.assert_allclose(a, np.array(d[key]), rtol=0, atol=1e-15)
+    for d in g["shape_quad4"]:
+        S, d0, d1 = oracle.shape_quad4(*d["at"])
+        for a, key in ((S, "S"), (d0, "dxi"), (d1, "deta")):
+            np.testing.assert_allclose(a, np.array(d[key]), rtol=0, atol=1e-15)
+
+
+def test_reference_leaf_live_if_present(oracle):
+    """When oracle/_ref was built here, compare against it directly as well."""
+    if not oracle.RefLeaf.available():
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    r = oracle.RefLeaf()
+    for k in range(1, 12):
+        x, w = oracle.gauss_1d(k)
+        xr, wr = r.gauss_1d(k)
+        np.testing.assert_array_equal(x, xr)
+        np.testing.assert_array_equal(w, wr)
+    rng = np.random.default_rng(0)
+    for p in rng.uniform(-1, 1, size=(50, 3)):
+        a = oracle.shape_hex8(*p)
+        b = r.shape_hex8(*p)
+        for u, v in zip(a, b):
+            np.testing.assert_allclose(u, v, rtol=0, atol=1e-15)
+
+
+def test_matrix_invert_kat(oracle):
+    k = _load("ref_matrix_kat.json")
+    inv = oracle.invert(np.array(k["B"], float))
+    np.testing.assert_allclose(inv, np.array(k["B_inverse"]), rtol=0, atol=10 ** -k["B_inverse_digits"])
+    A = np.array(k["A"], float)
+    B = np.array(k["B"], float)
+    np.testing.assert_array_equal(A @ B, np.array(k["A_times_B"]))
+    np.testing.assert_array_equal(A + B, np.array(k["A_plus_B"]))
+
+
+def _unit_hex(scale=(1.0, 1.0, 1.0), jitter=0.0):
+    xyz = np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], float)
+    return xyz * np.array(scale) + jitter * np.sin(np.arange(24).reshape(8, 3))
+
+
+def test_hex8_rigid_modes_and_symmetry(oracle):
+    xyz = _unit_hex((0.8, 1.2, 0.9), 0.07)
+    C = oracle.cmat_ortho3d(W.iso3d_params(np.array([1e4]), 0.3)[0])
+    st, K = oracle.ke_hex8(xyz, C, 2)
+    assert st == 0
+    np.testing.assert_allclose(K, K.T, rtol=0, atol=1e-9 * np.abs(K).max())
+    # six rigid-body modes lie in the null space
+    modes = []
+    for c in range(3):
+        m = np.zeros((8, 3)); m[:, c] = 1; modes.append(m.ravel())
+    for (i, j) in ((0, 1), (1, 2), (0, 2)):
+        m = np.zeros((8, 3)); m[:, i] = -xyz[:, j]; m[:, j] = xyz[:, i]; modes.append(m.ravel())
+    for m in modes:
+        assert np.abs(K @ m).max() < 1e-9 * np.abs(K).max()
+    ev = np.linalg.eigvalsh(K)
+    assert (ev[6:] > 1e-8 * ev[-1]).all()
+
+
+def test_hex8_constant_strain_patch(oracle):
+    """A linear displacement field gives Fe = K u consistent with uniform stress."""
+    xyz = _unit_hex((1.0, 1.0, 1.0), 0.05)
+    C = oracle.cmat_ortho3d(W.iso3d_params(np.array([200.0]), 0.25)[0])
+    grad = np.array([[1e-3, 2e-4, 0], [0, -5e-4, 1e-4], [3e-4, 0, 2e-3]])
+    u = (xyz @ grad.T).ravel()
+    st, K = oracle.ke_hex8(xyz, C, 2)
+    fe = oracle.fe_hex8(xyz, C, u, 2)
+    np.testing.assert_allclose(K @ u, fe, rtol=1e-12, atol=1e-15)
+
+
+def test_quad4_and_heat_properties(oracle):
+    xy = np.array([[0, 0], [1.2, 0.1], [1.0, 0.9], [-0.1, 1.0]], float)
+    st, K = oracle.ke_quad4(xy, oracle.cmat_plane_stress(W.pstress_params(np.array([70e3]), 0.3)[0]), 2)
+    assert st == 0
+    for m in (np.tile([1, 0], 4), np.tile([0, 1], 4), np.stack([-xy[:, 1], xy[:, 0]], 1).ravel()):
+        assert np.abs(K @ m).max() < 1e-9 * np.abs(K).max()
+    xyz = _unit_hex((0.5, 0.7, 0.3), 0.02)
+    st, Kh, Mh = oracle.km_hex8_heat(xyz, [1.0, 2.0, 3.0], 1.5, 3)
+    assert np.abs(Kh @ np.ones(8)).max() < 1e-12 * np.abs(Kh).max()
+    # sum of the consistent capacity matrix = c * volume
+    vol = 0.0
+    xi, eta, zeta, w = oracle.hex_points(3)
+    for p in range(len(w)):
+        _, d0, d1, d2 = oracle.shape_hex8(xi[p], eta[p], zeta[p])
+        J = np.stack([d0 @ xyz, d1 @ xyz, d2 @ xyz])
+        vol += np.linalg.det(J) * w[p]
+    assert abs(Mh.sum() - 1.5 * vol) < 1e-12
+
+
+def test_small_system_solves_to_reference_rule(oracle):
+    m = W.plate_quad4(8)
+    s = oracle.System(m)
+    assert s.set_bc(m.restrained, m.prescribed, m.load) == 0
+    s.build_pattern()
+    assert s.assemble(m.params, m.order) == 0
+    rc, u, st = s.solve(eps=1e-10, maxit=10000)
+    assert rc == 0 and st.last_norm < 1e-10
+    # the lower-triangle product equals the full symmetric product
+    rp, col, val = s.export_lower()
+    n = m.ndof
+    A = np.zeros((n, n))
+    for i in range(n):
+        for k in range(rp[i], rp[i + 1]):
+            A[i, col[k]] = val[k]
+            A[col[k], i] = val[k]
+    x = np.random.default_rng(1).normal(size=n)
+    np.testing.assert_allclose(s.matvec(x), A @ x, rtol=1e-13, atol=1e-12)
+    b = s.rhs()
+    np.testing.assert_allclose(A @ u, b, rtol=0, atol=1e-8 * np.abs(b).max())
+
+
+def test_load_on_restrained_is_an_error(oracle):
+    m = W.plate_quad4(4)
+    load = m.load.copy()
+    load[0] = 1.0  # dof 0 belongs to the clamped left edge
+    s = oracle.System(m)
+    assert s.set_bc(m.restrained, m.prescribed, load) == oracle.ERR_LOAD_ON_RESTRAINED
+
+
+def test_oracle_threaded_pcg_matches_serial(oracle):
+    m = W.cube_hex8(5, seed=3)
+    s = oracle.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    s.assemble(m.params, m.order)
+    b = s.rhs()
+    rc1, u1, st1 = s.solve(eps=1e-12, maxit=20000)
+    rc2, u2, st2 = s.solve_threaded(b, eps=1e-12, maxit=20000, threads=4)
+    assert rc1 == 0 and rc2 == 0
+    assert np.linalg.norm(u1 - u2) / np.linalg.norm(u1) < 1e-9
