@@ -21,7 +21,7 @@ NVCC_FLAGS = [
     "-O3", "-std=c++17",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo",
-    "-Xcompiler", "-fPIC,-pthread,-fvisibility=hidden",
+    "-Xcompiler", "-fPIC,-pthread,-fvisibility=hidden,-Wall",
     "-shared", "-cudart", "static",
 ]
 

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -167,6 +168,20 @@ struct beta_gpu_ctx {
 
 namespace {
 
+// BETA_GPU_TRACE=1 in the environment prints each traced step to stderr.
+bool trace_on() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = std::getenv("BETA_GPU_TRACE");
+    on = (e && e[0] && e[0] != '0') ? 1 : 0;
+  }
+  return on == 1;
+}
+#define TRACE(msg)                                                         \
+  do {                                                                     \
+    if (trace_on()) std::fprintf(stderr, "[beta_gpu] %s:%d %s\n", __func__, __LINE__, msg); \
+  } while (0)
+
 int fail(beta_gpu_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
   return code;
@@ -199,12 +214,12 @@ void launch(beta_gpu_ctx* c, void (*k)(KArgs...), int grid, int block, size_t sm
 
 cudaError_t h2d(beta_gpu_ctx* c, void* dst, const void* src, size_t bytes) {
   c->n_h2d += (long long)bytes;
-  return h2d(c, dst, src, bytes);
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
 }
 
 cudaError_t d2h(beta_gpu_ctx* c, void* dst, const void* src, size_t bytes) {
   c->n_d2h += (long long)bytes;
-  return d2h(c, dst, src, bytes);
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
 }
 
 int grid_for(beta_gpu_ctx* c, long long work_items, int per_block) {
@@ -216,8 +231,11 @@ int grid_for(beta_gpu_ctx* c, long long work_items, int per_block) {
 
 template <typename T>
 int upload(beta_gpu_ctx* c, DBuf<T>& d, const T* h, size_t n) {
+  if (trace_on()) std::fprintf(stderr, "[beta_gpu] upload %zu x %zu bytes, buf %p/%zu, stream %p\n", n, sizeof(T), (void*)d.p, d.n, (void*)c->stream);
   CK(d.alloc(n));
+  TRACE("allocated");
   if (n) CK(h2d(c, d.p, h, n * sizeof(T)));
+  TRACE("copy queued");
   return BETA_GPU_OK;
 }
 
@@ -616,7 +634,9 @@ int beta_gpu_counters(const beta_gpu_ctx* c, long long* out, int n) {
 int beta_gpu_mesh_upload(beta_gpu_ctx* c, int kind, int ndim, int nnode, const double* xyz, int nelem,
                          int nnpe, const int* conn, const int* first_dof, int ndpn, int order) {
   if (!c) return BETA_GPU_ERR_ARG;
+  TRACE("enter");
   cudaSetDevice(c->device);
+  TRACE("device set");
   int want_nnpe = 0, want_ndim = 0, want_ndpn = 0;
   switch (kind) {
     case BETA_GPU_QUAD4_PSTRESS: want_nnpe = 4; want_ndim = 2; want_ndpn = 2; break;
@@ -635,14 +655,20 @@ int beta_gpu_mesh_upload(beta_gpu_ctx* c, int kind, int ndim, int nnode, const d
     if (conn[k] < 0 || conn[k] >= nnode) return fail(c, BETA_GPU_ERR_ARG, "connectivity out of range");
   c->kind = kind; c->ndim = ndim; c->nnode = nnode; c->nelem = nelem; c->nnpe = nnpe; c->ndpn = ndpn;
   c->ndof = nnode * ndpn; c->order = order;
+  TRACE("validated");
   c->h_conn.assign(conn, conn + (size_t)nelem * nnpe);
   c->h_first_dof.assign(first_dof, first_dof + nnode);
   int rc;
   if ((rc = upload(c, c->xyz, xyz, (size_t)nnode * ndim))) return rc;
+  TRACE("xyz uploaded");
   if ((rc = upload(c, c->conn, conn, (size_t)nelem * nnpe))) return rc;
+  TRACE("conn uploaded");
   make_gauss_table(ndim, order, c->h_gt);
+  TRACE("gauss table built");
   if ((rc = upload(c, c->gt, &c->h_gt, 1))) return rc;
+  TRACE("gauss table uploaded");
   CK(cudaStreamSynchronize(c->stream));
+  TRACE("synchronized");
   c->have_pattern = false;
   c->have_bc = false;
   c->have_mat = false;
