@@ -26,6 +26,8 @@ TIMEOUT = 10
 ERR_NOT_FINITE = 11
 ERR_LOAD_ON_RESTRAINED = 12
 ERR_UNSUPPORTED = 13
+ERR_TOO_LARGE = 14
+NOALLOC_MAX_ROWS = 262144
 
 QUAD4_PSTRESS = 1
 HEX8_ELASTIC = 2
@@ -47,7 +49,7 @@ STOP_RB = 1
 STATUS_NAMES = {
     0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_STATE", 4: "MAXIT", 5: "BREAKDOWN",
     6: "ERR_NEGDIAG", 7: "ERR_ZERODIAG", 8: "ERR_OOM", 9: "REJECTED", 10: "TIMEOUT",
-    11: "ERR_NOT_FINITE", 12: "ERR_LOAD_ON_RESTRAINED", 13: "ERR_UNSUPPORTED",
+    11: "ERR_NOT_FINITE", 12: "ERR_LOAD_ON_RESTRAINED", 13: "ERR_UNSUPPORTED", 14: "ERR_TOO_LARGE",
 }
 
 
@@ -97,6 +99,7 @@ SIGNATURES = {
     "beta_gpu_heat_run": (_I, [_P, _D, _D, _I, C.POINTER(SolveOpts), C.POINTER(SolveStats), C.POINTER(_I)]),
     "beta_gpu_heat_get_state": (_I, [_P, _P]),
     "beta_gpu_csr_pcg_device": (_I, [_I, _P, _P, _P, _P, _P, _I, _D, _I, _P, C.POINTER(SolveStats)]),
+    "beta_gpu_csr_pcg_device_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _D, _I, _P, C.POINTER(SolveStats)]),
 }
 
 _lib = None

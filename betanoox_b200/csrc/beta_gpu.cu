@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -561,6 +562,33 @@ int fp64_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve_stat
   return status;
 }
 
+}  // namespace
+
+// ---- scratch of beta_gpu_csr_pcg_device_noalloc ----------------------------
+// One fixed array per GPU that loads the library (held until process exit).
+// Host code must never pass g_noalloc_scratch itself to a kernel: on the host
+// the name is a stand-in, not a device address.  noalloc_scratch_address()
+// looks up the real address once per device with cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BETA_GPU_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoallocMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device (set-up on first use).
+cudaError_t noalloc_scratch_address(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = (unsigned char*)g_noalloc_addr[dev];
+  return cudaSuccess;
+}
 }  // namespace
 
 // =============================== C ABI ======================================
@@ -1137,6 +1165,89 @@ int beta_gpu_csr_pcg_device(int n, const int* d_rp, const int* d_ci, const doubl
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(scratch);
+  if (cudaGetLastError() != cudaSuccess && status == BETA_GPU_OK) status = BETA_GPU_ERR_CUDA;
+  return status;
+}
+
+// Jacobi-PCG on caller-owned device CSR with scratch in g_noalloc_scratch:
+// no cudaMalloc/cudaFree, no event creation.  See include/beta_gpu.h.
+int beta_gpu_csr_pcg_device_noalloc(int n, const int* d_rp, const int* d_ci, const double* d_v, const double* d_b,
+                                    double* d_x, int stop_rule, double tol, int maxit, void* stream_ptr,
+                                    beta_gpu_solve_stats* stats) {
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (n > BETA_GPU_NOALLOC_MAX_ROWS) {
+    if (stats) stats->status = BETA_GPU_ERR_TOO_LARGE;
+    return BETA_GPU_ERR_TOO_LARGE;
+  }
+  if (n <= 0 || !d_rp || !d_ci || !d_v || !d_b || !d_x || !(tol > 0)) return BETA_GPU_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream_ptr;
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return BETA_GPU_ERR_CUDA;
+  }
+  unsigned char* scratch = nullptr;
+  if (noalloc_scratch_address(dev, &scratch) != cudaSuccess) {
+    cudaGetLastError();
+    return BETA_GPU_ERR_CUDA;
+  }
+  const int max_grid = std::min(nsm * 8, BETA_GPU_NOALLOC_MAX_BLOCKS);
+  auto grid = [&](long long items) { long long g = (items + 255) / 256; return (int)std::max(1LL, std::min<long long>(g, max_grid)); };
+  // layout inside the fixed array (sized for BETA_GPU_NOALLOC_MAX_ROWS rows)
+  double* r = (double*)scratch;
+  double* p = r + BETA_GPU_NOALLOC_MAX_ROWS;
+  double* q = p + BETA_GPU_NOALLOC_MAX_ROWS;
+  double* dinv = q + BETA_GPU_NOALLOC_MAX_ROWS;
+  double* partials = dinv + BETA_GPU_NOALLOC_MAX_ROWS;
+  double* sums = partials + (size_t)BETA_GPU_NOALLOC_MAX_BLOCKS * 4;
+  PcgState* st = (PcgState*)(sums + 8);
+  unsigned* flags = (unsigned*)(st + 1);
+  unsigned* ticket = flags + 1;
+  static_assert(sizeof(PcgState) + 2 * sizeof(unsigned) <= 256, "noalloc scratch tail");
+  int status = BETA_GPU_OK;
+  PcgState h;
+  std::memset(&h, 0, sizeof(h));
+  h.rule = stop_rule == BETA_GPU_STOP_REF ? kStopRef : kStopRB;
+  h.tol2 = tol * tol;
+  h.maxit = maxit > 0 ? maxit : 10000;
+  CsrMat A{n, d_rp, d_ci, d_v};
+  // The array keeps the previous call's contents: reset the counters and state.
+  cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned), s);
+  cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, s);
+  k_csr_dinv<<<grid(n), 256, 0, s>>>(A, dinv, flags);
+  k_csr_spmv<<<grid((long long)n * 8), 256, 0, s>>>(A, d_x, r, d_b);
+  k_start_s<<<grid(n), 256, 0, s>>>(n, d_x, r, d_b, dinv, p, st, partials);
+  unsigned hf[2] = {0, 0};
+  cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) status = BETA_GPU_ERR_CUDA;
+  else if (hf[0] & 8u) status = BETA_GPU_ERR_ZERODIAG;
+  else if (hf[0] & 16u) status = BETA_GPU_ERR_NEGDIAG;
+  while (status == BETA_GPU_OK) {
+    for (int k = 0; k < 16; ++k) {
+      k_csr_spmv_dot<<<grid((long long)n * 8), 256, 0, s>>>(A, p, q, st, partials);
+      k_update_s<<<grid(n), 256, 0, s>>>(n, d_x, r, p, q, dinv, st, partials);
+      k_pupd_s<<<grid(n), 256, 0, s>>>(n, p, r, dinv, st);
+    }
+    cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) { status = BETA_GPU_ERR_CUDA; break; }
+    if (h.done) {
+      status = h.status == kStatusOk ? BETA_GPU_OK : (h.status == kStatusMaxit ? BETA_GPU_MAXIT : BETA_GPU_BREAKDOWN);
+      break;
+    }
+  }
+  if (status == BETA_GPU_OK || status == BETA_GPU_MAXIT) {
+    k_csr_spmv<<<grid((long long)n * 8), 256, 0, s>>>(A, d_x, q, d_b);
+    k_norm2_diff<<<grid(n), 256, 0, s>>>(n, q, nullptr, sums, partials, ticket);
+    double rr = 0.0;
+    cudaMemcpyAsync(&rr, sums, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) status = BETA_GPU_ERR_CUDA;
+    if (stats) {
+      stats->iterations = h.iter;
+      stats->final_norm = h.last;
+      stats->true_rel_residual = h.bb > 0 ? std::sqrt(rr / h.bb) : std::sqrt(rr);
+    }
+  }
+  if (stats) stats->status = status;
   if (cudaGetLastError() != cudaSuccess && status == BETA_GPU_OK) status = BETA_GPU_ERR_CUDA;
   return status;
 }

@@ -52,7 +52,8 @@ enum {
   BETA_GPU_TIMEOUT = 10,         /* bounded device wait expired                          */
   BETA_GPU_ERR_NOT_FINITE = 11,  /* NaN/Inf in inputs                                    */
   BETA_GPU_ERR_LOAD_ON_RESTRAINED = 12, /* equation.cpp:858-861                          */
-  BETA_GPU_ERR_UNSUPPORTED = 13  /* layout or element kind not supported                 */
+  BETA_GPU_ERR_UNSUPPORTED = 13, /* layout or element kind not supported                 */
+  BETA_GPU_ERR_TOO_LARGE = 14    /* size above a fixed capacity (see the no-alloc solver) */
 };
 
 /* ---- element / material kinds ------------------------------------------ */
@@ -227,6 +228,39 @@ BETA_GPU_API int beta_gpu_heat_get_state(beta_gpu_ctx* ctx, double* u);
 BETA_GPU_API int beta_gpu_csr_pcg_device(int n, const int* d_row_ptr, const int* d_col, const double* d_val,
                             const double* d_b, double* d_x, int stop_rule, double tol, int maxit,
                             void* stream, beta_gpu_solve_stats* stats);
+
+/* ---- allocation-free variant of beta_gpu_csr_pcg_device ------------------ */
+/* No counterpart in the reference (BETA's solvers allocate their work vectors
+ * with new[] on every call, sparse.cpp:139-159).
+ *
+ * Some callers cannot let a library call cudaMalloc: an application that hands
+ * nearly all of HBM to its own memory pool at start-up (a framework's caching
+ * allocator, a serving loop sized to the card) would see the allocation fail
+ * or fragment its pool, and cudaMalloc/cudaFree also synchronize the device,
+ * stalling the caller's other streams.  This entry point allocates nothing: its
+ * scratch (Krylov vectors r, p, q, 1/diag, reduction partials and solver state)
+ * lives in one fixed device array inside the library, of
+ * BETA_GPU_NOALLOC_SCRATCH_BYTES (about 8.1 MiB), which every GPU that loads
+ * the library keeps until the process exits.
+ *
+ * Same arguments, algorithm and results as beta_gpu_csr_pcg_device, except:
+ *   - n may not exceed BETA_GPU_NOALLOC_MAX_ROWS; larger systems return
+ *     BETA_GPU_ERR_TOO_LARGE before any device work;
+ *   - the first call on a device looks up the array's device address for that
+ *     device (make that device current first, and make the first call before
+ *     any stream capture);
+ *   - all calls share the one array: calls that overlap on the GPU (other
+ *     streams, other host threads) race and corrupt each other -- serialize them;
+ *   - stats->ms_solve is not measured (0).
+ * The caller still owns and passes the matrix, b and x. */
+#define BETA_GPU_NOALLOC_MAX_ROWS 262144
+#define BETA_GPU_NOALLOC_MAX_BLOCKS 2048
+#define BETA_GPU_NOALLOC_SCRATCH_BYTES \
+  (8 * (4 * (BETA_GPU_NOALLOC_MAX_ROWS) + 4 * (BETA_GPU_NOALLOC_MAX_BLOCKS) + 8) + 256)
+BETA_GPU_API int beta_gpu_csr_pcg_device_noalloc(int n, const int* d_row_ptr, const int* d_col,
+                                                 const double* d_val, const double* d_b, double* d_x,
+                                                 int stop_rule, double tol, int maxit, void* stream,
+                                                 beta_gpu_solve_stats* stats);
 
 #ifdef __cplusplus
 }
