@@ -44,32 +44,44 @@ def _dist():
 
 
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons in the background."""
+    """Samples SM clock and throttle reasons every 200 ms during the timed
+    region through NVML in-process (no nvidia-smi process per sample)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap"}
 
     def __init__(self, gpu):
         self.gpu = gpu
         self.rows = []
         self._stop = threading.Event()
         self._t = None
+        self._h = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(gpu)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report it, keep timing
+            self._err = str(e)
+            self.max_mhz = None
 
     def _run(self):
+        nv = self._nv
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for line in out.stdout.strip().splitlines():
-                    self.rows.append([x.strip() for x in line.split(",")])
+                sm = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                self.rows.append((sm, rs))
             except Exception:
                 pass
             self._stop.wait(0.2)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
         return self
 
     def __exit__(self, *a):
@@ -79,17 +91,15 @@ class Clocks:
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz,
+                    "reasons": [getattr(self, "_err", "no samples")], "samples": 0}
         reasons = set()
-        for r in self.rows:
-            for k, nm in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+        for _, rs in self.rows:
+            for bit, nm in self.REASONS.items():
+                if rs & bit:
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(self.rows), "source": "nvml"}
 
 
 def _peaks():
@@ -293,7 +303,7 @@ def run_ours(args):
             "config": {"workload": f"hex8 elasticity cube {m.meta['n']}^3, {m.ndof} dofs, lognormal E, "
                                    f"2x2x2 Gauss, z=0 clamped, p=1 on z=1",
                        "global_batch": ws, "ndof": m.ndof, "nelem": m.nelem, "parallelism": f"replicas x{ws}",
-                       "tol": tol, "stop_rule": "||b-Au||/||b||", "inner_tol": args.inner_tol,
+                       "tol": tol, "stop_rule": "||b-Au||/||b||", "replace_delta": args.inner_tol,
                        "l2": "inputs larger than L2 (FP32 matrix ~1 GB per replica)"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "mixed": {"iterations": [s.iterations for s in st_mp], "outer": [s.outer_iterations for s in st_mp],
@@ -419,7 +429,7 @@ def main():
     ap.add_argument("--config", default="cube")
     ap.add_argument("--n", type=int, default=100)
     ap.add_argument("--tol", type=float, default=1e-10)
-    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--inner-tol", type=float, default=0.01)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")

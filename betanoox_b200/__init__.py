@@ -28,7 +28,7 @@ def _ptr(a):
 
 
 def opts(mode=_abi.MODE_MPIR, precond=_abi.PRECOND_BLOCK_JACOBI, stop_rule=_abi.STOP_RB, tol=1e-10,
-         maxit=100000, inner_tol=1e-5, max_outer=40, use_last_solution=0, check_every=0, profile=False):
+         maxit=100000, inner_tol=0.01, max_outer=60, use_last_solution=0, check_every=0, profile=False):
     return SolveOpts(mode, precond, stop_rule, maxit, tol, inner_tol, max_outer, use_last_solution, check_every,
                      1 if profile else 0)
 

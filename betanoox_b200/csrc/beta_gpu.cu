@@ -6,9 +6,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -165,6 +168,7 @@ struct beta_gpu_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> evs;
   int max_grid = 0;
+  std::map<std::tuple<const void*, int, size_t>, int> occ;
 };
 
 namespace {
@@ -206,9 +210,27 @@ int cuda_fail(beta_gpu_ctx* c, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(c, e_, what);  \
   } while (0)
 
-// Kernel launch on the context stream, counted.
+// Resident blocks per SM of a kernel at (block, smem), cached per context.
+int occupancy(beta_gpu_ctx* c, const void* k, int block, size_t smem) {
+  auto key = std::make_tuple(k, block, smem);
+  auto it = c->occ.find(key);
+  if (it != c->occ.end()) return it->second;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, smem) != cudaSuccess || nb < 1) {
+    cudaGetLastError();
+    nb = 1;
+  }
+  c->occ[key] = nb;
+  return nb;
+}
+
+// Kernel launch on the context stream, counted.  Every kernel here is a
+// grid-stride loop, so the grid is clamped to one full wave of resident
+// blocks (SM count x occupancy): no partial second wave.
 template <typename... KArgs, typename... Args>
 void launch(beta_gpu_ctx* c, void (*k)(KArgs...), int grid, int block, size_t smem, Args... args) {
+  const int wave = c->nsm * occupancy(c, (const void*)k, block, smem);
+  if (grid > wave) grid = wave;
   k<<<grid, block, smem, c->stream>>>(args...);
   ++c->n_launch;
 }
@@ -391,10 +413,9 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
         launch(c, k_spmv_dot_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, 
             A, c->p64.p, c->q64.p, c->st.p, c->partials.p);
       } else {
-        using V = typename NV<ND>::T;
         BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p};
-        launch(c, k_spmv_dot_b<ND>, grid_for(c, (long long)c->P.nslice * 32, 256), 256, 0, 
-            A, (const V*)c->v32[2].p, (V*)c->v32[3].p, c->st.p, c->partials.p);
+        launch(c, k_spmv_dot_b<ND>, grid_for(c, (long long)c->P.nslice * 32, 256), 256, 0,
+            A, (const float*)c->v32[2].p, c->v32[3].p, c->st.p, c->partials.p);
       }
       if (prof && prof->on) CK(cudaEventRecord(c->evs[2 * k + 1], c->stream));
       if constexpr (ND == 0) {
@@ -402,12 +423,11 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
                                                                      c->q64.p, c->d64.p, c->st.p, c->partials.p);
         launch(c, k_pupd_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->p64.p, c->r64.p, c->d64.p, c->st.p);
       } else {
-        using V = typename NV<ND>::T;
-        launch(c, k_update_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
-            c->nnode, (V*)c->v32[0].p, (V*)c->v32[1].p, (const V*)c->v32[2].p, (const V*)c->v32[3].p,
-            (const V*)c->minv.p, c->st.p, c->partials.p);
-        launch(c, k_pupd_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
-            c->nnode, (V*)c->v32[2].p, (const V*)c->v32[1].p, (const V*)c->minv.p, c->st.p);
+        launch(c, k_update_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->v32[0].p, c->v32[1].p,
+               (const float*)c->v32[2].p, (const float*)c->v32[3].p, (const float*)c->minv.p, c->st.p,
+               c->partials.p);
+        launch(c, k_pupd_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->v32[2].p,
+               (const float*)c->v32[1].p, (const float*)c->minv.p, (const PcgState*)c->st.p);
       }
     }
     CKL("pcg launch");
@@ -434,9 +454,8 @@ int ensure_workspace(beta_gpu_ctx* c) {
   const size_t n = c->ndof;
   for (DBuf<double>* b : {&c->b64, &c->x64, &c->r64, &c->p64, &c->q64, &c->d64, &c->y64, &c->t64})
     CK(b->alloc(n));
-  const size_t nv = (size_t)c->nnode * (c->ndpn == 3 ? 4 : c->ndpn);
-  for (auto& v : c->v32) CK(v.alloc(nv));
-  CK(c->minv.alloc(nv * c->ndpn));
+  for (auto& v : c->v32) CK(v.alloc((size_t)c->nnode * (c->ndpn == 3 ? 4 : c->ndpn)));  // p (v32[2]) padded for ndpn 3
+  CK(c->minv.alloc((size_t)c->nnode * (c->ndpn * (c->ndpn + 1) / 2)));
   CK(c->u.alloc(n));
   return BETA_GPU_OK;
 }
@@ -446,7 +465,7 @@ int compute_minv(beta_gpu_ctx* c, int precond) {
   if (c->minv_kind == precond) return BETA_GPU_OK;
   CK(cudaMemsetAsync(c->flags.p, 0, sizeof(unsigned), c->stream));
   launch(c, k_minv_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
-      c->nnode, c->bsoff.p, c->ndiag.p, c->bval.p, (typename NV<ND>::T*)c->minv.p,
+      c->nnode, c->bsoff.p, c->ndiag.p, c->bval.p, c->minv.p,
       precond == BETA_GPU_PRECOND_JACOBI ? 1 : 0, c->flags.p);
   CKL("k_minv_b");
   unsigned f = 0;
@@ -457,57 +476,99 @@ int compute_minv(beta_gpu_ctx* c, int precond) {
   return BETA_GPU_OK;
 }
 
-// Mixed-precision refinement on A64 x = b with
-//   residual r = rest ? 0 : load - [K (c1 x + c2 w2) + cm M x]
-// (FP64 matrix-free) and inner FP32 node-block PCG on the assembled matrix.
+// Mixed-precision solve of A64 x = b with reliable updates:
+//   * inner: FP32 block-Jacobi PCG on the assembled node-block matrix,
+//     accumulating its correction y32; alpha, beta and norms are FP64
+//     reductions of FP32 products;
+//   * whenever the FP32 recursive residual has fallen by `delta`
+//     (opts.inner_tol) since the last replacement, or below the target,
+//     x64 += y32 and the residual is replaced by the FP64 true residual
+//       r = rest ? 0 : load - [K (c1 x + c2 w2) + cm M x]
+//     (matrix-free, FP64); the search direction p is kept, so the Krylov
+//     process continues instead of restarting.
 // x64 holds the initial iterate (prescribed values on restrained dofs) on
 // entry and the solution on exit.  bnorm is ||b||.
 template <int ND>
 int mpir_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c2, const double* w2,
               double cm, const double* loadv, double bnorm, beta_gpu_solve_stats* stats, ProfAcc* prof) {
   int rc;
-  using V = typename NV<ND>::T;
   if ((rc = compute_minv<ND>(c, o->precond)) != BETA_GPU_OK) return rc;
+  const int n = c->ndof;
   const int maxit = o->maxit > 0 ? o->maxit : 10000;
-  const int max_outer = o->max_outer > 0 ? o->max_outer : 30;
-  const double itol = o->inner_tol > 0 ? o->inner_tol : 1e-5;
+  const int max_repl = o->max_outer > 0 ? o->max_outer : 40;
+  const double delta = (o->inner_tol > 0 && o->inner_tol < 1) ? o->inner_tol : 0.1;
   const int ce = o->check_every > 0 ? o->check_every : std::max(8, std::min(64, c->ndof / 20000));
-  int total = 0, outer = 0, status = BETA_GPU_OK;
+  const bool ref_rule = o->stop_rule == BETA_GPU_STOP_REF;
+  int status = BETA_GPU_OK, repl = 0;
   double q = 1.0;
-  for (;;) {
-    if ((rc = mf_apply(c, c1, c->x64.p, c2, w2, cm, c->y64.p)) != BETA_GPU_OK) return rc;
-    launch(c, k_residual64, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->rest.p, loadv, c->y64.p,
-                                                                    c->x64.p, c->r64.p, c->sums.p,
-                                                                    c->partials.p, c->ticket.p);
+  float* y32 = c->v32[0].p;
+  float* r32 = c->v32[1].p;
+  // true residual of x64 -> r64, returns ||r|| and ||x||
+  auto true_residual = [&](double* rn, double* xn) -> int {
+    int e;
+    if ((e = mf_apply(c, c1, c->x64.p, c2, w2, cm, c->y64.p)) != BETA_GPU_OK) return e;
+    launch(c, k_residual64, grid_for(c, n, 256), 256, 0, n, c->rest.p, loadv, c->y64.p, c->x64.p, c->r64.p,
+           c->sums.p, c->partials.p, c->ticket.p);
     CKL("k_residual64");
     double s2[2];
-    if ((rc = read_sums(c, 2, s2)) != BETA_GPU_OK) return rc;
-    const double rn = std::sqrt(s2[0]);
-    if (o->stop_rule == BETA_GPU_STOP_REF) q = s2[1] > 0 ? rn / std::sqrt(s2[1]) : (rn == 0 ? 0 : 1e300);
-    else q = bnorm > 0 ? rn / bnorm : rn;
-    if (!std::isfinite(q)) { status = BETA_GPU_BREAKDOWN; break; }
-    if (q < o->tol || rn == 0.0) break;
-    if (outer >= max_outer || total >= maxit) { status = BETA_GPU_MAXIT; break; }
-    ++outer;
-    launch(c, k_to_node32<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->r64.p, 1.0 / rn,
-                                                                        (V*)c->v32[1].p);
-    if ((rc = init_state(c, kStopRel, itol, std::max(1, maxit - total))) != BETA_GPU_OK) return rc;
-    launch(c, k_start_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
-        c->nnode, (V*)c->v32[0].p, (const V*)c->v32[1].p, (V*)c->v32[2].p, (const V*)c->minv.p, c->st.p,
-        c->partials.p);
+    if ((e = read_sums(c, 2, s2)) != BETA_GPU_OK) return e;
+    *rn = std::sqrt(s2[0]);
+    *xn = std::sqrt(s2[1]);
+    return BETA_GPU_OK;
+  };
+  auto stop_q = [&](double rn, double xn) {
+    return ref_rule ? (xn > 0 ? rn / xn : (rn == 0 ? 0.0 : 1e300)) : (bnorm > 0 ? rn / bnorm : rn);
+  };
+  auto set_tolabs = [&](double xn) -> int {
+    // replace early once the FP32 residual says the target is met
+    const double ta = 0.5 * o->tol * (ref_rule ? xn : bnorm);
+    c->h_st->tolabs2 = ta * ta;
+    CK(h2d(c, (char*)c->st.p + offsetof(PcgState, tolabs2), &c->h_st->tolabs2, sizeof(double)));
+    return BETA_GPU_OK;
+  };
+  double rn = 0.0, xn = 0.0;
+  if ((rc = true_residual(&rn, &xn)) != BETA_GPU_OK) return rc;
+  q = stop_q(rn, xn);
+  int iters = 0;
+  if (!std::isfinite(q)) {
+    status = BETA_GPU_BREAKDOWN;
+  } else if (!(q < o->tol) && rn != 0.0) {
+    launch(c, k_to32, grid_for(c, n, 256), 256, 0, (long long)n, (const double*)c->r64.p, 1.0, r32);
+    if ((rc = init_state(c, kRuleReliable, o->tol, maxit)) != BETA_GPU_OK) return rc;
+    c->h_st->delta2 = delta * delta;
+    CK(h2d(c, (char*)c->st.p + offsetof(PcgState, delta2), &c->h_st->delta2, sizeof(double)));
+    if ((rc = set_tolabs(xn)) != BETA_GPU_OK) return rc;
+    launch(c, k_start_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, y32, (const float*)r32, c->v32[2].p,
+           (const float*)c->minv.p, c->st.p, c->partials.p);
     CKL("k_start_b");
-    PcgState s;
-    if ((rc = pcg_loop<ND>(c, ce, prof, &s)) != BETA_GPU_OK) return rc;
-    total += s.iter;
-    if (s.status == kStatusBreakdown && s.iter == 0) { status = BETA_GPU_BREAKDOWN; break; }
-    launch(c, k_axpy_from_node32<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->x64.p, rn,
-                                                                               (const V*)c->v32[0].p);
-    CKL("k_axpy_from_node32");
+    for (;;) {
+      PcgState s;
+      if ((rc = pcg_loop<ND>(c, ce, prof, &s)) != BETA_GPU_OK) return rc;
+      iters = s.iter;
+      if (s.status == kStatusBreakdown) { status = BETA_GPU_BREAKDOWN; break; }
+      // fold the FP32 correction into the FP64 iterate, then measure the truth
+      launch(c, k_axpy_from32, grid_for(c, n, 256), 256, 0, (long long)n, c->x64.p, 1.0, (const float*)y32);
+      CK(cudaMemsetAsync(y32, 0, sizeof(float) * n, c->stream));
+      if ((rc = true_residual(&rn, &xn)) != BETA_GPU_OK) return rc;
+      q = stop_q(rn, xn);
+      if (!std::isfinite(q)) { status = BETA_GPU_BREAKDOWN; break; }
+      if (q < o->tol || rn == 0.0) break;
+      if (s.status == kStatusMaxit || iters >= maxit || repl >= max_repl) { status = BETA_GPU_MAXIT; break; }
+      ++repl;
+      // residual replacement, keep the search direction
+      launch(c, k_to32, grid_for(c, n, 256), 256, 0, (long long)n, (const double*)c->r64.p, 1.0, r32);
+      if (ref_rule && (rc = set_tolabs(xn)) != BETA_GPU_OK) return rc;
+      launch(c, k_replace_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, (const float*)r32,
+             (const float*)c->minv.p, c->st.p, c->partials.p);
+      launch(c, k_pupd_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->v32[2].p, (const float*)r32,
+             (const float*)c->minv.p, (const PcgState*)c->st.p);
+      CKL("replacement");
+    }
   }
   if (stats) {
     stats->status = status;
-    stats->iterations = total;
-    stats->outer_iterations = outer;
+    stats->iterations = iters;
+    stats->outer_iterations = repl;
     stats->final_norm = q;
   }
   return status;
@@ -975,21 +1036,13 @@ int beta_gpu_matvec(beta_gpu_ctx* c, int precision, const double* x, double* y) 
   } else {
     if (!c->have32) return fail(c, BETA_GPU_ERR_STATE, "no FP32 matrix");
     BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p};
-    const int g = grid_for(c, (long long)c->P.nslice * 32, 256), gn = grid_for(c, c->nnode, 256);
-    if (c->ndpn == 3) {
-      launch(c, k_to_node32<3>, gn, 256, 0, c->nnode, c->t64.p, 1.0, (float4*)c->v32[0].p);
-      launch(c, k_spmv_b<3>, g, 256, 0, A, (const float4*)c->v32[0].p, (float4*)c->v32[1].p);
-    } else if (c->ndpn == 2) {
-      launch(c, k_to_node32<2>, gn, 256, 0, c->nnode, c->t64.p, 1.0, (float2*)c->v32[0].p);
-      launch(c, k_spmv_b<2>, g, 256, 0, A, (const float2*)c->v32[0].p, (float2*)c->v32[1].p);
-    } else {
-      launch(c, k_to_node32<1>, gn, 256, 0, c->nnode, c->t64.p, 1.0, c->v32[0].p);
-      launch(c, k_spmv_b<1>, g, 256, 0, A, c->v32[0].p, c->v32[1].p);
-    }
+    const int g = grid_for(c, (long long)c->P.nslice * 32, 256), gn = grid_for(c, n, 256);
+    launch(c, k_to32, gn, 256, 0, (long long)n, (const double*)c->t64.p, 1.0, c->v32[0].p);
+    if (c->ndpn == 3) launch(c, k_spmv_b<3>, g, 256, 0, A, (const float*)c->v32[0].p, c->v32[1].p);
+    else if (c->ndpn == 2) launch(c, k_spmv_b<2>, g, 256, 0, A, (const float*)c->v32[0].p, c->v32[1].p);
+    else launch(c, k_spmv_b<1>, g, 256, 0, A, (const float*)c->v32[0].p, c->v32[1].p);
     CK(cudaMemsetAsync(c->y64.p, 0, sizeof(double) * n, c->stream));
-    if (c->ndpn == 3) launch(c, k_axpy_from_node32<3>, gn, 256, 0, c->nnode, c->y64.p, 1.0, (const float4*)c->v32[1].p);
-    else if (c->ndpn == 2) launch(c, k_axpy_from_node32<2>, gn, 256, 0, c->nnode, c->y64.p, 1.0, (const float2*)c->v32[1].p);
-    else launch(c, k_axpy_from_node32<1>, gn, 256, 0, c->nnode, c->y64.p, 1.0, c->v32[1].p);
+    launch(c, k_axpy_from32, gn, 256, 0, (long long)n, c->y64.p, 1.0, (const float*)c->v32[1].p);
   }
   CKL("matvec");
   CK(d2h(c, y, c->y64.p, sizeof(double) * n));

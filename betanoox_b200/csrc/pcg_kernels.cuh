@@ -10,9 +10,9 @@
 // Two storage forms:
 //   scalar  : FP64 values, one row per dof, restrained columns removed
 //             (plain FP64 PCG, Jacobi)
-//   block   : FP32 values, one row per node with ND x ND blocks, vectors as
-//             float / float2 / float4 per node (mixed-precision inner PCG,
-//             Jacobi or node block-Jacobi)
+//   block   : FP32 values, one row per node with ND x ND blocks, packed FP32
+//             dof vectors (mixed-precision inner PCG, Jacobi or node
+//             block-Jacobi, with reliable updates of the residual)
 #pragma once
 #include "common.cuh"
 
@@ -28,12 +28,16 @@ struct PcgState {
   double tol2;    // squared tolerance
   double last;    // last stop quantity (not squared)
   double pq;
+  double maxrr;   // reliable updates: largest r.r since the last replacement
+  double delta2;  // reliable updates: replace when r.r < delta2 * maxrr
+  double tolabs2; // reliable updates: also replace when r.r < tolabs2
   int iter, maxit, status, done;
   int rule;
   unsigned ticket;
 };
 
-constexpr int kStatusOk = 0, kStatusMaxit = 4, kStatusBreakdown = 5;
+constexpr int kStatusOk = 0, kStatusMaxit = 4, kStatusBreakdown = 5, kStatusReplace = 6;
+enum : int { kRuleReliable = 3 };
 
 // ---- block reduction with last-block finish --------------------------------
 // Each block reduces NV values, writes them to partials[block*NV+k]; the last
@@ -106,9 +110,20 @@ __device__ __forceinline__ void finish_update(PcgState* st, double rz, double rr
     st->done = 1;
     return;
   }
+  if (st->rule == kRuleReliable) {
+    // The FP32 recursive residual has dropped by delta (or below the target):
+    // stop the chunk so the host can replace it with the FP64 true residual.
+    // rho keeps r_old.z_old; beta is formed after the replacement.
+    if (rr > st->maxrr) st->maxrr = rr;
+    if (rr < st->tolabs2 || rr < st->delta2 * st->maxrr) {
+      st->status = kStatusReplace;
+      st->done = 1;
+      return;
+    }
+  }
   st->beta = st->rho != 0.0 ? rz / st->rho : 0.0;
   st->rho = rz;
-  if (q < st->tol2) {
+  if (st->rule != kRuleReliable && q < st->tol2) {
     st->status = kStatusOk;
     st->done = 1;
   } else if (st->iter >= st->maxit) {
@@ -131,16 +146,19 @@ __device__ __forceinline__ double spmv_row_s(const ScalarMat& A, int s, int lane
   const int w = (int)((A.ssoff[s + 1] - A.ssoff[s]) >> 5);
   const int* cp = A.scol + beg;
   const double* vp = A.sval + beg;
-  double acc0 = 0.0, acc1 = 0.0;
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
   int k = 0;
-  for (; k + 1 < w; k += 2) {
-    const int c0 = __ldcs(cp + (long long)k * 32), c1 = __ldcs(cp + (long long)(k + 1) * 32);
-    const double v0 = __ldcs(vp + (long long)k * 32), v1 = __ldcs(vp + (long long)(k + 1) * 32);
+  for (; k + 3 < w; k += 4) {
+    const long long o = (long long)k * 32;
+    const int c0 = __ldcs(cp + o), c1 = __ldcs(cp + o + 32), c2 = __ldcs(cp + o + 64), c3 = __ldcs(cp + o + 96);
+    const double v0 = __ldcs(vp + o), v1 = __ldcs(vp + o + 32), v2 = __ldcs(vp + o + 64), v3 = __ldcs(vp + o + 96);
     acc0 += v0 * __ldg(x + c0);
     acc1 += v1 * __ldg(x + c1);
+    acc2 += v2 * __ldg(x + c2);
+    acc3 += v3 * __ldg(x + c3);
   }
-  if (k < w) acc0 += __ldcs(vp + (long long)k * 32) * __ldg(x + __ldcs(cp + (long long)k * 32));
-  return acc0 + acc1;
+  for (; k < w; ++k) acc0 += __ldcs(vp + (long long)k * 32) * __ldg(x + __ldcs(cp + (long long)k * 32));
+  return (acc0 + acc1) + (acc2 + acc3);
 }
 
 // y = A x (optionally y = b - A x), no reduction.
@@ -249,20 +267,86 @@ __global__ void k_dinv_s(int n, const long long* sdiag, const double* sval, doub
 }
 
 // =========================== node-block FP32 ===============================
-template <int ND> struct NV;
-template <> struct NV<1> { using T = float; };
-template <> struct NV<2> { using T = float2; };
-template <> struct NV<3> { using T = float4; };
+// FP32 vectors are packed dof vectors (node I owns entries ND*I .. ND*I+ND-1,
+// the node-major numbering), so no padding is read or written.  Block-Jacobi
+// factors are the ND*(ND+1)/2 upper entries of the symmetric inverse of each
+// node's diagonal block, packed per node.
+template <int ND>
+struct NodeIO {
+  static constexpr int S = ND * (ND + 1) / 2;
+  __device__ static __forceinline__ void ld(const float* __restrict__ v, long long I, float* o) {
+    if constexpr (ND == 2) {
+      const float2 t = reinterpret_cast<const float2*>(v)[I];
+      o[0] = t.x; o[1] = t.y;
+    } else {
+#pragma unroll
+      for (int i = 0; i < ND; ++i) o[i] = v[ND * I + i];
+    }
+  }
+  __device__ static __forceinline__ void ldg(const float* __restrict__ v, long long I, float* o) {
+    if constexpr (ND == 2) {
+      const float2 t = __ldg(reinterpret_cast<const float2*>(v) + I);
+      o[0] = t.x; o[1] = t.y;
+    } else {
+#pragma unroll
+      for (int i = 0; i < ND; ++i) o[i] = __ldg(v + ND * I + i);
+    }
+  }
+  __device__ static __forceinline__ void st(float* __restrict__ v, long long I, const float* a) {
+    if constexpr (ND == 2) {
+      reinterpret_cast<float2*>(v)[I] = make_float2(a[0], a[1]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < ND; ++i) v[ND * I + i] = a[i];
+    }
+  }
+  // z = M r with M symmetric, packed upper rows: (00,01,02,11,12,22) for ND=3
+  __device__ static __forceinline__ void prec(const float* __restrict__ m, long long I, const float* r, float* z) {
+    float a[S];
+#pragma unroll
+    for (int t = 0; t < S; ++t) a[t] = m[S * I + t];
+    if constexpr (ND == 1) {
+      z[0] = a[0] * r[0];
+    } else if constexpr (ND == 2) {
+      z[0] = fmaf(a[0], r[0], a[1] * r[1]);
+      z[1] = fmaf(a[1], r[0], a[2] * r[1]);
+    } else {
+      z[0] = fmaf(a[0], r[0], fmaf(a[1], r[1], a[2] * r[2]));
+      z[1] = fmaf(a[1], r[0], fmaf(a[3], r[1], a[4] * r[2]));
+      z[2] = fmaf(a[2], r[0], fmaf(a[4], r[1], a[5] * r[2]));
+    }
+  }
+};
 
-template <int ND> __device__ __forceinline__ float comp(const typename NV<ND>::T& v, int i);
-template <> __device__ __forceinline__ float comp<1>(const float& v, int) { return v; }
-template <> __device__ __forceinline__ float comp<2>(const float2& v, int i) { return i ? v.y : v.x; }
-template <> __device__ __forceinline__ float comp<3>(const float4& v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
-
-template <int ND> __device__ __forceinline__ typename NV<ND>::T mk(const float* a);
-template <> __device__ __forceinline__ float mk<1>(const float* a) { return a[0]; }
-template <> __device__ __forceinline__ float2 mk<2>(const float* a) { return make_float2(a[0], a[1]); }
-template <> __device__ __forceinline__ float4 mk<3>(const float* a) { return make_float4(a[0], a[1], a[2], 0.f); }
+// The search direction p is the vector the SpMV gathers: for ND=3 it is
+// padded to float4 per node so a gather is one 16-byte load.
+template <int ND>
+struct PVec {
+  static constexpr int W = (ND == 3) ? 4 : ND;
+  __device__ static __forceinline__ void ldg(const float* __restrict__ v, long long I, float* o) {
+    if constexpr (ND == 3) {
+      const float4 t = __ldg(reinterpret_cast<const float4*>(v) + I);
+      o[0] = t.x; o[1] = t.y; o[2] = t.z;
+    } else {
+      NodeIO<ND>::ldg(v, I, o);
+    }
+  }
+  __device__ static __forceinline__ void ld(const float* __restrict__ v, long long I, float* o) {
+    if constexpr (ND == 3) {
+      const float4 t = reinterpret_cast<const float4*>(v)[I];
+      o[0] = t.x; o[1] = t.y; o[2] = t.z;
+    } else {
+      NodeIO<ND>::ld(v, I, o);
+    }
+  }
+  __device__ static __forceinline__ void st(float* __restrict__ v, long long I, const float* a) {
+    if constexpr (ND == 3) {
+      reinterpret_cast<float4*>(v)[I] = make_float4(a[0], a[1], a[2], 0.f);
+    } else {
+      NodeIO<ND>::st(v, I, a);
+    }
+  }
+};
 
 struct BlockMat {
   int nnode, nslice;
@@ -271,9 +355,9 @@ struct BlockMat {
   const float* bval;
 };
 
-template <int ND>
-__device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane,
-                                           const typename NV<ND>::T* __restrict__ x, float* acc) {
+template <int ND, bool PADDED>
+__device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane, const float* __restrict__ x,
+                                           float* acc) {
   constexpr int BB = ND * ND;
   const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
   const int* cp = A.bcol + (long long)c0 * 32 + lane;
@@ -283,46 +367,48 @@ __device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane,
 #pragma unroll 2
   for (int k = 0; k < w; ++k) {
     const int J = __ldcs(cp + k * 32);
-    const typename NV<ND>::T xv = __ldg(x + J);
+    float xv[ND];
+    if constexpr (PADDED) PVec<ND>::ldg(x, J, xv);
+    else NodeIO<ND>::ldg(x, J, xv);
     float v[BB];
 #pragma unroll
     for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);
 #pragma unroll
     for (int i = 0; i < ND; ++i)
 #pragma unroll
-      for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], comp<ND>(xv, j), acc[i]);
+      for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], xv[j], acc[i]);
   }
 }
 
 template <int ND>
-__global__ void __launch_bounds__(256) k_spmv_b(BlockMat A, const typename NV<ND>::T* __restrict__ x,
-                                                typename NV<ND>::T* __restrict__ y) {
+__global__ void __launch_bounds__(256) k_spmv_b(BlockMat A, const float* __restrict__ x, float* __restrict__ y) {
   const int lane = threadIdx.x & 31;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslice; s += (gridDim.x * blockDim.x) >> 5) {
     float acc[ND];
-    spmv_row_b<ND>(A, s, lane, x, acc);
+    spmv_row_b<ND, false>(A, s, lane, x, acc);
     const int I = s * 32 + lane;
-    if (I < A.nnode) y[I] = mk<ND>(acc);
+    if (I < A.nnode) NodeIO<ND>::st(y, I, acc);
   }
 }
 
+// q = A p, alpha = rho / (p.q)
 template <int ND>
-__global__ void __launch_bounds__(256) k_spmv_dot_b(BlockMat A, const typename NV<ND>::T* __restrict__ p,
-                                                    typename NV<ND>::T* __restrict__ q, PcgState* st,
-                                                    double* partials) {
+__global__ void __launch_bounds__(256) k_spmv_dot_b(BlockMat A, const float* __restrict__ p, float* __restrict__ q,
+                                                    PcgState* st, double* partials) {
   if (st->done) return;
   const int lane = threadIdx.x & 31;
   double acc_d[1] = {0.0};
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslice; s += (gridDim.x * blockDim.x) >> 5) {
     float acc[ND];
-    spmv_row_b<ND>(A, s, lane, p, acc);
+    spmv_row_b<ND, true>(A, s, lane, p, acc);
     const int I = s * 32 + lane;
     if (I < A.nnode) {
-      q[I] = mk<ND>(acc);
-      const typename NV<ND>::T pv = p[I];
+      NodeIO<ND>::st(q, I, acc);
+      float pv[ND];
+      PVec<ND>::ld(p, I, pv);
       float t = 0.f;
 #pragma unroll
-      for (int i = 0; i < ND; ++i) t = fmaf(comp<ND>(pv, i), acc[i], t);
+      for (int i = 0; i < ND; ++i) t = fmaf(pv[i], acc[i], t);
       acc_d[0] += (double)t;
     }
   }
@@ -338,48 +424,34 @@ __global__ void __launch_bounds__(256) k_spmv_dot_b(BlockMat A, const typename N
   }
 }
 
-// Block-Jacobi apply z = Minv r with Minv stored as ND row vectors per node.
+// x += alpha p; r -= alpha q; z = M r; (r.z, r.r, x.x) in FP64
 template <int ND>
-__device__ __forceinline__ void prec_apply(const typename NV<ND>::T* __restrict__ minv, int nnode, int I,
-                                           const float* r, float* z) {
-#pragma unroll
-  for (int i = 0; i < ND; ++i) {
-    const typename NV<ND>::T m = minv[(long long)i * nnode + I];
-    float t = 0.f;
-#pragma unroll
-    for (int j = 0; j < ND; ++j) t = fmaf(comp<ND>(m, j), r[j], t);
-    z[i] = t;
-  }
-}
-
-// x += alpha p; r -= alpha q; z = Minv r; (r.z, r.r, x.x) in FP64
-template <int ND>
-__global__ void __launch_bounds__(256) k_update_b(int nnode, typename NV<ND>::T* __restrict__ x,
-                                                  typename NV<ND>::T* __restrict__ r,
-                                                  const typename NV<ND>::T* __restrict__ p,
-                                                  const typename NV<ND>::T* __restrict__ q,
-                                                  const typename NV<ND>::T* __restrict__ minv, PcgState* st,
-                                                  double* partials) {
+__global__ void __launch_bounds__(256) k_update_b(int nnode, float* __restrict__ x, float* __restrict__ r,
+                                                  const float* __restrict__ p, const float* __restrict__ q,
+                                                  const float* __restrict__ minv, PcgState* st, double* partials) {
   if (st->done) return;
   const float a = (float)st->alpha;
   double acc[3] = {0.0, 0.0, 0.0};
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
-    const typename NV<ND>::T xv = x[I], rv = r[I], pv = p[I], qv = q[I];
-    float xn[ND], rn[ND], z[ND];
+    float xv[ND], rv[ND], pv[ND], qv[ND], z[ND];
+    NodeIO<ND>::ld(x, I, xv);
+    NodeIO<ND>::ld(r, I, rv);
+    PVec<ND>::ld(p, I, pv);
+    NodeIO<ND>::ld(q, I, qv);
 #pragma unroll
     for (int i = 0; i < ND; ++i) {
-      xn[i] = fmaf(a, comp<ND>(pv, i), comp<ND>(xv, i));
-      rn[i] = fmaf(-a, comp<ND>(qv, i), comp<ND>(rv, i));
+      xv[i] = fmaf(a, pv[i], xv[i]);
+      rv[i] = fmaf(-a, qv[i], rv[i]);
     }
-    x[I] = mk<ND>(xn);
-    r[I] = mk<ND>(rn);
-    prec_apply<ND>(minv, nnode, I, rn, z);
+    NodeIO<ND>::st(x, I, xv);
+    NodeIO<ND>::st(r, I, rv);
+    NodeIO<ND>::prec(minv, I, rv, z);
     float rz = 0.f, r2 = 0.f, x2 = 0.f;
 #pragma unroll
     for (int i = 0; i < ND; ++i) {
-      rz = fmaf(rn[i], z[i], rz);
-      r2 = fmaf(rn[i], rn[i], r2);
-      x2 = fmaf(xn[i], xn[i], x2);
+      rz = fmaf(rv[i], z[i], rz);
+      r2 = fmaf(rv[i], rv[i], r2);
+      x2 = fmaf(xv[i], xv[i], x2);
     }
     acc[0] += rz;
     acc[1] += r2;
@@ -389,50 +461,46 @@ __global__ void __launch_bounds__(256) k_update_b(int nnode, typename NV<ND>::T*
   if (reduce_last<3>(acc, partials, &st->ticket, out) && threadIdx.x == 0) finish_update(st, out[0], out[1], out[2]);
 }
 
-// p = Minv r + beta p
+// p = M r + beta p
 template <int ND>
-__global__ void __launch_bounds__(256) k_pupd_b(int nnode, typename NV<ND>::T* __restrict__ p,
-                                                const typename NV<ND>::T* __restrict__ r,
-                                                const typename NV<ND>::T* __restrict__ minv,
-                                                const PcgState* st) {
+__global__ void __launch_bounds__(256) k_pupd_b(int nnode, float* __restrict__ p, const float* __restrict__ r,
+                                                const float* __restrict__ minv, const PcgState* st) {
   if (st->done) return;
   const float bt = (float)st->beta;
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
-    const typename NV<ND>::T rv = r[I], pv = p[I];
-    float rr[ND], z[ND], pn[ND];
+    float rv[ND], pv[ND], z[ND];
+    NodeIO<ND>::ld(r, I, rv);
+    PVec<ND>::ld(p, I, pv);
+    NodeIO<ND>::prec(minv, I, rv, z);
 #pragma unroll
-    for (int i = 0; i < ND; ++i) rr[i] = comp<ND>(rv, i);
-    prec_apply<ND>(minv, nnode, I, rr, z);
-#pragma unroll
-    for (int i = 0; i < ND; ++i) pn[i] = fmaf(bt, comp<ND>(pv, i), z[i]);
-    p[I] = mk<ND>(pn);
+    for (int i = 0; i < ND; ++i) pv[i] = fmaf(bt, pv[i], z[i]);
+    PVec<ND>::st(p, I, pv);
   }
 }
 
-// Inner start: x = 0, r given, p = z = Minv r, rho = r.z, ref0 = r.r
+// Inner start: x = 0, r given, p = z = M r, rho = r.z, ref0 = maxrr = r.r
 template <int ND>
-__global__ void __launch_bounds__(256) k_start_b(int nnode, typename NV<ND>::T* __restrict__ x,
-                                                 const typename NV<ND>::T* __restrict__ r,
-                                                 typename NV<ND>::T* __restrict__ p,
-                                                 const typename NV<ND>::T* __restrict__ minv, PcgState* st,
+__global__ void __launch_bounds__(256) k_start_b(int nnode, float* __restrict__ x, const float* __restrict__ r,
+                                                 float* __restrict__ p, const float* __restrict__ minv, PcgState* st,
                                                  double* partials) {
   double acc[2] = {0.0, 0.0};
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
-    const typename NV<ND>::T rv = r[I];
-    float rr[ND], z[ND], zero[ND];
+    float rv[ND], z[ND], zero[ND];
+    NodeIO<ND>::ld(r, I, rv);
 #pragma unroll
-    for (int i = 0; i < ND; ++i) { rr[i] = comp<ND>(rv, i); zero[i] = 0.f; }
-    prec_apply<ND>(minv, nnode, I, rr, z);
-    p[I] = mk<ND>(z);
-    x[I] = mk<ND>(zero);
+    for (int i = 0; i < ND; ++i) zero[i] = 0.f;
+    NodeIO<ND>::prec(minv, I, rv, z);
+    PVec<ND>::st(p, I, z);
+    NodeIO<ND>::st(x, I, zero);
 #pragma unroll
-    for (int i = 0; i < ND; ++i) { acc[0] += (double)rr[i] * z[i]; acc[1] += (double)rr[i] * rr[i]; }
+    for (int i = 0; i < ND; ++i) { acc[0] += (double)rv[i] * z[i]; acc[1] += (double)rv[i] * rv[i]; }
   }
   double out[2];
   if (reduce_last<2>(acc, partials, &st->ticket, out) && threadIdx.x == 0) {
     st->rho = out[0];
     st->rr = out[1];
     st->ref0 = out[1];
+    st->maxrr = out[1];
     st->xx = 0.0;
     st->iter = 0;
     st->status = kStatusOk;
@@ -443,12 +511,38 @@ __global__ void __launch_bounds__(256) k_start_b(int nnode, typename NV<ND>::T* 
   }
 }
 
-// Block-Jacobi factors: invert the node diagonal block (in FP64) and store its
-// rows; jacobi_only keeps just 1/diag.  Flags non-positive diagonals.
+// Reliable update, second half: r has been replaced by the true residual.
+// rho_new = r.z, beta = rho_new / rho_old, rho = rho_new, maxrr = r.r, and
+// the solve continues (done = 0).  The following k_pupd_b forms p.
 template <int ND>
-__global__ void k_minv_b(int nnode, const int* bsoff, const int* ndiag, const float* bval,
-                         typename NV<ND>::T* minv, int jacobi_only, unsigned* flags) {
-  constexpr int BB = ND * ND;
+__global__ void __launch_bounds__(256) k_replace_b(int nnode, const float* __restrict__ r,
+                                                   const float* __restrict__ minv, PcgState* st, double* partials) {
+  double acc[2] = {0.0, 0.0};
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
+    float rv[ND], z[ND];
+    NodeIO<ND>::ld(r, I, rv);
+    NodeIO<ND>::prec(minv, I, rv, z);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) { acc[0] += (double)rv[i] * z[i]; acc[1] += (double)rv[i] * rv[i]; }
+  }
+  double out[2];
+  if (reduce_last<2>(acc, partials, &st->ticket, out) && threadIdx.x == 0) {
+    st->beta = st->rho != 0.0 ? out[0] / st->rho : 0.0;
+    st->rho = out[0];
+    st->rr = out[1];
+    st->maxrr = out[1];
+    st->status = kStatusOk;
+    st->done = (out[0] == out[0]) ? 0 : 1;
+    if (st->done) st->status = kStatusBreakdown;
+  }
+}
+
+// Block-Jacobi factors: invert the node diagonal block in FP64 and store the
+// packed upper triangle; jacobi_only keeps 1/diag.  Flags non-positive diagonals.
+template <int ND>
+__global__ void k_minv_b(int nnode, const int* bsoff, const int* ndiag, const float* bval, float* minv,
+                         int jacobi_only, unsigned* flags) {
+  constexpr int BB = ND * ND, S = ND * (ND + 1) / 2;
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
     const long long chunk = (long long)bsoff[I >> 5] + ndiag[I];
     double D[9] = {0}, Di[9] = {0};
@@ -464,35 +558,23 @@ __global__ void k_minv_b(int nnode, const int* bsoff, const int* ndiag, const fl
     } else {
       inv3<double>(D, Di);
     }
-    for (int i = 0; i < ND; ++i) {
-      float row[ND];
-      for (int j = 0; j < ND; ++j) row[j] = (float)Di[i * ND + j];
-      minv[(long long)i * nnode + I] = mk<ND>(row);
-    }
+    int t = 0;
+    for (int i = 0; i < ND; ++i)
+      for (int j = i; j < ND; ++j) minv[(long long)S * I + (t++)] = (float)(0.5 * (Di[i * ND + j] + Di[j * ND + i]));
   }
 }
 
-// ======================== FP64 <-> node-block glue ===========================
-// r32 = (float)(r64 * scale) in node layout
-template <int ND>
-__global__ void k_to_node32(int nnode, const double* __restrict__ r64, double scale, typename NV<ND>::T* r32) {
-  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
-    float t[ND];
-#pragma unroll
-    for (int i = 0; i < ND; ++i) t[i] = (float)(r64[(long long)I * ND + i] * scale);
-    r32[I] = mk<ND>(t);
-  }
+// ======================== FP64 <-> FP32 glue ===========================
+// r32 = (float)(r64 * scale)
+__global__ void k_to32(long long n, const double* __restrict__ r64, double scale, float* __restrict__ r32) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    r32[i] = (float)(r64[i] * scale);
 }
 
-// x64 += scale * d32 (node layout)
-template <int ND>
-__global__ void k_axpy_from_node32(int nnode, double* __restrict__ x64, double scale,
-                                   const typename NV<ND>::T* __restrict__ d32) {
-  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
-    const typename NV<ND>::T d = d32[I];
-#pragma unroll
-    for (int i = 0; i < ND; ++i) x64[(long long)I * ND + i] += scale * (double)comp<ND>(d, i);
-  }
+// x64 += scale * d32
+__global__ void k_axpy_from32(long long n, double* __restrict__ x64, double scale, const float* __restrict__ d32) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x64[i] += scale * (double)d32[i];
 }
 
 // ===================== caller-owned CSR (device pointers) =====================
