@@ -15,7 +15,7 @@ import numpy as np
 from . import _abi
 from ._abi import BetaGpuError, SolveOpts, SolveStats
 
-__all__ = ["Solver", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
+__all__ = ["Solver", "Batch", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
 
 
 def build(force: bool = False) -> str:
@@ -151,3 +151,90 @@ class Solver:
         u = np.zeros(self.model.ndof)
         self._check(self.lib.beta_gpu_heat_get_state(self.h, _ptr(u)), "heat_get_state")
         return u
+
+
+class Batch:
+    """Many independent systems solved in one persistent launch (beta_gpu_batch)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, max_systems: int = 4096):
+        self.lib = _abi.load()
+        h = C.c_void_p()
+        st = self.lib.beta_gpu_batch_create(C.byref(h), device, int(hbm_budget), int(max_systems))
+        if st != _abi.OK:
+            raise BetaGpuError(st, "beta_gpu_batch_create failed")
+        self.h = h
+        self.models = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.beta_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _err(self, st, what):
+        msg = self.lib.beta_gpu_batch_last_error(self.h)
+        return BetaGpuError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def add(self, m, raise_on_reject=True):
+        """Returns the system id, or None when the pool has no room (REJECTED)."""
+        xyz = np.ascontiguousarray(m.xyz, dtype=np.float64)
+        conn = np.ascontiguousarray(m.conn, dtype=np.int32)
+        fd = np.ascontiguousarray(m.first_dof, dtype=np.int32)
+        p = np.ascontiguousarray(m.params, dtype=np.float64)
+        r = np.ascontiguousarray(m.restrained, dtype=np.uint8)
+        pr = np.ascontiguousarray(m.prescribed, dtype=np.float64)
+        ld = np.ascontiguousarray(m.load, dtype=np.float64)
+        sid = C.c_int(-1)
+        st = self.lib.beta_gpu_batch_add(self.h, m.kind, m.ndim, m.nnode, _ptr(xyz), m.nelem, m.nnpe, _ptr(conn),
+                                         _ptr(fd), m.ndpn, m.order, p.shape[0], p.shape[1], _ptr(p), None, _ptr(r),
+                                         _ptr(pr), _ptr(ld), C.byref(sid))
+        if st == _abi.REJECTED and not raise_on_reject:
+            return None
+        if st != _abi.OK:
+            raise self._err(st, "batch_add")
+        self.models[sid.value] = m
+        return sid.value
+
+    def run(self, o=None, iters_per_launch=0):
+        """One persistent launch; returns the number of unfinished systems."""
+        o = o or opts()
+        left = C.c_int(0)
+        st = self.lib.beta_gpu_batch_run(self.h, C.byref(o), int(iters_per_launch), C.byref(left))
+        if st != _abi.OK:
+            raise self._err(st, "batch_run")
+        return left.value
+
+    def result(self, sid, with_u=True):
+        st = SolveStats()
+        u = np.zeros(self.models[sid].ndof) if with_u else None
+        rc = self.lib.beta_gpu_batch_result(self.h, sid, _ptr(u), C.byref(st))
+        return rc, u, st
+
+    def remove(self, sid):
+        st = self.lib.beta_gpu_batch_remove(self.h, sid)
+        if st != _abi.OK:
+            raise self._err(st, "batch_remove")
+        self.models.pop(sid, None)
+
+    def tune(self, threads, ctas_per_sm=1):
+        st = self.lib.beta_gpu_batch_tune(self.h, threads, ctas_per_sm)
+        if st != _abi.OK:
+            raise self._err(st, "batch_tune")
+
+    def autotune(self, o=None, budget=40):
+        o = o or opts()
+        t, c = C.c_int(0), C.c_int(0)
+        st = self.lib.beta_gpu_batch_autotune(self.h, C.byref(o), budget, C.byref(t), C.byref(c))
+        if st != _abi.OK:
+            raise self._err(st, "batch_autotune")
+        return t.value, c.value
+
+    def info(self):
+        a = (C.c_longlong * 6)()
+        self.lib.beta_gpu_batch_info(self.h, a, 6)
+        return dict(zip(["live", "used", "pool", "launches", "h2d", "d2h"], list(a)))

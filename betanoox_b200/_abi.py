@@ -99,6 +99,16 @@ SIGNATURES = {
     "beta_gpu_heat_run": (_I, [_P, _D, _D, _I, C.POINTER(SolveOpts), C.POINTER(SolveStats), C.POINTER(_I)]),
     "beta_gpu_heat_get_state": (_I, [_P, _P]),
     "beta_gpu_csr_pcg_device": (_I, [_I, _P, _P, _P, _P, _P, _I, _D, _I, _P, C.POINTER(SolveStats)]),
+    "beta_gpu_batch_create": (_I, [C.POINTER(_P), _I, C.c_longlong, _I]),
+    "beta_gpu_batch_destroy": (_I, [_P]),
+    "beta_gpu_batch_last_error": (C.c_char_p, [_P]),
+    "beta_gpu_batch_add": (_I, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, C.POINTER(_I)]),
+    "beta_gpu_batch_run": (_I, [_P, C.POINTER(SolveOpts), _I, C.POINTER(_I)]),
+    "beta_gpu_batch_result": (_I, [_P, _I, _P, C.POINTER(SolveStats)]),
+    "beta_gpu_batch_remove": (_I, [_P, _I]),
+    "beta_gpu_batch_tune": (_I, [_P, _I, _I]),
+    "beta_gpu_batch_autotune": (_I, [_P, C.POINTER(SolveOpts), _I, C.POINTER(_I), C.POINTER(_I)]),
+    "beta_gpu_batch_info": (_I, [_P, C.POINTER(C.c_longlong), _I]),
     "beta_gpu_csr_pcg_device_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _D, _I, _P, C.POINTER(SolveStats)]),
 }
 

@@ -21,6 +21,7 @@
 #include "mf_kernels.cuh"
 #include "pattern.hpp"
 #include "pcg_kernels.cuh"
+#include "batch_kernels.cuh"
 
 using namespace betagpu;
 
@@ -624,6 +625,8 @@ int fp64_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve_stat
 }
 
 }  // namespace
+
+#include "batch_host.cuh"
 
 // ---- scratch of beta_gpu_csr_pcg_device_noalloc ----------------------------
 // One fixed array per GPU that loads the library (held until process exit).
@@ -1303,6 +1306,294 @@ int beta_gpu_csr_pcg_device_noalloc(int n, const int* d_rp, const int* d_ci, con
   if (stats) stats->status = status;
   if (cudaGetLastError() != cudaSuccess && status == BETA_GPU_OK) status = BETA_GPU_ERR_CUDA;
   return status;
+}
+
+
+// ============================ batch C ABI ====================================
+int beta_gpu_batch_create(beta_gpu_batch** out, int device, long long budget, int max_systems) {
+  if (!out || budget <= 0 || max_systems <= 0 || max_systems > (1 << 20)) return BETA_GPU_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<beta_gpu_batch> bp(new beta_gpu_batch());
+  beta_gpu_batch* b = bp.get();
+  b->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return BETA_GPU_ERR_CUDA; }
+  BCK(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device));
+  BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  BCK(cudaMalloc(&b->pool, (size_t)budget));
+  b->pool_bytes = (size_t)budget;
+  b->free_list[0] = b->pool_bytes & ~size_t(255);
+  b->cap = max_systems;
+  BCK(cudaMalloc(&b->d_sys, sizeof(BSys) * max_systems));
+  BCK(cudaMalloc(&b->d_states, sizeof(BState) * max_systems));
+  BCK(cudaMalloc(&b->d_active, sizeof(int) * max_systems));
+  BCK(cudaMalloc(&b->d_counter, sizeof(int)));
+  BCK(cudaMalloc(&b->d_params, sizeof(BParams)));
+  BCK(cudaMallocHost(&b->h_sys, sizeof(BSys) * max_systems));
+  BCK(cudaMallocHost(&b->h_states, sizeof(BState) * max_systems));
+  BCK(cudaMallocHost(&b->h_active, sizeof(int) * max_systems));
+  BCK(cudaMallocHost(&b->h_params, sizeof(BParams)));
+  *out = bp.release();
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_destroy(beta_gpu_batch* b) {
+  if (!b) return BETA_GPU_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto& g : b->graphs) cudaGraphExecDestroy(g.second);
+  for (auto& t : b->gts) cudaFree(t.second);
+  cudaFree(b->pool);
+  cudaFree(b->d_sys);
+  cudaFree(b->d_states);
+  cudaFree(b->d_active);
+  cudaFree(b->d_counter);
+  cudaFree(b->d_params);
+  cudaFreeHost(b->h_sys);
+  cudaFreeHost(b->h_states);
+  cudaFreeHost(b->h_active);
+  cudaFreeHost(b->h_params);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return BETA_GPU_OK;
+}
+
+const char* beta_gpu_batch_last_error(const beta_gpu_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int beta_gpu_batch_add(beta_gpu_batch* b, int kind, int ndim, int nnode, const double* xyz, int nelem, int nnpe,
+                       const int* conn, const int* first_dof, int ndpn, int order, int ngroups, int nparams,
+                       const double* gp, const int* eg, const unsigned char* restrained, const double* prescribed,
+                       const double* load, int* sys_id) {
+  if (!b || !sys_id) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(b->device);
+  int want_nnpe = 0, want_ndim = 0, want_ndpn = 0, want_np = 0;
+  switch (kind) {
+    case BETA_GPU_QUAD4_PSTRESS: want_nnpe = 4; want_ndim = 2; want_ndpn = 2; want_np = 4; break;
+    case BETA_GPU_HEX8_ELASTIC: want_nnpe = 8; want_ndim = 3; want_ndpn = 3; want_np = 9; break;
+    case BETA_GPU_HEX8_HEAT: want_nnpe = 8; want_ndim = 3; want_ndpn = 1; want_np = 4; break;
+    default: return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "unknown element kind");
+  }
+  if (nnpe != want_nnpe || ndim != want_ndim || ndpn != want_ndpn || nparams != want_np)
+    return bfail(b, BETA_GPU_ERR_ARG, "sizes do not match the element kind");
+  if (nnode <= 0 || nelem <= 0 || !xyz || !conn || !first_dof || !gp || ngroups <= 0 || order < 1 || order > 4)
+    return bfail(b, BETA_GPU_ERR_ARG, "bad mesh or material arguments");
+  if (!eg && ngroups != nelem) return bfail(b, BETA_GPU_ERR_ARG, "without elem_group there must be one group per element");
+  const size_t ndof = (size_t)nnode * ndpn;
+  if (!all_finite(xyz, (size_t)nnode * ndim) || !all_finite(gp, (size_t)ngroups * nparams) ||
+      (prescribed && !all_finite(prescribed, ndof)) || (load && !all_finite(load, ndof)))
+    return bfail(b, BETA_GPU_ERR_NOT_FINITE, "non-finite input");
+  for (long long k = 0; k < (long long)nelem * nnpe; ++k)
+    if (conn[k] < 0 || conn[k] >= nnode) return bfail(b, BETA_GPU_ERR_ARG, "connectivity out of range");
+  if (eg)
+    for (int e = 0; e < nelem; ++e)
+      if (eg[e] < 0 || eg[e] >= ngroups) return bfail(b, BETA_GPU_ERR_ARG, "elem_group out of range");
+  std::vector<unsigned char> r(ndof, 0);
+  if (restrained)
+    for (size_t i = 0; i < ndof; ++i) r[i] = restrained[i] ? 1 : 0;
+  if (load)
+    for (size_t i = 0; i < ndof; ++i)
+      if (r[i] && load[i] != 0.0)
+        return bfail(b, BETA_GPU_ERR_LOAD_ON_RESTRAINED, "Cannot add load to a restrained degree of freedom.");
+  HostPattern P;
+  std::string msg = build_pattern(nnode, nelem, nnpe, ndpn, conn, first_dof, r.data(), P, false);
+  if (!msg.empty()) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, msg);
+  SysLayout L = layout_for(ndim, nnode, nelem, nnpe, ndpn, ngroups, nparams, eg != nullptr, P);
+  int id;
+  if (!b->free_ids.empty()) id = b->free_ids.back();
+  else if ((int)b->sys.size() < b->cap) id = (int)b->sys.size();
+  else return bfail(b, BETA_GPU_REJECTED, "batch holds max_systems systems");
+  const long long off = pool_alloc(b, L.total);
+  if (off < 0) return bfail(b, BETA_GPU_REJECTED, "HBM budget exhausted: the system does not fit in the pool");
+  if (!b->free_ids.empty()) b->free_ids.pop_back();
+  else b->sys.emplace_back();
+  unsigned char* base = b->pool + off;
+  const GaussTable* gt = batch_gauss(b, ndim, order);
+  int rc = gt ? BETA_GPU_OK : BETA_GPU_ERR_CUDA;
+  std::vector<double> zero(ndof, 0.0);
+  auto up = [&](size_t o, const void* src, size_t bytes) { if (!rc) rc = batch_h2d(b, base + o, src, bytes); };
+  up(L.o_xyz, xyz, sizeof(double) * nnode * ndim);
+  up(L.o_conn, conn, sizeof(int) * (size_t)nelem * nnpe);
+  up(L.o_gp, gp, sizeof(double) * (size_t)ngroups * nparams);
+  if (eg) up(L.o_eg, eg, sizeof(int) * nelem);
+  up(L.o_rest, r.data(), ndof);
+  up(L.o_presc, prescribed ? prescribed : zero.data(), sizeof(double) * ndof);
+  up(L.o_load, load ? load : zero.data(), sizeof(double) * ndof);
+  up(L.o_cptr, P.color_ptr.data(), sizeof(int) * P.color_ptr.size());
+  up(L.o_elems, P.elem_by_color.data(), sizeof(int) * P.elem_by_color.size());
+  up(L.o_slot, P.slot.data(), sizeof(int) * P.slot.size());
+  up(L.o_nrp, P.nrp.data(), sizeof(int) * P.nrp.size());
+  up(L.o_ndiag, P.ndiag.data(), sizeof(int) * P.ndiag.size());
+  up(L.o_bsoff, P.bsoff.data(), sizeof(int) * P.bsoff.size());
+  up(L.o_bcol, P.bcol.data(), sizeof(int) * P.bcol.size());
+  if (rc == BETA_GPU_OK && cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); rc = BETA_GPU_ERR_CUDA; }
+  beta_gpu_batch::Sys& S = b->sys[id];
+  if (rc != BETA_GPU_OK) {
+    pool_free(b, off, L.total);
+    S.live = false;
+    b->free_ids.push_back(id);
+    return bfail(b, rc, "upload of the system failed");
+  }
+  S.live = true;
+  S.kind = kind; S.ndim = ndim; S.nnode = nnode; S.nelem = nelem; S.nnpe = nnpe; S.ndpn = ndpn;
+  S.ndof = (int)ndof; S.order = order; S.off = (size_t)off; S.bytes = L.total;
+  S.work = (long long)P.nchunk * 32 * ndpn * ndpn;
+  BSys& D = S.desc;
+  std::memset(&D, 0, sizeof(D));
+  GaussTable hg;
+  make_gauss_table(ndim, order, hg);
+  D.kind = kind; D.ndpn = ndpn; D.nnode = nnode; D.nelem = nelem; D.ndof = (int)ndof; D.nip = hg.nip;
+  D.ncolor = P.ncolor; D.nslice = P.nslice; D.nparams = nparams; D.ndim = ndim;
+  D.xyz = (const double*)(base + L.o_xyz);
+  D.conn = (const int*)(base + L.o_conn);
+  D.gparams = (const double*)(base + L.o_gp);
+  D.egroup = eg ? (const int*)(base + L.o_eg) : nullptr;
+  D.rest = base + L.o_rest;
+  D.presc = (const double*)(base + L.o_presc);
+  D.load = (const double*)(base + L.o_load);
+  D.color_ptr = (const int*)(base + L.o_cptr);
+  D.elems = (const int*)(base + L.o_elems);
+  D.slot = (const int*)(base + L.o_slot);
+  D.nrp = (const int*)(base + L.o_nrp);
+  D.ndiag = (const int*)(base + L.o_ndiag);
+  D.bsoff = (const int*)(base + L.o_bsoff);
+  D.bcol = (const int*)(base + L.o_bcol);
+  D.bval = (float*)(base + L.o_bval);
+  D.x64 = (double*)(base + L.o_x64);
+  D.r64 = (double*)(base + L.o_r64);
+  D.y64 = (double*)(base + L.o_y64);
+  D.y32 = (float*)(base + L.o_y32);
+  D.r32 = (float*)(base + L.o_r32);
+  D.p32 = (float*)(base + L.o_p32);
+  D.q32 = (float*)(base + L.o_q32);
+  D.minv = (float*)(base + L.o_minv);
+  D.gt = gt;
+  D.st = b->d_states + id;
+  D.nchunk = P.nchunk;
+  BState s0;
+  std::memset(&s0, 0, sizeof(s0));
+  s0.phase = kPhaseNew;
+  s0.status = kBRunning;
+  S.st = s0;
+  b->h_states[id] = s0;
+  if ((rc = batch_h2d(b, b->d_states + id, b->h_states + id, sizeof(BState)))) return rc;
+  BCK(cudaStreamSynchronize(b->stream));
+  *sys_id = id;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_run(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int iters_per_launch, int* n_unfinished) {
+  if (!b || !o) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(b->device);
+  int na = 0, rc;
+  if ((rc = batch_prepare(b, o, iters_per_launch, &na))) return rc;
+  if (na > 0) {
+    if ((rc = batch_launch_graph(b))) return rc;
+    if ((rc = batch_pull_states(b))) return rc;
+  }
+  int left = 0;
+  for (auto& S : b->sys)
+    if (S.live && S.st.phase != kPhaseDone) ++left;
+  if (n_unfinished) *n_unfinished = left;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_result(beta_gpu_batch* b, int id, double* u, beta_gpu_solve_stats* st) {
+  if (!b || id < 0 || id >= (int)b->sys.size() || !b->sys[id].live) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(b->device);
+  const beta_gpu_batch::Sys& S = b->sys[id];
+  int status;
+  switch (S.st.status) {
+    case kBConverged: status = S.st.phase == kPhaseDone ? BETA_GPU_OK : BETA_GPU_ERR_STATE; break;
+    case kBMaxit: status = BETA_GPU_MAXIT; break;
+    case kBBreakdown: status = BETA_GPU_BREAKDOWN; break;
+    case kBNegDiag: status = BETA_GPU_ERR_NEGDIAG; break;
+    default: status = BETA_GPU_ERR_STATE;  // still running
+  }
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    st->status = status;
+    st->iterations = S.st.iter;
+    st->outer_iterations = S.st.repl;
+    st->final_norm = S.st.bn > 0 ? S.st.rn / S.st.bn : S.st.rn;
+    st->true_rel_residual = st->final_norm;
+  }
+  if (u) {
+    b->n_d2h += (long long)(sizeof(double) * S.ndof);
+    BCK(cudaMemcpyAsync(u, S.desc.x64, sizeof(double) * S.ndof, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+  }
+  return status;
+}
+
+int beta_gpu_batch_remove(beta_gpu_batch* b, int id) {
+  if (!b || id < 0 || id >= (int)b->sys.size() || !b->sys[id].live) return BETA_GPU_ERR_ARG;
+  beta_gpu_batch::Sys& S = b->sys[id];
+  pool_free(b, S.off, S.bytes);
+  S.live = false;
+  S.st.phase = kPhaseDone;
+  b->free_ids.push_back(id);
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_tune(beta_gpu_batch* b, int threads, int ctas_per_sm) {
+  if (!b || !(threads == 256 || threads == 512 || threads == 1024) || ctas_per_sm < 1 || ctas_per_sm > 4)
+    return BETA_GPU_ERR_ARG;
+  int nb = 0;
+  const void* k = threads == 256 ? (const void*)k_batch_solve<256>
+                                 : threads == 1024 ? (const void*)k_batch_solve<1024> : (const void*)k_batch_solve<512>;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, 0) != cudaSuccess) { cudaGetLastError(); nb = 1; }
+  if (ctas_per_sm > nb) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "launch shape exceeds the SM's resident-block limit");
+  b->threads = threads;
+  b->ctas_per_sm = ctas_per_sm;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, int* threads_out,
+                            int* ctas_out) {
+  if (!b || !o || budget <= 0) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(b->device);
+  const int shapes[][2] = {{256, 1}, {256, 2}, {512, 1}, {512, 2}, {1024, 1}};
+  double best = 1e300;
+  int bt = b->threads, bc = b->ctas_per_sm, rc = BETA_GPU_OK;
+  cudaEvent_t e0, e1;
+  BCK(cudaEventCreate(&e0));
+  BCK(cudaEventCreate(&e1));
+  for (auto& sh : shapes) {
+    if (beta_gpu_batch_tune(b, sh[0], sh[1]) != BETA_GPU_OK) continue;
+    if ((rc = batch_reset_states(b))) break;
+    int na = 0;
+    if ((rc = batch_prepare(b, o, budget, &na))) break;
+    if (na == 0) break;
+    cudaEventRecord(e0, b->stream);
+    if ((rc = batch_launch_graph(b))) break;
+    cudaEventRecord(e1, b->stream);
+    if ((rc = batch_pull_states(b))) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    long long its = 0;
+    for (auto& S : b->sys)
+      if (S.live) its += S.st.iter;
+    const double per_it = its > 0 ? ms / its : 1e300;
+    if (per_it < best) { best = per_it; bt = sh[0]; bc = sh[1]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != BETA_GPU_OK) return rc;
+  b->threads = bt;
+  b->ctas_per_sm = bc;
+  if ((rc = batch_reset_states(b))) return rc;
+  BCK(cudaStreamSynchronize(b->stream));
+  if (threads_out) *threads_out = bt;
+  if (ctas_out) *ctas_out = bc;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_info(const beta_gpu_batch* b, long long* out, int n) {
+  if (!b || !out || n < 0 || n > 6) return BETA_GPU_ERR_ARG;
+  long long live = 0;
+  for (auto& S : b->sys) live += S.live ? 1 : 0;
+  const long long v[6] = {live, (long long)b->used, (long long)b->pool_bytes, b->n_launch, b->n_h2d, b->n_d2h};
+  for (int i = 0; i < n; ++i) out[i] = v[i];
+  return BETA_GPU_OK;
 }
 
 }  // extern "C"

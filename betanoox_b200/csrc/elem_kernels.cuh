@@ -110,18 +110,11 @@ __device__ __forceinline__ void scatter_block64(const ElemArgs& A, int I, int J,
 // ---- hex8 linear elasticity, one warp per element ------------------------
 // lane = 8*a0 + b handles pairs (a0,b) and (a0+4,b).
 template <typename T>
-__global__ void __launch_bounds__(256) k_asm_hex8_elastic(ElemArgs A, const int* __restrict__ elems,
-                                                          int nel) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s_dN = reinterpret_cast<T*>(smem_raw);
-  T* s_N = s_dN + A.nip * 24;
-  T* s_w = s_N + A.nip * 8;
-  stage_gauss<T, 8, 3>(A.gt, A.nip, s_dN, s_N, s_w);
-
+__device__ __forceinline__ void asm_hex8_elastic_warp(const ElemArgs& A, const int* __restrict__ elems, int nel, int w,
+    const T* s_dN, const T* s_N, const T* s_w) {
   const int lane = threadIdx.x & 31;
   const int b = lane & 7, a0 = lane >> 3, a1 = a0 + 4;
-  const int wpb = blockDim.x >> 5;
-  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < nel; w += gridDim.x * wpb) {
+  {
     const int e = elems[w];
     const int* ce = A.conn + (long long)e * 8;
     const int J = ce[b];
@@ -208,21 +201,27 @@ __global__ void __launch_bounds__(256) k_asm_hex8_elastic(ElemArgs A, const int*
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_asm_hex8_elastic(ElemArgs A, const int* __restrict__ elems,
+    int nel) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_dN = reinterpret_cast<T*>(smem_raw);
+  T* s_N = s_dN + A.nip * 24;
+  T* s_w = s_N + A.nip * 8;
+  stage_gauss<T, 8, 3>(A.gt, A.nip, s_dN, s_N, s_w);
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < nel; w += gridDim.x * wpb)
+    asm_hex8_elastic_warp<T>(A, elems, nel, w, s_dN, s_N, s_w);
+}
+
 // ---- quad4 plane stress, two elements per warp ---------------------------
 // lane = 16*sub + 4*a + b handles pair (a,b) of element 2*warp+sub.
 template <typename T>
-__global__ void __launch_bounds__(256) k_asm_quad4_pstress(ElemArgs A, const int* __restrict__ elems,
-                                                           int nel) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s_dN = reinterpret_cast<T*>(smem_raw);
-  T* s_N = s_dN + A.nip * 8;
-  T* s_w = s_N + A.nip * 4;
-  stage_gauss<T, 4, 2>(A.gt, A.nip, s_dN, s_N, s_w);
-
+__device__ __forceinline__ void asm_quad4_pstress_warp(const ElemArgs& A, const int* __restrict__ elems, int nel, int w,
+    const T* s_dN, const T* s_N, const T* s_w) {
   const int lane = threadIdx.x & 31;
   const int sub = lane >> 4, q = lane & 15, a = q >> 2, b = q & 3;
-  const int wpb = blockDim.x >> 5;
-  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 2 * w < nel; w += gridDim.x * wpb) {
+  {
     const int idx = 2 * w + sub;
     const bool valid = idx < nel;
     const int e = elems[valid ? idx : nel - 1];
@@ -270,20 +269,26 @@ __global__ void __launch_bounds__(256) k_asm_quad4_pstress(ElemArgs A, const int
   }
 }
 
-// ---- hex8 diffusion: kscale*K + mscale*M, one warp per element -------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_asm_hex8_heat(ElemArgs A, const int* __restrict__ elems,
-                                                       int nel) {
+__global__ void __launch_bounds__(256) k_asm_quad4_pstress(ElemArgs A, const int* __restrict__ elems,
+    int nel) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_dN = reinterpret_cast<T*>(smem_raw);
-  T* s_N = s_dN + A.nip * 24;
-  T* s_w = s_N + A.nip * 8;
-  stage_gauss<T, 8, 3>(A.gt, A.nip, s_dN, s_N, s_w);
+  T* s_N = s_dN + A.nip * 8;
+  T* s_w = s_N + A.nip * 4;
+  stage_gauss<T, 4, 2>(A.gt, A.nip, s_dN, s_N, s_w);
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 2 * w < nel; w += gridDim.x * wpb)
+    asm_quad4_pstress_warp<T>(A, elems, nel, w, s_dN, s_N, s_w);
+}
 
+// ---- hex8 diffusion: kscale*K + mscale*M, one warp per element -------------
+template <typename T>
+__device__ __forceinline__ void asm_hex8_heat_warp(const ElemArgs& A, const int* __restrict__ elems, int nel, int w,
+    const T* s_dN, const T* s_N, const T* s_w) {
   const int lane = threadIdx.x & 31;
   const int b = lane & 7, a0 = lane >> 3, a1 = a0 + 4;
-  const int wpb = blockDim.x >> 5;
-  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < nel; w += gridDim.x * wpb) {
+  {
     const int e = elems[w];
     const int* ce = A.conn + (long long)e * 8;
     const int J = ce[b];
@@ -341,6 +346,19 @@ __global__ void __launch_bounds__(256) k_asm_hex8_heat(ElemArgs A, const int* __
       }
     }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_asm_hex8_heat(ElemArgs A, const int* __restrict__ elems,
+    int nel) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_dN = reinterpret_cast<T*>(smem_raw);
+  T* s_N = s_dN + A.nip * 24;
+  T* s_w = s_N + A.nip * 8;
+  stage_gauss<T, 8, 3>(A.gt, A.nip, s_dN, s_N, s_w);
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < nel; w += gridDim.x * wpb)
+    asm_hex8_heat_warp<T>(A, elems, nel, w, s_dN, s_N, s_w);
 }
 
 // Restrained diagonals = 1 (Equations::addMatrix, equation.cpp:500).

@@ -28,19 +28,10 @@ struct MfArgs {
 };
 
 // hex8 elasticity: 8 lanes per element, 4 elements per warp.
-__global__ void __launch_bounds__(256) k_mf_hex8_elastic(MfArgs A, const int* __restrict__ elems,
-                                                         int nel, const double* __restrict__ w1,
-                                                         const double* __restrict__ w2,
-                                                         double* __restrict__ y) {
-  __shared__ double s_dN[kMaxIP * 24];
-  __shared__ double s_w[kMaxIP];
-  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
-    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
-  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
-  __syncthreads();
+__device__ __forceinline__ void mf_hex8_elastic_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
+    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y, const double* s_dN, const double* s_w) {
   const int lane = threadIdx.x & 31, b = lane & 7;
-  const int wpb = blockDim.x >> 5;
-  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 4 * w < nel; w += gridDim.x * wpb) {
+  {
     const int idx = 4 * w + (lane >> 3);
     const bool valid = idx < nel;
     const int e = elems[valid ? idx : nel - 1];
@@ -95,19 +86,24 @@ __global__ void __launch_bounds__(256) k_mf_hex8_elastic(MfArgs A, const int* __
   }
 }
 
-// quad4 plane stress: 4 lanes per element, 8 elements per warp.
-__global__ void __launch_bounds__(256) k_mf_quad4_pstress(MfArgs A, const int* __restrict__ elems,
-                                                          int nel, const double* __restrict__ w1,
-                                                          const double* __restrict__ w2,
-                                                          double* __restrict__ y) {
-  __shared__ double s_dN[kMaxIP * 8];
+__global__ void __launch_bounds__(256) k_mf_hex8_elastic(MfArgs A, const int* __restrict__ elems, int nel,
+    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 24];
   __shared__ double s_w[kMaxIP];
-  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_dN[i] = A.gt->dN[i / 8][(i / 4) % 2][i % 4];
+  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
+    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
   for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
   __syncthreads();
-  const int lane = threadIdx.x & 31, b = lane & 3;
   const int wpb = blockDim.x >> 5;
-  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 8 * w < nel; w += gridDim.x * wpb) {
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 4 * w < nel; w += gridDim.x * wpb)
+    mf_hex8_elastic_warp(A, elems, nel, w, w1, w2, y, s_dN, s_w);
+}
+
+// quad4 plane stress: 4 lanes per element, 8 elements per warp.
+__device__ __forceinline__ void mf_quad4_pstress_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
+    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y, const double* s_dN, const double* s_w) {
+  const int lane = threadIdx.x & 31, b = lane & 3;
+  {
     const int idx = 8 * w + (lane >> 2);
     const bool valid = idx < nel;
     const int e = elems[valid ? idx : nel - 1];
@@ -140,22 +136,23 @@ __global__ void __launch_bounds__(256) k_mf_quad4_pstress(MfArgs A, const int* _
   }
 }
 
-// hex8 diffusion: y += K (c1 w1 + c2 w2) + cm M w1, 8 lanes per element.
-__global__ void __launch_bounds__(256) k_mf_hex8_heat(MfArgs A, const int* __restrict__ elems, int nel,
-                                                      const double* __restrict__ w1,
-                                                      const double* __restrict__ w2,
-                                                      double* __restrict__ y) {
-  __shared__ double s_dN[kMaxIP * 24];
-  __shared__ double s_N[kMaxIP * 8];
+__global__ void __launch_bounds__(256) k_mf_quad4_pstress(MfArgs A, const int* __restrict__ elems, int nel,
+    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 8];
   __shared__ double s_w[kMaxIP];
-  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
-    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
-  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_N[i] = A.gt->N[i / 8][i % 8];
+  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_dN[i] = A.gt->dN[i / 8][(i / 4) % 2][i % 4];
   for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
   __syncthreads();
-  const int lane = threadIdx.x & 31, b = lane & 7;
   const int wpb = blockDim.x >> 5;
-  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 4 * w < nel; w += gridDim.x * wpb) {
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 8 * w < nel; w += gridDim.x * wpb)
+    mf_quad4_pstress_warp(A, elems, nel, w, w1, w2, y, s_dN, s_w);
+}
+
+// hex8 diffusion: y += K (c1 w1 + c2 w2) + cm M w1, 8 lanes per element.
+__device__ __forceinline__ void mf_hex8_heat_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
+    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y, const double* s_dN, const double* s_N, const double* s_w) {
+  const int lane = threadIdx.x & 31, b = lane & 7;
+  {
     const int idx = 4 * w + (lane >> 3);
     const bool valid = idx < nel;
     const int e = elems[valid ? idx : nel - 1];
@@ -190,6 +187,21 @@ __global__ void __launch_bounds__(256) k_mf_hex8_heat(MfArgs A, const int* __res
     }
     if (valid) y[J] += f;
   }
+}
+
+__global__ void __launch_bounds__(256) k_mf_hex8_heat(MfArgs A, const int* __restrict__ elems, int nel,
+    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 24];
+  __shared__ double s_N[kMaxIP * 8];
+  __shared__ double s_w[kMaxIP];
+  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
+    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
+  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_N[i] = A.gt->N[i / 8][i % 8];
+  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
+  __syncthreads();
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 4 * w < nel; w += gridDim.x * wpb)
+    mf_hex8_heat_warp(A, elems, nel, w, w1, w2, y, s_dN, s_N, s_w);
 }
 
 }  // namespace betagpu

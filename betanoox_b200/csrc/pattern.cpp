@@ -21,7 +21,7 @@ static void parallel_for(long long n, const std::function<void(long long, long l
 }
 
 std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* conn,
-                          const int* first_dof, const unsigned char* rest, HostPattern& P) {
+                          const int* first_dof, const unsigned char* rest, HostPattern& P, bool with_scalar) {
   if (nnode <= 0 || nelem <= 0 || nnpe <= 0 || nnpe > 8 || ndpn < 1 || ndpn > 3)
     return "build_pattern: bad sizes";
   for (int i = 0; i < nnode; ++i)
@@ -142,6 +142,7 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   });
 
   // ---- scalar sliced ELL over dofs ------------------------------------
+  if (!with_scalar) return "";
   const int ndof = P.ndof;
   std::vector<int> ufree(nnode, 0);
   for (int i = 0; i < nnode; ++i)

@@ -61,8 +61,10 @@ struct HostPattern {
 
 // Builds everything above.  conn: nelem*nnpe; restrained: ndof (0/1).
 // Returns an empty string on success, else an error message.
+// with_scalar = false skips the scalar FP64 layout (mixed-precision-only users).
 std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* conn,
-                          const int* first_dof, const unsigned char* restrained, HostPattern& P);
+                          const int* first_dof, const unsigned char* restrained, HostPattern& P,
+                          bool with_scalar = true);
 
 // Lower-triangle pattern export in SymmetricSparseMatrix order.
 void export_lower_pattern(const HostPattern& P, const unsigned char* restrained,

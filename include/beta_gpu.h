@@ -229,6 +229,49 @@ BETA_GPU_API int beta_gpu_csr_pcg_device(int n, const int* d_row_ptr, const int*
                             const double* d_b, double* d_x, int stop_rule, double tol, int maxit,
                             void* stream, beta_gpu_solve_stats* stats);
 
+/* ---- batched systems in one persistent launch ----------------------------- */
+/* No single counterpart in the reference, which solves one model per run
+ * (BasicModel::DoAnalysis, BasicModel.cpp:1169-1220); each system goes through
+ * the same path: structure (equation.cpp:1216-1267), FP32 assembly
+ * (SerialAssembler.cpp:35-59 + equation.cpp:445-562) and the solve of
+ * sparse.cpp:114-242, here in mixed precision with FP64 residual replacement.
+ *
+ * A batch owns a device pool of hbm_budget_bytes.  beta_gpu_batch_add builds a
+ * system's structure on the host and copies it into the pool, or returns
+ * BETA_GPU_REJECTED when the pool has no room (admission by HBM budget).
+ * beta_gpu_batch_run assembles and solves every unfinished system in one
+ * persistent launch (a replayed CUDA graph): each CTA takes whole systems,
+ * largest first.  iters_per_launch > 0 bounds the PCG iterations each system
+ * gets per launch, so a serving loop can admit and retire systems between
+ * launches; the Krylov state stays in the pool.  Stop rule: ||b-Au||/||b||
+ * (opts->tol); opts->inner_tol is the residual-replacement factor.  Batched
+ * diffusion systems are steady (conductivity only). */
+typedef struct beta_gpu_batch beta_gpu_batch;
+BETA_GPU_API int beta_gpu_batch_create(beta_gpu_batch** batch, int device, long long hbm_budget_bytes,
+                                       int max_systems);
+BETA_GPU_API int beta_gpu_batch_destroy(beta_gpu_batch* batch);
+BETA_GPU_API const char* beta_gpu_batch_last_error(const beta_gpu_batch* batch);
+BETA_GPU_API int beta_gpu_batch_add(beta_gpu_batch* batch, int kind, int ndim, int nnode, const double* xyz,
+                                    int nelem, int nnpe, const int* conn, const int* first_dof, int ndof_per_node,
+                                    int integration_order, int ngroups, int nparams, const double* group_params,
+                                    const int* elem_group, const unsigned char* restrained,
+                                    const double* prescribed, const double* load, int* sys_id);
+BETA_GPU_API int beta_gpu_batch_run(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int iters_per_launch,
+                                    int* n_unfinished);
+/* Status/iterations of one system; u (ndof, may be NULL) receives its current solution. */
+BETA_GPU_API int beta_gpu_batch_result(beta_gpu_batch* batch, int sys_id, double* u,
+                                       beta_gpu_solve_stats* stats);
+BETA_GPU_API int beta_gpu_batch_remove(beta_gpu_batch* batch, int sys_id);
+/* Launch shape: threads per CTA (256, 512 or 1024) and CTAs per SM. */
+BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta, int ctas_per_sm);
+/* Times every launch shape on the current systems for `budget` iterations each
+ * (systems are reset to unsolved afterwards) and keeps the fastest. */
+BETA_GPU_API int beta_gpu_batch_autotune(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int budget,
+                                         int* threads_per_cta, int* ctas_per_sm);
+/* out[0] live systems, out[1] pool bytes in use, out[2] pool bytes, out[3]
+ * launches, out[4] bytes host->device, out[5] bytes device->host; n <= 6. */
+BETA_GPU_API int beta_gpu_batch_info(const beta_gpu_batch* batch, long long* out, int n);
+
 /* ---- allocation-free variant of beta_gpu_csr_pcg_device ------------------ */
 /* No counterpart in the reference (BETA's solvers allocate their work vectors
  * with new[] on every call, sparse.cpp:139-159).

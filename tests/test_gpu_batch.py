@@ -1,0 +1,97 @@
+"""Batched persistent solves: every system's answer equals its own solve.
+
+Each system in a batch is checked against the FP64 oracle solution (1e-8
+relative L2, the mixed-precision contract), and a batch advanced in short
+launches (the serving loop's preemption) must give bit-identical iterates to
+one uninterrupted launch.
+"""
+import numpy as np
+import pytest
+
+from betanoox_b200 import Batch, _abi, opts
+from betanoox_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _truth(oracle, m):
+    s = oracle.System(m)
+    assert s.set_bc(m.restrained, m.prescribed, m.load) == 0
+    s.build_pattern()
+    assert s.assemble(m.params, m.order) == 0
+    rc, u, _ = s.solve(eps=1e-14, maxit=300000)
+    return u
+
+
+def _steady_heat(n=6):
+    m = W.heat_slab(n, n, n // 2 + 2, order=2)
+    pres = np.zeros(m.ndof)
+    pres[np.isclose(m.xyz[:, 0], 0.0)] = 1.0  # T = 1 on x = 0, T = 0 on the other faces
+    m.prescribed = pres
+    return m
+
+
+def _mix():
+    return [W.rve_hex8(6, 1), W.cube_hex8(5, seed=2), W.plate_quad4(10), _steady_heat(6), W.rve_hex8(8, 3),
+            W.plate_quad4(7, E=2e4)]
+
+
+def test_batch_each_system_matches_oracle(oracle):
+    models = _mix()
+    b = Batch(hbm_budget=1 << 30)
+    ids = [b.add(m) for m in models]
+    assert b.run(opts(tol=1e-12)) == 0
+    for sid, m in zip(ids, models):
+        rc, u, st = b.result(sid)
+        assert rc == _abi.OK, st.as_dict()
+        ut = _truth(oracle, m)
+        assert np.linalg.norm(u - ut) / np.linalg.norm(ut) <= 1e-8, (m.name, st.as_dict())
+
+
+def test_batch_short_launches_equal_one_launch():
+    models = _mix()
+    b1 = Batch(hbm_budget=1 << 30)
+    ids1 = [b1.add(m) for m in models]
+    b1.run(opts(tol=1e-12))
+    b2 = Batch(hbm_budget=1 << 30)
+    ids2 = [b2.add(m) for m in models]
+    launches = 0
+    while b2.run(opts(tol=1e-12), iters_per_launch=7) > 0:
+        launches += 1
+        assert launches < 10000
+    assert launches > 1
+    for i1, i2 in zip(ids1, ids2):
+        _, u1, s1 = b1.result(i1)
+        _, u2, s2 = b2.result(i2)
+        assert s1.iterations == s2.iterations
+        np.testing.assert_array_equal(u1, u2)
+
+
+def test_batch_admission_by_budget_and_reuse():
+    small = W.rve_hex8(6, 4)
+    b = Batch(hbm_budget=24 << 20)  # room for only a few small systems
+    ids = []
+    while True:
+        sid = b.add(small, raise_on_reject=False)
+        if sid is None:
+            break
+        ids.append(sid)
+        assert len(ids) < 1000
+    assert len(ids) >= 1
+    info = b.info()
+    assert info["used"] <= info["pool"]
+    b.remove(ids[0])
+    assert b.add(small, raise_on_reject=False) is not None  # freed memory is reused
+
+
+def test_batch_autotune_keeps_results(oracle):
+    models = _mix()[:3]
+    b = Batch(hbm_budget=1 << 30)
+    ids = [b.add(m) for m in models]
+    t, c = b.autotune(opts(tol=1e-12), budget=10)
+    assert t in (256, 512, 1024) and c >= 1
+    assert b.run(opts(tol=1e-12)) == 0
+    for sid, m in zip(ids, models):
+        rc, u, st = b.result(sid)
+        ut = _truth(oracle, m)
+        assert rc == _abi.OK and np.linalg.norm(u - ut) / np.linalg.norm(ut) <= 1e-8
