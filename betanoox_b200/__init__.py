@@ -221,8 +221,8 @@ class Batch:
             raise self._err(st, "batch_remove")
         self.models.pop(sid, None)
 
-    def tune(self, threads, ctas_per_sm=1):
-        st = self.lib.beta_gpu_batch_tune(self.h, threads, ctas_per_sm)
+    def tune(self, threads, cluster=1):
+        st = self.lib.beta_gpu_batch_tune(self.h, threads, cluster)
         if st != _abi.OK:
             raise self._err(st, "batch_tune")
 

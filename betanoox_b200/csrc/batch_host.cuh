@@ -2,7 +2,7 @@
 // beta_gpu_batch_*): a device memory pool with first-fit allocation and an
 // HBM budget, per-system structure building and upload, the descriptor table
 // and work list, the launch (captured once into a CUDA graph and replayed),
-// and a small autotuner over CTA size and CTAs per SM.
+// and a small autotuner over CTA size and cluster size.
 // Included by beta_gpu.cu (one translation unit).
 #pragma once
 
@@ -38,8 +38,8 @@ struct beta_gpu_batch {
   BState* h_states = nullptr;
   int* h_active = nullptr;
   BParams* h_params = nullptr;
-  // launch shape
-  int threads = 512, ctas_per_sm = 1;
+  // launch shape: threads per CTA and CTAs per cluster (one system per cluster)
+  int threads = 512, cluster = 1;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   long long n_launch = 0, n_h2d = 0, n_d2h = 0;
 };
@@ -164,16 +164,55 @@ const GaussTable* batch_gauss(beta_gpu_batch* b, int ndim, int order) {
 }
 
 template <int T>
-cudaError_t batch_launch_raw(beta_gpu_batch* b, int grid) {
-  k_batch_solve<T><<<grid, T, 0, b->stream>>>(b->d_sys, b->d_active, b->d_counter, b->d_params);
-  return cudaGetLastError();
+cudaLaunchConfig_t batch_cfg(beta_gpu_batch* b, int grid, cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(T, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = b->stream;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = b->cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
 }
 
-cudaError_t batch_launch(beta_gpu_batch* b, int grid) {
+// Clusters of the current shape that are resident at once (one full wave).
+template <int T>
+int batch_clusters_raw(beta_gpu_batch* b) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = batch_cfg<T>(b, b->cluster, attr);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_batch_solve<T>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int batch_clusters(beta_gpu_batch* b) {
   switch (b->threads) {
-    case 256: return batch_launch_raw<256>(b, grid);
-    case 1024: return batch_launch_raw<1024>(b, grid);
-    default: return batch_launch_raw<512>(b, grid);
+    case 256: return batch_clusters_raw<256>(b);
+    case 1024: return batch_clusters_raw<1024>(b);
+    default: return batch_clusters_raw<512>(b);
+  }
+}
+
+template <int T>
+cudaError_t batch_launch_raw(beta_gpu_batch* b, int nclusters) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = batch_cfg<T>(b, nclusters * b->cluster, attr);
+  return cudaLaunchKernelEx(&cfg, k_batch_solve<T>, (const BSys*)b->d_sys, (const int*)b->d_active, b->d_counter,
+                            (const BParams*)b->d_params);
+}
+
+cudaError_t batch_launch(beta_gpu_batch* b, int nclusters) {
+  switch (b->threads) {
+    case 256: return batch_launch_raw<256>(b, nclusters);
+    case 1024: return batch_launch_raw<1024>(b, nclusters);
+    default: return batch_launch_raw<512>(b, nclusters);
   }
 }
 
@@ -182,14 +221,15 @@ cudaError_t batch_launch(beta_gpu_batch* b, int grid) {
 // reads the work list and parameters from fixed device buffers, so the graph
 // stays valid while systems come and go.
 int batch_launch_graph(beta_gpu_batch* b) {
-  const int grid = b->nsm * b->ctas_per_sm;
-  auto key = std::make_pair(b->threads, b->ctas_per_sm);
+  const int ncl = batch_clusters(b);
+  if (ncl < 1) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "no cluster of this launch shape fits on the GPU");
+  auto key = std::make_pair(b->threads, b->cluster);
   auto it = b->graphs.find(key);
   if (it == b->graphs.end()) {
     cudaGraph_t g = nullptr;
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e1 = cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream);
-    cudaError_t e2 = batch_launch(b, grid);
+    cudaError_t e2 = batch_launch(b, ncl);
     cudaError_t e3 = cudaStreamEndCapture(b->stream, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
       cudaGetLastError();

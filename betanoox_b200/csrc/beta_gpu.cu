@@ -1534,26 +1534,29 @@ int beta_gpu_batch_remove(beta_gpu_batch* b, int id) {
   return BETA_GPU_OK;
 }
 
-int beta_gpu_batch_tune(beta_gpu_batch* b, int threads, int ctas_per_sm) {
-  if (!b || !(threads == 256 || threads == 512 || threads == 1024) || ctas_per_sm < 1 || ctas_per_sm > 4)
+int beta_gpu_batch_tune(beta_gpu_batch* b, int threads, int cluster) {
+  if (!b || !(threads == 256 || threads == 512 || threads == 1024) ||
+      !(cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8))
     return BETA_GPU_ERR_ARG;
-  int nb = 0;
-  const void* k = threads == 256 ? (const void*)k_batch_solve<256>
-                                 : threads == 1024 ? (const void*)k_batch_solve<1024> : (const void*)k_batch_solve<512>;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, 0) != cudaSuccess) { cudaGetLastError(); nb = 1; }
-  if (ctas_per_sm > nb) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "launch shape exceeds the SM's resident-block limit");
+  cudaSetDevice(b->device);
+  const int ot = b->threads, oc = b->cluster;
   b->threads = threads;
-  b->ctas_per_sm = ctas_per_sm;
+  b->cluster = cluster;
+  if (batch_clusters(b) < 1) {
+    b->threads = ot;
+    b->cluster = oc;
+    return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "no cluster of this launch shape fits on the GPU");
+  }
   return BETA_GPU_OK;
 }
 
 int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, int* threads_out,
-                            int* ctas_out) {
+                            int* cluster_out) {
   if (!b || !o || budget <= 0) return BETA_GPU_ERR_ARG;
   cudaSetDevice(b->device);
-  const int shapes[][2] = {{256, 1}, {256, 2}, {512, 1}, {512, 2}, {1024, 1}};
+  const int shapes[][2] = {{256, 1}, {512, 1}, {1024, 1}, {256, 2}, {512, 2}, {512, 4}, {512, 8}, {256, 8}};
   double best = 1e300;
-  int bt = b->threads, bc = b->ctas_per_sm, rc = BETA_GPU_OK;
+  int bt = b->threads, bc = b->cluster, rc = BETA_GPU_OK;
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
@@ -1569,21 +1572,22 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
     if ((rc = batch_pull_states(b))) break;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    long long its = 0;
+    // the measure is time per unit of work: iterations x matrix size
+    double work = 0.0;
     for (auto& S : b->sys)
-      if (S.live) its += S.st.iter;
-    const double per_it = its > 0 ? ms / its : 1e300;
-    if (per_it < best) { best = per_it; bt = sh[0]; bc = sh[1]; }
+      if (S.live) work += (double)S.st.iter * (double)S.work;
+    const double per = work > 0 ? ms / work : 1e300;
+    if (per < best) { best = per; bt = sh[0]; bc = sh[1]; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != BETA_GPU_OK) return rc;
   b->threads = bt;
-  b->ctas_per_sm = bc;
+  b->cluster = bc;
   if ((rc = batch_reset_states(b))) return rc;
   BCK(cudaStreamSynchronize(b->stream));
   if (threads_out) *threads_out = bt;
-  if (ctas_out) *ctas_out = bc;
+  if (cluster_out) *cluster_out = bc;
   return BETA_GPU_OK;
 }
 

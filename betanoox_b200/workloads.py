@@ -219,19 +219,22 @@ def rve_hex8(n, seed, order=2, E_matrix=1e3, contrast=10.0, nu=0.3, ux=0.01):
     xyz, conn = grid_hex8(n, n, n)
     ne = conn.shape[0]
     vf_target = 0.2 + 0.2 * uniform(seed, 11, 0)[()]
-    centres, radii = [], []
+    tries = np.arange(20000, dtype=np.uint64)
+    R = 0.05 + 0.10 * uniform(seed, 12, tries)
+    CC = np.stack([uniform(seed, 13, tries), uniform(seed, 14, tries), uniform(seed, 15, tries)], axis=1)
+    CC = R[:, None] + (1 - 2 * R[:, None]) * CC
+    acc_c = np.zeros((0, 3))
+    acc_r = np.zeros(0)
     vol = 0.0
-    for t in range(20000):
+    for t in range(len(R)):
         if vol >= vf_target:
             break
-        r = 0.05 + 0.10 * uniform(seed, 12, t)[()]
-        cc = np.array([uniform(seed, 13, t)[()], uniform(seed, 14, t)[()], uniform(seed, 15, t)[()]])
-        cc = r + (1 - 2 * r) * cc
-        if any(np.linalg.norm(cc - c2) < r + r2 for c2, r2 in zip(centres, radii)):
+        if acc_r.size and np.any(np.sqrt(((acc_c - CC[t]) ** 2).sum(axis=1)) < R[t] + acc_r):
             continue
-        centres.append(cc)
-        radii.append(r)
-        vol += 4.0 / 3.0 * math.pi * r ** 3
+        acc_c = np.vstack([acc_c, CC[t]])
+        acc_r = np.append(acc_r, R[t])
+        vol += 4.0 / 3.0 * math.pi * R[t] ** 3
+    centres, radii = list(acc_c), list(acc_r)
     cen = xyz[conn].mean(axis=1)
     inc = np.zeros(ne, bool)
     for cc, r in zip(centres, radii):

@@ -243,7 +243,9 @@ BETA_GPU_API int beta_gpu_csr_pcg_device(int n, const int* d_row_ptr, const int*
  * persistent launch (a replayed CUDA graph): each CTA takes whole systems,
  * largest first.  iters_per_launch > 0 bounds the PCG iterations each system
  * gets per launch, so a serving loop can admit and retire systems between
- * launches; the Krylov state stays in the pool.  Stop rule: ||b-Au||/||b||
+ * launches; the Krylov state stays in the pool.  A system is solved by one
+ * thread-block cluster of 1-8 CTAs (SMs) sharing DSMEM reductions and the
+ * cluster barrier.  Stop rule: ||b-Au||/||b||
  * (opts->tol); opts->inner_tol is the residual-replacement factor.  Batched
  * diffusion systems are steady (conductivity only). */
 typedef struct beta_gpu_batch beta_gpu_batch;
@@ -262,12 +264,14 @@ BETA_GPU_API int beta_gpu_batch_run(beta_gpu_batch* batch, const beta_gpu_solve_
 BETA_GPU_API int beta_gpu_batch_result(beta_gpu_batch* batch, int sys_id, double* u,
                                        beta_gpu_solve_stats* stats);
 BETA_GPU_API int beta_gpu_batch_remove(beta_gpu_batch* batch, int sys_id);
-/* Launch shape: threads per CTA (256, 512 or 1024) and CTAs per SM. */
-BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta, int ctas_per_sm);
+/* Launch shape: threads per CTA (256, 512 or 1024) and CTAs per cluster
+ * (1, 2, 4 or 8) working on one system. */
+BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta, int cluster_ctas);
 /* Times every launch shape on the current systems for `budget` iterations each
- * (systems are reset to unsolved afterwards) and keeps the fastest. */
+ * (systems are reset to unsolved afterwards) and keeps the one with the least
+ * time per unit of work. */
 BETA_GPU_API int beta_gpu_batch_autotune(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int budget,
-                                         int* threads_per_cta, int* ctas_per_sm);
+                                         int* threads_per_cta, int* cluster_ctas);
 /* out[0] live systems, out[1] pool bytes in use, out[2] pool bytes, out[3]
  * launches, out[4] bytes host->device, out[5] bytes device->host; n <= 6. */
 BETA_GPU_API int beta_gpu_batch_info(const beta_gpu_batch* batch, long long* out, int n);

@@ -89,7 +89,7 @@ def test_batch_autotune_keeps_results(oracle):
     b = Batch(hbm_budget=1 << 30)
     ids = [b.add(m) for m in models]
     t, c = b.autotune(opts(tol=1e-12), budget=10)
-    assert t in (256, 512, 1024) and c >= 1
+    assert t in (256, 512, 1024) and c in (1, 2, 4, 8)
     assert b.run(opts(tol=1e-12)) == 0
     for sid, m in zip(ids, models):
         rc, u, st = b.result(sid)
