@@ -11,6 +11,13 @@ Jacobi-PCG is measured on the same workload for the mixed/plain ratio.
 Multi-GPU (torchrun): every rank solves its own replica (the path does not
 shard: one system per GPU); value = total dofs solved / max-over-ranks time.
 
+--config batch: 512 two-phase RVE cubes (n ~ U{8..40}) solved together in one
+persistent launch (thread-block cluster per system, autotuned launch shape);
+one step = reset + assembly + mixed-precision solve of all 512.
+--config serve: a Poisson stream of requests (quad4 / hex8 elasticity / hex8
+diffusion, log-uniform 1e3-5e5 dofs) through the continuous-batching server at
+80% of its measured capacity; reports throughput and p50/p99 latency.
+
 --impl reference: the reference's CPU algorithm (the oracle restatement,
 all host cores) on a bounded sample of the same workload, extrapolated to
 the full solve (see cpu_baseline.sample in the output).
@@ -420,6 +427,418 @@ def run_reference(args):
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+
+# ---- batched RVEs (one persistent launch) ---------------------------------
+def iter_bytes(nblk, nnode, nd):
+    """Algorithmic bytes of one inner FP32 PCG iteration of the batched solver
+    for one system: SpMV (every stored block's nd*nd values + column index, the
+    direction gathered once, q written once), the update pass (y, r, q, p and
+    the packed block-Jacobi factor read; y, r written) and the direction pass
+    (r, p, factor read; p written).  p is padded to float4 for nd = 3."""
+    nd4 = 4 * nd
+    pv = 16 if nd == 3 else nd4
+    mv = 4 * nd * (nd + 1) // 2
+    return nblk * (4 * nd * nd + 4) + nnode * (7 * nd4 + 4 * pv + 2 * mv)
+
+
+def structured_nblk(m):
+    """Node-pair blocks of a structured n^3 hex8 cube: the node graph is the
+    tensor product of three 1-D graphs with 3n+1 entries each."""
+    n = int(m.meta["n"])
+    return (3 * n + 1) ** 3
+
+
+def cpu_full_solves(models, tol, budget_s, threads):
+    """The reference algorithm on the host (oracle restatement): structure,
+    FP64 assembly and threaded Jacobi-PCG (stop rule sqrt(r.r/x.x) < tol) of
+    whole systems, in list order, until budget_s seconds have been spent."""
+    from oracle import beta_oracle as bo
+    done, dofs, secs = 0, 0, 0.0
+    for m in models:
+        t0 = time.perf_counter()
+        s = bo.System(m)
+        s.set_bc(m.restrained, m.prescribed, m.load)
+        s.build_pattern()
+        s.assemble(m.params, m.order)
+        rc, x, st = s.solve_threaded(s.rhs(), tol, maxit=200000, threads=threads)
+        secs += time.perf_counter() - t0
+        done += 1
+        dofs += m.ndof
+        del s
+        if secs >= budget_s:
+            break
+    return done, dofs, secs
+
+
+def _init_dist(dev):
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(dev)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
+    return ws, rank
+
+
+def _max_over_ranks(v, dev):
+    ws, _, _ = _dist()
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], device=f"cuda:{dev}", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier():
+    import torch
+    ws, _, _ = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_batch(args):
+    import torch
+    from betanoox_b200 import Batch, Solver, _abi, opts
+    from betanoox_b200 import workloads as W
+    ws, rank, dev = _dist()
+    _init_dist(dev)
+    t0 = time.perf_counter()
+    models = W.rve_batch(count=args.count, seed=args.seed)
+    t_gen = time.perf_counter() - t0
+    ndof_tot = sum(m.ndof for m in models)
+    o = opts(mode=_abi.MODE_MPIR, tol=args.tol, inner_tol=args.inner_tol)
+    b = Batch(dev, hbm_budget=int(args.pool_gb * (1 << 30)), max_systems=len(models) + 8)
+    t0 = time.perf_counter()
+    ids = b.add_many(models)
+    t_add = time.perf_counter() - t0
+    assert all(i is not None for i in ids), "pool too small for the batch"
+    t0 = time.perf_counter()
+    threads, cluster = b.autotune(o, budget=args.tune_iters)
+    t_tune = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        b.reset()
+        b.run(o)
+    _barrier()
+    ms = []
+    l0 = b.info()["launches"]
+    with Clocks(dev) as clk:
+        for _ in range(args.steps):
+            b.reset()
+            left = b.run(o)
+            assert left == 0
+            ms.append(b.info()["last_launch_ns"] / 1e6)
+    launches = b.info()["launches"] - l0
+    _barrier()
+    res = [b.result(i, with_u=False) for i in ids]
+    bad = [(models[k].name, _abi.STATUS_NAMES.get(r[0])) for k, r in enumerate(res) if r[0] != _abi.OK]
+    iters = [r[2].iterations for r in res]
+    tot_ms = _max_over_ranks(sum(ms), dev)
+    value = ws * ndof_tot * args.steps / (tot_ms / 1e3)
+
+    out = None
+    if rank == 0:
+        # accuracy on a sample: batch solution vs a tight plain FP64 GPU solve
+        errs = []
+        fp64_ms, fp64_dofs, fp64_iters = 0.0, 0, []
+        stream = torch.cuda.Stream(device=dev)
+        for k, (sid, m) in enumerate(zip(ids, models)):
+            want_acc = k % args.check_every == 0
+            want_64 = k < args.fp64_sample
+            if not (want_acc or want_64):
+                continue
+            g = Solver(dev)
+            g.lib.beta_gpu_set_stream(g.h, C.c_void_p(stream.cuda_stream))
+            g.load_model(m)
+            g.build_pattern()
+            if want_64:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(stream):
+                    e0.record(stream)
+                    g.assemble(_abi.FP64)
+                    rc, st = g.solve(opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=args.tol))
+                    e1.record(stream)
+                stream.synchronize()
+                fp64_ms += e0.elapsed_time(e1)
+                fp64_dofs += m.ndof
+                fp64_iters.append(st.iterations)
+            if want_acc:
+                g.assemble(_abi.FP64)
+                g.solve(opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=1e-13))
+                ut = g.download()
+                _, u, _ = b.result(sid)
+                errs.append(float(np.linalg.norm(u - ut) / np.linalg.norm(ut)))
+            g.close()
+        # end to end: host models in, solutions out, through the batch API
+        e2e = None
+        if not args.skip_e2e:
+            tw = []
+            for _ in range(max(1, args.e2e_steps)):
+                t1 = time.perf_counter()
+                be = Batch(dev, hbm_budget=int(args.pool_gb * (1 << 30)), max_systems=len(models) + 8)
+                be.tune(threads, cluster)
+                eids = be.add_many(models)
+                be.run(o)
+                for sid in eids:
+                    be.result(sid)
+                tw.append(time.perf_counter() - t1)
+                inf = be.info()
+                be.close()
+            e2e = {"value": ws * ndof_tot / statistics.median(tw), "unit": UNIT,
+                   "h2d_bytes_per_step": inf["h2d"], "d2h_bytes_per_step": inf["d2h"],
+                   "ms_per_step": 1e3 * statistics.median(tw),
+                   "includes": "host structure build (all cores), pool upload, one launch, solution download"}
+        peak, peak_kind = _peaks()
+        ms_launch = statistics.median(ms)
+        alg = sum(it * iter_bytes(structured_nblk(m), m.nnode, 3) for it, m in zip(iters, models))
+        achieved = alg / (ms_launch * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": f"k_batch_solve<{threads}> (cluster {cluster}): assembly + all PCG",
+                "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_launch,
+                "note": "inner-iteration bytes only (assembly and FP64 residual replacements excluded); "
+                        "small systems re-read their matrix from L2",
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s"}
+        sizes = sorted(m.meta["n"] for m in models)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 inner / fp64 outer",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"{len(models)} two-phase RVE hex8 cubes n~U{{8..40}} "
+                                   f"(n {sizes[0]}..{sizes[-1]}), {ndof_tot} dofs total, one persistent launch",
+                       "global_batch": ws * len(models), "ndof_total": ndof_tot, "parallelism": f"replicas x{ws}",
+                       "tol": args.tol, "stop_rule": "||b-Au||/||b||", "launch_shape": [threads, cluster],
+                       "l2": f"inputs larger than L2 (pool {b.info()['used'] / 2**30:.1f} GiB)"},
+            "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+            "batch": {"ms_steps": ms, "iterations_total": int(sum(iters)), "iterations_max": int(max(iters)),
+                      "not_converged": bad[:5], "n_not_converged": len(bad), "setup_s": {"generate": t_gen,
+                      "add_many": t_add, "autotune": t_tune}},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clk.summary(),
+        }
+        if errs:
+            out["rel_err_vs_fp64_reference"] = {"max": max(errs), "n_checked": len(errs)}
+        if fp64_dofs:
+            v64 = fp64_dofs / (fp64_ms / 1e3)
+            out["fp64_plain"] = {"value": ws * v64, "systems": min(args.fp64_sample, len(models)),
+                                 "how": "sequential per-system plain FP64 Jacobi-PCG (FP64 assembly + solve, "
+                                        "CUDA events), same stop rule and tol",
+                                 "iterations_median": int(statistics.median(fp64_iters))}
+            out["mixed_over_fp64"] = value / (ws * v64)
+        if not args.skip_cpu:
+            th = os.cpu_count() or 1
+            n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s, th)
+            out["cpu_baseline"] = {"value": d / sec, "unit": UNIT, "cores": th, "kind": "port",
+                                   "sample": f"first {n} of {len(models)} RVEs solved whole on the host "
+                                             f"({d} dofs in {sec:.1f} s): FP64 assembly + threaded Jacobi-PCG"}
+    b.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return out
+
+
+def run_batch_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return None
+    from betanoox_b200 import workloads as W
+    models = W.rve_batch(count=args.count, seed=args.seed)
+    ndof_tot = sum(m.ndof for m in models)
+    th = os.cpu_count() or 1
+    vals, last = [], None
+    for k in range(max(1, args.warmup and 1) + args.steps):
+        n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
+        if k >= 1:
+            vals.append(d / sec)
+            last = (n, d, sec)
+    v = statistics.median(vals)
+    n, d, sec = last
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * ndof_tot / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": {"workload": f"{len(models)} two-phase RVE hex8 cubes n~U{{8..40}}, {ndof_tot} dofs total",
+                       "ndof_total": ndof_tot},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port",
+                             "sample": f"first {n} RVEs solved whole per step ({d} dofs, {sec:.1f} s): "
+                                       f"FP64 assembly + threaded Jacobi-PCG, one system at a time"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ---- serving: Poisson stream through the continuous-batching server ---------
+def _serve_stream(server, models, arrivals, threads):
+    """Submits models[j % len(models)] at arrivals[j] seconds (from a pool of
+    submitter threads, which build each request's structure), collects every
+    result, and returns per-request (latency s, dofs, state, status, final_norm)
+    and the wall time from the first arrival to the last completion."""
+    import queue
+    from betanoox_b200 import _abi
+    n = len(arrivals)
+    q = queue.Queue()
+    subs = [None] * n  # (rid, t_submit_start, t_submit_end)
+    t_base = time.perf_counter() + 0.05
+
+    def submitter():
+        while True:
+            j = q.get()
+            if j is None:
+                return
+            m = models[j % len(models)]
+            ts = time.perf_counter()
+            rid = server.submit(m)
+            subs[j] = (rid, ts)
+
+    pool = [threading.Thread(target=submitter, daemon=True) for _ in range(threads)]
+    for t in pool:
+        t.start()
+    for j in range(n):
+        now = time.perf_counter() - t_base
+        if arrivals[j] > now:
+            time.sleep(arrivals[j] - now)
+        q.put(j)
+    for _ in pool:
+        q.put(None)
+    for t in pool:
+        t.join()
+    out = []
+    t_end = 0.0
+    for j in range(n):
+        rid, ts = subs[j]
+        state, _, st, lat_ms = server.wait(rid, timeout_s=600.0)
+        done_at = (ts - t_base) + lat_ms / 1e3
+        t_end = max(t_end, done_at)
+        out.append(((done_at - arrivals[j]), models[j % len(models)].ndof, state, st.status, st.final_norm))
+    return out, t_end - arrivals[0]
+
+
+def run_serve(args):
+    import torch
+    from betanoox_b200 import Server, _abi, opts
+    from betanoox_b200 import workloads as W
+    ws, rank, dev = _dist()
+    _init_dist(dev)
+    t0 = time.perf_counter()
+    pool_n = min(args.requests, args.serve_pool)
+    models = [W.serve_request(args.seed + 1000 * rank, j) for j in range(pool_n)]
+    t_gen = time.perf_counter() - t0
+    o = opts(mode=_abi.MODE_MPIR, tol=args.tol, inner_tol=args.inner_tol)
+    th = args.submit_threads or (os.cpu_count() or 1)
+    srv = Server(dev, hbm_budget=int(args.pool_gb * (1 << 30)), max_systems=4096, o=o,
+                 iters_per_launch=args.iters_per_launch, threads=args.threads, cluster=args.cluster)
+    # capacity: a burst of the first `cap` pool models submitted at once
+    cap_n = min(args.capacity_requests, pool_n)
+    for _ in range(args.warmup):
+        _serve_stream(srv, models[:min(cap_n, 32)], np.zeros(min(cap_n, 32)), th)
+    res_cap, wall_cap = _serve_stream(srv, models[:cap_n], np.zeros(cap_n), th)
+    cap_rps = cap_n / wall_cap
+    lam = args.load * cap_rps
+    rng = np.random.default_rng(args.seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, size=args.requests))
+    arrivals -= arrivals[0]
+    s0 = srv.stats()
+    _barrier()
+    with Clocks(dev) as clk:
+        res, wall = _serve_stream(srv, models, arrivals, th)
+    s1 = srv.stats()
+    wall = _max_over_ranks(wall, dev)
+    lat = np.array([r[0] for r in res]) * 1e3
+    dofs = sum(r[1] for r in res)
+    states = [r[2] for r in res]
+    value = ws * dofs / wall
+    out = None
+    if rank == 0:
+        ok = sum(1 for r in res if r[2] == _abi.REQ_DONE and r[3] == _abi.OK)
+        # plain FP64 GPU PCG, one request at a time end to end (same API level)
+        fp64 = None
+        if args.serve_fp64_sample:
+            from betanoox_b200 import Solver
+            tw, d64 = 0.0, 0
+            for m in models[:args.serve_fp64_sample]:
+                t1 = time.perf_counter()
+                g = Solver(dev)
+                g.load_model(m)
+                g.build_pattern()
+                g.assemble(_abi.FP64)
+                g.solve(opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=args.tol))
+                g.download()
+                g.close()
+                tw += time.perf_counter() - t1
+                d64 += m.ndof
+            fp64 = {"value": ws * d64 / tw, "requests": min(args.serve_fp64_sample, len(models)),
+                    "how": "sequential requests through the single-system API, plain FP64 Jacobi-PCG, "
+                           "host structure build + upload + assembly + solve + download"}
+        fams = {}
+        for j in range(len(res)):
+            f = models[j % len(models)].meta["family"]
+            fams[f] = fams.get(f, 0) + 1
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": 1, "warmup": args.warmup,
+            "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 inner / fp64 outer", "data": "synthetic (seeded generator)",
+            "config": {"workload": f"Poisson stream of {args.requests} requests (quad4 / hex8 elasticity / hex8 "
+                                   f"diffusion, log-uniform 1e3-5e5 dofs) at {args.load:.0%} of measured capacity",
+                       "requests": args.requests, "distinct_models": pool_n, "families": fams,
+                       "lambda_per_s": lam, "capacity_req_per_s": cap_rps, "tol": args.tol,
+                       "iters_per_launch": args.iters_per_launch, "submit_threads": th,
+                       "launch_shape": [args.threads, args.cluster], "parallelism": f"replicas x{ws}",
+                       "l2": "working set above L2 (pool of resident systems)"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "mean": float(lat.mean()), "max": float(lat.max())},
+            "serve": {"done_ok": ok, "states": {str(k): states.count(k) for k in set(states)},
+                      "max_final_norm": float(max(r[4] for r in res)), "launches": s1["launches"] - s0["launches"],
+                      "busy_frac": (s1["busy_us"] - s0["busy_us"]) / 1e6 / wall, "wall_s": wall,
+                      "generate_s": t_gen, "capacity_burst": {"requests": cap_n, "wall_s": wall_cap}},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": s1["h2d"] - s0["h2d"],
+                    "d2h_bytes_per_step": s1["d2h"] - s0["d2h"],
+                    "includes": "arrival to result on host: structure build, admission, solve, download"},
+            "gpu_launches": s1["launches"] - s0["launches"], "clocks": clk.summary(),
+        }
+        if fp64:
+            out["fp64_plain"] = fp64
+            out["mixed_over_fp64"] = value / fp64["value"]
+        if not args.skip_cpu:
+            thc = os.cpu_count() or 1
+            n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s, thc)
+            out["cpu_baseline"] = {"value": d / sec, "unit": UNIT, "cores": thc, "kind": "port",
+                                   "sample": f"first {n} requests solved whole on the host, one at a time "
+                                             f"({d} dofs in {sec:.1f} s): FP64 assembly + threaded Jacobi-PCG"}
+    srv.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return out
+
+
+def run_serve_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return None
+    from betanoox_b200 import workloads as W
+    pool_n = min(args.requests, args.serve_pool)
+    models = [W.serve_request(args.seed, j) for j in range(pool_n)]
+    th = os.cpu_count() or 1
+    vals, last = [], None
+    for k in range(1 + args.steps):
+        n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
+        if k >= 1:
+            vals.append(d / sec)
+            last = (n, d, sec)
+    v = statistics.median(vals)
+    n, d, sec = last
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * d / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": {"workload": f"stream of {args.requests} requests (quad4 / hex8 elasticity / hex8 diffusion, "
+                                   f"log-uniform 1e3-5e5 dofs), solved one at a time"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port",
+                             "sample": f"first {n} requests solved whole per step ({d} dofs, {sec:.1f} s)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -439,10 +858,33 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=30)
     ap.add_argument("--cpu-iters", type=int, default=30)
     ap.add_argument("--cpu-assumed-iters", type=int, default=2000)
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0)
+    # batch / serve
+    ap.add_argument("--count", type=int, default=512)
+    ap.add_argument("--seed", type=int, default=99)
+    ap.add_argument("--pool-gb", type=float, default=48.0)
+    ap.add_argument("--tune-iters", type=int, default=30)
+    ap.add_argument("--check-every", type=int, default=32)
+    ap.add_argument("--fp64-sample", type=int, default=512)
+    ap.add_argument("--requests", type=int, default=10000)
+    ap.add_argument("--serve-pool", type=int, default=1000)
+    ap.add_argument("--capacity-requests", type=int, default=400)
+    ap.add_argument("--load", type=float, default=0.8)
+    ap.add_argument("--iters-per-launch", type=int, default=200)
+    ap.add_argument("--threads", type=int, default=512)
+    ap.add_argument("--cluster", type=int, default=4)
+    ap.add_argument("--submit-threads", type=int, default=0)
+    ap.add_argument("--serve-fp64-sample", type=int, default=100)
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
-    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    ref = args.impl == "reference"
+    if args.config == "batch":
+        out = run_batch_reference(args) if ref else run_batch(args)
+    elif args.config == "serve":
+        out = run_serve_reference(args) if ref else run_serve(args)
+    else:
+        out = run_reference(args) if ref else run_ours(args)
     if out is not None:
         print(json.dumps(out))
 

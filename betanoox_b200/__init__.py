@@ -15,7 +15,7 @@ import numpy as np
 from . import _abi
 from ._abi import BetaGpuError, SolveOpts, SolveStats
 
-__all__ = ["Solver", "Batch", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
+__all__ = ["Solver", "Batch", "Server", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
 
 
 def build(force: bool = False) -> str:
@@ -200,6 +200,40 @@ class Batch:
         self.models[sid.value] = m
         return sid.value
 
+    def add_many(self, models, host_threads=0):
+        """Adds models with their structures built on host_threads host
+        threads (0 = all cores); returns the ids (None where REJECTED)."""
+        keep = []
+        arr = (_abi.System * len(models))()
+        for k, m in enumerate(models):
+            a = dict(xyz=np.ascontiguousarray(m.xyz, dtype=np.float64),
+                     conn=np.ascontiguousarray(m.conn, dtype=np.int32),
+                     first_dof=np.ascontiguousarray(m.first_dof, dtype=np.int32),
+                     group_params=np.ascontiguousarray(m.params, dtype=np.float64),
+                     restrained=np.ascontiguousarray(m.restrained, dtype=np.uint8),
+                     prescribed=np.ascontiguousarray(m.prescribed, dtype=np.float64),
+                     load=np.ascontiguousarray(m.load, dtype=np.float64))
+            keep.append(a)
+            s = arr[k]
+            s.kind, s.ndim, s.nnode, s.nelem, s.nnpe = m.kind, m.ndim, m.nnode, m.nelem, m.nnpe
+            s.ndof_per_node, s.integration_order = m.ndpn, m.order
+            s.ngroups, s.nparams = a["group_params"].shape
+            for f, v in a.items():
+                setattr(s, f, v.ctypes.data)
+        ids = (C.c_int * max(1, len(models)))()
+        st = self.lib.beta_gpu_batch_add_many(self.h, len(models), arr, int(host_threads), ids)
+        out = []
+        for k, m in enumerate(models):
+            if ids[k] >= 0:
+                self.models[ids[k]] = m
+                out.append(ids[k])
+            elif -ids[k] == _abi.REJECTED:
+                out.append(None)
+            else:
+                raise self._err(-ids[k], f"batch_add_many (system {k})")
+        del keep
+        return out
+
     def run(self, o=None, iters_per_launch=0):
         """One persistent launch; returns the number of unfinished systems."""
         o = o or opts()
@@ -234,7 +268,108 @@ class Batch:
             raise self._err(st, "batch_autotune")
         return t.value, c.value
 
+    def reset(self):
+        """Marks every system unsolved (the next run re-assembles and re-solves)."""
+        st = self.lib.beta_gpu_batch_reset(self.h)
+        if st != _abi.OK:
+            raise self._err(st, "batch_reset")
+
     def info(self):
-        a = (C.c_longlong * 6)()
-        self.lib.beta_gpu_batch_info(self.h, a, 6)
-        return dict(zip(["live", "used", "pool", "launches", "h2d", "d2h"], list(a)))
+        a = (C.c_longlong * 7)()
+        self.lib.beta_gpu_batch_info(self.h, a, 7)
+        return dict(zip(["live", "used", "pool", "launches", "h2d", "d2h", "last_launch_ns"], list(a)))
+
+
+class Server:
+    """Continuous-batching solve server (beta_gpu_server): submit systems at any
+    time; a native worker thread admits them into an HBM pool, solves them in
+    bounded persistent launches alongside whatever else is in flight, and
+    retires each as soon as it converges."""
+
+    STATS = ["submitted", "done", "rejected", "failed", "cancelled", "queued", "running", "launches",
+             "pool_used", "pool_bytes", "busy_us", "h2d", "d2h"]
+
+    def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, max_systems: int = 4096, o=None,
+                 iters_per_launch: int = 200, threads: int = 0, cluster: int = 0):
+        self.lib = _abi.load()
+        self.o = o or opts()
+        h = C.c_void_p()
+        st = self.lib.beta_gpu_server_create(C.byref(h), device, int(hbm_budget), int(max_systems),
+                                             C.byref(self.o), int(iters_per_launch), int(threads), int(cluster))
+        if st != _abi.OK:
+            raise BetaGpuError(st, "beta_gpu_server_create failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.beta_gpu_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, m):
+        """Queues model m; returns the request id (input errors raise at once)."""
+        xyz = np.ascontiguousarray(m.xyz, dtype=np.float64)
+        conn = np.ascontiguousarray(m.conn, dtype=np.int32)
+        fd = np.ascontiguousarray(m.first_dof, dtype=np.int32)
+        p = np.ascontiguousarray(m.params, dtype=np.float64)
+        r = np.ascontiguousarray(m.restrained, dtype=np.uint8)
+        pr = np.ascontiguousarray(m.prescribed, dtype=np.float64)
+        ld = np.ascontiguousarray(m.load, dtype=np.float64)
+        rid = C.c_longlong(0)
+        st = self.lib.beta_gpu_server_submit(self.h, m.kind, m.ndim, m.nnode, _ptr(xyz), m.nelem, m.nnpe, _ptr(conn),
+                                             _ptr(fd), m.ndpn, m.order, p.shape[0], p.shape[1], _ptr(p), None,
+                                             _ptr(r), _ptr(pr), _ptr(ld), C.byref(rid))
+        if st != _abi.OK:
+            msg = self.lib.beta_gpu_server_last_error(self.h)
+            raise BetaGpuError(st, f"server_submit: {msg.decode() if msg else ''}")
+        return rid.value
+
+    def poll(self, rid, wait_ms=0, release=False):
+        """Returns (state, u or None, stats, latency_ms)."""
+        state, nd = C.c_int(0), C.c_int(0)
+        st = SolveStats()
+        lat = C.c_double(-1.0)
+        rc = self.lib.beta_gpu_server_poll(self.h, rid, 0, C.byref(state), C.byref(nd), None, None, None, 0)
+        if rc != _abi.OK:
+            raise BetaGpuError(rc, f"server_poll: unknown request {rid}")
+        u = np.zeros(nd.value)
+        rc = self.lib.beta_gpu_server_poll(self.h, rid, int(wait_ms), C.byref(state), None, _ptr(u), C.byref(st),
+                                           C.byref(lat), int(bool(release)))
+        if rc != _abi.OK:
+            raise BetaGpuError(rc, f"server_poll: unknown request {rid}")
+        return state.value, (u if state.value == _abi.REQ_DONE else None), st, lat.value
+
+    def wait(self, rid, timeout_s=120.0, release=True):
+        """Blocks until the request is final; returns (state, u, stats, latency_ms)."""
+        import time
+        end = time.monotonic() + timeout_s
+        while True:
+            left = max(1, int((end - time.monotonic()) * 1000))
+            state, u, st, lat = self.poll(rid, wait_ms=min(left, 1000), release=False)
+            if state >= _abi.REQ_DONE:
+                if release:
+                    self.poll(rid, release=True)
+                return state, u, st, lat
+            if time.monotonic() > end:
+                raise TimeoutError(f"request {rid} not finished after {timeout_s} s")
+
+    def cancel(self, rid):
+        rc = self.lib.beta_gpu_server_cancel(self.h, rid)
+        if rc != _abi.OK:
+            raise BetaGpuError(rc, f"server_cancel: unknown request {rid}")
+
+    def stats(self):
+        a = (C.c_longlong * len(self.STATS))()
+        self.lib.beta_gpu_server_stats(self.h, a, len(self.STATS))
+        return dict(zip(self.STATS, list(a)))

@@ -29,6 +29,14 @@ ERR_UNSUPPORTED = 13
 ERR_TOO_LARGE = 14
 NOALLOC_MAX_ROWS = 262144
 
+# server request states
+REQ_QUEUED = 0
+REQ_RUNNING = 1
+REQ_DONE = 2
+REQ_REJECTED = 3
+REQ_CANCELLED = 4
+REQ_FAILED = 5
+
 QUAD4_PSTRESS = 1
 HEX8_ELASTIC = 2
 HEX8_HEAT = 3
@@ -72,6 +80,16 @@ class SolveStats(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
 
 
+class System(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("ndim", C.c_int), ("nnode", C.c_int), ("nelem", C.c_int), ("nnpe", C.c_int),
+        ("ndof_per_node", C.c_int), ("integration_order", C.c_int), ("ngroups", C.c_int), ("nparams", C.c_int),
+        ("reserved", C.c_int),
+        ("xyz", C.c_void_p), ("conn", C.c_void_p), ("first_dof", C.c_void_p), ("group_params", C.c_void_p),
+        ("elem_group", C.c_void_p), ("restrained", C.c_void_p), ("prescribed", C.c_void_p), ("load", C.c_void_p),
+    ]
+
+
 # Every exported symbol with its signature (kept in step with include/beta_gpu.h).
 _P = C.c_void_p
 _I = C.c_int
@@ -103,12 +121,23 @@ SIGNATURES = {
     "beta_gpu_batch_destroy": (_I, [_P]),
     "beta_gpu_batch_last_error": (C.c_char_p, [_P]),
     "beta_gpu_batch_add": (_I, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, C.POINTER(_I)]),
+    "beta_gpu_batch_add_many": (_I, [_P, _I, C.POINTER(System), _I, C.POINTER(_I)]),
     "beta_gpu_batch_run": (_I, [_P, C.POINTER(SolveOpts), _I, C.POINTER(_I)]),
     "beta_gpu_batch_result": (_I, [_P, _I, _P, C.POINTER(SolveStats)]),
     "beta_gpu_batch_remove": (_I, [_P, _I]),
     "beta_gpu_batch_tune": (_I, [_P, _I, _I]),
     "beta_gpu_batch_autotune": (_I, [_P, C.POINTER(SolveOpts), _I, C.POINTER(_I), C.POINTER(_I)]),
+    "beta_gpu_batch_reset": (_I, [_P]),
     "beta_gpu_batch_info": (_I, [_P, C.POINTER(C.c_longlong), _I]),
+    "beta_gpu_server_create": (_I, [C.POINTER(_P), _I, C.c_longlong, _I, C.POINTER(SolveOpts), _I, _I, _I]),
+    "beta_gpu_server_destroy": (_I, [_P]),
+    "beta_gpu_server_last_error": (C.c_char_p, [_P]),
+    "beta_gpu_server_submit": (_I, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P,
+                                    C.POINTER(C.c_longlong)]),
+    "beta_gpu_server_poll": (_I, [_P, C.c_longlong, _I, C.POINTER(_I), C.POINTER(_I), _P, C.POINTER(SolveStats),
+                                  C.POINTER(_D), _I]),
+    "beta_gpu_server_cancel": (_I, [_P, C.c_longlong]),
+    "beta_gpu_server_stats": (_I, [_P, C.POINTER(C.c_longlong), _I]),
     "beta_gpu_csr_pcg_device_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _D, _I, _P, C.POINTER(SolveStats)]),
 }
 

@@ -42,6 +42,8 @@ struct beta_gpu_batch {
   int threads = 512, cluster = 1;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   long long n_launch = 0, n_h2d = 0, n_d2h = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket the last launch on `stream`
+  float last_ms = 0.f;
 };
 
 namespace {

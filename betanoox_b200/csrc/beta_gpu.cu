@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstddef>
@@ -14,6 +15,7 @@
 #include <tuple>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -627,6 +629,168 @@ int fp64_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve_stat
 }  // namespace
 
 #include "batch_host.cuh"
+
+namespace {
+
+// A system checked and structured on the host, ready to be copied into a pool
+// (CPU work only; safe to run on any thread).
+struct PreparedSys {
+  int kind = 0, ndim = 0, nnode = 0, nelem = 0, nnpe = 0, ndpn = 0, order = 0, ngroups = 0, nparams = 0;
+  std::vector<double> xyz, gp, presc, load;
+  std::vector<int> conn, eg;
+  std::vector<unsigned char> rest;
+  HostPattern P;
+  SysLayout L;
+  size_t ndof() const { return (size_t)nnode * ndpn; }
+};
+
+int prepare_system(int kind, int ndim, int nnode, const double* xyz, int nelem, int nnpe, const int* conn,
+                   const int* first_dof, int ndpn, int order, int ngroups, int nparams, const double* gp,
+                   const int* eg, const unsigned char* restrained, const double* prescribed, const double* load,
+                   PreparedSys& S, std::string& err) {
+  int want_nnpe = 0, want_ndim = 0, want_ndpn = 0, want_np = 0;
+  switch (kind) {
+    case BETA_GPU_QUAD4_PSTRESS: want_nnpe = 4; want_ndim = 2; want_ndpn = 2; want_np = 4; break;
+    case BETA_GPU_HEX8_ELASTIC: want_nnpe = 8; want_ndim = 3; want_ndpn = 3; want_np = 9; break;
+    case BETA_GPU_HEX8_HEAT: want_nnpe = 8; want_ndim = 3; want_ndpn = 1; want_np = 4; break;
+    default: err = "unknown element kind"; return BETA_GPU_ERR_UNSUPPORTED;
+  }
+  if (nnpe != want_nnpe || ndim != want_ndim || ndpn != want_ndpn || nparams != want_np) {
+    err = "sizes do not match the element kind";
+    return BETA_GPU_ERR_ARG;
+  }
+  if (nnode <= 0 || nelem <= 0 || !xyz || !conn || !first_dof || !gp || ngroups <= 0 || order < 1 || order > 4) {
+    err = "bad mesh or material arguments";
+    return BETA_GPU_ERR_ARG;
+  }
+  if (!eg && ngroups != nelem) { err = "without elem_group there must be one group per element"; return BETA_GPU_ERR_ARG; }
+  const size_t ndof = (size_t)nnode * ndpn;
+  if (!all_finite(xyz, (size_t)nnode * ndim) || !all_finite(gp, (size_t)ngroups * nparams) ||
+      (prescribed && !all_finite(prescribed, ndof)) || (load && !all_finite(load, ndof))) {
+    err = "non-finite input";
+    return BETA_GPU_ERR_NOT_FINITE;
+  }
+  for (long long k = 0; k < (long long)nelem * nnpe; ++k)
+    if (conn[k] < 0 || conn[k] >= nnode) { err = "connectivity out of range"; return BETA_GPU_ERR_ARG; }
+  if (eg)
+    for (int e = 0; e < nelem; ++e)
+      if (eg[e] < 0 || eg[e] >= ngroups) { err = "elem_group out of range"; return BETA_GPU_ERR_ARG; }
+  S.kind = kind; S.ndim = ndim; S.nnode = nnode; S.nelem = nelem; S.nnpe = nnpe; S.ndpn = ndpn; S.order = order;
+  S.ngroups = ngroups; S.nparams = nparams;
+  S.rest.assign(ndof, 0);
+  if (restrained)
+    for (size_t i = 0; i < ndof; ++i) S.rest[i] = restrained[i] ? 1 : 0;
+  if (load)
+    for (size_t i = 0; i < ndof; ++i)
+      if (S.rest[i] && load[i] != 0.0) {
+        err = "Cannot add load to a restrained degree of freedom.";
+        return BETA_GPU_ERR_LOAD_ON_RESTRAINED;
+      }
+  std::string msg = build_pattern(nnode, nelem, nnpe, ndpn, conn, first_dof, S.rest.data(), S.P, false);
+  if (!msg.empty()) { err = msg; return BETA_GPU_ERR_UNSUPPORTED; }
+  S.xyz.assign(xyz, xyz + (size_t)nnode * ndim);
+  S.conn.assign(conn, conn + (size_t)nelem * nnpe);
+  S.gp.assign(gp, gp + (size_t)ngroups * nparams);
+  if (eg) S.eg.assign(eg, eg + nelem);
+  S.presc.assign(ndof, 0.0);
+  S.load.assign(ndof, 0.0);
+  if (prescribed) std::copy(prescribed, prescribed + ndof, S.presc.begin());
+  if (load) std::copy(load, load + ndof, S.load.begin());
+  S.L = layout_for(ndim, nnode, nelem, nnpe, ndpn, ngroups, nparams, eg != nullptr, S.P);
+  return BETA_GPU_OK;
+}
+
+// Copies a prepared system into the pool: BETA_GPU_REJECTED when it does not fit.
+int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
+  cudaSetDevice(b->device);
+  const HostPattern& P = Q.P;
+  const SysLayout& L = Q.L;
+  const size_t ndof = Q.ndof();
+  int id;
+  if (!b->free_ids.empty()) id = b->free_ids.back();
+  else if ((int)b->sys.size() < b->cap) id = (int)b->sys.size();
+  else return bfail(b, BETA_GPU_REJECTED, "batch holds max_systems systems");
+  const long long off = pool_alloc(b, L.total);
+  if (off < 0) return bfail(b, BETA_GPU_REJECTED, "HBM budget exhausted: the system does not fit in the pool");
+  if (!b->free_ids.empty()) b->free_ids.pop_back();
+  else b->sys.emplace_back();
+  unsigned char* base = b->pool + off;
+  const GaussTable* gt = batch_gauss(b, Q.ndim, Q.order);
+  int rc = gt ? BETA_GPU_OK : BETA_GPU_ERR_CUDA;
+  auto up = [&](size_t o, const void* src, size_t bytes) { if (!rc) rc = batch_h2d(b, base + o, src, bytes); };
+  up(L.o_xyz, Q.xyz.data(), sizeof(double) * Q.xyz.size());
+  up(L.o_conn, Q.conn.data(), sizeof(int) * Q.conn.size());
+  up(L.o_gp, Q.gp.data(), sizeof(double) * Q.gp.size());
+  if (!Q.eg.empty()) up(L.o_eg, Q.eg.data(), sizeof(int) * Q.eg.size());
+  up(L.o_rest, Q.rest.data(), ndof);
+  up(L.o_presc, Q.presc.data(), sizeof(double) * ndof);
+  up(L.o_load, Q.load.data(), sizeof(double) * ndof);
+  up(L.o_cptr, P.color_ptr.data(), sizeof(int) * P.color_ptr.size());
+  up(L.o_elems, P.elem_by_color.data(), sizeof(int) * P.elem_by_color.size());
+  up(L.o_slot, P.slot.data(), sizeof(int) * P.slot.size());
+  up(L.o_nrp, P.nrp.data(), sizeof(int) * P.nrp.size());
+  up(L.o_ndiag, P.ndiag.data(), sizeof(int) * P.ndiag.size());
+  up(L.o_bsoff, P.bsoff.data(), sizeof(int) * P.bsoff.size());
+  up(L.o_bcol, P.bcol.data(), sizeof(int) * P.bcol.size());
+  if (rc == BETA_GPU_OK && cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); rc = BETA_GPU_ERR_CUDA; }
+  beta_gpu_batch::Sys& S = b->sys[id];
+  if (rc != BETA_GPU_OK) {
+    pool_free(b, off, L.total);
+    S.live = false;
+    b->free_ids.push_back(id);
+    return bfail(b, rc, "upload of the system failed");
+  }
+  S.live = true;
+  S.kind = Q.kind; S.ndim = Q.ndim; S.nnode = Q.nnode; S.nelem = Q.nelem; S.nnpe = Q.nnpe; S.ndpn = Q.ndpn;
+  S.ndof = (int)ndof; S.order = Q.order; S.off = (size_t)off; S.bytes = L.total;
+  S.work = (long long)P.nchunk * 32 * Q.ndpn * Q.ndpn;
+  BSys& D = S.desc;
+  std::memset(&D, 0, sizeof(D));
+  GaussTable hg;
+  make_gauss_table(Q.ndim, Q.order, hg);
+  D.kind = Q.kind; D.ndpn = Q.ndpn; D.nnode = Q.nnode; D.nelem = Q.nelem; D.ndof = (int)ndof; D.nip = hg.nip;
+  D.ncolor = P.ncolor; D.nslice = P.nslice; D.nparams = Q.nparams; D.ndim = Q.ndim;
+  D.xyz = (const double*)(base + L.o_xyz);
+  D.conn = (const int*)(base + L.o_conn);
+  D.gparams = (const double*)(base + L.o_gp);
+  D.egroup = Q.eg.empty() ? nullptr : (const int*)(base + L.o_eg);
+  D.rest = base + L.o_rest;
+  D.presc = (const double*)(base + L.o_presc);
+  D.load = (const double*)(base + L.o_load);
+  D.color_ptr = (const int*)(base + L.o_cptr);
+  D.elems = (const int*)(base + L.o_elems);
+  D.slot = (const int*)(base + L.o_slot);
+  D.nrp = (const int*)(base + L.o_nrp);
+  D.ndiag = (const int*)(base + L.o_ndiag);
+  D.bsoff = (const int*)(base + L.o_bsoff);
+  D.bcol = (const int*)(base + L.o_bcol);
+  D.bval = (float*)(base + L.o_bval);
+  D.x64 = (double*)(base + L.o_x64);
+  D.r64 = (double*)(base + L.o_r64);
+  D.y64 = (double*)(base + L.o_y64);
+  D.y32 = (float*)(base + L.o_y32);
+  D.r32 = (float*)(base + L.o_r32);
+  D.p32 = (float*)(base + L.o_p32);
+  D.q32 = (float*)(base + L.o_q32);
+  D.minv = (float*)(base + L.o_minv);
+  D.gt = gt;
+  D.st = b->d_states + id;
+  D.nchunk = P.nchunk;
+  BState s0;
+  std::memset(&s0, 0, sizeof(s0));
+  s0.phase = kPhaseNew;
+  s0.status = kBRunning;
+  S.st = s0;
+  b->h_states[id] = s0;
+  if ((rc = batch_h2d(b, b->d_states + id, b->h_states + id, sizeof(BState)))) return rc;
+  BCK(cudaStreamSynchronize(b->stream));
+  *sys_id = id;
+  return BETA_GPU_OK;
+}
+
+}  // namespace
+
+#include "server_host.cuh"
 
 // ---- scratch of beta_gpu_csr_pcg_device_noalloc ----------------------------
 // One fixed array per GPU that loads the library (held until process exit).
@@ -1319,6 +1483,8 @@ int beta_gpu_batch_create(beta_gpu_batch** out, int device, long long budget, in
   if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return BETA_GPU_ERR_CUDA; }
   BCK(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device));
   BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  BCK(cudaEventCreate(&b->ev0));
+  BCK(cudaEventCreate(&b->ev1));
   BCK(cudaMalloc(&b->pool, (size_t)budget));
   b->pool_bytes = (size_t)budget;
   b->free_list[0] = b->pool_bytes & ~size_t(255);
@@ -1352,6 +1518,8 @@ int beta_gpu_batch_destroy(beta_gpu_batch* b) {
   cudaFreeHost(b->h_states);
   cudaFreeHost(b->h_active);
   cudaFreeHost(b->h_params);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return BETA_GPU_OK;
@@ -1364,120 +1532,51 @@ int beta_gpu_batch_add(beta_gpu_batch* b, int kind, int ndim, int nnode, const d
                        const double* gp, const int* eg, const unsigned char* restrained, const double* prescribed,
                        const double* load, int* sys_id) {
   if (!b || !sys_id) return BETA_GPU_ERR_ARG;
-  cudaSetDevice(b->device);
-  int want_nnpe = 0, want_ndim = 0, want_ndpn = 0, want_np = 0;
-  switch (kind) {
-    case BETA_GPU_QUAD4_PSTRESS: want_nnpe = 4; want_ndim = 2; want_ndpn = 2; want_np = 4; break;
-    case BETA_GPU_HEX8_ELASTIC: want_nnpe = 8; want_ndim = 3; want_ndpn = 3; want_np = 9; break;
-    case BETA_GPU_HEX8_HEAT: want_nnpe = 8; want_ndim = 3; want_ndpn = 1; want_np = 4; break;
-    default: return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "unknown element kind");
+  PreparedSys P;
+  std::string err;
+  int rc = prepare_system(kind, ndim, nnode, xyz, nelem, nnpe, conn, first_dof, ndpn, order, ngroups, nparams, gp,
+                          eg, restrained, prescribed, load, P, err);
+  if (rc != BETA_GPU_OK) return bfail(b, rc, err);
+  return admit_system(b, P, sys_id);
+}
+
+int beta_gpu_batch_add_many(beta_gpu_batch* b, int count, const beta_gpu_system* sy, int host_threads,
+                            int* ids) {
+  if (!b || count < 0 || (count > 0 && (!sy || !ids))) return BETA_GPU_ERR_ARG;
+  std::vector<PreparedSys> P(count);
+  std::vector<int> rc(count, BETA_GPU_OK);
+  std::vector<std::string> err(count);
+  unsigned hw = std::thread::hardware_concurrency();
+  int nt = host_threads > 0 ? host_threads : (int)(hw ? hw : 1);
+  nt = std::max(1, std::min(nt, count));
+  std::atomic<int> next(0);
+  auto work = [&]() {
+    pattern_serial_on_this_thread(nt > 1);
+    for (int i; (i = next.fetch_add(1)) < count;) {
+      const beta_gpu_system& q = sy[i];
+      rc[i] = prepare_system(q.kind, q.ndim, q.nnode, q.xyz, q.nelem, q.nnpe, q.conn, q.first_dof, q.ndof_per_node,
+                             q.integration_order, q.ngroups, q.nparams, q.group_params, q.elem_group, q.restrained,
+                             q.prescribed, q.load, P[i], err[i]);
+    }
+    pattern_serial_on_this_thread(false);
+  };
+  if (nt == 1) {
+    work();
+  } else {
+    std::vector<std::thread> th;
+    for (int k = 0; k < nt; ++k) th.emplace_back(work);
+    for (auto& t : th) t.join();
   }
-  if (nnpe != want_nnpe || ndim != want_ndim || ndpn != want_ndpn || nparams != want_np)
-    return bfail(b, BETA_GPU_ERR_ARG, "sizes do not match the element kind");
-  if (nnode <= 0 || nelem <= 0 || !xyz || !conn || !first_dof || !gp || ngroups <= 0 || order < 1 || order > 4)
-    return bfail(b, BETA_GPU_ERR_ARG, "bad mesh or material arguments");
-  if (!eg && ngroups != nelem) return bfail(b, BETA_GPU_ERR_ARG, "without elem_group there must be one group per element");
-  const size_t ndof = (size_t)nnode * ndpn;
-  if (!all_finite(xyz, (size_t)nnode * ndim) || !all_finite(gp, (size_t)ngroups * nparams) ||
-      (prescribed && !all_finite(prescribed, ndof)) || (load && !all_finite(load, ndof)))
-    return bfail(b, BETA_GPU_ERR_NOT_FINITE, "non-finite input");
-  for (long long k = 0; k < (long long)nelem * nnpe; ++k)
-    if (conn[k] < 0 || conn[k] >= nnode) return bfail(b, BETA_GPU_ERR_ARG, "connectivity out of range");
-  if (eg)
-    for (int e = 0; e < nelem; ++e)
-      if (eg[e] < 0 || eg[e] >= ngroups) return bfail(b, BETA_GPU_ERR_ARG, "elem_group out of range");
-  std::vector<unsigned char> r(ndof, 0);
-  if (restrained)
-    for (size_t i = 0; i < ndof; ++i) r[i] = restrained[i] ? 1 : 0;
-  if (load)
-    for (size_t i = 0; i < ndof; ++i)
-      if (r[i] && load[i] != 0.0)
-        return bfail(b, BETA_GPU_ERR_LOAD_ON_RESTRAINED, "Cannot add load to a restrained degree of freedom.");
-  HostPattern P;
-  std::string msg = build_pattern(nnode, nelem, nnpe, ndpn, conn, first_dof, r.data(), P, false);
-  if (!msg.empty()) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, msg);
-  SysLayout L = layout_for(ndim, nnode, nelem, nnpe, ndpn, ngroups, nparams, eg != nullptr, P);
-  int id;
-  if (!b->free_ids.empty()) id = b->free_ids.back();
-  else if ((int)b->sys.size() < b->cap) id = (int)b->sys.size();
-  else return bfail(b, BETA_GPU_REJECTED, "batch holds max_systems systems");
-  const long long off = pool_alloc(b, L.total);
-  if (off < 0) return bfail(b, BETA_GPU_REJECTED, "HBM budget exhausted: the system does not fit in the pool");
-  if (!b->free_ids.empty()) b->free_ids.pop_back();
-  else b->sys.emplace_back();
-  unsigned char* base = b->pool + off;
-  const GaussTable* gt = batch_gauss(b, ndim, order);
-  int rc = gt ? BETA_GPU_OK : BETA_GPU_ERR_CUDA;
-  std::vector<double> zero(ndof, 0.0);
-  auto up = [&](size_t o, const void* src, size_t bytes) { if (!rc) rc = batch_h2d(b, base + o, src, bytes); };
-  up(L.o_xyz, xyz, sizeof(double) * nnode * ndim);
-  up(L.o_conn, conn, sizeof(int) * (size_t)nelem * nnpe);
-  up(L.o_gp, gp, sizeof(double) * (size_t)ngroups * nparams);
-  if (eg) up(L.o_eg, eg, sizeof(int) * nelem);
-  up(L.o_rest, r.data(), ndof);
-  up(L.o_presc, prescribed ? prescribed : zero.data(), sizeof(double) * ndof);
-  up(L.o_load, load ? load : zero.data(), sizeof(double) * ndof);
-  up(L.o_cptr, P.color_ptr.data(), sizeof(int) * P.color_ptr.size());
-  up(L.o_elems, P.elem_by_color.data(), sizeof(int) * P.elem_by_color.size());
-  up(L.o_slot, P.slot.data(), sizeof(int) * P.slot.size());
-  up(L.o_nrp, P.nrp.data(), sizeof(int) * P.nrp.size());
-  up(L.o_ndiag, P.ndiag.data(), sizeof(int) * P.ndiag.size());
-  up(L.o_bsoff, P.bsoff.data(), sizeof(int) * P.bsoff.size());
-  up(L.o_bcol, P.bcol.data(), sizeof(int) * P.bcol.size());
-  if (rc == BETA_GPU_OK && cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); rc = BETA_GPU_ERR_CUDA; }
-  beta_gpu_batch::Sys& S = b->sys[id];
-  if (rc != BETA_GPU_OK) {
-    pool_free(b, off, L.total);
-    S.live = false;
-    b->free_ids.push_back(id);
-    return bfail(b, rc, "upload of the system failed");
+  int first = BETA_GPU_OK;
+  for (int i = 0; i < count; ++i) {
+    int id = -1;
+    if (rc[i] == BETA_GPU_OK) rc[i] = admit_system(b, P[i], &id);
+    else bfail(b, rc[i], err[i]);
+    P[i] = PreparedSys();  // release host copies as we go
+    ids[i] = rc[i] == BETA_GPU_OK ? id : -rc[i];
+    if (rc[i] != BETA_GPU_OK && first == BETA_GPU_OK) first = rc[i];
   }
-  S.live = true;
-  S.kind = kind; S.ndim = ndim; S.nnode = nnode; S.nelem = nelem; S.nnpe = nnpe; S.ndpn = ndpn;
-  S.ndof = (int)ndof; S.order = order; S.off = (size_t)off; S.bytes = L.total;
-  S.work = (long long)P.nchunk * 32 * ndpn * ndpn;
-  BSys& D = S.desc;
-  std::memset(&D, 0, sizeof(D));
-  GaussTable hg;
-  make_gauss_table(ndim, order, hg);
-  D.kind = kind; D.ndpn = ndpn; D.nnode = nnode; D.nelem = nelem; D.ndof = (int)ndof; D.nip = hg.nip;
-  D.ncolor = P.ncolor; D.nslice = P.nslice; D.nparams = nparams; D.ndim = ndim;
-  D.xyz = (const double*)(base + L.o_xyz);
-  D.conn = (const int*)(base + L.o_conn);
-  D.gparams = (const double*)(base + L.o_gp);
-  D.egroup = eg ? (const int*)(base + L.o_eg) : nullptr;
-  D.rest = base + L.o_rest;
-  D.presc = (const double*)(base + L.o_presc);
-  D.load = (const double*)(base + L.o_load);
-  D.color_ptr = (const int*)(base + L.o_cptr);
-  D.elems = (const int*)(base + L.o_elems);
-  D.slot = (const int*)(base + L.o_slot);
-  D.nrp = (const int*)(base + L.o_nrp);
-  D.ndiag = (const int*)(base + L.o_ndiag);
-  D.bsoff = (const int*)(base + L.o_bsoff);
-  D.bcol = (const int*)(base + L.o_bcol);
-  D.bval = (float*)(base + L.o_bval);
-  D.x64 = (double*)(base + L.o_x64);
-  D.r64 = (double*)(base + L.o_r64);
-  D.y64 = (double*)(base + L.o_y64);
-  D.y32 = (float*)(base + L.o_y32);
-  D.r32 = (float*)(base + L.o_r32);
-  D.p32 = (float*)(base + L.o_p32);
-  D.q32 = (float*)(base + L.o_q32);
-  D.minv = (float*)(base + L.o_minv);
-  D.gt = gt;
-  D.st = b->d_states + id;
-  D.nchunk = P.nchunk;
-  BState s0;
-  std::memset(&s0, 0, sizeof(s0));
-  s0.phase = kPhaseNew;
-  s0.status = kBRunning;
-  S.st = s0;
-  b->h_states[id] = s0;
-  if ((rc = batch_h2d(b, b->d_states + id, b->h_states + id, sizeof(BState)))) return rc;
-  BCK(cudaStreamSynchronize(b->stream));
-  *sys_id = id;
-  return BETA_GPU_OK;
+  return first;
 }
 
 int beta_gpu_batch_run(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int iters_per_launch, int* n_unfinished) {
@@ -1486,8 +1585,11 @@ int beta_gpu_batch_run(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int iter
   int na = 0, rc;
   if ((rc = batch_prepare(b, o, iters_per_launch, &na))) return rc;
   if (na > 0) {
+    BCK(cudaEventRecord(b->ev0, b->stream));
     if ((rc = batch_launch_graph(b))) return rc;
+    BCK(cudaEventRecord(b->ev1, b->stream));
     if ((rc = batch_pull_states(b))) return rc;
+    BCK(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
   }
   int left = 0;
   for (auto& S : b->sys)
@@ -1591,11 +1693,137 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
   return BETA_GPU_OK;
 }
 
+int beta_gpu_batch_reset(beta_gpu_batch* b) {
+  if (!b) return BETA_GPU_ERR_ARG;
+  cudaSetDevice(b->device);
+  int rc = batch_reset_states(b);
+  if (rc) return rc;
+  BCK(cudaStreamSynchronize(b->stream));
+  return BETA_GPU_OK;
+}
+
 int beta_gpu_batch_info(const beta_gpu_batch* b, long long* out, int n) {
-  if (!b || !out || n < 0 || n > 6) return BETA_GPU_ERR_ARG;
+  if (!b || !out || n < 0 || n > 7) return BETA_GPU_ERR_ARG;
   long long live = 0;
   for (auto& S : b->sys) live += S.live ? 1 : 0;
-  const long long v[6] = {live, (long long)b->used, (long long)b->pool_bytes, b->n_launch, b->n_h2d, b->n_d2h};
+  const long long v[7] = {live, (long long)b->used, (long long)b->pool_bytes, b->n_launch, b->n_h2d, b->n_d2h,
+                          (long long)((double)b->last_ms * 1e6)};
+  for (int i = 0; i < n; ++i) out[i] = v[i];
+  return BETA_GPU_OK;
+}
+
+// ============================ server C ABI ===================================
+int beta_gpu_server_create(beta_gpu_server** out, int device, long long budget, int max_systems,
+                           const beta_gpu_solve_opts* o, int iters_per_launch, int threads, int cluster) {
+  if (!out || !o || iters_per_launch <= 0) return BETA_GPU_ERR_ARG;
+  *out = nullptr;
+  beta_gpu_batch* b = nullptr;
+  int rc = beta_gpu_batch_create(&b, device, budget, max_systems);
+  if (rc != BETA_GPU_OK) return rc;
+  if ((threads || cluster) && (rc = beta_gpu_batch_tune(b, threads ? threads : b->threads,
+                                                         cluster ? cluster : b->cluster)) != BETA_GPU_OK) {
+    beta_gpu_batch_destroy(b);
+    return rc;
+  }
+  std::unique_ptr<beta_gpu_server> S(new beta_gpu_server());
+  S->batch = b;
+  S->opts = *o;
+  S->iters_per_launch = iters_per_launch;
+  S->pool_bytes = (long long)b->pool_bytes;
+  try {
+    S->worker = std::thread(server_loop, S.get());
+  } catch (...) {
+    beta_gpu_batch_destroy(b);
+    return BETA_GPU_ERR_STATE;
+  }
+  *out = S.release();
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_server_destroy(beta_gpu_server* S) {
+  if (!S) return BETA_GPU_OK;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->wake.notify_all();
+  if (S->worker.joinable()) S->worker.join();
+  beta_gpu_batch_destroy(S->batch);
+  delete S;
+  return BETA_GPU_OK;
+}
+
+const char* beta_gpu_server_last_error(const beta_gpu_server* S) { return S ? S->err.c_str() : "null server"; }
+
+int beta_gpu_server_submit(beta_gpu_server* S, int kind, int ndim, int nnode, const double* xyz, int nelem,
+                           int nnpe, const int* conn, const int* first_dof, int ndpn, int order, int ngroups,
+                           int nparams, const double* gp, const int* eg, const unsigned char* restrained,
+                           const double* prescribed, const double* load, long long* request_id) {
+  if (!S || !request_id) return BETA_GPU_ERR_ARG;
+  const auto t0 = beta_gpu_server::clock::now();
+  std::unique_ptr<PreparedSys> P(new PreparedSys());
+  std::string err;
+  const int rc = prepare_system(kind, ndim, nnode, xyz, nelem, nnpe, conn, first_dof, ndpn, order, ngroups, nparams,
+                                gp, eg, restrained, prescribed, load, *P, err);
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (rc != BETA_GPU_OK) {
+    S->err = err;
+    return rc;
+  }
+  if (S->stop) return BETA_GPU_ERR_STATE;
+  const long long id = S->next_id++;
+  beta_gpu_server::Req& R = S->reqs[id];
+  R.ndof = (int)P->ndof();
+  R.prep = std::move(P);
+  R.t_submit = t0;
+  std::memset(&R.st, 0, sizeof(R.st));
+  S->queue.push_back(id);
+  ++S->n_submitted;
+  *request_id = id;
+  S->wake.notify_one();
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_server_poll(beta_gpu_server* S, long long id, int wait_ms, int* state, int* ndof, double* u,
+                         beta_gpu_solve_stats* st, double* latency_ms, int release) {
+  if (!S) return BETA_GPU_ERR_ARG;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end()) return BETA_GPU_ERR_ARG;
+  if (wait_ms > 0 && !req_final(it->second.state)) {
+    const auto until = beta_gpu_server::clock::now() + std::chrono::milliseconds(wait_ms);
+    S->done.wait_until(lk, until, [&] { return req_final(S->reqs.at(id).state); });
+  }
+  beta_gpu_server::Req& R = S->reqs.at(id);
+  if (state) *state = R.state;
+  if (ndof) *ndof = R.ndof;
+  if (st) {
+    *st = R.st;
+    st->status = req_final(R.state) ? R.status : BETA_GPU_ERR_STATE;
+  }
+  if (latency_ms)
+    *latency_ms = req_final(R.state) ? std::chrono::duration<double, std::milli>(R.t_done - R.t_submit).count() : -1.0;
+  if (u && R.state == kReqDone) std::copy(R.u.begin(), R.u.end(), u);
+  if (release && req_final(R.state)) S->reqs.erase(id);
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_server_cancel(beta_gpu_server* S, long long id) {
+  if (!S) return BETA_GPU_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end()) return BETA_GPU_ERR_ARG;
+  if (!req_final(it->second.state)) it->second.cancel = true;
+  S->wake.notify_one();
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_server_stats(beta_gpu_server* S, long long* out, int n) {
+  if (!S || !out || n < 0 || n > 13) return BETA_GPU_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  const long long v[13] = {S->n_submitted, S->n_done,      S->n_rejected,          S->n_failed,
+                           S->n_cancelled, (long long)S->queue.size(), S->n_running, S->n_launches,
+                           S->pool_used,   S->pool_bytes, (long long)(S->busy_ms * 1000.0), S->h2d, S->d2h};
   for (int i = 0; i < n; ++i) out[i] = v[i];
   return BETA_GPU_OK;
 }

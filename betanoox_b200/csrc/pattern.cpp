@@ -8,10 +8,14 @@
 
 namespace betagpu {
 
+static thread_local bool t_serial = false;
+
+void pattern_serial_on_this_thread(bool on) { t_serial = on; }
+
 static void parallel_for(long long n, const std::function<void(long long, long long)>& body) {
   unsigned hw = std::thread::hardware_concurrency();
   int t = (int)std::min<unsigned>(hw ? hw : 1, 64);
-  if (n < 20000 || t <= 1) { body(0, n); return; }
+  if (t_serial || n < 20000 || t <= 1) { body(0, n); return; }
   std::vector<std::thread> th;
   for (int k = 0; k < t; ++k) {
     long long lo = n * k / t, hi = n * (k + 1) / t;

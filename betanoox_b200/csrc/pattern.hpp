@@ -66,6 +66,10 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
                           const int* first_dof, const unsigned char* restrained, HostPattern& P,
                           bool with_scalar = true);
 
+// Makes build_pattern on the calling thread single-threaded (for callers that
+// already build many patterns in parallel).
+void pattern_serial_on_this_thread(bool on);
+
 // Lower-triangle pattern export in SymmetricSparseMatrix order.
 void export_lower_pattern(const HostPattern& P, const unsigned char* restrained,
                           long long* row_ptr, int* col);

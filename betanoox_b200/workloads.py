@@ -212,33 +212,79 @@ def heat_slab(nx=256, ny=256, nz=64, seed=7, order=3, lx=1.0, ly=1.0):
 
 
 # ---- configuration 4: two-phase RVE cubes ------------------------------------
+def _sqdist(a, b):
+    """Squared distances between the rows of a and of b, summed x, y, z in order."""
+    dx = a[:, None, 0] - b[None, :, 0]
+    dy = a[:, None, 1] - b[None, :, 1]
+    dz = a[:, None, 2] - b[None, :, 2]
+    return dx * dx + dy * dy + dz * dz
+
+
+def _place_spheres(CC, R, vf_target, block=256):
+    """Sequential random addition: candidate t is accepted when it overlaps no
+    sphere accepted before it, until the accepted volume reaches vf_target.
+    Candidates are screened in blocks against the spheres accepted before the
+    block (vectorised); survivors are then checked in order against the ones
+    accepted inside the block, which gives exactly the sequential result."""
+    acc_c = np.zeros((0, 3))
+    acc_r = np.zeros(0)
+    vol = 0.0
+    for b0 in range(0, len(R), block):
+        if vol >= vf_target:
+            break
+        cb, rb = CC[b0:b0 + block], R[b0:b0 + block]
+        if acc_r.size:
+            d = np.sqrt(_sqdist(cb, acc_c))
+            ok = ~np.any(d < rb[:, None] + acc_r[None, :], axis=1)
+        else:
+            ok = np.ones(len(rb), bool)
+        cand = np.flatnonzero(ok)
+        cc, rr = cb[cand], rb[cand]
+        ov = (np.sqrt(_sqdist(cc, cc)) < rr[:, None] + rr[None, :]).tolist()
+        taken = []
+        for a in range(len(cand)):
+            if vol >= vf_target:
+                break
+            row = ov[a]
+            if any(row[q] for q in taken):
+                continue
+            taken.append(a)
+            vol += 4.0 / 3.0 * math.pi * float(rr[a]) ** 3
+        if taken:
+            acc_c = np.vstack([acc_c, cc[taken]])
+            acc_r = np.append(acc_r, rr[taken])
+    return acc_c, acc_r
+
+
+def _mark_inclusions(n, centres, radii):
+    """Elements of the n^3 unit-cube grid whose centre lies inside a sphere
+    (each sphere visits only the element block of its bounding box)."""
+    h = 1.0 / n
+    g = (np.arange(n) + 0.5) * h  # element-centre coordinates along each axis
+    inc = np.zeros((n, n, n), bool)  # [k, j, i] = element i + n*(j + n*k)
+    for c, r in zip(centres, radii):
+        lo = np.maximum(np.floor((c - r) / h - 0.5).astype(int), 0)
+        hi = np.minimum(np.ceil((c + r) / h - 0.5).astype(int) + 1, n)
+        dx = (g[lo[0]:hi[0]] - c[0]) ** 2
+        dy = (g[lo[1]:hi[1]] - c[1]) ** 2
+        dz = (g[lo[2]:hi[2]] - c[2]) ** 2
+        inside = dz[:, None, None] + dy[None, :, None] + dx[None, None, :] <= r * r
+        inc[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] |= inside
+    return inc.ravel()
+
+
 def rve_hex8(n, seed, order=2, E_matrix=1e3, contrast=10.0, nu=0.3, ux=0.01):
     """n^3 hex8 unit cube with non-overlapping spherical inclusions placed by
     seeded rejection until the drawn volume fraction ~U[0.2,0.4] is reached
     (radii ~U[0.05,0.15]); E_incl = contrast*E_matrix; x=0 clamped, u_x = ux on x=1."""
     xyz, conn = grid_hex8(n, n, n)
-    ne = conn.shape[0]
     vf_target = 0.2 + 0.2 * uniform(seed, 11, 0)[()]
     tries = np.arange(20000, dtype=np.uint64)
     R = 0.05 + 0.10 * uniform(seed, 12, tries)
     CC = np.stack([uniform(seed, 13, tries), uniform(seed, 14, tries), uniform(seed, 15, tries)], axis=1)
     CC = R[:, None] + (1 - 2 * R[:, None]) * CC
-    acc_c = np.zeros((0, 3))
-    acc_r = np.zeros(0)
-    vol = 0.0
-    for t in range(len(R)):
-        if vol >= vf_target:
-            break
-        if acc_r.size and np.any(np.sqrt(((acc_c - CC[t]) ** 2).sum(axis=1)) < R[t] + acc_r):
-            continue
-        acc_c = np.vstack([acc_c, CC[t]])
-        acc_r = np.append(acc_r, R[t])
-        vol += 4.0 / 3.0 * math.pi * R[t] ** 3
-    centres, radii = list(acc_c), list(acc_r)
-    cen = xyz[conn].mean(axis=1)
-    inc = np.zeros(ne, bool)
-    for cc, r in zip(centres, radii):
-        inc |= np.sum((cen - cc) ** 2, axis=1) <= r * r
+    centres, radii = _place_spheres(CC, R, vf_target)
+    inc = _mark_inclusions(n, centres, radii)
     E = np.where(inc, contrast * E_matrix, E_matrix)
     params = iso3d_params(E, nu)
     ndof = 3 * xyz.shape[0]
@@ -258,3 +304,75 @@ def rve_batch(count=512, seed=99, n_lo=8, n_hi=40):
     sides = n_lo + (uniform(seed, 21, np.arange(count, dtype=np.uint64)) * (n_hi - n_lo + 1)).astype(int)
     sides = np.minimum(sides, n_hi)
     return [rve_hex8(int(n), seed * 100003 + i) for i, n in enumerate(sides)]
+
+
+# ---- configuration 5: serving request stream ----------------------------------
+SERVE_FAMILIES = ("quad4_pstress", "hex8_elastic", "hex8_heat")
+
+
+def serve_request(seed, i, dof_lo=1e3, dof_hi=5e5):
+    """Request i of a seeded serving stream.  Element family uniform over quad4
+    plane stress, hex8 elasticity and hex8 steady diffusion; size log-uniform
+    in [dof_lo, dof_hi] dofs; box aspect ratios ~U[0.5, 2] with cubic cells of
+    side h = 1/nx (seeded geometry); per-element lognormal moduli as the cube
+    (E = 1e4 exp(N(0, 0.5^2)), nu ~ U[0.20, 0.35]) or conductivity
+    k = exp(N(0, 1)).  Loads: quad4 -- left edge clamped, unit +x traction on
+    the right edge; hex8 elasticity -- z=0 clamped, unit pressure on the top;
+    diffusion -- T = 1 on x=0 and T = 0 on x=lx."""
+    rs = seed * 1000003 + i
+    fam = int(uniform(rs, 31, 0)[()] * 3) % 3
+    target = math.exp(math.log(dof_lo) + (math.log(dof_hi) - math.log(dof_lo)) * uniform(rs, 32, 0)[()])
+    a = 0.5 * 4.0 ** uniform(rs, 33, 0)[()]
+    b = 0.5 * 4.0 ** uniform(rs, 34, 0)[()]
+    if fam == 0:  # 2 (nx+1)(ny+1) ~ target
+        nx = max(2, int(round(math.sqrt(target / 2.0 / a))) - 1)
+        ny = max(2, int(round(nx * a)))
+        xyz, conn = grid_quad4(nx, ny, 1.0, ny / nx)
+        ne = conn.shape[0]
+        eid = np.arange(ne, dtype=np.uint64)
+        params = pstress_params(1e4 * np.exp(0.5 * normal(rs, 1, eid)), 0.20 + 0.15 * uniform(rs, 3, eid))
+        ndof = 2 * xyz.shape[0]
+        rest = np.zeros(ndof, np.uint8)
+        left = np.where(np.isclose(xyz[:, 0], 0.0))[0]
+        rest[2 * left] = 1
+        rest[2 * left + 1] = 1
+        right = np.where(np.isclose(xyz[:, 0], 1.0))[0]
+        h = 1.0 / nx
+        w = np.full(right.shape, h)
+        w[np.isclose(xyz[right, 1], 0.0) | np.isclose(xyz[right, 1], ny / nx)] = h / 2
+        load = np.zeros(ndof)
+        load[2 * right] = w
+        return Model(f"serve_{i}_quad4_{nx}x{ny}", _abi.QUAD4_PSTRESS, 2, xyz, conn, 2, params, rest,
+                     np.zeros(ndof), load, 2, {"family": SERVE_FAMILIES[fam], "i": i, "seed": seed})
+    ndpn = 3 if fam == 1 else 1
+    nx = max(2, int(round((target / ndpn / (a * b)) ** (1.0 / 3.0))) - 1)
+    ny, nz = max(2, int(round(nx * a))), max(2, int(round(nx * b)))
+    lx, ly, lz = 1.0, ny / nx, nz / nx
+    xyz, conn = grid_hex8(nx, ny, nz, lx, ly, lz)
+    ne = conn.shape[0]
+    eid = np.arange(ne, dtype=np.uint64)
+    nnode = xyz.shape[0]
+    if fam == 1:
+        params = iso3d_params(1e4 * np.exp(0.5 * normal(rs, 1, eid)), 0.20 + 0.15 * uniform(rs, 3, eid))
+        ndof = 3 * nnode
+        rest = np.zeros(ndof, np.uint8)
+        bot = np.where(np.isclose(xyz[:, 2], 0.0))[0]
+        for c in range(3):
+            rest[3 * bot + c] = 1
+        top = np.where(np.isclose(xyz[:, 2], lz))[0]
+        h = 1.0 / nx
+        onx = np.isclose(xyz[top, 0], 0.0) | np.isclose(xyz[top, 0], lx)
+        ony = np.isclose(xyz[top, 1], 0.0) | np.isclose(xyz[top, 1], ly)
+        nface = 4 // (1 + onx.astype(int)) // (1 + ony.astype(int))
+        load = np.zeros(ndof)
+        load[3 * top + 2] = -h * h / 4.0 * nface
+        return Model(f"serve_{i}_hex8_{nx}x{ny}x{nz}", _abi.HEX8_ELASTIC, 3, xyz, conn, 3, params, rest,
+                     np.zeros(ndof), load, 2, {"family": SERVE_FAMILIES[fam], "i": i, "seed": seed})
+    k = np.exp(normal(rs, 5, eid))
+    params = np.stack([k, k, k, np.ones(ne)], axis=1)
+    x0 = np.isclose(xyz[:, 0], 0.0)
+    x1 = np.isclose(xyz[:, 0], lx)
+    rest = (x0 | x1).astype(np.uint8)
+    presc = np.where(x0, 1.0, 0.0)
+    return Model(f"serve_{i}_heat_{nx}x{ny}x{nz}", _abi.HEX8_HEAT, 3, xyz, conn, 1, params, rest, presc,
+                 np.zeros(nnode), 2, {"family": SERVE_FAMILIES[fam], "i": i, "seed": seed})

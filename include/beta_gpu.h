@@ -258,6 +258,25 @@ BETA_GPU_API int beta_gpu_batch_add(beta_gpu_batch* batch, int kind, int ndim, i
                                     int integration_order, int ngroups, int nparams, const double* group_params,
                                     const int* elem_group, const unsigned char* restrained,
                                     const double* prescribed, const double* load, int* sys_id);
+/* One system for beta_gpu_batch_add_many: the arguments of beta_gpu_batch_add. */
+typedef struct beta_gpu_system {
+  int kind, ndim, nnode, nelem, nnpe, ndof_per_node, integration_order, ngroups, nparams, reserved;
+  const double* xyz;
+  const int* conn;
+  const int* first_dof;
+  const double* group_params;
+  const int* elem_group;
+  const unsigned char* restrained;
+  const double* prescribed;
+  const double* load;
+} beta_gpu_system;
+/* Adds `count` systems: their structures are built on up to `host_threads`
+ * host threads (0 = all cores), then they are copied into the pool in order.
+ * sys_ids[i] receives the id, or -(status) for a system that was not added
+ * (bad input, or BETA_GPU_REJECTED when the pool is full).  Returns
+ * BETA_GPU_OK when every system was added, else the first failing status. */
+BETA_GPU_API int beta_gpu_batch_add_many(beta_gpu_batch* batch, int count, const beta_gpu_system* systems,
+                                         int host_threads, int* sys_ids);
 BETA_GPU_API int beta_gpu_batch_run(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int iters_per_launch,
                                     int* n_unfinished);
 /* Status/iterations of one system; u (ndof, may be NULL) receives its current solution. */
@@ -272,9 +291,63 @@ BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta,
  * time per unit of work. */
 BETA_GPU_API int beta_gpu_batch_autotune(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int budget,
                                          int* threads_per_cta, int* cluster_ctas);
+/* Marks every system unsolved: its next launch assembles and solves it again
+ * from the data already in the pool (repeat solves without re-upload). */
+BETA_GPU_API int beta_gpu_batch_reset(beta_gpu_batch* batch);
 /* out[0] live systems, out[1] pool bytes in use, out[2] pool bytes, out[3]
- * launches, out[4] bytes host->device, out[5] bytes device->host; n <= 6. */
+ * launches, out[4] bytes host->device, out[5] bytes device->host, out[6]
+ * device time of the last launch in ns (CUDA events on the batch's stream);
+ * n <= 7. */
 BETA_GPU_API int beta_gpu_batch_info(const beta_gpu_batch* batch, long long* out, int n);
+
+/* ---- continuous-batching server ------------------------------------------ */
+/* No counterpart in the reference (one model per process run).  A server owns
+ * a batch and one worker thread.  beta_gpu_server_submit checks a system and
+ * builds its structure on the calling thread, then queues it; the worker
+ * admits queued systems in arrival order while the HBM pool has room, runs
+ * bounded launches of iters_per_launch iterations over every admitted system
+ * (new systems join between launches, with their assembly inside the launch)
+ * and retires finished ones to host memory.  A request that does not fit into
+ * an empty pool ends REJECTED.  Every system is solved exactly as
+ * beta_gpu_batch_run solves it, so its result does not depend on what else is
+ * in flight. */
+#define BETA_GPU_REQ_QUEUED 0
+#define BETA_GPU_REQ_RUNNING 1
+#define BETA_GPU_REQ_DONE 2
+#define BETA_GPU_REQ_REJECTED 3
+#define BETA_GPU_REQ_CANCELLED 4
+#define BETA_GPU_REQ_FAILED 5
+typedef struct beta_gpu_server beta_gpu_server;
+/* threads_per_cta / cluster_ctas as in beta_gpu_batch_tune; 0 keeps the default. */
+BETA_GPU_API int beta_gpu_server_create(beta_gpu_server** server, int device, long long hbm_budget_bytes,
+                                        int max_systems, const beta_gpu_solve_opts* opts, int iters_per_launch,
+                                        int threads_per_cta, int cluster_ctas);
+/* Stops the worker after its current launch; unfinished requests are dropped. */
+BETA_GPU_API int beta_gpu_server_destroy(beta_gpu_server* server);
+BETA_GPU_API const char* beta_gpu_server_last_error(const beta_gpu_server* server);
+/* Same system arguments as beta_gpu_batch_add; input errors return at once. */
+BETA_GPU_API int beta_gpu_server_submit(beta_gpu_server* server, int kind, int ndim, int nnode, const double* xyz,
+                                        int nelem, int nnpe, const int* conn, const int* first_dof,
+                                        int ndof_per_node, int integration_order, int ngroups, int nparams,
+                                        const double* group_params, const int* elem_group,
+                                        const unsigned char* restrained, const double* prescribed,
+                                        const double* load, long long* request_id);
+/* Waits up to wait_ms for the request to reach a final state (DONE, REJECTED,
+ * CANCELLED, FAILED), then reports its state, ndof, stats (stats->status is
+ * the solve status once final, BETA_GPU_ERR_STATE before) and latency from
+ * submit to completion in ms (-1 before).  u (ndof doubles, may be NULL)
+ * receives the solution of a DONE request.  release != 0 forgets a final
+ * request.  Returns BETA_GPU_ERR_ARG for an unknown id. */
+BETA_GPU_API int beta_gpu_server_poll(beta_gpu_server* server, long long request_id, int wait_ms, int* state,
+                                      int* ndof, double* u, beta_gpu_solve_stats* stats, double* latency_ms,
+                                      int release);
+/* Queued requests end CANCELLED before admission, running ones after the current launch. */
+BETA_GPU_API int beta_gpu_server_cancel(beta_gpu_server* server, long long request_id);
+/* out[0] submitted, [1] done, [2] rejected, [3] failed, [4] cancelled,
+ * [5] queued, [6] running, [7] launches, [8] pool bytes in use, [9] pool
+ * bytes, [10] microseconds the worker spent in launches, [11] bytes
+ * host->device, [12] bytes device->host; n <= 13. */
+BETA_GPU_API int beta_gpu_server_stats(beta_gpu_server* server, long long* out, int n);
 
 /* ---- allocation-free variant of beta_gpu_csr_pcg_device ------------------ */
 /* No counterpart in the reference (BETA's solvers allocate their work vectors

@@ -100,3 +100,21 @@ def test_create_without_gpu_fails_cleanly(abi):
     h = C.c_void_p()
     st = abi.beta_gpu_create(C.byref(h), 0)
     assert st != 0 and not h.value
+
+
+def test_structured_block_count_matches_pattern():
+    """The batch bench counts node-pair blocks of n^3 cubes as (3n+1)^3."""
+    import bench
+    for n in (1, 2, 5):
+        m = W.rve_hex8(n, 3)
+        assert bench.structured_nblk(m) == bench._nblk(m)
+
+
+def test_serve_requests_cover_families_and_sizes():
+    ms = [W.serve_request(5, i) for i in range(60)]
+    fams = {m.meta["family"] for m in ms}
+    assert fams == set(W.SERVE_FAMILIES)
+    nd = np.array([m.ndof for m in ms])
+    assert nd.min() >= 500 and nd.max() <= 6e5
+    for m in ms[:6]:
+        assert m.restrained.any() and np.isfinite(m.params).all()

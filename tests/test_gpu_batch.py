@@ -95,3 +95,20 @@ def test_batch_autotune_keeps_results(oracle):
         rc, u, st = b.result(sid)
         ut = _truth(oracle, m)
         assert rc == _abi.OK and np.linalg.norm(u - ut) / np.linalg.norm(ut) <= 1e-8
+
+
+def test_add_many_equals_add_and_reset_repeats():
+    models = _mix()
+    b1 = Batch(hbm_budget=1 << 30)
+    ids1 = [b1.add(m) for m in models]
+    b2 = Batch(hbm_budget=1 << 30)
+    ids2 = b2.add_many(models, host_threads=4)
+    assert b1.run(opts(tol=1e-12)) == 0 and b2.run(opts(tol=1e-12)) == 0
+    first = [b2.result(i)[1] for i in ids2]
+    for i1, i2 in zip(ids1, ids2):
+        np.testing.assert_array_equal(b1.result(i1)[1], b2.result(i2)[1])
+    assert b2.info()["last_launch_ns"] > 0
+    b2.reset()  # same systems again, re-assembled from the pool
+    assert b2.run(opts(tol=1e-12)) == 0
+    for i2, u in zip(ids2, first):
+        np.testing.assert_array_equal(b2.result(i2)[1], u)
