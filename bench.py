@@ -12,7 +12,8 @@ Multi-GPU (torchrun): every rank solves its own replica (the path does not
 shard: one system per GPU); value = total dofs solved / max-over-ranks time.
 
 --config batch: 512 two-phase RVE cubes (n ~ U{8..40}) solved together in one
-persistent launch (thread-block cluster per system, autotuned launch shape);
+persistent launch (gangs of CTAs for big systems, single CTAs for small ones,
+autotuned launch shape);
 one step = reset + assembly + mixed-precision solve of all 512.
 --config serve: a Poisson stream of requests (quad4 / hex8 elasticity / hex8
 diffusion, log-uniform 1e3-5e5 dofs) through the continuous-batching server at
@@ -518,7 +519,7 @@ def run_batch(args):
     t_add = time.perf_counter() - t0
     assert all(i is not None for i in ids), "pool too small for the batch"
     t0 = time.perf_counter()
-    threads, cluster = b.autotune(o, budget=args.tune_iters)
+    threads, boost = b.autotune(o, budget=args.tune_iters)
     t_tune = time.perf_counter() - t0
     for _ in range(args.warmup):
         b.reset()
@@ -533,6 +534,7 @@ def run_batch(args):
             assert left == 0
             ms.append(b.info()["last_launch_ns"] / 1e6)
     launches = b.info()["launches"] - l0
+    ginfo = b.info()
     _barrier()
     res = [b.result(i, with_u=False) for i in ids]
     bad = [(models[k].name, _abi.STATUS_NAMES.get(r[0])) for k, r in enumerate(res) if r[0] != _abi.OK]
@@ -580,7 +582,7 @@ def run_batch(args):
             for _ in range(max(1, args.e2e_steps)):
                 t1 = time.perf_counter()
                 be = Batch(dev, hbm_budget=int(args.pool_gb * (1 << 30)), max_systems=len(models) + 8)
-                be.tune(threads, cluster)
+                be.tune(threads, boost)
                 eids = be.add_many(models)
                 be.run(o)
                 for sid in eids:
@@ -597,7 +599,7 @@ def run_batch(args):
         alg = sum(it * iter_bytes(structured_nblk(m), m.nnode, 3) for it, m in zip(iters, models))
         achieved = alg / (ms_launch * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": f"k_batch_solve<{threads}> (cluster {cluster}): assembly + all PCG",
+                "traffic": None, "kernel": f"k_batch_solve<{threads}> (gang boost {boost}): assembly + all PCG",
                 "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_launch,
                 "note": "inner-iteration bytes only (assembly and FP64 residual replacements excluded); "
                         "small systems re-read their matrix from L2",
@@ -612,7 +614,9 @@ def run_batch(args):
             "config": {"workload": f"{len(models)} two-phase RVE hex8 cubes n~U{{8..40}} "
                                    f"(n {sizes[0]}..{sizes[-1]}), {ndof_tot} dofs total, one persistent launch",
                        "global_batch": ws * len(models), "ndof_total": ndof_tot, "parallelism": f"replicas x{ws}",
-                       "tol": args.tol, "stop_rule": "||b-Au||/||b||", "launch_shape": [threads, cluster],
+                       "tol": args.tol, "stop_rule": "||b-Au||/||b||",
+                       "launch_shape": {"threads": threads, "gang_boost": boost, "gangs": ginfo["gangs"],
+                                        "gang_ctas": ginfo["gang_ctas"]},
                        "l2": f"inputs larger than L2 (pool {b.info()['used'] / 2**30:.1f} GiB)"},
             "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
             "batch": {"ms_steps": ms, "iterations_total": int(sum(iters)), "iterations_max": int(max(iters)),
@@ -728,7 +732,7 @@ def run_serve(args):
     o = opts(mode=_abi.MODE_MPIR, tol=args.tol, inner_tol=args.inner_tol)
     th = args.submit_threads or (os.cpu_count() or 1)
     srv = Server(dev, hbm_budget=int(args.pool_gb * (1 << 30)), max_systems=4096, o=o,
-                 iters_per_launch=args.iters_per_launch, threads=args.threads, cluster=args.cluster)
+                 iters_per_launch=args.iters_per_launch, threads=args.threads, gang_boost=args.gang_boost)
     # capacity: a burst of the first `cap` pool models submitted at once
     cap_n = min(args.capacity_requests, pool_n)
     for _ in range(args.warmup):
@@ -784,7 +788,8 @@ def run_serve(args):
                        "requests": args.requests, "distinct_models": pool_n, "families": fams,
                        "lambda_per_s": lam, "capacity_req_per_s": cap_rps, "tol": args.tol,
                        "iters_per_launch": args.iters_per_launch, "submit_threads": th,
-                       "launch_shape": [args.threads, args.cluster], "parallelism": f"replicas x{ws}",
+                       "launch_shape": {"threads": args.threads, "gang_boost": args.gang_boost},
+                       "parallelism": f"replicas x{ws}",
                        "l2": "working set above L2 (pool of resident systems)"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "mean": float(lat.mean()), "max": float(lat.max())},
@@ -863,7 +868,7 @@ def main():
     ap.add_argument("--count", type=int, default=512)
     ap.add_argument("--seed", type=int, default=99)
     ap.add_argument("--pool-gb", type=float, default=48.0)
-    ap.add_argument("--tune-iters", type=int, default=30)
+    ap.add_argument("--tune-iters", type=int, default=0, help="0: autotune on complete solves")
     ap.add_argument("--check-every", type=int, default=32)
     ap.add_argument("--fp64-sample", type=int, default=512)
     ap.add_argument("--requests", type=int, default=10000)
@@ -872,7 +877,7 @@ def main():
     ap.add_argument("--load", type=float, default=0.8)
     ap.add_argument("--iters-per-launch", type=int, default=200)
     ap.add_argument("--threads", type=int, default=512)
-    ap.add_argument("--cluster", type=int, default=4)
+    ap.add_argument("--gang-boost", type=int, default=4)
     ap.add_argument("--submit-threads", type=int, default=0)
     ap.add_argument("--serve-fp64-sample", type=int, default=100)
     args = ap.parse_args()

@@ -255,12 +255,15 @@ class Batch:
             raise self._err(st, "batch_remove")
         self.models.pop(sid, None)
 
-    def tune(self, threads, cluster=1):
-        st = self.lib.beta_gpu_batch_tune(self.h, threads, cluster)
+    def tune(self, threads, gang_boost=4):
+        """threads per CTA (256/512/1024); a system gets about gang_boost x its
+        share of the batch's CTAs as one gang when that is >= 2 (0: no gangs)."""
+        st = self.lib.beta_gpu_batch_tune(self.h, threads, gang_boost)
         if st != _abi.OK:
             raise self._err(st, "batch_tune")
 
     def autotune(self, o=None, budget=40):
+        """budget iterations per system for each launch shape; 0 = complete solves."""
         o = o or opts()
         t, c = C.c_int(0), C.c_int(0)
         st = self.lib.beta_gpu_batch_autotune(self.h, C.byref(o), budget, C.byref(t), C.byref(c))
@@ -274,10 +277,13 @@ class Batch:
         if st != _abi.OK:
             raise self._err(st, "batch_reset")
 
+    INFO = ["live", "used", "pool", "launches", "h2d", "d2h", "last_launch_ns", "gangs", "gang_ctas", "threads",
+            "gang_boost"]
+
     def info(self):
-        a = (C.c_longlong * 7)()
-        self.lib.beta_gpu_batch_info(self.h, a, 7)
-        return dict(zip(["live", "used", "pool", "launches", "h2d", "d2h", "last_launch_ns"], list(a)))
+        a = (C.c_longlong * len(self.INFO))()
+        self.lib.beta_gpu_batch_info(self.h, a, len(self.INFO))
+        return dict(zip(self.INFO, list(a)))
 
 
 class Server:
@@ -290,12 +296,12 @@ class Server:
              "pool_used", "pool_bytes", "busy_us", "h2d", "d2h"]
 
     def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, max_systems: int = 4096, o=None,
-                 iters_per_launch: int = 200, threads: int = 0, cluster: int = 0):
+                 iters_per_launch: int = 200, threads: int = 0, gang_boost: int = -1):
         self.lib = _abi.load()
         self.o = o or opts()
         h = C.c_void_p()
         st = self.lib.beta_gpu_server_create(C.byref(h), device, int(hbm_budget), int(max_systems),
-                                             C.byref(self.o), int(iters_per_launch), int(threads), int(cluster))
+                                             C.byref(self.o), int(iters_per_launch), int(threads), int(gang_boost))
         if st != _abi.OK:
             raise BetaGpuError(st, "beta_gpu_server_create failed")
         self.h = h

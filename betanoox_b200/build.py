@@ -15,7 +15,6 @@ SRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libbeta_gpu.so")
 SOURCES = ["beta_gpu.cu", "pattern.cpp"]
-HEADERS = ["common.cuh", "elem_kernels.cuh", "mf_kernels.cuh", "pcg_kernels.cuh", "pattern.hpp"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",
@@ -37,7 +36,7 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(SRC, f) for f in SOURCES + HEADERS]
+    deps = [os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith((".cu", ".cuh", ".cpp", ".hpp", ".h"))]
     deps.append(os.path.join(HERE, "..", "include", "beta_gpu.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

@@ -1,8 +1,9 @@
 // batch_host.cuh -- host side of the batched persistent solver (C ABI
 // beta_gpu_batch_*): a device memory pool with first-fit allocation and an
 // HBM budget, per-system structure building and upload, the descriptor table
-// and work list, the launch (captured once into a CUDA graph and replayed),
-// and a small autotuner over CTA size and cluster size.
+// and work list, the gang plan of each launch, the cooperative launch
+// (captured once into a CUDA graph and replayed), and a small autotuner over
+// CTA size and gang sizing.
 // Included by beta_gpu.cu (one translation unit).
 #pragma once
 
@@ -20,7 +21,8 @@ struct beta_gpu_batch {
     bool live = false;
     int kind = 0, ndim = 0, nnode = 0, nelem = 0, nnpe = 0, ndpn = 0, ndof = 0, order = 0;
     size_t off = 0, bytes = 0;
-    long long work = 0;
+    long long work = 0;  // stored FP32 matrix values
+    int nslice = 0;
     BSys desc;
     BState st;
   };
@@ -32,18 +34,25 @@ struct beta_gpu_batch {
   BSys* d_sys = nullptr;
   BState* d_states = nullptr;
   int* d_active = nullptr;
-  int* d_counter = nullptr;
   BParams* d_params = nullptr;
-  BSys* h_sys = nullptr;  // pinned staging
+  BPlan* d_plan = nullptr;  // one entry per CTA slot (kMaxCtas)
+  int* d_ctl = nullptr;     // [0] work counter, [1] abort flag, [2..2+kMaxCtas) gang arrival counters
+  BSys* h_sys = nullptr;    // pinned staging
   BState* h_states = nullptr;
   int* h_active = nullptr;
   BParams* h_params = nullptr;
-  // launch shape: threads per CTA and CTAs per cluster (one system per cluster)
-  int threads = 512, cluster = 1;
-  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+  BPlan* h_plan = nullptr;
+  int* h_ctl = nullptr;
+  // launch shape: threads per CTA; gang sizing: a system gets about
+  // gang_boost x (its share of the batch's matrix values) of the CTAs, and a
+  // gang when that is at least 2 (0: every system on one CTA)
+  int threads = 512, gang_boost = 4;
+  int last_ngang = 0, last_gang_ctas = 0;
+  std::map<int, cudaGraphExec_t> graphs;
   long long n_launch = 0, n_h2d = 0, n_d2h = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket the last launch on `stream`
   float last_ms = 0.f;
+  static constexpr int kMaxCtas = 4096;
 };
 
 namespace {
@@ -100,7 +109,7 @@ void pool_free(beta_gpu_batch* b, size_t off, size_t bytes) {
 struct SysLayout {
   size_t total = 0;
   size_t o_xyz, o_conn, o_gp, o_eg, o_rest, o_presc, o_load, o_cptr, o_elems, o_slot, o_nrp, o_ndiag, o_bsoff,
-      o_bcol, o_bval, o_x64, o_r64, o_y64, o_y32, o_r32, o_p32, o_q32, o_minv;
+      o_bcol, o_bval, o_x64, o_r64, o_y64, o_y32, o_r32, o_p32, o_q32, o_minv, o_part, o_gflag;
   size_t add(size_t bytes) {
     const size_t o = total;
     total += (bytes + 255) & ~size_t(255);
@@ -135,6 +144,8 @@ SysLayout layout_for(int ndim, int nnode, int nelem, int nnpe, int ndpn, int ngr
   L.o_p32 = L.add(sizeof(float) * (size_t)nnode * (ndpn == 3 ? 4 : ndpn));
   L.o_q32 = L.add(sizeof(float) * ndof);
   L.o_minv = L.add(sizeof(float) * (size_t)nnode * (ndpn * (ndpn + 1) / 2));
+  L.o_part = L.add(sizeof(double) * 4 * (size_t)P.nslice);
+  L.o_gflag = L.add(16);
   return L;
 }
 
@@ -172,84 +183,122 @@ cudaLaunchConfig_t batch_cfg(beta_gpu_batch* b, int grid, cudaLaunchAttribute* a
   cfg.blockDim = dim3(T, 1, 1);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = b->stream;
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = b->cluster;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
+  attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: gang barriers can complete
+  attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cfg;
 }
 
-// Clusters of the current shape that are resident at once (one full wave).
+// CTAs of the current shape that are resident at once (one full wave).
 template <int T>
-int batch_clusters_raw(beta_gpu_batch* b) {
-  cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = batch_cfg<T>(b, b->cluster, attr);
-  int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k_batch_solve<T>, &cfg) != cudaSuccess) {
+int batch_ctas_raw(beta_gpu_batch* b) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve<T>, T, 0) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  return n;
+  return std::min(per_sm * b->nsm, beta_gpu_batch::kMaxCtas);
 }
 
-int batch_clusters(beta_gpu_batch* b) {
+int batch_ctas(beta_gpu_batch* b) {
   switch (b->threads) {
-    case 256: return batch_clusters_raw<256>(b);
-    case 1024: return batch_clusters_raw<1024>(b);
-    default: return batch_clusters_raw<512>(b);
+    case 256: return batch_ctas_raw<256>(b);
+    case 1024: return batch_ctas_raw<1024>(b);
+    default: return batch_ctas_raw<512>(b);
   }
 }
 
 template <int T>
-cudaError_t batch_launch_raw(beta_gpu_batch* b, int nclusters) {
+cudaError_t batch_launch_raw(beta_gpu_batch* b, int nctas) {
   cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = batch_cfg<T>(b, nclusters * b->cluster, attr);
-  return cudaLaunchKernelEx(&cfg, k_batch_solve<T>, (const BSys*)b->d_sys, (const int*)b->d_active, b->d_counter,
+  cudaLaunchConfig_t cfg = batch_cfg<T>(b, nctas, attr);
+  return cudaLaunchKernelEx(&cfg, k_batch_solve<T>, (const BSys*)b->d_sys, (const int*)b->d_active,
+                            (const BPlan*)b->d_plan, (unsigned*)(b->d_ctl + 2), b->d_ctl, b->d_ctl + 1,
                             (const BParams*)b->d_params);
 }
 
-cudaError_t batch_launch(beta_gpu_batch* b, int nclusters) {
+cudaError_t batch_launch(beta_gpu_batch* b, int nctas) {
   switch (b->threads) {
-    case 256: return batch_launch_raw<256>(b, nclusters);
-    case 1024: return batch_launch_raw<1024>(b, nclusters);
-    default: return batch_launch_raw<512>(b, nclusters);
+    case 256: return batch_launch_raw<256>(b, nctas);
+    case 1024: return batch_launch_raw<1024>(b, nctas);
+    default: return batch_launch_raw<512>(b, nctas);
   }
 }
 
-// One persistent launch over the active list: a graph of (reset work
-// counter, kernel) captured once per launch shape and replayed.  The kernel
-// reads the work list and parameters from fixed device buffers, so the graph
-// stays valid while systems come and go.
+// One persistent launch over the active list: a graph of (zero the work
+// counter, abort flag and gang counters; kernel) captured once per CTA size
+// and replayed.  The kernel reads the plan, work list and parameters from
+// fixed device buffers, so the graph stays valid while systems come and go.
 int batch_launch_graph(beta_gpu_batch* b) {
-  const int ncl = batch_clusters(b);
-  if (ncl < 1) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "no cluster of this launch shape fits on the GPU");
-  auto key = std::make_pair(b->threads, b->cluster);
-  auto it = b->graphs.find(key);
+  const int nctas = batch_ctas(b);
+  if (nctas < 1) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "no CTA of this launch shape fits on the GPU");
+  const size_t ctl_bytes = sizeof(int) * (2 + (size_t)nctas);
+  auto it = b->graphs.find(b->threads);
   if (it == b->graphs.end()) {
     cudaGraph_t g = nullptr;
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream);
-    cudaError_t e2 = batch_launch(b, ncl);
+    cudaError_t e1 = cudaMemsetAsync(b->d_ctl, 0, ctl_bytes, b->stream);
+    cudaError_t e2 = batch_launch(b, nctas);
     cudaError_t e3 = cudaStreamEndCapture(b->stream, &g);
-    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
-      cudaGetLastError();
-      if (g) cudaGraphDestroy(g);
-      return bfail(b, BETA_GPU_ERR_CUDA, "capturing the batch launch failed");
-    }
     cudaGraphExec_t ge = nullptr;
-    cudaError_t e4 = cudaGraphInstantiate(&ge, g, 0);
-    cudaGraphDestroy(g);
+    cudaError_t e4 = cudaErrorUnknown;
+    if (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess) e4 = cudaGraphInstantiate(&ge, g, 0);
+    if (g) cudaGraphDestroy(g);
     if (e4 != cudaSuccess) {
+      // a cooperative launch that cannot be captured still runs directly
       cudaGetLastError();
-      return bfail(b, BETA_GPU_ERR_CUDA, "instantiating the batch graph failed");
+      BCK(cudaMemsetAsync(b->d_ctl, 0, ctl_bytes, b->stream));
+      BCK(batch_launch(b, nctas));
+      b->n_launch += 1;
+      return BETA_GPU_OK;
     }
-    it = b->graphs.emplace(key, ge).first;
+    it = b->graphs.emplace(b->threads, ge).first;
   }
   BCK(cudaGraphLaunch(it->second, b->stream));
   b->n_launch += 1;
   return BETA_GPU_OK;
+}
+
+// Gang plan for the active list act[0..na) (sorted by matrix values, largest
+// first).  With N resident CTAs and W values in all, a system of w values
+// wants g = floor(gang_boost * w * N / W) CTAs, capped so every warp keeps at
+// least two 32-node slices; g >= 2 makes it a gang.  When the gangs want more
+// than N CTAs they shrink in proportion (to at least 2 each) and the smallest
+// are demoted to single-CTA systems until they fit.  CTAs outside the gangs
+// start on the small systems at once; a gang joins them when its system is
+// done.  Returns the number of gangs; they solve act[0..ngang).
+int batch_plan(beta_gpu_batch* b, const int* act, int na, int nctas) {
+  const int warps = b->threads / 32;
+  double W = 0.0;
+  for (int i = 0; i < na; ++i) W += (double)b->sys[act[i]].work;
+  auto want = [&](int i) {
+    const auto& S = b->sys[act[i]];
+    const int cap = std::max(1, S.nslice / (2 * warps));
+    return std::min(cap, (int)std::min<double>(nctas, std::floor(b->gang_boost * (double)S.work * nctas / W)));
+  };
+  int ngang = 0;
+  if (b->gang_boost > 0 && W > 0)
+    while (ngang < na && ngang < nctas / 2 && want(ngang) >= 2) ++ngang;  // sorted: later systems want less
+  std::vector<int> g;
+  for (; ngang > 0; --ngang) {
+    g.assign(ngang, 0);
+    long long want_sum = 0;
+    for (int i = 0; i < ngang; ++i) want_sum += (g[i] = want(i));
+    long long sum = want_sum;
+    if (want_sum > nctas) {
+      sum = 0;
+      for (int i = 0; i < ngang; ++i) sum += (g[i] = std::max(2, (int)((long long)g[i] * nctas / want_sum)));
+    }
+    if (sum <= nctas) break;
+  }
+  int c = 0;
+  for (int i = 0; i < ngang; ++i)
+    for (int r = 0; r < g[i]; ++r, ++c) b->h_plan[c] = BPlan{i, r, g[i], i};
+  b->last_gang_ctas = c;
+  for (; c < nctas; ++c) b->h_plan[c] = BPlan{-1, 0, 1, 0};
+  b->last_ngang = ngang;
+  return ngang;
 }
 
 // Uploads descriptors of live systems, the active list (unfinished, largest
@@ -263,6 +312,9 @@ int batch_prepare(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, i
   for (auto& w : order) b->h_active[na++] = w.second;
   for (int i = 0; i < (int)b->sys.size(); ++i)
     if (b->sys[i].live) b->h_sys[i] = b->sys[i].desc;
+  const int nctas = batch_ctas(b);
+  if (nctas < 1) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "no CTA of this launch shape fits on the GPU");
+  const int ngang = batch_plan(b, b->h_active, na, nctas);
   BParams& P = *b->h_params;
   P.tol = o->tol > 0 ? o->tol : 1e-10;
   P.delta = (o->inner_tol > 0 && o->inner_tol < 1) ? o->inner_tol : 0.01;
@@ -270,22 +322,28 @@ int batch_prepare(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, i
   P.max_repl = o->max_outer > 0 ? o->max_outer : 60;
   P.budget = budget;
   P.nactive = na;
+  P.nbig = ngang;
+  P.spin_ns = 2000000000LL;  // 2 s at one barrier: far beyond any phase of a resident gang
   int rc;
   if (!b->sys.empty() && (rc = batch_h2d(b, b->d_sys, b->h_sys, sizeof(BSys) * b->sys.size()))) return rc;
   if ((rc = batch_h2d(b, b->d_active, b->h_active, sizeof(int) * std::max(1, na)))) return rc;
+  if ((rc = batch_h2d(b, b->d_plan, b->h_plan, sizeof(BPlan) * nctas))) return rc;
   if ((rc = batch_h2d(b, b->d_params, b->h_params, sizeof(BParams)))) return rc;
   *nactive = na;
   return BETA_GPU_OK;
 }
 
+// Reads back every system's state and the launch's abort flag; a launch that
+// gave up at a gang barrier returns BETA_GPU_TIMEOUT.
 int batch_pull_states(beta_gpu_batch* b) {
   const size_t n = b->sys.size();
-  if (!n) return BETA_GPU_OK;
-  b->n_d2h += (long long)(sizeof(BState) * n);
-  BCK(cudaMemcpyAsync(b->h_states, b->d_states, sizeof(BState) * n, cudaMemcpyDeviceToHost, b->stream));
+  b->n_d2h += (long long)(sizeof(BState) * n + 2 * sizeof(int));
+  if (n) BCK(cudaMemcpyAsync(b->h_states, b->d_states, sizeof(BState) * n, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   for (size_t i = 0; i < n; ++i)
     if (b->sys[i].live) b->sys[i].st = b->h_states[i];
+  if (b->h_ctl[1]) return bfail(b, BETA_GPU_TIMEOUT, "a gang barrier waited past its limit; the launch stopped");
   return BETA_GPU_OK;
 }
 

@@ -1,23 +1,33 @@
 // batch_kernels.cuh -- many independent systems in one persistent launch.
 //
-// Each thread-block cluster (1, 2, 4 or 8 CTAs, chosen at launch) takes whole
-// systems off a device work list (largest first, one atomicAdd per system)
-// and runs, for that system alone: FP32 assembly (colour by colour),
-// block-Jacobi factors, the FP64 right-hand-side norm, and reliable-update
-// mixed-precision PCG (FP32 node-block SpMV + FP64 matrix-free residual
-// replacement).  The only barriers are the cluster's own hardware barrier
-// (cluster.sync, which covers the CTA barrier); reductions go through
-// distributed shared memory in fixed rank order, so every thread of the
-// cluster sees bit-identical sums and takes the same branches.  Clusters never
-// wait on each other.  An iteration budget per
-// launch lets a serving loop preempt systems between launches: the full
-// Krylov state stays in the system's own device memory.
+// One cooperative launch, one CTA per SM.  The host splits the CTAs into
+// gangs for the big systems (a gang of g CTAs solves one system, g chosen in
+// proportion to the system's share of the batch) and leaves the rest as
+// single CTAs that pull the small systems off a device work list (largest
+// first, one atomicAdd per system).  A gang's CTAs meet at a software barrier
+// (one arrival counter per gang in global memory, release/acquire at GPU
+// scope, a bounded wait); a single CTA only uses __syncthreads.  When its big
+// system is done, a gang breaks up and its CTAs pull small systems too.
 //
-// The per-warp element and matrix-free bodies are the ones the single-system
-// kernels use (elem_kernels.cuh, mf_kernels.cuh).
+// For a system the group (gang or CTA) runs: FP32 assembly (colour by
+// colour), block-Jacobi factors, the FP64 right-hand-side norm, and
+// reliable-update mixed-precision PCG (FP32 node-block SpMV + FP64
+// matrix-free residual replacement), for at most `budget` iterations per
+// launch (the serving loop's preemption: the Krylov state stays in the
+// system's own device memory).
+//
+// Every sum has one fixed order, whatever the group's size or the CTA's
+// thread count: lanes of a 32-node slice are combined by a warp butterfly and
+// written as that slice's partial; after the barrier every CTA adds the
+// partials in slice order through 256 fixed strided accumulators and a fixed
+// tree.  Element scatters are colour-exclusive, rows of the SpMV are summed in
+// storage order, the rest is element-wise.  So a system's iterates are
+// bit-identical whether it is solved alone, in any mix, by a gang of any size
+// or by one CTA.
+//
+// Data that other CTAs write during the launch is never read through the
+// read-only (non-coherent) cache path.
 #pragma once
-#include <cooperative_groups.h>
-
 #include "common.cuh"
 #include "elem_kernels.cuh"
 #include "mf_kernels.cuh"
@@ -26,7 +36,7 @@
 namespace betagpu {
 
 enum : int { kPhaseNew = 0, kPhaseIter = 1, kPhaseDone = 2 };
-enum : int { kBConverged = 0, kBRunning = 1, kBMaxit = 4, kBBreakdown = 5, kBNegDiag = 6 };
+enum : int { kBConverged = 0, kBRunning = 1, kBMaxit = 4, kBBreakdown = 5, kBNegDiag = 6, kBAborted = 10 };
 
 struct BState {
   double rho, rr, maxrr, bn, rn;
@@ -59,6 +69,8 @@ struct BSys {
   float* p32;
   float* q32;
   float* minv;
+  double* part;     // 2 buffers x 2 values x nslice slice partials
+  unsigned* gflag;  // assembly status bits of this system
   const GaussTable* gt;
   BState* st;
   long long nchunk;
@@ -67,41 +79,120 @@ struct BSys {
 struct BParams {
   double tol, delta;
   int maxit, max_repl, budget;  // budget: iterations per system per launch (0: no limit)
-  int nactive;
+  int nactive, nbig;            // active[0, nbig) are solved by gangs, the rest by single CTAs
+  long long spin_ns;            // longest wait at a gang barrier before the launch gives up
 };
 
-namespace cg = cooperative_groups;
+// Per CTA: the gang it belongs to for this launch.
+struct BPlan {
+  int k;     // index into active[] of the gang's system, -1: no gang (single CTA from the start)
+  int rank;  // rank of this CTA in the gang
+  int size;  // CTAs in the gang
+  int bar;   // index of the gang's arrival counter
+};
 
-// Cluster-wide sum of NV doubles (NV <= 4); every thread of the cluster gets
-// the same totals: per-CTA sums in fixed warp order, then the CTAs' sums read
-// through distributed shared memory in rank order.
-template <int NV>
-__device__ __forceinline__ void cl_sum(double (&v)[NV], double* sh, double* shtot) {
-  cg::cluster_group cl = cg::this_cluster();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int k = 0; k < NV; ++k) {
-    double t = warp_sum(v[k]);
-    if (lane == 0) sh[k * 32 + wid] = t;
+struct GangShared {
+  unsigned bar_no;
+  int abort;
+  int idx;
+  double wred[2][8];
+  double red[2];
+};
+
+__device__ __forceinline__ long long globaltimer_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The CTAs working on one system: a gang (ctr != nullptr) or this CTA alone.
+struct Grp {
+  int rank, size;
+  unsigned* ctr;
+  GangShared* gs;
+  int* gabort;
+  long long spin_ns;
+};
+
+// Barrier of the group.  Returns false once the launch is aborting (a wait
+// ran past spin_ns here or in another gang); the caller then stops.
+__device__ __forceinline__ bool gsync(const Grp& g) {
+  __syncthreads();
+  if (g.ctr == nullptr) return true;
+  if (threadIdx.x == 0) {
+    __threadfence();  // release this CTA's writes
+    const unsigned target = (++g.gs->bar_no) * (unsigned)g.size;
+    atomicAdd(g.ctr, 1u);
+    const long long t0 = globaltimer_ns();
+    unsigned polls = 0;
+    while (ld_acquire_u32(g.ctr) < target) {
+      if ((++polls & 63u) == 0u) {
+        if (*(volatile int*)g.gabort) { g.gs->abort = 1; break; }
+        if (globaltimer_ns() - t0 > g.spin_ns) {
+          g.gs->abort = 1;
+          atomicExch(g.gabort, 1);
+          break;
+        }
+      }
+      __nanosleep(64);
+    }
+    __threadfence();  // acquire the other CTAs' writes
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      double t = 0.0;
-      for (int i = 0; i < nw; ++i) t += sh[k * 32 + i];
-      shtot[k] = t;
-    }
-  }
-  cl.sync();
-  const int C = (int)cl.num_blocks();
+  return g.gs->abort == 0;
+}
+
+// Stage 1 of a fixed-order sum: the warp that owns slice s adds its 32 lane
+// values (butterfly) and lane 0 stores the slice partial.
+template <int NV>
+__device__ __forceinline__ void slice_partial(double* part, int nsl, int s, const double (&v)[NV]) {
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
-    double t = 0.0;
-    for (int r = 0; r < C; ++r) t += cl.map_shared_rank(shtot, r)[k];
-    v[k] = t;
+    const double t = warp_sum(v[k]);
+    if ((threadIdx.x & 31) == 0) part[(long long)k * nsl + s] = t;
   }
-  cl.sync();
+}
+
+// Stage 2: barrier, then every CTA adds the nsl slice partials of each value
+// in the same order (256 strided accumulators, warp butterflies, warps 0..7 in
+// order); all threads of the group get bit-identical totals.
+template <int NV>
+__device__ __forceinline__ bool group_sum(const Grp& g, const double* part, int nsl, double (&out)[NV]) {
+  if (!gsync(g)) return false;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  if (t < 256) {
+    double a[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) a[k] = 0.0;
+    for (int i = t; i < nsl; i += 256) {
+#pragma unroll
+      for (int k = 0; k < NV; ++k) a[k] += __ldcg(part + (long long)k * nsl + i);
+    }
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      a[k] = warp_sum(a[k]);
+      if (lane == 0) g.gs->wred[k][w] = a[k];
+    }
+  }
+  __syncthreads();
+  if (t == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double s = 0.0;
+      for (int i = 0; i < 8; ++i) s += g.gs->wred[k][i];
+      g.gs->red[k] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) out[k] = g.gs->red[k];
+  return true;
 }
 
 template <typename T>
@@ -115,15 +206,13 @@ __device__ __forceinline__ void b_stage(const GaussTable* gt, int nip, int nn, i
 }
 
 // y = K x for one system (FP64, matrix-free), colour by colour.
-__device__ void b_mf(const BSys& S, const MfArgs& M, const double* x, double* y, const double* s_dN,
-                     const double* s_N, const double* s_w) {
-  cg::cluster_group cl = cg::this_cluster();
-  const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
-  const int gt = rank * blockDim.x + threadIdx.x, gn = C * blockDim.x;
+__device__ bool b_mf(const BSys& S, const MfArgs& M, const double* x, double* y, const double* s_dN,
+                     const double* s_N, const double* s_w, const Grp& g) {
+  const int gt = g.rank * blockDim.x + threadIdx.x, gn = g.size * blockDim.x;
   for (int i = gt; i < S.ndof; i += gn) y[i] = 0.0;
-  cl.sync();
+  if (!gsync(g)) return false;
   const int nw = blockDim.x >> 5;
-  const int wid = rank * nw + (threadIdx.x >> 5), gw = C * nw;
+  const int wid = g.rank * nw + (threadIdx.x >> 5), gw = g.size * nw;
   for (int c = 0; c < S.ncolor; ++c) {
     const int beg = S.color_ptr[c], nel = S.color_ptr[c + 1] - beg;
     const int* el = S.elems + beg;
@@ -134,38 +223,95 @@ __device__ void b_mf(const BSys& S, const MfArgs& M, const double* x, double* y,
     } else {
       for (int w = wid; 8 * w < nel; w += gw) mf_quad4_pstress_warp(M, el, nel, w, x, nullptr, y, s_dN, s_w);
     }
-    cl.sync();
+    if (!gsync(g)) return false;
   }
+  return true;
+}
+
+// Residual b - K x on free dofs (0 on restrained ones) into r64 and r32, and
+// its squared norm (fixed order); with bb also ||b||^2, b = the prescribed
+// value on restrained dofs.  y64 holds K x.
+template <int ND>
+__device__ __forceinline__ bool b_residual(const BSys& S, const Grp& g, double* part, double (&out)[2], bool bb) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int wid = g.rank * nw + (threadIdx.x >> 5), gw = g.size * nw;
+  for (int s = wid; s < S.nslice; s += gw) {
+    double v[2] = {0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+      const long long i = 32LL * ND * s + 32 * k + lane;
+      if (i < S.ndof) {
+        const double r = S.rest[i] ? 0.0 : (S.load ? S.load[i] : 0.0) - S.y64[i];
+        S.r64[i] = r;
+        S.r32[i] = (float)r;
+        v[0] += r * r;
+        if (bb) {
+          const double b = S.rest[i] ? S.presc[i] : r;
+          v[1] += b * b;
+        }
+      }
+    }
+    slice_partial<2>(part, S.nslice, s, v);
+  }
+  return group_sum<2>(g, part, S.nslice, out);
+}
+
+// (r.z, r.r) with z = M r, optionally storing p = z (start of a cycle).
+template <int ND>
+__device__ __forceinline__ bool b_rz(const BSys& S, const Grp& g, double* part, double (&out)[2], bool set_p) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int wid = g.rank * nw + (threadIdx.x >> 5), gw = g.size * nw;
+  for (int s = wid; s < S.nslice; s += gw) {
+    const int I = 32 * s + lane;
+    double v[2] = {0.0, 0.0};
+    if (I < S.nnode) {
+      float rv[ND], z[ND];
+      NodeIO<ND>::ld(S.r32, I, rv);
+      NodeIO<ND>::prec(S.minv, I, rv, z);
+      if (set_p) PVec<ND>::st(S.p32, I, z);
+#pragma unroll
+      for (int i = 0; i < ND; ++i) { v[0] += (double)rv[i] * z[i]; v[1] += (double)rv[i] * rv[i]; }
+    }
+    slice_partial<2>(part, S.nslice, s, v);
+  }
+  return group_sum<2>(g, part, S.nslice, out);
 }
 
 template <int ND>
-__device__ void b_solve(const BSys& S, const BParams& P, double* sh, double* shtot, const double* s_dN,
-                        const double* s_N, const double* s_w, const float* s_dNf, const float* s_Nf,
-                        const float* s_wf, unsigned* s_flag) {
+__device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const double* s_dN, const double* s_N,
+                        const double* s_w, const float* s_dNf, const float* s_Nf, const float* s_wf) {
   constexpr int SM = ND * (ND + 1) / 2;
-  cg::cluster_group cl = cg::this_cluster();
-  const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
-  // cluster-global thread and warp indices
-  const int tid = rank * blockDim.x + threadIdx.x, nt = C * blockDim.x;
-  const int lane = threadIdx.x & 31, wid = rank * (blockDim.x >> 5) + (threadIdx.x >> 5), nw = C * (blockDim.x >> 5);
+  const int tid = g.rank * blockDim.x + threadIdx.x, nt = g.size * blockDim.x;
+  const int lane = threadIdx.x & 31, nwc = blockDim.x >> 5;
+  const int wid = g.rank * nwc + (threadIdx.x >> 5), nw = g.size * nwc;
+  const int nsl = S.nslice;
+  double* const partA = S.part;
+  double* const partB = S.part + 2LL * nsl;
+  // Partial buffers alternate: a buffer is rewritten only after the next
+  // sum's barrier, by which time every CTA has read it.
+  int pb = 0;
+  auto part = [&]() { pb ^= 1; return pb ? partA : partB; };
   BState st = *S.st;
   MfArgs M;
   M.xyz = S.xyz; M.conn = S.conn; M.gparams = S.gparams; M.egroup = S.egroup; M.nparams = S.nparams;
   M.nip = S.nip; M.gt = S.gt; M.c1 = 1.0; M.c2 = 0.0; M.cm = 0.0;
   const int n = S.ndof, nn = S.nnode;
   BlockMat A{S.nnode, S.nslice, S.bsoff, S.bcol, S.bval};
+  auto aborted = [&]() {
+    if (tid == 0) { st.status = kBAborted; *S.st = st; }
+  };
 
   if (st.phase == kPhaseNew) {
     // ---- FP32 assembly: zero, colour by colour, unit restrained diagonals
     const long long nv = S.nchunk * 32LL * ND * ND;
     for (long long i = tid; i < nv; i += nt) S.bval[i] = 0.f;
-    if (threadIdx.x == 0) *s_flag = 0u;
-    cl.sync();
+    if (tid == 0) *S.gflag = 0u;
+    if (!gsync(g)) return aborted();
     ElemArgs E;
     E.xyz = S.xyz; E.conn = S.conn; E.gparams = S.gparams; E.egroup = S.egroup; E.nparams = S.nparams;
     E.nip = S.nip; E.gt = S.gt; E.slot = S.slot; E.nrp = S.nrp; E.rest = S.rest; E.presc = S.presc;
     E.bsoff = S.bsoff; E.bval = S.bval; E.soff = nullptr; E.ssoff = nullptr; E.sval = nullptr; E.pseudo = nullptr;
-    E.kscale = 1.0; E.mscale = 0.0; E.flags = s_flag;
+    E.kscale = 1.0; E.mscale = 0.0; E.flags = S.gflag;
     for (int c = 0; c < S.ncolor; ++c) {
       const int beg = S.color_ptr[c], nel = S.color_ptr[c + 1] - beg;
       const int* el = S.elems + beg;
@@ -176,18 +322,17 @@ __device__ void b_solve(const BSys& S, const BParams& P, double* sh, double* sht
       } else {
         for (int w = wid; 2 * w < nel; w += nw) asm_quad4_pstress_warp<float>(E, el, nel, w, s_dNf, s_Nf, s_wf);
       }
-      cl.sync();
+      if (!gsync(g)) return aborted();
     }
     for (int I = tid; I < nn; I += nt) {
       const long long chunk = (long long)S.bsoff[I >> 5] + S.ndiag[I];
       for (int i = 0; i < ND; ++i)
         if (S.rest[I * ND + i]) S.bval[chunk * (32 * ND * ND) + (i * ND + i) * 32 + (I & 31)] = 1.0f;
     }
-    double fneg[1] = {threadIdx.x == 0 && (*s_flag & kFlagNegDiag) ? 1.0 : 0.0};
-    cl_sum<1>(fneg, sh, shtot);  // also the barrier after the diagonal fix-up
-    if (fneg[0] > 0.0) {
+    if (!gsync(g)) return aborted();
+    if (ld_acquire_u32(S.gflag) & kFlagNegDiag) {
       if (tid == 0) { st.phase = kPhaseDone; st.status = kBNegDiag; *S.st = st; }
-      cl.sync();
+      gsync(g);
       return;
     }
     // ---- block-Jacobi factors (FP64 inverse of the node diagonal block)
@@ -207,30 +352,17 @@ __device__ void b_solve(const BSys& S, const BParams& P, double* sh, double* sht
         for (int j = i; j < ND; ++j) S.minv[(long long)SM * I + (t++)] = (float)(0.5 * (Di[i * ND + j] + Di[j * ND + i]));
     }
     // ---- x = prescribed on restrained dofs, 0 elsewhere; r = b = load - K x (free rows)
-    for (int i = tid; i < n; i += nt) S.x64[i] = S.rest[i] ? S.presc[i] : 0.0;
-    cl.sync();
-    b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w);
-    double acc[1] = {0.0};
     for (int i = tid; i < n; i += nt) {
-      const double r = S.rest[i] ? 0.0 : (S.load ? S.load[i] : 0.0) - S.y64[i];
-      S.r64[i] = r;
-      const double bb = S.rest[i] ? S.presc[i] : r;
-      acc[0] += bb * bb;
-      S.r32[i] = (float)r;
+      S.x64[i] = S.rest[i] ? S.presc[i] : 0.0;
       S.y32[i] = 0.f;
     }
-    cl_sum<1>(acc, sh, shtot);
-    st.bn = sqrt(acc[0]);
-    double a2[2] = {0.0, 0.0};
-    for (int I = tid; I < nn; I += nt) {
-      float rv[ND], z[ND];
-      NodeIO<ND>::ld(S.r32, I, rv);
-      NodeIO<ND>::prec(S.minv, I, rv, z);
-      PVec<ND>::st(S.p32, I, z);
-#pragma unroll
-      for (int i = 0; i < ND; ++i) { a2[0] += (double)rv[i] * z[i]; a2[1] += (double)rv[i] * rv[i]; }
-    }
-    cl_sum<2>(a2, sh, shtot);
+    if (!gsync(g)) return aborted();
+    if (!b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w, g)) return aborted();
+    double a0[2];
+    if (!b_residual<ND>(S, g, part(), a0, true)) return aborted();
+    st.bn = sqrt(a0[1]);
+    double a2[2];
+    if (!b_rz<ND>(S, g, part(), a2, true)) return aborted();
     st.rho = a2[0];
     st.rr = st.maxrr = a2[1];
     st.iter = 0;
@@ -245,12 +377,13 @@ __device__ void b_solve(const BSys& S, const BParams& P, double* sh, double* sht
   const double delta2 = P.delta * P.delta;
   int spent = 0;
   while (st.phase == kPhaseIter && (P.budget <= 0 || spent < P.budget)) {
-    // q = A p, p.q
-    double a1[1] = {0.0};
-    for (int s = wid; s < S.nslice; s += nw) {
+    // q = A p, p.q  (one warp per 32-node slice)
+    double* pq = part();
+    for (int s = wid; s < nsl; s += nw) {
       float acc[ND];
-      spmv_row_b<ND, true>(A, s, lane, S.p32, acc);
+      spmv_row_b<ND, true, false>(A, s, lane, S.p32, acc);
       const int I = s * 32 + lane;
+      double v[1] = {0.0};
       if (I < nn) {
         NodeIO<ND>::st(S.q32, I, acc);
         float pv[ND];
@@ -258,32 +391,40 @@ __device__ void b_solve(const BSys& S, const BParams& P, double* sh, double* sht
         float t = 0.f;
 #pragma unroll
         for (int i = 0; i < ND; ++i) t = fmaf(pv[i], acc[i], t);
-        a1[0] += (double)t;
+        v[0] = (double)t;
       }
+      slice_partial<1>(pq, nsl, s, v);
     }
-    cl_sum<1>(a1, sh, shtot);
+    double a1[1];
+    if (!group_sum<1>(g, pq, nsl, a1)) return aborted();
     if (!(a1[0] > 0.0 && a1[0] < 1e308)) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
     const float alpha = (float)(st.rho / a1[0]);
     // y += alpha p, r -= alpha q, (r.z, r.r)
-    double a2[2] = {0.0, 0.0};
-    for (int I = tid; I < nn; I += nt) {
-      float yv[ND], rv[ND], pv[ND], qv[ND], z[ND];
-      NodeIO<ND>::ld(S.y32, I, yv);
-      NodeIO<ND>::ld(S.r32, I, rv);
-      PVec<ND>::ld(S.p32, I, pv);
-      NodeIO<ND>::ld(S.q32, I, qv);
+    double* rz = part();
+    for (int s = wid; s < nsl; s += nw) {
+      const int I = 32 * s + lane;
+      double v[2] = {0.0, 0.0};
+      if (I < nn) {
+        float yv[ND], rv[ND], pv[ND], qv[ND], z[ND];
+        NodeIO<ND>::ld(S.y32, I, yv);
+        NodeIO<ND>::ld(S.r32, I, rv);
+        PVec<ND>::ld(S.p32, I, pv);
+        NodeIO<ND>::ld(S.q32, I, qv);
 #pragma unroll
-      for (int i = 0; i < ND; ++i) {
-        yv[i] = fmaf(alpha, pv[i], yv[i]);
-        rv[i] = fmaf(-alpha, qv[i], rv[i]);
+        for (int i = 0; i < ND; ++i) {
+          yv[i] = fmaf(alpha, pv[i], yv[i]);
+          rv[i] = fmaf(-alpha, qv[i], rv[i]);
+        }
+        NodeIO<ND>::st(S.y32, I, yv);
+        NodeIO<ND>::st(S.r32, I, rv);
+        NodeIO<ND>::prec(S.minv, I, rv, z);
+#pragma unroll
+        for (int i = 0; i < ND; ++i) { v[0] += (double)rv[i] * z[i]; v[1] += (double)rv[i] * rv[i]; }
       }
-      NodeIO<ND>::st(S.y32, I, yv);
-      NodeIO<ND>::st(S.r32, I, rv);
-      NodeIO<ND>::prec(S.minv, I, rv, z);
-#pragma unroll
-      for (int i = 0; i < ND; ++i) { a2[0] += (double)rv[i] * z[i]; a2[1] += (double)rv[i] * rv[i]; }
+      slice_partial<2>(rz, nsl, s, v);
     }
-    cl_sum<2>(a2, sh, shtot);
+    double a2[2];
+    if (!group_sum<2>(g, rz, nsl, a2)) return aborted();
     st.iter += 1;
     ++spent;
     if (!(a2[0] == a2[0])) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
@@ -292,30 +433,17 @@ __device__ void b_solve(const BSys& S, const BParams& P, double* sh, double* sht
     if (a2[1] < tolabs2 || a2[1] < delta2 * st.maxrr || st.iter >= P.maxit) {
       // reliable update: fold y into x, replace r by the FP64 true residual
       for (int i = tid; i < n; i += nt) { S.x64[i] += (double)S.y32[i]; S.y32[i] = 0.f; }
-      cl.sync();
-      b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w);
-      double a3[1] = {0.0};
-      for (int i = tid; i < n; i += nt) {
-        const double r = S.rest[i] ? 0.0 : (S.load ? S.load[i] : 0.0) - S.y64[i];
-        S.r64[i] = r;
-        S.r32[i] = (float)r;
-        a3[0] += r * r;
-      }
-      cl_sum<1>(a3, sh, shtot);
+      if (!gsync(g)) return aborted();
+      if (!b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w, g)) return aborted();
+      double a3[2];
+      if (!b_residual<ND>(S, g, part(), a3, false)) return aborted();
       st.rn = sqrt(a3[0]);
       st.repl += 1;
       if (!(st.rn == st.rn)) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
       if (st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; break; }
       if (st.iter >= P.maxit || st.repl > P.max_repl) { st.phase = kPhaseDone; st.status = kBMaxit; break; }
-      double a4[2] = {0.0, 0.0};
-      for (int I = tid; I < nn; I += nt) {
-        float rv[ND], z[ND];
-        NodeIO<ND>::ld(S.r32, I, rv);
-        NodeIO<ND>::prec(S.minv, I, rv, z);
-#pragma unroll
-        for (int i = 0; i < ND; ++i) { a4[0] += (double)rv[i] * z[i]; a4[1] += (double)rv[i] * rv[i]; }
-      }
-      cl_sum<2>(a4, sh, shtot);
+      double a4[2];
+      if (!b_rz<ND>(S, g, part(), a4, false)) return aborted();
       beta = st.rho != 0.0 ? a4[0] / st.rho : 0.0;
       st.rho = a4[0];
       st.rr = st.maxrr = a4[1];
@@ -335,40 +463,51 @@ __device__ void b_solve(const BSys& S, const BParams& P, double* sh, double* sht
       for (int i = 0; i < ND; ++i) pv[i] = fmaf(bt, pv[i], z[i]);
       PVec<ND>::st(S.p32, I, pv);
     }
-    cl.sync();
+    if (!gsync(g)) return aborted();
   }
-  cl.sync();
   if (tid == 0) *S.st = st;
-  cl.sync();
+  gsync(g);
 }
 
-// The persistent batch kernel: clusters pull systems from active[] until
-// empty.  Launched with a cluster dimension of 1, 2, 4 or 8 CTAs.
+// The persistent batch kernel (cooperative launch: all CTAs resident).  CTAs
+// of a gang first solve their big system together; then every CTA pulls
+// small systems active[nbig..nactive) off the work counter on its own.
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restrict__ sys, const int* __restrict__ active,
-                                                            int* counter, const BParams* __restrict__ prm) {
-  __shared__ double sh[64];
-  __shared__ double shtot[4];
+                                                            const BPlan* __restrict__ plan, unsigned* bar, int* counter,
+                                                            int* gabort, const BParams* __restrict__ prm) {
+  __shared__ GangShared gs;
   __shared__ double s_dN[kMaxIP * 24], s_N[kMaxIP * 8], s_w[kMaxIP];
   __shared__ float s_dNf[kMaxIP * 24], s_Nf[kMaxIP * 8], s_wf[kMaxIP];
-  __shared__ int s_idx;
-  __shared__ unsigned s_flag;
-  cg::cluster_group cl = cg::this_cluster();
   const BParams P = *prm;
-  for (;;) {
-    if (cl.block_rank() == 0 && threadIdx.x == 0) s_idx = atomicAdd(counter, 1);
-    cl.sync();
-    const int k = *cl.map_shared_rank(&s_idx, 0);
-    cl.sync();  // rank 0 may overwrite s_idx only after every CTA has read it
-    if (k >= P.nactive) break;  // the same k in every CTA of the cluster
-    const BSys S = sys[active[k]];
+  const BPlan pl = plan[blockIdx.x];
+  if (threadIdx.x == 0) {
+    gs.bar_no = 0;
+    gs.abort = 0;
+  }
+  __syncthreads();
+  auto solve = [&](const BSys& S, const Grp& g) {
     const int nn = S.kind == 1 ? 4 : 8, ndir = S.kind == 1 ? 2 : 3;
     b_stage<double>(S.gt, S.nip, nn, ndir, s_dN, s_N, s_w);
     b_stage<float>(S.gt, S.nip, nn, ndir, s_dNf, s_Nf, s_wf);
     __syncthreads();
-    if (S.ndpn == 3) b_solve<3>(S, P, sh, shtot, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf, &s_flag);
-    else if (S.ndpn == 2) b_solve<2>(S, P, sh, shtot, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf, &s_flag);
-    else b_solve<1>(S, P, sh, shtot, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf, &s_flag);
+    if (S.ndpn == 3) b_solve<3>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf);
+    else if (S.ndpn == 2) b_solve<2>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf);
+    else b_solve<1>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf);
+  };
+  if (pl.k >= 0 && pl.k < P.nbig) {
+    const Grp gang{pl.rank, pl.size, bar + pl.bar, &gs, gabort, P.spin_ns};
+    solve(sys[active[pl.k]], gang);
+    if (gs.abort) return;
+  }
+  const Grp alone{0, 1, nullptr, &gs, gabort, P.spin_ns};
+  for (;;) {
+    if (threadIdx.x == 0) gs.idx = *(volatile int*)gabort ? P.nactive : P.nbig + atomicAdd(counter, 1);
+    __syncthreads();
+    const int k = gs.idx;
+    __syncthreads();  // gs.idx is rewritten only after every thread has read it
+    if (k >= P.nactive) return;
+    solve(sys[active[k]], alone);
   }
 }
 

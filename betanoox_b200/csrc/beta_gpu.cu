@@ -744,6 +744,7 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   S.kind = Q.kind; S.ndim = Q.ndim; S.nnode = Q.nnode; S.nelem = Q.nelem; S.nnpe = Q.nnpe; S.ndpn = Q.ndpn;
   S.ndof = (int)ndof; S.order = Q.order; S.off = (size_t)off; S.bytes = L.total;
   S.work = (long long)P.nchunk * 32 * Q.ndpn * Q.ndpn;
+  S.nslice = P.nslice;
   BSys& D = S.desc;
   std::memset(&D, 0, sizeof(D));
   GaussTable hg;
@@ -773,6 +774,8 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   D.p32 = (float*)(base + L.o_p32);
   D.q32 = (float*)(base + L.o_q32);
   D.minv = (float*)(base + L.o_minv);
+  D.part = (double*)(base + L.o_part);
+  D.gflag = (unsigned*)(base + L.o_gflag);
   D.gt = gt;
   D.st = b->d_states + id;
   D.nchunk = P.nchunk;
@@ -1492,8 +1495,11 @@ int beta_gpu_batch_create(beta_gpu_batch** out, int device, long long budget, in
   BCK(cudaMalloc(&b->d_sys, sizeof(BSys) * max_systems));
   BCK(cudaMalloc(&b->d_states, sizeof(BState) * max_systems));
   BCK(cudaMalloc(&b->d_active, sizeof(int) * max_systems));
-  BCK(cudaMalloc(&b->d_counter, sizeof(int)));
   BCK(cudaMalloc(&b->d_params, sizeof(BParams)));
+  BCK(cudaMalloc(&b->d_plan, sizeof(BPlan) * beta_gpu_batch::kMaxCtas));
+  BCK(cudaMalloc(&b->d_ctl, sizeof(int) * (2 + beta_gpu_batch::kMaxCtas)));
+  BCK(cudaMallocHost(&b->h_plan, sizeof(BPlan) * beta_gpu_batch::kMaxCtas));
+  BCK(cudaMallocHost(&b->h_ctl, sizeof(int) * 2));
   BCK(cudaMallocHost(&b->h_sys, sizeof(BSys) * max_systems));
   BCK(cudaMallocHost(&b->h_states, sizeof(BState) * max_systems));
   BCK(cudaMallocHost(&b->h_active, sizeof(int) * max_systems));
@@ -1512,8 +1518,11 @@ int beta_gpu_batch_destroy(beta_gpu_batch* b) {
   cudaFree(b->d_sys);
   cudaFree(b->d_states);
   cudaFree(b->d_active);
-  cudaFree(b->d_counter);
   cudaFree(b->d_params);
+  cudaFree(b->d_plan);
+  cudaFree(b->d_ctl);
+  cudaFreeHost(b->h_plan);
+  cudaFreeHost(b->h_ctl);
   cudaFreeHost(b->h_sys);
   cudaFreeHost(b->h_states);
   cudaFreeHost(b->h_active);
@@ -1636,29 +1645,29 @@ int beta_gpu_batch_remove(beta_gpu_batch* b, int id) {
   return BETA_GPU_OK;
 }
 
-int beta_gpu_batch_tune(beta_gpu_batch* b, int threads, int cluster) {
-  if (!b || !(threads == 256 || threads == 512 || threads == 1024) ||
-      !(cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8))
+int beta_gpu_batch_tune(beta_gpu_batch* b, int threads, int gang_boost) {
+  if (!b || !(threads == 256 || threads == 512 || threads == 1024) || gang_boost < 0 || gang_boost > 64)
     return BETA_GPU_ERR_ARG;
   cudaSetDevice(b->device);
-  const int ot = b->threads, oc = b->cluster;
+  const int ot = b->threads;
   b->threads = threads;
-  b->cluster = cluster;
-  if (batch_clusters(b) < 1) {
+  if (batch_ctas(b) < 1) {
     b->threads = ot;
-    b->cluster = oc;
-    return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "no cluster of this launch shape fits on the GPU");
+    return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "no CTA of this launch shape fits on the GPU");
   }
+  b->gang_boost = gang_boost;
   return BETA_GPU_OK;
 }
 
 int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, int* threads_out,
-                            int* cluster_out) {
-  if (!b || !o || budget <= 0) return BETA_GPU_ERR_ARG;
+                            int* boost_out) {
+  if (!b || !o || budget < 0) return BETA_GPU_ERR_ARG;
   cudaSetDevice(b->device);
-  const int shapes[][2] = {{256, 1}, {512, 1}, {1024, 1}, {256, 2}, {512, 2}, {512, 4}, {512, 8}, {256, 8}};
+  // (threads per CTA, gang boost)
+  const int shapes[][2] = {{512, 0}, {512, 1}, {512, 2}, {512, 4}, {512, 8}, {512, 16},
+                           {256, 4}, {256, 16}, {1024, 4}};
   double best = 1e300;
-  int bt = b->threads, bc = b->cluster, rc = BETA_GPU_OK;
+  int bt = b->threads, bg = b->gang_boost, rc = BETA_GPU_OK;
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
@@ -1679,17 +1688,17 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
     for (auto& S : b->sys)
       if (S.live) work += (double)S.st.iter * (double)S.work;
     const double per = work > 0 ? ms / work : 1e300;
-    if (per < best) { best = per; bt = sh[0]; bc = sh[1]; }
+    if (per < best) { best = per; bt = sh[0]; bg = sh[1]; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != BETA_GPU_OK) return rc;
   b->threads = bt;
-  b->cluster = bc;
+  b->gang_boost = bg;
   if ((rc = batch_reset_states(b))) return rc;
   BCK(cudaStreamSynchronize(b->stream));
   if (threads_out) *threads_out = bt;
-  if (cluster_out) *cluster_out = bc;
+  if (boost_out) *boost_out = bg;
   return BETA_GPU_OK;
 }
 
@@ -1703,25 +1712,27 @@ int beta_gpu_batch_reset(beta_gpu_batch* b) {
 }
 
 int beta_gpu_batch_info(const beta_gpu_batch* b, long long* out, int n) {
-  if (!b || !out || n < 0 || n > 7) return BETA_GPU_ERR_ARG;
+  if (!b || !out || n < 0 || n > 11) return BETA_GPU_ERR_ARG;
   long long live = 0;
   for (auto& S : b->sys) live += S.live ? 1 : 0;
-  const long long v[7] = {live, (long long)b->used, (long long)b->pool_bytes, b->n_launch, b->n_h2d, b->n_d2h,
-                          (long long)((double)b->last_ms * 1e6)};
+  const long long v[11] = {live, (long long)b->used, (long long)b->pool_bytes, b->n_launch, b->n_h2d, b->n_d2h,
+                           (long long)((double)b->last_ms * 1e6), b->last_ngang, b->last_gang_ctas, b->threads,
+                           b->gang_boost};
   for (int i = 0; i < n; ++i) out[i] = v[i];
   return BETA_GPU_OK;
 }
 
 // ============================ server C ABI ===================================
 int beta_gpu_server_create(beta_gpu_server** out, int device, long long budget, int max_systems,
-                           const beta_gpu_solve_opts* o, int iters_per_launch, int threads, int cluster) {
+                           const beta_gpu_solve_opts* o, int iters_per_launch, int threads, int gang_boost) {
   if (!out || !o || iters_per_launch <= 0) return BETA_GPU_ERR_ARG;
   *out = nullptr;
   beta_gpu_batch* b = nullptr;
   int rc = beta_gpu_batch_create(&b, device, budget, max_systems);
   if (rc != BETA_GPU_OK) return rc;
-  if ((threads || cluster) && (rc = beta_gpu_batch_tune(b, threads ? threads : b->threads,
-                                                         cluster ? cluster : b->cluster)) != BETA_GPU_OK) {
+  if ((threads || gang_boost >= 0) && (rc = beta_gpu_batch_tune(b, threads ? threads : b->threads,
+                                                                 gang_boost >= 0 ? gang_boost : b->gang_boost)) !=
+                                           BETA_GPU_OK) {
     beta_gpu_batch_destroy(b);
     return rc;
   }

@@ -29,7 +29,7 @@ struct MfArgs {
 
 // hex8 elasticity: 8 lanes per element, 4 elements per warp.
 __device__ __forceinline__ void mf_hex8_elastic_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
-    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y, const double* s_dN, const double* s_w) {
+    const double* w1, const double* w2, double* y, const double* s_dN, const double* s_w) {
   const int lane = threadIdx.x & 31, b = lane & 7;
   {
     const int idx = 4 * w + (lane >> 3);
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) k_mf_hex8_elastic(MfArgs A, const int* __
 
 // quad4 plane stress: 4 lanes per element, 8 elements per warp.
 __device__ __forceinline__ void mf_quad4_pstress_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
-    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y, const double* s_dN, const double* s_w) {
+    const double* w1, const double* w2, double* y, const double* s_dN, const double* s_w) {
   const int lane = threadIdx.x & 31, b = lane & 3;
   {
     const int idx = 8 * w + (lane >> 2);
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(256) k_mf_quad4_pstress(MfArgs A, const int* _
 
 // hex8 diffusion: y += K (c1 w1 + c2 w2) + cm M w1, 8 lanes per element.
 __device__ __forceinline__ void mf_hex8_heat_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
-    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y, const double* s_dN, const double* s_N, const double* s_w) {
+    const double* w1, const double* w2, double* y, const double* s_dN, const double* s_N, const double* s_w) {
   const int lane = threadIdx.x & 31, b = lane & 7;
   {
     const int idx = 4 * w + (lane >> 3);

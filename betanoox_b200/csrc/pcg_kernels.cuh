@@ -274,7 +274,7 @@ __global__ void k_dinv_s(int n, const long long* sdiag, const double* sval, doub
 template <int ND>
 struct NodeIO {
   static constexpr int S = ND * (ND + 1) / 2;
-  __device__ static __forceinline__ void ld(const float* __restrict__ v, long long I, float* o) {
+  __device__ static __forceinline__ void ld(const float* v, long long I, float* o) {
     if constexpr (ND == 2) {
       const float2 t = reinterpret_cast<const float2*>(v)[I];
       o[0] = t.x; o[1] = t.y;
@@ -292,7 +292,7 @@ struct NodeIO {
       for (int i = 0; i < ND; ++i) o[i] = __ldg(v + ND * I + i);
     }
   }
-  __device__ static __forceinline__ void st(float* __restrict__ v, long long I, const float* a) {
+  __device__ static __forceinline__ void st(float* v, long long I, const float* a) {
     if constexpr (ND == 2) {
       reinterpret_cast<float2*>(v)[I] = make_float2(a[0], a[1]);
     } else {
@@ -301,7 +301,7 @@ struct NodeIO {
     }
   }
   // z = M r with M symmetric, packed upper rows: (00,01,02,11,12,22) for ND=3
-  __device__ static __forceinline__ void prec(const float* __restrict__ m, long long I, const float* r, float* z) {
+  __device__ static __forceinline__ void prec(const float* m, long long I, const float* r, float* z) {
     float a[S];
 #pragma unroll
     for (int t = 0; t < S; ++t) a[t] = m[S * I + t];
@@ -331,7 +331,7 @@ struct PVec {
       NodeIO<ND>::ldg(v, I, o);
     }
   }
-  __device__ static __forceinline__ void ld(const float* __restrict__ v, long long I, float* o) {
+  __device__ static __forceinline__ void ld(const float* v, long long I, float* o) {
     if constexpr (ND == 3) {
       const float4 t = reinterpret_cast<const float4*>(v)[I];
       o[0] = t.x; o[1] = t.y; o[2] = t.z;
@@ -339,7 +339,7 @@ struct PVec {
       NodeIO<ND>::ld(v, I, o);
     }
   }
-  __device__ static __forceinline__ void st(float* __restrict__ v, long long I, const float* a) {
+  __device__ static __forceinline__ void st(float* v, long long I, const float* a) {
     if constexpr (ND == 3) {
       reinterpret_cast<float4*>(v)[I] = make_float4(a[0], a[1], a[2], 0.f);
     } else {
@@ -355,9 +355,10 @@ struct BlockMat {
   const float* bval;
 };
 
-template <int ND, bool PADDED>
-__device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane, const float* __restrict__ x,
-                                           float* acc) {
+// NC: gather x through the read-only cache (only when x is not written
+// during the kernel).
+template <int ND, bool PADDED, bool NC = true>
+__device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane, const float* x, float* acc) {
   constexpr int BB = ND * ND;
   const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
   const int* cp = A.bcol + (long long)c0 * 32 + lane;
@@ -368,8 +369,13 @@ __device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane, c
   for (int k = 0; k < w; ++k) {
     const int J = __ldcs(cp + k * 32);
     float xv[ND];
-    if constexpr (PADDED) PVec<ND>::ldg(x, J, xv);
-    else NodeIO<ND>::ldg(x, J, xv);
+    if constexpr (PADDED) {
+      if constexpr (NC) PVec<ND>::ldg(x, J, xv);
+      else PVec<ND>::ld(x, J, xv);
+    } else {
+      if constexpr (NC) NodeIO<ND>::ldg(x, J, xv);
+      else NodeIO<ND>::ld(x, J, xv);
+    }
     float v[BB];
 #pragma unroll
     for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);

@@ -240,12 +240,12 @@ BETA_GPU_API int beta_gpu_csr_pcg_device(int n, const int* d_row_ptr, const int*
  * system's structure on the host and copies it into the pool, or returns
  * BETA_GPU_REJECTED when the pool has no room (admission by HBM budget).
  * beta_gpu_batch_run assembles and solves every unfinished system in one
- * persistent launch (a replayed CUDA graph): each CTA takes whole systems,
- * largest first.  iters_per_launch > 0 bounds the PCG iterations each system
+ * persistent launch (a replayed CUDA graph).  iters_per_launch > 0 bounds the PCG iterations each system
  * gets per launch, so a serving loop can admit and retire systems between
- * launches; the Krylov state stays in the pool.  A system is solved by one
- * thread-block cluster of 1-8 CTAs (SMs) sharing DSMEM reductions and the
- * cluster barrier.  Stop rule: ||b-Au||/||b||
+ * launches; the Krylov state stays in the pool.  Big systems are solved by
+ * gangs of CTAs (SMs) meeting at software barriers, small ones by single
+ * CTAs; every sum has a fixed order, so a system's result does not depend on
+ * the mix or the gang size.  Stop rule: ||b-Au||/||b||
  * (opts->tol); opts->inner_tol is the residual-replacement factor.  Batched
  * diffusion systems are steady (conductivity only). */
 typedef struct beta_gpu_batch beta_gpu_batch;
@@ -283,21 +283,26 @@ BETA_GPU_API int beta_gpu_batch_run(beta_gpu_batch* batch, const beta_gpu_solve_
 BETA_GPU_API int beta_gpu_batch_result(beta_gpu_batch* batch, int sys_id, double* u,
                                        beta_gpu_solve_stats* stats);
 BETA_GPU_API int beta_gpu_batch_remove(beta_gpu_batch* batch, int sys_id);
-/* Launch shape: threads per CTA (256, 512 or 1024) and CTAs per cluster
- * (1, 2, 4 or 8) working on one system. */
-BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta, int cluster_ctas);
-/* Times every launch shape on the current systems for `budget` iterations each
- * (systems are reset to unsolved afterwards) and keeps the one with the least
- * time per unit of work. */
+/* Launch shape: threads per CTA (256, 512 or 1024; one CTA per SM) and gang
+ * sizing.  A system gets about gang_boost x (its share of the batch's FP32
+ * matrix values) of the CTAs, as one gang, when that is at least 2; the other
+ * systems are solved by single CTAs.  gang_boost 0: every system on one CTA.
+ * The result of a system does not depend on either choice. */
+BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta, int gang_boost);
+/* Times every launch shape (threads per CTA, gang boost) on the current
+ * systems for `budget` iterations each (budget 0: complete solves, which also
+ * measures the tail of the largest systems), resets the systems to unsolved
+ * afterwards and keeps the shape with the least time per unit of work. */
 BETA_GPU_API int beta_gpu_batch_autotune(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int budget,
-                                         int* threads_per_cta, int* cluster_ctas);
+                                         int* threads_per_cta, int* gang_boost);
 /* Marks every system unsolved: its next launch assembles and solves it again
  * from the data already in the pool (repeat solves without re-upload). */
 BETA_GPU_API int beta_gpu_batch_reset(beta_gpu_batch* batch);
 /* out[0] live systems, out[1] pool bytes in use, out[2] pool bytes, out[3]
  * launches, out[4] bytes host->device, out[5] bytes device->host, out[6]
- * device time of the last launch in ns (CUDA events on the batch's stream);
- * n <= 7. */
+ * device time of the last launch in ns (CUDA events on the batch's stream),
+ * out[7] gangs and out[8] CTAs in gangs in the last launch, out[9] threads
+ * per CTA, out[10] gang boost; n <= 11. */
 BETA_GPU_API int beta_gpu_batch_info(const beta_gpu_batch* batch, long long* out, int n);
 
 /* ---- continuous-batching server ------------------------------------------ */
@@ -318,10 +323,10 @@ BETA_GPU_API int beta_gpu_batch_info(const beta_gpu_batch* batch, long long* out
 #define BETA_GPU_REQ_CANCELLED 4
 #define BETA_GPU_REQ_FAILED 5
 typedef struct beta_gpu_server beta_gpu_server;
-/* threads_per_cta / cluster_ctas as in beta_gpu_batch_tune; 0 keeps the default. */
+/* threads_per_cta / gang_boost as in beta_gpu_batch_tune; 0 / -1 keep the defaults. */
 BETA_GPU_API int beta_gpu_server_create(beta_gpu_server** server, int device, long long hbm_budget_bytes,
                                         int max_systems, const beta_gpu_solve_opts* opts, int iters_per_launch,
-                                        int threads_per_cta, int cluster_ctas);
+                                        int threads_per_cta, int gang_boost);
 /* Stops the worker after its current launch; unfinished requests are dropped. */
 BETA_GPU_API int beta_gpu_server_destroy(beta_gpu_server* server);
 BETA_GPU_API const char* beta_gpu_server_last_error(const beta_gpu_server* server);

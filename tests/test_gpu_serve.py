@@ -43,7 +43,7 @@ def _alone(m, **kw):
 
 def test_served_mix_equals_each_alone_and_oracle(oracle):
     models = _mix()
-    kw = dict(iters_per_launch=25, threads=512, cluster=2)
+    kw = dict(iters_per_launch=25, threads=512, gang_boost=4)
     solo = [_alone(m, **kw) for m in models]
     with Server(hbm_budget=1 << 30, o=opts(tol=TOL), **kw) as s:
         rids = [None] * len(models)
