@@ -111,6 +111,10 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   return v;
 }
 
+// Slice partials of a CTA working alone stay in shared memory up to this
+// many slices (32K nodes); bigger systems and gangs use the pool.
+constexpr int kSharedSlices = 1024;
+
 // The CTAs working on one system: a gang (ctr != nullptr) or this CTA alone.
 struct Grp {
   int rank, size;
@@ -118,6 +122,7 @@ struct Grp {
   GangShared* gs;
   int* gabort;
   long long spin_ns;
+  double* spart;  // shared partials (2 x kSharedSlices) for a CTA alone
 };
 
 // Barrier of the group.  Returns false once the launch is aborting (a wait
@@ -170,9 +175,16 @@ __device__ __forceinline__ bool group_sum(const Grp& g, const double* part, int 
     double a[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) a[k] = 0.0;
-    for (int i = t; i < nsl; i += 256) {
+    if (part == g.spart) {
+      for (int i = t; i < nsl; i += 256) {
 #pragma unroll
-      for (int k = 0; k < NV; ++k) a[k] += __ldcg(part + (long long)k * nsl + i);
+        for (int k = 0; k < NV; ++k) a[k] += part[k * nsl + i];
+      }
+    } else {
+      for (int i = t; i < nsl; i += 256) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) a[k] += __ldcg(part + (long long)k * nsl + i);
+      }
     }
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
@@ -288,9 +300,15 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
   double* const partA = S.part;
   double* const partB = S.part + 2LL * nsl;
   // Partial buffers alternate: a buffer is rewritten only after the next
-  // sum's barrier, by which time every CTA has read it.
+  // sum's barrier, by which time every CTA has read it.  A CTA alone reads
+  // its partials back before the sum's last __syncthreads, so one shared
+  // buffer serves it.
+  const bool in_smem = g.ctr == nullptr && nsl <= kSharedSlices;
   int pb = 0;
-  auto part = [&]() { pb ^= 1; return pb ? partA : partB; };
+  auto part = [&]() {
+    pb ^= 1;
+    return in_smem ? g.spart : (pb ? partA : partB);
+  };
   BState st = *S.st;
   MfArgs M;
   M.xyz = S.xyz; M.conn = S.conn; M.gparams = S.gparams; M.egroup = S.egroup; M.nparams = S.nparams;
@@ -477,6 +495,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restri
                                                             const BPlan* __restrict__ plan, unsigned* bar, int* counter,
                                                             int* gabort, const BParams* __restrict__ prm) {
   __shared__ GangShared gs;
+  __shared__ double s_part[2 * kSharedSlices];
   __shared__ double s_dN[kMaxIP * 24], s_N[kMaxIP * 8], s_w[kMaxIP];
   __shared__ float s_dNf[kMaxIP * 24], s_Nf[kMaxIP * 8], s_wf[kMaxIP];
   const BParams P = *prm;
@@ -496,11 +515,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restri
     else b_solve<1>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf);
   };
   if (pl.k >= 0 && pl.k < P.nbig) {
-    const Grp gang{pl.rank, pl.size, bar + pl.bar, &gs, gabort, P.spin_ns};
+    const Grp gang{pl.rank, pl.size, bar + pl.bar, &gs, gabort, P.spin_ns, nullptr};
     solve(sys[active[pl.k]], gang);
     if (gs.abort) return;
   }
-  const Grp alone{0, 1, nullptr, &gs, gabort, P.spin_ns};
+  const Grp alone{0, 1, nullptr, &gs, gabort, P.spin_ns, s_part};
   for (;;) {
     if (threadIdx.x == 0) gs.idx = *(volatile int*)gabort ? P.nactive : P.nbig + atomicAdd(counter, 1);
     __syncthreads();
