@@ -15,6 +15,8 @@ shard: one system per GPU); value = total dofs solved / max-over-ranks time.
 persistent launch (gangs of CTAs for big systems, single CTAs for small ones,
 autotuned launch shape);
 one step = reset + assembly + mixed-precision solve of all 512.
+--config heat: transient diffusion on a 256x256x64 hex8 slab, 100 backward-Euler
+steps (each assembles C/dt + K in FP32 and solves it).
 --config serve: a Poisson stream of requests (quad4 / hex8 elasticity / hex8
 diffusion, log-uniform 1e3-5e5 dofs) through the continuous-batching server at
 80% of its measured capacity; reports throughput and p50/p99 latency.
@@ -429,6 +431,192 @@ def run_reference(args):
 
 
 
+# ---- transient diffusion (backward Euler) ------------------------------------
+def heat_model(args):
+    from betanoox_b200 import workloads as W
+    return W.heat_slab(args.heat_nx, args.heat_nx, args.heat_nz, order=2)
+
+
+def run_heat(args):
+    """One bench step = one backward-Euler time step: assemble C/dt + K in
+    FP32 and solve it by FP32 inner PCG with FP64 refinement (the state u_s
+    and the right-hand side stay on the device).  The timed region is
+    args.heat_steps consecutive time steps from the initial bump."""
+    import torch
+    from betanoox_b200 import Solver, _abi, opts
+    ws, rank, dev = _dist()
+    _init_dist(dev)
+    m = heat_model(args)
+    u0 = m.meta["u0"]
+    dt = args.dt
+    stream = torch.cuda.Stream(device=dev)
+    g = Solver(dev)
+    g.lib.beta_gpu_set_stream(g.h, C.c_void_p(stream.cuda_stream))
+    g.load_model(m)
+    g.build_pattern()
+    # Residual tolerance 1e-9: late in the run the field is smooth and an FP64
+    # residual b - A x of it cannot resolve much below 1e-10 of the step's
+    # right-hand side; the metric's bar is the solution error (<= 1e-8), which
+    # is measured below against a tightly converged FP64 march.
+    tol = args.heat_tol
+    o_mp = opts(mode=_abi.MODE_MPIR, tol=tol, inner_tol=args.inner_tol, profile=True)
+    o_64 = opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=tol, profile=True)
+
+    def counters():
+        a = (C.c_longlong * 3)()
+        g.lib.beta_gpu_counters(g.h, a, 3)
+        return list(a)
+
+    def march(prec, o, nsteps):
+        stats, ms = [], []
+        with torch.cuda.stream(stream):
+            for _ in range(nsteps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                g.assemble(prec, _abi.ASM_MBAR, dt, 1.0)
+                st, _ = g.heat_run(dt, 1, o)
+                e1.record(stream)
+                stats.append(st)
+                ms.append((e0, e1))
+        _barrier()
+        return [a.elapsed_time(b) for a, b in ms], stats
+
+    g.heat_set_state(u0)
+    march(_abi.FP32, o_mp, args.warmup)
+    g.heat_set_state(u0)
+    _barrier()
+    c0 = counters()
+    with Clocks(dev) as clk:
+        ms_mp, st_mp = march(_abi.FP32, o_mp, args.heat_steps)
+    c1 = counters()
+    u_mp = g.heat_get_state()
+    tot_ms = _max_over_ranks(sum(ms_mp), dev)
+    value = ws * m.ndof * args.heat_steps / (tot_ms / 1e3)
+    out = None
+    if rank == 0:
+        fp64 = None
+        if not args.skip_fp64:
+            g.heat_set_state(u0)
+            ms_64, st_64 = march(_abi.FP64, o_64, args.heat_steps)
+            u_64 = g.heat_get_state()
+            fp64 = {"value": ws * m.ndof * args.heat_steps / (sum(ms_64) / 1e3), "ms_total": sum(ms_64),
+                    "iterations_per_step_median": int(statistics.median([s.iterations for s in st_64]))}
+        err = None
+        if not args.skip_accuracy:
+            g.heat_set_state(u0)
+            march(_abi.FP64, opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=1e-13), args.heat_steps)
+            u_t = g.heat_get_state()
+            err = {"mixed": float(np.linalg.norm(u_mp - u_t) / np.linalg.norm(u_t))}
+            if fp64:
+                err["fp64"] = float(np.linalg.norm(u_64 - u_t) / np.linalg.norm(u_t))
+        e2e = None
+        if not args.skip_e2e:
+            pm = type(m)(m.name, m.kind, m.ndim, _pinned_copy(m.xyz), _pinned_copy(m.conn), m.ndpn,
+                         _pinned_copy(m.params), _pinned_copy(m.restrained), _pinned_copy(m.prescribed),
+                         _pinned_copy(m.load), m.order, m.meta)
+            u0p = _pinned_copy(u0)
+            u_host = _pinned_copy(np.zeros(m.ndof))
+            ge = Solver(dev)
+            ge.lib.beta_gpu_set_stream(ge.h, C.c_void_p(stream.cuda_stream))
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            ge.load_model(pm)
+            ge.build_pattern()
+            ge.lib.beta_gpu_heat_set_state(ge.h, u0p.ctypes.data_as(C.c_void_p))
+            for _ in range(args.heat_steps):
+                ge.assemble(_abi.FP32, _abi.ASM_MBAR, dt, 1.0)
+                ge.heat_run(dt, 1, o_mp)
+            ge.lib.beta_gpu_heat_get_state(ge.h, u_host.ctypes.data_as(C.c_void_p))
+            torch.cuda.synchronize()
+            tw = time.perf_counter() - t1
+            a = (C.c_longlong * 3)()
+            ge.lib.beta_gpu_counters(ge.h, a, 3)
+            e2e = {"value": ws * m.ndof * args.heat_steps / tw, "unit": UNIT, "h2d_bytes_per_step": a[1],
+                   "d2h_bytes_per_step": a[2], "ms_per_step": 1e3 * tw,
+                   "includes": f"upload, host structure, {args.heat_steps} x (FP32 assembly + solve), download; "
+                               f"a step here is the whole {args.heat_steps}-step run"}
+            ge.close()
+        peak, peak_kind = _peaks()
+        spmv_ms = statistics.median([s.ms_spmv_avg for s in st_mp])
+        alg = spmv_algorithmic_bytes(_nblk(m), m.nnode, 1)
+        achieved = alg / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "kernel": "k_spmv_dot_b<1> (FP32 sliced-ELL SpMV + p.Ap, one dof per node)",
+                "algorithmic_bytes_per_launch": alg, "ms_per_launch": spmv_ms,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s"}
+        its = [s.iterations for s in st_mp]
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.heat_steps,
+            "warmup": args.warmup, "ms_per_step": tot_ms / args.heat_steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 inner / fp64 outer",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"transient diffusion hex8 {args.heat_nx}x{args.heat_nx}x{args.heat_nz}, "
+                                   f"{m.ndof} dofs, backward Euler dt={dt}, k=exp(N(0,1)), c=1, T=0 on all faces, "
+                                   f"Gaussian bump; each step assembles C/dt+K (FP32) and solves it",
+                       "ndof": m.ndof, "time_steps": args.heat_steps, "tol": tol,
+                       "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (matrix ~1 GB)"},
+            "latency_ms": {"p50": float(np.percentile(ms_mp, 50)), "p99": float(np.percentile(ms_mp, 99))},
+            "heat": {"iterations_per_step": [min(its), int(statistics.median(its)), max(its)],
+                     "refinements_per_step_median": int(statistics.median([s.outer_iterations for s in st_mp]))},
+            "e2e": e2e, "gpu_launches": c1[0] - c0[0], "roofline": roof, "clocks": clk.summary(),
+        }
+        if fp64:
+            out["fp64_plain"] = fp64
+            out["mixed_over_fp64"] = value / fp64["value"]
+        if err:
+            out["rel_err_vs_fp64_reference"] = err
+        if not args.skip_cpu:
+            out["cpu_baseline"] = heat_cpu_baseline(args, m)
+    g.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return out
+
+
+def heat_cpu_baseline(args, m):
+    """The reference transient step on the host (oracle restatement: FP64
+    assembly of Mbar and F, threaded Jacobi-PCG) on a smaller slab with the
+    same cell size ratio, a few steps, scaled to the full workload by dofs."""
+    from oracle import beta_oracle as bo
+    from betanoox_b200 import workloads as W
+    nx, nz = args.cpu_heat_nx, max(2, args.cpu_heat_nx * args.heat_nz // args.heat_nx)
+    ms = W.heat_slab(nx, nx, nz, order=2)
+    s = bo.System(ms)
+    s.set_bc(ms.restrained, ms.prescribed, ms.load)
+    s.build_pattern()
+    u = ms.meta["u0"].copy()
+    t0 = time.perf_counter()
+    k = 0
+    while k < 2 or (time.perf_counter() - t0 < 10.0 and k < 20):
+        s.set_bc(ms.restrained, ms.prescribed, ms.load)
+        rc, u, st = s.heat_step(ms.params, ms.order, args.dt, u, eps=args.heat_tol, maxit=100000)
+        k += 1
+    per_dof_step = (time.perf_counter() - t0) / k / ms.ndof
+    return {"value": 1.0 / per_dof_step, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{k} backward-Euler steps of the {nx}x{nx}x{nz} slab ({ms.ndof} dofs) on one host thread "
+                      f"(FP64 assembly + Jacobi-PCG), rate per dof applied to the {m.ndof}-dof workload"}
+
+
+def run_heat_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return None
+    m = heat_model(args)
+    vals = [heat_cpu_baseline(args, m)["value"] for _ in range(max(1, args.steps))]
+    cb = heat_cpu_baseline(args, m)
+    v = statistics.median(vals)
+    cb["value"] = v
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * m.ndof / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": {"workload": f"transient diffusion hex8 {args.heat_nx}x{args.heat_nx}x{args.heat_nz}, "
+                                   f"{m.ndof} dofs, backward Euler dt={args.dt}", "ndof": m.ndof},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 # ---- batched RVEs (one persistent launch) ---------------------------------
 def iter_bytes(nblk, nnode, nd):
     """Algorithmic bytes of one inner FP32 PCG iteration of the batched solver
@@ -519,7 +707,11 @@ def run_batch(args):
     t_add = time.perf_counter() - t0
     assert all(i is not None for i in ids), "pool too small for the batch"
     t0 = time.perf_counter()
-    threads, boost = b.autotune(o, budget=args.tune_iters)
+    if args.shape:
+        threads, boost = (int(v) for v in args.shape.split(","))
+        b.tune(threads, boost)
+    else:
+        threads, boost = b.autotune(o, budget=args.tune_iters)
     t_tune = time.perf_counter() - t0
     for _ in range(args.warmup):
         b.reset()
@@ -870,6 +1062,7 @@ def main():
     ap.add_argument("--pool-gb", type=float, default=48.0)
     ap.add_argument("--tune-iters", type=int, default=0, help="0: autotune on complete solves")
     ap.add_argument("--check-every", type=int, default=32)
+    ap.add_argument("--shape", default="", help="threads,gang_boost: skip the autotuner")
     ap.add_argument("--fp64-sample", type=int, default=512)
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--serve-pool", type=int, default=1000)
@@ -880,11 +1073,20 @@ def main():
     ap.add_argument("--gang-boost", type=int, default=4)
     ap.add_argument("--submit-threads", type=int, default=0)
     ap.add_argument("--serve-fp64-sample", type=int, default=100)
+    # transient diffusion
+    ap.add_argument("--heat-nx", type=int, default=256)
+    ap.add_argument("--heat-nz", type=int, default=64)
+    ap.add_argument("--heat-steps", type=int, default=100)
+    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--heat-tol", type=float, default=1e-9)
+    ap.add_argument("--cpu-heat-nx", type=int, default=48)
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     ref = args.impl == "reference"
-    if args.config == "batch":
+    if args.config == "heat":
+        out = run_heat_reference(args) if ref else run_heat(args)
+    elif args.config == "batch":
         out = run_batch_reference(args) if ref else run_batch(args)
     elif args.config == "serve":
         out = run_serve_reference(args) if ref else run_serve(args)

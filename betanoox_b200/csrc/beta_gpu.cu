@@ -1282,6 +1282,17 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
       CKL("k_rhs64");
       rc = fp64_core(c, o, &s, &prof);
     } else {
+      // Scale of the step: ||(M/dt) u_s||, the right-hand side of the
+      // backward-Euler system for the new state.  The increment solved below
+      // has the same residual vector, but its own right-hand side shrinks as
+      // the field smooths out, below what an FP64 residual of a smooth field
+      // can resolve; the stop is taken relative to the larger of the two.
+      if ((rc = mf_apply(c, 0.0, c->us.p, 0.0, nullptr, ms, c->y64.p))) return rc;
+      launch(c, k_norm2_diff, grid_for(c, n, 256), 256, 0, n, (const double*)c->y64.p, (const double*)nullptr,
+             c->sums.p, c->partials.p, c->ticket.p);
+      CKL("k_norm2_diff");
+      double ff;
+      if ((rc = read_sums(c, 1, &ff))) return rc;
       // b = rest ? presc : -(kf K u_s + Mbar ubar_ext) ; r = -(K(ks x + kf u_s) + ms M x)
       launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, nullptr, c->t64.p);
       if ((rc = mf_apply(c, ks, c->t64.p, kf, c->us.p, ms, c->y64.p))) return rc;
@@ -1291,13 +1302,14 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
       double bb;
       if ((rc = read_sums(c, 1, &bb))) return rc;
       CK(cudaMemcpyAsync(c->x64.p, c->t64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
-      rc = mpir_dispatch(c, o, ks, kf, c->us.p, ms, nullptr, std::sqrt(bb), &s, &prof);
+      rc = mpir_dispatch(c, o, ks, kf, c->us.p, ms, nullptr, std::sqrt(std::max(bb, ff)), &s, &prof);
     }
     if (rc != BETA_GPU_OK) {
       if (stats) *stats = s;
       return rc;
     }
     total += s.iterations;
+    s.ms_spmv_avg = prof.launches ? prof.ms / prof.launches : 0.0;
     // u_s <- u_s + delta (DiffusionModel.cpp:800-818)
     launch(c, k_axpy64, grid_for(c, n, 256), 256, 0, n, c->us.p, 1.0, c->x64.p);
     CKL("k_axpy64");
