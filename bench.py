@@ -151,17 +151,60 @@ def spmv_algorithmic_bytes(nblk, nnode, nd):
     return nblk * (nd * nd * 4 + 4) + 2 * nnode * nd * 4
 
 
+def _init_dist(dev, backend="nccl"):
+    """One process per GPU under torchrun: a process group with a short
+    timeout (ranks that wait for a dead peer end with an error).  The backend
+    is NCCL on GPUs; the rank logic is the same with gloo on the host."""
+    import torch
+    ws, rank, local = _dist()
+    if backend == "nccl":
+        torch.cuda.set_device(dev)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        kw = {"device_id": torch.device("cuda", dev)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=timedelta(seconds=600), **kw)
+    return ws, rank
+
+
+def _max_over_ranks(v, dev):
+    """Max of a per-rank number over all ranks (every rank gets it)."""
+    ws, _, _ = _dist()
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    on_gpu = dist.get_backend() == "nccl"
+    t = torch.tensor([float(v)], dtype=torch.float64, device=f"cuda:{dev}" if on_gpu else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier():
+    import torch
+    ws, _, _ = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+
+
+def whole_job_rate(units_per_rank, seconds, dev=0):
+    """Weak-scaling aggregate: every rank processed units_per_rank; the job
+    took the slowest rank's time.  Returns (units/s for the whole job, max s)."""
+    ws, _, _ = _dist()
+    tmax = _max_over_ranks(seconds, dev)
+    return ws * units_per_rank / tmax, tmax
+
+
 def run_ours(args):
     import torch
     from betanoox_b200 import Solver, _abi, opts
 
     ws, rank, local = _dist()
     dev = local
-    torch.cuda.set_device(dev)
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
+    _init_dist(dev)
 
     m = make_model(args.config, args.n)
     stream = torch.cuda.Stream(device=dev)
@@ -193,11 +236,7 @@ def run_ours(args):
         rc, st = g.solve(o_64)
         return st
 
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-        torch.cuda.synchronize()
+    barrier = _barrier
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -270,26 +309,16 @@ def run_ours(args):
             tw.append(time.perf_counter() - t1)
         c1 = ecnt()
         k = max(1, args.e2e_steps)
-        tmax = max(tw)
-        if ws > 1:
-            import torch.distributed as dist
-            tt = torch.tensor([tmax], device=f"cuda:{dev}")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            tmax = float(tt.item())
-        e2e = {"value": ws * m.ndof / statistics.median(tw), "unit": UNIT,
+        ev, tmed = whole_job_rate(m.ndof, statistics.median(tw), dev)
+        e2e = {"value": ev, "unit": UNIT,
                "h2d_bytes_per_step": (c1[1] - c0[1]) // k, "d2h_bytes_per_step": (c1[2] - c0[2]) // k,
-               "ms_per_step": 1e3 * statistics.median(tw)}
+               "ms_per_step": 1e3 * tmed}
         ge.close()
 
     # -- reduce timing over ranks --
-    tot_ms = sum(ms_mp)
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([tot_ms], device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        tot_ms = float(tt.item())
+    value, tot_s = whole_job_rate(m.ndof * args.steps, sum(ms_mp) / 1e3, dev)
+    tot_ms = tot_s * 1e3
     ms_step = tot_ms / args.steps
-    value = ws * m.ndof * args.steps / (tot_ms / 1e3)
 
     out = None
     if rank == 0:
@@ -657,37 +686,6 @@ def cpu_full_solves(models, tol, budget_s, threads):
         if secs >= budget_s:
             break
     return done, dofs, secs
-
-
-def _init_dist(dev):
-    import torch
-    ws, rank, local = _dist()
-    torch.cuda.set_device(dev)
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
-    return ws, rank
-
-
-def _max_over_ranks(v, dev):
-    ws, _, _ = _dist()
-    if ws == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], device=f"cuda:{dev}", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def _barrier():
-    import torch
-    ws, _, _ = _dist()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize()
 
 
 def run_batch(args):

@@ -260,29 +260,26 @@ int batch_launch_graph(beta_gpu_batch* b) {
   return BETA_GPU_OK;
 }
 
-// Gang plan for the active list act[0..na) (sorted by matrix values, largest
-// first).  With N resident CTAs and W values in all, a system of w values
-// wants g = floor(gang_boost * w * N / W) CTAs, capped so every warp keeps at
-// least two 32-node slices; g >= 2 makes it a gang.  When the gangs want more
-// than N CTAs they shrink in proportion (to at least 2 each) and the smallest
-// are demoted to single-CTA systems until they fit.  CTAs outside the gangs
-// start on the small systems at once; a gang joins them when its system is
-// done.  Returns the number of gangs; they solve act[0..ngang).
-int batch_plan(beta_gpu_batch* b, const int* act, int na, int nctas) {
-  const int warps = b->threads / 32;
+// Gang sizes for systems sorted by stored matrix values, largest first.  With
+// N resident CTAs and W values in all, system i (w values, s 32-node slices)
+// wants g = floor(boost * w * N / W) CTAs, capped so every warp of the gang
+// keeps at least two slices; g >= 2 makes it a gang.  When the gangs want
+// more than N CTAs they shrink in proportion (to at least 2 each) and the
+// smallest are demoted to single-CTA systems until they fit.  CTAs outside
+// the gangs start on the small systems at once; a gang joins them when its
+// system is done.  Fills g[0..ngang) and returns ngang (the gangs solve
+// systems 0..ngang-1).
+int gang_plan(int na, const long long* work, const int* nslice, int nctas, int warps, int boost, int* g) {
   double W = 0.0;
-  for (int i = 0; i < na; ++i) W += (double)b->sys[act[i]].work;
+  for (int i = 0; i < na; ++i) W += (double)work[i];
   auto want = [&](int i) {
-    const auto& S = b->sys[act[i]];
-    const int cap = std::max(1, S.nslice / (2 * warps));
-    return std::min(cap, (int)std::min<double>(nctas, std::floor(b->gang_boost * (double)S.work * nctas / W)));
+    const int cap = std::max(1, nslice[i] / (2 * warps));
+    return std::min(cap, (int)std::min<double>(nctas, std::floor(boost * (double)work[i] * nctas / W)));
   };
   int ngang = 0;
-  if (b->gang_boost > 0 && W > 0)
+  if (boost > 0 && W > 0)
     while (ngang < na && ngang < nctas / 2 && want(ngang) >= 2) ++ngang;  // sorted: later systems want less
-  std::vector<int> g;
   for (; ngang > 0; --ngang) {
-    g.assign(ngang, 0);
     long long want_sum = 0;
     for (int i = 0; i < ngang; ++i) want_sum += (g[i] = want(i));
     long long sum = want_sum;
@@ -292,6 +289,18 @@ int batch_plan(beta_gpu_batch* b, const int* act, int na, int nctas) {
     }
     if (sum <= nctas) break;
   }
+  return ngang;
+}
+
+// Gang plan of one launch over act[0..na) (sorted largest first) into h_plan.
+int batch_plan(beta_gpu_batch* b, const int* act, int na, int nctas) {
+  std::vector<long long> work(na);
+  std::vector<int> nsl(na), g(std::max(1, na));
+  for (int i = 0; i < na; ++i) {
+    work[i] = b->sys[act[i]].work;
+    nsl[i] = b->sys[act[i]].nslice;
+  }
+  const int ngang = gang_plan(na, work.data(), nsl.data(), nctas, b->threads / 32, b->gang_boost, g.data());
   int c = 0;
   for (int i = 0; i < ngang; ++i)
     for (int r = 0; r < g[i]; ++r, ++c) b->h_plan[c] = BPlan{i, r, g[i], i};

@@ -1714,6 +1714,17 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
   return BETA_GPU_OK;
 }
 
+int beta_gpu_gang_plan(int nsys, const long long* matrix_values, const int* slices, int ctas, int threads_per_cta,
+                       int gang_boost, int* gang_ctas) {
+  if (nsys < 0 || (nsys > 0 && (!matrix_values || !slices || !gang_ctas)) || ctas < 1 || threads_per_cta < 32 ||
+      gang_boost < 0)
+    return -BETA_GPU_ERR_ARG;
+  for (int i = 0; i < nsys; ++i)
+    if (matrix_values[i] < 0 || slices[i] < 0 || (i > 0 && matrix_values[i] > matrix_values[i - 1]))
+      return -BETA_GPU_ERR_ARG;
+  return gang_plan(nsys, matrix_values, slices, ctas, threads_per_cta / 32, gang_boost, gang_ctas);
+}
+
 int beta_gpu_batch_reset(beta_gpu_batch* b) {
   if (!b) return BETA_GPU_ERR_ARG;
   cudaSetDevice(b->device);

@@ -299,6 +299,13 @@ BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta,
  * afterwards and keeps the shape with the least time per unit of work. */
 BETA_GPU_API int beta_gpu_batch_autotune(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int budget,
                                          int* threads_per_cta, int* gang_boost);
+/* The batch engine's CTA planner, exposed for inspection: for nsys systems
+ * sorted by stored FP32 matrix values (largest first) with their 32-node
+ * slice counts, fills gang_ctas[0..g) with the CTAs of each gang a launch of
+ * `ctas` CTAs would form and returns g (systems 0..g-1 are solved by gangs,
+ * the rest by single CTAs), or -BETA_GPU_ERR_ARG.  Host only. */
+BETA_GPU_API int beta_gpu_gang_plan(int nsys, const long long* matrix_values, const int* slices, int ctas,
+                                    int threads_per_cta, int gang_boost, int* gang_ctas);
 /* Marks every system unsolved: its next launch assembles and solves it again
  * from the data already in the pool (repeat solves without re-upload). */
 BETA_GPU_API int beta_gpu_batch_reset(beta_gpu_batch* batch);

@@ -118,3 +118,40 @@ def test_serve_requests_cover_families_and_sizes():
     assert nd.min() >= 500 and nd.max() <= 6e5
     for m in ms[:6]:
         assert m.restrained.any() and np.isfinite(m.params).all()
+
+
+def _plan(abi, work, slices, ctas=148, threads=512, boost=4):
+    n = len(work)
+    w = (C.c_longlong * max(1, n))(*work)
+    s = (C.c_int * max(1, n))(*slices)
+    g = (C.c_int * max(1, n))()
+    ng = abi.beta_gpu_gang_plan(n, w, s, ctas, threads, boost, g)
+    return ng, list(g)[:max(0, ng)]
+
+
+def test_gang_plan_single_system_takes_the_gpu(abi):
+    ng, g = _plan(abi, [10 ** 8], [100000])
+    assert ng == 1 and g == [148]
+    ng, g = _plan(abi, [10 ** 6], [200])  # capped: every warp keeps two slices
+    assert ng == 1 and g == [200 // 32]
+    assert _plan(abi, [10 ** 8], [100000], boost=0)[0] == 0
+
+
+def test_gang_plan_invariants_on_random_batches(abi):
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        n = int(rng.integers(1, 600))
+        sl = np.sort(rng.integers(1, 8000, size=n))[::-1]
+        work = sl.astype(np.int64) * 27 * 32 * 9
+        ctas = int(rng.integers(2, 300))
+        boost = int(rng.choice([0, 1, 2, 4, 8, 64]))
+        ng, g = _plan(abi, work.tolist(), sl.tolist(), ctas=ctas, boost=boost)
+        assert 0 <= ng <= min(n, ctas // 2)
+        assert sum(g) <= ctas and all(x >= 2 for x in g)
+        assert all(g[i] >= g[i + 1] for i in range(len(g) - 1))
+        for i, x in enumerate(g):
+            assert x <= max(2, sl[i] // 32)
+
+
+def test_gang_plan_rejects_unsorted_input(abi):
+    assert _plan(abi, [5, 9], [10, 10])[0] == -_abi.ERR_ARG
