@@ -271,6 +271,12 @@ class Batch:
             raise self._err(st, "batch_autotune")
         return t.value, c.value
 
+    def set_switch(self, iters_per_cycle):
+        """FP32 cycles longer than this switch a system to FP64 matrix-free PCG (0: never)."""
+        st = self.lib.beta_gpu_batch_set_switch(self.h, int(iters_per_cycle))
+        if st != _abi.OK:
+            raise self._err(st, "batch_set_switch")
+
     def reset(self):
         """Marks every system unsolved (the next run re-assembles and re-solves)."""
         st = self.lib.beta_gpu_batch_reset(self.h)

@@ -47,6 +47,9 @@ struct beta_gpu_batch {
   // gang_boost x (its share of the batch's matrix values) of the CTAs, and a
   // gang when that is at least 2 (0: every system on one CTA)
   int threads = 512, gang_boost = 4;
+  // a system whose FP32 inner solve needs more than this many iterations for
+  // one residual-replacement cycle continues in FP64, matrix-free (0: never)
+  int switch_iters = 2000;
   int last_ngang = 0, last_gang_ctas = 0;
   std::map<int, cudaGraphExec_t> graphs;
   long long n_launch = 0, n_h2d = 0, n_d2h = 0;
@@ -109,7 +112,7 @@ void pool_free(beta_gpu_batch* b, size_t off, size_t bytes) {
 struct SysLayout {
   size_t total = 0;
   size_t o_xyz, o_conn, o_gp, o_eg, o_rest, o_presc, o_load, o_cptr, o_elems, o_slot, o_nrp, o_ndiag, o_bsoff,
-      o_bcol, o_bval, o_x64, o_r64, o_y64, o_y32, o_r32, o_p32, o_q32, o_minv, o_part, o_gflag;
+      o_bcol, o_bval, o_x64, o_r64, o_y64, o_p64, o_q64, o_y32, o_r32, o_p32, o_p32b, o_z32, o_q32, o_minv, o_part, o_gflag;
   size_t add(size_t bytes) {
     const size_t o = total;
     total += (bytes + 255) & ~size_t(255);
@@ -139,9 +142,13 @@ SysLayout layout_for(int ndim, int nnode, int nelem, int nnpe, int ndpn, int ngr
   L.o_x64 = L.add(sizeof(double) * ndof);
   L.o_r64 = L.add(sizeof(double) * ndof);
   L.o_y64 = L.add(sizeof(double) * ndof);
+  L.o_p64 = L.add(sizeof(double) * ndof);
+  L.o_q64 = L.add(sizeof(double) * ndof);
   L.o_y32 = L.add(sizeof(float) * ndof);
   L.o_r32 = L.add(sizeof(float) * ndof);
   L.o_p32 = L.add(sizeof(float) * (size_t)nnode * (ndpn == 3 ? 4 : ndpn));
+  L.o_p32b = L.add(sizeof(float) * (size_t)nnode * (ndpn == 3 ? 4 : ndpn));
+  L.o_z32 = L.add(sizeof(float) * (size_t)nnode * (ndpn == 3 ? 4 : ndpn));
   L.o_q32 = L.add(sizeof(float) * ndof);
   L.o_minv = L.add(sizeof(float) * (size_t)nnode * (ndpn * (ndpn + 1) / 2));
   L.o_part = L.add(sizeof(double) * 4 * (size_t)P.nslice);
@@ -333,6 +340,7 @@ int batch_prepare(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, i
   P.nactive = na;
   P.nbig = ngang;
   P.spin_ns = 2000000000LL;  // 2 s at one barrier: far beyond any phase of a resident gang
+  P.switch_iters = b->switch_iters;
   int rc;
   if (!b->sys.empty() && (rc = batch_h2d(b, b->d_sys, b->h_sys, sizeof(BSys) * b->sys.size()))) return rc;
   if ((rc = batch_h2d(b, b->d_active, b->h_active, sizeof(int) * std::max(1, na)))) return rc;

@@ -41,6 +41,10 @@ enum : int { kBConverged = 0, kBRunning = 1, kBMaxit = 4, kBBreakdown = 5, kBNeg
 struct BState {
   double rho, rr, maxrr, bn, rn;
   int iter, repl, phase, status;
+  int mode;    // 0: FP32 inner PCG with FP64 reliable updates; 1: FP64 PCG, operator matrix-free
+  int cycle0;  // iteration at which the current FP32 replacement cycle began
+  float bt;    // FP32 mode: beta of the direction update the next SpMV applies
+  int pb;      // FP32 mode: which direction buffer holds the current p (0: p32, 1: p32b)
 };
 
 // Device descriptor of one system (all pointers into the batch pool).
@@ -64,9 +68,13 @@ struct BSys {
   double* x64;
   double* r64;
   double* y64;
+  double* p64;  // FP64 mode: search direction
+  double* q64;  // FP64 mode: K p, then M r
   float* y32;
   float* r32;
-  float* p32;
+  float* p32;   // direction (double-buffered with p32b; padded to float4 for nd = 3)
+  float* p32b;
+  float* z32;   // z = M r of the last update (same padding)
   float* q32;
   float* minv;
   double* part;     // 2 buffers x 2 values x nslice slice partials
@@ -81,6 +89,7 @@ struct BParams {
   int maxit, max_repl, budget;  // budget: iterations per system per launch (0: no limit)
   int nactive, nbig;            // active[0, nbig) are solved by gangs, the rest by single CTAs
   long long spin_ns;            // longest wait at a gang barrier before the launch gives up
+  int switch_iters;             // FP32 cycle longer than this: continue in FP64 (0: never)
 };
 
 // Per CTA: the gang it belongs to for this launch.
@@ -131,13 +140,14 @@ __device__ __forceinline__ bool gsync(const Grp& g) {
   __syncthreads();
   if (g.ctr == nullptr) return true;
   if (threadIdx.x == 0) {
-    __threadfence();  // release this CTA's writes
     const unsigned target = (++g.gs->bar_no) * (unsigned)g.size;
-    atomicAdd(g.ctr, 1u);
-    const long long t0 = globaltimer_ns();
+    // arrive: releases every write of this CTA ordered before the CTA barrier
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(g.ctr), "r"(1u) : "memory");
     unsigned polls = 0;
+    long long t0 = 0;
     while (ld_acquire_u32(g.ctr) < target) {
-      if ((++polls & 63u) == 0u) {
+      if ((++polls & 255u) == 0u) {
+        if (t0 == 0) t0 = globaltimer_ns();
         if (*(volatile int*)g.gabort) { g.gs->abort = 1; break; }
         if (globaltimer_ns() - t0 > g.spin_ns) {
           g.gs->abort = 1;
@@ -145,9 +155,8 @@ __device__ __forceinline__ bool gsync(const Grp& g) {
           break;
         }
       }
-      __nanosleep(64);
     }
-    __threadfence();  // acquire the other CTAs' writes
+    __threadfence();  // the other CTAs' writes are visible to every thread after the CTA barrier
   }
   __syncthreads();
   return g.gs->abort == 0;
@@ -181,7 +190,22 @@ __device__ __forceinline__ bool group_sum(const Grp& g, const double* part, int 
         for (int k = 0; k < NV; ++k) a[k] += part[k * nsl + i];
       }
     } else {
-      for (int i = t; i < nsl; i += 256) {
+      // Loads of 8 strided partials are issued before they are added (in the
+      // same order), so a long partial array costs a few L2 round trips, not
+      // one per partial.
+      int i = t;
+      for (; i + 7 * 256 < nsl; i += 8 * 256) {
+        double b[NV][8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+          for (int k = 0; k < NV; ++k) b[k][u] = __ldcg(part + (long long)k * nsl + i + u * 256);
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+          for (int k = 0; k < NV; ++k) a[k] += b[k][u];
+      }
+      for (; i < nsl; i += 256) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) a[k] += __ldcg(part + (long long)k * nsl + i);
       }
@@ -280,9 +304,83 @@ __device__ __forceinline__ bool b_rz(const BSys& S, const Grp& g, double* part, 
       float rv[ND], z[ND];
       NodeIO<ND>::ld(S.r32, I, rv);
       NodeIO<ND>::prec(S.minv, I, rv, z);
+      PVec<ND>::st(S.z32, I, z);
       if (set_p) PVec<ND>::st(S.p32, I, z);
 #pragma unroll
       for (int i = 0; i < ND; ++i) { v[0] += (double)rv[i] * z[i]; v[1] += (double)rv[i] * rv[i]; }
+    }
+    slice_partial<2>(part, S.nslice, s, v);
+  }
+  return group_sum<2>(g, part, S.nslice, out);
+}
+
+// One 32-node slice of q = A p_new with the direction update folded into the
+// gather: p_new[J] = fmaf(bt, p_old[J], z[J]) for every column J -- the same
+// arithmetic, and so the same bits, as updating p in a separate pass.  Saves
+// a pass over the vectors and a group barrier per iteration.
+template <int ND>
+__device__ __forceinline__ void spmv_row_fused(const BlockMat& A, int s, int lane, const float* pold,
+                                               const float* z, float bt, float* acc) {
+  constexpr int BB = ND * ND;
+  const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
+  const int* cp = A.bcol + (long long)c0 * 32 + lane;
+  const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) acc[i] = 0.f;
+#pragma unroll 2
+  for (int k = 0; k < w; ++k) {
+    const int J = __ldcs(cp + k * 32);
+    float po[ND], zv[ND];
+    PVec<ND>::ld(pold, J, po);
+    PVec<ND>::ld(z, J, zv);
+    float v[BB];
+#pragma unroll
+    for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);
+#pragma unroll
+    for (int i = 0; i < ND; ++i)
+#pragma unroll
+      for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], fmaf(bt, po[j], zv[j]), acc[i]);
+  }
+}
+
+// z = M r for one node in FP64 arithmetic (packed symmetric FP32 factor).
+template <int ND>
+__device__ __forceinline__ void prec64(const float* m, long long I, const double* r, double* z) {
+  constexpr int S = ND * (ND + 1) / 2;
+  double a[S];
+#pragma unroll
+  for (int t = 0; t < S; ++t) a[t] = (double)m[S * I + t];
+  if constexpr (ND == 1) {
+    z[0] = a[0] * r[0];
+  } else if constexpr (ND == 2) {
+    z[0] = a[0] * r[0] + a[1] * r[1];
+    z[1] = a[1] * r[0] + a[2] * r[1];
+  } else {
+    z[0] = a[0] * r[0] + a[1] * r[1] + a[2] * r[2];
+    z[1] = a[1] * r[0] + a[3] * r[1] + a[4] * r[2];
+    z[2] = a[2] * r[0] + a[4] * r[1] + a[5] * r[2];
+  }
+}
+
+// FP64 mode, start of a Krylov cycle from r64: p64 = z = M r64, returns (r.z, r.r).
+template <int ND>
+__device__ __forceinline__ bool b_rz64(const BSys& S, const Grp& g, double* part, double (&out)[2]) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int wid = g.rank * nw + (threadIdx.x >> 5), gw = g.size * nw;
+  for (int s = wid; s < S.nslice; s += gw) {
+    const int I = 32 * s + lane;
+    double v[2] = {0.0, 0.0};
+    if (I < S.nnode) {
+      double rv[ND], z[ND];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) rv[i] = S.r64[(long long)I * ND + i];
+      prec64<ND>(S.minv, I, rv, z);
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        S.p64[(long long)I * ND + i] = z[i];
+        v[0] += rv[i] * z[i];
+        v[1] += rv[i] * rv[i];
+      }
     }
     slice_partial<2>(part, S.nslice, s, v);
   }
@@ -385,6 +483,10 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     st.rr = st.maxrr = a2[1];
     st.iter = 0;
     st.repl = 0;
+    st.mode = 0;
+    st.cycle0 = 0;
+    st.bt = 0.f;  // p32 = z32 = M r: the first fused update gives p = z exactly
+    st.pb = 0;
     st.phase = kPhaseIter;
     st.status = kBRunning;
     st.rn = sqrt(a2[1]);
@@ -395,17 +497,121 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
   const double delta2 = P.delta * P.delta;
   int spent = 0;
   while (st.phase == kPhaseIter && (P.budget <= 0 || spent < P.budget)) {
-    // q = A p, p.q  (one warp per 32-node slice)
+    if (st.mode == 1) {
+      // ---- FP64 Jacobi-PCG, q = K p matrix-free (restrained dofs stay fixed)
+      if (!b_mf(S, M, S.p64, S.q64, s_dN, s_N, s_w, g)) return aborted();
+      double* pq = part();
+      for (int s = wid; s < nsl; s += nw) {
+        double v[1] = {0.0};
+#pragma unroll
+        for (int k = 0; k < ND; ++k) {
+          const long long i = 32LL * ND * s + 32 * k + lane;
+          if (i < n && !S.rest[i]) v[0] += S.p64[i] * S.q64[i];
+        }
+        slice_partial<1>(pq, nsl, s, v);
+      }
+      double a1[1];
+      if (!group_sum<1>(g, pq, nsl, a1)) return aborted();
+      if (!(a1[0] > 0.0 && a1[0] < 1e308)) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
+      const double alpha = st.rho / a1[0];
+      double* rz = part();
+      for (int s = wid; s < nsl; s += nw) {
+        const int I = 32 * s + lane;
+        double v[2] = {0.0, 0.0};
+        if (I < nn) {
+          double rv[ND], z[ND];
+#pragma unroll
+          for (int i = 0; i < ND; ++i) {
+            const long long d = (long long)I * ND + i;
+            S.x64[d] += alpha * S.p64[d];
+            rv[i] = S.rest[d] ? 0.0 : S.r64[d] - alpha * S.q64[d];
+            S.r64[d] = rv[i];
+          }
+          prec64<ND>(S.minv, I, rv, z);
+#pragma unroll
+          for (int i = 0; i < ND; ++i) {
+            S.q64[(long long)I * ND + i] = z[i];
+            v[0] += rv[i] * z[i];
+            v[1] += rv[i] * rv[i];
+          }
+        }
+        slice_partial<2>(rz, nsl, s, v);
+      }
+      double a2[2];
+      if (!group_sum<2>(g, rz, nsl, a2)) return aborted();
+      st.iter += 1;
+      ++spent;
+      if (!(a2[0] == a2[0])) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
+      if (a2[1] <= (P.tol * st.bn) * (P.tol * st.bn) || st.iter >= P.maxit) {
+        // confirm with the true residual; restart the cycle from it if short
+        if (!b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w, g)) return aborted();
+        double a3[2];
+        if (!b_residual<ND>(S, g, part(), a3, false)) return aborted();
+        st.rn = sqrt(a3[0]);
+        st.repl += 1;
+        if (!(st.rn == st.rn)) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
+        if (st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; break; }
+        if (st.iter >= P.maxit || st.repl > P.max_repl) { st.phase = kPhaseDone; st.status = kBMaxit; break; }
+        double a4[2];
+        if (!b_rz64<ND>(S, g, part(), a4)) return aborted();
+        st.rho = a4[0];
+        st.rr = a4[1];
+        continue;
+      }
+      const double beta = a2[0] / st.rho;
+      st.rho = a2[0];
+      st.rr = a2[1];
+      for (int I = tid; I < nn; I += nt) {
+#pragma unroll
+        for (int i = 0; i < ND; ++i) {
+          const long long d = (long long)I * ND + i;
+          S.p64[d] = S.q64[d] + beta * S.p64[d];
+        }
+      }
+      if (!gsync(g)) return aborted();
+      continue;
+    }
+    // p_new = z + bt p_old, q = A p_new, p_new.q (one warp per 32-node
+    // slice).  With 1-2 dofs per node the update is formed inside the SpMV's
+    // gather (the warp keeps p_new of its own rows), saving a pass and a group
+    // barrier; with 3 dofs per node (27 columns per row) the doubled gather
+    // costs more than that, so p_new is written in a pass of its own.  Both
+    // give the same bits.
+    constexpr bool kFused = ND < 3;
+    float* pold = st.pb ? S.p32b : S.p32;
+    float* pnew = st.pb ? S.p32 : S.p32b;
+    const float bt0 = st.bt;
+    if constexpr (!kFused) {
+      for (int I = tid; I < nn; I += nt) {
+        float po[ND], zv[ND], pv[ND];
+        PVec<ND>::ld(pold, I, po);
+        PVec<ND>::ld(S.z32, I, zv);
+#pragma unroll
+        for (int i = 0; i < ND; ++i) pv[i] = fmaf(bt0, po[i], zv[i]);
+        PVec<ND>::st(pnew, I, pv);
+      }
+      if (!gsync(g)) return aborted();
+    }
     double* pq = part();
     for (int s = wid; s < nsl; s += nw) {
       float acc[ND];
-      spmv_row_b<ND, true, false>(A, s, lane, S.p32, acc);
+      if constexpr (kFused) spmv_row_fused<ND>(A, s, lane, pold, S.z32, bt0, acc);
+      else spmv_row_b<ND, true, false>(A, s, lane, pnew, acc);
       const int I = s * 32 + lane;
       double v[1] = {0.0};
       if (I < nn) {
         NodeIO<ND>::st(S.q32, I, acc);
         float pv[ND];
-        PVec<ND>::ld(S.p32, I, pv);
+        if constexpr (kFused) {
+          float po[ND], zv[ND];
+          PVec<ND>::ld(pold, I, po);
+          PVec<ND>::ld(S.z32, I, zv);
+#pragma unroll
+          for (int i = 0; i < ND; ++i) pv[i] = fmaf(bt0, po[i], zv[i]);
+          PVec<ND>::st(pnew, I, pv);
+        } else {
+          PVec<ND>::ld(pnew, I, pv);
+        }
         float t = 0.f;
 #pragma unroll
         for (int i = 0; i < ND; ++i) t = fmaf(pv[i], acc[i], t);
@@ -415,9 +621,10 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     }
     double a1[1];
     if (!group_sum<1>(g, pq, nsl, a1)) return aborted();
+    st.pb ^= 1;  // p_new is the current direction from here on
     if (!(a1[0] > 0.0 && a1[0] < 1e308)) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
     const float alpha = (float)(st.rho / a1[0]);
-    // y += alpha p, r -= alpha q, (r.z, r.r)
+    // y += alpha p, r -= alpha q, z = M r (kept for the next gather), (r.z, r.r)
     double* rz = part();
     for (int s = wid; s < nsl; s += nw) {
       const int I = 32 * s + lane;
@@ -426,7 +633,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
         float yv[ND], rv[ND], pv[ND], qv[ND], z[ND];
         NodeIO<ND>::ld(S.y32, I, yv);
         NodeIO<ND>::ld(S.r32, I, rv);
-        PVec<ND>::ld(S.p32, I, pv);
+        PVec<ND>::ld(pnew, I, pv);
         NodeIO<ND>::ld(S.q32, I, qv);
 #pragma unroll
         for (int i = 0; i < ND; ++i) {
@@ -436,6 +643,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
         NodeIO<ND>::st(S.y32, I, yv);
         NodeIO<ND>::st(S.r32, I, rv);
         NodeIO<ND>::prec(S.minv, I, rv, z);
+        PVec<ND>::st(S.z32, I, z);
 #pragma unroll
         for (int i = 0; i < ND; ++i) { v[0] += (double)rv[i] * z[i]; v[1] += (double)rv[i] * rv[i]; }
       }
@@ -448,7 +656,8 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     if (!(a2[0] == a2[0])) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
     double beta;
     if (a2[1] > st.maxrr) st.maxrr = a2[1];
-    if (a2[1] < tolabs2 || a2[1] < delta2 * st.maxrr || st.iter >= P.maxit) {
+    const bool long_cycle = P.switch_iters > 0 && st.iter - st.cycle0 >= P.switch_iters;
+    if (a2[1] < tolabs2 || a2[1] < delta2 * st.maxrr || st.iter >= P.maxit || long_cycle) {
       // reliable update: fold y into x, replace r by the FP64 true residual
       for (int i = tid; i < n; i += nt) { S.x64[i] += (double)S.y32[i]; S.y32[i] = 0.f; }
       if (!gsync(g)) return aborted();
@@ -460,8 +669,18 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
       if (!(st.rn == st.rn)) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
       if (st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; break; }
       if (st.iter >= P.maxit || st.repl > P.max_repl) { st.phase = kPhaseDone; st.status = kBMaxit; break; }
+      if (long_cycle) {
+        // the FP32 recurrences have lost their rate: continue in FP64 from x64, r64
+        st.mode = 1;
+        double a4[2];
+        if (!b_rz64<ND>(S, g, part(), a4)) return aborted();
+        st.rho = a4[0];
+        st.rr = st.maxrr = a4[1];
+        continue;
+      }
+      st.cycle0 = st.iter;
       double a4[2];
-      if (!b_rz<ND>(S, g, part(), a4, false)) return aborted();
+      if (!b_rz<ND>(S, g, part(), a4, false)) return aborted();  // z32 = M r of the new r
       beta = st.rho != 0.0 ? a4[0] / st.rho : 0.0;
       st.rho = a4[0];
       st.rr = st.maxrr = a4[1];
@@ -470,18 +689,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
       st.rho = a2[0];
       st.rr = a2[1];
     }
-    // p = M r + beta p
-    const float bt = (float)beta;
-    for (int I = tid; I < nn; I += nt) {
-      float rv[ND], pv[ND], z[ND];
-      NodeIO<ND>::ld(S.r32, I, rv);
-      PVec<ND>::ld(S.p32, I, pv);
-      NodeIO<ND>::prec(S.minv, I, rv, z);
-#pragma unroll
-      for (int i = 0; i < ND; ++i) pv[i] = fmaf(bt, pv[i], z[i]);
-      PVec<ND>::st(S.p32, I, pv);
-    }
-    if (!gsync(g)) return aborted();
+    st.bt = (float)beta;  // applied by the next SpMV's gather
   }
   if (tid == 0) *S.st = st;
   gsync(g);

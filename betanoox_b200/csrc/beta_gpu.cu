@@ -769,9 +769,13 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   D.x64 = (double*)(base + L.o_x64);
   D.r64 = (double*)(base + L.o_r64);
   D.y64 = (double*)(base + L.o_y64);
+  D.p64 = (double*)(base + L.o_p64);
+  D.q64 = (double*)(base + L.o_q64);
   D.y32 = (float*)(base + L.o_y32);
   D.r32 = (float*)(base + L.o_r32);
   D.p32 = (float*)(base + L.o_p32);
+  D.p32b = (float*)(base + L.o_p32b);
+  D.z32 = (float*)(base + L.o_z32);
   D.q32 = (float*)(base + L.o_q32);
   D.minv = (float*)(base + L.o_minv);
   D.part = (double*)(base + L.o_part);
@@ -1636,6 +1640,7 @@ int beta_gpu_batch_result(beta_gpu_batch* b, int id, double* u, beta_gpu_solve_s
     st->status = status;
     st->iterations = S.st.iter;
     st->outer_iterations = S.st.repl;
+    st->reserved = S.st.mode;  // 1: finished in FP64 (matrix-free) after the FP32 inner solve stalled
     st->final_norm = S.st.bn > 0 ? S.st.rn / S.st.bn : S.st.rn;
     st->true_rel_residual = st->final_norm;
   }
@@ -1711,6 +1716,12 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
   BCK(cudaStreamSynchronize(b->stream));
   if (threads_out) *threads_out = bt;
   if (boost_out) *boost_out = bg;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_set_switch(beta_gpu_batch* b, int iters_per_cycle) {
+  if (!b || iters_per_cycle < 0) return BETA_GPU_ERR_ARG;
+  b->switch_iters = iters_per_cycle;
   return BETA_GPU_OK;
 }
 

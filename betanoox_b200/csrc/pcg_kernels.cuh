@@ -357,7 +357,9 @@ struct BlockMat {
 
 // NC: gather x through the read-only cache (only when x is not written
 // during the kernel).
-template <int ND, bool PADDED, bool NC = true>
+// U: chunks whose loads are issued together (more bytes in flight per warp
+// for kernels with few warps per SM).
+template <int ND, bool PADDED, bool NC = true, int U = 2>
 __device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane, const float* x, float* acc) {
   constexpr int BB = ND * ND;
   const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
@@ -365,7 +367,7 @@ __device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane, c
   const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
 #pragma unroll
   for (int i = 0; i < ND; ++i) acc[i] = 0.f;
-#pragma unroll 2
+#pragma unroll U
   for (int k = 0; k < w; ++k) {
     const int J = __ldcs(cp + k * 32);
     float xv[ND];

@@ -299,6 +299,13 @@ BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta,
  * afterwards and keeps the shape with the least time per unit of work. */
 BETA_GPU_API int beta_gpu_batch_autotune(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int budget,
                                          int* threads_per_cta, int* gang_boost);
+/* Precision per system: a system whose FP32 inner solve needs more than
+ * iters_per_cycle iterations for one residual-replacement cycle (a drop of
+ * ||r|| by inner_tol) continues as FP64 Jacobi-PCG with the operator applied
+ * matrix-free in FP64 (stats->reserved = 1 in beta_gpu_batch_result);
+ * FP32 Krylov recurrences lose their convergence rate on ill-conditioned
+ * systems.  0: never.  Default 2000.  The choice depends only on the system. */
+BETA_GPU_API int beta_gpu_batch_set_switch(beta_gpu_batch* batch, int iters_per_cycle);
 /* The batch engine's CTA planner, exposed for inspection: for nsys systems
  * sorted by stored FP32 matrix values (largest first) with their 32-node
  * slice counts, fills gang_ctas[0..g) with the CTAs of each gang a launch of

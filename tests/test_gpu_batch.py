@@ -132,3 +132,28 @@ def test_result_independent_of_gang_size_and_cta_size():
         for (i0, u0), (i1, u1) in zip(out[0], other):
             assert i0 == i1
             np.testing.assert_array_equal(u0, u1)
+
+
+def test_fp64_switch_matches_oracle_and_is_mix_independent(oracle):
+    """A system whose FP32 cycles are long continues as FP64 matrix-free PCG;
+    its answer still meets the oracle and does not depend on the mix."""
+    plate = W.serve_request(99, 46)  # slender quad4 plate (~64k dofs, slow FP32 cycles)
+    small = W.plate_quad4(12)
+    models = [plate, W.rve_hex8(6, 1), small]
+    b = Batch(hbm_budget=1 << 30)
+    b.set_switch(40)
+    ids = [b.add(m) for m in models]
+    assert b.run(opts(tol=1e-12)) == 0
+    rc, u, st = b.result(ids[0])
+    assert rc == _abi.OK and st.reserved == 1, st.as_dict()
+    ut = _truth(oracle, plate)
+    assert np.linalg.norm(u - ut) / np.linalg.norm(ut) <= 1e-8
+    b1 = Batch(hbm_budget=1 << 30)
+    b1.set_switch(40)
+    i1 = b1.add(plate)
+    assert b1.run(opts(tol=1e-12), iters_per_launch=37) >= 0
+    while b1.run(opts(tol=1e-12), iters_per_launch=37) > 0:
+        pass
+    rc1, u1, st1 = b1.result(i1)
+    assert st1.iterations == st.iterations
+    np.testing.assert_array_equal(u, u1)
