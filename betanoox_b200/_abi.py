@@ -129,6 +129,7 @@ SIGNATURES = {
     "beta_gpu_batch_autotune": (_I, [_P, C.POINTER(SolveOpts), _I, C.POINTER(_I), C.POINTER(_I)]),
     "beta_gpu_batch_reset": (_I, [_P]),
     "beta_gpu_batch_set_switch": (_I, [_P, _I]),
+    "beta_gpu_batch_test_barrier": (_I, [_P, C.c_longlong, _I]),
     "beta_gpu_gang_plan": (_I, [_I, C.POINTER(C.c_longlong), C.POINTER(_I), _I, _I, _I, C.POINTER(_I)]),
     "beta_gpu_batch_info": (_I, [_P, C.POINTER(C.c_longlong), _I]),
     "beta_gpu_server_create": (_I, [C.POINTER(_P), _I, C.c_longlong, _I, C.POINTER(SolveOpts), _I, _I, _I]),

@@ -50,6 +50,10 @@ struct beta_gpu_batch {
   // a system whose FP32 inner solve needs more than this many iterations for
   // one residual-replacement cycle continues in FP64, matrix-free (0: never)
   int switch_iters = 2000;
+  // gang barrier wait limit, and the failure-path test hook (see
+  // beta_gpu_batch_test_barrier): plan the first gang one CTA larger than it gets
+  long long spin_ns = 2000000000LL;
+  int phantom = 0;
   int last_ngang = 0, last_gang_ctas = 0;
   std::map<int, cudaGraphExec_t> graphs;
   long long n_launch = 0, n_h2d = 0, n_d2h = 0;
@@ -309,8 +313,11 @@ int batch_plan(beta_gpu_batch* b, const int* act, int na, int nctas) {
   }
   const int ngang = gang_plan(na, work.data(), nsl.data(), nctas, b->threads / 32, b->gang_boost, g.data());
   int c = 0;
-  for (int i = 0; i < ngang; ++i)
-    for (int r = 0; r < g[i]; ++r, ++c) b->h_plan[c] = BPlan{i, r, g[i], i};
+  for (int i = 0; i < ngang; ++i) {
+    const int size = g[i] + (i == 0 && b->phantom ? 1 : 0);  // a member that never arrives
+    for (int r = 0; r < g[i]; ++r, ++c) b->h_plan[c] = BPlan{i, r, size, i};
+  }
+  b->phantom = 0;
   b->last_gang_ctas = c;
   for (; c < nctas; ++c) b->h_plan[c] = BPlan{-1, 0, 1, 0};
   b->last_ngang = ngang;
@@ -339,7 +346,7 @@ int batch_prepare(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, i
   P.budget = budget;
   P.nactive = na;
   P.nbig = ngang;
-  P.spin_ns = 2000000000LL;  // 2 s at one barrier: far beyond any phase of a resident gang
+  P.spin_ns = b->spin_ns;  // default 2 s at one barrier: far beyond any phase of a resident gang
   P.switch_iters = b->switch_iters;
   int rc;
   if (!b->sys.empty() && (rc = batch_h2d(b, b->d_sys, b->h_sys, sizeof(BSys) * b->sys.size()))) return rc;

@@ -1613,7 +1613,23 @@ int beta_gpu_batch_run(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int iter
     BCK(cudaEventRecord(b->ev0, b->stream));
     if ((rc = batch_launch_graph(b))) return rc;
     BCK(cudaEventRecord(b->ev1, b->stream));
-    if ((rc = batch_pull_states(b))) return rc;
+    if ((rc = batch_pull_states(b))) {
+      if (rc == BETA_GPU_TIMEOUT) {
+        // the launch stopped mid-iteration: unfinished systems restart from scratch next time
+        const std::string msg = b->err;
+        for (size_t i = 0; i < b->sys.size(); ++i)
+          if (b->sys[i].live && b->sys[i].st.phase != kPhaseDone) {
+            std::memset(&b->sys[i].st, 0, sizeof(BState));
+            b->sys[i].st.phase = kPhaseNew;
+            b->sys[i].st.status = kBRunning;
+          }
+        for (size_t i = 0; i < b->sys.size(); ++i) b->h_states[i] = b->sys[i].st;
+        if (!b->sys.empty() && batch_h2d(b, b->d_states, b->h_states, sizeof(BState) * b->sys.size()) == BETA_GPU_OK)
+          cudaStreamSynchronize(b->stream);
+        b->err = msg;
+      }
+      return rc;
+    }
     BCK(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
   }
   int left = 0;
@@ -1722,6 +1738,13 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
 int beta_gpu_batch_set_switch(beta_gpu_batch* b, int iters_per_cycle) {
   if (!b || iters_per_cycle < 0) return BETA_GPU_ERR_ARG;
   b->switch_iters = iters_per_cycle;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_test_barrier(beta_gpu_batch* b, long long limit_ns, int phantom) {
+  if (!b || limit_ns < 1000000LL || limit_ns > 10000000000LL) return BETA_GPU_ERR_ARG;
+  b->spin_ns = limit_ns;
+  b->phantom = phantom ? 1 : 0;
   return BETA_GPU_OK;
 }
 

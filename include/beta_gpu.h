@@ -306,6 +306,14 @@ BETA_GPU_API int beta_gpu_batch_autotune(beta_gpu_batch* batch, const beta_gpu_s
  * FP32 Krylov recurrences lose their convergence rate on ill-conditioned
  * systems.  0: never.  Default 2000.  The choice depends only on the system. */
 BETA_GPU_API int beta_gpu_batch_set_switch(beta_gpu_batch* batch, int iters_per_cycle);
+/* Failure-path test hook.  Sets the longest wait at a gang barrier (1 ms to
+ * 10 s; default 2 s) and, with phantom != 0, plans the first gang of the next
+ * launch one CTA larger than the CTAs it is given, so its first barrier can
+ * only end by running out of time: that launch stops and returns
+ * BETA_GPU_TIMEOUT, its unfinished systems restart from scratch on the next
+ * beta_gpu_batch_run, the context stays usable, and the hook clears itself.
+ * Not for production use. */
+BETA_GPU_API int beta_gpu_batch_test_barrier(beta_gpu_batch* batch, long long limit_ns, int phantom);
 /* The batch engine's CTA planner, exposed for inspection: for nsys systems
  * sorted by stored FP32 matrix values (largest first) with their 32-node
  * slice counts, fills gang_ctas[0..g) with the CTAs of each gang a launch of
