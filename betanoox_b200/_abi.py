@@ -110,6 +110,7 @@ SIGNATURES = {
     "beta_gpu_assemble": (_I, [_P, _I, _I, _D, _D]),
     "beta_gpu_matrix_lower_values": (_I, [_P, _I, _P, _P]),
     "beta_gpu_solve": (_I, [_P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "beta_gpu_solve_rhs": (_I, [_P, _P, _P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "beta_gpu_download": (_I, [_P, _P]),
     "beta_gpu_matvec": (_I, [_P, _I, _P, _P]),
     "beta_gpu_internal_force": (_I, [_P, _P, _P]),

@@ -168,6 +168,8 @@ struct beta_gpu_ctx {
   // solution / transient state
   DBuf<double> u, us;
   bool have_u = false, have_us = false;
+  DBuf<double> rhs_presc, rhs_load;  // beta_gpu_solve_rhs: the caller's right-hand side as prescribed/load
+  bool rhs_staged = false;           // b64 already holds the caller's right-hand side (FP64 mode)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> evs;
   int max_grid = 0;
@@ -1139,7 +1141,8 @@ int beta_gpu_solve(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve
   if (o->mode == BETA_GPU_MODE_FP64) {
     if (!c->have64) return fail(c, BETA_GPU_ERR_STATE, "assemble in FP64 before an FP64 solve");
     if (c->what64 != BETA_GPU_ASM_K) return fail(c, BETA_GPU_ERR_STATE, "static solve needs the K assembly");
-    launch(c, k_rhs64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, c->load.p, c->pseudo.p, c->b64.p);
+    if (!c->rhs_staged)
+      launch(c, k_rhs64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, c->load.p, c->pseudo.p, c->b64.p);
     if (last) CK(cudaMemcpyAsync(c->x64.p, c->u.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
     else CK(cudaMemsetAsync(c->x64.p, 0, sizeof(double) * n, c->stream));
     CKL("k_rhs64");
@@ -1185,6 +1188,49 @@ int beta_gpu_solve(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve
   if (status == BETA_GPU_MAXIT) c->err = "Solution not converged...";
   if (status == BETA_GPU_BREAKDOWN) c->err = "PCG breakdown (p.Ap <= 0 or non-finite)";
   return status;
+}
+
+int beta_gpu_solve_rhs(beta_gpu_ctx* c, const double* b, const double* x0, const beta_gpu_solve_opts* o,
+                       beta_gpu_solve_stats* stats) {
+  if (!c || !b || !o) return BETA_GPU_ERR_ARG;
+  if (c->ndof <= 0 || !c->have_bc) return fail(c, BETA_GPU_ERR_STATE, "mesh and restraints required");
+  cudaSetDevice(c->device);
+  const int n = c->ndof;
+  if (!all_finite(b, (size_t)n) || (x0 && !all_finite(x0, (size_t)n)))
+    return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite right-hand side or initial guess");
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  CK(c->rhs_presc.alloc(n));
+  CK(c->rhs_load.alloc(n));
+  CK(h2d(c, c->b64.p, b, sizeof(double) * n));
+  if (x0) {
+    CK(h2d(c, c->u.p, x0, sizeof(double) * n));
+    c->have_u = true;
+  }
+  beta_gpu_solve_opts o2 = *o;
+  o2.use_last_solution = x0 ? 1 : 0;
+  if (o->mode == BETA_GPU_MODE_FP64) {
+    // the scalar FP64 matrix is already eliminated: b is its right-hand side as is
+    c->rhs_staged = true;
+    rc = beta_gpu_solve(c, &o2, stats);
+    c->rhs_staged = false;
+    return rc;
+  }
+  // prescribed := b on restrained rows, load := b + K x_ext on free rows, so
+  // that the solver's right-hand side load - K x_ext equals b
+  CK(cudaMemcpyAsync(c->rhs_presc.p, c->b64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, (const double*)c->b64.p, (const double*)nullptr,
+         c->t64.p);
+  if ((rc = mf_apply(c, 1.0, c->t64.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
+  launch(c, k_load_from_rhs, grid_for(c, n, 256), 256, 0, n, c->rest.p, (const double*)c->b64.p,
+         (const double*)c->y64.p, c->rhs_load.p);
+  CKL("k_load_from_rhs");
+  std::swap(c->presc.p, c->rhs_presc.p);
+  std::swap(c->load.p, c->rhs_load.p);
+  rc = beta_gpu_solve(c, &o2, stats);
+  std::swap(c->presc.p, c->rhs_presc.p);
+  std::swap(c->load.p, c->rhs_load.p);
+  return rc;
 }
 
 int beta_gpu_download(beta_gpu_ctx* c, double* u) {

@@ -678,6 +678,14 @@ __global__ void k_rhs64(int n, const unsigned char* rest, const double* presc, c
     b[i] = rest[i] ? presc[i] : (load ? load[i] : 0.0) + (pseudo ? pseudo[i] : 0.0);
 }
 
+// The load that reproduces an eliminated right-hand side b: on free rows
+// b + (K x_ext)_free with x_ext = b on restrained rows (y holds K x_ext), 0 on
+// restrained rows (their value comes from the prescribed array).
+__global__ void k_load_from_rhs(int n, const unsigned char* rest, const double* b, const double* y, double* load) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    load[i] = rest[i] ? 0.0 : b[i] + y[i];
+}
+
 // x_ext = rest ? presc : (x ? x : 0)
 __global__ void k_ext64(int n, const unsigned char* rest, const double* presc, const double* x, double* out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)

@@ -197,6 +197,14 @@ BETA_GPU_API int beta_gpu_matrix_lower_values(beta_gpu_ctx* ctx, int precision, 
 BETA_GPU_API int beta_gpu_solve(beta_gpu_ctx* ctx, const beta_gpu_solve_opts* opts,
                    beta_gpu_solve_stats* stats);
 BETA_GPU_API int beta_gpu_download(beta_gpu_ctx* ctx, double* u);
+/* LargeMatrix::solve(b, x0) on the assembled system (sparse.cpp:114-242):
+ * b (host, ndof) is the eliminated right-hand side -- load + pseudo-load on
+ * free dofs, the prescribed value on restrained ones, as Equations::solve
+ * forms it (equation.cpp:1288-1405) -- and x0 (host, ndof, may be NULL) the
+ * initial guess.  Same opts, stats and status as beta_gpu_solve; the solution
+ * is read with beta_gpu_download. */
+BETA_GPU_API int beta_gpu_solve_rhs(beta_gpu_ctx* ctx, const double* b, const double* x0,
+                                    const beta_gpu_solve_opts* opts, beta_gpu_solve_stats* stats);
 
 /* y = A x with the assembled matrix of `precision` (SymmetricSparseMatrix::
  * vectorProduct, sparse.cpp:452-478), host vectors of length ndof. */
