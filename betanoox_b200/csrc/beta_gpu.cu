@@ -146,6 +146,7 @@ struct beta_gpu_ctx {
   bool have_bc = false;
   // structure
   bool have_pattern = false;
+  bool have_scalar = false;  // scalar FP64 layout built and uploaded
   HostPattern P;
   DBuf<int> elems, slot, nrp, bsoff, bcol, ndiag, soff, scol;
   DBuf<long long> ssoff, sdiag;
@@ -1001,8 +1002,10 @@ int beta_gpu_build_pattern(beta_gpu_ctx* c, long long* nnz_lower) {
   if (!c) return BETA_GPU_ERR_ARG;
   if (!c->ndof || !c->have_bc) return fail(c, BETA_GPU_ERR_STATE, "upload mesh and boundary conditions first");
   cudaSetDevice(c->device);
+  // node-level structure only: the scalar FP64 layout is built the first
+  // time an FP64 assembly needs it (ensure_scalar)
   std::string msg = build_pattern(c->nnode, c->nelem, c->nnpe, c->ndpn, c->h_conn.data(), c->h_first_dof.data(),
-                                  c->h_rest.data(), c->P);
+                                  c->h_rest.data(), c->P, false);
   if (!msg.empty()) return fail(c, BETA_GPU_ERR_UNSUPPORTED, msg);
   const HostPattern& P = c->P;
   int rc;
@@ -1012,12 +1015,9 @@ int beta_gpu_build_pattern(beta_gpu_ctx* c, long long* nnz_lower) {
   if ((rc = upload(c, c->bsoff, P.bsoff.data(), P.bsoff.size()))) return rc;
   if ((rc = upload(c, c->bcol, P.bcol.data(), P.bcol.size()))) return rc;
   if ((rc = upload(c, c->ndiag, P.ndiag.data(), P.ndiag.size()))) return rc;
-  if ((rc = upload(c, c->soff, P.soff.data(), P.soff.size()))) return rc;
-  if ((rc = upload(c, c->ssoff, P.ssoff.data(), P.ssoff.size()))) return rc;
-  if ((rc = upload(c, c->scol, P.scol.data(), P.scol.size()))) return rc;
-  if ((rc = upload(c, c->sdiag, P.sdiag.data(), P.sdiag.size()))) return rc;
   CK(cudaStreamSynchronize(c->stream));
   c->have_pattern = true;
+  c->have_scalar = false;
   invalidate_matrices(c);
   if (nnz_lower) *nnz_lower = P.nnz_lower;
   return BETA_GPU_OK;
@@ -1062,6 +1062,19 @@ int beta_gpu_assemble(beta_gpu_ctx* c, int what, int precision, double dt, doubl
   CK(cudaMemsetAsync(c->flags.p, 0, sizeof(unsigned), c->stream));
   int rc;
   if (precision == BETA_GPU_FP64) {
+    if (!c->have_scalar) {
+      std::string m2 = build_scalar(c->P, c->h_rest.data());
+      if (!m2.empty()) return fail(c, BETA_GPU_ERR_UNSUPPORTED, m2);
+      const HostPattern& P = c->P;
+      if ((rc = upload(c, c->soff, P.soff.data(), P.soff.size()))) return rc;
+      if ((rc = upload(c, c->ssoff, P.ssoff.data(), P.ssoff.size()))) return rc;
+      if ((rc = upload(c, c->scol, P.scol.data(), P.scol.size()))) return rc;
+      if ((rc = upload(c, c->sdiag, P.sdiag.data(), P.sdiag.size()))) return rc;
+      CK(cudaStreamSynchronize(c->stream));
+      c->have_scalar = true;
+    }
+    A.soff = c->soff.p;
+    A.ssoff = c->ssoff.p;
     CK(c->sval.alloc(c->P.ssoff.back()));
     CK(c->pseudo.alloc(c->ndof));
     CK(cudaMemsetAsync(c->sval.p, 0, sizeof(double) * c->sval.n, c->stream));

@@ -145,30 +145,9 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     }
   });
 
-  // ---- scalar sliced ELL over dofs ------------------------------------
-  if (!with_scalar) return "";
-  const int ndof = P.ndof;
-  std::vector<int> ufree(nnode, 0);
-  for (int i = 0; i < nnode; ++i)
-    for (int j = 0; j < ndpn; ++j) ufree[i] += rest[ndpn * i + j] ? 0 : 1;
-  P.soff.resize(P.nblk);
-  std::vector<int> nodelen(nnode);
-  parallel_for(nnode, [&](long long lo, long long hi) {
-    for (long long i = lo; i < hi; ++i) {
-      int acc = 0;
-      for (int k = P.nrp[i]; k < P.nrp[i + 1]; ++k) { P.soff[k] = acc; acc += ufree[P.ncol[k]]; }
-      nodelen[i] = acc;
-    }
-  });
-  P.srowlen.resize(ndof);
-  P.nnz_full = 0;
-  P.nnz_lower = 0;
-  for (int r = 0; r < ndof; ++r) {
-    P.srowlen[r] = rest[r] ? 1 : nodelen[r / ndpn];
-    P.nnz_full += P.srowlen[r];
-  }
-  // lower count per free row: free columns c <= r in the node's row
+  // ---- the reference's lower-triangle count --------------------------
   {
+    const int ndof = P.ndof;
     std::vector<long long> lower(ndof, 0);
     parallel_for(nnode, [&](long long lo, long long hi) {
       for (long long I = lo; I < hi; ++I)
@@ -186,7 +165,33 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
           lower[r] = cnt ? cnt : 1;
         }
     });
+    P.nnz_lower = 0;
     for (int r = 0; r < ndof; ++r) P.nnz_lower += lower[r];
+  }
+  if (!with_scalar) return "";
+  return build_scalar(P, rest);
+}
+
+std::string build_scalar(HostPattern& P, const unsigned char* rest) {
+  const int nnode = P.nnode, ndpn = P.ndpn;
+  const int ndof = P.ndof;
+  std::vector<int> ufree(nnode, 0);
+  for (int i = 0; i < nnode; ++i)
+    for (int j = 0; j < ndpn; ++j) ufree[i] += rest[ndpn * i + j] ? 0 : 1;
+  P.soff.resize(P.nblk);
+  std::vector<int> nodelen(nnode);
+  parallel_for(nnode, [&](long long lo, long long hi) {
+    for (long long i = lo; i < hi; ++i) {
+      int acc = 0;
+      for (int k = P.nrp[i]; k < P.nrp[i + 1]; ++k) { P.soff[k] = acc; acc += ufree[P.ncol[k]]; }
+      nodelen[i] = acc;
+    }
+  });
+  P.srowlen.resize(ndof);
+  P.nnz_full = 0;
+  for (int r = 0; r < ndof; ++r) {
+    P.srowlen[r] = rest[r] ? 1 : nodelen[r / ndpn];
+    P.nnz_full += P.srowlen[r];
   }
   P.nsslice = (ndof + 31) / 32;
   P.ssoff.assign(P.nsslice + 1, 0);

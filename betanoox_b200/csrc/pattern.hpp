@@ -61,10 +61,15 @@ struct HostPattern {
 
 // Builds everything above.  conn: nelem*nnpe; restrained: ndof (0/1).
 // Returns an empty string on success, else an error message.
-// with_scalar = false skips the scalar FP64 layout (mixed-precision-only users).
+// with_scalar = false skips the scalar FP64 layout (mixed-precision-only
+// users; build_scalar adds it later).  nnz_lower is always computed.
 std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* conn,
                           const int* first_dof, const unsigned char* restrained, HostPattern& P,
                           bool with_scalar = true);
+
+// The scalar FP64 layout (soff, srowlen, nnz_full, ssoff, scol, sdiag) for a
+// pattern built without it.  Returns an empty string on success.
+std::string build_scalar(HostPattern& P, const unsigned char* restrained);
 
 // Makes build_pattern on the calling thread single-threaded (for callers that
 // already build many patterns in parallel).
