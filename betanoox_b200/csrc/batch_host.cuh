@@ -137,7 +137,7 @@ SysLayout layout_for(int ndim, int nnode, int nelem, int nnpe, int ndpn, int ngr
   L.o_load = L.add(sizeof(double) * ndof);
   L.o_cptr = L.add(sizeof(int) * (P.ncolor + 1));
   L.o_elems = L.add(sizeof(int) * nelem);
-  L.o_slot = L.add(sizeof(int) * P.slot.size());
+  L.o_slot = L.add(sizeof(uint16_t) * P.slot.size());
   L.o_nrp = L.add(sizeof(int) * P.nrp.size());
   L.o_ndiag = L.add(sizeof(int) * P.ndiag.size());
   L.o_bsoff = L.add(sizeof(int) * P.bsoff.size());

@@ -59,7 +59,7 @@ struct BSys {
   const double* load;
   const int* color_ptr;  // ncolor+1 offsets into elems
   const int* elems;
-  const int* slot;
+  const uint16_t* slot;  // position of node J in node I's graph row, per element node pair
   const int* nrp;
   const int* ndiag;
   const int* bsoff;

@@ -148,7 +148,8 @@ struct beta_gpu_ctx {
   bool have_pattern = false;
   bool have_scalar = false;  // scalar FP64 layout built and uploaded
   HostPattern P;
-  DBuf<int> elems, slot, nrp, bsoff, bcol, ndiag, soff, scol;
+  DBuf<int> elems, nrp, bsoff, bcol, ndiag, soff, scol;
+  DBuf<uint16_t> slot;
   DBuf<long long> ssoff, sdiag;
   // matrices
   DBuf<double> sval, pseudo;
@@ -730,7 +731,7 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   up(L.o_load, Q.load.data(), sizeof(double) * ndof);
   up(L.o_cptr, P.color_ptr.data(), sizeof(int) * P.color_ptr.size());
   up(L.o_elems, P.elem_by_color.data(), sizeof(int) * P.elem_by_color.size());
-  up(L.o_slot, P.slot.data(), sizeof(int) * P.slot.size());
+  up(L.o_slot, P.slot.data(), sizeof(uint16_t) * P.slot.size());
   up(L.o_nrp, P.nrp.data(), sizeof(int) * P.nrp.size());
   up(L.o_ndiag, P.ndiag.data(), sizeof(int) * P.ndiag.size());
   up(L.o_bsoff, P.bsoff.data(), sizeof(int) * P.bsoff.size());
@@ -763,7 +764,7 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   D.load = (const double*)(base + L.o_load);
   D.color_ptr = (const int*)(base + L.o_cptr);
   D.elems = (const int*)(base + L.o_elems);
-  D.slot = (const int*)(base + L.o_slot);
+  D.slot = (const uint16_t*)(base + L.o_slot);
   D.nrp = (const int*)(base + L.o_nrp);
   D.ndiag = (const int*)(base + L.o_ndiag);
   D.bsoff = (const int*)(base + L.o_bsoff);

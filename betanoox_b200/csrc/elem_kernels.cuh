@@ -29,7 +29,7 @@ struct ElemArgs {
   int nparams;
   int nip;
   const GaussTable* gt;       // device
-  const int* slot;            // nelem*nnpe*nnpe node-pair block index
+  const uint16_t* slot;       // nelem*nnpe*nnpe: position of node J in node I's graph row
   const int* nrp;             // node graph row pointers
   const unsigned char* rest;  // ndof
   const double* presc;        // ndof
@@ -63,9 +63,8 @@ __device__ __forceinline__ void stage_gauss(const GaussTable* gt, int nip, T* s_
 // entry (i,j) at chunk*32*ND*ND + (i*ND+j)*32 + I%32.  Restrained rows and
 // columns stay zero; their diagonal is set to 1 afterwards (equation.cpp:500).
 template <int ND>
-__device__ __forceinline__ void scatter_block32(const ElemArgs& A, int I, int J, int blk,
+__device__ __forceinline__ void scatter_block32(const ElemArgs& A, int I, int J, int pos,
                                                 const float* K) {
-  const int pos = blk - A.nrp[I];
   const long long chunk = (long long)A.bsoff[I >> 5] + pos;
   float* base = A.bval + chunk * (32 * ND * ND) + (I & 31);
 #pragma unroll
@@ -84,9 +83,9 @@ __device__ __forceinline__ void scatter_block32(const ElemArgs& A, int I, int J,
 // as F[I] -= K_IJ * u_J (equation.cpp:499-503).  Returns the row partials of
 // the pseudo load in pl[ND].
 template <int ND>
-__device__ __forceinline__ void scatter_block64(const ElemArgs& A, int I, int J, int blk,
+__device__ __forceinline__ void scatter_block64(const ElemArgs& A, int I, int J, int pos,
                                                 const double* K, double* pl) {
-  const int kb = A.soff[blk];
+  const int kb = A.soff[A.nrp[I] + pos];
 #pragma unroll
   for (int i = 0; i < ND; ++i) {
     pl[i] = 0.0;
@@ -177,7 +176,7 @@ __device__ __forceinline__ void asm_hex8_elastic_warp(const ElemArgs& A, const i
 
     const int I0 = __shfl_sync(0xffffffffu, J, a0);
     const int I1 = __shfl_sync(0xffffffffu, J, a1);
-    const int* sl = A.slot + (long long)e * 64;
+    const uint16_t* sl = A.slot + (long long)e * 64;
     if constexpr (sizeof(T) == 4) {
       scatter_block32<3>(A, I0, J, sl[a0 * 8 + b], K0);
       scatter_block32<3>(A, I1, J, sl[a1 * 8 + b], K1);
@@ -253,7 +252,7 @@ __device__ __forceinline__ void asm_quad4_pstress_warp(const ElemArgs& A, const 
     }
     if (valid && a == b && !(K[0] > 0 && K[3] > 0)) atomicOr(A.flags, kFlagNegDiag);
     const int I = __shfl_sync(0xffffffffu, J, src);
-    const int blk = A.slot[(long long)e * 16 + a * 4 + b];
+    const int blk = A.slot[(long long)e * 16 + a * 4 + b];  // position in node I's row
     if constexpr (sizeof(T) == 4) {
       if (valid) scatter_block32<2>(A, I, J, blk, K);
     } else {
@@ -330,7 +329,7 @@ __device__ __forceinline__ void asm_hex8_heat_warp(const ElemArgs& A, const int*
     T K1[1] = {T(A.kscale) * Kk[1] + T(A.mscale) * Km[1]};
     const int I0 = __shfl_sync(0xffffffffu, J, a0);
     const int I1 = __shfl_sync(0xffffffffu, J, a1);
-    const int* sl = A.slot + (long long)e * 64;
+    const uint16_t* sl = A.slot + (long long)e * 64;
     if constexpr (sizeof(T) == 4) {
       scatter_block32<1>(A, I0, J, sl[a0 * 8 + b], K0);
       scatter_block32<1>(A, I1, J, sl[a1 * 8 + b], K1);

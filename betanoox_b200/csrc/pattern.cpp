@@ -48,22 +48,30 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   }
 
   // ---- node graph (two passes: count, then fill) ---------------------
-  auto collect = [&](int i, std::vector<int>& buf) {
+  // Neighbours of node i are deduplicated with a per-thread marker array
+  // (mark[J] == i + 1 once J is taken), so only the distinct ones are sorted.
+  auto collect = [&](int i, std::vector<int>& buf, std::vector<int>& mark, bool sorted) {
     buf.clear();
     for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
       const int* ce = conn + (long long)inc[k] * nnpe;
-      for (int a = 0; a < nnpe; ++a) buf.push_back(ce[a]);
+      for (int a = 0; a < nnpe; ++a) {
+        const int J = ce[a];
+        if (mark[J] != i + 1) {
+          mark[J] = i + 1;
+          buf.push_back(J);
+        }
+      }
     }
     if (buf.empty()) buf.push_back(i);  // a node in no element keeps its diagonal
-    std::sort(buf.begin(), buf.end());
-    buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+    if (sorted) std::sort(buf.begin(), buf.end());
   };
   P.nrp.assign(nnode + 1, 0);
   parallel_for(nnode, [&](long long lo, long long hi) {
-    std::vector<int> buf;
-    for (long long i = lo; i < hi; ++i) { collect((int)i, buf); P.nrp[i + 1] = (int)buf.size(); }
+    std::vector<int> buf, mark(nnode, 0);
+    for (long long i = lo; i < hi; ++i) { collect((int)i, buf, mark, false); P.nrp[i + 1] = (int)buf.size(); }
   });
   for (int i = 0; i < nnode; ++i) {
+    if (P.nrp[i + 1] > 65535) return "build_pattern: a node with more than 65535 neighbours";
     if ((long long)P.nrp[i] + P.nrp[i + 1] > 2000000000LL) return "build_pattern: node graph too large";
     P.nrp[i + 1] += P.nrp[i];
   }
@@ -71,9 +79,9 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   P.ncol.resize(P.nblk);
   P.ndiag.resize(nnode);
   parallel_for(nnode, [&](long long lo, long long hi) {
-    std::vector<int> buf;
+    std::vector<int> buf, mark(nnode, 0);
     for (long long i = lo; i < hi; ++i) {
-      collect((int)i, buf);
+      collect((int)i, buf, mark, true);
       std::copy(buf.begin(), buf.end(), P.ncol.begin() + P.nrp[i]);
       P.ndiag[i] = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
     }
@@ -106,16 +114,29 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   // ---- element -> node-pair block map --------------------------------
   const int npair = nnpe * nnpe;
   P.slot.resize((size_t)nelem * npair);
+  // The element's nodes are sorted once; each row is then walked once
+  // alongside them (a merge) instead of searched per pair.
   parallel_for(nelem, [&](long long lo, long long hi) {
+    int ord[8], sv[8];
     for (long long e = lo; e < hi; ++e) {
       const int* ce = conn + e * nnpe;
+      for (int b = 0; b < nnpe; ++b) {  // insertion sort of the element's <= 8 nodes
+        int t = b;
+        while (t > 0 && sv[t - 1] > ce[b]) {
+          sv[t] = sv[t - 1];
+          ord[t] = ord[t - 1];
+          --t;
+        }
+        sv[t] = ce[b];
+        ord[t] = b;
+      }
       for (int a = 0; a < nnpe; ++a) {
         const int I = ce[a];
-        const int* rb = P.ncol.data() + P.nrp[I];
-        const int* re = P.ncol.data() + P.nrp[I + 1];
-        for (int b = 0; b < nnpe; ++b) {
-          const int* it = std::lower_bound(rb, re, ce[b]);
-          P.slot[e * npair + a * nnpe + b] = (int)(it - P.ncol.data());
+        const int rb = P.nrp[I], re = P.nrp[I + 1];
+        int k = rb;
+        for (int t = 0; t < nnpe; ++t) {
+          while (k < re && P.ncol[k] < sv[t]) ++k;  // every element node is in row I
+          P.slot[e * npair + a * nnpe + ord[t]] = (uint16_t)(k - rb);
         }
       }
     }
@@ -146,27 +167,40 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   });
 
   // ---- the reference's lower-triangle count --------------------------
+  // A free row r = I*ndpn + i holds the free dofs c <= r of its node row: all
+  // free dofs of the neighbours J < I (the row is sorted, so those before the
+  // diagonal) and the free dofs j <= i of I itself; a restrained row holds its
+  // diagonal only.
   {
-    const int ndof = P.ndof;
-    std::vector<long long> lower(ndof, 0);
-    parallel_for(nnode, [&](long long lo, long long hi) {
-      for (long long I = lo; I < hi; ++I)
-        for (int i = 0; i < ndpn; ++i) {
-          int r = (int)I * ndpn + i;
-          if (rest[r]) { lower[r] = 1; continue; }
-          long long cnt = 0;
-          for (int k = P.nrp[I]; k < P.nrp[I + 1]; ++k) {
-            int J = P.ncol[k];
-            for (int j = 0; j < ndpn; ++j) {
-              int c = J * ndpn + j;
-              if (!rest[c] && c <= r) ++cnt;
+    std::vector<int> ufree(nnode, 0);
+    for (int I = 0; I < nnode; ++I)
+      for (int j = 0; j < ndpn; ++j) ufree[I] += rest[ndpn * I + j] ? 0 : 1;
+    unsigned hw = std::thread::hardware_concurrency();
+    const int nt = (int)std::max(1u, std::min(hw ? hw : 1u, 64u));
+    std::vector<long long> part(nt, 0);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+      th.emplace_back([&, t]() {
+        long long acc = 0;
+        for (long long I = (long long)nnode * t / nt; I < (long long)nnode * (t + 1) / nt; ++I) {
+          long long below = 0;
+          for (int k = P.nrp[I]; k < P.nrp[I] + P.ndiag[I]; ++k) below += ufree[P.ncol[k]];
+          int own = 0;
+          for (int i = 0; i < ndpn; ++i) {
+            const long long r = I * ndpn + i;
+            if (rest[r]) {
+              acc += 1;
+            } else {
+              ++own;
+              acc += below + own;
             }
           }
-          lower[r] = cnt ? cnt : 1;
         }
-    });
+        part[t] = acc;
+      });
+    for (auto& x : th) x.join();
     P.nnz_lower = 0;
-    for (int r = 0; r < ndof; ++r) P.nnz_lower += lower[r];
+    for (long long v : part) P.nnz_lower += v;
   }
   if (!with_scalar) return "";
   return build_scalar(P, rest);

@@ -5,8 +5,9 @@
 //   * node graph: for every node the sorted set of nodes sharing an element;
 //   * element colouring: no two elements of one colour share a node, so the
 //     device scatter needs no atomics and sums in a fixed order;
-//   * element->slot map: for element e and local node pair (a,b) the index of
-//     the node-pair block (conn[e][a], conn[e][b]) in the node graph;
+//   * element->slot map: for element e and local node pair (a,b) the position
+//     of node conn[e][b] in node conn[e][a]'s graph row (16 bits; a block's
+//     index is nrp[I] + position);
 //   * two sliced-ELL layouts of the global matrix (32 rows per slice, entry
 //     (row, k) stored at slice_base + k*32 + row%32 so a warp reads 128-byte
 //     lines): node-block rows for the FP32 inner solver and scalar DOF rows
@@ -35,8 +36,8 @@ struct HostPattern {
   std::vector<int> color_ptr;     // ncolor+1
   std::vector<int> elem_by_color; // nelem
 
-  // element -> node-pair block index, nelem * nnpe * nnpe
-  std::vector<int> slot;
+  // element -> position of node J in node I's row, nelem * nnpe * nnpe
+  std::vector<uint16_t> slot;
 
   // node-block sliced ELL: slice s covers nodes [32s, 32s+32)
   int nslice = 0;
