@@ -15,7 +15,7 @@ import numpy as np
 from . import _abi
 from ._abi import BetaGpuError, SolveOpts, SolveStats
 
-__all__ = ["Solver", "Batch", "Server", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
+__all__ = ["Solver", "Batch", "Server", "write_lower", "read_lower", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
 
 
 def build(force: bool = False) -> str:
@@ -103,6 +103,10 @@ class Solver:
     def assemble(self, precision=_abi.FP32, what=_abi.ASM_K, dt=0.0, alpha=1.0):
         self._check(self.lib.beta_gpu_assemble(self.h, what, precision, dt, alpha), "assemble")
 
+    def export_matrix(self, path, fmt, precision=_abi.FP64):
+        """Writes the assembled matrix in one of BETA's exchange formats."""
+        self._check(self.lib.beta_gpu_export_matrix(self.h, precision, int(fmt), str(path).encode()), "export_matrix")
+
     def lower_values(self, precision):
         vals = np.zeros(self.nnz_lower)
         pl = np.zeros(self.model.ndof)
@@ -151,6 +155,34 @@ class Solver:
         u = np.zeros(self.model.ndof)
         self._check(self.lib.beta_gpu_heat_get_state(self.h, _ptr(u)), "heat_get_state")
         return u
+
+
+def write_lower(path, fmt, row_ptr, col, val):
+    """Writes a lower triangle in one of BETA's exchange formats (_abi.FMT_*)."""
+    lib = _abi.load()
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    c = np.ascontiguousarray(col, dtype=np.int32)
+    v = np.ascontiguousarray(val, dtype=np.float64)
+    st = lib.beta_gpu_write_lower(str(path).encode(), int(fmt), len(rp) - 1, _ptr(rp), _ptr(c), _ptr(v))
+    if st != _abi.OK:
+        raise BetaGpuError(st, f"write_lower {path}")
+
+
+def read_lower(path, fmt):
+    """Reads a lower triangle written in one of BETA's exchange formats: (row_ptr, col, val)."""
+    lib = _abi.load()
+    n, nnz = C.c_int(0), C.c_longlong(0)
+    st = lib.beta_gpu_read_lower(str(path).encode(), int(fmt), C.byref(n), C.byref(nnz), None, None, None)
+    if st != _abi.OK:
+        raise BetaGpuError(st, f"read_lower {path}")
+    rp = np.zeros(n.value + 1, np.int64)
+    col = np.zeros(nnz.value, np.int32)
+    val = np.zeros(nnz.value)
+    st = lib.beta_gpu_read_lower(str(path).encode(), int(fmt), C.byref(n), C.byref(nnz), _ptr(rp), _ptr(col),
+                                 _ptr(val))
+    if st != _abi.OK:
+        raise BetaGpuError(st, f"read_lower {path}")
+    return rp, col, val
 
 
 class Batch:

@@ -29,6 +29,13 @@ ERR_UNSUPPORTED = 13
 ERR_TOO_LARGE = 14
 NOALLOC_MAX_ROWS = 262144
 
+# system exchange formats
+FMT_ADDRESS_LOWER = 1
+FMT_ADDRESS_UPPER = 2
+FMT_COMPRESSED_ROW = 3
+FMT_CSR_ASCII = 4
+FMT_CSR_BINARY = 5
+
 # server request states
 REQ_QUEUED = 0
 REQ_RUNNING = 1
@@ -111,6 +118,9 @@ SIGNATURES = {
     "beta_gpu_matrix_lower_values": (_I, [_P, _I, _P, _P]),
     "beta_gpu_solve": (_I, [_P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "beta_gpu_solve_rhs": (_I, [_P, _P, _P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "beta_gpu_write_lower": (_I, [C.c_char_p, _I, _I, _P, _P, _P]),
+    "beta_gpu_read_lower": (_I, [C.c_char_p, _I, C.POINTER(_I), C.POINTER(C.c_longlong), _P, _P, _P]),
+    "beta_gpu_export_matrix": (_I, [_P, _I, _I, C.c_char_p]),
     "beta_gpu_download": (_I, [_P, _P]),
     "beta_gpu_matvec": (_I, [_P, _I, _P, _P]),
     "beta_gpu_internal_force": (_I, [_P, _P, _P]),

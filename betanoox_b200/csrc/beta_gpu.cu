@@ -1044,6 +1044,21 @@ int beta_gpu_pattern_lower_host(int nnode, int nelem, int nnpe, int ndpn, const 
   return BETA_GPU_OK;
 }
 
+int beta_gpu_export_matrix(beta_gpu_ctx* c, int precision, int format, const char* path) {
+  if (!c || !path) return BETA_GPU_ERR_ARG;
+  if (!c->have_pattern) return fail(c, BETA_GPU_ERR_STATE, "build the pattern first");
+  const size_t n = c->ndof;
+  std::vector<long long> rp(n + 1);
+  std::vector<int> col(c->P.nnz_lower);
+  std::vector<double> val(c->P.nnz_lower);
+  export_lower_pattern(c->P, c->h_rest.data(), rp.data(), col.data());
+  int rc = beta_gpu_matrix_lower_values(c, precision, val.data(), nullptr);
+  if (rc != BETA_GPU_OK) return rc;
+  rc = beta_gpu_write_lower(path, format, (int)n, rp.data(), col.data(), val.data());
+  if (rc != BETA_GPU_OK) return fail(c, rc, "writing the matrix failed");
+  return BETA_GPU_OK;
+}
+
 int beta_gpu_assemble(beta_gpu_ctx* c, int what, int precision, double dt, double alpha) {
   if (!c) return BETA_GPU_ERR_ARG;
   if (!c->have_pattern || !c->have_mat) return fail(c, BETA_GPU_ERR_STATE, "pattern and materials required");

@@ -215,6 +215,31 @@ BETA_GPU_API int beta_gpu_matvec(beta_gpu_ctx* ctx, int precision, const double*
  * restrained-row skip): host u[ndof] -> host f[ndof]. */
 BETA_GPU_API int beta_gpu_internal_force(beta_gpu_ctx* ctx, const double* u, double* f);
 
+/* ---- system exchange formats -------------------------------------------- */
+/* The lower triangle of a symmetric matrix (SymmetricSparseMatrix order: rows
+ * ascending, columns ascending, diagonal last) in BETA's dump layouts, for
+ * cross-checks against external solvers:
+ *   ADDRESS_LOWER  printMatrixAddressFormat (sparse.cpp:295-325)
+ *   ADDRESS_UPPER  printMatrixAddressFormatUpper (sparse.cpp:263-293)
+ *   COMPRESSED_ROW printCompressedRowFormat (sparse.cpp:327-355)
+ *   CSR_ASCII      writeCSRMatrixInASCII / readCSRMatrixInASCII (SparseMatrixUtility.cpp:11-26, 60-78)
+ *   CSR_BINARY     writeCSRMatrixInBinary / readCSRMatrixInBinary (SparseMatrixUtility.cpp:28-58)
+ * The CSR files hold the lower triangle's 0-based row pointers and columns as
+ * 32-bit ints (BETA_GPU_ERR_TOO_LARGE beyond 2^31-1 entries).  Host only. */
+#define BETA_GPU_FMT_ADDRESS_LOWER 1
+#define BETA_GPU_FMT_ADDRESS_UPPER 2
+#define BETA_GPU_FMT_COMPRESSED_ROW 3
+#define BETA_GPU_FMT_CSR_ASCII 4
+#define BETA_GPU_FMT_CSR_BINARY 5
+BETA_GPU_API int beta_gpu_write_lower(const char* path, int format, int n, const long long* row_ptr, const int* col,
+                                      const double* val);
+/* Reads a file written in `format`: call with row_ptr/col/val NULL for n and
+ * nnz, then with arrays of n+1, nnz, nnz. */
+BETA_GPU_API int beta_gpu_read_lower(const char* path, int format, int* n, long long* nnz, long long* row_ptr,
+                                     int* col, double* val);
+/* Writes the assembled matrix of `precision` (FP32 values widened). */
+BETA_GPU_API int beta_gpu_export_matrix(beta_gpu_ctx* ctx, int precision, int format, const char* path);
+
 /* ---- transient diffusion (DiffusionModel::DoTransientNonLinearAnalysis) -- */
 /* Sets u_s (host, ndof) as the current field. */
 BETA_GPU_API int beta_gpu_heat_set_state(beta_gpu_ctx* ctx, const double* u0);
