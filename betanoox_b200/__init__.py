@@ -15,7 +15,7 @@ import numpy as np
 from . import _abi
 from ._abi import BetaGpuError, SolveOpts, SolveStats
 
-__all__ = ["Solver", "Batch", "Server", "write_lower", "read_lower", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
+__all__ = ["Solver", "Batch", "Server", "write_lower", "read_lower", "read_mesh", "write_mesh", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
 
 
 def build(force: bool = False) -> str:
@@ -183,6 +183,34 @@ def read_lower(path, fmt):
     if st != _abi.OK:
         raise BetaGpuError(st, f"read_lower {path}")
     return rp, col, val
+
+
+def read_mesh(path, binary=False):
+    """Reads a BETA mesh file: (xyz[nnode, ndim], conn[nelem, nnpe]) with
+    0-based node indices in BETA's local order."""
+    lib = _abi.load()
+    nd, nn, ne, npe = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    args = (str(path).encode(), int(bool(binary)), C.byref(nd), C.byref(nn), C.byref(ne), C.byref(npe))
+    st = lib.beta_gpu_read_mesh(*args, None, None)
+    if st != _abi.OK:
+        raise BetaGpuError(st, f"read_mesh {path}")
+    xyz = np.zeros((nn.value, nd.value))
+    conn = np.zeros((ne.value, npe.value), np.int32)
+    st = lib.beta_gpu_read_mesh(*args, _ptr(xyz), _ptr(conn))
+    if st != _abi.OK:
+        raise BetaGpuError(st, f"read_mesh {path}")
+    return xyz, conn
+
+
+def write_mesh(path, xyz, conn, binary=False, first_number=1):
+    """Writes a mesh in BETA's mesh-file layout (nodes and elements numbered from first_number)."""
+    lib = _abi.load()
+    x = np.ascontiguousarray(xyz, dtype=np.float64)
+    c = np.ascontiguousarray(conn, dtype=np.int32)
+    st = lib.beta_gpu_write_mesh(str(path).encode(), int(bool(binary)), x.shape[1], x.shape[0], _ptr(x), c.shape[0],
+                                 c.shape[1], _ptr(c), int(first_number))
+    if st != _abi.OK:
+        raise BetaGpuError(st, f"write_mesh {path}")
 
 
 class Batch:

@@ -118,6 +118,9 @@ SIGNATURES = {
     "beta_gpu_matrix_lower_values": (_I, [_P, _I, _P, _P]),
     "beta_gpu_solve": (_I, [_P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "beta_gpu_solve_rhs": (_I, [_P, _P, _P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "beta_gpu_read_mesh": (_I, [C.c_char_p, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), _P,
+                                _P]),
+    "beta_gpu_write_mesh": (_I, [C.c_char_p, _I, _I, _I, _P, _I, _I, _P, _I]),
     "beta_gpu_write_lower": (_I, [C.c_char_p, _I, _I, _P, _P, _P]),
     "beta_gpu_read_lower": (_I, [C.c_char_p, _I, C.POINTER(_I), C.POINTER(C.c_longlong), _P, _P, _P]),
     "beta_gpu_export_matrix": (_I, [_P, _I, _I, C.c_char_p]),

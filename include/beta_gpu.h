@@ -215,6 +215,21 @@ BETA_GPU_API int beta_gpu_matvec(beta_gpu_ctx* ctx, int precision, const double*
  * restrained-row skip): host u[ndof] -> host f[ndof]. */
 BETA_GPU_API int beta_gpu_internal_force(beta_gpu_ctx* ctx, const double* u, double* f);
 
+/* ---- mesh files ------------------------------------------------------------ */
+/* BETA's mesh files, text (BasicMesh::ReadMesh, BasicMesh.cpp:79-190, with the
+ * processCommands / setCoordinateReadOption block) or binary (ReadMeshBinary,
+ * :192-268).  Returns xyz (nnode x ndim) and the connectivity as 0-based node
+ * indices in BETA's local order (node numbers may start at 0 or 1), elements
+ * in ascending element number; all elements must share nnpe
+ * (BETA_GPU_ERR_UNSUPPORTED otherwise).  Call with xyz/conn NULL for the
+ * sizes, then with arrays.  Host only. */
+BETA_GPU_API int beta_gpu_read_mesh(const char* path, int binary, int* ndim, int* nnode, int* nelem, int* nnpe,
+                                    double* xyz, int* conn);
+/* Writes a mesh in the same layouts, numbering nodes and elements from
+ * first_number (0 or 1). */
+BETA_GPU_API int beta_gpu_write_mesh(const char* path, int binary, int ndim, int nnode, const double* xyz, int nelem,
+                                     int nnpe, const int* conn, int first_number);
+
 /* ---- system exchange formats -------------------------------------------- */
 /* The lower triangle of a symmetric matrix (SymmetricSparseMatrix order: rows
  * ascending, columns ascending, diagonal last) in BETA's dump layouts, for
