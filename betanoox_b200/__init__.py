@@ -103,6 +103,18 @@ class Solver:
     def assemble(self, precision=_abi.FP32, what=_abi.ASM_K, dt=0.0, alpha=1.0):
         self._check(self.lib.beta_gpu_assemble(self.h, what, precision, dt, alpha), "assemble")
 
+    def element_outputs(self, u=None):
+        """Per element [volume, int stress dV, int strain dV, strain energy]
+        (getVolAvgValues) and their sums over the mesh; u: displacements or
+        None for the last solution."""
+        m = self.model
+        ns = 6 if m.kind == _abi.HEX8_ELASTIC else 3
+        per = np.zeros((m.nelem, 2 * ns + 2))
+        tot = np.zeros(2 * ns + 2)
+        uu = None if u is None else np.ascontiguousarray(u, dtype=np.float64)
+        self._check(self.lib.beta_gpu_element_outputs(self.h, _ptr(uu), _ptr(per), _ptr(tot)), "element_outputs")
+        return per, tot
+
     def export_matrix(self, path, fmt, precision=_abi.FP64):
         """Writes the assembled matrix in one of BETA's exchange formats."""
         self._check(self.lib.beta_gpu_export_matrix(self.h, precision, int(fmt), str(path).encode()), "export_matrix")

@@ -124,6 +124,7 @@ SIGNATURES = {
     "beta_gpu_write_lower": (_I, [C.c_char_p, _I, _I, _P, _P, _P]),
     "beta_gpu_read_lower": (_I, [C.c_char_p, _I, C.POINTER(_I), C.POINTER(C.c_longlong), _P, _P, _P]),
     "beta_gpu_export_matrix": (_I, [_P, _I, _I, C.c_char_p]),
+    "beta_gpu_element_outputs": (_I, [_P, _P, _P, _P]),
     "beta_gpu_download": (_I, [_P, _P]),
     "beta_gpu_matvec": (_I, [_P, _I, _P, _P]),
     "beta_gpu_internal_force": (_I, [_P, _P, _P]),

@@ -24,6 +24,7 @@
 #include "pattern.hpp"
 #include "pcg_kernels.cuh"
 #include "batch_kernels.cuh"
+#include "post_kernels.cuh"
 
 using namespace betagpu;
 
@@ -1309,6 +1310,49 @@ int beta_gpu_internal_force(beta_gpu_ctx* c, const double* u, double* f) {
   if ((rc = mf_apply(c, 1.0, c->t64.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
   CK(d2h(c, f, c->y64.p, sizeof(double) * c->ndof));
   CK(cudaStreamSynchronize(c->stream));
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_element_outputs(beta_gpu_ctx* c, const double* u, double* per_element, double* totals) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  if (c->kind != BETA_GPU_HEX8_ELASTIC && c->kind != BETA_GPU_QUAD4_PSTRESS)
+    return fail(c, BETA_GPU_ERR_UNSUPPORTED, "element outputs are defined for the elasticity elements");
+  if (!c->have_mat || !c->ndof) return fail(c, BETA_GPU_ERR_STATE, "mesh and materials required");
+  if (!u && !c->have_u) return fail(c, BETA_GPU_ERR_STATE, "no solution");
+  cudaSetDevice(c->device);
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  const double* ud = c->u.p;
+  if (u) {
+    CK(h2d(c, c->t64.p, u, sizeof(double) * c->ndof));
+    ud = c->t64.p;
+  }
+  const int ns = c->kind == BETA_GPU_HEX8_ELASTIC ? 6 : 3, w = 2 * ns + 2;
+  DBuf<double> out;
+  CK(out.alloc((size_t)c->nelem * w));
+  const int grid = (c->nelem + 127) / 128;
+  const int* eg = c->have_egroup ? c->egroup.p : nullptr;
+  if (c->kind == BETA_GPU_HEX8_ELASTIC)
+    k_outputs_hex8<<<grid, 128, 0, c->stream>>>(c->nelem, c->xyz.p, c->conn.p, c->gparams.p, eg, c->nparams,
+                                                c->gt.p, ud, out.p);
+  else
+    k_outputs_quad4<<<grid, 128, 0, c->stream>>>(c->nelem, c->xyz.p, c->conn.p, c->gparams.p, eg, c->nparams,
+                                                 c->gt.p, ud, out.p);
+  c->n_launch += 1;
+  CKL("element outputs");
+  std::vector<double> h;
+  double* dst = per_element;
+  if (!dst) {
+    h.resize((size_t)c->nelem * w);
+    dst = h.data();
+  }
+  CK(d2h(c, dst, out.p, sizeof(double) * (size_t)c->nelem * w));
+  CK(cudaStreamSynchronize(c->stream));
+  if (totals) {  // element order: the same sum on every call
+    for (int k = 0; k < w; ++k) totals[k] = 0.0;
+    for (long long e = 0; e < c->nelem; ++e)
+      for (int k = 0; k < w; ++k) totals[k] += dst[e * w + k];
+  }
   return BETA_GPU_OK;
 }
 

@@ -41,7 +41,8 @@ def _splitmix64_raw(x: np.ndarray) -> np.ndarray:
 def uniform(seed: int, stream: int, idx) -> np.ndarray:
     """U[0,1) keyed by (seed, stream, idx)."""
     idx = np.asarray(idx, dtype=np.uint64)
-    key = _splitmix64(np.uint64(seed) * np.uint64(0x100000001B3) + np.uint64(stream) * np.uint64(0x9E3779B1))
+    with np.errstate(over="ignore"):  # wrap-around multiplication is intended
+        key = _splitmix64(np.uint64(seed) * np.uint64(0x100000001B3) + np.uint64(stream) * np.uint64(0x9E3779B1))
     with np.errstate(over="ignore"):
         u = _splitmix64(idx ^ key)
     return (u >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)

@@ -255,6 +255,16 @@ BETA_GPU_API int beta_gpu_read_lower(const char* path, int format, int* n, long 
 /* Writes the assembled matrix of `precision` (FP32 values widened). */
 BETA_GPU_API int beta_gpu_export_matrix(beta_gpu_ctx* ctx, int precision, int format, const char* path);
 
+/* ---- post-solve element outputs ------------------------------------------- */
+/* ElasticityElement3D::getVolAvgValues (ElasticityElement3D.cpp:417-558) for
+ * every element of an elasticity mesh, in FP64 on the device: per element
+ * [volume, int stress dV (ns), int strain dV (ns), strain energy], ns = 6
+ * (hex8: xx,yy,zz,xy,yz,xz, engineering shear) or 3 (quad4 plane stress:
+ * xx,yy,xy; unit thickness).  u: host displacements (ndof) or NULL for the
+ * last solution.  per_element: nelem*(2ns+2) or NULL; totals: 2ns+2 sums over
+ * the mesh in element order or NULL (volume averages = totals / volume). */
+BETA_GPU_API int beta_gpu_element_outputs(beta_gpu_ctx* ctx, const double* u, double* per_element, double* totals);
+
 /* ---- transient diffusion (DiffusionModel::DoTransientNonLinearAnalysis) -- */
 /* Sets u_s (host, ndof) as the current field. */
 BETA_GPU_API int beta_gpu_heat_set_state(beta_gpu_ctx* ctx, const double* u0);

@@ -794,6 +794,75 @@ int oracle_internal_force_hex8(int nelem, const int* conn, const double* xyz,
   return OR_OK;
 }
 
+// Element volume integrals after a solve: ElasticityElement3D::getVolAvgValues
+// (ElasticityElement3D.cpp:417-558) -- per integration point dV = detJ * w
+// (unit thickness), strain = B u_e (engineering shear), stress = C strain,
+// and the sums volume += dV, stress_int += stress dV, strain_int += strain dV,
+// energy += 0.5 stress.strain dV.  The quad4 plane-stress element gets the
+// same integrals with its 3 components (ElasticityElement2D).  ns = 6 (hex8)
+// or 3 (quad4); out rows: [volume, stress_int[ns], strain_int[ns], energy].
+int oracle_element_outputs(int kind, int nelem, const int* conn, const double* xyz, const int* first_dof,
+                           const double* params, int order, const double* u, double* out) {
+  const bool hex = kind == 2;
+  if (!hex && kind != 1) return OR_ERR_ARG;
+  if (order < 1 || order > 4) return OR_ERR_ARG;
+  const int nnpe = hex ? 8 : 4, ndim = hex ? 3 : 2, ns = hex ? 6 : 3, nd = nnpe * ndim;
+  double xi[64], eta[64], zeta[64], w[64];
+  int nip;
+  if (hex) {
+    oracle_hex_points(order, xi, eta, zeta, w);
+    nip = order * order * order;
+  } else {
+    oracle_quad_points(order, xi, eta, w);
+    nip = order * order;
+  }
+  for (int e = 0; e < nelem; ++e) {
+    const int* ce = conn + (size_t)e * nnpe;
+    double xe[24], ue[24], C[36];
+    int map[24];
+    gather_xyz(nnpe, ndim, ce, xyz, xe);
+    elem_dofs(nnpe, ndim, ce, first_dof, map);
+    for (int i = 0; i < nd; ++i) ue[i] = u[map[i]];
+    if (hex) {
+      int st = oracle_cmat_ortho3d(params + (size_t)e * 9, C);
+      if (st) return st;
+    } else {
+      oracle_cmat_plane_stress(params + (size_t)e * 4, C);
+    }
+    double* o = out + (size_t)e * (2 * ns + 2);
+    for (int k = 0; k < 2 * ns + 2; ++k) o[k] = 0.0;
+    for (int ip = 0; ip < nip; ++ip) {
+      double eps[6] = {0}, sig[6] = {0}, dv;
+      if (hex) {
+        double d0[8], d1[8], d2[8], g[3][8], B[6][24];
+        oracle_shape_hex8(xi[ip], eta[ip], zeta[ip], nullptr, d0, d1, d2);
+        dv = jac3(xe, d0, d1, d2, g) * w[ip];
+        bmat3(g, B);
+        for (int k = 0; k < 6; ++k)
+          for (int i = 0; i < 24; ++i) eps[k] += B[k][i] * ue[i];
+      } else {
+        double d0[4], d1[4], g[2][4];
+        oracle_shape_quad4(xi[ip], eta[ip], nullptr, d0, d1);
+        dv = jac2(xe, d0, d1, g) * w[ip];
+        for (int a = 0; a < 4; ++a) {  // ElasticityElement2D::calculateBmatrix rows xx, yy, xy
+          eps[0] += g[0][a] * ue[2 * a];
+          eps[1] += g[1][a] * ue[2 * a + 1];
+          eps[2] += g[1][a] * ue[2 * a] + g[0][a] * ue[2 * a + 1];
+        }
+      }
+      for (int k = 0; k < ns; ++k)
+        for (int m = 0; m < ns; ++m) sig[k] += C[k * ns + m] * eps[m];
+      o[0] += dv;
+      for (int k = 0; k < ns; ++k) {
+        o[1 + k] += sig[k] * dv;
+        o[1 + ns + k] += eps[k] * dv;
+        o[1 + 2 * ns] += 0.5 * sig[k] * eps[k] * dv;
+      }
+    }
+  }
+  return OR_OK;
+}
+
 // One backward-Euler family step of DiffusionModel::DoTransientNonLinearAnalysis
 // (DiffusionModel.cpp:743-818) with linear conductivity:
 //   a1 = alpha*dt, a2 = (1-alpha)*dt                                  (:745-746)

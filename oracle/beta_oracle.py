@@ -79,6 +79,7 @@ def _load():
         "oracle_sys_specify_mesh": (None, [V, I, I, I, _ip, _ip]),
         "oracle_sys_assemble_mesh": (I, [V, I, I, I, I, I, _ip, _dp, _ip, _dp, I, I]),
         "oracle_internal_force_hex8": (I, [I, _ip, _dp, _ip, _dp, I, P, _dp, _dp]),
+        "oracle_element_outputs": (I, [I, I, _ip, _dp, _ip, _dp, I, _dp, _dp]),
         "oracle_heat_step": (I, [V, I, _ip, _dp, _ip, _dp, I, D, D, _dp, D, I, C.POINTER(SolveStats)]),
         "oracle_csr_from_sys": (V, [V]),
         "oracle_csr_destroy": (None, [V]),
@@ -290,6 +291,17 @@ def internal_force_hex8(mesh, params, order, u, restrained=None):
                                           None if r is None else r.ctypes.data, _f64(u), f)
     assert st == 0
     return f
+
+
+def element_outputs(mesh, params, order, u):
+    """Per element [volume, int stress dV, int strain dV, strain energy]
+    (ElasticityElement3D::getVolAvgValues), hex8 (6 components) or quad4 (3)."""
+    ns = 6 if mesh.kind == 2 else 3
+    out = np.zeros((mesh.nelem, 2 * ns + 2))
+    st = lib().oracle_element_outputs(mesh.kind, mesh.nelem, _i32(mesh.conn).reshape(-1), _f64(mesh.xyz).reshape(-1),
+                                      _i32(mesh.first_dof), _f64(params).reshape(-1), order, _f64(u), out)
+    assert st == 0
+    return out
 
 
 def element_matrices_threaded(mesh, params, order, e0, e1, threads=0):

@@ -267,3 +267,23 @@ def test_maxit_is_reported_not_fatal():
     # the context stays usable
     rc, st = g.solve(opts(mode=_abi.MODE_FP64, tol=1e-10, check_every=8))
     assert rc == 0
+
+
+@pytest.mark.parametrize("name", ["rve", "quad4"])
+def test_element_outputs_match_oracle(oracle, name):
+    """Post-solve volume integrals (getVolAvgValues) of the solved field."""
+    m = MODELS[name]()
+    g = Solver()
+    g.load_model(m)
+    g.build_pattern()
+    g.assemble(_abi.FP32)
+    g.solve(opts(tol=1e-12))
+    u = g.download()
+    per, tot = g.element_outputs()
+    ref = oracle.element_outputs(m, m.params, m.order, u)
+    scale = np.abs(ref).max(axis=0)
+    scale[scale == 0] = 1.0
+    assert (np.abs(per - ref) / scale).max() <= 1e-12
+    np.testing.assert_allclose(tot, per.sum(axis=0), rtol=1e-12, atol=1e-300)
+    per2, _ = g.element_outputs(u)  # explicit displacements give the same
+    np.testing.assert_array_equal(per, per2)

@@ -175,3 +175,31 @@ def test_oracle_threaded_pcg_matches_serial(oracle):
     rc2, u2, st2 = s.solve_threaded(b, eps=1e-12, maxit=20000, threads=4)
     assert rc1 == 0 and rc2 == 0
     assert np.linalg.norm(u1 - u2) / np.linalg.norm(u1) < 1e-9
+
+
+def test_element_outputs_known_answer_for_a_uniform_strain(oracle):
+    """getVolAvgValues under u = H x (a uniform strain): every element's
+    strain integral is E V, its stress integral C E V and its energy
+    0.5 E.C E V -- exact for any element shape and material."""
+    rng = np.random.default_rng(11)
+    m = W.cube_hex8(3, seed=8)
+    m.xyz = m.xyz + 0.05 * rng.uniform(-1, 1, size=m.xyz.shape) / 3  # distorted hexes
+    H = rng.normal(size=(3, 3)) * 1e-3
+    u = (m.xyz @ H.T).reshape(-1)
+    E = np.array([H[0, 0], H[1, 1], H[2, 2], H[0, 1] + H[1, 0], H[1, 2] + H[2, 1], H[0, 2] + H[2, 0]])
+    out = oracle.element_outputs(m, m.params, m.order, u)
+    for e in range(m.nelem):
+        C = oracle.cmat_ortho3d(m.params[e])
+        V = out[e, 0]
+        np.testing.assert_allclose(out[e, 7:13], E * V, rtol=1e-9, atol=1e-18)
+        np.testing.assert_allclose(out[e, 1:7], C @ E * V, rtol=1e-9, atol=1e-12)
+        assert abs(out[e, 13] - 0.5 * E @ C @ E * V) <= 1e-9 * abs(0.5 * E @ C @ E * V)
+    q = W.plate_quad4(4)
+    Hq = rng.normal(size=(2, 2)) * 1e-3
+    uq = (q.xyz @ Hq.T).reshape(-1)
+    Eq = np.array([Hq[0, 0], Hq[1, 1], Hq[0, 1] + Hq[1, 0]])
+    outq = oracle.element_outputs(q, q.params, q.order, uq)
+    assert abs(outq[:, 0].sum() - 1.0) < 1e-12  # undistorted unit square
+    Cq = oracle.cmat_plane_stress(q.params[0])
+    np.testing.assert_allclose(outq[:, 4:7].sum(axis=0), Eq, rtol=1e-9)
+    np.testing.assert_allclose(outq[:, 1:4].sum(axis=0), Cq @ Eq, rtol=1e-9)
