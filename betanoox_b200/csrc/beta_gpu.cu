@@ -351,7 +351,7 @@ int mf_apply(beta_gpu_ctx* c, double c1, const double* w1, double c2, const doub
     if (c->kind == BETA_GPU_HEX8_ELASTIC)
       launch(c, k_mf_hex8_elastic, grid_for(c, nel, 32), 256, 0, A, el, nel, w1, w2, y);
     else if (c->kind == BETA_GPU_HEX8_HEAT)
-      launch(c, k_mf_hex8_heat, grid_for(c, nel, 32), 256, 0, A, el, nel, w1, w2, y);
+      launch(c, k_mf_hex8_heat_t, grid_for(c, nel, 256), 256, 0, A, el, nel, w1, w2, y);
     else
       launch(c, k_mf_quad4_pstress, grid_for(c, nel, 64), 256, 0, A, el, nel, w1, w2, y);
     CKL("matrix-free kernel launch");
@@ -497,8 +497,12 @@ int compute_minv(beta_gpu_ctx* c, int precond) {
 // x64 holds the initial iterate (prescribed values on restrained dofs) on
 // entry and the solution on exit.  bnorm is ||b||.
 template <int ND>
+// start_from_rhs: x64 is the boundary extension of the prescribed values and
+// b64 the eliminated right-hand side, so the first residual is b64 itself
+// (free rows) and no operator apply is needed for it.
 int mpir_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c2, const double* w2,
-              double cm, const double* loadv, double bnorm, beta_gpu_solve_stats* stats, ProfAcc* prof) {
+              double cm, const double* loadv, double bnorm, beta_gpu_solve_stats* stats, ProfAcc* prof,
+              bool start_from_rhs) {
   int rc;
   if ((rc = compute_minv<ND>(c, o->precond)) != BETA_GPU_OK) return rc;
   const int n = c->ndof;
@@ -535,7 +539,18 @@ int mpir_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c
     return BETA_GPU_OK;
   };
   double rn = 0.0, xn = 0.0;
-  if ((rc = true_residual(&rn, &xn)) != BETA_GPU_OK) return rc;
+  if (start_from_rhs) {
+    CK(cudaMemsetAsync(c->y64.p, 0, sizeof(double) * n, c->stream));
+    launch(c, k_residual64, grid_for(c, n, 256), 256, 0, n, c->rest.p, (const double*)c->b64.p,
+           (const double*)c->y64.p, (const double*)c->x64.p, c->r64.p, c->sums.p, c->partials.p, c->ticket.p);
+    CKL("k_residual64");
+    double s2[2];
+    if ((rc = read_sums(c, 2, s2)) != BETA_GPU_OK) return rc;
+    rn = std::sqrt(s2[0]);
+    xn = std::sqrt(s2[1]);
+  } else if ((rc = true_residual(&rn, &xn)) != BETA_GPU_OK) {
+    return rc;
+  }
   q = stop_q(rn, xn);
   int iters = 0;
   if (!std::isfinite(q)) {
@@ -582,12 +597,13 @@ int mpir_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c
   return status;
 }
 
-int mpir_dispatch(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c2, const double* w2,
+int mpir_dispatch(beta_gpu_ctx* c, bool start_from_rhs, const beta_gpu_solve_opts* o, double c1, double c2,
+                  const double* w2,
                   double cm, const double* loadv, double bnorm, beta_gpu_solve_stats* stats, ProfAcc* prof) {
   switch (c->ndpn) {
-    case 1: return mpir_core<1>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof);
-    case 2: return mpir_core<2>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof);
-    default: return mpir_core<3>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof);
+    case 1: return mpir_core<1>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof, start_from_rhs);
+    case 2: return mpir_core<2>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof, start_from_rhs);
+    default: return mpir_core<3>(c, o, c1, c2, w2, cm, loadv, bnorm, stats, prof, start_from_rhs);
   }
 }
 
@@ -1190,7 +1206,7 @@ int beta_gpu_solve(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve
     if ((rc = read_sums(c, 1, &bb))) return rc;
     launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, last ? c->u.p : nullptr, c->x64.p);
     CKL("k_ext64");
-    status = mpir_dispatch(c, o, 1.0, 0.0, nullptr, 0.0, c->load.p, std::sqrt(bb), stats, &prof);
+    status = mpir_dispatch(c, !last, o, 1.0, 0.0, nullptr, 0.0, c->load.p, std::sqrt(bb), stats, &prof);
     if (stats && (status == BETA_GPU_OK || status == BETA_GPU_MAXIT)) {
       // true FP64 residual of the returned iterate
       if ((rc = mf_apply(c, 1.0, c->x64.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
@@ -1425,7 +1441,7 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
       double bb;
       if ((rc = read_sums(c, 1, &bb))) return rc;
       CK(cudaMemcpyAsync(c->x64.p, c->t64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
-      rc = mpir_dispatch(c, o, ks, kf, c->us.p, ms, nullptr, std::sqrt(std::max(bb, ff)), &s, &prof);
+      rc = mpir_dispatch(c, true, o, ks, kf, c->us.p, ms, nullptr, std::sqrt(std::max(bb, ff)), &s, &prof);
     }
     if (rc != BETA_GPU_OK) {
       if (stats) *stats = s;

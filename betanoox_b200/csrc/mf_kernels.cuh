@@ -189,6 +189,84 @@ __device__ __forceinline__ void mf_hex8_heat_warp(const MfArgs& A, const int* __
   }
 }
 
+// hex8 diffusion, one thread per element: y += K (c1 w1 + c2 w2) + cm M w1
+// for element elems[i].  A scalar field has 8 unknowns per element, so the
+// whole element fits in one thread's registers; compared with 8 lanes per
+// element this trades 13 group sums (39 FP64 shuffles) per Gauss point for
+// plain FMAs.  The element gradients are recomputed in the second pass
+// instead of held (fewer registers).
+__device__ __forceinline__ void mf_hex8_heat_elem(const MfArgs& A, int e, const double* w1, const double* w2,
+                                                  double* y, const double* s_dN, const double* s_N,
+                                                  const double* s_w) {
+  const int* ce = A.conn + (long long)e * 8;
+  int nd[8];
+  double x[8][3], vk[8], vm[8], f[8];
+  const int n0 = ce[0];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    nd[a] = ce[a];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[a][c] = A.xyz[3LL * nd[a] + c] - A.xyz[3LL * n0 + c];
+    vm[a] = w1[nd[a]];
+    vk[a] = A.c1 * vm[a] + (w2 ? A.c2 * w2[nd[a]] : 0.0);
+    f[a] = 0.0;
+  }
+  const double* pm = A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams;
+  const double k0 = pm[0], k1 = pm[1], k2 = pm[2], cap = A.cm * pm[3];
+  for (int ip = 0; ip < A.nip; ++ip) {
+    const double* d = s_dN + ip * 24;
+    const double* N = s_N + ip * 8;
+    double M[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double t = 0.0;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) t += d[r * 8 + a] * x[a][c];
+        M[r * 3 + c] = t;
+      }
+    double Mi[9];
+    const double det = inv3<double>(M, Mi);
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, tv = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const double g0 = Mi[0] * d[a] + Mi[1] * d[8 + a] + Mi[2] * d[16 + a];
+      const double g1 = Mi[3] * d[a] + Mi[4] * d[8 + a] + Mi[5] * d[16 + a];
+      const double g2 = Mi[6] * d[a] + Mi[7] * d[8 + a] + Mi[8] * d[16 + a];
+      t0 += vk[a] * g0;
+      t1 += vk[a] * g1;
+      t2 += vk[a] * g2;
+      tv += vm[a] * N[a];
+    }
+    const double fw = det * s_w[ip];
+    const double q0 = fw * k0 * t0, q1 = fw * k1 * t1, q2 = fw * k2 * t2, qm = fw * cap * tv;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const double g0 = Mi[0] * d[a] + Mi[1] * d[8 + a] + Mi[2] * d[16 + a];
+      const double g1 = Mi[3] * d[a] + Mi[4] * d[8 + a] + Mi[5] * d[16 + a];
+      const double g2 = Mi[6] * d[a] + Mi[7] * d[8 + a] + Mi[8] * d[16 + a];
+      f[a] += g0 * q0 + g1 * q1 + g2 * q2 + N[a] * qm;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a) y[nd[a]] += f[a];
+}
+
+__global__ void __launch_bounds__(256) k_mf_hex8_heat_t(MfArgs A, const int* __restrict__ elems, int nel,
+    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 24];
+  __shared__ double s_N[kMaxIP * 8];
+  __shared__ double s_w[kMaxIP];
+  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
+    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
+  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_N[i] = A.gt->N[i / 8][i % 8];
+  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nel; i += gridDim.x * blockDim.x)
+    mf_hex8_heat_elem(A, elems[i], w1, w2, y, s_dN, s_N, s_w);
+}
+
 __global__ void __launch_bounds__(256) k_mf_hex8_heat(MfArgs A, const int* __restrict__ elems, int nel,
     const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y) {
   __shared__ double s_dN[kMaxIP * 24];
