@@ -171,6 +171,8 @@ struct beta_gpu_ctx {
   // solution / transient state
   DBuf<double> u, us;
   bool have_u = false, have_us = false;
+  DBuf<double> dprev;        // transient: the last step's increment, the next step's initial guess
+  bool have_dprev = false;
   DBuf<double> rhs_presc, rhs_load;  // beta_gpu_solve_rhs: the caller's right-hand side as prescribed/load
   bool rhs_staged = false;           // b64 already holds the caller's right-hand side (FP64 mode)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1381,6 +1383,7 @@ int beta_gpu_heat_set_state(beta_gpu_ctx* c, const double* u0) {
   if ((rc = upload(c, c->us, u0, c->ndof))) return rc;
   CK(cudaStreamSynchronize(c->stream));
   c->have_us = true;
+  c->have_dprev = false;
   return BETA_GPU_OK;
 }
 
@@ -1406,6 +1409,7 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
                                     : (c->have32 && c->what32 == BETA_GPU_ASM_MBAR && c->kscale32 == ks && c->mscale32 == ms);
   if (!have && (rc = beta_gpu_assemble(c, BETA_GPU_ASM_MBAR, prec, dt, alpha))) return rc;
   if ((rc = ensure_workspace(c))) return rc;
+  CK(c->dprev.alloc(c->ndof));
   const int n = c->ndof;
   int total = 0;
   beta_gpu_solve_stats s;
@@ -1417,7 +1421,10 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
       // F = -(a1+a2)/dt K u_s (formF_s_new) on free rows, + pseudo load
       if ((rc = mf_apply(c, -kf, c->us.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
       launch(c, k_rhs64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, c->y64.p, c->pseudo.p, c->b64.p);
-      CK(cudaMemsetAsync(c->x64.p, 0, sizeof(double) * n, c->stream));
+      if (c->have_dprev)  // start from the last increment (a smooth field changes little per step)
+        CK(cudaMemcpyAsync(c->x64.p, c->dprev.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+      else
+        CK(cudaMemsetAsync(c->x64.p, 0, sizeof(double) * n, c->stream));
       CKL("k_rhs64");
       rc = fp64_core(c, o, &s, &prof);
     } else {
@@ -1440,8 +1447,13 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
       CKL("k_rhs_elim64");
       double bb;
       if ((rc = read_sums(c, 1, &bb))) return rc;
-      CK(cudaMemcpyAsync(c->x64.p, c->t64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
-      rc = mpir_dispatch(c, true, o, ks, kf, c->us.p, ms, nullptr, std::sqrt(std::max(bb, ff)), &s, &prof);
+      if (c->have_dprev)  // start from the last increment (a smooth field changes little per step)
+        launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, (const double*)c->dprev.p,
+               c->x64.p);
+      else
+        CK(cudaMemcpyAsync(c->x64.p, c->t64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+      rc = mpir_dispatch(c, !c->have_dprev, o, ks, kf, c->us.p, ms, nullptr, std::sqrt(std::max(bb, ff)), &s,
+                         &prof);
     }
     if (rc != BETA_GPU_OK) {
       if (stats) *stats = s;
@@ -1452,6 +1464,8 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
     // u_s <- u_s + delta (DiffusionModel.cpp:800-818)
     launch(c, k_axpy64, grid_for(c, n, 256), 256, 0, n, c->us.p, 1.0, c->x64.p);
     CKL("k_axpy64");
+    CK(cudaMemcpyAsync(c->dprev.p, c->x64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    c->have_dprev = true;
   }
   if (stats) *stats = s;
   if (total_iterations) *total_iterations = total;

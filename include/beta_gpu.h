@@ -271,6 +271,8 @@ BETA_GPU_API int beta_gpu_heat_set_state(beta_gpu_ctx* ctx, const double* u0);
 /* Runs nsteps steps of size dt with the generalized-alpha family (alpha=1:
  * backward Euler), assembling Mbar = (a1 K + M)/dt once (linear conductivity)
  * and solving Mbar du = -(a1+a2) K u_s / dt per step (DiffusionModel.cpp:743-818).
+ * Every step after the first starts its solve from the previous step's
+ * increment (beta_gpu_heat_set_state forgets it).
  * With BETA_GPU_STOP_RB a mixed-precision step stops at
  * ||r|| <= tol * max(||b||, ||(M/dt) u_s||): the increment's right-hand side b
  * shrinks as the field smooths, the new state's does not, and both systems
