@@ -922,13 +922,15 @@ def run_serve(args):
     o = opts(mode=_abi.MODE_MPIR, tol=args.tol, inner_tol=args.inner_tol)
     th = args.submit_threads or (os.cpu_count() or 1)
     srv = Server(dev, hbm_budget=int(args.pool_gb * (1 << 30)), max_systems=4096, o=o,
-                 iters_per_launch=args.iters_per_launch, threads=args.threads, gang_boost=args.gang_boost)
+                 iters_per_launch=args.iters_per_launch, threads=args.threads, gang_boost=args.gang_boost,
+                 slice_us=args.slice_us)
     # capacity: a burst of the first `cap` pool models submitted at once
     cap_n = min(args.capacity_requests, pool_n)
     for _ in range(args.warmup):
         _serve_stream(srv, models[:min(cap_n, 32)], np.zeros(min(cap_n, 32)), th)
     res_cap, wall_cap = _serve_stream(srv, models[:cap_n], np.zeros(cap_n), th)
     cap_rps = cap_n / wall_cap
+    cap_dofs = sum(r[1] for r in res_cap) / wall_cap
     lam = args.load * cap_rps
     rng = np.random.default_rng(args.seed)
     arrivals = np.cumsum(rng.exponential(1.0 / lam, size=args.requests))
@@ -977,7 +979,7 @@ def run_serve(args):
                                    f"diffusion, log-uniform 1e3-5e5 dofs) at {args.load:.0%} of measured capacity",
                        "requests": args.requests, "distinct_models": pool_n, "families": fams,
                        "lambda_per_s": lam, "capacity_req_per_s": cap_rps, "tol": args.tol,
-                       "iters_per_launch": args.iters_per_launch, "submit_threads": th,
+                       "iters_per_launch": args.iters_per_launch, "slice_us": args.slice_us, "submit_threads": th,
                        "launch_shape": {"threads": args.threads, "gang_boost": args.gang_boost},
                        "parallelism": f"replicas x{ws}",
                        "l2": "working set above L2 (pool of resident systems)"},
@@ -986,7 +988,8 @@ def run_serve(args):
             "serve": {"done_ok": ok, "states": {str(k): states.count(k) for k in set(states)},
                       "max_final_norm": float(max(r[4] for r in res)), "launches": s1["launches"] - s0["launches"],
                       "busy_frac": (s1["busy_us"] - s0["busy_us"]) / 1e6 / wall, "wall_s": wall,
-                      "generate_s": t_gen, "capacity_burst": {"requests": cap_n, "wall_s": wall_cap}},
+                      "generate_s": t_gen,
+                      "capacity_burst": {"requests": cap_n, "wall_s": wall_cap, "dofs_per_s": cap_dofs}},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": s1["h2d"] - s0["h2d"],
                     "d2h_bytes_per_step": s1["d2h"] - s0["d2h"],
                     "includes": "arrival to result on host: structure build, admission, solve, download"},
@@ -995,6 +998,7 @@ def run_serve(args):
         if fp64:
             out["fp64_plain"] = fp64
             out["mixed_over_fp64"] = value / fp64["value"]
+            out["capacity_over_fp64"] = cap_dofs / fp64["value"]
         if not args.skip_cpu:
             thc = os.cpu_count() or 1
             n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s, thc)
@@ -1064,11 +1068,12 @@ def main():
     ap.add_argument("--fp64-sample", type=int, default=512)
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--serve-pool", type=int, default=1000)
-    ap.add_argument("--capacity-requests", type=int, default=400)
+    ap.add_argument("--capacity-requests", type=int, default=1000)
     ap.add_argument("--load", type=float, default=0.8)
-    ap.add_argument("--iters-per-launch", type=int, default=200)
+    ap.add_argument("--iters-per-launch", type=int, default=1000000)
     ap.add_argument("--threads", type=int, default=512)
-    ap.add_argument("--gang-boost", type=int, default=4)
+    ap.add_argument("--gang-boost", type=int, default=16)
+    ap.add_argument("--slice-us", type=int, default=40000, help="serve: time slice of a launch")
     ap.add_argument("--submit-threads", type=int, default=0)
     ap.add_argument("--serve-fp64-sample", type=int, default=100)
     # transient diffusion

@@ -349,6 +349,13 @@ class Batch:
         if st != _abi.OK:
             raise self._err(st, "batch_set_switch")
 
+    def set_slice(self, slice_us):
+        """Time slice of a launch in microseconds (0: off): systems stop after
+        the iteration in which it ends; results do not change."""
+        st = self.lib.beta_gpu_batch_set_slice(self.h, int(slice_us))
+        if st != _abi.OK:
+            raise self._err(st, "batch_set_slice")
+
     def reset(self):
         """Marks every system unsolved (the next run re-assembles and re-solves)."""
         st = self.lib.beta_gpu_batch_reset(self.h)
@@ -374,7 +381,7 @@ class Server:
              "pool_used", "pool_bytes", "busy_us", "h2d", "d2h"]
 
     def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, max_systems: int = 4096, o=None,
-                 iters_per_launch: int = 200, threads: int = 0, gang_boost: int = -1):
+                 iters_per_launch: int = 200, threads: int = 0, gang_boost: int = -1, slice_us: int = 0):
         self.lib = _abi.load()
         self.o = o or opts()
         h = C.c_void_p()
@@ -383,6 +390,11 @@ class Server:
         if st != _abi.OK:
             raise BetaGpuError(st, "beta_gpu_server_create failed")
         self.h = h
+        if slice_us:
+            st = self.lib.beta_gpu_server_set_slice(h, int(slice_us))
+            if st != _abi.OK:
+                self.close()
+                raise BetaGpuError(st, "beta_gpu_server_set_slice failed")
 
     def close(self):
         if getattr(self, "h", None):

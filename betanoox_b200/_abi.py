@@ -144,6 +144,7 @@ SIGNATURES = {
     "beta_gpu_batch_autotune": (_I, [_P, C.POINTER(SolveOpts), _I, C.POINTER(_I), C.POINTER(_I)]),
     "beta_gpu_batch_reset": (_I, [_P]),
     "beta_gpu_batch_set_switch": (_I, [_P, _I]),
+    "beta_gpu_batch_set_slice": (_I, [_P, C.c_longlong]),
     "beta_gpu_batch_test_barrier": (_I, [_P, C.c_longlong, _I]),
     "beta_gpu_gang_plan": (_I, [_I, C.POINTER(C.c_longlong), C.POINTER(_I), _I, _I, _I, C.POINTER(_I)]),
     "beta_gpu_batch_info": (_I, [_P, C.POINTER(C.c_longlong), _I]),
@@ -155,6 +156,7 @@ SIGNATURES = {
     "beta_gpu_server_poll": (_I, [_P, C.c_longlong, _I, C.POINTER(_I), C.POINTER(_I), _P, C.POINTER(SolveStats),
                                   C.POINTER(_D), _I]),
     "beta_gpu_server_cancel": (_I, [_P, C.c_longlong]),
+    "beta_gpu_server_set_slice": (_I, [_P, C.c_longlong]),
     "beta_gpu_server_stats": (_I, [_P, C.POINTER(C.c_longlong), _I]),
     "beta_gpu_csr_pcg_device_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _D, _I, _P, C.POINTER(SolveStats)]),
 }

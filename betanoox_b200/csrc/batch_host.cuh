@@ -23,6 +23,7 @@ struct beta_gpu_batch {
     size_t off = 0, bytes = 0;
     long long work = 0;  // stored FP32 matrix values
     int nslice = 0;
+    long long served = 0;  // last launch in which the system made progress
     BSys desc;
     BState st;
   };
@@ -49,11 +50,14 @@ struct beta_gpu_batch {
   int threads = 512, gang_boost = 4;
   // a system whose FP32 inner solve needs more than this many iterations for
   // one residual-replacement cycle continues in FP64, matrix-free (0: never)
-  int switch_iters = 2000;
+  int switch_iters = 500;
   // gang barrier wait limit, and the failure-path test hook (see
   // beta_gpu_batch_test_barrier): plan the first gang one CTA larger than it gets
   long long spin_ns = 2000000000LL;
   int phantom = 0;
+  // time slice of a launch (0: a launch ends when every system has converged
+  // or used its iteration budget)
+  long long slice_ns = 0;
   int last_ngang = 0, last_gang_ctas = 0;
   std::map<int, cudaGraphExec_t> graphs;
   long long n_launch = 0, n_h2d = 0, n_d2h = 0;
@@ -116,7 +120,7 @@ void pool_free(beta_gpu_batch* b, size_t off, size_t bytes) {
 struct SysLayout {
   size_t total = 0;
   size_t o_xyz, o_conn, o_gp, o_eg, o_rest, o_presc, o_load, o_cptr, o_elems, o_slot, o_nrp, o_ndiag, o_bsoff,
-      o_bcol, o_bval, o_x64, o_r64, o_y64, o_p64, o_q64, o_y32, o_r32, o_p32, o_p32b, o_z32, o_q32, o_minv, o_part, o_gflag;
+      o_bcol, o_bval, o_x64, o_r64, o_y64, o_p64, o_q64, o_w64, o_y32, o_r32, o_p32, o_p32b, o_z32, o_q32, o_minv, o_part, o_gflag;
   size_t add(size_t bytes) {
     const size_t o = total;
     total += (bytes + 255) & ~size_t(255);
@@ -148,6 +152,7 @@ SysLayout layout_for(int ndim, int nnode, int nelem, int nnpe, int ndpn, int ngr
   L.o_y64 = L.add(sizeof(double) * ndof);
   L.o_p64 = L.add(sizeof(double) * ndof);
   L.o_q64 = L.add(sizeof(double) * ndof);
+  L.o_w64 = L.add(sizeof(double) * ndof);
   L.o_y32 = L.add(sizeof(float) * ndof);
   L.o_r32 = L.add(sizeof(float) * ndof);
   L.o_p32 = L.add(sizeof(float) * (size_t)nnode * (ndpn == 3 ? 4 : ndpn));
@@ -338,6 +343,10 @@ int batch_prepare(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, i
   const int nctas = batch_ctas(b);
   if (nctas < 1) return bfail(b, BETA_GPU_ERR_UNSUPPORTED, "no CTA of this launch shape fits on the GPU");
   const int ngang = batch_plan(b, b->h_active, na, nctas);
+  // single-CTA systems: the least recently served first, so that under a
+  // time slice every system is reached within a few launches
+  std::stable_sort(b->h_active + ngang, b->h_active + na,
+                   [&](int x, int y) { return b->sys[x].served < b->sys[y].served; });
   BParams& P = *b->h_params;
   P.tol = o->tol > 0 ? o->tol : 1e-10;
   P.delta = (o->inner_tol > 0 && o->inner_tol < 1) ? o->inner_tol : 0.01;
@@ -348,6 +357,7 @@ int batch_prepare(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, i
   P.nbig = ngang;
   P.spin_ns = b->spin_ns;  // default 2 s at one barrier: far beyond any phase of a resident gang
   P.switch_iters = b->switch_iters;
+  P.slice_ns = b->slice_ns;
   int rc;
   if (!b->sys.empty() && (rc = batch_h2d(b, b->d_sys, b->h_sys, sizeof(BSys) * b->sys.size()))) return rc;
   if ((rc = batch_h2d(b, b->d_active, b->h_active, sizeof(int) * std::max(1, na)))) return rc;
@@ -365,8 +375,12 @@ int batch_pull_states(beta_gpu_batch* b) {
   if (n) BCK(cudaMemcpyAsync(b->h_states, b->d_states, sizeof(BState) * n, cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
-  for (size_t i = 0; i < n; ++i)
-    if (b->sys[i].live) b->sys[i].st = b->h_states[i];
+  for (size_t i = 0; i < n; ++i) {
+    if (!b->sys[i].live) continue;
+    const BState& s = b->h_states[i];
+    if (s.iter != b->sys[i].st.iter || s.phase != b->sys[i].st.phase) b->sys[i].served = b->n_launch;
+    b->sys[i].st = s;
+  }
   if (b->h_ctl[1]) return bfail(b, BETA_GPU_TIMEOUT, "a gang barrier waited past its limit; the launch stopped");
   return BETA_GPU_OK;
 }

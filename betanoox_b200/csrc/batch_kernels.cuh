@@ -41,10 +41,12 @@ enum : int { kBConverged = 0, kBRunning = 1, kBMaxit = 4, kBBreakdown = 5, kBNeg
 struct BState {
   double rho, rr, maxrr, bn, rn;
   int iter, repl, phase, status;
-  int mode;    // 0: FP32 inner PCG with FP64 reliable updates; 1: FP64 PCG, operator matrix-free
+  int mode;    // 0: FP32 inner PCG with FP64 reliable updates; 1: the same with FP64 vectors and arithmetic
   int cycle0;  // iteration at which the current FP32 replacement cycle began
   float bt;    // FP32 mode: beta of the direction update the next SpMV applies
   int pb;      // FP32 mode: which direction buffer holds the current p (0: p32, 1: p32b)
+  long long busy_ns;  // device time spent on the system (its group's, summed over launches)
+  int sub;            // setup: the next step (kPhaseNew)
 };
 
 // Device descriptor of one system (all pointers into the batch pool).
@@ -70,6 +72,7 @@ struct BSys {
   double* y64;
   double* p64;  // FP64 mode: search direction
   double* q64;  // FP64 mode: K p, then M r
+  double* w64;  // FP64 mode: correction since the last residual replacement
   float* y32;
   float* r32;
   float* p32;   // direction (double-buffered with p32b; padded to float4 for nd = 3)
@@ -78,7 +81,7 @@ struct BSys {
   float* q32;
   float* minv;
   double* part;     // 2 buffers x 2 values x nslice slice partials
-  unsigned* gflag;  // assembly status bits of this system
+  unsigned* gflag;  // [0] assembly status bits; where a time slice ends: [1] iteration, [2] setup step
   const GaussTable* gt;
   BState* st;
   long long nchunk;
@@ -90,6 +93,7 @@ struct BParams {
   int nactive, nbig;            // active[0, nbig) are solved by gangs, the rest by single CTAs
   long long spin_ns;            // longest wait at a gang barrier before the launch gives up
   int switch_iters;             // FP32 cycle longer than this: continue in FP64 (0: never)
+  long long slice_ns;           // time slice: systems stop after the iteration in which it ends (0: none)
 };
 
 // Per CTA: the gang it belongs to for this launch.
@@ -103,7 +107,7 @@ struct BPlan {
 struct GangShared {
   unsigned bar_no;
   int abort;
-  int idx;
+  int idx, skip;
   double wred[2][8];
   double red[2];
 };
@@ -132,6 +136,7 @@ struct Grp {
   int* gabort;
   long long spin_ns;
   double* spart;  // shared partials (2 x kSharedSlices) for a CTA alone
+  long long t0;   // %globaltimer when this CTA started
 };
 
 // Barrier of the group.  Returns false once the launch is aborting (a wait
@@ -314,19 +319,39 @@ __device__ __forceinline__ bool b_rz(const BSys& S, const Grp& g, double* part, 
   return group_sum<2>(g, part, S.nslice, out);
 }
 
-// One 32-node slice of q = A p_new with the direction update folded into the
-// gather: p_new[J] = fmaf(bt, p_old[J], z[J]) for every column J -- the same
-// arithmetic, and so the same bits, as updating p in a separate pass.  Saves
-// a pass over the vectors and a group barrier per iteration.
+// Row-sum form of the FP32 matrix.  The diagonal block of node I holds the
+// block row sum S_I = sum_J A_IJ, taken from the FP64 operator, and the
+// product is formed from differences:
+//   (A p)_I = sum_{J != I} A_IJ (p_J - p_I) + S_I p_I.
+// Rounding every stored entry to FP32 perturbs the low-frequency modes of a
+// stiffness matrix by about eps32 * ||A|| unless the row sums are kept exact
+// (they are zero away from the boundary: rigid translations cost no energy);
+// with them kept the inner iteration count stays close to the FP64 one, and
+// the differences of a smooth p carry no cancellation.  Padding entries hold
+// zeros, so their column does not matter.
+
+// One 32-node slice of q = A p_new in FP32 with the direction update folded
+// into the gather: p_new[J] = fmaf(bt, p_old[J], z[J]) for every column J --
+// the same arithmetic, and so the same bits, as updating p in a separate
+// pass.  Saves a pass over the vectors and a group barrier per iteration.
+// pI receives p_new of the lane's own node.
 template <int ND>
 __device__ __forceinline__ void spmv_row_fused(const BlockMat& A, int s, int lane, const float* pold,
-                                               const float* z, float bt, float* acc) {
+                                               const float* z, float bt, float* acc, float* pI) {
   constexpr int BB = ND * ND;
+  const int I = 32 * s + lane;
   const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
   const int* cp = A.bcol + (long long)c0 * 32 + lane;
   const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
 #pragma unroll
-  for (int i = 0; i < ND; ++i) acc[i] = 0.f;
+  for (int i = 0; i < ND; ++i) { acc[i] = 0.f; pI[i] = 0.f; }
+  if (I < A.nnode) {
+    float po[ND], zv[ND];
+    PVec<ND>::ld(pold, I, po);
+    PVec<ND>::ld(z, I, zv);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) pI[i] = fmaf(bt, po[i], zv[i]);
+  }
 #pragma unroll 2
   for (int k = 0; k < w; ++k) {
     const int J = __ldcs(cp + k * 32);
@@ -336,10 +361,85 @@ __device__ __forceinline__ void spmv_row_fused(const BlockMat& A, int s, int lan
     float v[BB];
 #pragma unroll
     for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);
+    float d[ND];
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      const float pj = fmaf(bt, po[j], zv[j]);
+      d[j] = J == I ? pI[j] : pj - pI[j];
+    }
 #pragma unroll
     for (int i = 0; i < ND; ++i)
 #pragma unroll
-      for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], fmaf(bt, po[j], zv[j]), acc[i]);
+      for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], d[j], acc[i]);
+  }
+}
+
+// One 32-node slice of q = A p in FP32 (p written before the pass).
+template <int ND>
+__device__ __forceinline__ void spmv_row_rs(const BlockMat& A, int s, int lane, const float* p, float* acc,
+                                            float* pI) {
+  constexpr int BB = ND * ND;
+  const int I = 32 * s + lane;
+  const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
+  const int* cp = A.bcol + (long long)c0 * 32 + lane;
+  const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) { acc[i] = 0.f; pI[i] = 0.f; }
+  if (I < A.nnode) PVec<ND>::ld(p, I, pI);
+#pragma unroll 2
+  for (int k = 0; k < w; ++k) {
+    const int J = __ldcs(cp + k * 32);
+    float pj[ND];
+    PVec<ND>::ld(p, J, pj);
+    float v[BB];
+#pragma unroll
+    for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);
+    float d[ND];
+#pragma unroll
+    for (int j = 0; j < ND; ++j) d[j] = J == I ? pI[j] : pj[j] - pI[j];
+#pragma unroll
+    for (int i = 0; i < ND; ++i)
+#pragma unroll
+      for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], d[j], acc[i]);
+  }
+}
+
+// One 32-node slice of q = A p with FP64 vectors and arithmetic on the FP32
+// row-sum matrix (p64 node-interleaved).
+template <int ND>
+__device__ __forceinline__ void spmv_row_rs64(const BlockMat& A, int s, int lane, const double* p, double* acc,
+                                              double* pI) {
+  constexpr int BB = ND * ND;
+  const int I = 32 * s + lane;
+  const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
+  const int* cp = A.bcol + (long long)c0 * 32 + lane;
+  const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) { acc[i] = 0.0; pI[i] = 0.0; }
+  if (I < A.nnode)
+#pragma unroll
+    for (int i = 0; i < ND; ++i) pI[i] = p[(long long)I * ND + i];
+#pragma unroll 2
+  for (int k = 0; k < w; ++k) {
+    const int J = __ldcs(cp + k * 32);
+    double pj[ND];
+    if constexpr (ND == 2) {
+      const double2 t = reinterpret_cast<const double2*>(p)[J];
+      pj[0] = t.x; pj[1] = t.y;
+    } else {
+#pragma unroll
+      for (int j = 0; j < ND; ++j) pj[j] = p[(long long)J * ND + j];
+    }
+    float v[BB];
+#pragma unroll
+    for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);
+    double d[ND];
+#pragma unroll
+    for (int j = 0; j < ND; ++j) d[j] = J == I ? pI[j] : pj[j] - pI[j];
+#pragma unroll
+    for (int i = 0; i < ND; ++i)
+#pragma unroll
+      for (int j = 0; j < ND; ++j) acc[i] = fma((double)v[i * ND + j], d[j], acc[i]);
   }
 }
 
@@ -362,9 +462,10 @@ __device__ __forceinline__ void prec64(const float* m, long long I, const double
   }
 }
 
-// FP64 mode, start of a Krylov cycle from r64: p64 = z = M r64, returns (r.z, r.r).
+// FP64 mode: zdst = z = M r64 (p64 to start a Krylov cycle, q64 for a
+// reliable update), returns (r.z, r.r).
 template <int ND>
-__device__ __forceinline__ bool b_rz64(const BSys& S, const Grp& g, double* part, double (&out)[2]) {
+__device__ __forceinline__ bool b_rz64(const BSys& S, const Grp& g, double* part, double (&out)[2], double* zdst) {
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int wid = g.rank * nw + (threadIdx.x >> 5), gw = g.size * nw;
   for (int s = wid; s < S.nslice; s += gw) {
@@ -377,7 +478,7 @@ __device__ __forceinline__ bool b_rz64(const BSys& S, const Grp& g, double* part
       prec64<ND>(S.minv, I, rv, z);
 #pragma unroll
       for (int i = 0; i < ND; ++i) {
-        S.p64[(long long)I * ND + i] = z[i];
+        zdst[(long long)I * ND + i] = z[i];
         v[0] += rv[i] * z[i];
         v[1] += rv[i] * rv[i];
       }
@@ -416,97 +517,173 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
   auto aborted = [&]() {
     if (tid == 0) { st.status = kBAborted; *S.st = st; }
   };
+  // Time slice.  Thread 0 of rank 0 decides once, before the barrier of an
+  // iteration's second sum, that the group stops after that iteration and
+  // publishes the iteration number; every CTA reads it after that barrier, so
+  // all CTAs of a gang stop after the same iteration.  A CTA that reads it one
+  // iteration early sees a number it has not reached yet and goes on.  The
+  // group stops as soon as one more iteration, as long as the last one, would
+  // end past the slice, so a slow group does not hold the whole launch.
+  volatile unsigned* const stop_at = S.gflag + 1;
+  const long long t_in = tid == 0 ? globaltimer_ns() : 0;
+  if (tid == 0) *stop_at = 0xFFFFFFFFu;
+  bool stop_sent = false, slice_end = false;
+  long long t_mark = t_in, t_step = 0;
+  auto mark_slice = [&]() {
+    if (P.slice_ns > 0 && tid == 0 && !stop_sent) {
+      const long long now = globaltimer_ns();
+      t_step = now - t_mark;
+      t_mark = now;
+      if (now + t_step - g.t0 >= P.slice_ns) {
+        *stop_at = (unsigned)(st.iter + 1);
+        stop_sent = true;
+      }
+    }
+  };
 
   if (st.phase == kPhaseNew) {
-    // ---- FP32 assembly: zero, colour by colour, unit restrained diagonals
-    const long long nv = S.nchunk * 32LL * ND * ND;
-    for (long long i = tid; i < nv; i += nt) S.bval[i] = 0.f;
-    if (tid == 0) *S.gflag = 0u;
-    if (!gsync(g)) return aborted();
+    // Setup in steps that each end at a group barrier: zero the matrix, one
+    // step per element colour (FP32 assembly), unit restrained diagonals and
+    // the block-Jacobi factors, one step per column of the row sums, and the
+    // start of the solve.  Under a time slice a group stops between steps,
+    // decided as for iterations, so a long setup spreads over launches
+    // instead of holding one.
+    volatile unsigned* const stop_step = S.gflag + 2;
+    if (tid == 0) *stop_step = 0xFFFFFFFFu;
+    bool step_sent = false;
     ElemArgs E;
     E.xyz = S.xyz; E.conn = S.conn; E.gparams = S.gparams; E.egroup = S.egroup; E.nparams = S.nparams;
     E.nip = S.nip; E.gt = S.gt; E.slot = S.slot; E.nrp = S.nrp; E.rest = S.rest; E.presc = S.presc;
     E.bsoff = S.bsoff; E.bval = S.bval; E.soff = nullptr; E.ssoff = nullptr; E.sval = nullptr; E.pseudo = nullptr;
     E.kscale = 1.0; E.mscale = 0.0; E.flags = S.gflag;
-    for (int c = 0; c < S.ncolor; ++c) {
-      const int beg = S.color_ptr[c], nel = S.color_ptr[c + 1] - beg;
-      const int* el = S.elems + beg;
-      if (S.kind == 2) {
-        for (int w = wid; w < nel; w += nw) asm_hex8_elastic_warp<float>(E, el, nel, w, s_dNf, s_Nf, s_wf);
-      } else if (S.kind == 3) {
-        for (int w = wid; w < nel; w += nw) asm_hex8_heat_warp<float>(E, el, nel, w, s_dNf, s_Nf, s_wf);
+    while (st.phase == kPhaseNew) {
+      const int k = st.sub;
+      if (k == 0) {
+        const long long nv = S.nchunk * 32LL * ND * ND;
+        for (long long i = tid; i < nv; i += nt) S.bval[i] = 0.f;
+        if (tid == 0) *S.gflag = 0u;
+      } else if (k <= S.ncolor) {
+        const int c = k - 1;
+        const int beg = S.color_ptr[c], nel = S.color_ptr[c + 1] - beg;
+        const int* el = S.elems + beg;
+        if (S.kind == 2) {
+          for (int w = wid; w < nel; w += nw) asm_hex8_elastic_warp<float>(E, el, nel, w, s_dNf, s_Nf, s_wf);
+        } else if (S.kind == 3) {
+          for (int w = wid; w < nel; w += nw) asm_hex8_heat_warp<float>(E, el, nel, w, s_dNf, s_Nf, s_wf);
+        } else {
+          for (int w = wid; 2 * w < nel; w += nw) asm_quad4_pstress_warp<float>(E, el, nel, w, s_dNf, s_Nf, s_wf);
+        }
+      } else if (k == S.ncolor + 1) {
+        for (int I = tid; I < nn; I += nt) {
+          const long long chunk = (long long)S.bsoff[I >> 5] + S.ndiag[I];
+          for (int i = 0; i < ND; ++i)
+            if (S.rest[I * ND + i]) S.bval[chunk * (32 * ND * ND) + (i * ND + i) * 32 + (I & 31)] = 1.0f;
+        }
+        if (!gsync(g)) return aborted();
+        if (ld_acquire_u32(S.gflag) & kFlagNegDiag) {
+          if (tid == 0) {
+            st.phase = kPhaseDone;
+            st.status = kBNegDiag;
+            st.busy_ns += globaltimer_ns() - t_in;
+            *S.st = st;
+          }
+          gsync(g);
+          return;
+        }
+        // block-Jacobi factors (FP64 inverse of the node diagonal block)
+        for (int I = tid; I < nn; I += nt) {
+          const long long chunk = (long long)S.bsoff[I >> 5] + S.ndiag[I];
+          double D[9] = {0}, Di[9] = {0};
+          for (int t = 0; t < ND * ND; ++t) D[t] = S.bval[chunk * 32 * ND * ND + t * 32 + (I & 31)];
+          if (ND == 1) Di[0] = 1.0 / D[0];
+          else if (ND == 2) {
+            const double id = 1.0 / (D[0] * D[3] - D[1] * D[2]);
+            Di[0] = D[3] * id; Di[1] = -D[1] * id; Di[2] = -D[2] * id; Di[3] = D[0] * id;
+          } else {
+            inv3<double>(D, Di);
+          }
+          int t = 0;
+          for (int i = 0; i < ND; ++i)
+            for (int j = i; j < ND; ++j)
+              S.minv[(long long)SM * I + (t++)] = (float)(0.5 * (Di[i * ND + j] + Di[j * ND + i]));
+        }
+      } else if (k <= S.ncolor + 1 + ND) {
+        // row-sum form: column j of every diagonal block becomes (K t_j) on
+        // the free rows, t_j = 1 on the free dofs of component j (restrained
+        // columns are eliminated), and the unit row on restrained rows
+        const int j = k - S.ncolor - 2;
+        for (int i = tid; i < n; i += nt) S.x64[i] = (i % ND == j && !S.rest[i]) ? 1.0 : 0.0;
+        if (!gsync(g)) return aborted();
+        if (!b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w, g)) return aborted();
+        for (int I = tid; I < nn; I += nt) {
+          const long long chunk = (long long)S.bsoff[I >> 5] + S.ndiag[I];
+          for (int c = 0; c < ND; ++c) {
+            const long long d = (long long)I * ND + c;
+            S.bval[chunk * (32 * ND * ND) + (c * ND + j) * 32 + (I & 31)] =
+                S.rest[d] ? (c == j ? 1.f : 0.f) : (float)S.y64[d];
+          }
+        }
       } else {
-        for (int w = wid; 2 * w < nel; w += nw) asm_quad4_pstress_warp<float>(E, el, nel, w, s_dNf, s_Nf, s_wf);
+        // x = prescribed on restrained dofs, 0 elsewhere; r = b = load - K x (free rows)
+        for (int i = tid; i < n; i += nt) {
+          S.x64[i] = S.rest[i] ? S.presc[i] : 0.0;
+          S.w64[i] = 0.0;
+          S.y32[i] = 0.f;
+        }
+        if (!gsync(g)) return aborted();
+        if (!b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w, g)) return aborted();
+        double a0[2];
+        if (!b_residual<ND>(S, g, part(), a0, true)) return aborted();
+        st.bn = sqrt(a0[1]);
+        double a2[2];
+        if (!b_rz<ND>(S, g, part(), a2, true)) return aborted();
+        st.rho = a2[0];
+        st.rr = st.maxrr = a2[1];
+        st.iter = 0;
+        st.repl = 0;
+        st.mode = 0;
+        st.cycle0 = 0;
+        st.bt = 0.f;  // p32 = z32 = M r: the first fused update gives p = z exactly
+        st.pb = 0;
+        st.phase = kPhaseIter;
+        st.status = kBRunning;
+        st.rn = sqrt(a2[1]);
+        if (a2[1] == 0.0 || st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; }
+        break;
+      }
+      if (P.slice_ns > 0 && tid == 0 && !step_sent && globaltimer_ns() - g.t0 >= P.slice_ns) {
+        *stop_step = (unsigned)k;
+        step_sent = true;
       }
       if (!gsync(g)) return aborted();
-    }
-    for (int I = tid; I < nn; I += nt) {
-      const long long chunk = (long long)S.bsoff[I >> 5] + S.ndiag[I];
-      for (int i = 0; i < ND; ++i)
-        if (S.rest[I * ND + i]) S.bval[chunk * (32 * ND * ND) + (i * ND + i) * 32 + (I & 31)] = 1.0f;
-    }
-    if (!gsync(g)) return aborted();
-    if (ld_acquire_u32(S.gflag) & kFlagNegDiag) {
-      if (tid == 0) { st.phase = kPhaseDone; st.status = kBNegDiag; *S.st = st; }
-      gsync(g);
-      return;
-    }
-    // ---- block-Jacobi factors (FP64 inverse of the node diagonal block)
-    for (int I = tid; I < nn; I += nt) {
-      const long long chunk = (long long)S.bsoff[I >> 5] + S.ndiag[I];
-      double D[9] = {0}, Di[9] = {0};
-      for (int t = 0; t < ND * ND; ++t) D[t] = S.bval[chunk * 32 * ND * ND + t * 32 + (I & 31)];
-      if (ND == 1) Di[0] = 1.0 / D[0];
-      else if (ND == 2) {
-        const double id = 1.0 / (D[0] * D[3] - D[1] * D[2]);
-        Di[0] = D[3] * id; Di[1] = -D[1] * id; Di[2] = -D[2] * id; Di[3] = D[0] * id;
-      } else {
-        inv3<double>(D, Di);
+      st.sub = k + 1;
+      if ((unsigned)k >= *stop_step) {
+        slice_end = true;
+        break;
       }
-      int t = 0;
-      for (int i = 0; i < ND; ++i)
-        for (int j = i; j < ND; ++j) S.minv[(long long)SM * I + (t++)] = (float)(0.5 * (Di[i * ND + j] + Di[j * ND + i]));
     }
-    // ---- x = prescribed on restrained dofs, 0 elsewhere; r = b = load - K x (free rows)
-    for (int i = tid; i < n; i += nt) {
-      S.x64[i] = S.rest[i] ? S.presc[i] : 0.0;
-      S.y32[i] = 0.f;
-    }
-    if (!gsync(g)) return aborted();
-    if (!b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w, g)) return aborted();
-    double a0[2];
-    if (!b_residual<ND>(S, g, part(), a0, true)) return aborted();
-    st.bn = sqrt(a0[1]);
-    double a2[2];
-    if (!b_rz<ND>(S, g, part(), a2, true)) return aborted();
-    st.rho = a2[0];
-    st.rr = st.maxrr = a2[1];
-    st.iter = 0;
-    st.repl = 0;
-    st.mode = 0;
-    st.cycle0 = 0;
-    st.bt = 0.f;  // p32 = z32 = M r: the first fused update gives p = z exactly
-    st.pb = 0;
-    st.phase = kPhaseIter;
-    st.status = kBRunning;
-    st.rn = sqrt(a2[1]);
-    if (a2[1] == 0.0 || st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; }
   }
 
   const double tolabs2 = (0.5 * P.tol * st.bn) * (0.5 * P.tol * st.bn);
   const double delta2 = P.delta * P.delta;
   int spent = 0;
-  while (st.phase == kPhaseIter && (P.budget <= 0 || spent < P.budget)) {
+  while (st.phase == kPhaseIter && (P.budget <= 0 || spent < P.budget) && !slice_end) {
     if (st.mode == 1) {
-      // ---- FP64 Jacobi-PCG, q = K p matrix-free (restrained dofs stay fixed)
-      if (!b_mf(S, M, S.p64, S.q64, s_dN, s_N, s_w, g)) return aborted();
+      // ---- FP64 vectors and arithmetic on the FP32 row-sum matrix, with the
+      // same reliable updates (restrained dofs stay fixed)
       double* pq = part();
       for (int s = wid; s < nsl; s += nw) {
+        double acc[ND], pI[ND];
+        spmv_row_rs64<ND>(A, s, lane, S.p64, acc, pI);
+        const int I = 32 * s + lane;
         double v[1] = {0.0};
+        if (I < nn) {
 #pragma unroll
-        for (int k = 0; k < ND; ++k) {
-          const long long i = 32LL * ND * s + 32 * k + lane;
-          if (i < n && !S.rest[i]) v[0] += S.p64[i] * S.q64[i];
+          for (int i = 0; i < ND; ++i) {
+            const long long d = (long long)I * ND + i;
+            S.q64[d] = acc[i];
+            if (!S.rest[d]) v[0] += pI[i] * acc[i];
+          }
         }
         slice_partial<1>(pq, nsl, s, v);
       }
@@ -523,7 +700,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
 #pragma unroll
           for (int i = 0; i < ND; ++i) {
             const long long d = (long long)I * ND + i;
-            S.x64[d] += alpha * S.p64[d];
+            S.w64[d] += alpha * S.p64[d];
             rv[i] = S.rest[d] ? 0.0 : S.r64[d] - alpha * S.q64[d];
             S.r64[d] = rv[i];
           }
@@ -538,12 +715,20 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
         slice_partial<2>(rz, nsl, s, v);
       }
       double a2[2];
+      mark_slice();
       if (!group_sum<2>(g, rz, nsl, a2)) return aborted();
       st.iter += 1;
       ++spent;
+      slice_end = (unsigned)st.iter >= *stop_at;
       if (!(a2[0] == a2[0])) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
-      if (a2[1] <= (P.tol * st.bn) * (P.tol * st.bn) || st.iter >= P.maxit) {
-        // confirm with the true residual; restart the cycle from it if short
+      if (a2[1] > st.maxrr) st.maxrr = a2[1];
+      double beta;
+      if (a2[1] < tolabs2 || a2[1] < delta2 * st.maxrr || st.iter >= P.maxit) {
+        // reliable update: fold the correction into x (x changes only here,
+        // so its rounding does not pile up over the iterations), r64 = the
+        // FP64 matrix-free true residual
+        for (int i = tid; i < n; i += nt) { S.x64[i] += S.w64[i]; S.w64[i] = 0.0; }
+        if (!gsync(g)) return aborted();
         if (!b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w, g)) return aborted();
         double a3[2];
         if (!b_residual<ND>(S, g, part(), a3, false)) return aborted();
@@ -553,14 +738,15 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
         if (st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; break; }
         if (st.iter >= P.maxit || st.repl > P.max_repl) { st.phase = kPhaseDone; st.status = kBMaxit; break; }
         double a4[2];
-        if (!b_rz64<ND>(S, g, part(), a4)) return aborted();
+        if (!b_rz64<ND>(S, g, part(), a4, S.q64)) return aborted();
+        beta = st.rho != 0.0 ? a4[0] / st.rho : 0.0;
         st.rho = a4[0];
-        st.rr = a4[1];
-        continue;
+        st.rr = st.maxrr = a4[1];
+      } else {
+        beta = a2[0] / st.rho;
+        st.rho = a2[0];
+        st.rr = a2[1];
       }
-      const double beta = a2[0] / st.rho;
-      st.rho = a2[0];
-      st.rr = a2[1];
       for (int I = tid; I < nn; I += nt) {
 #pragma unroll
         for (int i = 0; i < ND; ++i) {
@@ -594,24 +780,14 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     }
     double* pq = part();
     for (int s = wid; s < nsl; s += nw) {
-      float acc[ND];
-      if constexpr (kFused) spmv_row_fused<ND>(A, s, lane, pold, S.z32, bt0, acc);
-      else spmv_row_b<ND, true, false>(A, s, lane, pnew, acc);
+      float acc[ND], pv[ND];
+      if constexpr (kFused) spmv_row_fused<ND>(A, s, lane, pold, S.z32, bt0, acc, pv);
+      else spmv_row_rs<ND>(A, s, lane, pnew, acc, pv);
       const int I = s * 32 + lane;
       double v[1] = {0.0};
       if (I < nn) {
         NodeIO<ND>::st(S.q32, I, acc);
-        float pv[ND];
-        if constexpr (kFused) {
-          float po[ND], zv[ND];
-          PVec<ND>::ld(pold, I, po);
-          PVec<ND>::ld(S.z32, I, zv);
-#pragma unroll
-          for (int i = 0; i < ND; ++i) pv[i] = fmaf(bt0, po[i], zv[i]);
-          PVec<ND>::st(pnew, I, pv);
-        } else {
-          PVec<ND>::ld(pnew, I, pv);
-        }
+        if constexpr (kFused) PVec<ND>::st(pnew, I, pv);
         float t = 0.f;
 #pragma unroll
         for (int i = 0; i < ND; ++i) t = fmaf(pv[i], acc[i], t);
@@ -650,9 +826,11 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
       slice_partial<2>(rz, nsl, s, v);
     }
     double a2[2];
+    mark_slice();
     if (!group_sum<2>(g, rz, nsl, a2)) return aborted();
     st.iter += 1;
     ++spent;
+    slice_end = (unsigned)st.iter >= *stop_at;
     if (!(a2[0] == a2[0])) { st.phase = kPhaseDone; st.status = kBBreakdown; break; }
     double beta;
     if (a2[1] > st.maxrr) st.maxrr = a2[1];
@@ -673,7 +851,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
         // the FP32 recurrences have lost their rate: continue in FP64 from x64, r64
         st.mode = 1;
         double a4[2];
-        if (!b_rz64<ND>(S, g, part(), a4)) return aborted();
+        if (!b_rz64<ND>(S, g, part(), a4, S.p64)) return aborted();
         st.rho = a4[0];
         st.rr = st.maxrr = a4[1];
         continue;
@@ -691,13 +869,19 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     }
     st.bt = (float)beta;  // applied by the next SpMV's gather
   }
-  if (tid == 0) *S.st = st;
+  if (tid == 0) {
+    st.busy_ns += globaltimer_ns() - t_in;
+    *S.st = st;
+  }
   gsync(g);
 }
 
 // The persistent batch kernel (cooperative launch: all CTAs resident).  CTAs
 // of a gang first solve their big system together; then every CTA pulls
-// small systems active[nbig..nactive) off the work counter on its own.
+// small systems active[nbig..nactive) off the work counter on its own.  With
+// a time slice, every system stops after the iteration in which the slice
+// ends, and no CTA takes a new system after it; the host puts the systems a
+// launch did not reach first in the next one.
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restrict__ sys, const int* __restrict__ active,
                                                             const BPlan* __restrict__ plan, unsigned* bar, int* counter,
@@ -706,13 +890,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restri
   __shared__ double s_part[2 * kSharedSlices];
   __shared__ double s_dN[kMaxIP * 24], s_N[kMaxIP * 8], s_w[kMaxIP];
   __shared__ float s_dNf[kMaxIP * 24], s_Nf[kMaxIP * 8], s_wf[kMaxIP];
+  __shared__ long long s_t0;
   const BParams P = *prm;
   const BPlan pl = plan[blockIdx.x];
   if (threadIdx.x == 0) {
     gs.bar_no = 0;
     gs.abort = 0;
+    s_t0 = globaltimer_ns();
   }
   __syncthreads();
+  const long long t0 = s_t0;
   auto solve = [&](const BSys& S, const Grp& g) {
     const int nn = S.kind == 1 ? 4 : 8, ndir = S.kind == 1 ? 2 : 3;
     b_stage<double>(S.gt, S.nip, nn, ndir, s_dN, s_N, s_w);
@@ -723,17 +910,27 @@ __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restri
     else b_solve<1>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf);
   };
   if (pl.k >= 0 && pl.k < P.nbig) {
-    const Grp gang{pl.rank, pl.size, bar + pl.bar, &gs, gabort, P.spin_ns, nullptr};
+    const Grp gang{pl.rank, pl.size, bar + pl.bar, &gs, gabort, P.spin_ns, nullptr, t0};
     solve(sys[active[pl.k]], gang);
     if (gs.abort) return;
   }
-  const Grp alone{0, 1, nullptr, &gs, gabort, P.spin_ns, s_part};
+  const Grp alone{0, 1, nullptr, &gs, gabort, P.spin_ns, s_part, t0};
   for (;;) {
-    if (threadIdx.x == 0) gs.idx = *(volatile int*)gabort ? P.nactive : P.nbig + atomicAdd(counter, 1);
+    if (threadIdx.x == 0) {
+      // past the time slice no CTA starts another system, and an assembly,
+      // which is not cut short, starts only in the first half of it
+      const long long el = globaltimer_ns() - t0;
+      const bool over = P.slice_ns > 0 && el >= P.slice_ns;
+      const int k = (*(volatile int*)gabort || over) ? P.nactive : P.nbig + atomicAdd(counter, 1);
+      gs.skip = k < P.nactive && P.slice_ns > 0 && 2 * el > P.slice_ns && sys[active[k]].st->phase == kPhaseNew;
+      gs.idx = k;
+    }
     __syncthreads();
     const int k = gs.idx;
+    const bool skip = gs.skip != 0;
     __syncthreads();  // gs.idx is rewritten only after every thread has read it
     if (k >= P.nactive) return;
+    if (skip) continue;
     solve(sys[active[k]], alone);
   }
 }

@@ -794,6 +794,7 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   D.y64 = (double*)(base + L.o_y64);
   D.p64 = (double*)(base + L.o_p64);
   D.q64 = (double*)(base + L.o_q64);
+  D.w64 = (double*)(base + L.o_w64);
   D.y32 = (float*)(base + L.o_y32);
   D.r32 = (float*)(base + L.o_r32);
   D.p32 = (float*)(base + L.o_p32);
@@ -1808,6 +1809,7 @@ int beta_gpu_batch_result(beta_gpu_batch* b, int id, double* u, beta_gpu_solve_s
     st->reserved = S.st.mode;  // 1: finished in FP64 (matrix-free) after the FP32 inner solve stalled
     st->final_norm = S.st.bn > 0 ? S.st.rn / S.st.bn : S.st.rn;
     st->true_rel_residual = st->final_norm;
+    st->ms_solve = 1e-6 * (double)S.st.busy_ns;
   }
   if (u) {
     b->n_d2h += (long long)(sizeof(double) * S.ndof);
@@ -1850,6 +1852,8 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
                            {256, 4}, {256, 16}, {1024, 4}};
   double best = 1e300;
   int bt = b->threads, bg = b->gang_boost, rc = BETA_GPU_OK;
+  const long long slice = b->slice_ns;
+  b->slice_ns = 0;  // each shape runs the same iterations
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
@@ -1874,6 +1878,7 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  b->slice_ns = slice;
   if (rc != BETA_GPU_OK) return rc;
   b->threads = bt;
   b->gang_boost = bg;
@@ -1887,6 +1892,12 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
 int beta_gpu_batch_set_switch(beta_gpu_batch* b, int iters_per_cycle) {
   if (!b || iters_per_cycle < 0) return BETA_GPU_ERR_ARG;
   b->switch_iters = iters_per_cycle;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_batch_set_slice(beta_gpu_batch* b, long long slice_us) {
+  if (!b || slice_us < 0 || slice_us > 60000000LL) return BETA_GPU_ERR_ARG;
+  b->slice_ns = slice_us * 1000LL;
   return BETA_GPU_OK;
 }
 
@@ -1954,6 +1965,12 @@ int beta_gpu_server_create(beta_gpu_server** out, int device, long long budget, 
     return BETA_GPU_ERR_STATE;
   }
   *out = S.release();
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_server_set_slice(beta_gpu_server* S, long long slice_us) {
+  if (!S || slice_us < 0 || slice_us > 60000000LL) return BETA_GPU_ERR_ARG;
+  S->slice_us.store(slice_us);
   return BETA_GPU_OK;
 }
 

@@ -6,8 +6,10 @@
 //   1. admit queued requests in arrival order while the HBM pool has room
 //      (a request that cannot fit even into an empty pool is rejected);
 //   2. run one persistent launch in which every admitted system gets at most
-//      iters_per_launch PCG iterations -- systems admitted since the last
-//      launch are assembled inside it, so new work overlaps running work;
+//      iters_per_launch PCG iterations, and with a time slice (set_slice)
+//      stops after the iteration in which the slice ends -- systems admitted
+//      since the last launch are assembled inside it, so new work overlaps
+//      running work;
 //   3. retire finished systems: copy the solution to host memory, free their
 //      pool memory, record the completion time.
 // Requests join and leave between launches while the Krylov state of running
@@ -66,6 +68,7 @@ struct beta_gpu_server {
   long long pool_used = 0, pool_bytes = 0;  // copied from the batch by the worker
   long long h2d = 0, d2h = 0;                // bytes copied host->device / device->host
   double busy_ms = 0.0;  // wall time the worker spent in launches
+  std::atomic<long long> slice_us{0};  // time slice of a launch (0: iteration budget only)
 };
 
 namespace {
@@ -137,6 +140,7 @@ void server_loop(beta_gpu_server* S) {
     if (run.empty()) continue;
 
     const auto t0 = beta_gpu_server::clock::now();
+    b->slice_ns = S->slice_us.load() * 1000LL;
     int left = 0;
     const int rc = beta_gpu_batch_run(b, &S->opts, S->iters_per_launch, &left);
     const auto t1 = beta_gpu_server::clock::now();

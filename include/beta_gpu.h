@@ -343,7 +343,9 @@ BETA_GPU_API int beta_gpu_batch_add_many(beta_gpu_batch* batch, int count, const
                                          int host_threads, int* sys_ids);
 BETA_GPU_API int beta_gpu_batch_run(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int iters_per_launch,
                                     int* n_unfinished);
-/* Status/iterations of one system; u (ndof, may be NULL) receives its current solution. */
+/* Status/iterations of one system; u (ndof, may be NULL) receives its current
+ * solution.  stats->ms_solve: device time spent on the system so far (the wall
+ * time of the CTAs that solved it, summed over launches). */
 BETA_GPU_API int beta_gpu_batch_result(beta_gpu_batch* batch, int sys_id, double* u,
                                        beta_gpu_solve_stats* stats);
 BETA_GPU_API int beta_gpu_batch_remove(beta_gpu_batch* batch, int sys_id);
@@ -359,13 +361,25 @@ BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta,
  * afterwards and keeps the shape with the least time per unit of work. */
 BETA_GPU_API int beta_gpu_batch_autotune(beta_gpu_batch* batch, const beta_gpu_solve_opts* opts, int budget,
                                          int* threads_per_cta, int* gang_boost);
-/* Precision per system: a system whose FP32 inner solve needs more than
- * iters_per_cycle iterations for one residual-replacement cycle (a drop of
- * ||r|| by inner_tol) continues as FP64 Jacobi-PCG with the operator applied
- * matrix-free in FP64 (stats->reserved = 1 in beta_gpu_batch_result);
- * FP32 Krylov recurrences lose their convergence rate on ill-conditioned
- * systems.  0: never.  Default 2000.  The choice depends only on the system. */
+/* Precision per system.  The FP32 matrix of a batch system is kept in
+ * row-sum form: each diagonal block holds the block row sum of the FP64
+ * operator and the product is formed from differences, so rounding the
+ * entries to FP32 leaves the rigid-body (low-energy) modes exact.  A system
+ * whose FP32 inner solve needs more than iters_per_cycle iterations for one
+ * residual-replacement cycle (a drop of ||r|| by inner_tol) continues with
+ * FP64 vectors and arithmetic on the same FP32 matrix, with the same FP64
+ * reliable updates (stats->reserved = 1 in beta_gpu_batch_result): FP32
+ * Krylov recurrences lose their convergence rate on ill-conditioned systems
+ * such as long plates.  0: never.  Default 500.  The choice depends only on
+ * the system. */
 BETA_GPU_API int beta_gpu_batch_set_switch(beta_gpu_batch* batch, int iters_per_cycle);
+/* Time slice of a launch (0 to 60 s; 0, the default: off).  With a slice, a
+ * launch stops every system after the iteration in which the slice ends (on
+ * top of the iteration budget of beta_gpu_batch_run), and no CTA starts a new
+ * system after it; the systems a launch did not reach go first in the next.
+ * A big system then no longer holds every other one for its whole budget.
+ * Stopping and resuming leave the results unchanged. */
+BETA_GPU_API int beta_gpu_batch_set_slice(beta_gpu_batch* batch, long long slice_us);
 /* Failure-path test hook.  Sets the longest wait at a gang barrier (1 ms to
  * 10 s; default 2 s) and, with phantom != 0, plans the first gang of the next
  * launch one CTA larger than the CTAs it is given, so its first barrier can
@@ -432,6 +446,9 @@ BETA_GPU_API int beta_gpu_server_submit(beta_gpu_server* server, int kind, int n
 BETA_GPU_API int beta_gpu_server_poll(beta_gpu_server* server, long long request_id, int wait_ms, int* state,
                                       int* ndof, double* u, beta_gpu_solve_stats* stats, double* latency_ms,
                                       int release);
+/* Time slice of each launch, as beta_gpu_batch_set_slice (0, the default:
+ * iters_per_launch alone bounds a launch); takes effect at the next launch. */
+BETA_GPU_API int beta_gpu_server_set_slice(beta_gpu_server* server, long long slice_us);
 /* Queued requests end CANCELLED before admission, running ones after the current launch. */
 BETA_GPU_API int beta_gpu_server_cancel(beta_gpu_server* server, long long request_id);
 /* out[0] submitted, [1] done, [2] rejected, [3] failed, [4] cancelled,

@@ -134,6 +134,38 @@ def test_result_independent_of_gang_size_and_cta_size():
             np.testing.assert_array_equal(u0, u1)
 
 
+def test_time_sliced_launches_equal_one_launch():
+    """Launches cut by a time slice -- gangs and single CTAs, FP32 and FP64
+    modes -- give the iterates of one uninterrupted launch."""
+    models = [W.rve_hex8(12, 5), W.plate_quad4(40), _steady_heat(10), W.rve_hex8(6, 1), W.plate_quad4(7, E=2e4)]
+
+    def solve(slice_us):
+        b = Batch(hbm_budget=1 << 30)
+        b.tune(512, 64)
+        b.set_switch(30)
+        b.set_slice(slice_us)
+        ids = [b.add(m) for m in models]
+        launches = 1
+        while b.run(opts(tol=1e-12)) > 0:
+            launches += 1
+            assert launches < 20000
+        out = []
+        for i in ids:
+            rc, u, st = b.result(i)
+            assert rc == _abi.OK, st.as_dict()
+            out.append((st.iterations, st.reserved, u))
+        b.close()
+        return launches, out
+
+    n1, ref = solve(0)
+    n2, cut = solve(300)
+    assert n1 == 1 and n2 > 3
+    assert any(r for _, r, _ in ref)  # some system went on in FP64
+    for (i0, r0, u0), (i1, r1, u1) in zip(ref, cut):
+        assert i0 == i1 and r0 == r1
+        np.testing.assert_array_equal(u0, u1)
+
+
 def test_fp64_switch_matches_oracle_and_is_mix_independent(oracle):
     """A system whose FP32 cycles are long continues as FP64 matrix-free PCG;
     its answer still meets the oracle and does not depend on the mix."""

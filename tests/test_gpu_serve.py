@@ -41,9 +41,11 @@ def _alone(m, **kw):
         return u, st
 
 
-def test_served_mix_equals_each_alone_and_oracle(oracle):
+@pytest.mark.parametrize("kw", [dict(iters_per_launch=25, threads=512, gang_boost=4),
+                                dict(iters_per_launch=100000, threads=512, gang_boost=16, slice_us=400)],
+                         ids=["budget", "slice"])
+def test_served_mix_equals_each_alone_and_oracle(oracle, kw):
     models = _mix()
-    kw = dict(iters_per_launch=25, threads=512, gang_boost=4)
     solo = [_alone(m, **kw) for m in models]
     with Server(hbm_budget=1 << 30, o=opts(tol=TOL), **kw) as s:
         rids = [None] * len(models)
