@@ -108,6 +108,10 @@ struct GangShared {
   unsigned bar_no;
   int abort;
   int idx, skip;
+  // time-slice bookkeeping of the system being solved (thread 0 only; kept
+  // here rather than in registers, which the SpMV loop needs)
+  long long t_in, t_mark;
+  int stop_sent;
   double wred[2][8];
   double red[2];
 };
@@ -334,8 +338,9 @@ __device__ __forceinline__ bool b_rz(const BSys& S, const Grp& g, double* part, 
 // into the gather: p_new[J] = fmaf(bt, p_old[J], z[J]) for every column J --
 // the same arithmetic, and so the same bits, as updating p in a separate
 // pass.  Saves a pass over the vectors and a group barrier per iteration.
-// pI receives p_new of the lane's own node.
-template <int ND>
+// pI receives p_new of the lane's own node.  RS: the matrix is in row-sum
+// form (else the plain assembled one).
+template <int ND, bool RS>
 __device__ __forceinline__ void spmv_row_fused(const BlockMat& A, int s, int lane, const float* pold,
                                                const float* z, float bt, float* acc, float* pI) {
   constexpr int BB = ND * ND;
@@ -365,7 +370,8 @@ __device__ __forceinline__ void spmv_row_fused(const BlockMat& A, int s, int lan
 #pragma unroll
     for (int j = 0; j < ND; ++j) {
       const float pj = fmaf(bt, po[j], zv[j]);
-      d[j] = J == I ? pI[j] : pj - pI[j];
+      if constexpr (RS) d[j] = J == I ? pI[j] : pj - pI[j];
+      else d[j] = pj;
     }
 #pragma unroll
     for (int i = 0; i < ND; ++i)
@@ -419,7 +425,7 @@ __device__ __forceinline__ void spmv_row_rs64(const BlockMat& A, int s, int lane
   if (I < A.nnode)
 #pragma unroll
     for (int i = 0; i < ND; ++i) pI[i] = p[(long long)I * ND + i];
-#pragma unroll 2
+#pragma unroll 1
   for (int k = 0; k < w; ++k) {
     const int J = __ldcs(cp + k * 32);
     double pj[ND];
@@ -525,32 +531,59 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
   // group stops as soon as one more iteration, as long as the last one, would
   // end past the slice, so a slow group does not hold the whole launch.
   volatile unsigned* const stop_at = S.gflag + 1;
-  const long long t_in = tid == 0 ? globaltimer_ns() : 0;
+  if (threadIdx.x == 0) {
+    g.gs->t_in = g.gs->t_mark = globaltimer_ns();
+    g.gs->stop_sent = 0;
+  }
   if (tid == 0) *stop_at = 0xFFFFFFFFu;
-  bool stop_sent = false, slice_end = false;
-  long long t_mark = t_in, t_step = 0;
+  bool slice_end = false;
   auto mark_slice = [&]() {
-    if (P.slice_ns > 0 && tid == 0 && !stop_sent) {
+    if (P.slice_ns > 0 && tid == 0 && !g.gs->stop_sent) {
       const long long now = globaltimer_ns();
-      t_step = now - t_mark;
-      t_mark = now;
+      const long long t_step = now - g.gs->t_mark;
+      g.gs->t_mark = now;
       if (now + t_step - g.t0 >= P.slice_ns) {
         *stop_at = (unsigned)(st.iter + 1);
-        stop_sent = true;
+        g.gs->stop_sent = 1;
       }
     }
   };
 
+  // The FP32 inner solve runs on the row-sum form for elasticity: on quad4
+  // it costs nothing per iteration and saves iterations on long plates, on
+  // hex8 it costs ~16 % per iteration and saves 8 % of the iterations of the
+  // 512-RVE batch (2.03 s -> 1.84 s per step).  For diffusion (1 dof per
+  // node) the differences cost ~27 % per iteration, so the plain assembled
+  // matrix is kept until a switch to FP64 vectors, which converts it (FP64
+  // arithmetic needs the row sums).
+  constexpr bool kRowSum0 = ND != 1;
+  // Row-sum form, column j: column j of every diagonal block becomes (K t_j)
+  // on the free rows, t_j = 1 on the free dofs of component j (restrained
+  // columns are eliminated), and the unit row on restrained rows.  t is
+  // scratch for t_j; y64 receives K t_j.
+  auto row_sum_column = [&](int j, double* t) -> bool {
+    for (int i = tid; i < n; i += nt) t[i] = (i % ND == j && !S.rest[i]) ? 1.0 : 0.0;
+    if (!gsync(g)) return false;
+    if (!b_mf(S, M, t, S.y64, s_dN, s_N, s_w, g)) return false;
+    for (int I = tid; I < nn; I += nt) {
+      const long long chunk = (long long)S.bsoff[I >> 5] + S.ndiag[I];
+      for (int c = 0; c < ND; ++c) {
+        const long long d = (long long)I * ND + c;
+        S.bval[chunk * (32 * ND * ND) + (c * ND + j) * 32 + (I & 31)] =
+            S.rest[d] ? (c == j ? 1.f : 0.f) : (float)S.y64[d];
+      }
+    }
+    return true;
+  };
   if (st.phase == kPhaseNew) {
     // Setup in steps that each end at a group barrier: zero the matrix, one
     // step per element colour (FP32 assembly), unit restrained diagonals and
-    // the block-Jacobi factors, one step per column of the row sums, and the
-    // start of the solve.  Under a time slice a group stops between steps,
+    // the block-Jacobi factors, one step per column of the row sums
+    // (elasticity), and the start of the solve.  Under a time slice a group stops between steps,
     // decided as for iterations, so a long setup spreads over launches
     // instead of holding one.
     volatile unsigned* const stop_step = S.gflag + 2;
     if (tid == 0) *stop_step = 0xFFFFFFFFu;
-    bool step_sent = false;
     ElemArgs E;
     E.xyz = S.xyz; E.conn = S.conn; E.gparams = S.gparams; E.egroup = S.egroup; E.nparams = S.nparams;
     E.nip = S.nip; E.gt = S.gt; E.slot = S.slot; E.nrp = S.nrp; E.rest = S.rest; E.presc = S.presc;
@@ -584,7 +617,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
           if (tid == 0) {
             st.phase = kPhaseDone;
             st.status = kBNegDiag;
-            st.busy_ns += globaltimer_ns() - t_in;
+            st.busy_ns += globaltimer_ns() - g.gs->t_in;
             *S.st = st;
           }
           gsync(g);
@@ -608,21 +641,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
               S.minv[(long long)SM * I + (t++)] = (float)(0.5 * (Di[i * ND + j] + Di[j * ND + i]));
         }
       } else if (k <= S.ncolor + 1 + ND) {
-        // row-sum form: column j of every diagonal block becomes (K t_j) on
-        // the free rows, t_j = 1 on the free dofs of component j (restrained
-        // columns are eliminated), and the unit row on restrained rows
-        const int j = k - S.ncolor - 2;
-        for (int i = tid; i < n; i += nt) S.x64[i] = (i % ND == j && !S.rest[i]) ? 1.0 : 0.0;
-        if (!gsync(g)) return aborted();
-        if (!b_mf(S, M, S.x64, S.y64, s_dN, s_N, s_w, g)) return aborted();
-        for (int I = tid; I < nn; I += nt) {
-          const long long chunk = (long long)S.bsoff[I >> 5] + S.ndiag[I];
-          for (int c = 0; c < ND; ++c) {
-            const long long d = (long long)I * ND + c;
-            S.bval[chunk * (32 * ND * ND) + (c * ND + j) * 32 + (I & 31)] =
-                S.rest[d] ? (c == j ? 1.f : 0.f) : (float)S.y64[d];
-          }
-        }
+        if (!row_sum_column(k - S.ncolor - 2, S.x64)) return aborted();
       } else {
         // x = prescribed on restrained dofs, 0 elsewhere; r = b = load - K x (free rows)
         for (int i = tid; i < n; i += nt) {
@@ -651,12 +670,12 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
         if (a2[1] == 0.0 || st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; }
         break;
       }
-      if (P.slice_ns > 0 && tid == 0 && !step_sent && globaltimer_ns() - g.t0 >= P.slice_ns) {
+      if (P.slice_ns > 0 && tid == 0 && !g.gs->stop_sent && globaltimer_ns() - g.t0 >= P.slice_ns) {
         *stop_step = (unsigned)k;
-        step_sent = true;
+        g.gs->stop_sent = 1;
       }
       if (!gsync(g)) return aborted();
-      st.sub = k + 1;
+      st.sub = (k == S.ncolor + 1 && !kRowSum0) ? S.ncolor + 2 + ND : k + 1;
       if ((unsigned)k >= *stop_step) {
         slice_end = true;
         break;
@@ -781,8 +800,11 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     double* pq = part();
     for (int s = wid; s < nsl; s += nw) {
       float acc[ND], pv[ND];
-      if constexpr (kFused) spmv_row_fused<ND>(A, s, lane, pold, S.z32, bt0, acc, pv);
-      else spmv_row_rs<ND>(A, s, lane, pnew, acc, pv);
+      if constexpr (kFused) {
+        spmv_row_fused<ND, kRowSum0>(A, s, lane, pold, S.z32, bt0, acc, pv);
+      } else {
+        spmv_row_rs<ND>(A, s, lane, pnew, acc, pv);
+      }
       const int I = s * 32 + lane;
       double v[1] = {0.0};
       if (I < nn) {
@@ -848,7 +870,14 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
       if (st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; break; }
       if (st.iter >= P.maxit || st.repl > P.max_repl) { st.phase = kPhaseDone; st.status = kBMaxit; break; }
       if (long_cycle) {
-        // the FP32 recurrences have lost their rate: continue in FP64 from x64, r64
+        // the FP32 recurrences have lost their rate: continue with FP64
+        // vectors from x64, r64, on the row-sum form of the matrix (q64 is
+        // free here and serves as scratch)
+        if constexpr (!kRowSum0) {
+          for (int j = 0; j < ND; ++j)
+            if (!row_sum_column(j, S.q64)) return aborted();
+          if (!gsync(g)) return aborted();
+        }
         st.mode = 1;
         double a4[2];
         if (!b_rz64<ND>(S, g, part(), a4, S.p64)) return aborted();
@@ -870,7 +899,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     st.bt = (float)beta;  // applied by the next SpMV's gather
   }
   if (tid == 0) {
-    st.busy_ns += globaltimer_ns() - t_in;
+    st.busy_ns += globaltimer_ns() - g.gs->t_in;
     *S.st = st;
   }
   gsync(g);
