@@ -862,6 +862,7 @@ int beta_gpu_create(beta_gpu_ctx** out, int device) {
   *out = nullptr;
   std::unique_ptr<beta_gpu_ctx> c(new beta_gpu_ctx());
   c->device = device;
+  c->P.keep_scratch = true;  // a context rebuilds its structure into the same memory
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) { cudaGetLastError(); return BETA_GPU_ERR_CUDA; }
   beta_gpu_ctx* cp = c.get();

@@ -12,16 +12,47 @@ static thread_local bool t_serial = false;
 
 void pattern_serial_on_this_thread(bool on) { t_serial = on; }
 
-static void parallel_for(long long n, const std::function<void(long long, long long)>& body) {
+// Number of contiguous chunks parallel_chunks splits n items into.
+static int chunk_count(long long n) {
   unsigned hw = std::thread::hardware_concurrency();
   int t = (int)std::min<unsigned>(hw ? hw : 1, 64);
-  if (t_serial || n < 20000 || t <= 1) { body(0, n); return; }
+  return (t_serial || n < 20000 || t <= 1) ? 1 : t;
+}
+
+// body(chunk, lo, hi) over chunk_count(n) contiguous ranges, one thread each.
+static void parallel_chunks(long long n, const std::function<void(int, long long, long long)>& body) {
+  const int t = chunk_count(n);
+  if (t == 1) { body(0, 0, n); return; }
   std::vector<std::thread> th;
-  for (int k = 0; k < t; ++k) {
-    long long lo = n * k / t, hi = n * (k + 1) / t;
-    th.emplace_back(body, lo, hi);
-  }
+  for (int k = 0; k < t; ++k) th.emplace_back(body, k, n * k / t, n * (k + 1) / t);
   for (auto& x : th) x.join();
+}
+
+static void parallel_for(long long n, const std::function<void(long long, long long)>& body) {
+  parallel_chunks(n, [&](int, long long lo, long long hi) { body(lo, hi); });
+}
+
+// Empties every output of P but keeps the memory of its vectors.
+static void reset_keep(HostPattern& P) {
+  P.nnode = P.nelem = P.nnpe = P.ndpn = P.ndof = 0;
+  for (auto* v : {&P.nrp, &P.ncol, &P.ndiag, &P.color_ptr, &P.elem_by_color, &P.bsoff, &P.bcol, &P.scol, &P.soff,
+                  &P.srowlen})
+    v->clear();
+  P.slot.clear();
+  P.ssoff.clear();
+  P.sdiag.clear();
+  P.nblk = P.nchunk = P.nnz_full = P.nnz_lower = 0;
+  P.ncolor = P.nslice = P.nsslice = 0;
+}
+
+static void release_scratch(HostPattern& P) {
+  if (P.keep_scratch) return;
+  std::vector<int>().swap(P.s_icnt);
+  std::vector<int>().swap(P.s_inc);
+  std::vector<int>().swap(P.s_color);
+  std::vector<int>().swap(P.s_ufree);
+  std::vector<uint64_t>().swap(P.s_used);
+  std::vector<std::vector<int>>().swap(P.s_mark);
 }
 
 std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* conn,
@@ -33,14 +64,16 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
       return "build_pattern: first_dof must be the uniform node-major numbering ndpn*node";
   for (long long k = 0; k < (long long)nelem * nnpe; ++k)
     if (conn[k] < 0 || conn[k] >= nnode) return "build_pattern: connectivity out of range";
-  P = HostPattern();
+  reset_keep(P);
   P.nnode = nnode; P.nelem = nelem; P.nnpe = nnpe; P.ndpn = ndpn; P.ndof = nnode * ndpn;
 
   // ---- node -> element incidence -------------------------------------
-  std::vector<int> icnt(nnode + 1, 0);
+  std::vector<int>& icnt = P.s_icnt;
+  icnt.assign(nnode + 1, 0);
   for (long long k = 0; k < (long long)nelem * nnpe; ++k) icnt[conn[k] + 1]++;
   for (int i = 0; i < nnode; ++i) icnt[i + 1] += icnt[i];
-  std::vector<int> inc(icnt[nnode]);
+  std::vector<int>& inc = P.s_inc;
+  inc.resize(icnt[nnode]);
   {
     std::vector<int> fill(icnt.begin(), icnt.end() - 1);
     for (int e = 0; e < nelem; ++e)
@@ -49,15 +82,16 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
 
   // ---- node graph (two passes: count, then fill) ---------------------
   // Neighbours of node i are deduplicated with a per-thread marker array
-  // (mark[J] == i + 1 once J is taken), so only the distinct ones are sorted.
-  auto collect = [&](int i, std::vector<int>& buf, std::vector<int>& mark, bool sorted) {
+  // (mark[J] == stamp once J is taken; the stamps of the two passes differ),
+  // so only the distinct ones are sorted.
+  auto collect = [&](int i, std::vector<int>& buf, std::vector<int>& mark, int stamp, bool sorted) {
     buf.clear();
     for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
       const int* ce = conn + (long long)inc[k] * nnpe;
       for (int a = 0; a < nnpe; ++a) {
         const int J = ce[a];
-        if (mark[J] != i + 1) {
-          mark[J] = i + 1;
+        if (mark[J] != stamp) {
+          mark[J] = stamp;
           buf.push_back(J);
         }
       }
@@ -65,10 +99,16 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     if (buf.empty()) buf.push_back(i);  // a node in no element keeps its diagonal
     if (sorted) std::sort(buf.begin(), buf.end());
   };
+  P.s_mark.resize(chunk_count(nnode));
   P.nrp.assign(nnode + 1, 0);
-  parallel_for(nnode, [&](long long lo, long long hi) {
-    std::vector<int> buf, mark(nnode, 0);
-    for (long long i = lo; i < hi; ++i) { collect((int)i, buf, mark, false); P.nrp[i + 1] = (int)buf.size(); }
+  parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
+    std::vector<int> buf;
+    std::vector<int>& mark = P.s_mark[ck];
+    mark.assign(nnode, 0);
+    for (long long i = lo; i < hi; ++i) {
+      collect((int)i, buf, mark, (int)i + 1, false);
+      P.nrp[i + 1] = (int)buf.size();
+    }
   });
   for (int i = 0; i < nnode; ++i) {
     if (P.nrp[i + 1] > 65535) return "build_pattern: a node with more than 65535 neighbours";
@@ -78,10 +118,11 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   P.nblk = P.nrp[nnode];
   P.ncol.resize(P.nblk);
   P.ndiag.resize(nnode);
-  parallel_for(nnode, [&](long long lo, long long hi) {
-    std::vector<int> buf, mark(nnode, 0);
+  parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
+    std::vector<int> buf;
+    std::vector<int>& mark = P.s_mark[ck];
     for (long long i = lo; i < hi; ++i) {
-      collect((int)i, buf, mark, true);
+      collect((int)i, buf, mark, nnode + (int)i + 1, true);
       std::copy(buf.begin(), buf.end(), P.ncol.begin() + P.nrp[i]);
       P.ndiag[i] = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
     }
@@ -89,8 +130,10 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
 
   // ---- greedy element colouring (one 64-bit colour mask per node) ----
   {
-    std::vector<uint64_t> used(nnode, 0);
-    std::vector<int> color(nelem);
+    std::vector<uint64_t>& used = P.s_used;
+    used.assign(nnode, 0);
+    std::vector<int>& color = P.s_color;
+    color.resize(nelem);
     int maxc = 0;
     for (int e = 0; e < nelem; ++e) {
       const int* ce = conn + (long long)e * nnpe;
@@ -172,7 +215,8 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   // diagonal) and the free dofs j <= i of I itself; a restrained row holds its
   // diagonal only.
   {
-    std::vector<int> ufree(nnode, 0);
+    std::vector<int>& ufree = P.s_ufree;
+    ufree.assign(nnode, 0);
     for (int I = 0; I < nnode; ++I)
       for (int j = 0; j < ndpn; ++j) ufree[I] += rest[ndpn * I + j] ? 0 : 1;
     unsigned hw = std::thread::hardware_concurrency();
@@ -202,8 +246,13 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     P.nnz_lower = 0;
     for (long long v : part) P.nnz_lower += v;
   }
-  if (!with_scalar) return "";
-  return build_scalar(P, rest);
+  if (!with_scalar) {
+    release_scratch(P);
+    return "";
+  }
+  std::string msg = build_scalar(P, rest);
+  release_scratch(P);
+  return msg;
 }
 
 std::string build_scalar(HostPattern& P, const unsigned char* rest) {

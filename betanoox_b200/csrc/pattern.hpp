@@ -58,6 +58,16 @@ struct HostPattern {
 
   // reference lower-triangle pattern
   long long nnz_lower = 0;
+
+  // Scratch of the build.  A caller that rebuilds meshes of similar size
+  // into the same HostPattern (a solver context) sets keep_scratch, so the
+  // scratch and the outputs above keep their memory between builds and a
+  // rebuild writes to resident pages instead of faulting fresh ones in;
+  // otherwise the scratch is released when the build ends.
+  bool keep_scratch = false;
+  std::vector<int> s_icnt, s_inc, s_color, s_ufree;
+  std::vector<uint64_t> s_used;
+  std::vector<std::vector<int>> s_mark;  // one marker array per build thread
 };
 
 // Builds everything above.  conn: nelem*nnpe; restrained: ndof (0/1).
