@@ -1,0 +1,108 @@
+// Host structure build: a pattern rebuilt into the memory of an earlier one
+// (HostPattern::keep_scratch, as a solver context does) must equal a fresh
+// build of the same mesh in every field.  Meshes of different sizes and
+// kinds are built one after another into one reused pattern: hex8 grids
+// with 3 and 1 dofs per node, natural and shuffled node numberings, and a
+// quad4 plate with an unused node and a degenerate element (a repeated
+// node).  Exit code 0 when every build matches.
+#include "../../betanoox_b200/csrc/pattern.hpp"
+
+#include <algorithm>
+#include <cstdio>
+#include <random>
+#include <string>
+#include <vector>
+
+using betagpu::HostPattern;
+
+template <class A>
+static bool same(const A& a, const A& b) {
+  return a.size() == b.size() && std::equal(a.begin(), a.end(), b.begin());
+}
+
+static bool equal(const HostPattern& P, const HostPattern& Q) {
+  return same(P.nrp, Q.nrp) && same(P.ncol, Q.ncol) && same(P.ndiag, Q.ndiag) && P.nblk == Q.nblk &&
+         P.ncolor == Q.ncolor && same(P.color_ptr, Q.color_ptr) && same(P.elem_by_color, Q.elem_by_color) &&
+         same(P.slot, Q.slot) && P.nslice == Q.nslice && same(P.bsoff, Q.bsoff) && same(P.bcol, Q.bcol) &&
+         P.nchunk == Q.nchunk && P.nsslice == Q.nsslice && same(P.ssoff, Q.ssoff) && same(P.scol, Q.scol) &&
+         same(P.soff, Q.soff) && same(P.srowlen, Q.srowlen) && same(P.sdiag, Q.sdiag) &&
+         P.nnz_full == Q.nnz_full && P.nnz_lower == Q.nnz_lower;
+}
+
+struct Mesh {
+  std::string name;
+  int nnode = 0, nelem = 0, nnpe = 0, nd = 0;
+  std::vector<int> conn;
+  std::vector<unsigned char> rest;
+};
+
+static Mesh hex8(int n, int nd, bool shuffled, unsigned seed) {
+  Mesh M;
+  const int m = n + 1;
+  M.name = "hex8 n=" + std::to_string(n) + " nd=" + std::to_string(nd) + (shuffled ? " shuffled" : "");
+  M.nnode = m * m * m;
+  M.nelem = n * n * n;
+  M.nnpe = 8;
+  M.nd = nd;
+  std::vector<int> p(M.nnode);
+  for (int i = 0; i < M.nnode; ++i) p[i] = i;
+  if (shuffled) {
+    std::mt19937 rng(seed);
+    std::shuffle(p.begin(), p.end(), rng);
+  }
+  auto nid = [&](int a, int b, int c) { return p[a + m * (b + m * c)]; };
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        const int c[8] = {nid(i, j, k),     nid(i, j + 1, k),     nid(i, j + 1, k + 1),     nid(i, j, k + 1),
+                          nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i + 1, j + 1, k + 1), nid(i + 1, j, k + 1)};
+        M.conn.insert(M.conn.end(), c, c + 8);
+      }
+  M.rest.assign((size_t)M.nnode * nd, 0);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < m; ++i) M.rest[(size_t)nd * nid(i, j, 0)] = 1;  // first component on z = 0
+  return M;
+}
+
+static Mesh quad4_with_extras(int nx, int ny) {
+  Mesh M;
+  const int m = nx + 1;
+  M.name = "quad4 " + std::to_string(nx) + "x" + std::to_string(ny) + " + unused node + degenerate element";
+  M.nnode = m * (ny + 1) + 1;  // the last node belongs to no element
+  M.nelem = nx * ny + 1;
+  M.nnpe = 4;
+  M.nd = 2;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const int c[4] = {i + m * j, i + 1 + m * j, i + 1 + m * (j + 1), i + m * (j + 1)};
+      M.conn.insert(M.conn.end(), c, c + 4);
+    }
+  const int d[4] = {0, 1, 1, m};  // a repeated node
+  M.conn.insert(M.conn.end(), d, d + 4);
+  M.rest.assign((size_t)M.nnode * 2, 0);
+  for (int j = 0; j <= ny; ++j) M.rest[2 * (m * j)] = M.rest[2 * (m * j) + 1] = 1;
+  return M;
+}
+
+int main() {
+  std::vector<Mesh> meshes = {hex8(6, 3, false, 0),  hex8(24, 3, false, 0), hex8(24, 1, true, 3),
+                              quad4_with_extras(150, 90), hex8(40, 3, true, 5), hex8(5, 1, false, 0),
+                              hex8(24, 3, false, 0)};
+  HostPattern reused;
+  reused.keep_scratch = true;
+  int bad = 0;
+  for (const Mesh& M : meshes) {
+    std::vector<int> fd(M.nnode);
+    for (int i = 0; i < M.nnode; ++i) fd[i] = M.nd * i;
+    HostPattern fresh;
+    const std::string e1 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, M.conn.data(), fd.data(),
+                                                  M.rest.data(), fresh, true);
+    const std::string e2 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, M.conn.data(), fd.data(),
+                                                  M.rest.data(), reused, true);
+    const bool ok = e1.empty() && e2.empty() && equal(fresh, reused) && fresh.s_mark.empty() &&
+                    !reused.s_mark.empty();
+    std::printf("%-60s %s\n", M.name.c_str(), ok ? "equal" : "DIFFERENT");
+    bad += ok ? 0 : 1;
+  }
+  return bad ? 1 : 0;
+}

@@ -1,0 +1,18 @@
+"""Host structure build reused by a solver context (HostPattern::keep_scratch):
+a pattern rebuilt into the memory of an earlier, different mesh equals a
+fresh build in every field (tests/cpp/pattern_reuse_check.cpp, compiled
+here against the host sources; no GPU needed)."""
+import os
+import subprocess
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reused_pattern_equals_fresh_build(tmp_path):
+    exe = os.path.join(str(tmp_path), "pattern_reuse_check")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-pthread", "-Wall",
+                    os.path.join(ROOT, "tests", "cpp", "pattern_reuse_check.cpp"),
+                    os.path.join(ROOT, "betanoox_b200", "csrc", "pattern.cpp"), "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.count("equal") == 7
