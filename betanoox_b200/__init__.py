@@ -15,7 +15,7 @@ import numpy as np
 from . import _abi
 from ._abi import BetaGpuError, SolveOpts, SolveStats
 
-__all__ = ["Solver", "Batch", "Server", "write_lower", "read_lower", "read_mesh", "write_mesh", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
+__all__ = ["Solver", "Batch", "Server", "surface_flux_load", "write_lower", "read_lower", "read_mesh", "write_mesh", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
 
 
 def build(force: bool = False) -> str:
@@ -167,6 +167,30 @@ class Solver:
         u = np.zeros(self.model.ndof)
         self._check(self.lib.beta_gpu_heat_get_state(self.h, _ptr(u)), "heat_get_state")
         return u
+
+
+def surface_flux_load(face_conn, xyz, nodal_flux, first_dof, ndof, load=None):
+    """Consistent nodal loads of a nodal surface flux (SurfaceLoad::applyTo):
+    face_conn (nface x 4, 6 or 8 node ids), xyz (nnode x 3), nodal_flux
+    (nnode), first_dof (nnode).  The loads are added to `load` (a new zero
+    vector of ndof when None), which is returned."""
+    lib = _abi.load()
+    fc = np.ascontiguousarray(face_conn, dtype=np.int32)
+    if fc.ndim != 2:
+        raise ValueError("face_conn must be nface x nodes_per_face")
+    x = np.ascontiguousarray(xyz, dtype=np.float64)
+    q = np.ascontiguousarray(nodal_flux, dtype=np.float64)
+    fd = np.ascontiguousarray(first_dof, dtype=np.int32)
+    out = np.zeros(ndof) if load is None else load
+    if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape != (ndof,):
+        raise ValueError("load must be a contiguous float64 vector of ndof")
+    if x.shape != (q.shape[0], 3) or fd.shape != q.shape:
+        raise ValueError("xyz must be nnode x 3, nodal_flux and first_dof nnode")
+    st = lib.beta_gpu_surface_flux_load(fc.shape[0], fc.shape[1], _ptr(fc), q.shape[0], _ptr(x), _ptr(q), _ptr(fd),
+                                        int(ndof), _ptr(out))
+    if st != _abi.OK:
+        raise BetaGpuError(st, "surface_flux_load")
+    return out
 
 
 def write_lower(path, fmt, row_ptr, col, val):

@@ -1420,8 +1420,11 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
   prof.on = o->reserved & 1;
   for (int step = 0; step < nsteps; ++step) {
     if (prec == BETA_GPU_FP64) {
-      // F = -(a1+a2)/dt K u_s (formF_s_new) on free rows, + pseudo load
+      // F = load - (a1+a2)/dt K u_s (formF_s_new) on free rows, + pseudo load;
+      // the load holds the step's external heat input (point loads, surface
+      // flux: beta_gpu_surface_flux_load), as Equations adds it per step
       if ((rc = mf_apply(c, -kf, c->us.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
+      launch(c, k_axpy64, grid_for(c, n, 256), 256, 0, n, c->y64.p, 1.0, (const double*)c->load.p);
       launch(c, k_rhs64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, c->y64.p, c->pseudo.p, c->b64.p);
       if (c->have_dprev)  // start from the last increment (a smooth field changes little per step)
         CK(cudaMemcpyAsync(c->x64.p, c->dprev.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
@@ -1441,10 +1444,10 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
       CKL("k_norm2_diff");
       double ff;
       if ((rc = read_sums(c, 1, &ff))) return rc;
-      // b = rest ? presc : -(kf K u_s + Mbar ubar_ext) ; r = -(K(ks x + kf u_s) + ms M x)
+      // b = rest ? presc : load - (kf K u_s + Mbar ubar_ext) ; r = load - (K(ks x + kf u_s) + ms M x)
       launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, nullptr, c->t64.p);
       if ((rc = mf_apply(c, ks, c->t64.p, kf, c->us.p, ms, c->y64.p))) return rc;
-      launch(c, k_rhs_elim64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, nullptr, c->y64.p,
+      launch(c, k_rhs_elim64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, (const double*)c->load.p, c->y64.p,
                                                               c->b64.p, c->sums.p, c->partials.p, c->ticket.p);
       CKL("k_rhs_elim64");
       double bb;
@@ -1454,7 +1457,7 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
                c->x64.p);
       else
         CK(cudaMemcpyAsync(c->x64.p, c->t64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
-      rc = mpir_dispatch(c, !c->have_dprev, o, ks, kf, c->us.p, ms, nullptr, std::sqrt(std::max(bb, ff)), &s,
+      rc = mpir_dispatch(c, !c->have_dprev, o, ks, kf, c->us.p, ms, c->load.p, std::sqrt(std::max(bb, ff)), &s,
                          &prof);
     }
     if (rc != BETA_GPU_OK) {

@@ -230,6 +230,19 @@ BETA_GPU_API int beta_gpu_read_mesh(const char* path, int binary, int* ndim, int
 BETA_GPU_API int beta_gpu_write_mesh(const char* path, int binary, int ndim, int nnode, const double* xyz, int nelem,
                                      int nnpe, const int* conn, int first_number);
 
+/* ---- surface flux loads ---------------------------------------------------- */
+/* SurfaceLoad::applyTo (beta/BCs/SurfaceLoad.cpp:16-255) without its
+ * shared-memory coupling: for each of nsurf surface faces (node ids into the
+ * model's nodes, nodes_per_face 4 or 8 = quadrilateral, 6 = triangle, node
+ * orders of shape.cpp's shapeQuad4 / shapeQuad8 / shapeTri6) the nodal flux
+ * is interpolated to the integration points (3x3 Gauss on quadrilaterals,
+ * 7 points on triangles), scaled by |dx/dxi x dx/deta| and its consistent
+ * nodal loads are ADDED to load[first_dof[node]] (the node's first dof, as
+ * the reference does).  xyz: nnode x 3.  Host only. */
+BETA_GPU_API int beta_gpu_surface_flux_load(int nsurf, int nodes_per_face, const int* face_conn, int nnode,
+                                            const double* xyz, const double* nodal_flux, const int* first_dof,
+                                            int ndof, double* load);
+
 /* ---- system exchange formats -------------------------------------------- */
 /* The lower triangle of a symmetric matrix (SymmetricSparseMatrix order: rows
  * ascending, columns ascending, diagonal last) in BETA's dump layouts, for

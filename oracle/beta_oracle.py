@@ -314,6 +314,81 @@ def element_matrices_threaded(mesh, params, order, e0, e1, threads=0):
     return st, out
 
 
+# -- SurfaceLoad::applyTo flux integration ------------------------------------
+# Restated from beta/BCs/SurfaceLoad.cpp:16-255 (without the shared-memory
+# coupling that supplies the nodal fluxes there): per surface element, the
+# nodal flux is interpolated to each integration point, the surface scale
+# |g| = |dx/dxi x dx/deta| is formed, and w * q(xi) * N_i * |g| is added to
+# the first dof of node i.  4- and 8-node quadrilaterals use the 3x3 Gauss
+# rule (SurfaceLoad.cpp:66-99), 6-node triangles the 7-point rule with the
+# weights halved (SurfaceLoad.cpp:100-139).  Shapes: beta/elements/shape.cpp
+# (shapeQuad4 / shapeQuad8 / shapeTri6 and their derivatives, node orders
+# as there).
+_G3 = 0.774596669241483
+SURF_QUAD_RULE = (np.array([_G3, 0.0, -_G3] * 3), np.repeat([_G3, 0.0, -_G3], 3),
+                  np.array([25, 40, 25, 40, 64, 40, 25, 40, 25], dtype=float) / 81.0)
+_T7 = (0.101286507323, 0.797426985353, 0.470142064105, 0.059715871789)
+SURF_TRI_RULE = (np.array([1.0 / 3, _T7[0], _T7[0], _T7[1], _T7[2], _T7[2], _T7[3]]),
+                 np.array([1.0 / 3, _T7[0], _T7[1], _T7[0], _T7[2], _T7[3], _T7[2]]),
+                 0.5 * np.array([0.225] + [0.125939180544] * 3 + [0.132394152788] * 3))
+
+
+def surface_shape(npe, xi, eta):
+    """(N, dN/dxi, dN/deta) of a 4-node quad, 8-node quad or 6-node triangle."""
+    if npe == 4:
+        sx, se = np.array([-1.0, 1.0, 1.0, -1.0]), np.array([-1.0, -1.0, 1.0, 1.0])
+        N = 0.25 * (1 + sx * xi) * (1 + se * eta)
+        return N, 0.25 * sx * (1 + se * eta), 0.25 * se * (1 + sx * xi)
+    if npe == 8:
+        # corner, mid-side, corner, ... counter-clockwise from (-1, -1)
+        px = np.array([-1.0, 0.0, 1.0, 1.0, 1.0, 0.0, -1.0, -1.0])
+        pe = np.array([-1.0, -1.0, -1.0, 0.0, 1.0, 1.0, 1.0, 0.0])
+        N, dx, de = np.zeros(8), np.zeros(8), np.zeros(8)
+        for i in range(8):
+            a, b = px[i], pe[i]
+            if a != 0 and b != 0:  # corner
+                N[i] = 0.25 * (1 + a * xi) * (1 + b * eta) * (a * xi + b * eta - 1)
+                dx[i] = 0.25 * a * (1 + b * eta) * (2 * a * xi + b * eta)
+                de[i] = 0.25 * b * (1 + a * xi) * (a * xi + 2 * b * eta)
+            elif a == 0:  # mid-side on eta = b
+                N[i] = 0.5 * (1 - xi * xi) * (1 + b * eta)
+                dx[i] = -xi * (1 + b * eta)
+                de[i] = 0.5 * b * (1 - xi * xi)
+            else:  # mid-side on xi = a
+                N[i] = 0.5 * (1 + a * xi) * (1 - eta * eta)
+                dx[i] = 0.5 * a * (1 - eta * eta)
+                de[i] = -eta * (1 + a * xi)
+        return N, dx, de
+    if npe == 6:
+        l0 = 1 - xi - eta  # area coordinates (l0, xi, eta); corner, mid-side, ...
+        N = np.array([l0 * (2 * l0 - 1), 4 * xi * l0, xi * (2 * xi - 1), 4 * xi * eta, eta * (2 * eta - 1),
+                      4 * eta * l0])
+        dx = np.array([1 - 4 * l0, 4 * (l0 - xi), 4 * xi - 1, 4 * eta, 0.0, -4 * eta])
+        de = np.array([1 - 4 * l0, -4 * xi, 0.0, 4 * xi, 4 * eta - 1, 4 * (l0 - eta)])
+        return N, dx, de
+    raise ValueError("surface elements have 4, 6 or 8 nodes")
+
+
+def surface_flux_load(surf_conn, xyz, nodal_flux, first_dof, ndof):
+    """Nodal loads of a nodal surface flux (SurfaceLoad::applyTo)."""
+    surf_conn = np.asarray(surf_conn)
+    npe = surf_conn.shape[1]
+    xs, es, ws = SURF_TRI_RULE if npe == 6 else SURF_QUAD_RULE
+    F = np.zeros(ndof)
+    for nodes in surf_conn:
+        X = np.asarray(xyz, dtype=float)[nodes]
+        q = np.asarray(nodal_flux, dtype=float)[nodes]
+        fe = np.zeros(npe)
+        for xi, eta, w in zip(xs, es, ws):
+            N, dx, de = surface_shape(npe, xi, eta)
+            gx, ge = dx @ X, de @ X
+            modg = np.linalg.norm(np.cross(gx, ge))
+            fe += w * (N @ q) * N * modg
+        for i, nd in enumerate(nodes):
+            F[first_dof[nd]] += fe[i]
+    return F
+
+
 # -- the reference's own leaf code (oracle/_ref) -----------------------------
 class RefLeaf:
     """The reference's gauss.cpp + shape.cpp, compiled unmodified."""
@@ -328,6 +403,8 @@ class RefLeaf:
         self.lib.ref_quad_points.argtypes = [I, _dp, _dp, _dp]
         self.lib.ref_shape_hex8.argtypes = [D, D, D, _dp, _dp, _dp, _dp]
         self.lib.ref_shape_quad4.argtypes = [D, D, _dp, _dp, _dp]
+        self.lib.ref_shape_quad8.argtypes = [D, D, _dp, _dp, _dp]
+        self.lib.ref_shape_tri6.argtypes = [D, D, _dp, _dp, _dp]
 
     @staticmethod
     def available():
@@ -358,4 +435,14 @@ class RefLeaf:
     def shape_quad4(self, xi, eta):
         S, d0, d1 = (np.zeros(4) for _ in range(3))
         self.lib.ref_shape_quad4(xi, eta, S, d0, d1)
+        return S, d0, d1
+
+    def shape_quad8(self, xi, eta):
+        S, d0, d1 = (np.zeros(8) for _ in range(3))
+        self.lib.ref_shape_quad8(xi, eta, S, d0, d1)
+        return S, d0, d1
+
+    def shape_tri6(self, xi, eta):
+        S, d0, d1 = (np.zeros(6) for _ in range(3))
+        self.lib.ref_shape_tri6(xi, eta, S, d0, d1)
         return S, d0, d1

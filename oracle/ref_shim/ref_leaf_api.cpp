@@ -9,6 +9,10 @@ void shapeHex8(double* S, double xi, double eta, double zeta);
 void derivHex8(double* Sxi, double* Seta, double* Szeta, double xi, double eta, double zeta);
 void shapeQuad4(double* S, double zeta, double eta);
 void derivQuad4(double* Szeta, double* Seta, double zeta, double eta);
+void shapeQuad8(double* S, double xi, double eta);
+void derivQuad8(double* Szeta, double* Seta, double zeta, double eta);
+void shapeTri6(double* S, double xi, double eta);
+void derivTri6(double* Sxi, double* Seta, double xi, double eta);
 
 extern "C" {
 int ref_gauss_1d(int k, double* x, double* w) {
@@ -36,5 +40,14 @@ void ref_shape_hex8(double xi, double eta, double zeta, double* S, double* dxi, 
 void ref_shape_quad4(double xi, double eta, double* S, double* dxi, double* deta) {
   shapeQuad4(S, xi, eta);
   derivQuad4(dxi, deta, xi, eta);
+}
+// surface elements of SurfaceLoad::applyTo (8-node quad, 6-node triangle)
+void ref_shape_quad8(double xi, double eta, double* S, double* dxi, double* deta) {
+  shapeQuad8(S, xi, eta);
+  derivQuad8(dxi, deta, xi, eta);
+}
+void ref_shape_tri6(double xi, double eta, double* S, double* dxi, double* deta) {
+  shapeTri6(S, xi, eta);
+  derivTri6(dxi, deta, xi, eta);
 }
 }

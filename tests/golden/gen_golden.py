@@ -8,7 +8,8 @@ the compiled reference leaf library (``make -C oracle``):
 * ``ref_quadrature.json`` -- Gauss-Legendre points/weights (orders 1-8) and the
   hex/quad tensor lists (orders 1-4) produced by the reference's own
   beta/math/gaussQuadrature/gauss.cpp, and hex8/quad4 shape functions and
-  local derivatives from beta/elements/shape.cpp, at a fixed set of points.
+  local derivatives (plus the quad8/tri6 surface shapes SurfaceLoad uses)
+  from beta/elements/shape.cpp, at a fixed set of points.
   These are outputs of the reference code itself (oracle/_ref).
 * ``ref_matrix_kat.json`` -- the known answers written in the reference's
   DEBUG_MATRIX_CLASS main (beta/math/matrix.cpp:679-696).
@@ -31,11 +32,13 @@ from betanoox_b200 import workloads as W  # noqa: E402
 OUT = os.path.dirname(os.path.abspath(__file__))
 SAMPLE_HEX = [(-0.9, 0.1, 0.7), (0.3, -0.7, 0.1), (-0.57735, 0.57735, -0.57735), (0.0, 0.0, 0.0), (1.0, -1.0, 1.0)]
 SAMPLE_QUAD = [(-0.9, 0.1), (0.3, -0.7), (0.57735, -0.57735), (0.0, 0.0), (-1.0, 1.0)]
+SAMPLE_TRI = [(0.1, 0.2), (1.0 / 3, 1.0 / 3), (0.7, 0.05), (0.0, 0.0), (0.5, 0.5)]
 
 
 def ref_quadrature():
     r = bo.RefLeaf()
-    out = {"gauss": {}, "hex": {}, "quad": {}, "shape_hex8": [], "shape_quad4": []}
+    out = {"gauss": {}, "hex": {}, "quad": {}, "shape_hex8": [], "shape_quad4": [], "shape_quad8": [],
+           "shape_tri6": []}
     for k in range(1, 9):
         x, w = r.gauss_1d(k)
         out["gauss"][str(k)] = {"x": x.tolist(), "w": w.tolist()}
@@ -50,6 +53,11 @@ def ref_quadrature():
     for p in SAMPLE_QUAD:
         S, d0, d1 = r.shape_quad4(*p)
         out["shape_quad4"].append({"at": p, "S": S.tolist(), "dxi": d0.tolist(), "deta": d1.tolist()})
+        S, d0, d1 = r.shape_quad8(*p)
+        out["shape_quad8"].append({"at": p, "S": S.tolist(), "dxi": d0.tolist(), "deta": d1.tolist()})
+    for p in SAMPLE_TRI:
+        S, d0, d1 = r.shape_tri6(*p)
+        out["shape_tri6"].append({"at": p, "S": S.tolist(), "dxi": d0.tolist(), "deta": d1.tolist()})
     out["source"] = "reference gauss.cpp + shape.cpp compiled unmodified (oracle/_ref)"
     return out
 

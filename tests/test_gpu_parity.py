@@ -197,6 +197,50 @@ def test_heat_steps_match_oracle(oracle, mode):
     assert tot > 0
 
 
+def _slab_with_top_flux(nx=10, ny=8, nz=6):
+    """Diffusion slab held at T = 0 on x = 0 and x = lx only, heated by a
+    nodal flux q = 5 + 3x on its top face (SurfaceLoad::applyTo loads)."""
+    from betanoox_b200 import surface_flux_load
+    m = W.heat_slab(nx, ny, nz, order=3)
+    x = m.xyz[:, 0]
+    rest = (np.isclose(x, 0.0) | np.isclose(x, x.max())).astype(np.uint8)
+    m.restrained = rest
+    m.prescribed = np.zeros(m.ndof)
+    ztop = m.xyz[:, 2].max()
+    faces = m.conn[:, [3, 2, 6, 7]]  # hex8 face zeta = +1 (BETA node order)
+    faces = faces[np.all(np.isclose(m.xyz[faces, 2], ztop), axis=1)]
+    assert len(faces) == nx * ny
+    load = surface_flux_load(faces, m.xyz, 5.0 + 3.0 * x, m.first_dof, m.ndof)
+    load[rest.astype(bool)] = 0.0  # the restrained nodes' value is prescribed
+    m.load = load
+    u0 = m.meta["u0"].copy()
+    u0[rest.astype(bool)] = 0.0
+    return m, u0
+
+
+@pytest.mark.parametrize("mode", [_abi.MODE_FP64, _abi.MODE_MPIR])
+def test_heat_steps_with_surface_flux_match_oracle(oracle, mode):
+    m, u0 = _slab_with_top_flux()
+    assert np.abs(m.load).max() > 0
+    dt = 1e-3
+    s = oracle.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    u_ref = u0.copy()
+    for _ in range(3):
+        s.set_bc(m.restrained, m.prescribed, m.load)
+        rc, u_ref, st = s.heat_step(m.params, m.order, dt, u_ref, eps=1e-14, maxit=100000)
+        assert rc == 0
+    g = Solver()
+    g.load_model(m)
+    g.build_pattern()
+    g.heat_set_state(u0)
+    st, tot = g.heat_run(dt, 3, opts(mode=mode, tol=1e-13, inner_tol=0.01, check_every=4))
+    u = g.heat_get_state()
+    assert np.linalg.norm(u - u0) > 1e-3 * np.linalg.norm(u0)  # the flux heats the slab
+    assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-8
+
+
 def test_csr_device_pcg(oracle):
     import torch
     m = MODELS["quad4"]()
