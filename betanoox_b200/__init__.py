@@ -15,7 +15,7 @@ import numpy as np
 from . import _abi
 from ._abi import BetaGpuError, SolveOpts, SolveStats
 
-__all__ = ["Solver", "Batch", "Server", "surface_flux_load", "write_lower", "read_lower", "read_mesh", "write_mesh", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
+__all__ = ["Solver", "Batch", "Server", "surface_flux_load", "parse_element_groups", "write_lower", "read_lower", "read_mesh", "write_mesh", "SolveOpts", "SolveStats", "BetaGpuError", "build", "opts"]
 
 
 def build(force: bool = False) -> str:
@@ -167,6 +167,20 @@ class Solver:
         u = np.zeros(self.model.ndof)
         self._check(self.lib.beta_gpu_heat_get_state(self.h, _ptr(u)), "heat_get_state")
         return u
+
+
+def parse_element_groups(text, nelem, init=-1):
+    """Element -> material group map from the body of a setElementMaterial
+    block of a BETA input deck (lines "first last increment group" or
+    "all group", ended by "end"); elements not named keep `init`."""
+    lib = _abi.load()
+    g = np.full(int(nelem), int(init), dtype=np.int32)
+    n = C.c_int(0)
+    st = lib.beta_gpu_parse_element_groups(text.encode() if isinstance(text, str) else bytes(text), int(nelem),
+                                           _ptr(g), C.byref(n))
+    if st != _abi.OK:
+        raise BetaGpuError(st, "parse_element_groups: malformed setElementMaterial block")
+    return g
 
 
 def surface_flux_load(face_conn, xyz, nodal_flux, first_dof, ndof, load=None):

@@ -122,6 +122,7 @@ SIGNATURES = {
                                 _P]),
     "beta_gpu_write_mesh": (_I, [C.c_char_p, _I, _I, _I, _P, _I, _I, _P, _I]),
     "beta_gpu_surface_flux_load": (_I, [_I, _I, _P, _I, _P, _P, _P, _I, _P]),
+    "beta_gpu_parse_element_groups": (_I, [C.c_char_p, _I, _P, _P]),
     "beta_gpu_write_lower": (_I, [C.c_char_p, _I, _I, _P, _P, _P]),
     "beta_gpu_read_lower": (_I, [C.c_char_p, _I, C.POINTER(_I), C.POINTER(C.c_longlong), _P, _P, _P]),
     "beta_gpu_export_matrix": (_I, [_P, _I, _I, C.c_char_p]),

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libbeta_gpu.so")
-SOURCES = ["beta_gpu.cu", "pattern.cpp", "exchange.cpp", "mesh_io.cpp", "surface_load.cpp"]
+SOURCES = ["beta_gpu.cu", "pattern.cpp", "exchange.cpp", "mesh_io.cpp", "surface_load.cpp", "element_groups.cpp"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",

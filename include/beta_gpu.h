@@ -230,6 +230,20 @@ BETA_GPU_API int beta_gpu_read_mesh(const char* path, int binary, int* ndim, int
 BETA_GPU_API int beta_gpu_write_mesh(const char* path, int binary, int ndim, int nnode, const double* xyz, int nelem,
                                      int nnpe, const int* conn, int first_number);
 
+/* ---- material groups of an input deck -------------------------------------- */
+/* The body of a setElementMaterial block (BasicModel::ProcessSetElementProperty,
+ * BasicModel.cpp:682-775): lines "first last increment group" or
+ * "all group", blank/tab separated, with // and slash-star comments, ended
+ * by a line "end" (any case) or a negative first element.  Sets
+ * elem_group[e] for the elements named (others keep their value), in line
+ * order; *nlines (may be NULL) receives the number of lines applied.
+ * BETA_GPU_ERR_ARG for a malformed line, last >= nelem (the reference
+ * accepts last == numElements and writes past its element array), a line of
+ * 2-3 tokens that is not "all" (the reference reads undefined values), or an
+ * unpaired comment.  The map feeds beta_gpu_materials_upload's elem_group.
+ * Host only. */
+BETA_GPU_API int beta_gpu_parse_element_groups(const char* text, int nelem, int* elem_group, int* nlines);
+
 /* ---- surface flux loads ---------------------------------------------------- */
 /* SurfaceLoad::applyTo (beta/BCs/SurfaceLoad.cpp:16-255) without its
  * shared-memory coupling: for each of nsurf surface faces (node ids into the

@@ -314,6 +314,44 @@ def element_matrices_threaded(mesh, params, order, e0, e1, threads=0):
     return st, out
 
 
+# -- setElementMaterial block of an input deck ----------------------------------
+def element_groups_from_block(text, nelem, init=-1):
+    """BasicModel::ProcessSetElementProperty (BasicModel.cpp:682-775) for the
+    material command, lines read as getLineAndTokenize does
+    (getLineAndTokenize.cpp:210-237: blank/tab tokens, comments stripped,
+    empty lines skipped, case-insensitive terminator "end").  Returns the
+    group per element, or None where the reference's input would be
+    refused or undefined."""
+    import re
+    body = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    if "/*" in body:
+        return None
+    g = [init] * nelem
+    for line in body.split("\n"):
+        tok = line.split("//")[0].replace("\r", " ").split()
+        if not tok:
+            continue
+        if tok[0].lower() == "end":
+            break
+        try:
+            if len(tok) >= 2 and tok[0].lower() == "all":
+                first, last, inc, grp = 0, nelem - 1, 1, int(tok[1])
+            else:
+                first = int(tok[0])
+                if first < 0:
+                    break
+                if len(tok) < 4:
+                    return None
+                last, inc, grp = int(tok[1]), int(tok[2]), int(tok[3])
+        except ValueError:
+            return None
+        if first > last or last >= nelem or inc < 1 or grp < 0:
+            return None
+        for e in range(first, last + 1, inc):
+            g[e] = grp
+    return g
+
+
 # -- SurfaceLoad::applyTo flux integration ------------------------------------
 # Restated from beta/BCs/SurfaceLoad.cpp:16-255 (without the shared-memory
 # coupling that supplies the nodal fluxes there): per surface element, the
