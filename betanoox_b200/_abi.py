@@ -47,6 +47,7 @@ REQ_FAILED = 5
 QUAD4_PSTRESS = 1
 HEX8_ELASTIC = 2
 HEX8_HEAT = 3
+QUAD4_HEAT = 4
 
 ASM_K = 1
 ASM_MBAR = 2

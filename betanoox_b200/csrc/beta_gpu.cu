@@ -322,6 +322,9 @@ int launch_assembly(beta_gpu_ctx* c, const ElemArgs& A) {
     } else if (c->kind == BETA_GPU_HEX8_HEAT) {
       size_t sm = (size_t)nip * 33 * sizeof(T);
       launch(c, k_asm_hex8_heat<T>, grid_for(c, nel, 8), 256, sm, A, el, nel);
+    } else if (c->kind == BETA_GPU_QUAD4_HEAT) {
+      size_t sm = (size_t)nip * 13 * sizeof(T);
+      launch(c, k_asm_quad4_heat<T>, grid_for(c, nel, 16), 256, sm, A, el, nel);
     } else {
       size_t sm = (size_t)nip * 13 * sizeof(T);
       launch(c, k_asm_quad4_pstress<T>, grid_for(c, nel, 16), 256, sm, A, el, nel);
@@ -330,6 +333,8 @@ int launch_assembly(beta_gpu_ctx* c, const ElemArgs& A) {
   }
   return BETA_GPU_OK;
 }
+
+bool is_diffusion(int kind) { return kind == BETA_GPU_HEX8_HEAT || kind == BETA_GPU_QUAD4_HEAT; }
 
 // y = K (c1 w1 + c2 w2) + cm M w1 (FP64, matrix-free), y zeroed first.
 int mf_apply(beta_gpu_ctx* c, double c1, const double* w1, double c2, const double* w2, double cm,
@@ -354,6 +359,8 @@ int mf_apply(beta_gpu_ctx* c, double c1, const double* w1, double c2, const doub
       launch(c, k_mf_hex8_elastic, grid_for(c, nel, 32), 256, 0, A, el, nel, w1, w2, y);
     else if (c->kind == BETA_GPU_HEX8_HEAT)
       launch(c, k_mf_hex8_heat_t, grid_for(c, nel, 256), 256, 0, A, el, nel, w1, w2, y);
+    else if (c->kind == BETA_GPU_QUAD4_HEAT)
+      launch(c, k_mf_quad4_heat, grid_for(c, nel, 64), 256, 0, A, el, nel, w1, w2, y);
     else
       launch(c, k_mf_quad4_pstress, grid_for(c, nel, 64), 256, 0, A, el, nel, w1, w2, y);
     CKL("matrix-free kernel launch");
@@ -930,6 +937,7 @@ int beta_gpu_mesh_upload(beta_gpu_ctx* c, int kind, int ndim, int nnode, const d
     case BETA_GPU_QUAD4_PSTRESS: want_nnpe = 4; want_ndim = 2; want_ndpn = 2; break;
     case BETA_GPU_HEX8_ELASTIC: want_nnpe = 8; want_ndim = 3; want_ndpn = 3; break;
     case BETA_GPU_HEX8_HEAT: want_nnpe = 8; want_ndim = 3; want_ndpn = 1; break;
+    case BETA_GPU_QUAD4_HEAT: want_nnpe = 4; want_ndim = 2; want_ndpn = 1; break;
     default: return fail(c, BETA_GPU_ERR_UNSUPPORTED, "unknown element kind");
   }
   if (nnpe != want_nnpe || ndim != want_ndim || ndpn != want_ndpn)
@@ -1086,7 +1094,7 @@ int beta_gpu_assemble(beta_gpu_ctx* c, int what, int precision, double dt, doubl
   cudaSetDevice(c->device);
   double ks = 1.0, ms = 0.0;
   if (what == BETA_GPU_ASM_MBAR) {
-    if (c->kind != BETA_GPU_HEX8_HEAT) return fail(c, BETA_GPU_ERR_UNSUPPORTED, "Mbar assembly is for diffusion elements");
+    if (!is_diffusion(c->kind)) return fail(c, BETA_GPU_ERR_UNSUPPORTED, "Mbar assembly is for diffusion elements");
     if (!(dt > 0)) return fail(c, BETA_GPU_ERR_ARG, "dt must be positive");
     ks = alpha * dt / dt;  // (a1 K + M)/dt with a1 = alpha*dt (formK_s, HeatTransferElement3DTransient.cpp:341)
     ms = 1.0 / dt;
@@ -1378,7 +1386,7 @@ int beta_gpu_element_outputs(beta_gpu_ctx* c, const double* u, double* per_eleme
 
 int beta_gpu_heat_set_state(beta_gpu_ctx* c, const double* u0) {
   if (!c || !u0) return BETA_GPU_ERR_ARG;
-  if (c->kind != BETA_GPU_HEX8_HEAT) return fail(c, BETA_GPU_ERR_UNSUPPORTED, "transient state is for diffusion");
+  if (!is_diffusion(c->kind)) return fail(c, BETA_GPU_ERR_UNSUPPORTED, "transient state is for diffusion");
   cudaSetDevice(c->device);
   if (!all_finite(u0, c->ndof)) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite initial field");
   int rc;
@@ -1401,7 +1409,7 @@ int beta_gpu_heat_get_state(beta_gpu_ctx* c, double* u) {
 int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, const beta_gpu_solve_opts* o,
                       beta_gpu_solve_stats* stats, int* total_iterations) {
   if (!c || !o || nsteps < 0) return BETA_GPU_ERR_ARG;
-  if (c->kind != BETA_GPU_HEX8_HEAT || !c->have_us) return fail(c, BETA_GPU_ERR_STATE, "diffusion mesh and state required");
+  if (!is_diffusion(c->kind) || !c->have_us) return fail(c, BETA_GPU_ERR_STATE, "diffusion mesh and state required");
   cudaSetDevice(c->device);
   int rc;
   const int prec = o->mode == BETA_GPU_MODE_MPIR ? BETA_GPU_FP32 : BETA_GPU_FP64;

@@ -360,6 +360,67 @@ __global__ void __launch_bounds__(256) k_asm_hex8_heat(ElemArgs A, const int* __
     asm_hex8_heat_warp<T>(A, elems, nel, w, s_dN, s_N, s_w);
 }
 
+// ---- quad4 diffusion: kscale*K + mscale*M, 16 lanes per element ----------
+// HeatTransferElement2Dtransient (HeatTransferElement2DTransient.cpp:67-108):
+// K = int grad N^T diag(k11, k22) grad N (k12 = 0 for the unrotated
+// orthotropic material), M = int c N N^T, unit thickness.  Lane (a, b) of an
+// element's 16 forms entry (a, b); two elements per warp.
+template <typename T>
+__device__ __forceinline__ void asm_quad4_heat_warp(const ElemArgs& A, const int* __restrict__ elems, int nel, int w,
+    const T* s_dN, const T* s_N, const T* s_w) {
+  const int lane = threadIdx.x & 31;
+  const int sub = lane >> 4, q = lane & 15, a = q >> 2, b = q & 3;
+  const int idx = 2 * w + sub;
+  const bool valid = idx < nel;
+  const int e = elems[valid ? idx : nel - 1];
+  const int* ce = A.conn + (long long)e * 4;
+  const int J = ce[b];
+  const int n0 = ce[0];
+  const T xr0 = (T)(A.xyz[2LL * J] - A.xyz[2LL * n0]);
+  const T xr1 = (T)(A.xyz[2LL * J + 1] - A.xyz[2LL * n0 + 1]);
+  const double* pm = A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams;
+  const T k11 = pm[0], k22 = pm[1], cap = pm[3];
+  const int src = (lane & 16) + a;  // a lane holding node a of this element (b == a there)
+  T Kk = T(0), Km = T(0);
+  for (int ip = 0; ip < A.nip; ++ip) {
+    const T d0 = s_dN[ip * 8 + b], d1 = s_dN[ip * 8 + 4 + b];
+    const T M00 = group_sum<4>(d0 * xr0), M01 = group_sum<4>(d0 * xr1);
+    const T M10 = group_sum<4>(d1 * xr0), M11 = group_sum<4>(d1 * xr1);
+    const T det = M00 * M11 - M01 * M10;
+    const T id = T(1) / det;
+    const T g0 = (M11 * d0 - M01 * d1) * id;
+    const T g1 = (-M10 * d0 + M00 * d1) * id;
+    const T f = det * s_w[ip];
+    const T h0 = __shfl_sync(0xffffffffu, g0, src), h1 = __shfl_sync(0xffffffffu, g1, src);
+    Kk += (h0 * k11 * g0 + h1 * k22 * g1) * f;
+    Km += s_N[ip * 4 + a] * s_N[ip * 4 + b] * f * cap;
+  }
+  T K[1] = {T(A.kscale) * Kk + T(A.mscale) * Km};
+  if (valid && a == b && !(K[0] > 0)) atomicOr(A.flags, kFlagNegDiag);
+  const int I = __shfl_sync(0xffffffffu, J, src);
+  const int blk = A.slot[(long long)e * 16 + a * 4 + b];  // position in node I's row
+  if constexpr (sizeof(T) == 4) {
+    if (valid) scatter_block32<1>(A, I, J, blk, K);
+  } else {
+    double pl[1] = {0.0};
+    if (valid) scatter_block64<1>(A, I, J, blk, K, pl);
+    pl[0] = group_sum<4>(pl[0]);
+    if (valid && b == 0 && !A.rest[I]) A.pseudo[I] += pl[0];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_asm_quad4_heat(ElemArgs A, const int* __restrict__ elems, int nel) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_dN = reinterpret_cast<T*>(smem_raw);
+  T* s_N = s_dN + A.nip * 8;
+  T* s_w = s_N + A.nip * 4;
+  stage_gauss<T, 4, 2>(A.gt, A.nip, s_dN, s_N, s_w);
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 2 * w < nel; w += gridDim.x * wpb)
+    asm_quad4_heat_warp<T>(A, elems, nel, w, s_dN, s_N, s_w);
+}
+
 // Restrained diagonals = 1 (Equations::addMatrix, equation.cpp:500).
 template <int ND>
 __global__ void k_set_restrained_diag32(int nnode, const unsigned char* rest, const int* bsoff,

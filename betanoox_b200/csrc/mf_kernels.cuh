@@ -148,6 +148,50 @@ __global__ void __launch_bounds__(256) k_mf_quad4_pstress(MfArgs A, const int* _
     mf_quad4_pstress_warp(A, elems, nel, w, w1, w2, y, s_dN, s_w);
 }
 
+// quad4 diffusion: y += K (c1 w1 + c2 w2) + cm M w1, 4 lanes per element
+// (unit thickness, k12 = 0 as in the assembly).
+__device__ __forceinline__ void mf_quad4_heat_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
+    const double* w1, const double* w2, double* y, const double* s_dN, const double* s_N, const double* s_w) {
+  const int lane = threadIdx.x & 31, b = lane & 3;
+  const int idx = 8 * w + (lane >> 2);
+  const bool valid = idx < nel;
+  const int e = elems[valid ? idx : nel - 1];
+  const int* ce = A.conn + (long long)e * 4;
+  const int J = ce[b], n0 = ce[0];
+  const double xr0 = A.xyz[2LL * J] - A.xyz[2LL * n0], xr1 = A.xyz[2LL * J + 1] - A.xyz[2LL * n0 + 1];
+  const double vk = A.c1 * w1[J] + (w2 ? A.c2 * w2[J] : 0.0);
+  const double vm = w1[J];
+  const double* pm = A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams;
+  double f = 0;
+  for (int ip = 0; ip < A.nip; ++ip) {
+    const double d0 = s_dN[ip * 8 + b], d1 = s_dN[ip * 8 + 4 + b];
+    const double M00 = group_sum<4>(d0 * xr0), M01 = group_sum<4>(d0 * xr1);
+    const double M10 = group_sum<4>(d1 * xr0), M11 = group_sum<4>(d1 * xr1);
+    const double det = M00 * M11 - M01 * M10, id = 1.0 / det;
+    const double g0 = (M11 * d0 - M01 * d1) * id, g1 = (-M10 * d0 + M00 * d1) * id;
+    const double t0 = group_sum<4>(vk * g0), t1 = group_sum<4>(vk * g1);
+    const double Sb = s_N[ip * 4 + b];
+    const double tv = group_sum<4>(vm * Sb);
+    const double fw = det * s_w[ip];
+    f += fw * (g0 * pm[0] * t0 + g1 * pm[1] * t1 + A.cm * pm[3] * Sb * tv);
+  }
+  if (valid) y[J] += f;
+}
+
+__global__ void __launch_bounds__(256) k_mf_quad4_heat(MfArgs A, const int* __restrict__ elems, int nel,
+    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 8];
+  __shared__ double s_N[kMaxIP * 4];
+  __shared__ double s_w[kMaxIP];
+  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_dN[i] = A.gt->dN[i / 8][(i / 4) % 2][i % 4];
+  for (int i = threadIdx.x; i < A.nip * 4; i += blockDim.x) s_N[i] = A.gt->N[i / 4][i % 4];
+  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
+  __syncthreads();
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 8 * w < nel; w += gridDim.x * wpb)
+    mf_quad4_heat_warp(A, elems, nel, w, w1, w2, y, s_dN, s_N, s_w);
+}
+
 // hex8 diffusion: y += K (c1 w1 + c2 w2) + cm M w1, 8 lanes per element.
 __device__ __forceinline__ void mf_hex8_heat_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
     const double* w1, const double* w2, double* y, const double* s_dN, const double* s_N, const double* s_w) {

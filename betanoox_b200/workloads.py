@@ -212,6 +212,31 @@ def heat_slab(nx=256, ny=256, nz=64, seed=7, order=3, lx=1.0, ly=1.0):
     return m
 
 
+def heat_plate(nx=64, ny=48, seed=7, order=3, lx=1.0, heat=0.0):
+    """2D transient diffusion on [0,lx]x[0,ly] (ly = lx*ny/nx, square cells),
+    quad4 diffusion elements; k_e = exp(N(0,1)) in both directions, capacity 1;
+    T = 0 on x = 0 and x = lx; u0 a Gaussian bump (sigma = 0.15 lx) at the
+    centre, zeroed on the Dirichlet nodes; `heat` > 0 adds a uniform nodal
+    heat input of heat * cell area on the free nodes."""
+    ly = lx * ny / nx
+    xyz, conn = grid_quad4(nx, ny, lx, ly)
+    nnode = xyz.shape[0]
+    ne = conn.shape[0]
+    k = np.exp(normal(seed, 6, np.arange(ne, dtype=np.uint64)))
+    params = np.stack([k, k, k, np.ones(ne)], axis=1)
+    on = np.isclose(xyz[:, 0], 0) | np.isclose(xyz[:, 0], lx)
+    rest = on.astype(np.uint8)
+    sig = 0.15 * lx
+    c = np.array([lx / 2, ly / 2])
+    u0 = np.exp(-np.sum((xyz - c) ** 2, axis=1) / (2 * sig * sig))
+    u0[on] = 0.0
+    load = np.where(on, 0.0, heat * (lx / nx) ** 2)
+    m = Model(f"heat_plate_{nx}x{ny}", _abi.QUAD4_HEAT, 2, xyz, conn, 1, params, rest, np.zeros(nnode), load,
+              order, {"nx": nx, "ny": ny, "seed": seed})
+    m.meta["u0"] = u0
+    return m
+
+
 # ---- configuration 4: two-phase RVE cubes ------------------------------------
 def _sqdist(a, b):
     """Squared distances between the rows of a and of b, summed x, y, z in order."""

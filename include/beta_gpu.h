@@ -66,7 +66,12 @@ enum {
   BETA_GPU_HEX8_ELASTIC = 2,
   /* HeatTransferElement3Dtransient hex8 + HeatTransferMaterial: 4 params per
      group (k11, k22, k33, capacity c) (heatTransferMaterial.cpp:89-92). */
-  BETA_GPU_HEX8_HEAT = 3
+  BETA_GPU_HEX8_HEAT = 3,
+  /* HeatTransferElement2Dtransient quad4 (HeatTransferElement2DTransient.cpp:
+     67-108) + the same material and 4 params; k11 and k22 act in the plane
+     (k12 = 0 for the unrotated orthotropic material), unit thickness.  Single
+     systems only (steady solves and beta_gpu_heat_run), not batches. */
+  BETA_GPU_QUAD4_HEAT = 4
 };
 
 /* ---- what to assemble (Element::update action letters) ------------------ */

@@ -375,6 +375,32 @@ int oracle_km_hex8_heat(const double* xyz24, const double* k9, double c, int ord
   return OR_OK;
 }
 
+// quad4 diffusion: the 2D transient element's conductivity
+// K = int grad N^T k grad N (HeatTransferElement2Dtransient::addToKe,
+// HeatTransferElement2DTransient.cpp:67-108, k11/k12/k22 of the material's
+// conductivity matrix; k12 = 0 for the unrotated orthotropic
+// HeatTransferMaterial) and capacity M = int c N N^T, unit thickness.  Upper
+// triangles of 4x4 row-major K and M.
+int oracle_km_quad4_heat(const double* xy8, const double* k4, double c, int order, double* K, double* M) {
+  double xi[16], eta[16], w[16];
+  if (order < 1 || order > 4) return OR_ERR_ARG;
+  oracle_quad_points(order, xi, eta, w);
+  for (int i = 0; i < 16; ++i) K[i] = M[i] = 0.;
+  for (int ip = 0; ip < order * order; ++ip) {
+    double S[4], d0[4], d1[4], g[2][4];
+    oracle_shape_quad4(xi[ip], eta[ip], S, d0, d1);
+    double f = jac2(xy8, d0, d1, g) * w[ip];
+    for (int i = 0; i < 4; ++i)
+      for (int j = i; j < 4; ++j) {
+        double kg0 = g[0][j] * k4[0] + g[1][j] * k4[1];
+        double kg1 = g[0][j] * k4[2] + g[1][j] * k4[3];
+        K[i * 4 + j] += (kg0 * g[0][i] + kg1 * g[1][i]) * f;
+        M[i * 4 + j] += S[i] * S[j] * f * c;
+      }
+  }
+  return OR_OK;
+}
+
 // Internal force of one hex8 element for nodal displacements ue[24]:
 // strain = B ue (ElasticityElement3D::derivativesOfFields/calculateStrain
 // :124-207), stress = C strain (ElasticMaterial::calculateStress,
@@ -748,6 +774,10 @@ int oracle_element_matrix(int kind, const double* xe, const double* params, int 
     double k9[9] = {params[0], 0, 0, 0, params[1], 0, 0, 0, params[2]};
     double Mtmp[64];
     return oracle_km_hex8_heat(xe, k9, params[3], order, Ke, Me ? Me : Mtmp);
+  } else if (kind == 4) {
+    double k4[4] = {params[0], 0, 0, params[1]};
+    double Mtmp[16];
+    return oracle_km_quad4_heat(xe, k4, params[3], order, Ke, Me ? Me : Mtmp);
   }
   return OR_ERR_ARG;
 }
@@ -871,32 +901,33 @@ int oracle_element_outputs(int kind, int nelem, const int* conn, const double* x
 //   delta = solve(initGuess = u_s)                                     (:786)
 //   u_s <- u_s + delta                                                 (:800-818)
 // Restraints/prescribed values must already be set (they prescribe delta).
-int oracle_heat_step(void* h, int nelem, const int* conn, const double* xyz, const int* first_dof,
+int oracle_heat_step(void* h, int kind, int nelem, const int* conn, const double* xyz, const int* first_dof,
                      const double* params, int order, double dt, double alpha, double* u_s,
                      double eps, int maxit, OracleSolveStats* st) {
   auto* s = (OracleSystem*)h;
+  if (kind != 3 && kind != 4) return OR_ERR_ARG;
+  const int nn = kind == 3 ? 8 : 4, ndim = kind == 3 ? 3 : 2;  // hex8 / quad4 diffusion
   double a1 = alpha * dt, a2 = (1 - alpha) * dt;
   double xe[24], K[64], M[64], Mbar[64], Fe[8];
   int map[8];
   oracle_sys_zero(h);
   for (int e = 0; e < nelem; ++e) {
-    const int* ce = conn + (size_t)e * 8;
-    gather_xyz(8, 3, ce, xyz, xe);
-    const double* pe = params + (size_t)e * 4;
-    double k9[9] = {pe[0], 0, 0, 0, pe[1], 0, 0, 0, pe[2]};
-    oracle_km_hex8_heat(xe, k9, pe[3], order, K, M);
-    elem_dofs(8, 1, ce, first_dof, map);
-    for (int i = 0; i < 8; ++i)
-      for (int j = 0; j < 8; ++j) Mbar[i * 8 + j] = (a1 * K[i * 8 + j] + M[i * 8 + j]) / dt;
-    for (int i = 0; i < 8; ++i) {
+    const int* ce = conn + (size_t)e * nn;
+    gather_xyz(nn, ndim, ce, xyz, xe);
+    int rc = oracle_element_matrix(kind, xe, params + (size_t)e * 4, order, K, M);
+    if (rc) return rc;
+    elem_dofs(nn, 1, ce, first_dof, map);
+    for (int i = 0; i < nn; ++i)
+      for (int j = 0; j < nn; ++j) Mbar[i * nn + j] = (a1 * K[i * nn + j] + M[i * nn + j]) / dt;
+    for (int i = 0; i < nn; ++i) {
       double acc = 0.0;
-      for (int j = 0; j < 8; ++j) {
-        double Ku = (j >= i ? K[i * 8 + j] : K[j * 8 + i]) * u_s[map[j]];
+      for (int j = 0; j < nn; ++j) {
+        double Ku = (j >= i ? K[i * nn + j] : K[j * nn + i]) * u_s[map[j]];
         acc += -(a1 + a2) * Ku;
       }
       Fe[i] = acc / dt;
     }
-    int rc = oracle_sys_add_matrix(h, Mbar, map, 8, Fe);
+    rc = oracle_sys_add_matrix(h, Mbar, map, nn, Fe);
     if (rc) return rc;
   }
   std::vector<double> delta(s->n);

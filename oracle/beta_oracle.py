@@ -62,6 +62,7 @@ def _load():
         "oracle_ke_hex8": (I, [_dp, _dp, I, _dp]),
         "oracle_ke_quad4": (I, [_dp, _dp, I, _dp]),
         "oracle_km_hex8_heat": (I, [_dp, _dp, D, I, _dp, _dp]),
+        "oracle_km_quad4_heat": (I, [_dp, _dp, D, I, _dp, _dp]),
         "oracle_fe_hex8": (I, [_dp, _dp, I, _dp, _dp]),
         "oracle_sys_create": (V, [I]),
         "oracle_sys_destroy": (None, [V]),
@@ -80,7 +81,7 @@ def _load():
         "oracle_sys_assemble_mesh": (I, [V, I, I, I, I, I, _ip, _dp, _ip, _dp, I, I]),
         "oracle_internal_force_hex8": (I, [I, _ip, _dp, _ip, _dp, I, P, _dp, _dp]),
         "oracle_element_outputs": (I, [I, I, _ip, _dp, _ip, _dp, I, _dp, _dp]),
-        "oracle_heat_step": (I, [V, I, _ip, _dp, _ip, _dp, I, D, D, _dp, D, I, C.POINTER(SolveStats)]),
+        "oracle_heat_step": (I, [V, I, I, _ip, _dp, _ip, _dp, I, D, D, _dp, D, I, C.POINTER(SolveStats)]),
         "oracle_csr_from_sys": (V, [V]),
         "oracle_csr_destroy": (None, [V]),
         "oracle_csr_pcg_threaded": (I, [V, _dp, _dp, D, I, I, C.POINTER(SolveStats)]),
@@ -188,6 +189,14 @@ def km_hex8_heat(xyz, k3, c, order=2):
     return st, _full_from_upper(K.reshape(8, 8)), _full_from_upper(M.reshape(8, 8))
 
 
+def km_quad4_heat(xy, k2, c, order=2):
+    """quad4 diffusion K and M (full 4x4) for conductivities k2 = (k11, k22)."""
+    K, M = np.zeros(16), np.zeros(16)
+    k4 = np.diag(np.asarray(k2, dtype=np.float64)).reshape(-1)
+    st = lib().oracle_km_quad4_heat(_f64(xy).reshape(-1), _f64(k4), float(c), order, K, M)
+    return st, _full_from_upper(K.reshape(4, 4)), _full_from_upper(M.reshape(4, 4))
+
+
 def fe_hex8(xyz, C36, ue, order=2):
     Fe = np.zeros(24)
     assert lib().oracle_fe_hex8(_f64(xyz).reshape(-1), _f64(C36).reshape(-1), order, _f64(ue), Fe) == 0
@@ -277,7 +286,7 @@ class System:
         m = self.mesh
         st = SolveStats()
         u = _f64(u_s).copy()
-        rc = lib().oracle_heat_step(self.h, m.nelem, _i32(m.conn).reshape(-1), _f64(m.xyz).reshape(-1),
+        rc = lib().oracle_heat_step(self.h, m.kind, m.nelem, _i32(m.conn).reshape(-1), _f64(m.xyz).reshape(-1),
                                     _i32(m.first_dof), _f64(params).reshape(-1), order, dt, alpha, u,
                                     eps, maxit, C.byref(st))
         return rc, u, st

@@ -43,6 +43,7 @@ MODELS = {
     "hex8": lambda: W.cube_hex8(6, seed=11),
     "heat": lambda: W.heat_slab(8, 7, 5, order=3),
     "rve": lambda: W.rve_hex8(7, 5),
+    "heat2d": lambda: W.heat_plate(12, 9, heat=2.0),
 }
 
 
@@ -89,7 +90,7 @@ def test_assembly_is_deterministic():
     np.testing.assert_array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("name", ["quad4", "hex8", "heat"])
+@pytest.mark.parametrize("name", ["quad4", "hex8", "heat", "heat2d"])
 def test_matvec(oracle, name):
     m = MODELS[name]()
     s = _oracle_system(oracle, m)
@@ -113,7 +114,7 @@ def _truth(oracle, m):
     return s, u
 
 
-@pytest.mark.parametrize("name", ["quad4", "hex8", "rve"])
+@pytest.mark.parametrize("name", ["quad4", "hex8", "rve", "heat2d"])
 def test_fp64_pcg_reference_rule(oracle, name):
     """Same algorithm and stop rule (sqrt(r.r/x.x) < eps) as sparse.cpp."""
     m = MODELS[name]()
@@ -133,7 +134,7 @@ def test_fp64_pcg_reference_rule(oracle, name):
     assert err_gpu <= max(10 * err_ref, 1e-12)
 
 
-@pytest.mark.parametrize("name", ["quad4", "hex8", "rve"])
+@pytest.mark.parametrize("name", ["quad4", "hex8", "rve", "heat2d"])
 @pytest.mark.parametrize("precond", [_abi.PRECOND_JACOBI, _abi.PRECOND_BLOCK_JACOBI])
 def test_mpir_reaches_1e8(oracle, name, precond):
     m = MODELS[name]()
@@ -177,6 +178,31 @@ def test_internal_force_matches_oracle(oracle):
 @pytest.mark.parametrize("mode", [_abi.MODE_FP64, _abi.MODE_MPIR])
 def test_heat_steps_match_oracle(oracle, mode):
     m = W.heat_slab(10, 8, 6, order=3)
+    u0 = m.meta["u0"]
+    dt = 1e-3
+    s = oracle.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    u_ref = u0.copy()
+    for _ in range(3):
+        s.set_bc(m.restrained, m.prescribed, m.load)
+        rc, u_ref, st = s.heat_step(m.params, m.order, dt, u_ref, eps=1e-14, maxit=100000)
+        assert rc == 0
+    g = Solver()
+    g.load_model(m)
+    g.build_pattern()
+    g.heat_set_state(u0)
+    st, tot = g.heat_run(dt, 3, opts(mode=mode, tol=1e-13, inner_tol=0.01, check_every=4))
+    u = g.heat_get_state()
+    assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-8
+    assert tot > 0
+
+
+@pytest.mark.parametrize("mode", [_abi.MODE_FP64, _abi.MODE_MPIR])
+def test_quad4_heat_steps_match_oracle(oracle, mode):
+    """The 2D transient element (HeatTransferElement2Dtransient) marched
+    three backward-Euler steps with a heat input, against the oracle."""
+    m = W.heat_plate(16, 11, heat=2.0)
     u0 = m.meta["u0"]
     dt = 1e-3
     s = oracle.System(m)
