@@ -203,3 +203,25 @@ def test_element_outputs_known_answer_for_a_uniform_strain(oracle):
     Cq = oracle.cmat_plane_stress(q.params[0])
     np.testing.assert_allclose(outq[:, 4:7].sum(axis=0), Eq, rtol=1e-9)
     np.testing.assert_allclose(outq[:, 1:4].sum(axis=0), Cq @ Eq, rtol=1e-9)
+
+
+def test_quad4_diffusion_known_answers(oracle):
+    """2D transient element on the unit square, k = 1, c = 2: the bilinear
+    conductivity (4, -1, -2, -1)/6 and consistent capacity c A (4, 2, 1, 2)/36
+    patterns; K annihilates constants; anisotropy and scaling as they must."""
+    sq = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], dtype=float)
+    st, K, M = oracle.km_quad4_heat(sq, (1.0, 1.0), 2.0, order=2)
+    assert st == 0
+    k_row = np.array([4, -1, -2, -1]) / 6.0
+    m_row = 2.0 * np.array([4, 2, 1, 2]) / 36.0
+    for i in range(4):
+        np.testing.assert_allclose(K[i], np.roll(k_row, i), atol=1e-15)
+        np.testing.assert_allclose(M[i], np.roll(m_row, i), atol=1e-15)
+    # a rectangle 3 x 0.5 with k11 = 2, k22 = 5: K x-part scales by k11 h/w, y-part by k22 w/h
+    rect = sq * np.array([3.0, 0.5])
+    _, K2, M2 = oracle.km_quad4_heat(rect, (2.0, 5.0), 1.0, order=3)
+    assert np.abs(K2 @ np.ones(4)).max() <= 1e-13
+    assert abs(M2.sum() - 1.5) <= 1e-13  # c * area
+    kx = 2.0 * 0.5 / 3.0 * np.array([[2, -2, -1, 1], [-2, 2, 1, -1], [-1, 1, 2, -2], [1, -1, -2, 2]]) / 6.0
+    ky = 5.0 * 3.0 / 0.5 * np.array([[2, 1, -1, -2], [1, 2, -2, -1], [-1, -2, 2, 1], [-2, -1, 1, 2]]) / 6.0
+    np.testing.assert_allclose(K2, kx + ky, atol=1e-12)
