@@ -61,7 +61,7 @@ class LargeMatrix {
 // element, Factory_Material.cpp:30-47) and the Equations' restraints,
 // prescribed values and nodal loads (equation.cpp:306-341, 851-868).
 struct ModelArrays {
-  int kind = 0;  // BETA_GPU_QUAD4_PSTRESS, BETA_GPU_HEX8_ELASTIC, BETA_GPU_HEX8_HEAT
+  int kind = 0;  // BETA_GPU_QUAD4_PSTRESS, BETA_GPU_HEX8_ELASTIC, BETA_GPU_HEX8_HEAT, BETA_GPU_QUAD4_HEAT
   int ndim = 0, nnode = 0, nelem = 0, nnpe = 0, ndof_per_node = 0, integration_order = 2;
   const double* xyz = nullptr;     // nnode*ndim
   const int* conn = nullptr;       // nelem*nnpe, BETA local node order
