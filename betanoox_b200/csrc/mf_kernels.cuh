@@ -311,19 +311,4 @@ __global__ void __launch_bounds__(256) k_mf_hex8_heat_t(MfArgs A, const int* __r
     mf_hex8_heat_elem(A, elems[i], w1, w2, y, s_dN, s_N, s_w);
 }
 
-__global__ void __launch_bounds__(256) k_mf_hex8_heat(MfArgs A, const int* __restrict__ elems, int nel,
-    const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y) {
-  __shared__ double s_dN[kMaxIP * 24];
-  __shared__ double s_N[kMaxIP * 8];
-  __shared__ double s_w[kMaxIP];
-  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
-    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
-  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_N[i] = A.gt->N[i / 8][i % 8];
-  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
-  __syncthreads();
-  const int wpb = blockDim.x >> 5;
-  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 4 * w < nel; w += gridDim.x * wpb)
-    mf_hex8_heat_warp(A, elems, nel, w, w1, w2, y, s_dN, s_N, s_w);
-}
-
 }  // namespace betagpu
