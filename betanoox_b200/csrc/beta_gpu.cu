@@ -683,6 +683,8 @@ int prepare_system(int kind, int ndim, int nnode, const double* xyz, int nelem, 
     case BETA_GPU_QUAD4_PSTRESS: want_nnpe = 4; want_ndim = 2; want_ndpn = 2; want_np = 4; break;
     case BETA_GPU_HEX8_ELASTIC: want_nnpe = 8; want_ndim = 3; want_ndpn = 3; want_np = 9; break;
     case BETA_GPU_HEX8_HEAT: want_nnpe = 8; want_ndim = 3; want_ndpn = 1; want_np = 4; break;
+    case BETA_GPU_QUAD4_HEAT: err = "the 2D diffusion element is solved as a single system, not in batches";
+      return BETA_GPU_ERR_UNSUPPORTED;
     default: err = "unknown element kind"; return BETA_GPU_ERR_UNSUPPORTED;
   }
   if (nnpe != want_nnpe || ndim != want_ndim || ndpn != want_ndpn || nparams != want_np) {
