@@ -452,6 +452,7 @@ class RefLeaf:
         self.lib.ref_shape_quad4.argtypes = [D, D, _dp, _dp, _dp]
         self.lib.ref_shape_quad8.argtypes = [D, D, _dp, _dp, _dp]
         self.lib.ref_shape_tri6.argtypes = [D, D, _dp, _dp, _dp]
+        self.lib.ref_sparse_solve_file.argtypes = [C.c_char_p, _dp, D, I, _dp, C.POINTER(C.c_int)]
 
     @staticmethod
     def available():
@@ -493,3 +494,14 @@ class RefLeaf:
         S, d0, d1 = (np.zeros(6) for _ in range(3))
         self.lib.ref_shape_tri6(xi, eta, S, d0, d1)
         return S, d0, d1
+
+    def sparse_solve_file(self, path, rhs, eps, maxit=1000000):
+        """The reference's SymmetricSparseMatrix::readMatrixAddressFormat +
+        solve on a lower-triangle address-format file; returns (x, iterations)."""
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.zeros_like(rhs)
+        it = C.c_int(0)
+        rc = self.lib.ref_sparse_solve_file(str(path).encode(), rhs, float(eps), int(maxit), x, C.byref(it))
+        if rc:
+            raise ValueError("not a lower-triangle address-format file")
+        return x, it.value

@@ -1,9 +1,27 @@
-// C entry points over the reference's own gauss.cpp and shape.cpp, compiled
-// unmodified into oracle/_ref/libbeta_ref_leaf.so.  Test infrastructure: used
-// only to pin the oracle's restatement against the reference's code.
+// C entry points over the reference's own gauss.cpp, shape.cpp, sparse.cpp
+// and largeMatrix.cpp, compiled unmodified into oracle/_ref/libbeta_ref_leaf.so.
+// Test infrastructure: used only to pin the oracle's restatement against the
+// reference's code.
+#include <fstream>
+
 #include "gauss.hpp"
 #include "hexQuadPoint.hpp"
 #include "quadQuadPoint.hpp"
+#include "sparse.hpp"
+
+namespace {
+// SymmetricSparseMatrix that counts its matrix-vector products (one for the
+// initial residual, one per CG iteration).
+class CountingSparse : public SymmetricSparseMatrix {
+ public:
+  explicit CountingSparse(int n) : SymmetricSparseMatrix(n) {}
+  void vectorProduct(double* result, double* vector) override {
+    ++products;
+    SymmetricSparseMatrix::vectorProduct(result, vector);
+  }
+  int products = 0;
+};
+}  // namespace
 
 void shapeHex8(double* S, double xi, double eta, double zeta);
 void derivHex8(double* Sxi, double* Seta, double* Szeta, double xi, double eta, double zeta);
@@ -49,5 +67,25 @@ void ref_shape_quad8(double xi, double eta, double* S, double* dxi, double* deta
 void ref_shape_tri6(double xi, double eta, double* S, double* dxi, double* deta) {
   shapeTri6(S, xi, eta);
   derivTri6(dxi, deta, xi, eta);
+}
+// The reference's own Jacobi-PCG (SymmetricSparseMatrix::solve) on a lower
+// triangle read by its own readMatrixAddressFormat from a file in the
+// printMatrixAddressFormat layout ("1", "n nnz", then row-wise triples).
+// x receives the solution (rhs copied in first: solve overwrites its
+// argument); *iterations the CG iterations.  The reference exits the process
+// when maxit is reached, so callers pass a generous maxit.
+int ref_sparse_solve_file(const char* path, const double* rhs, double eps, int maxit, double* x, int* iterations) {
+  std::ifstream is(path);
+  int type = 0, n = 0;
+  if (!(is >> type >> n) || type != 1 || n <= 0) return 1;
+  CountingSparse A(n);
+  A.readMatrixAddressFormat(&is);
+  A.setSOLUTION_EPSILON(eps);
+  A.setMAX_NUMBER_ITERATIONS(maxit);
+  for (int i = 0; i < n; ++i) x[i] = rhs[i];
+  A.products = 0;
+  A.solve(x, 0);
+  *iterations = A.products - 1;
+  return 0;
 }
 }

@@ -1,0 +1,13 @@
+// Shim: the reference's error-handling macros, reduced to what sparse.cpp and
+// largeMatrix.cpp need (fatal errors abort the test program).
+#pragma once
+#include <cstdlib>
+#include <iostream>
+#define CreateErrorHandler(cls)
+#define WhoClass(x)
+#define WhoMethod(x)
+#define DeleteWhoMethod(x)
+#define DEBUG3(x)
+#define Assert(x) do { if (!(x)) { std::cerr << "allocation failed\n"; std::abort(); } } while (0)
+#define FatalError(msg) do { std::cerr << (msg) << '\n'; std::abort(); } while (0)
+#define Warning(msg) (std::cerr << (msg) << '\n')

@@ -11,6 +11,10 @@ the compiled reference leaf library (``make -C oracle``):
   local derivatives (plus the quad8/tri6 surface shapes SurfaceLoad uses)
   from beta/elements/shape.cpp, at a fixed set of points.
   These are outputs of the reference code itself (oracle/_ref).
+* ``ref_cg.json`` -- the reference's own Jacobi-PCG (sparse.cpp
+  SymmetricSparseMatrix::solve, compiled unmodified with largeMatrix.cpp)
+  on small assembled systems read by its own readMatrixAddressFormat from
+  files in the lower-triangle address format: iterations and solutions.
 * ``ref_matrix_kat.json`` -- the known answers written in the reference's
   DEBUG_MATRIX_CLASS main (beta/math/matrix.cpp:679-696).
 * ``oracle_small.json`` -- small end-to-end cases from the oracle (element
@@ -62,6 +66,27 @@ def ref_quadrature():
     return out
 
 
+def ref_cg():
+    import tempfile
+    from betanoox_b200 import _abi, write_lower
+    r = bo.RefLeaf()
+    out = {"source": "reference sparse.cpp + largeMatrix.cpp compiled unmodified (oracle/_ref)", "cases": []}
+    for name, m in [("plate_quad4_12", W.plate_quad4(12)), ("cube_hex8_5_s3", W.cube_hex8(5, seed=3)),
+                    ("heat_plate_12x9", W.heat_plate(12, 9, heat=2.0))]:
+        s = bo.System(m)
+        s.set_bc(m.restrained, m.prescribed, m.load)
+        s.build_pattern()
+        s.assemble(m.params, m.order)
+        rp, col, val = s.export_lower()
+        b = s.rhs()
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "k.txt")
+            write_lower(p, _abi.FMT_ADDRESS_LOWER, rp, col, val)
+            x, it = r.sparse_solve_file(p, b, 1e-10)
+        out["cases"].append({"name": name, "eps": 1e-10, "iterations": it, "x": x.tolist()})
+    return out
+
+
 def matrix_kat():
     return {
         "source": "beta/math/matrix.cpp:679-696 (DEBUG_MATRIX_CLASS expected values)",
@@ -105,6 +130,8 @@ def oracle_small():
 if __name__ == "__main__":
     with open(os.path.join(OUT, "ref_quadrature.json"), "w") as f:
         json.dump(ref_quadrature(), f)
+    with open(os.path.join(OUT, "ref_cg.json"), "w") as f:
+        json.dump(ref_cg(), f)
     with open(os.path.join(OUT, "ref_matrix_kat.json"), "w") as f:
         json.dump(matrix_kat(), f, indent=1)
     with open(os.path.join(OUT, "oracle_small.json"), "w") as f:

@@ -225,3 +225,35 @@ def test_quad4_diffusion_known_answers(oracle):
     kx = 2.0 * 0.5 / 3.0 * np.array([[2, -2, -1, 1], [-2, 2, 1, -1], [-1, 1, 2, -2], [1, -1, -2, 2]]) / 6.0
     ky = 5.0 * 3.0 / 0.5 * np.array([[2, 1, -1, -2], [1, 2, -2, -1], [-1, -2, 2, 1], [-2, -1, 1, 2]]) / 6.0
     np.testing.assert_allclose(K2, kx + ky, atol=1e-12)
+
+
+_CG_MODELS = {"plate_quad4_12": lambda: W.plate_quad4(12), "cube_hex8_5_s3": lambda: W.cube_hex8(5, seed=3),
+              "heat_plate_12x9": lambda: W.heat_plate(12, 9, heat=2.0)}
+
+
+@pytest.mark.parametrize("name", list(_CG_MODELS))
+def test_oracle_pcg_matches_the_reference_cg(oracle, name, tmp_path):
+    """The oracle's Jacobi-PCG against the reference's own
+    SymmetricSparseMatrix::solve (sparse.cpp, compiled unmodified): the same
+    iteration count and the same solution, on the reference's golden outputs
+    and, where oracle/_ref is built, live on the matrix written in the
+    lower-triangle address format and read by the reference's own reader."""
+    case = {c["name"]: c for c in _load("ref_cg.json")["cases"]}[name]
+    m = _CG_MODELS[name]()
+    s = oracle.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    s.assemble(m.params, m.order)
+    rc, x, st = s.solve(eps=case["eps"], maxit=100000)
+    assert rc == 0
+    xr = np.array(case["x"])
+    assert st.iterations == case["iterations"]
+    assert np.abs(x - xr).max() <= 1e-12 * np.abs(xr).max()
+    if oracle.RefLeaf.available():
+        from betanoox_b200 import _abi, write_lower
+        rp, col, val = s.export_lower()
+        p = tmp_path / "k.txt"
+        write_lower(p, _abi.FMT_ADDRESS_LOWER, rp, col, val)
+        x_live, it_live = oracle.RefLeaf().sparse_solve_file(p, s.rhs(), case["eps"])
+        assert it_live == st.iterations
+        assert np.abs(x_live - x).max() <= 1e-12 * np.abs(x).max()
