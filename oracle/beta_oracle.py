@@ -453,6 +453,12 @@ class RefLeaf:
         self.lib.ref_shape_quad8.argtypes = [D, D, _dp, _dp, _dp]
         self.lib.ref_shape_tri6.argtypes = [D, D, _dp, _dp, _dp]
         self.lib.ref_sparse_solve_file.argtypes = [C.c_char_p, _dp, D, I, _dp, C.POINTER(C.c_int)]
+        _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+        _ipc = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+        self.lib.ref_print_lower.argtypes = [C.c_char_p, I, I, _lp, _ipc, _dp]
+        self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
+        self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
+                                          C.c_void_p, C.c_void_p]
 
     @staticmethod
     def available():
@@ -494,6 +500,33 @@ class RefLeaf:
         S, d0, d1 = (np.zeros(6) for _ in range(3))
         self.lib.ref_shape_tri6(xi, eta, S, d0, d1)
         return S, d0, d1
+
+    def print_lower(self, path, fmt, row_ptr, col, val):
+        """The reference's printMatrixAddressFormat (fmt 1), ...Upper (2) or
+        printCompressedRowFormat (3) of a lower triangle."""
+        rc = self.lib.ref_print_lower(str(path).encode(), int(fmt), len(row_ptr) - 1,
+                                      np.ascontiguousarray(row_ptr, dtype=np.int64),
+                                      np.ascontiguousarray(col, dtype=np.int32),
+                                      np.ascontiguousarray(val, dtype=np.float64))
+        if rc:
+            raise ValueError("ref_print_lower failed")
+
+    def write_csr(self, path, binary, row_ptr, col, val):
+        """The reference's writeCSRMatrixIn{ASCII,Binary}."""
+        self.lib.ref_write_csr(str(path).encode(), int(binary), len(row_ptr) - 1, len(col),
+                               np.ascontiguousarray(row_ptr, dtype=np.int32), np.ascontiguousarray(col, dtype=np.int32),
+                               np.ascontiguousarray(val, dtype=np.float64))
+
+    def read_csr(self, path, binary):
+        """The reference's readCSRMatrixIn{ASCII,Binary}: (row_ptr, col, val)."""
+        n, nz = C.c_int(0), C.c_int(0)
+        self.lib.ref_read_csr(str(path).encode(), int(binary), C.byref(n), C.byref(nz), None, None, None)
+        ia = np.zeros(n.value + 1, dtype=np.int32)
+        ja = np.zeros(nz.value, dtype=np.int32)
+        a = np.zeros(nz.value)
+        self.lib.ref_read_csr(str(path).encode(), int(binary), C.byref(n), C.byref(nz), ia.ctypes.data,
+                              ja.ctypes.data, a.ctypes.data)
+        return ia, ja, a
 
     def sparse_solve_file(self, path, rhs, eps, maxit=1000000):
         """The reference's SymmetricSparseMatrix::readMatrixAddressFormat +

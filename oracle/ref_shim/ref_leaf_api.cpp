@@ -3,11 +3,18 @@
 // Test infrastructure: used only to pin the oracle's restatement against the
 // reference's code.
 #include <fstream>
+#include <string>
 
 #include "gauss.hpp"
 #include "hexQuadPoint.hpp"
 #include "quadQuadPoint.hpp"
 #include "sparse.hpp"
+
+// SparseMatrixUtility.cpp (no header in the reference)
+void writeCSRMatrixInASCII(char* filename, int*& ia, int*& ja, double*& a, int numberOfEquations, int ncoefs);
+void writeCSRMatrixInBinary(char* filename, int*& ia, int*& ja, double*& a, int numberOfEquations, int ncoefs);
+void readCSRMatrixInBinary(char* filename, int*& ia, int*& ja, double*& a, int& numberOfEquations, int& ncoefs);
+void readCSRMatrixInASCII(char* filename, int*& ia, int*& ja, double*& a, int& n);
 
 namespace {
 // SymmetricSparseMatrix that counts its matrix-vector products (one for the
@@ -86,6 +93,60 @@ int ref_sparse_solve_file(const char* path, const double* rhs, double eps, int m
   A.products = 0;
   A.solve(x, 0);
   *iterations = A.products - 1;
+  return 0;
+}
+
+// A lower triangle (0-based CSR, diagonal last in each row) written by the
+// reference's own SymmetricSparseMatrix printers: format 1
+// printMatrixAddressFormat, 2 printMatrixAddressFormatUpper, 3
+// printCompressedRowFormat.
+int ref_print_lower(const char* path, int format, int n, const long long* rp, const int* col, const double* val) {
+  SymmetricSparseMatrix A(n);
+  for (int i = 0; i < n; ++i)
+    for (long long k = rp[i]; k < rp[i + 1]; ++k) A.specifyNonZeroLocation(i, col[k]);
+  A.allocate();
+  for (int i = 0; i < n; ++i)
+    for (long long k = rp[i]; k < rp[i + 1]; ++k) A(i, col[k]) = val[k];
+  std::ofstream os(path);
+  char msg[1] = {0};
+  if (format == 1) A.printMatrixAddressFormat(msg, &os);
+  else if (format == 2) A.printMatrixAddressFormatUpper(msg, &os);
+  else if (format == 3) A.printCompressedRowFormat(msg, &os);
+  else return 1;
+  return os.good() ? 0 : 1;
+}
+
+// The reference's CSR writers and readers (SparseMatrixUtility.cpp).
+int ref_write_csr(const char* path, int binary, int n, int nnz, const int* ia_in, const int* ja_in,
+                  const double* a_in) {
+  int* ia = const_cast<int*>(ia_in);
+  int* ja = const_cast<int*>(ja_in);
+  double* a = const_cast<double*>(a_in);
+  std::string p(path);
+  if (binary) writeCSRMatrixInBinary(&p[0], ia, ja, a, n, nnz);
+  else writeCSRMatrixInASCII(&p[0], ia, ja, a, n, nnz);
+  return 0;
+}
+// Call with ia == NULL for *n and *nnz, then with arrays of n+1, nnz, nnz.
+int ref_read_csr(const char* path, int binary, int* n, int* nnz, int* ia_out, int* ja_out, double* a_out) {
+  int *ia = nullptr, *ja = nullptr, nn = 0, nz = 0;
+  double* a = nullptr;
+  std::string p(path);
+  if (binary) {
+    readCSRMatrixInBinary(&p[0], ia, ja, a, nn, nz);
+  } else {
+    readCSRMatrixInASCII(&p[0], ia, ja, a, nn);
+    nz = ia ? ia[nn] - ia[0] : 0;
+  }
+  *n = nn;
+  *nnz = nz;
+  if (ia_out) {
+    for (int i = 0; i <= nn; ++i) ia_out[i] = ia[i];
+    for (int k = 0; k < nz; ++k) { ja_out[k] = ja[k]; a_out[k] = a[k]; }
+  }
+  delete[] ia;
+  delete[] ja;
+  delete[] a;
   return 0;
 }
 }

@@ -15,6 +15,10 @@ the compiled reference leaf library (``make -C oracle``):
   SymmetricSparseMatrix::solve, compiled unmodified with largeMatrix.cpp)
   on small assembled systems read by its own readMatrixAddressFormat from
   files in the lower-triangle address format: iterations and solutions.
+* ``ref_exchange.json`` -- SHA-256 of the files the reference's own
+  writers (sparse.cpp printMatrixAddressFormat[Upper], printCompressedRowFormat;
+  SparseMatrixUtility.cpp writeCSRMatrixIn{ASCII,Binary}) produce for the
+  assembled lower triangle of a small RVE.
 * ``ref_matrix_kat.json`` -- the known answers written in the reference's
   DEBUG_MATRIX_CLASS main (beta/math/matrix.cpp:679-696).
 * ``oracle_small.json`` -- small end-to-end cases from the oracle (element
@@ -87,6 +91,31 @@ def ref_cg():
     return out
 
 
+def ref_exchange():
+    import hashlib
+    import tempfile
+    r = bo.RefLeaf()
+    m = W.rve_hex8(5, 3)
+    s = bo.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    s.assemble(m.params, m.order)
+    rp, col, val = s.export_lower()
+    out = {"source": "reference sparse.cpp / SparseMatrixUtility.cpp writers compiled unmodified (oracle/_ref)",
+           "model": "rve_hex8(5, 3)", "sha256": {}}
+    with tempfile.TemporaryDirectory() as d:
+        for name, f in [("address_lower", lambda p: r.print_lower(p, 1, rp, col, val)),
+                        ("address_upper", lambda p: r.print_lower(p, 2, rp, col, val)),
+                        ("compressed_row", lambda p: r.print_lower(p, 3, rp, col, val)),
+                        ("csr_ascii", lambda p: r.write_csr(p, 0, rp, col, val)),
+                        ("csr_binary", lambda p: r.write_csr(p, 1, rp, col, val))]:
+            p = os.path.join(d, name)
+            f(p)
+            with open(p, "rb") as fh:
+                out["sha256"][name] = hashlib.sha256(fh.read()).hexdigest()
+    return out
+
+
 def matrix_kat():
     return {
         "source": "beta/math/matrix.cpp:679-696 (DEBUG_MATRIX_CLASS expected values)",
@@ -132,6 +161,8 @@ if __name__ == "__main__":
         json.dump(ref_quadrature(), f)
     with open(os.path.join(OUT, "ref_cg.json"), "w") as f:
         json.dump(ref_cg(), f)
+    with open(os.path.join(OUT, "ref_exchange.json"), "w") as f:
+        json.dump(ref_exchange(), f, indent=1)
     with open(os.path.join(OUT, "ref_matrix_kat.json"), "w") as f:
         json.dump(matrix_kat(), f, indent=1)
     with open(os.path.join(OUT, "oracle_small.json"), "w") as f:
