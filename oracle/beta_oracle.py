@@ -456,6 +456,7 @@ class RefLeaf:
         _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
         _ipc = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
         self.lib.ref_print_lower.argtypes = [C.c_char_p, I, I, _lp, _ipc, _dp]
+        self.lib.ref_heat2d_add_to_ke.argtypes = [D, D, D, I, _dp, _dp, D, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
         self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
                                           C.c_void_p, C.c_void_p]
@@ -500,6 +501,15 @@ class RefLeaf:
         S, d0, d1 = (np.zeros(6) for _ in range(3))
         self.lib.ref_shape_tri6(xi, eta, S, d0, d1)
         return S, d0, d1
+
+    def heat2d_add_to_ke(self, k11, k22, k12, dx, dy, factor, Ke):
+        """HeatTransferElement2Dtransient::addToKe at one integration point;
+        Ke (n x n, upper triangle) is accumulated in place."""
+        n = len(dx)
+        K = np.ascontiguousarray(Ke, dtype=np.float64).reshape(-1).copy()
+        self.lib.ref_heat2d_add_to_ke(float(k11), float(k22), float(k12), n, np.ascontiguousarray(dx, dtype=float),
+                                      np.ascontiguousarray(dy, dtype=float), float(factor), K)
+        return K.reshape(n, n)
 
     def print_lower(self, path, fmt, row_ptr, col, val):
         """The reference's printMatrixAddressFormat (fmt 1), ...Upper (2) or

@@ -4,11 +4,15 @@
 // reference's code.
 #include <fstream>
 #include <string>
+#include <vector>
 
 #include "gauss.hpp"
 #include "hexQuadPoint.hpp"
 #include "quadQuadPoint.hpp"
 #include "sparse.hpp"
+#include "HeatTransferElement2DTransient.hpp"
+
+int verboseFlag = 0;  // a global the reference's element files declare extern
 
 // SparseMatrixUtility.cpp (no header in the reference)
 void writeCSRMatrixInASCII(char* filename, int*& ia, int*& ja, double*& a, int numberOfEquations, int ncoefs);
@@ -93,6 +97,33 @@ int ref_sparse_solve_file(const char* path, const double* rhs, double eps, int m
   A.products = 0;
   A.solve(x, 0);
   *iterations = A.products - 1;
+  return 0;
+}
+
+// HeatTransferElement2Dtransient::addToKe (the reference's own) at one
+// integration point: Ke (ndof x ndof, row-major, upper triangle accumulated)
+// += the conductivity term for shape-function gradients dx, dy and the
+// conductivity matrix [[k11, k12], [k12, k22]], times factor.
+int ref_heat2d_add_to_ke(double k11, double k22, double k12, int ndof, const double* dx, const double* dy,
+                         double factor, double* Ke) {
+  HeatTransferElement2Dtransient e;
+  Matrix K(ndof, ndof), c(2, 2);
+  for (int i = 0; i < ndof; ++i)
+    for (int j = 0; j < ndof; ++j) K(i, j) = Ke[i * ndof + j];
+  c(0, 0) = k11;
+  c(1, 1) = k22;
+  c(0, 1) = c(1, 0) = k12;
+  std::vector<double> gx(dx, dx + ndof), gy(dy, dy + ndof), S(ndof, 0.0);
+  InterpAndSolDerivatives id;
+  id.numberOfInterp = ndof;
+  id.S = S.data();
+  id.p_S_x1 = gx.data();
+  id.p_S_x2 = gy.data();
+  e.Ke = &K;
+  e.numDof = ndof;
+  e.addToKe(&c, &id, factor);
+  for (int i = 0; i < ndof; ++i)
+    for (int j = 0; j < ndof; ++j) Ke[i * ndof + j] = K(i, j);
   return 0;
 }
 

@@ -9,7 +9,9 @@ the compiled reference leaf library (``make -C oracle``):
   hex/quad tensor lists (orders 1-4) produced by the reference's own
   beta/math/gaussQuadrature/gauss.cpp, and hex8/quad4 shape functions and
   local derivatives (plus the quad8/tri6 surface shapes SurfaceLoad uses)
-  from beta/elements/shape.cpp, at a fixed set of points.
+  from beta/elements/shape.cpp, at a fixed set of points, and the
+  conductivity matrix of one distorted quad4 accumulated by the reference's
+  own HeatTransferElement2Dtransient::addToKe over its own Gauss points.
   These are outputs of the reference code itself (oracle/_ref).
 * ``ref_cg.json`` -- the reference's own Jacobi-PCG (sparse.cpp
   SymmetricSparseMatrix::solve, compiled unmodified with largeMatrix.cpp)
@@ -66,7 +68,19 @@ def ref_quadrature():
     for p in SAMPLE_TRI:
         S, d0, d1 = r.shape_tri6(*p)
         out["shape_tri6"].append({"at": p, "S": S.tolist(), "dxi": d0.tolist(), "deta": d1.tolist()})
-    out["source"] = "reference gauss.cpp + shape.cpp compiled unmodified (oracle/_ref)"
+    xy = np.array([[0.0, 0.0], [1.3, 0.1], [1.1, 0.9], [-0.1, 1.2]])
+    out["heat2d_ke"] = {"xy": xy.tolist(), "k11": 2.0, "k22": 0.7, "orders": {}}
+    for order in (2, 3):
+        xi, eta, w = r.quad_points(order)
+        K = np.zeros((4, 4))
+        for a, b, wt in zip(xi, eta, w):
+            _, dxi, deta = r.shape_quad4(a, b)
+            J = np.array([dxi @ xy, deta @ xy])
+            g = np.linalg.solve(J, np.array([dxi, deta]))
+            K = r.heat2d_add_to_ke(2.0, 0.7, 0.0, g[0], g[1], np.linalg.det(J) * wt, K)
+        out["heat2d_ke"]["orders"][str(order)] = K.tolist()
+    out["source"] = ("reference gauss.cpp + shape.cpp + HeatTransferElement2DTransient.cpp compiled "
+                     "unmodified (oracle/_ref)")
     return out
 
 

@@ -257,3 +257,17 @@ def test_oracle_pcg_matches_the_reference_cg(oracle, name, tmp_path):
         x_live, it_live = oracle.RefLeaf().sparse_solve_file(p, s.rhs(), case["eps"])
         assert it_live == st.iterations
         assert np.abs(x_live - x).max() <= 1e-12 * np.abs(x).max()
+
+
+def test_quad4_diffusion_equals_the_reference_addToKe(oracle):
+    """The oracle's 2D diffusion conductivity against the reference's own
+    HeatTransferElement2Dtransient::addToKe (compiled unmodified),
+    accumulated over the reference's Gauss points on a distorted quad."""
+    case = _load("ref_quadrature.json")["heat2d_ke"]
+    xy = np.array(case["xy"])
+    iu = np.triu_indices(4)
+    for order, Kref in case["orders"].items():
+        st, K, _ = oracle.km_quad4_heat(xy, (case["k11"], case["k22"]), 1.0, order=int(order))
+        assert st == 0
+        Kref = np.array(Kref)
+        assert np.abs(K[iu] - Kref[iu]).max() <= 1e-14 * np.abs(Kref).max()
