@@ -99,7 +99,8 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     if (buf.empty()) buf.push_back(i);  // a node in no element keeps its diagonal
     if (sorted) std::sort(buf.begin(), buf.end());
   };
-  P.s_mark.resize(chunk_count(nnode));
+  const int nck = chunk_count(nnode);
+  P.s_mark.resize(2 * nck);  // per chunk: the marker, and the positions of the current row
   P.nrp.assign(nnode + 1, 0);
   parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
     std::vector<int> buf;
@@ -118,13 +119,32 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   P.nblk = P.nrp[nnode];
   P.ncol.resize(P.nblk);
   P.ndiag.resize(nnode);
+  // The fill pass also writes the element -> node-pair block map: with row i
+  // sorted, pos[J] holds J's position in it, so each incident element (e, a)
+  // with conn[e][a] == i gets slot[e][a][b] = position of conn[e][b] by
+  // lookup (every node of the element is in the row).  Each (e, a) belongs to
+  // one row, so the writes do not overlap, and each row is read once.
+  const int npair = nnpe * nnpe;
+  P.slot.resize((size_t)nelem * npair);
   parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
     std::vector<int> buf;
     std::vector<int>& mark = P.s_mark[ck];
+    std::vector<int>& pos = P.s_mark[nck + ck];
+    if ((long long)pos.size() < nnode) pos.resize(nnode);
     for (long long i = lo; i < hi; ++i) {
       collect((int)i, buf, mark, nnode + (int)i + 1, true);
       std::copy(buf.begin(), buf.end(), P.ncol.begin() + P.nrp[i]);
       P.ndiag[i] = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
+      for (int k = 0; k < (int)buf.size(); ++k) pos[buf[k]] = k;
+      for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
+        const long long e = inc[k];
+        const int* ce = conn + e * nnpe;
+        for (int a = 0; a < nnpe; ++a) {
+          if (ce[a] != (int)i) continue;
+          uint16_t* sl = P.slot.data() + e * npair + a * nnpe;
+          for (int b = 0; b < nnpe; ++b) sl[b] = (uint16_t)pos[ce[b]];
+        }
+      }
     }
   });
 
@@ -153,37 +173,6 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     std::vector<int> fill(P.color_ptr.begin(), P.color_ptr.end() - 1);
     for (int e = 0; e < nelem; ++e) P.elem_by_color[fill[color[e]]++] = e;
   }
-
-  // ---- element -> node-pair block map --------------------------------
-  const int npair = nnpe * nnpe;
-  P.slot.resize((size_t)nelem * npair);
-  // The element's nodes are sorted once; each row is then walked once
-  // alongside them (a merge) instead of searched per pair.
-  parallel_for(nelem, [&](long long lo, long long hi) {
-    int ord[8], sv[8];
-    for (long long e = lo; e < hi; ++e) {
-      const int* ce = conn + e * nnpe;
-      for (int b = 0; b < nnpe; ++b) {  // insertion sort of the element's <= 8 nodes
-        int t = b;
-        while (t > 0 && sv[t - 1] > ce[b]) {
-          sv[t] = sv[t - 1];
-          ord[t] = ord[t - 1];
-          --t;
-        }
-        sv[t] = ce[b];
-        ord[t] = b;
-      }
-      for (int a = 0; a < nnpe; ++a) {
-        const int I = ce[a];
-        const int rb = P.nrp[I], re = P.nrp[I + 1];
-        int k = rb;
-        for (int t = 0; t < nnpe; ++t) {
-          while (k < re && P.ncol[k] < sv[t]) ++k;  // every element node is in row I
-          P.slot[e * npair + a * nnpe + ord[t]] = (uint16_t)(k - rb);
-        }
-      }
-    }
-  });
 
   // ---- node-block sliced ELL ------------------------------------------
   P.nslice = (nnode + 31) / 32;
