@@ -68,16 +68,24 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   P.nnode = nnode; P.nelem = nelem; P.nnpe = nnpe; P.ndpn = ndpn; P.ndof = nnode * ndpn;
 
   // ---- node -> element incidence -------------------------------------
+  // Counted and filled by all threads with atomic adds; the order of a
+  // node's elements is then arbitrary, which nothing downstream sees (rows
+  // are sorted, slots are looked up, the colouring walks elements in order).
   std::vector<int>& icnt = P.s_icnt;
   icnt.assign(nnode + 1, 0);
-  for (long long k = 0; k < (long long)nelem * nnpe; ++k) icnt[conn[k] + 1]++;
+  const long long nent = (long long)nelem * nnpe;
+  parallel_for(nent, [&](long long lo, long long hi) {
+    for (long long k = lo; k < hi; ++k) __atomic_fetch_add(&icnt[conn[k] + 1], 1, __ATOMIC_RELAXED);
+  });
   for (int i = 0; i < nnode; ++i) icnt[i + 1] += icnt[i];
   std::vector<int>& inc = P.s_inc;
   inc.resize(icnt[nnode]);
   {
     std::vector<int> fill(icnt.begin(), icnt.end() - 1);
-    for (int e = 0; e < nelem; ++e)
-      for (int a = 0; a < nnpe; ++a) inc[fill[conn[(long long)e * nnpe + a]]++] = e;
+    parallel_for(nent, [&](long long lo, long long hi) {
+      for (long long k = lo; k < hi; ++k)
+        inc[__atomic_fetch_add(&fill[conn[k]], 1, __ATOMIC_RELAXED)] = (int)(k / nnpe);
+    });
   }
 
   // ---- node graph (two passes: count, then fill) ---------------------
