@@ -183,8 +183,11 @@ def ke_quad4(xy, C9, order=2):
 
 
 def km_hex8_heat(xyz, k3, c, order=2):
+    """hex8 diffusion K and M (full 8x8); k3: (k11, k22, k33) or a full 3x3
+    conductivity."""
     K, M = np.zeros(64), np.zeros(64)
-    k9 = np.diag(np.asarray(k3, dtype=np.float64)).reshape(-1)
+    k = np.asarray(k3, dtype=np.float64)
+    k9 = (np.diag(k) if k.ndim == 1 else k).reshape(-1).copy()
     st = lib().oracle_km_hex8_heat(_f64(xyz).reshape(-1), _f64(k9), float(c), order, K, M)
     return st, _full_from_upper(K.reshape(8, 8)), _full_from_upper(M.reshape(8, 8))
 
@@ -457,6 +460,8 @@ class RefLeaf:
         _ipc = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
         self.lib.ref_print_lower.argtypes = [C.c_char_p, I, I, _lp, _ipc, _dp]
         self.lib.ref_heat2d_add_to_ke.argtypes = [D, D, D, I, _dp, _dp, D, _dp]
+        self.lib.ref_heat3d_add_to_km.argtypes = [_dp, D, _dp, _dp, _dp, _dp, D, _dp, _dp]
+        self.lib.ref_heat3d_step_terms.argtypes = [_dp, _dp, _dp, D, D, D, _dp, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
         self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
                                           C.c_void_p, C.c_void_p]
@@ -510,6 +515,24 @@ class RefLeaf:
         self.lib.ref_heat2d_add_to_ke(float(k11), float(k22), float(k12), n, np.ascontiguousarray(dx, dtype=float),
                                       np.ascontiguousarray(dy, dtype=float), float(factor), K)
         return K.reshape(n, n)
+
+    def heat3d_add_to_km(self, k9, cap, S, dx, dy, dz, factor, K, M):
+        """HeatTransferElement3Dtransient::addToKe + addToMe at one point;
+        returns the accumulated (K, M) upper triangles (8 x 8)."""
+        K = np.ascontiguousarray(K, dtype=float).reshape(-1).copy()
+        M = np.ascontiguousarray(M, dtype=float).reshape(-1).copy()
+        f = lambda a: np.ascontiguousarray(a, dtype=float)  # noqa: E731
+        self.lib.ref_heat3d_add_to_km(f(np.asarray(k9).reshape(-1)), float(cap), f(S), f(dx), f(dy), f(dz),
+                                      float(factor), K, M)
+        return K.reshape(8, 8), M.reshape(8, 8)
+
+    def heat3d_step_terms(self, K, M, u_s, a1, a2, dt):
+        """formK_s and formF_s_new of the reference's 3D diffusion element:
+        (Mbar 8 x 8, F 8)."""
+        Mb, F = np.zeros(64), np.zeros(8)
+        f = lambda a: np.ascontiguousarray(a, dtype=float).reshape(-1)  # noqa: E731
+        self.lib.ref_heat3d_step_terms(f(K), f(M), f(u_s), float(a1), float(a2), float(dt), Mb, F)
+        return Mb.reshape(8, 8), F
 
     def print_lower(self, path, fmt, row_ptr, col, val):
         """The reference's printMatrixAddressFormat (fmt 1), ...Upper (2) or

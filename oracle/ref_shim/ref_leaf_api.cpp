@@ -11,6 +11,7 @@
 #include "quadQuadPoint.hpp"
 #include "sparse.hpp"
 #include "HeatTransferElement2DTransient.hpp"
+#include "HeatTransferElement3DTransient.hpp"
 
 int verboseFlag = 0;  // a global the reference's element files declare extern
 
@@ -124,6 +125,66 @@ int ref_heat2d_add_to_ke(double k11, double k22, double k12, int ndof, const dou
   e.addToKe(&c, &id, factor);
   for (int i = 0; i < ndof; ++i)
     for (int j = 0; j < ndof; ++j) Ke[i * ndof + j] = K(i, j);
+  return 0;
+}
+
+// HeatTransferElement3Dtransient (the reference's own), one integration point
+// of a hex8: addToKe with the 3x3 conductivity k9 (row-major) and addToMe with
+// capacity cap, accumulated into K and M (8 x 8 row-major, upper triangles).
+int ref_heat3d_add_to_km(const double* k9, double cap, const double* S, const double* dx, const double* dy,
+                         const double* dz, double factor, double* K, double* M) {
+  HeatTransferElement3Dtransient e;
+  Matrix Km(8, 8), Mm(8, 8), c(3, 3);
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) { Km(i, j) = K[i * 8 + j]; Mm(i, j) = M[i * 8 + j]; }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) c(i, j) = k9[i * 3 + j];
+  HeatTransferMaterial mat;
+  mat.saturation = cap;
+  std::vector<double> s(S, S + 8), gx(dx, dx + 8), gy(dy, dy + 8), gz(dz, dz + 8);
+  InterpAndSolDerivatives id;
+  id.numberOfInterp = 8;
+  id.S = s.data();
+  id.p_S_x1 = gx.data();
+  id.p_S_x2 = gy.data();
+  id.p_S_x3 = gz.data();
+  e.material = &mat;
+  e.Ke = &Km;
+  e.Me = &Mm;
+  e.numDof = 8;
+  e.addToKe(&c, &id, factor);
+  e.addToMe(nullptr, &id, factor);
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) { K[i * 8 + j] = Km(i, j); M[i * 8 + j] = Mm(i, j); }
+  return 0;
+}
+
+// The element side of one backward-Euler step (DiffusionModel with a1, a2):
+// formK_s gives Mbar = (a1 K + M)/dt, formF_s_new F = -(a1+a2)/dt K u_s, from
+// the element's K and M (upper triangles, 8 x 8 row-major) and its nodal u_s.
+int ref_heat3d_step_terms(const double* K, const double* M, const double* u_s, double a1, double a2, double dt,
+                          double* Mbar, double* F) {
+  HeatTransferElement3Dtransient e;
+  Matrix Km(8, 8), Mm(8, 8), Kb(8, 8);
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) { Km(i, j) = K[i * 8 + j]; Mm(i, j) = M[i * 8 + j]; }
+  std::vector<double> fe(8, 0.0), us(u_s, u_s + 8);
+  int dofs[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+  e.Ke = &Km;
+  e.Me = &Mm;
+  e.Ke_orig = &Kb;
+  e.Fe = fe.data();
+  e.dofList = dofs;
+  e.numDof = 8;
+  Array<double> ap(2);
+  ap[0] = a1;
+  ap[1] = a2;
+  e.formK_s(ap, dt);
+  e.formF_s_new(ap, us.data(), nullptr, nullptr, dt);
+  for (int i = 0; i < 8; ++i) {
+    F[i] = fe[i];
+    for (int j = 0; j < 8; ++j) Mbar[i * 8 + j] = Kb(i, j);
+  }
   return 0;
 }
 

@@ -11,7 +11,9 @@ the compiled reference leaf library (``make -C oracle``):
   local derivatives (plus the quad8/tri6 surface shapes SurfaceLoad uses)
   from beta/elements/shape.cpp, at a fixed set of points, and the
   conductivity matrix of one distorted quad4 accumulated by the reference's
-  own HeatTransferElement2Dtransient::addToKe over its own Gauss points.
+  own HeatTransferElement2Dtransient::addToKe over its own Gauss points; for
+  one distorted hex8, the 3D element's addToKe (anisotropic k) and addToMe
+  and the step terms formK_s / formF_s_new.
   These are outputs of the reference code itself (oracle/_ref).
 * ``ref_cg.json`` -- the reference's own Jacobi-PCG (sparse.cpp
   SymmetricSparseMatrix::solve, compiled unmodified with largeMatrix.cpp)
@@ -79,7 +81,26 @@ def ref_quadrature():
             g = np.linalg.solve(J, np.array([dxi, deta]))
             K = r.heat2d_add_to_ke(2.0, 0.7, 0.0, g[0], g[1], np.linalg.det(J) * wt, K)
         out["heat2d_ke"]["orders"][str(order)] = K.tolist()
-    out["source"] = ("reference gauss.cpp + shape.cpp + HeatTransferElement2DTransient.cpp compiled "
+    # 3D diffusion element: addToKe (full anisotropic k) + addToMe over the
+    # reference's hex Gauss points, then formK_s / formF_s_new of one step
+    X = (np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], float)
+         * np.array([1.2, 0.9, 1.1]) + np.random.default_rng(2).uniform(-0.08, 0.08, (8, 3)))
+    k9 = np.array([[2.0, 0.3, 0.1], [0.3, 1.5, 0.2], [0.1, 0.2, 0.8]])
+    us = np.random.default_rng(5).normal(size=8)
+    h3 = {"xyz": X.tolist(), "k9": k9.tolist(), "cap": 1.7, "u_s": us.tolist(), "a1": 1.0, "a2": 0.0,
+          "dt": 1e-3, "orders": {}}
+    for order in (2, 3):
+        xi, eta, zeta, w = r.hex_points(order)
+        K, M = np.zeros((8, 8)), np.zeros((8, 8))
+        for a, b, c, wt in zip(xi, eta, zeta, w):
+            S, d0, d1, d2 = r.shape_hex8(a, b, c)
+            J = np.array([d0 @ X, d1 @ X, d2 @ X])
+            g = np.linalg.solve(J, np.array([d0, d1, d2]))
+            K, M = r.heat3d_add_to_km(k9, 1.7, S, g[0], g[1], g[2], np.linalg.det(J) * wt, K, M)
+        Mb, F = r.heat3d_step_terms(K, M, us, 1.0, 0.0, 1e-3)
+        h3["orders"][str(order)] = {"K": K.tolist(), "M": M.tolist(), "Mbar": Mb.tolist(), "F": F.tolist()}
+    out["heat3d"] = h3
+    out["source"] = ("reference gauss.cpp + shape.cpp + HeatTransfer{2D,3D}Transient element files compiled "
                      "unmodified (oracle/_ref)")
     return out
 

@@ -271,3 +271,25 @@ def test_quad4_diffusion_equals_the_reference_addToKe(oracle):
         assert st == 0
         Kref = np.array(Kref)
         assert np.abs(K[iu] - Kref[iu]).max() <= 1e-14 * np.abs(Kref).max()
+
+
+def test_hex8_diffusion_equals_the_reference_element(oracle):
+    """The oracle's hex8 diffusion K (full anisotropic conductivity) and M,
+    and the step's Mbar = (a1 K + M)/dt and F = -(a1+a2)/dt K u_s, against
+    the reference's own HeatTransferElement3Dtransient::addToKe, addToMe,
+    formK_s and formF_s_new (compiled unmodified) on a distorted hex8."""
+    case = _load("ref_quadrature.json")["heat3d"]
+    X, k9 = np.array(case["xyz"]), np.array(case["k9"])
+    iu = np.triu_indices(8)
+    for order, ref in case["orders"].items():
+        st, K, M = oracle.km_hex8_heat(X, k9, case["cap"], order=int(order))
+        assert st == 0
+        Kr, Mr = np.array(ref["K"]), np.array(ref["M"])
+        assert np.abs(K[iu] - Kr[iu]).max() <= 1e-14 * np.abs(Kr).max()
+        assert np.abs(M[iu] - Mr[iu]).max() <= 1e-14 * np.abs(Mr).max()
+        # the step terms, from the upper triangles as the reference keeps them
+        Ku, Mu = np.triu(K), np.triu(M)
+        mbar = (case["a1"] * Ku + Mu) / case["dt"]
+        f = -(case["a1"] + case["a2"]) / case["dt"] * (K @ np.array(case["u_s"]))
+        assert np.abs(mbar - np.array(ref["Mbar"])).max() <= 1e-14 * np.abs(mbar).max()
+        assert np.abs(f - np.array(ref["F"])).max() <= 1e-13 * np.abs(f).max()
