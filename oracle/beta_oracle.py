@@ -462,6 +462,7 @@ class RefLeaf:
         self.lib.ref_heat2d_add_to_ke.argtypes = [D, D, D, I, _dp, _dp, D, _dp]
         self.lib.ref_heat3d_add_to_km.argtypes = [_dp, D, _dp, _dp, _dp, _dp, D, _dp, _dp]
         self.lib.ref_heat3d_step_terms.argtypes = [_dp, _dp, _dp, D, D, D, _dp, _dp]
+        self.lib.ref_elastic_point.argtypes = [I, I, _dp, _dp, _dp, C.c_void_p, C.c_void_p, D, _dp, _dp, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
         self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
                                           C.c_void_p, C.c_void_p]
@@ -533,6 +534,27 @@ class RefLeaf:
         f = lambda a: np.ascontiguousarray(a, dtype=float).reshape(-1)  # noqa: E731
         self.lib.ref_heat3d_step_terms(f(K), f(M), f(u_s), float(a1), float(a2), float(dt), Mb, F)
         return Mb.reshape(8, 8), F
+
+    def elastic_point(self, C_mat, dx, dy, dz, factor, Ke, u=None, Fe=None):
+        """ElasticityElement3D (dz given) or ElasticityElement2D (dz None), the
+        reference's own, at one integration point: calculateBmatrix + addToKe
+        accumulated into Ke (upper triangle) and, for nodal displacements u
+        (interleaved), derivativesOfFields + calculateStrain + addToFe of
+        C * strain into Fe.  Returns (Ke, Fe, strain)."""
+        dim = 2 if dz is None else 3
+        n = len(dx)
+        f = lambda a: np.ascontiguousarray(a, dtype=float).reshape(-1).copy()  # noqa: E731
+        K = f(Ke)
+        F = f(np.zeros(dim * n) if Fe is None else Fe)
+        eps = np.zeros(6)
+        dzv = None if dz is None else f(dz)
+        uv = None if u is None else f(u)
+        rc = self.lib.ref_elastic_point(dim, n, f(C_mat), f(dx), f(dy),
+                                        None if dzv is None else dzv.ctypes.data,
+                                        None if uv is None else uv.ctypes.data, float(factor), K, F, eps)
+        if rc:
+            raise ValueError("ref_elastic_point refused the element size")
+        return K.reshape(dim * n, dim * n), F, eps[:3 if dim == 2 else 6]
 
     def print_lower(self, path, fmt, row_ptr, col, val):
         """The reference's printMatrixAddressFormat (fmt 1), ...Upper (2) or

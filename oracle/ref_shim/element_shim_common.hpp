@@ -1,13 +1,18 @@
-// Shim: the parts of the reference's element hierarchy that the diffusion
-// element files (HeatTransferElement2DTransient.cpp,
-// HeatTransferElement3DTransient.cpp) touch, declared from how those files
-// use them because the reference ships no headers.  Only the routines a test
-// calls do real work (the interpolation record, the dense matrix, the
-// material's capacity); every other base-class service is an inert stub so
-// that the element files compile and link unmodified.
+// Shim: the parts of the reference's element hierarchy that the element
+// files compiled here (HeatTransferElement2DTransient.cpp,
+// HeatTransferElement3DTransient.cpp, ElasticityElement3D.cpp,
+// ElasticityElement2D.cpp) touch, declared from how those files use them
+// because the reference ships no headers.  Only the routines a test calls do
+// real work (the interpolation record, the dense matrix, the material's
+// capacity and stiffness); every other base-class service is an inert stub
+// so that the element files compile and link unmodified.
 #pragma once
+#include <algorithm>
 #include <cstring>
+#include <fstream>
+#include <iomanip>
 #include <iostream>
+#include <string>
 #include <vector>
 
 #include "utility/excepts.hpp"
@@ -18,6 +23,14 @@
 #endif
 
 enum { Min = 0, Max = 3 };  // verbosity levels compared with verboseFlag
+
+#ifndef GEOMETRIC_NONLINEAR
+#define LINEAR 0
+#define GEOMETRIC_NONLINEAR 1
+#endif
+#ifndef EXIT_BETA
+#define EXIT_BETA(msg) do { std::cerr << (msg) << '\n'; std::abort(); } while (0)
+#endif
 
 template <class T>
 class Array {
@@ -48,6 +61,8 @@ struct InterpAndSolDerivatives {
   double *nodalValues_u1 = nullptr, *nodalValues_u2 = nullptr, *nodalValues_u3 = nullptr;
   double *xCoor = nullptr, *yCoor = nullptr, *zCoor = nullptr;
   double p_u1_x1 = 0.0, p_u1_x2 = 0.0, p_u1_x3 = 0.0;
+  double p_u2_x1 = 0.0, p_u2_x2 = 0.0, p_u2_x3 = 0.0;
+  double p_u3_x1 = 0.0, p_u3_x2 = 0.0, p_u3_x3 = 0.0;
   double detJ = 0.0;
 
  private:
@@ -84,6 +99,14 @@ struct IntegrationDataType {
 struct ElementWorkspace {
   double **rotatedFluxes = nullptr, **extrapolatedFluxes = nullptr, **quadPointFluxes = nullptr;
   double** quadPointStresses = nullptr;
+  // elasticity: B rows, per-point strains/stresses and volume sums
+  double** b = nullptr;
+  double **quadPointStrains = nullptr, **rotatedStresses = nullptr, **rotatedStrains = nullptr;
+  double **extrapolatedStresses = nullptr, **extrapolatedStrains = nullptr;
+  double *strainVolume_total = nullptr, *stressVolume_total = nullptr;
+  double *localStressVolume_total = nullptr, *energyVolume_total = nullptr;
+  double *strainVolume_element = nullptr, *stressVolume_element = nullptr;
+  double *energyVolume_element = nullptr, *localStressVolume_element = nullptr;
   double totalVolume = 0.0, temperatureVolume = 0.0, elementVolume = 0.0, temperatureVolume_element = 0.0;
   double *fluxVolume_total = nullptr, *gradientVolume_total = nullptr;
   double *fluxVolume_element = nullptr, *gradientVolume_element = nullptr;
@@ -96,11 +119,20 @@ struct ElementWorkspace {
 class Rotation {
  public:
   void interpolate_rotation_by_angle(InterpAndSolDerivatives*, void*) {}
+  // identity orientation: local and global axes coincide
+  void rotate_Voigt_stress_from_global_to_local(double* g, double* l) const { std::copy(g, g + 6, l); }
+  void rotate_Voigt_engineering_strain_from_global_to_local(double* g, double* l) const { std::copy(g, g + 6, l); }
+};
+
+class BasicISV {
+ public:
+  virtual ~BasicISV() {}
 };
 
 class Material {
  public:
   virtual ~Material() {}
+  virtual void allocateISVs(std::vector<BasicISV*>&, const int&) const {}
 };
 
 // The capacity the 3D element's addToMe reads is the material's saturation
@@ -120,6 +152,7 @@ class ElementGroup;
 
 struct ElementNode {
   int nodeNum = 0;
+  int numDof = 0;
 };
 
 class BasicElement {
@@ -131,6 +164,13 @@ class BasicElement {
   int getMaterialNumber() const { return materialGroup; }
   int* getDofList() { return dofList; }
   int getNumDof() const { return numDof; }
+  bool checkForAllocatedISVs() const { return !isv.empty(); }
+  int getTotalNumberOfIPs() const { return 0; }
+  void checkForNegativeDiagonal() {}
+  int analysisType = LINEAR;
+  bool activeElementFlag = true;
+  int newElementNumber = 0;
+  std::vector<BasicISV*> isv;
   Material* material = nullptr;
   Matrix* Ke = nullptr;
   double* Fe = nullptr;

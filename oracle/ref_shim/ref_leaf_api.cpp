@@ -1,5 +1,7 @@
-// C entry points over the reference's own gauss.cpp, shape.cpp, sparse.cpp
-// and largeMatrix.cpp, compiled unmodified into oracle/_ref/libbeta_ref_leaf.so.
+// C entry points over the reference's own gauss.cpp, shape.cpp, sparse.cpp,
+// largeMatrix.cpp, SparseMatrixUtility.cpp and element files (2D/3D
+// diffusion, 2D/3D elasticity), compiled unmodified into
+// oracle/_ref/libbeta_ref_leaf.so.
 // Test infrastructure: used only to pin the oracle's restatement against the
 // reference's code.
 #include <fstream>
@@ -12,6 +14,7 @@
 #include "sparse.hpp"
 #include "HeatTransferElement2DTransient.hpp"
 #include "HeatTransferElement3DTransient.hpp"
+#include "ElasticityElement2D.hpp"
 
 int verboseFlag = 0;  // a global the reference's element files declare extern
 
@@ -43,6 +46,62 @@ void shapeQuad8(double* S, double xi, double eta);
 void derivQuad8(double* Szeta, double* Seta, double zeta, double eta);
 void shapeTri6(double* S, double xi, double eta);
 void derivTri6(double* Sxi, double* Seta, double xi, double eta);
+
+namespace {
+// One integration point of the reference's own elasticity element E
+// (ElasticityElement3D or ElasticityElement2D): calculateBmatrix + addToKe
+// into Ke (ndof x ndof row-major, upper triangle) and, when u is given,
+// derivativesOfFields + calculateStrain, the material's stress C * strain and
+// addToFe into Fe (ndof); strain (numStrains) is returned when non-null.
+template <class E>
+int elastic_point(int dim, int nnode, const double* C, const double* dx, const double* dy, const double* dz,
+                  const double* u, double factor, double* Ke, double* Fe, double* strain) {
+  E e;
+  const int ndof = dim * nnode, ns = e.numStrains;
+  if (ndof > (dim == 3 ? 96 : 36)) return 1;  // the reference's addToKe work arrays
+  std::vector<double> brows((size_t)6 * ndof, 0.0);
+  double* rows[6];
+  for (int r = 0; r < 6; ++r) rows[r] = brows.data() + (size_t)r * ndof;
+  Matrix K(ndof, ndof), c(ns, ns);
+  for (int i = 0; i < ndof; ++i)
+    for (int j = 0; j < ndof; ++j) K(i, j) = Ke[i * ndof + j];
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j < ns; ++j) c(i, j) = C[i * ns + j];
+  InterpAndSolDerivatives id(nnode, nnode);
+  id.allocate();
+  id.numberOfInterp = nnode;
+  for (int a = 0; a < nnode; ++a) {
+    id.p_S_x1[a] = dx[a];
+    id.p_S_x2[a] = dy[a];
+    id.p_S_x3[a] = dz ? dz[a] : 0.0;
+    if (u) {
+      id.nodalValues_u1[a] = u[a * dim];
+      id.nodalValues_u2[a] = u[a * dim + 1];
+      id.nodalValues_u3[a] = dim == 3 ? u[a * dim + 2] : 0.0;
+    }
+  }
+  e.b = rows;
+  e.Ke = &K;
+  e.numDof = ndof;
+  e.calculateBmatrix(&id, rows);
+  double stress[6] = {0, 0, 0, 0, 0, 0}, eps[6] = {0, 0, 0, 0, 0, 0};
+  e.addToKe(&c, &id, factor, stress);
+  for (int i = 0; i < ndof; ++i)
+    for (int j = 0; j < ndof; ++j) Ke[i * ndof + j] = K(i, j);
+  if (u) {
+    ElasticMaterial mat;
+    mat.numStrains = ns;
+    mat.cmat = c;
+    e.derivativesOfFields(&id);
+    e.calculateStrain(&id, eps);
+    mat.calculateStress(stress, eps, nullptr, nullptr);
+    e.addToFe(ndof, ns, rows, stress, factor, Fe);
+    if (strain)
+      for (int i = 0; i < ns; ++i) strain[i] = eps[i];
+  }
+  return 0;
+}
+}  // namespace
 
 extern "C" {
 int ref_gauss_1d(int k, double* x, double* w) {
@@ -157,6 +216,17 @@ int ref_heat3d_add_to_km(const double* k9, double cap, const double* S, const do
   for (int i = 0; i < 8; ++i)
     for (int j = 0; j < 8; ++j) { K[i * 8 + j] = Km(i, j); M[i * 8 + j] = Mm(i, j); }
   return 0;
+}
+
+// ElasticityElement3D (dim 3, 6 strains) or ElasticityElement2D (dim 2,
+// 3 strains), the reference's own, at one integration point: see
+// elastic_point.  C is the numStrains x numStrains constitutive matrix
+// (row-major); u (interleaved nodal displacements) may be null.
+int ref_elastic_point(int dim, int nnode, const double* C, const double* dx, const double* dy, const double* dz,
+                      const double* u, double factor, double* Ke, double* Fe, double* strain) {
+  if (dim == 3) return elastic_point<ElasticityElement3D>(3, nnode, C, dx, dy, dz, u, factor, Ke, Fe, strain);
+  if (dim == 2) return elastic_point<ElasticityElement2D>(2, nnode, C, dx, dy, nullptr, u, factor, Ke, Fe, strain);
+  return 1;
 }
 
 // The element side of one backward-Euler step (DiffusionModel with a1, a2):

@@ -13,7 +13,10 @@ the compiled reference leaf library (``make -C oracle``):
   conductivity matrix of one distorted quad4 accumulated by the reference's
   own HeatTransferElement2Dtransient::addToKe over its own Gauss points; for
   one distorted hex8, the 3D element's addToKe (anisotropic k) and addToMe
-  and the step terms formK_s / formF_s_new.
+  and the step terms formK_s / formF_s_new; for a distorted hex8 and quad4,
+  the elasticity elements' stiffness (calculateBmatrix + addToKe) and, for
+  the hex8, the internal force (derivativesOfFields + calculateStrain +
+  addToFe) for a general constitutive matrix.
   These are outputs of the reference code itself (oracle/_ref).
 * ``ref_cg.json`` -- the reference's own Jacobi-PCG (sparse.cpp
   SymmetricSparseMatrix::solve, compiled unmodified with largeMatrix.cpp)
@@ -100,8 +103,43 @@ def ref_quadrature():
         Mb, F = r.heat3d_step_terms(K, M, us, 1.0, 0.0, 1e-3)
         h3["orders"][str(order)] = {"K": K.tolist(), "M": M.tolist(), "Mbar": Mb.tolist(), "F": F.tolist()}
     out["heat3d"] = h3
-    out["source"] = ("reference gauss.cpp + shape.cpp + HeatTransfer{2D,3D}Transient element files compiled "
-                     "unmodified (oracle/_ref)")
+    # elasticity elements: ElasticityElement3D's calculateBmatrix + addToKe and
+    # derivativesOfFields + calculateStrain + addToFe (hex8, general SPD 6x6 C),
+    # ElasticityElement2D's (quad4, general SPD 3x3 C), over the reference's
+    # Gauss points
+    rng = np.random.default_rng(7)
+    X = (np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], float)
+         * np.array([1.1, 0.95, 1.05]) + rng.uniform(-0.08, 0.08, (8, 3)))
+    A = rng.normal(size=(6, 6))
+    C6 = A @ A.T + 6 * np.eye(6)
+    u = rng.normal(size=24)
+    e3 = {"xyz": X.tolist(), "C": C6.tolist(), "u": u.tolist(), "orders": {}}
+    for order in (2, 3):
+        xi, eta, zeta, w = r.hex_points(order)
+        K, F = np.zeros((24, 24)), np.zeros(24)
+        for a, b, c, wt in zip(xi, eta, zeta, w):
+            S, d0, d1, d2 = r.shape_hex8(a, b, c)
+            J = np.array([d0 @ X, d1 @ X, d2 @ X])
+            g = np.linalg.solve(J, np.array([d0, d1, d2]))
+            K, F, _ = r.elastic_point(C6, g[0], g[1], g[2], np.linalg.det(J) * wt, K, u=u, Fe=F)
+        e3["orders"][str(order)] = {"K": K.tolist(), "F": F.tolist()}
+    out["elastic3d"] = e3
+    X2 = np.array([[0.0, 0.0], [1.2, 0.1], [1.1, 0.9], [-0.05, 1.0]])
+    A = rng.normal(size=(3, 3))
+    C3 = A @ A.T + 3 * np.eye(3)
+    e2 = {"xy": X2.tolist(), "C": C3.tolist(), "orders": {}}
+    for order in (2, 3):
+        xi, eta, w = r.quad_points(order)
+        K = np.zeros((8, 8))
+        for a, b, wt in zip(xi, eta, w):
+            S, d0, d1 = r.shape_quad4(a, b)
+            J = np.array([d0 @ X2, d1 @ X2])
+            g = np.linalg.solve(J, np.array([d0, d1]))
+            K, _, _ = r.elastic_point(C3, g[0], g[1], None, np.linalg.det(J) * wt, K)
+        e2["orders"][str(order)] = {"K": K.tolist()}
+    out["elastic2d"] = e2
+    out["source"] = ("reference gauss.cpp + shape.cpp + HeatTransfer{2D,3D}Transient and Elasticity{2D,3D} "
+                     "element files compiled unmodified (oracle/_ref)")
     return out
 
 

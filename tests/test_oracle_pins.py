@@ -293,3 +293,58 @@ def test_hex8_diffusion_equals_the_reference_element(oracle):
         f = -(case["a1"] + case["a2"]) / case["dt"] * (K @ np.array(case["u_s"]))
         assert np.abs(mbar - np.array(ref["Mbar"])).max() <= 1e-14 * np.abs(mbar).max()
         assert np.abs(f - np.array(ref["F"])).max() <= 1e-13 * np.abs(f).max()
+
+
+def _ref_elastic_hex8(r, X, C6, u, order):
+    xi, eta, zeta, w = r.hex_points(order)
+    K, F = np.zeros((24, 24)), np.zeros(24)
+    for a, b, c, wt in zip(xi, eta, zeta, w):
+        S, d0, d1, d2 = r.shape_hex8(a, b, c)
+        J = np.array([d0 @ X, d1 @ X, d2 @ X])
+        g = np.linalg.solve(J, np.array([d0, d1, d2]))
+        K, F, _ = r.elastic_point(C6, g[0], g[1], g[2], np.linalg.det(J) * wt, K, u=u, Fe=F)
+    return K, F
+
+
+def test_elasticity_equals_the_reference_elements(oracle):
+    """The oracle's hex8 stiffness and internal force and its quad4 plane
+    stiffness, for general (anisotropic) constitutive matrices, against the
+    reference's own ElasticityElement3D (calculateBmatrix, addToKe,
+    derivativesOfFields, calculateStrain, addToFe) and ElasticityElement2D
+    (calculateBmatrix, addToKe), compiled unmodified, summed over the
+    reference's Gauss points on distorted elements."""
+    g = _load("ref_quadrature.json")
+    case = g["elastic3d"]
+    X, C6, u = np.array(case["xyz"]), np.array(case["C"]), np.array(case["u"])
+    iu = np.triu_indices(24)
+    for order, ref in case["orders"].items():
+        st, K = oracle.ke_hex8(X, C6, order=int(order))
+        assert st == 0
+        Kr, Fr = np.array(ref["K"]), np.array(ref["F"])
+        assert np.abs(K[iu] - Kr[iu]).max() <= 1e-14 * np.abs(Kr).max()
+        F = oracle.fe_hex8(X, C6, u, order=int(order))
+        assert np.abs(F - Fr).max() <= 1e-14 * np.abs(Fr).max()
+    case = g["elastic2d"]
+    X2, C3 = np.array(case["xy"]), np.array(case["C"])
+    iu = np.triu_indices(8)
+    for order, ref in case["orders"].items():
+        st, K = oracle.ke_quad4(X2, C3, order=int(order))
+        assert st == 0
+        Kr = np.array(ref["K"])
+        assert np.abs(K[iu] - Kr[iu]).max() <= 1e-14 * np.abs(Kr).max()
+    if oracle.RefLeaf.available():
+        # live, on further random elements and the oracle's own D matrices
+        r = oracle.RefLeaf()
+        rng = np.random.default_rng(11)
+        base = np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]],
+                        float)
+        for trial in range(3):
+            X = base * rng.uniform(0.5, 2.0, 3) + rng.uniform(-0.1, 0.1, (8, 3))
+            C6 = oracle.cmat_ortho3d([rng.uniform(50, 200), rng.uniform(5, 20), rng.uniform(5, 20),
+                                      0.25, 0.3, 0.28, 4.0, 3.0, 5.0])
+            u = rng.normal(size=24)
+            Kr, Fr = _ref_elastic_hex8(r, X, C6, u, 2)
+            st, K = oracle.ke_hex8(X, C6, order=2)
+            assert np.abs(K[np.triu_indices(24)] - Kr[np.triu_indices(24)]).max() <= 1e-14 * np.abs(Kr).max()
+            F = oracle.fe_hex8(X, C6, u, order=2)
+            assert np.abs(F - Fr).max() <= 1e-14 * np.abs(Fr).max()
