@@ -144,42 +144,75 @@ void oracle_shape_quad4(double xi, double eta, double* S, double* dxi, double* d
 }
 
 // ---------------------------------------------------------------------------
-// Dense inverse by LU with partial pivoting (Matrix::invert,
-// beta/math/matrix.cpp:350-370: factor once, back-substitute the identity
-// columns).  A is row-major n x n, overwritten with its inverse.
+// Dense inverse (Matrix::invert, beta/math/matrix.cpp:350-370, with its
+// ludcmp :272-348 and lubksb :393-431).  The reference factors by Crout's
+// method with implicit partial pivoting, the published algorithm of Press et
+// al., Numerical Recipes in C, 2nd ed., sect. 2.3: each row is scaled by the
+// reciprocal of its largest magnitude for the pivot search only, column j
+// first finishes U(0..j-1, j) and then the candidates L(j.., j), the pivot is
+// the last row of largest scaled magnitude, and the sub-diagonal column is
+// multiplied by the reciprocal pivot (a zero pivot becomes 1e-20).  Each
+// identity column is then solved by forward substitution (starting at its
+// first nonzero) and back substitution.  The sums run in the same order as
+// the reference's so that constitutive matrices come out bit-identical.
+// A is row-major n x n, overwritten with its inverse.
 int oracle_invert(int n, double* A) {
   if (n < 1 || n > 16 || !A) return OR_ERR_ARG;
-  std::vector<double> lu(A, A + n * n), inv(n * n, 0.0);
-  std::vector<int> perm(n);
-  for (int i = 0; i < n; ++i) perm[i] = i;
-  for (int k = 0; k < n; ++k) {
-    int p = k;
-    double best = std::fabs(lu[k * n + k]);
-    for (int i = k + 1; i < n; ++i)
-      if (std::fabs(lu[i * n + k]) > best) { best = std::fabs(lu[i * n + k]); p = i; }
-    if (best == 0.0) return OR_ERR_ZERO_DIAG;
-    if (p != k) {
-      for (int j = 0; j < n; ++j) std::swap(lu[k * n + j], lu[p * n + j]);
-      std::swap(perm[k], perm[p]);
+  std::vector<double> a(A, A + n * n), scale(n), x(n);
+  std::vector<int> piv(n);
+  auto at = [&](int r, int c) -> double& { return a[r * n + c]; };
+  for (int r = 0; r < n; ++r) {
+    double big = 0.0;
+    for (int c = 0; c < n; ++c) big = std::max(big, std::fabs(at(r, c)));
+    if (big == 0.0) return OR_ERR_ZERO_DIAG;
+    scale[r] = 1.0 / big;
+  }
+  for (int j = 0; j < n; ++j) {
+    for (int r = 0; r < j; ++r) {
+      double sum = at(r, j);
+      for (int k = 0; k < r; ++k) sum -= at(r, k) * at(k, j);
+      at(r, j) = sum;
     }
-    for (int i = k + 1; i < n; ++i) {
-      double f = lu[i * n + k] / lu[k * n + k];
-      lu[i * n + k] = f;
-      for (int j = k + 1; j < n; ++j) lu[i * n + j] -= f * lu[k * n + j];
+    double best = 0.0;
+    int p = j;
+    for (int r = j; r < n; ++r) {
+      double sum = at(r, j);
+      for (int k = 0; k < j; ++k) sum -= at(r, k) * at(k, j);
+      at(r, j) = sum;
+      const double score = scale[r] * std::fabs(sum);
+      if (score >= best) { best = score; p = r; }
+    }
+    if (p != j) {
+      for (int c = 0; c < n; ++c) std::swap(at(p, c), at(j, c));
+      scale[p] = scale[j];
+    }
+    piv[j] = p;
+    if (at(j, j) == 0.0) at(j, j) = 1e-20;
+    if (j != n - 1) {
+      const double rcp = 1.0 / at(j, j);
+      for (int r = j + 1; r < n; ++r) at(r, j) *= rcp;
     }
   }
-  for (int c = 0; c < n; ++c) {
-    std::vector<double> y(n);
-    for (int i = 0; i < n; ++i) {
-      double s = (perm[i] == c) ? 1.0 : 0.0;
-      for (int j = 0; j < i; ++j) s -= lu[i * n + j] * y[j];
-      y[i] = s;
+  std::vector<double> inv(n * n);
+  for (int col = 0; col < n; ++col) {
+    std::fill(x.begin(), x.end(), 0.0);
+    x[col] = 1.0;
+    int first = -1;
+    for (int r = 0; r < n; ++r) {
+      double sum = x[piv[r]];
+      x[piv[r]] = x[r];
+      if (first >= 0)
+        for (int k = first; k < r; ++k) sum -= at(r, k) * x[k];
+      else if (sum != 0.0)
+        first = r;
+      x[r] = sum;
     }
-    for (int i = n - 1; i >= 0; --i) {
-      double s = y[i];
-      for (int j = i + 1; j < n; ++j) s -= lu[i * n + j] * inv[j * n + c];
-      inv[i * n + c] = s / lu[i * n + i];
+    for (int r = n - 1; r >= 0; --r) {
+      double sum = x[r];
+      for (int k = r + 1; k < n; ++k) sum -= at(r, k) * x[k];
+      x[r] = sum / at(r, r);
     }
+    for (int r = 0; r < n; ++r) inv[r * n + col] = x[r];
   }
   std::memcpy(A, inv.data(), sizeof(double) * n * n);
   return OR_OK;

@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libbeta_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libbeta_ref_leaf.so")
+REF_MATERIAL_LIB = os.path.join(HERE, "_ref", "libbeta_ref_material.so")
 
 KIND_QUAD4_PSTRESS = 1
 KIND_HEX8_ELASTIC = 2
@@ -440,6 +441,54 @@ def surface_flux_load(surf_conn, xyz, nodal_flux, first_dof, ndof):
 
 
 # -- the reference's own leaf code (oracle/_ref) -----------------------------
+class RefMaterial:
+    """The reference's matrix.cpp, elastic.cpp and pStress.cpp, compiled
+    unmodified: the constitutive matrices as the materials' own read()
+    builds them from input constants, and the dense LU inverse."""
+
+    def __init__(self):
+        if not os.path.exists(REF_MATERIAL_LIB):
+            raise FileNotFoundError(REF_MATERIAL_LIB)
+        self.lib = C.CDLL(REF_MATERIAL_LIB)
+        self.lib.ref_matrix_invert.argtypes = [C.c_int, _dp]
+        self.lib.ref_cmat_ortho3d.argtypes = [_dp, _dp, C.c_void_p]
+        self.lib.ref_cmat_plane_stress.argtypes = [_dp, _dp]
+        self.lib.ref_elastic_stress.argtypes = [_dp, _dp, _dp]
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_MATERIAL_LIB)
+
+    def invert(self, A):
+        """Matrix::invert of a square matrix."""
+        A = np.ascontiguousarray(A, dtype=float)
+        B = A.reshape(-1).copy()
+        self.lib.ref_matrix_invert(A.shape[0], B)
+        return B.reshape(A.shape)
+
+    def cmat_ortho3d(self, m9):
+        """ElasticMaterial read of readModuli (E11, E22, E33, nu12, nu23,
+        nu13, G12, G23, G13): the 6 x 6 stiffness."""
+        Cm = np.zeros(36)
+        if self.lib.ref_cmat_ortho3d(_f64(m9), Cm, None):
+            raise ValueError("ElasticMaterial::read failed")
+        return Cm.reshape(6, 6)
+
+    def cmat_plane_stress(self, m4):
+        """PlaneStress read of (E11, E22, nu12, G12): the 3 x 3 stiffness."""
+        Cm = np.zeros(9)
+        if self.lib.ref_cmat_plane_stress(_f64(np.asarray(m4, dtype=float)[:4]), Cm):
+            raise ValueError("PlaneStress::read failed")
+        return Cm.reshape(3, 3)
+
+    def elastic_stress(self, m9, strain):
+        """ElasticMaterial::calculateStress at zero temperature and moisture."""
+        out = np.zeros(6)
+        if self.lib.ref_elastic_stress(_f64(m9), _f64(strain), out):
+            raise ValueError("ElasticMaterial::read failed")
+        return out
+
+
 class RefLeaf:
     """The reference's gauss.cpp + shape.cpp, compiled unmodified."""
 

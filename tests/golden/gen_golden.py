@@ -26,6 +26,11 @@ the compiled reference leaf library (``make -C oracle``):
   writers (sparse.cpp printMatrixAddressFormat[Upper], printCompressedRowFormat;
   SparseMatrixUtility.cpp writeCSRMatrixIn{ASCII,Binary}) produce for the
   assembled lower triangle of a small RVE.
+* ``ref_materials.json`` -- constitutive matrices built by the reference's
+  own material code (beta/materials/3D/elastic.cpp ElasticMaterial::read of
+  a readModuli block, beta/materials/2D/pStress.cpp PlaneStress::read) and
+  inverses by its own Matrix::invert (beta/math/matrix.cpp), compiled
+  unmodified into oracle/_ref/libbeta_ref_material.so.
 * ``ref_matrix_kat.json`` -- the known answers written in the reference's
   DEBUG_MATRIX_CLASS main (beta/math/matrix.cpp:679-696).
 * ``oracle_small.json`` -- small end-to-end cases from the oracle (element
@@ -229,6 +234,24 @@ def oracle_small():
     return out
 
 
+
+def ref_materials():
+    r = bo.RefMaterial()
+    rng = np.random.default_rng(21)
+    ortho = [W.iso3d_params(np.array([e]), nu)[0].tolist() for e, nu in ((200.0, 0.3), (1e4, 0.25), (3.5, 0.45))]
+    ortho += [[150.0, 12.0, 9.0, 0.25, 0.32, 0.28, 5.0, 3.5, 4.2], [72.0, 72.0, 10.0, 0.3, 0.35, 0.35, 27.7, 4.0, 4.0]]
+    pstress = [W.pstress_params(np.array([e]), nu)[0][:4].tolist() for e, nu in ((70e3, 0.3), (1.0, 0.49))]
+    pstress += [[140.0, 10.0, 0.3, 5.0]]
+    inv = []
+    for n in (3, 6, 9):
+        A = rng.normal(size=(n, n)) + n * np.eye(n)
+        inv.append({"A": A.tolist(), "inverse": r.invert(A).tolist()})
+    return {"source": "reference elastic.cpp + pStress.cpp + matrix.cpp compiled unmodified (oracle/_ref)",
+            "ortho3d": [{"m9": m, "C": r.cmat_ortho3d(m).tolist()} for m in ortho],
+            "plane_stress": [{"m4": m, "C": r.cmat_plane_stress(m).tolist()} for m in pstress],
+            "invert": inv}
+
+
 if __name__ == "__main__":
     with open(os.path.join(OUT, "ref_quadrature.json"), "w") as f:
         json.dump(ref_quadrature(), f)
@@ -236,6 +259,8 @@ if __name__ == "__main__":
         json.dump(ref_cg(), f)
     with open(os.path.join(OUT, "ref_exchange.json"), "w") as f:
         json.dump(ref_exchange(), f, indent=1)
+    with open(os.path.join(OUT, "ref_materials.json"), "w") as f:
+        json.dump(ref_materials(), f, indent=1)
     with open(os.path.join(OUT, "ref_matrix_kat.json"), "w") as f:
         json.dump(matrix_kat(), f, indent=1)
     with open(os.path.join(OUT, "oracle_small.json"), "w") as f:

@@ -348,3 +348,34 @@ def test_elasticity_equals_the_reference_elements(oracle):
             assert np.abs(K[np.triu_indices(24)] - Kr[np.triu_indices(24)]).max() <= 1e-14 * np.abs(Kr).max()
             F = oracle.fe_hex8(X, C6, u, order=2)
             assert np.abs(F - Fr).max() <= 1e-14 * np.abs(Fr).max()
+
+
+def test_constitutive_matrices_equal_the_reference_materials(oracle):
+    """The oracle's 3D orthotropic stiffness (compliance filled from the nine
+    constants, then inverted) and plane-stress stiffness are bit-identical to
+    what the reference's own ElasticMaterial::read (readModuli) and
+    PlaneStress::read build, compiled unmodified with its Matrix::invert, and
+    the oracle's dense inverse (the same Crout factorisation) is
+    bit-identical to Matrix::invert."""
+    g = _load("ref_materials.json")
+    for case in g["ortho3d"]:
+        np.testing.assert_array_equal(oracle.cmat_ortho3d(case["m9"]), np.array(case["C"]))
+    for case in g["plane_stress"]:
+        np.testing.assert_array_equal(oracle.cmat_plane_stress(case["m4"]), np.array(case["C"]))
+    for case in g["invert"]:
+        np.testing.assert_array_equal(oracle.invert(np.array(case["A"])), np.array(case["inverse"]))
+    if oracle.RefMaterial.available():
+        r = oracle.RefMaterial()
+        rng = np.random.default_rng(5)
+        for _ in range(20):
+            e = rng.uniform(1.0, 300.0, 3)
+            m9 = [e[0], e[1], e[2], rng.uniform(0.1, 0.35), rng.uniform(0.1, 0.35), rng.uniform(0.1, 0.35),
+                  *rng.uniform(1.0, 50.0, 3)]
+            C = oracle.cmat_ortho3d(m9)
+            np.testing.assert_array_equal(C, r.cmat_ortho3d(m9))
+            eps = rng.normal(size=6)
+            assert np.abs(C @ eps - r.elastic_stress(m9, eps)).max() <= 1e-14 * np.abs(C @ eps).max()
+            m4 = [e[0], e[1], m9[3], m9[6]]
+            np.testing.assert_array_equal(oracle.cmat_plane_stress(m4), r.cmat_plane_stress(m4))
+            A = rng.normal(size=(7, 7))
+            np.testing.assert_array_equal(oracle.invert(A), r.invert(A))
