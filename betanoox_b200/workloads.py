@@ -140,6 +140,29 @@ def pstress_params(E, nu):
     return np.stack([E, E, nu, E / (2.0 * (1.0 + nu))], axis=1)
 
 
+def renumbered(m, seed, unused_node=False):
+    """A copy of model m with its nodes renumbered by a seeded permutation
+    (connectivity, coordinates and the per-node restraints, prescribed values
+    and loads follow their nodes), optionally with one node appended that no
+    element uses (its dofs restrained at zero).  The system is the same up to
+    the numbering, which changes the sparsity pattern's order."""
+    perm = np.random.default_rng(seed).permutation(m.nnode)      # old node -> new node
+    inv = np.argsort(perm)                                        # new node -> old node
+    def per_node(a, fill):
+        a = np.asarray(a).reshape(m.nnode, m.ndpn)[inv]
+        if unused_node:
+            a = np.vstack([a, np.full((1, m.ndpn), fill, dtype=a.dtype)])
+        return np.ascontiguousarray(a.reshape(-1))
+    xyz = m.xyz[inv]
+    if unused_node:
+        xyz = np.vstack([xyz, xyz.max(axis=0) + 1.0])
+    return dataclasses.replace(
+        m, name=m.name + "_renumbered", xyz=np.ascontiguousarray(xyz),
+        conn=np.ascontiguousarray(perm[m.conn].astype(np.int32)),
+        restrained=per_node(m.restrained, 1), prescribed=per_node(m.prescribed, 0.0),
+        load=per_node(m.load, 0.0), meta=dict(m.meta))
+
+
 # ---- configuration 1: quad4 plane stress plate ------------------------------
 def plate_quad4(n=64, E=70e3, nu=0.3, traction=1.0, order=2):
     """Unit square, n x n quad4, left edge clamped, +x traction on the right edge."""

@@ -19,6 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libbeta_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libbeta_ref_leaf.so")
 REF_MATERIAL_LIB = os.path.join(HERE, "_ref", "libbeta_ref_material.so")
+REF_EQUATIONS_LIB = os.path.join(HERE, "_ref", "libbeta_ref_equations.so")
 
 KIND_QUAD4_PSTRESS = 1
 KIND_HEX8_ELASTIC = 2
@@ -487,6 +488,47 @@ class RefMaterial:
         if self.lib.ref_elastic_stress(_f64(m9), _f64(strain), out):
             raise ValueError("ElasticMaterial::read failed")
         return out
+
+
+class RefEquations:
+    """The reference's Equations (equation.cpp, addeqn.cpp) over its
+    SymmetricSparseMatrix (sparse.cpp) and Matrix (matrix.cpp), compiled
+    unmodified: the global pattern, addMatrix scatter with restraint
+    elimination, loads and CG solve for given element matrices and maps."""
+
+    def __init__(self):
+        if not os.path.exists(REF_EQUATIONS_LIB):
+            raise FileNotFoundError(REF_EQUATIONS_LIB)
+        self.lib = C.CDLL(REF_EQUATIONS_LIB)
+        _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+        _ipc = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+        _u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+        I, D = C.c_int, C.c_double
+        self.lib.ref_equations_assemble.argtypes = [I, I, I, _ipc, _dp, _u8, _dp, _dp, D, I, _lp, _ipc, _dp,
+                                                    C.c_longlong, C.POINTER(C.c_longlong), _dp, _dp, C.c_void_p]
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_EQUATIONS_LIB)
+
+    def assemble(self, n, maps, Ke, restrained, prescribed, load, solve=False, eps=1e-4, maxit=10000):
+        """Returns (rowptr, col, val, pseudo_load, load_vector, x or None)."""
+        maps = np.ascontiguousarray(maps, dtype=np.int32)
+        nelem, nde = maps.shape
+        Ke = np.ascontiguousarray(Ke, dtype=float).reshape(-1)
+        cap = nelem * nde * nde + n
+        rp, col, val = np.zeros(n + 1, np.int64), np.zeros(cap, np.int32), np.zeros(cap)
+        pseudo, lv = np.zeros(n), np.zeros(n)
+        x = np.zeros(n) if solve else None
+        nnz = C.c_longlong(0)
+        rc = self.lib.ref_equations_assemble(n, nelem, nde, maps.reshape(-1), Ke,
+                                             np.ascontiguousarray(restrained, dtype=np.uint8), _f64(prescribed),
+                                             _f64(load), float(eps), int(maxit), rp, col, val, cap, C.byref(nnz),
+                                             pseudo, lv, None if x is None else x.ctypes.data)
+        if rc:
+            raise ValueError("ref_equations_assemble returned %d" % rc)
+        k = nnz.value
+        return rp, col[:k].copy(), val[:k].copy(), pseudo, lv, x
 
 
 class RefLeaf:

@@ -22,7 +22,7 @@
 #define BETA_OUT std::cout
 #endif
 
-enum { Min = 0, Max = 3 };  // verbosity levels compared with verboseFlag
+#include "verbose_level.hpp"  // levels compared with verboseFlag
 
 #ifndef GEOMETRIC_NONLINEAR
 #define LINEAR 0

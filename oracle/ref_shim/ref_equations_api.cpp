@@ -1,0 +1,112 @@
+// C entry point over the reference's own Equations (equation.cpp, with
+// addeqn.cpp), SymmetricSparseMatrix (sparse.cpp, largeMatrix.cpp) and
+// Matrix (matrix.cpp), compiled unmodified into
+// oracle/_ref/libbeta_ref_equations.so.  Test infrastructure: it runs the
+// reference's assembly path -- restraints, setupStorage, the per-element
+// sparsity pattern, allocate, addMatrix with its boundary-condition
+// elimination, point loads, solve -- on element matrices and dof maps the
+// caller supplies, so the oracle's pattern, scatter and right-hand side can
+// be compared with the reference's.
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+#include <strings.h>
+
+#include "equation.hpp"
+#include "sparse.hpp"
+
+// Helpers equation.cpp calls from the reference's utility.cpp (not compiled
+// here): the command reader is never driven by the entry point.
+int getLineAndTokenize(std::istream* in, char* terminateString, char* tokenList[], int& numberOfTokens) {
+  static char line[1024];
+  for (;;) {
+    numberOfTokens = 0;
+    if (!in->getline(line, sizeof line)) return 1;
+    char* save = nullptr;
+    for (char* t = strtok_r(line, " \t\r", &save); t && numberOfTokens < 20; t = strtok_r(nullptr, " \t\r", &save))
+      tokenList[numberOfTokens++] = t;
+    if (numberOfTokens == 0 || std::strncmp(tokenList[0], "//", 2) == 0) continue;
+    return strcasecmp(tokenList[0], terminateString) == 0 ? 1 : 0;
+  }
+}
+void displayTime(const char*, std::ostream&) {}
+std::ifstream* openFileForInput(char* filename) { return new std::ifstream(filename); }
+extern "C" int omp_get_max_threads() { return 1; }  // the constructor records it as the solver thread count
+
+namespace {
+struct QuietStreams {  // the solve reports to cout/cerr; keep that out of the caller's output
+  std::stringstream sink;
+  std::streambuf *out, *err;
+  QuietStreams() : out(std::cout.rdbuf(sink.rdbuf())), err(std::cerr.rdbuf(sink.rdbuf())) {}
+  ~QuietStreams() {
+    std::cout.rdbuf(out);
+    std::cerr.rdbuf(err);
+  }
+};
+}  // namespace
+
+extern "C" {
+// n unknowns; nelem elements of nde dofs each, maps (nelem x nde) their
+// equation numbers and Ke (nelem x nde x nde, row-major, upper triangle read)
+// their matrices; restrained (n, 0/1) with prescribed values; point loads.
+// Runs, in the reference's order: setRestraint for each restrained unknown,
+// setupStorage(Sparse, n), setSolution of the prescribed values,
+// specifyNonZeroLocation per element, allocate, zeroMatrix, addMatrix per
+// element, addLoadToEqn per nonzero load, then (when x is non-null) solve
+// with the reference's CG (tolerance eps, at most maxit iterations).
+// Outputs: the lower triangle as 0-based CSR (rp n+1, col/val up to cap
+// entries, *nnz the count), the pseudo-load vector, the load vector, and x.
+// Returns 0; 1 when cap is too small; 2 when a load sits on a restrained
+// unknown (the reference stops there with "Cannot add load to a restrained
+// degree of freedom").
+int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const double* Ke,
+                           const unsigned char* restrained, const double* prescribed, const double* load,
+                           double eps, int maxit, long long* rp, int* col, double* val, long long cap,
+                           long long* nnz, double* pseudo, double* loadvec, double* x) {
+  for (int i = 0; i < n; ++i)
+    if (restrained[i] && load[i] != 0.0) return 2;
+  QuietStreams quiet;
+  Equations eq;
+  eq.setMaxIterations(maxit);
+  eq.setSOLUTION_EPSILON(eps);
+  for (int i = 0; i < n; ++i)
+    if (restrained[i]) eq.setRestraint(i, true);
+  eq.setupStorage(Sparse, n);
+  for (int i = 0; i < n; ++i)
+    if (restrained[i]) eq.setSolution(prescribed[i], i);
+  for (int e = 0; e < nelem; ++e) eq.specifyNonZeroLocation(maps + (size_t)e * nde, nde);
+  eq.allocate();
+  eq.zeroMatrix();
+  Matrix K(nde, nde);
+  for (int e = 0; e < nelem; ++e) {
+    const double* ke = Ke + (size_t)e * nde * nde;
+    for (int i = 0; i < nde; ++i)
+      for (int j = 0; j < nde; ++j) K(i, j) = ke[i * nde + j];
+    eq.addMatrix(K, maps + (size_t)e * nde, nde, 0, 0);
+  }
+  for (int i = 0; i < n; ++i)
+    if (load[i] != 0.0) eq.addLoadToEqn(load[i], i, false);
+  SymmetricSparseMatrix& A = *static_cast<SymmetricSparseMatrix*>(eq.a);
+  long long k = 0;
+  rp[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    const int m = A.row[i].getNum();
+    if (k + m > cap) return 1;
+    for (int t = 0; t < m; ++t, ++k) {
+      col[k] = A.row[i][t];
+      val[k] = A.mat[i][t];
+    }
+    rp[i + 1] = k;
+  }
+  *nnz = k;
+  for (int i = 0; i < n; ++i) {
+    pseudo[i] = eq.pseudoLoadVector[i];
+    loadvec[i] = eq.loadVector[i];
+  }
+  if (x) {
+    const double* u = eq.solve(0);
+    for (int i = 0; i < n; ++i) x[i] = u[i];
+  }
+  return 0;
+}
+}

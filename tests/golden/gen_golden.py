@@ -31,6 +31,14 @@ the compiled reference leaf library (``make -C oracle``):
   a readModuli block, beta/materials/2D/pStress.cpp PlaneStress::read) and
   inverses by its own Matrix::invert (beta/math/matrix.cpp), compiled
   unmodified into oracle/_ref/libbeta_ref_material.so.
+* ``ref_equations.json`` -- the reference's own global assembly
+  (beta/math/equation/equation.cpp Equations: setRestraint, setupStorage,
+  setSolution, specifyNonZeroLocation, allocate, zeroMatrix, addMatrix,
+  addLoadToEqn, solve; with addeqn.cpp, sparse.cpp, largeMatrix.cpp and
+  matrix.cpp, compiled unmodified into oracle/_ref/libbeta_ref_equations.so)
+  on small meshes -- renumbered, with nonzero prescribed values, an unused
+  node -- given the oracle's element matrices: the lower triangle (CSR), the
+  pseudo-load vector and the solution.
 * ``ref_matrix_kat.json`` -- the known answers written in the reference's
   DEBUG_MATRIX_CLASS main (beta/math/matrix.cpp:679-696).
 * ``oracle_small.json`` -- small end-to-end cases from the oracle (element
@@ -252,6 +260,37 @@ def ref_materials():
             "invert": inv}
 
 
+
+def element_maps(m):
+    nd = m.nnpe * m.ndpn
+    return (m.first_dof[m.conn][:, :, None] + np.arange(m.ndpn)[None, None, :]).reshape(m.nelem, nd)
+
+
+EQUATION_CASES = {
+    "plate4_renumbered": lambda: W.renumbered(W.plate_quad4(4), 1),
+    "plate4_unused_node": lambda: W.renumbered(W.plate_quad4(4), 2, unused_node=True),
+    "rve2_prescribed": lambda: W.rve_hex8(2, seed=1),
+    "heat_plate_4x3": lambda: W.heat_plate(4, 3, heat=2.0),
+}
+
+
+def ref_equations():
+    r = bo.RefEquations()
+    out = {"source": "reference equation.cpp + addeqn.cpp + sparse.cpp + largeMatrix.cpp + matrix.cpp compiled "
+                     "unmodified (oracle/_ref)", "eps": 1e-10, "cases": {}}
+    for name, make in EQUATION_CASES.items():
+        m = make()
+        nd = m.nnpe * m.ndpn
+        st, Ke = bo.element_matrices_threaded(m, m.params, m.order, 0, m.nelem)
+        solve = not name.endswith("unused_node")  # the unused node's row is a zero diagonal
+        rp, col, val, pseudo, lv, x = r.assemble(m.ndof, element_maps(m), Ke.reshape(m.nelem, nd, nd), m.restrained,
+                                                 m.prescribed, m.load, solve=solve, eps=1e-10)
+        out["cases"][name] = {"rowptr": rp.tolist(), "col": col.tolist(), "val": val.tolist(),
+                              "pseudo": pseudo.tolist(), "load": lv.tolist(),
+                              "x": None if x is None else x.tolist()}
+    return out
+
+
 if __name__ == "__main__":
     with open(os.path.join(OUT, "ref_quadrature.json"), "w") as f:
         json.dump(ref_quadrature(), f)
@@ -261,6 +300,8 @@ if __name__ == "__main__":
         json.dump(ref_exchange(), f, indent=1)
     with open(os.path.join(OUT, "ref_materials.json"), "w") as f:
         json.dump(ref_materials(), f, indent=1)
+    with open(os.path.join(OUT, "ref_equations.json"), "w") as f:
+        json.dump(ref_equations(), f)
     with open(os.path.join(OUT, "ref_matrix_kat.json"), "w") as f:
         json.dump(matrix_kat(), f, indent=1)
     with open(os.path.join(OUT, "oracle_small.json"), "w") as f:

@@ -4,7 +4,12 @@
   shape.cpp (golden vectors produced by those files, tests/golden).
 * Dense LU inverse vs the known answer in the reference's matrix.cpp debug main.
 * Analytic element properties the reference's elements must satisfy.
+* Element matrices, constitutive matrices and the global assembly and solve
+  against the reference's own element, material and Equations code compiled
+  unmodified (oracle/_ref), through committed golden vectors and, where that
+  build exists, live.
 """
+import importlib.util
 import json
 import os
 
@@ -379,3 +384,51 @@ def test_constitutive_matrices_equal_the_reference_materials(oracle):
             np.testing.assert_array_equal(oracle.cmat_plane_stress(m4), r.cmat_plane_stress(m4))
             A = rng.normal(size=(7, 7))
             np.testing.assert_array_equal(oracle.invert(A), r.invert(A))
+
+
+def _oracle_system(oracle, m, solve, eps):
+    s = oracle.System(m)
+    assert s.set_bc(m.restrained, m.prescribed, m.load) == 0
+    s.build_pattern()
+    assert s.assemble(m.params, m.order) == 0
+    rp, col, val = s.export_lower()
+    x = s.solve(eps=eps, maxit=10000)[1] if solve else None
+    return rp, col, val, s.pseudo_load(), x
+
+
+def test_global_assembly_equals_the_reference_equations(oracle):
+    """The oracle's global system -- lower-triangle pattern, assembled values
+    with the restraint elimination, pseudo-load vector and CG solution -- is
+    bit-identical to the reference's own Equations (equation.cpp:
+    specifyNonZeroLocation, allocate, addMatrix, addLoadToEqn, solve over
+    sparse.cpp's SymmetricSparseMatrix, compiled unmodified) given the same
+    element matrices: on renumbered meshes, with nonzero prescribed
+    displacements, an unused node, elasticity and diffusion."""
+    spec = importlib.util.spec_from_file_location("gen_golden", os.path.join(GOLD, "gen_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    EQUATION_CASES, element_maps = gen.EQUATION_CASES, gen.element_maps
+    g = _load("ref_equations.json")
+    for name, make in EQUATION_CASES.items():
+        ref = g["cases"][name]
+        m = make()
+        rp, col, val, pseudo, x = _oracle_system(oracle, m, ref["x"] is not None, g["eps"])
+        np.testing.assert_array_equal(rp, np.array(ref["rowptr"]))
+        np.testing.assert_array_equal(col, np.array(ref["col"]))
+        np.testing.assert_array_equal(val, np.array(ref["val"]))
+        np.testing.assert_array_equal(pseudo, np.array(ref["pseudo"]))
+        if x is not None:
+            np.testing.assert_allclose(x, np.array(ref["x"]), rtol=0, atol=1e-14 * np.abs(x).max())
+    if oracle.RefEquations.available():
+        r = oracle.RefEquations()
+        for m, solve in ((W.renumbered(W.cube_hex8(3, seed=4), 9, unused_node=True), False),
+                         (W.renumbered(W.rve_hex8(3, seed=2), 5), True)):
+            nd = m.nnpe * m.ndpn
+            st, Ke = oracle.element_matrices_threaded(m, m.params, m.order, 0, m.nelem)
+            got = r.assemble(m.ndof, element_maps(m), Ke.reshape(m.nelem, nd, nd), m.restrained, m.prescribed,
+                             m.load, solve=solve, eps=1e-10)
+            rp, col, val, pseudo, x = _oracle_system(oracle, m, solve, 1e-10)
+            for a, b in ((rp, got[0]), (col, got[1]), (val, got[2]), (pseudo, got[3])):
+                np.testing.assert_array_equal(a, b)
+            if solve:
+                np.testing.assert_allclose(x, got[5], rtol=0, atol=1e-14 * np.abs(x).max())
