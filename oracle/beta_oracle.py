@@ -504,15 +504,19 @@ class RefEquations:
         _ipc = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
         _u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
         I, D = C.c_int, C.c_double
-        self.lib.ref_equations_assemble.argtypes = [I, I, I, _ipc, _dp, _u8, _dp, _dp, D, I, _lp, _ipc, _dp,
-                                                    C.c_longlong, C.POINTER(C.c_longlong), _dp, _dp, C.c_void_p]
+        self.lib.ref_equations_assemble.argtypes = [I, I, I, _ipc, _dp, C.c_void_p, _u8, _dp, _dp, D, I, C.c_void_p,
+                                                    _lp, _ipc, _dp, C.c_longlong, C.POINTER(C.c_longlong), _dp, _dp,
+                                                    C.c_void_p]
 
     @staticmethod
     def available():
         return os.path.exists(REF_EQUATIONS_LIB)
 
-    def assemble(self, n, maps, Ke, restrained, prescribed, load, solve=False, eps=1e-4, maxit=10000):
-        """Returns (rowptr, col, val, pseudo_load, load_vector, x or None)."""
+    def assemble(self, n, maps, Ke, restrained, prescribed, load, solve=False, eps=1e-4, maxit=10000, Fe=None,
+                 x0=None):
+        """Element matrices Ke (and force vectors Fe) through the reference's
+        Equations; solve from the initial guess x0 when asked.  Returns
+        (rowptr, col, val, pseudo_load, load_vector, x or None)."""
         maps = np.ascontiguousarray(maps, dtype=np.int32)
         nelem, nde = maps.shape
         Ke = np.ascontiguousarray(Ke, dtype=float).reshape(-1)
@@ -521,10 +525,14 @@ class RefEquations:
         pseudo, lv = np.zeros(n), np.zeros(n)
         x = np.zeros(n) if solve else None
         nnz = C.c_longlong(0)
+        fe = None if Fe is None else _f64(Fe).reshape(-1).copy()
+        g = None if x0 is None else _f64(x0).copy()
         rc = self.lib.ref_equations_assemble(n, nelem, nde, maps.reshape(-1), Ke,
+                                             None if fe is None else fe.ctypes.data,
                                              np.ascontiguousarray(restrained, dtype=np.uint8), _f64(prescribed),
-                                             _f64(load), float(eps), int(maxit), rp, col, val, cap, C.byref(nnz),
-                                             pseudo, lv, None if x is None else x.ctypes.data)
+                                             _f64(load), float(eps), int(maxit), None if g is None else g.ctypes.data,
+                                             rp, col, val, cap, C.byref(nnz), pseudo, lv,
+                                             None if x is None else x.ctypes.data)
         if rc:
             raise ValueError("ref_equations_assemble returned %d" % rc)
         k = nnz.value

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <sstream>
 #include <strings.h>
+#include <vector>
 
 #include "equation.hpp"
 #include "sparse.hpp"
@@ -48,20 +49,24 @@ struct QuietStreams {  // the solve reports to cout/cerr; keep that out of the c
 extern "C" {
 // n unknowns; nelem elements of nde dofs each, maps (nelem x nde) their
 // equation numbers and Ke (nelem x nde x nde, row-major, upper triangle read)
-// their matrices; restrained (n, 0/1) with prescribed values; point loads.
+// their matrices, Fe (nelem x nde, may be null) their force vectors;
+// restrained (n, 0/1) with prescribed values; point loads.
 // Runs, in the reference's order: setRestraint for each restrained unknown,
 // setupStorage(Sparse, n), setSolution of the prescribed values,
 // specifyNonZeroLocation per element, allocate, zeroMatrix, addMatrix per
-// element, addLoadToEqn per nonzero load, then (when x is non-null) solve
-// with the reference's CG (tolerance eps, at most maxit iterations).
+// element (with its force vector), addLoadToEqn per nonzero load, then (when
+// x is non-null) solve with the reference's CG (tolerance eps, at most maxit
+// iterations) from the initial guess x0 (null: the reference's default, its
+// last solution, zero here) -- the sequence DiffusionModel's transient step
+// runs with Mbar_e and Fbar_e and x0 = u_s.
 // Outputs: the lower triangle as 0-based CSR (rp n+1, col/val up to cap
 // entries, *nnz the count), the pseudo-load vector, the load vector, and x.
 // Returns 0; 1 when cap is too small; 2 when a load sits on a restrained
 // unknown (the reference stops there with "Cannot add load to a restrained
 // degree of freedom").
 int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const double* Ke,
-                           const unsigned char* restrained, const double* prescribed, const double* load,
-                           double eps, int maxit, long long* rp, int* col, double* val, long long cap,
+                           const double* Fe, const unsigned char* restrained, const double* prescribed,
+                           const double* load, double eps, int maxit, const double* x0, long long* rp, int* col, double* val, long long cap,
                            long long* nnz, double* pseudo, double* loadvec, double* x) {
   for (int i = 0; i < n; ++i)
     if (restrained[i] && load[i] != 0.0) return 2;
@@ -82,7 +87,7 @@ int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const dou
     const double* ke = Ke + (size_t)e * nde * nde;
     for (int i = 0; i < nde; ++i)
       for (int j = 0; j < nde; ++j) K(i, j) = ke[i * nde + j];
-    eq.addMatrix(K, maps + (size_t)e * nde, nde, 0, 0);
+    eq.addMatrix(K, maps + (size_t)e * nde, nde, Fe ? Fe + (size_t)e * nde : 0, 0);
   }
   for (int i = 0; i < n; ++i)
     if (load[i] != 0.0) eq.addLoadToEqn(load[i], i, false);
@@ -104,7 +109,9 @@ int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const dou
     loadvec[i] = eq.loadVector[i];
   }
   if (x) {
-    const double* u = eq.solve(0);
+    std::vector<double> guess;
+    if (x0) guess.assign(x0, x0 + n);
+    const double* u = eq.solve(x0 ? guess.data() : 0);
     for (int i = 0; i < n; ++i) x[i] = u[i];
   }
   return 0;

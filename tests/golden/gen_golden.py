@@ -39,12 +39,19 @@ the compiled reference leaf library (``make -C oracle``):
   on small meshes -- renumbered, with nonzero prescribed values, an unused
   node -- given the oracle's element matrices: the lower triangle (CSR), the
   pseudo-load vector and the solution.
+* ``ref_heat_steps.json`` -- backward-Euler steps of a small hex8 slab
+  (with and without a heat input, alpha 1 and 0.5) composed from the
+  reference's own code in DiffusionModel's order (DiffusionModel.cpp:743-818,
+  322-347): per element its formK_s / formF_s_new
+  (HeatTransferElement3DTransient.cpp) on the oracle's element K and M, the
+  Equations addMatrix of Mbar_e with Fbar_e, and solve from u_s.
 * ``ref_matrix_kat.json`` -- the known answers written in the reference's
   DEBUG_MATRIX_CLASS main (beta/math/matrix.cpp:679-696).
 * ``oracle_small.json`` -- small end-to-end cases from the oracle (element
   matrices, assembled lower-triangle systems, PCG solutions) used as
   regression fixtures by the GPU parity tests.
 """
+import dataclasses
 import json
 import os
 import sys
@@ -291,6 +298,49 @@ def ref_equations():
     return out
 
 
+
+def heat_step_case(with_load):
+    m = W.heat_slab(6, 5, 4, order=3)
+    if with_load:
+        rng = np.random.default_rng(17)
+        load = np.where(m.restrained.astype(bool), 0.0, rng.uniform(0.0, 0.5, m.ndof))
+        m = dataclasses.replace(m, load=load)
+    return m
+
+
+def ref_heat_step(leaf, req, m, u_s, dt, alpha, eps):
+    """One step of DiffusionModel's alpha family from the reference's own
+    element step terms, assembly and solve (oracle element K and M)."""
+    a1, a2 = alpha * dt, (1 - alpha) * dt
+    maps = element_maps(m)
+    nd = maps.shape[1]
+    Mb, F = np.zeros((m.nelem, nd, nd)), np.zeros((m.nelem, nd))
+    for e in range(m.nelem):
+        st, K, M = bo.km_hex8_heat(m.xyz[m.conn[e]], m.params[e, :3], m.params[e, 3], order=m.order)
+        Mb[e], F[e] = leaf.heat3d_step_terms(np.triu(K), np.triu(M), u_s[maps[e]], a1, a2, dt)
+    x = req.assemble(m.ndof, maps, Mb, m.restrained, m.prescribed, m.load, solve=True, eps=eps, maxit=100000,
+                     Fe=F, x0=u_s)[5]
+    return u_s + x
+
+
+def ref_heat_steps():
+    leaf, req = bo.RefLeaf(), bo.RefEquations()
+    out = {"source": "reference HeatTransferElement3DTransient.cpp formK_s/formF_s_new + equation.cpp "
+                     "addMatrix/solve compiled unmodified (oracle/_ref), in DiffusionModel's order",
+           "dt": 1e-3, "eps": 1e-14, "steps": 3, "cases": {}}
+    for with_load in (False, True):
+        for alpha in (1.0, 0.5):
+            m = heat_step_case(with_load)
+            u = m.meta["u0"].copy()
+            traj = []
+            for _ in range(3):
+                u = ref_heat_step(leaf, req, m, u, 1e-3, alpha, 1e-14)
+                traj.append(u.tolist())
+            out["cases"]["%s_alpha%g" % ("load" if with_load else "free", alpha)] = {
+                "with_load": with_load, "alpha": alpha, "u": traj}
+    return out
+
+
 if __name__ == "__main__":
     with open(os.path.join(OUT, "ref_quadrature.json"), "w") as f:
         json.dump(ref_quadrature(), f)
@@ -302,6 +352,8 @@ if __name__ == "__main__":
         json.dump(ref_materials(), f, indent=1)
     with open(os.path.join(OUT, "ref_equations.json"), "w") as f:
         json.dump(ref_equations(), f)
+    with open(os.path.join(OUT, "ref_heat_steps.json"), "w") as f:
+        json.dump(ref_heat_steps(), f)
     with open(os.path.join(OUT, "ref_matrix_kat.json"), "w") as f:
         json.dump(matrix_kat(), f, indent=1)
     with open(os.path.join(OUT, "oracle_small.json"), "w") as f:

@@ -26,6 +26,15 @@ def _load(name):
         return json.load(f)
 
 
+def _gen_golden():
+    """The fixture generator, for the cases it defines (it imports the oracle
+    and the workloads, nothing from the reference at import time)."""
+    spec = importlib.util.spec_from_file_location("gen_golden", os.path.join(GOLD, "gen_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    return gen
+
+
 def test_gauss_matches_reference_golden(oracle):
     g = _load("ref_quadrature.json")
     for k, d in g["gauss"].items():
@@ -404,9 +413,7 @@ def test_global_assembly_equals_the_reference_equations(oracle):
     sparse.cpp's SymmetricSparseMatrix, compiled unmodified) given the same
     element matrices: on renumbered meshes, with nonzero prescribed
     displacements, an unused node, elasticity and diffusion."""
-    spec = importlib.util.spec_from_file_location("gen_golden", os.path.join(GOLD, "gen_golden.py"))
-    gen = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(gen)
+    gen = _gen_golden()
     EQUATION_CASES, element_maps = gen.EQUATION_CASES, gen.element_maps
     g = _load("ref_equations.json")
     for name, make in EQUATION_CASES.items():
@@ -432,3 +439,37 @@ def test_global_assembly_equals_the_reference_equations(oracle):
                 np.testing.assert_array_equal(a, b)
             if solve:
                 np.testing.assert_allclose(x, got[5], rtol=0, atol=1e-14 * np.abs(x).max())
+
+
+def test_transient_steps_equal_the_reference_step(oracle):
+    """Three backward-Euler steps of a hex8 slab (alpha 1 and 0.5, with and
+    without a heat input): the oracle's heat_step is bit-identical to the
+    step composed from the reference's own code in DiffusionModel's order
+    (DiffusionModel.cpp:743-818, 322-347) -- formK_s / formF_s_new of
+    HeatTransferElement3Dtransient per element, Equations::addMatrix of
+    Mbar_e with Fbar_e, Equations::solve from u_s, u_s + delta."""
+    gen = _gen_golden()
+    g = _load("ref_heat_steps.json")
+    for name, case in g["cases"].items():
+        m = gen.heat_step_case(case["with_load"])
+        s = oracle.System(m)
+        s.set_bc(m.restrained, m.prescribed, m.load)
+        s.build_pattern()
+        u = m.meta["u0"].copy()
+        for k in range(g["steps"]):
+            s.set_bc(m.restrained, m.prescribed, m.load)
+            rc, u, st = s.heat_step(m.params, m.order, g["dt"], u, alpha=case["alpha"], eps=g["eps"], maxit=100000)
+            assert rc == 0
+            np.testing.assert_array_equal(u, np.array(case["u"][k]), err_msg=f"{name} step {k}")
+    if oracle.RefLeaf.available() and oracle.RefEquations.available():
+        leaf, req = oracle.RefLeaf(), oracle.RefEquations()
+        m = gen.heat_step_case(True)
+        s = oracle.System(m)
+        s.set_bc(m.restrained, m.prescribed, m.load)
+        s.build_pattern()
+        u_o = u_r = m.meta["u0"] + 0.1
+        for _ in range(2):
+            s.set_bc(m.restrained, m.prescribed, m.load)
+            rc, u_o, st = s.heat_step(m.params, m.order, 5e-4, u_o, alpha=0.75, eps=1e-14, maxit=100000)
+            u_r = gen.ref_heat_step(leaf, req, m, u_r, 5e-4, 0.75, 1e-14)
+            np.testing.assert_array_equal(u_o, u_r)
