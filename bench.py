@@ -21,9 +21,13 @@ steps (each assembles C/dt + K in FP32 and solves it).
 diffusion, log-uniform 1e3-5e5 dofs) through the continuous-batching server at
 80% of its measured capacity; reports throughput and p50/p99 latency.
 
---impl reference: the reference's CPU algorithm (the oracle restatement,
-all host cores) on a bounded sample of the same workload, extrapolated to
-the full solve (see cpu_baseline.sample in the output).
+--impl reference: the reference's CPU path on a bounded sample of the same
+workload, extrapolated to the full solve (see cpu_baseline.sample in the
+output).  For the cube this is the reference's own code compiled from its
+sources (oracle/_ref: element B/addToKe, Equations pattern and addMatrix,
+SymmetricSparseMatrix::solve), serial as its default path is, with the
+oracle's all-core port beside it; elsewhere, or without oracle/_ref, the
+oracle's port on all host cores.
 """
 from __future__ import annotations
 
@@ -424,6 +428,62 @@ def cpu_baseline(m, args, st_64_iters=None, steps=1):
             "seconds_full_solve_est": t_total}
 
 
+def reference_code_baseline(m, args, iters_full):
+    """The reference's own code (oracle/_ref, compiled from its sources), run
+    serially as its default SerialAssembler + SymmetricSparseMatrix::solve
+    path runs, on a bounded sample of the workload, extrapolated:
+      * element matrices: ElasticityElement3D calculateBmatrix + addToKe with
+        the reference's Gauss rule and shape functions on a slice of the mesh;
+      * structure and scatter: Equations specifyNonZeroLocation / allocate and
+        addMatrix on a smaller cube of the same generator, per element;
+      * solve: SymmetricSparseMatrix::solve (its Jacobi-PCG and stop rule) on
+        that cube, per iteration, scaled by stored lower-triangle entries, times
+        the full solve's iteration count.
+    Returns None when oracle/_ref is absent (the reference tree was not
+    present where the repository was built)."""
+    from oracle import beta_oracle as bo
+    from betanoox_b200 import workloads as W
+    if not (bo.RefLeaf.available() and bo.RefEquations.available()):
+        return None
+    leaf, req = bo.RefLeaf(), bo.RefEquations()
+    ne_s = min(m.nelem, args.cpu_elems)
+    C_s = np.stack([bo.cmat_ortho3d(p) for p in m.params[:ne_s]])
+    xe = np.ascontiguousarray(m.xyz[m.conn[:ne_s]])
+    t0 = time.perf_counter()
+    leaf.elastic_hex8_ke(xe, C_s, m.order)
+    t_el = (time.perf_counter() - t0) / ne_s
+    ms = W.cube_hex8(args.cpu_ref_n)
+    Ke = leaf.elastic_hex8_ke(ms.xyz[ms.conn], np.stack([bo.cmat_ortho3d(p) for p in ms.params]), ms.order)
+    nd = ms.nnpe * ms.ndpn
+    maps = (ms.first_dof[ms.conn][:, :, None] + np.arange(ms.ndpn)[None, None, :]).reshape(ms.nelem, nd)
+    # the oracle's serial PCG is the reference's step for step: its count is the
+    # reference's, and it proves convergence first (the reference exits otherwise)
+    s = bo.System(ms)
+    s.set_bc(ms.restrained, ms.prescribed, ms.load)
+    s.build_pattern()
+    s.assemble(ms.params, ms.order)
+    rc, _, sst = s.solve(eps=args.cpu_ref_eps, maxit=100000)
+    if rc != 0:
+        return None
+    secs = []
+    rp, _, _, _, _, _ = req.assemble(ms.ndof, maps, Ke, ms.restrained, ms.prescribed, ms.load, solve=True,
+                                     eps=args.cpu_ref_eps, maxit=100000, timings=secs)
+    t_struct, t_scatter, t_solve = secs
+    t_it = t_solve / max(1, sst.iterations)
+    nnz_s, nnz_full = int(rp[-1]), _lower_nnz(m)
+    t_it_full = t_it * nnz_full / nnz_s
+    per_elem = t_el + (t_struct + t_scatter) / ms.nelem
+    t_total = per_elem * m.nelem + iters_full * t_it_full
+    return {"value": m.ndof / t_total, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": (f"extrapolated, the reference's own code compiled from its sources (oracle/_ref), serial: "
+                       f"element matrices of {ne_s} of {m.nelem} elements ({t_el * 1e6:.2f} us/elem); "
+                       f"Equations pattern + addMatrix on the {args.cpu_ref_n}^3 cube "
+                       f"({(t_struct + t_scatter) / ms.nelem * 1e6:.2f} us/elem); SymmetricSparseMatrix::solve "
+                       f"there, {sst.iterations} iterations at eps {args.cpu_ref_eps:g} ({t_it * 1e3:.2f} ms/iter, "
+                       f"scaled by lower-triangle entries {nnz_full}/{nnz_s}) x {iters_full} iterations"),
+            "seconds_full_solve_est": t_total}
+
+
 def _lower_nnz(m):
     from betanoox_b200 import _abi
     lib = _abi.load()
@@ -437,6 +497,9 @@ def _lower_nnz(m):
 
 
 def run_reference(args):
+    """The reference's own code when oracle/_ref was built (serial, as its
+    default path runs), else the oracle's all-core port; the port's figure is
+    reported beside the reference's either way."""
     ws, rank, local = _dist()
     if rank != 0:
         return None
@@ -444,11 +507,21 @@ def run_reference(args):
     iters = args.cpu_assumed_iters
     vals = []
     cb = None
-    for _ in range(args.warmup and 1):
-        cpu_baseline(m, args, None)
+    port = cpu_baseline(m, args, None)
+    if args.warmup:
+        reference_code_baseline(m, args, iters)
     for _ in range(args.steps):
-        cb = cpu_baseline(m, args, None)
+        cb = reference_code_baseline(m, args, iters)
+        if cb is None:
+            break
         vals.append(cb["value"])
+    if cb is None:
+        vals = []
+        for _ in range(args.steps):
+            cb = cpu_baseline(m, args, None)
+            vals.append(cb["value"])
+    else:
+        cb["port_all_cores"] = {k: port[k] for k in ("value", "unit", "cores", "kind", "sample")}
     v = statistics.median(vals)
     cb["value"] = v
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -1057,6 +1130,10 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=30)
     ap.add_argument("--cpu-iters", type=int, default=30)
     ap.add_argument("--cpu-assumed-iters", type=int, default=2000)
+    # the reference-code solve sample: a cube as large as the port's (its matrix
+    # out of cache), a loose stop rule only to bound the sample's iterations
+    ap.add_argument("--cpu-ref-n", type=int, default=30)
+    ap.add_argument("--cpu-ref-eps", type=float, default=1e-3)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     # batch / serve
     ap.add_argument("--count", type=int, default=512)

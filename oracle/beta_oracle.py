@@ -506,17 +506,18 @@ class RefEquations:
         I, D = C.c_int, C.c_double
         self.lib.ref_equations_assemble.argtypes = [I, I, I, _ipc, _dp, C.c_void_p, _u8, _dp, _dp, D, I, C.c_void_p,
                                                     _lp, _ipc, _dp, C.c_longlong, C.POINTER(C.c_longlong), _dp, _dp,
-                                                    C.c_void_p]
+                                                    C.c_void_p, _dp]
 
     @staticmethod
     def available():
         return os.path.exists(REF_EQUATIONS_LIB)
 
     def assemble(self, n, maps, Ke, restrained, prescribed, load, solve=False, eps=1e-4, maxit=10000, Fe=None,
-                 x0=None):
+                 x0=None, timings=None):
         """Element matrices Ke (and force vectors Fe) through the reference's
         Equations; solve from the initial guess x0 when asked.  Returns
-        (rowptr, col, val, pseudo_load, load_vector, x or None)."""
+        (rowptr, col, val, pseudo_load, load_vector, x or None); a list given
+        as timings receives the seconds of structure, scatter and solve."""
         maps = np.ascontiguousarray(maps, dtype=np.int32)
         nelem, nde = maps.shape
         Ke = np.ascontiguousarray(Ke, dtype=float).reshape(-1)
@@ -526,16 +527,19 @@ class RefEquations:
         x = np.zeros(n) if solve else None
         nnz = C.c_longlong(0)
         fe = None if Fe is None else _f64(Fe).reshape(-1).copy()
+        secs = np.zeros(3)
         g = None if x0 is None else _f64(x0).copy()
         rc = self.lib.ref_equations_assemble(n, nelem, nde, maps.reshape(-1), Ke,
                                              None if fe is None else fe.ctypes.data,
                                              np.ascontiguousarray(restrained, dtype=np.uint8), _f64(prescribed),
                                              _f64(load), float(eps), int(maxit), None if g is None else g.ctypes.data,
                                              rp, col, val, cap, C.byref(nnz), pseudo, lv,
-                                             None if x is None else x.ctypes.data)
+                                             None if x is None else x.ctypes.data, secs)
         if rc:
             raise ValueError("ref_equations_assemble returned %d" % rc)
         k = nnz.value
+        if timings is not None:
+            timings[:] = secs.tolist()
         return rp, col[:k].copy(), val[:k].copy(), pseudo, lv, x
 
 
@@ -562,6 +566,7 @@ class RefLeaf:
         self.lib.ref_heat3d_add_to_km.argtypes = [_dp, D, _dp, _dp, _dp, _dp, D, _dp, _dp]
         self.lib.ref_heat3d_step_terms.argtypes = [_dp, _dp, _dp, D, D, D, _dp, _dp]
         self.lib.ref_elastic_point.argtypes = [I, I, _dp, _dp, _dp, C.c_void_p, C.c_void_p, D, _dp, _dp, _dp]
+        self.lib.ref_elastic_hex8_ke.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
         self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
                                           C.c_void_p, C.c_void_p]
@@ -654,6 +659,19 @@ class RefLeaf:
         if rc:
             raise ValueError("ref_elastic_point refused the element size")
         return K.reshape(dim * n, dim * n), F, eps[:3 if dim == 2 else 6]
+
+    def elastic_hex8_ke(self, xyz, C36, order):
+        """Hex8 stiffness (upper triangles, nel x 24 x 24) of elements xyz
+        (nel x 8 x 3) with constitutive matrices C36 (nel x 6 x 6) through the
+        reference's Gauss rule, shape functions and ElasticityElement3D B and
+        addToKe (a serial loop)."""
+        xyz = _f64(xyz).reshape(-1, 24)
+        nel = xyz.shape[0]
+        Ke = np.zeros(nel * 576)
+        rc = self.lib.ref_elastic_hex8_ke(nel, xyz.reshape(-1).copy(), _f64(C36).reshape(-1).copy(), int(order), Ke)
+        if rc:
+            raise ValueError("ref_elastic_hex8_ke: non-positive Jacobian")
+        return Ke.reshape(nel, 24, 24)
 
     def print_lower(self, path, fmt, row_ptr, col, val):
         """The reference's printMatrixAddressFormat (fmt 1), ...Upper (2) or

@@ -7,6 +7,7 @@
 // elimination, point loads, solve -- on element matrices and dof maps the
 // caller supplies, so the oracle's pattern, scatter and right-hand side can
 // be compared with the reference's.
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <sstream>
@@ -60,17 +61,21 @@ extern "C" {
 // last solution, zero here) -- the sequence DiffusionModel's transient step
 // runs with Mbar_e and Fbar_e and x0 = u_s.
 // Outputs: the lower triangle as 0-based CSR (rp n+1, col/val up to cap
-// entries, *nnz the count), the pseudo-load vector, the load vector, and x.
+// entries, *nnz the count), the pseudo-load vector, the load vector, x, and
+// (when non-null) seconds[3]: wall time of the structure (setup, pattern,
+// allocate), of the element scatter (addMatrix, loads) and of the solve.
 // Returns 0; 1 when cap is too small; 2 when a load sits on a restrained
 // unknown (the reference stops there with "Cannot add load to a restrained
 // degree of freedom").
 int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const double* Ke,
                            const double* Fe, const unsigned char* restrained, const double* prescribed,
                            const double* load, double eps, int maxit, const double* x0, long long* rp, int* col, double* val, long long cap,
-                           long long* nnz, double* pseudo, double* loadvec, double* x) {
+                           long long* nnz, double* pseudo, double* loadvec, double* x, double* seconds) {
   for (int i = 0; i < n; ++i)
     if (restrained[i] && load[i] != 0.0) return 2;
   QuietStreams quiet;
+  auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+  double t0 = now(), t1 = 0.0, t2 = 0.0;
   Equations eq;
   eq.setMaxIterations(maxit);
   eq.setSOLUTION_EPSILON(eps);
@@ -82,6 +87,7 @@ int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const dou
   for (int e = 0; e < nelem; ++e) eq.specifyNonZeroLocation(maps + (size_t)e * nde, nde);
   eq.allocate();
   eq.zeroMatrix();
+  t1 = now();
   Matrix K(nde, nde);
   for (int e = 0; e < nelem; ++e) {
     const double* ke = Ke + (size_t)e * nde * nde;
@@ -91,6 +97,7 @@ int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const dou
   }
   for (int i = 0; i < n; ++i)
     if (load[i] != 0.0) eq.addLoadToEqn(load[i], i, false);
+  t2 = now();
   SymmetricSparseMatrix& A = *static_cast<SymmetricSparseMatrix*>(eq.a);
   long long k = 0;
   rp[0] = 0;
@@ -111,8 +118,15 @@ int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const dou
   if (x) {
     std::vector<double> guess;
     if (x0) guess.assign(x0, x0 + n);
+    const double t3 = now();
     const double* u = eq.solve(x0 ? guess.data() : 0);
+    if (seconds) seconds[2] = now() - t3;
     for (int i = 0; i < n; ++i) x[i] = u[i];
+  }
+  if (seconds) {
+    seconds[0] = t1 - t0;
+    seconds[1] = t2 - t1;
+    if (!x) seconds[2] = 0.0;
   }
   return 0;
 }

@@ -229,6 +229,70 @@ int ref_elastic_point(int dim, int nnode, const double* C, const double* dx, con
   return 1;
 }
 
+// Hex8 elasticity stiffness of nel elements the way the reference forms it:
+// its own HexQuadPoints rule of the given order and shapeHex8/derivHex8, the
+// Jacobian J (rows d/dxi, d/deta, d/dzeta of the coordinates), its
+// determinant and inverse by cofactors (IsoElement::jacobian,
+// isoElement.cpp:250-389, restated: that file does not compile here), then
+// ElasticityElement3D::calculateBmatrix + addToKe at every point.  xyz is
+// nel x 8 x 3, C36 nel x 6 x 6 (row-major), Ke nel x 24 x 24 (upper
+// triangles).  A serial loop, as the reference's SerialAssembler runs it.
+int ref_elastic_hex8_ke(int nel, const double* xyz, const double* C36, int order, double* Ke) {
+  double *gx, *gy, *gz, *gw;
+  HexQuadPoints::getQuadraturePointsForHex(order, &gx, &gy, &gz, &gw);
+  const int nip = order * order * order;
+  ElasticityElement3D e;
+  std::vector<double> brows(6 * 24, 0.0);
+  double* rows[6];
+  for (int r = 0; r < 6; ++r) rows[r] = brows.data() + r * 24;
+  Matrix K(24, 24), c(6, 6);
+  InterpAndSolDerivatives id(8, 8);
+  id.allocate();
+  id.numberOfInterp = 8;
+  e.b = rows;
+  e.Ke = &K;
+  e.numDof = 24;
+  double S[8], d0[8], d1[8], d2[8], stress[6] = {0, 0, 0, 0, 0, 0};
+  for (int el = 0; el < nel; ++el) {
+    const double* X = xyz + (size_t)el * 24;
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) c(i, j) = C36[(size_t)el * 36 + i * 6 + j];
+    for (int i = 0; i < 24; ++i)
+      for (int j = 0; j < 24; ++j) K(i, j) = 0.0;
+    for (int ip = 0; ip < nip; ++ip) {
+      shapeHex8(S, gx[ip], gy[ip], gz[ip]);
+      derivHex8(d0, d1, d2, gx[ip], gy[ip], gz[ip]);
+      double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int a = 0; a < 8; ++a)
+        for (int k = 0; k < 3; ++k) {
+          J[0][k] += d0[a] * X[a * 3 + k];
+          J[1][k] += d1[a] * X[a * 3 + k];
+          J[2][k] += d2[a] * X[a * 3 + k];
+        }
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
+                   c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      if (!(det > 0.0)) return 2;
+      const double inv[3][3] = {
+          {c00 / det, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det, (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det},
+          {c01 / det, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det, (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det},
+          {c02 / det, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det, (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det}};
+      for (int a = 0; a < 8; ++a) {
+        id.S[a] = S[a];
+        id.p_S_x1[a] = inv[0][0] * d0[a] + inv[0][1] * d1[a] + inv[0][2] * d2[a];
+        id.p_S_x2[a] = inv[1][0] * d0[a] + inv[1][1] * d1[a] + inv[1][2] * d2[a];
+        id.p_S_x3[a] = inv[2][0] * d0[a] + inv[2][1] * d1[a] + inv[2][2] * d2[a];
+      }
+      e.calculateBmatrix(&id, rows);
+      e.addToKe(&c, &id, det * gw[ip], stress);
+    }
+    double* out = Ke + (size_t)el * 576;
+    for (int i = 0; i < 24; ++i)
+      for (int j = 0; j < 24; ++j) out[i * 24 + j] = K(i, j);
+  }
+  return 0;
+}
+
 // The element side of one backward-Euler step (DiffusionModel with a1, a2):
 // formK_s gives Mbar = (a1 K + M)/dt, formF_s_new F = -(a1+a2)/dt K u_s, from
 // the element's K and M (upper triangles, 8 x 8 row-major) and its nodal u_s.
