@@ -504,7 +504,7 @@ class RefEquations:
         _ipc = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
         _u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
         I, D = C.c_int, C.c_double
-        self.lib.ref_equations_assemble.argtypes = [I, I, I, _ipc, _dp, C.c_void_p, _u8, _dp, _dp, D, I, C.c_void_p,
+        self.lib.ref_equations_assemble.argtypes = [I, I, I, I, _ipc, _dp, C.c_void_p, _u8, _dp, _dp, D, I, C.c_void_p,
                                                     _lp, _ipc, _dp, C.c_longlong, C.POINTER(C.c_longlong), _dp, _dp,
                                                     C.c_void_p, _dp]
 
@@ -513,11 +513,13 @@ class RefEquations:
         return os.path.exists(REF_EQUATIONS_LIB)
 
     def assemble(self, n, maps, Ke, restrained, prescribed, load, solve=False, eps=1e-4, maxit=10000, Fe=None,
-                 x0=None, timings=None):
+                 x0=None, timings=None, parcg=False):
         """Element matrices Ke (and force vectors Fe) through the reference's
         Equations; solve from the initial guess x0 when asked.  Returns
         (rowptr, col, val, pseudo_load, load_vector, x or None); a list given
-        as timings receives the seconds of structure, scatter and solve."""
+        as timings receives the seconds of structure, scatter and solve.
+        parcg selects the reference's two-thread ParCG storage and solver
+        instead of the default serial SymmetricSparseMatrix."""
         maps = np.ascontiguousarray(maps, dtype=np.int32)
         nelem, nde = maps.shape
         Ke = np.ascontiguousarray(Ke, dtype=float).reshape(-1)
@@ -529,7 +531,7 @@ class RefEquations:
         fe = None if Fe is None else _f64(Fe).reshape(-1).copy()
         secs = np.zeros(3)
         g = None if x0 is None else _f64(x0).copy()
-        rc = self.lib.ref_equations_assemble(n, nelem, nde, maps.reshape(-1), Ke,
+        rc = self.lib.ref_equations_assemble(int(bool(parcg)), n, nelem, nde, maps.reshape(-1), Ke,
                                              None if fe is None else fe.ctypes.data,
                                              np.ascontiguousarray(restrained, dtype=np.uint8), _f64(prescribed),
                                              _f64(load), float(eps), int(maxit), None if g is None else g.ctypes.data,

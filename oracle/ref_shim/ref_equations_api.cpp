@@ -10,6 +10,8 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <fcntl.h>
+#include <unistd.h>
 #include <sstream>
 #include <strings.h>
 #include <vector>
@@ -33,14 +35,28 @@ int getLineAndTokenize(std::istream* in, char* terminateString, char* tokenList[
 }
 void displayTime(const char*, std::ostream&) {}
 std::ifstream* openFileForInput(char* filename) { return new std::ifstream(filename); }
-extern "C" int omp_get_max_threads() { return 1; }  // the constructor records it as the solver thread count
 
 namespace {
-struct QuietStreams {  // the solve reports to cout/cerr; keep that out of the caller's output
+// The solvers report to cout/cerr and (ParCG) to C stdout; keep all of it
+// out of the caller's output: the C++ streams go to a string, file
+// descriptor 1 to /dev/null for the duration.
+struct QuietStreams {
   std::stringstream sink;
   std::streambuf *out, *err;
-  QuietStreams() : out(std::cout.rdbuf(sink.rdbuf())), err(std::cerr.rdbuf(sink.rdbuf())) {}
+  int saved_fd = -1;
+  QuietStreams() : out(std::cout.rdbuf(sink.rdbuf())), err(std::cerr.rdbuf(sink.rdbuf())) {
+    std::fflush(stdout);
+    saved_fd = dup(1);
+    const int devnull = open("/dev/null", O_WRONLY);
+    if (saved_fd >= 0 && devnull >= 0) dup2(devnull, 1);
+    if (devnull >= 0) close(devnull);
+  }
   ~QuietStreams() {
+    std::fflush(stdout);
+    if (saved_fd >= 0) {
+      dup2(saved_fd, 1);
+      close(saved_fd);
+    }
     std::cout.rdbuf(out);
     std::cerr.rdbuf(err);
   }
@@ -53,7 +69,8 @@ extern "C" {
 // their matrices, Fe (nelem x nde, may be null) their force vectors;
 // restrained (n, 0/1) with prescribed values; point loads.
 // Runs, in the reference's order: setRestraint for each restrained unknown,
-// setupStorage(Sparse, n), setSolution of the prescribed values,
+// setupStorage(Sparse, n) -- or ParCG when parcg is nonzero, the
+// reference's two-thread OpenMP solver --, setSolution of the prescribed values,
 // specifyNonZeroLocation per element, allocate, zeroMatrix, addMatrix per
 // element (with its force vector), addLoadToEqn per nonzero load, then (when
 // x is non-null) solve with the reference's CG (tolerance eps, at most maxit
@@ -67,7 +84,7 @@ extern "C" {
 // Returns 0; 1 when cap is too small; 2 when a load sits on a restrained
 // unknown (the reference stops there with "Cannot add load to a restrained
 // degree of freedom").
-int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const double* Ke,
+int ref_equations_assemble(int parcg, int n, int nelem, int nde, const int* maps, const double* Ke,
                            const double* Fe, const unsigned char* restrained, const double* prescribed,
                            const double* load, double eps, int maxit, const double* x0, long long* rp, int* col, double* val, long long cap,
                            long long* nnz, double* pseudo, double* loadvec, double* x, double* seconds) {
@@ -81,7 +98,7 @@ int ref_equations_assemble(int n, int nelem, int nde, const int* maps, const dou
   eq.setSOLUTION_EPSILON(eps);
   for (int i = 0; i < n; ++i)
     if (restrained[i]) eq.setRestraint(i, true);
-  eq.setupStorage(Sparse, n);
+  eq.setupStorage(parcg ? ParCG : Sparse, n);
   for (int i = 0; i < n; ++i)
     if (restrained[i]) eq.setSolution(prescribed[i], i);
   for (int e = 0; e < nelem; ++e) eq.specifyNonZeroLocation(maps + (size_t)e * nde, nde);

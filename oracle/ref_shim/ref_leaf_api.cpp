@@ -4,7 +4,12 @@
 // oracle/_ref/libbeta_ref_leaf.so.
 // Test infrastructure: used only to pin the oracle's restatement against the
 // reference's code.
+#include <fcntl.h>
+#include <unistd.h>
+
+#include <cstdio>
 #include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -48,6 +53,29 @@ void shapeTri6(double* S, double xi, double eta);
 void derivTri6(double* Sxi, double* Seta, double xi, double eta);
 
 namespace {
+// Keeps what the reference code prints (C++ streams and C stdout) out of the
+// caller's standard output while a timing entry point runs.
+struct QuietStdout {
+  std::stringstream sink;
+  std::streambuf* out;
+  int saved_fd = -1;
+  QuietStdout() : out(std::cout.rdbuf(sink.rdbuf())) {
+    std::fflush(stdout);
+    saved_fd = dup(1);
+    const int devnull = open("/dev/null", O_WRONLY);
+    if (saved_fd >= 0 && devnull >= 0) dup2(devnull, 1);
+    if (devnull >= 0) close(devnull);
+  }
+  ~QuietStdout() {
+    std::fflush(stdout);
+    if (saved_fd >= 0) {
+      dup2(saved_fd, 1);
+      close(saved_fd);
+    }
+    std::cout.rdbuf(out);
+  }
+};
+
 // One integration point of the reference's own elasticity element E
 // (ElasticityElement3D or ElasticityElement2D): calculateBmatrix + addToKe
 // into Ke (ndof x ndof row-major, upper triangle) and, when u is given,
@@ -238,6 +266,7 @@ int ref_elastic_point(int dim, int nnode, const double* C, const double* dx, con
 // nel x 8 x 3, C36 nel x 6 x 6 (row-major), Ke nel x 24 x 24 (upper
 // triangles).  A serial loop, as the reference's SerialAssembler runs it.
 int ref_elastic_hex8_ke(int nel, const double* xyz, const double* C36, int order, double* Ke) {
+  QuietStdout quiet;  // the Gauss-rule code announces each order it computes
   double *gx, *gy, *gz, *gw;
   HexQuadPoints::getQuadraturePointsForHex(order, &gx, &gy, &gz, &gw);
   const int nip = order * order * order;

@@ -1,7 +1,8 @@
 """The bench's reference arm on the host: where the reference's own code was
 compiled (oracle/_ref), the cube's reference figure comes from it -- element
-B/addToKe, Equations pattern and addMatrix, SymmetricSparseMatrix::solve --
-serially, with the oracle's all-core port beside it."""
+B/addToKe, Equations pattern and addMatrix, and the faster of
+SymmetricSparseMatrix::solve and the two-thread ParCG solve -- with the
+oracle's all-core port beside it."""
 import os
 import sys
 from types import SimpleNamespace
@@ -21,6 +22,26 @@ def test_reference_code_baseline_times_the_reference(oracle):
     m = W.cube_hex8(6, seed=2)
     args = SimpleNamespace(cpu_elems=64, cpu_ref_n=4, cpu_ref_eps=1e-6)
     cb = bench.reference_code_baseline(m, args, 100)
-    assert cb["kind"] == "reference" and cb["cores"] == 1
+    assert cb["kind"] == "reference" and cb["cores"] in (1, 2)
     assert cb["value"] > 0 and cb["seconds_full_solve_est"] > 0
-    assert "SymmetricSparseMatrix::solve" in cb["sample"]
+    assert "SymmetricSparseMatrix::solve" in cb["sample"] and "ParCGMatrix::solve" in cb["sample"]
+
+
+def test_reference_arm_prints_one_json_line():
+    """bench.py --impl reference on a small cube: standard output is exactly
+    one JSON line (the reference code's own messages are kept off it), with
+    the reference's figure and, where oracle/_ref exists, the port beside it."""
+    import json
+    import subprocess
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--n", "12", "--cpu-elems", "500", "--cpu-ref-n", "6", "--cpu-n", "8",
+                        "--cpu-iters", "5"], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["value"] == d["value"]
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port")
+    if cb["kind"] == "reference":
+        assert cb["port_all_cores"]["kind"] == "port"

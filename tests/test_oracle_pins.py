@@ -473,3 +473,21 @@ def test_transient_steps_equal_the_reference_step(oracle):
             rc, u_o, st = s.heat_step(m.params, m.order, 5e-4, u_o, alpha=0.75, eps=1e-14, maxit=100000)
             u_r = gen.ref_heat_step(leaf, req, m, u_r, 5e-4, 0.75, 1e-14)
             np.testing.assert_array_equal(u_o, u_r)
+
+
+def test_parcg_solves_like_the_oracle(oracle):
+    """The reference's two-thread solver (ParCG.cpp ParCGMatrix::solve, the
+    same Jacobi-PCG with its dot products split between two OpenMP threads,
+    compiled unmodified) reaches the oracle's solution to rounding on a system
+    assembled through the reference's Equations."""
+    if not oracle.RefEquations.available():
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    gen = _gen_golden()
+    req = oracle.RefEquations()
+    for m in (W.rve_hex8(3, seed=2), W.renumbered(W.cube_hex8(6, seed=1), 4)):
+        nd = m.nnpe * m.ndpn
+        st, Ke = oracle.element_matrices_threaded(m, m.params, m.order, 0, m.nelem)
+        got = req.assemble(m.ndof, gen.element_maps(m), Ke.reshape(m.nelem, nd, nd), m.restrained, m.prescribed,
+                           m.load, solve=True, eps=1e-10, maxit=100000, parcg=True)
+        x = _oracle_system(oracle, m, True, 1e-10)[4]
+        assert np.abs(got[5] - x).max() <= 1e-11 * np.abs(x).max()
