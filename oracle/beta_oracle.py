@@ -567,6 +567,7 @@ class RefLeaf:
         self.lib.ref_heat2d_add_to_ke.argtypes = [D, D, D, I, _dp, _dp, D, _dp]
         self.lib.ref_heat3d_add_to_km.argtypes = [_dp, D, _dp, _dp, _dp, _dp, D, _dp, _dp]
         self.lib.ref_heat3d_step_terms.argtypes = [_dp, _dp, _dp, D, D, D, _dp, _dp]
+        self.lib.ref_heat_step_terms.argtypes = [I, _dp, _dp, _dp, D, D, D, _dp, _dp]
         self.lib.ref_elastic_point.argtypes = [I, I, _dp, _dp, _dp, C.c_void_p, C.c_void_p, D, _dp, _dp, _dp]
         self.lib.ref_elastic_hex8_ke.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
@@ -632,6 +633,16 @@ class RefLeaf:
         self.lib.ref_heat3d_add_to_km(f(np.asarray(k9).reshape(-1)), float(cap), f(S), f(dx), f(dy), f(dz),
                                       float(factor), K, M)
         return K.reshape(8, 8), M.reshape(8, 8)
+
+    def heat_step_terms(self, K, M, u_s, a1, a2, dt):
+        """formK_s and formF_s_new for an element of n = len(u_s) nodes (8:
+        hex8, 4: quad4): (Mbar n x n, F n)."""
+        n = len(u_s)
+        Mb, F = np.zeros(n * n), np.zeros(n)
+        f = lambda a: np.ascontiguousarray(a, dtype=float).reshape(-1)  # noqa: E731
+        if self.lib.ref_heat_step_terms(n, f(K), f(M), f(u_s), float(a1), float(a2), float(dt), Mb, F):
+            raise ValueError("ref_heat_step_terms: bad size")
+        return Mb.reshape(n, n), F
 
     def heat3d_step_terms(self, K, M, u_s, a1, a2, dt):
         """formK_s and formF_s_new of the reference's 3D diffusion element:

@@ -324,31 +324,39 @@ int ref_elastic_hex8_ke(int nel, const double* xyz, const double* C36, int order
 
 // The element side of one backward-Euler step (DiffusionModel with a1, a2):
 // formK_s gives Mbar = (a1 K + M)/dt, formF_s_new F = -(a1+a2)/dt K u_s, from
-// the element's K and M (upper triangles, 8 x 8 row-major) and its nodal u_s.
-int ref_heat3d_step_terms(const double* K, const double* M, const double* u_s, double a1, double a2, double dt,
-                          double* Mbar, double* F) {
+// the element's K and M (upper triangles, n x n row-major) and its nodal u_s.
+// n = 8 for the hex8 element; n = 4 for the quad4 element, which inherits
+// both from HeatTransferElement3Dtransient.
+int ref_heat_step_terms(int n, const double* K, const double* M, const double* u_s, double a1, double a2, double dt,
+                        double* Mbar, double* F) {
+  if (n < 1 || n > 27) return 1;
   HeatTransferElement3Dtransient e;
-  Matrix Km(8, 8), Mm(8, 8), Kb(8, 8);
-  for (int i = 0; i < 8; ++i)
-    for (int j = 0; j < 8; ++j) { Km(i, j) = K[i * 8 + j]; Mm(i, j) = M[i * 8 + j]; }
-  std::vector<double> fe(8, 0.0), us(u_s, u_s + 8);
-  int dofs[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+  Matrix Km(n, n), Mm(n, n), Kb(n, n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) { Km(i, j) = K[i * n + j]; Mm(i, j) = M[i * n + j]; }
+  std::vector<double> fe(n, 0.0), us(u_s, u_s + n);
+  std::vector<int> dofs(n);
+  for (int i = 0; i < n; ++i) dofs[i] = i;
   e.Ke = &Km;
   e.Me = &Mm;
   e.Ke_orig = &Kb;
   e.Fe = fe.data();
-  e.dofList = dofs;
-  e.numDof = 8;
+  e.dofList = dofs.data();
+  e.numDof = n;
   Array<double> ap(2);
   ap[0] = a1;
   ap[1] = a2;
   e.formK_s(ap, dt);
   e.formF_s_new(ap, us.data(), nullptr, nullptr, dt);
-  for (int i = 0; i < 8; ++i) {
+  for (int i = 0; i < n; ++i) {
     F[i] = fe[i];
-    for (int j = 0; j < 8; ++j) Mbar[i * 8 + j] = Kb(i, j);
+    for (int j = 0; j < n; ++j) Mbar[i * n + j] = Kb(i, j);
   }
   return 0;
+}
+int ref_heat3d_step_terms(const double* K, const double* M, const double* u_s, double a1, double a2, double dt,
+                          double* Mbar, double* F) {
+  return ref_heat_step_terms(8, K, M, u_s, a1, a2, dt, Mbar, F);
 }
 
 // A lower triangle (0-based CSR, diagonal last in each row) written by the

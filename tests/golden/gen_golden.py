@@ -40,7 +40,8 @@ the compiled reference leaf library (``make -C oracle``):
   node -- given the oracle's element matrices: the lower triangle (CSR), the
   pseudo-load vector and the solution.
 * ``ref_heat_steps.json`` -- backward-Euler steps of a small hex8 slab
-  (with and without a heat input, alpha 1 and 0.5) composed from the
+  (with and without a heat input) and a quad4 plate with a heat input
+  (the 2D element), alpha 1 and 0.5, composed from the
   reference's own code in DiffusionModel's order (DiffusionModel.cpp:743-818,
   322-347): per element its formK_s / formF_s_new
   (HeatTransferElement3DTransient.cpp) on the oracle's element K and M, the
@@ -299,7 +300,9 @@ def ref_equations():
 
 
 
-def heat_step_case(with_load):
+def heat_step_case(with_load, quad4=False):
+    if quad4:
+        return W.heat_plate(7, 5, heat=2.0)  # the 2D element, a heat input on its free nodes
     m = W.heat_slab(6, 5, 4, order=3)
     if with_load:
         rng = np.random.default_rng(17)
@@ -316,8 +319,11 @@ def ref_heat_step(leaf, req, m, u_s, dt, alpha, eps):
     nd = maps.shape[1]
     Mb, F = np.zeros((m.nelem, nd, nd)), np.zeros((m.nelem, nd))
     for e in range(m.nelem):
-        st, K, M = bo.km_hex8_heat(m.xyz[m.conn[e]], m.params[e, :3], m.params[e, 3], order=m.order)
-        Mb[e], F[e] = leaf.heat3d_step_terms(np.triu(K), np.triu(M), u_s[maps[e]], a1, a2, dt)
+        if m.nnpe == 8:
+            st, K, M = bo.km_hex8_heat(m.xyz[m.conn[e]], m.params[e, :3], m.params[e, 3], order=m.order)
+        else:
+            st, K, M = bo.km_quad4_heat(m.xyz[m.conn[e]], m.params[e, :2], m.params[e, 3], order=m.order)
+        Mb[e], F[e] = leaf.heat_step_terms(np.triu(K), np.triu(M), u_s[maps[e]], a1, a2, dt)
     x = req.assemble(m.ndof, maps, Mb, m.restrained, m.prescribed, m.load, solve=True, eps=eps, maxit=100000,
                      Fe=F, x0=u_s)[5]
     return u_s + x
@@ -328,16 +334,16 @@ def ref_heat_steps():
     out = {"source": "reference HeatTransferElement3DTransient.cpp formK_s/formF_s_new + equation.cpp "
                      "addMatrix/solve compiled unmodified (oracle/_ref), in DiffusionModel's order",
            "dt": 1e-3, "eps": 1e-14, "steps": 3, "cases": {}}
-    for with_load in (False, True):
+    for quad4, with_load in ((False, False), (False, True), (True, True)):
         for alpha in (1.0, 0.5):
-            m = heat_step_case(with_load)
+            m = heat_step_case(with_load, quad4)
             u = m.meta["u0"].copy()
             traj = []
             for _ in range(3):
                 u = ref_heat_step(leaf, req, m, u, 1e-3, alpha, 1e-14)
                 traj.append(u.tolist())
-            out["cases"]["%s_alpha%g" % ("load" if with_load else "free", alpha)] = {
-                "with_load": with_load, "alpha": alpha, "u": traj}
+            out["cases"]["%s%s_alpha%g" % ("quad4_" if quad4 else "", "load" if with_load else "free", alpha)] = {
+                "with_load": with_load, "quad4": quad4, "alpha": alpha, "u": traj}
     return out
 
 

@@ -443,7 +443,9 @@ def test_global_assembly_equals_the_reference_equations(oracle):
 
 def test_transient_steps_equal_the_reference_step(oracle):
     """Three backward-Euler steps of a hex8 slab (alpha 1 and 0.5, with and
-    without a heat input): the oracle's heat_step is bit-identical to the
+    without a heat input) and of a quad4 plate with a heat input (the 2D
+    element, which inherits the step terms): the oracle's heat_step is
+    bit-identical to the
     step composed from the reference's own code in DiffusionModel's order
     (DiffusionModel.cpp:743-818, 322-347) -- formK_s / formF_s_new of
     HeatTransferElement3Dtransient per element, Equations::addMatrix of
@@ -451,7 +453,7 @@ def test_transient_steps_equal_the_reference_step(oracle):
     gen = _gen_golden()
     g = _load("ref_heat_steps.json")
     for name, case in g["cases"].items():
-        m = gen.heat_step_case(case["with_load"])
+        m = gen.heat_step_case(case["with_load"], case.get("quad4", False))
         s = oracle.System(m)
         s.set_bc(m.restrained, m.prescribed, m.load)
         s.build_pattern()
