@@ -35,9 +35,10 @@ static void parallel_for(long long n, const std::function<void(long long, long l
 // Empties every output of P but keeps the memory of its vectors.
 static void reset_keep(HostPattern& P) {
   P.nnode = P.nelem = P.nnpe = P.ndpn = P.ndof = 0;
-  for (auto* v : {&P.nrp, &P.ncol, &P.ndiag, &P.color_ptr, &P.elem_by_color, &P.bsoff, &P.bcol, &P.scol, &P.soff,
-                  &P.srowlen})
+  for (auto* v : {&P.nrp, &P.ndiag, &P.color_ptr, &P.elem_by_color, &P.bsoff, &P.scol, &P.soff, &P.srowlen})
     v->clear();
+  P.ncol.clear();
+  P.bcol.clear();
   P.slot.clear();
   P.ssoff.clear();
   P.sdiag.clear();
@@ -66,6 +67,49 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     if (conn[k] < 0 || conn[k] >= nnode) return "build_pattern: connectivity out of range";
   reset_keep(P);
   P.nnode = nnode; P.nelem = nelem; P.nnpe = nnpe; P.ndpn = ndpn; P.ndof = nnode * ndpn;
+
+  // ---- greedy element colouring (one 64-bit colour mask per node) ----
+  // Serial (each element's colour depends on the ones before it) and
+  // independent of the node graph, so it runs on its own thread while the
+  // graph passes below use the others.  It writes only its own outputs.
+  std::string colour_err;
+  auto colour = [&]() {
+    std::vector<uint64_t>& used = P.s_used;
+    used.assign(nnode, 0);
+    std::vector<int>& color = P.s_color;
+    color.resize(nelem);
+    int maxc = 0;
+    for (int e = 0; e < nelem; ++e) {
+      const int* ce = conn + (long long)e * nnpe;
+      uint64_t m = 0;
+      for (int a = 0; a < nnpe; ++a) m |= used[ce[a]];
+      if (m == ~0ULL) {
+        colour_err = "build_pattern: more than 64 element colours";
+        return;
+      }
+      int c = __builtin_ctzll(~m);
+      color[e] = c;
+      maxc = std::max(maxc, c + 1);
+      for (int a = 0; a < nnpe; ++a) used[ce[a]] |= (1ULL << c);
+    }
+    P.ncolor = maxc;
+    P.color_ptr.assign(maxc + 1, 0);
+    for (int e = 0; e < nelem; ++e) P.color_ptr[color[e] + 1]++;
+    for (int c = 0; c < maxc; ++c) P.color_ptr[c + 1] += P.color_ptr[c];
+    P.elem_by_color.resize(nelem);
+    std::vector<int> fill(P.color_ptr.begin(), P.color_ptr.end() - 1);
+    for (int e = 0; e < nelem; ++e) P.elem_by_color[fill[color[e]]++] = e;
+  };
+  struct Joiner {  // the colouring thread is joined on every way out
+    std::thread t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } colouring;
+  if (chunk_count(nelem) > 1)
+    colouring.t = std::thread(colour);
+  else
+    colour();
 
   // ---- node -> element incidence -------------------------------------
   // Counted and filled by all threads with atomic adds; the order of a
@@ -125,64 +169,8 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     P.nrp[i + 1] += P.nrp[i];
   }
   P.nblk = P.nrp[nnode];
-  P.ncol.resize(P.nblk);
-  P.ndiag.resize(nnode);
-  // The fill pass also writes the element -> node-pair block map: with row i
-  // sorted, pos[J] holds J's position in it, so each incident element (e, a)
-  // with conn[e][a] == i gets slot[e][a][b] = position of conn[e][b] by
-  // lookup (every node of the element is in the row).  Each (e, a) belongs to
-  // one row, so the writes do not overlap, and each row is read once.
-  const int npair = nnpe * nnpe;
-  P.slot.resize((size_t)nelem * npair);
-  parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
-    std::vector<int> buf;
-    std::vector<int>& mark = P.s_mark[ck];
-    std::vector<int>& pos = P.s_mark[nck + ck];
-    if ((long long)pos.size() < nnode) pos.resize(nnode);
-    for (long long i = lo; i < hi; ++i) {
-      collect((int)i, buf, mark, nnode + (int)i + 1, true);
-      std::copy(buf.begin(), buf.end(), P.ncol.begin() + P.nrp[i]);
-      P.ndiag[i] = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
-      for (int k = 0; k < (int)buf.size(); ++k) pos[buf[k]] = k;
-      for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
-        const long long e = inc[k];
-        const int* ce = conn + e * nnpe;
-        for (int a = 0; a < nnpe; ++a) {
-          if (ce[a] != (int)i) continue;
-          uint16_t* sl = P.slot.data() + e * npair + a * nnpe;
-          for (int b = 0; b < nnpe; ++b) sl[b] = (uint16_t)pos[ce[b]];
-        }
-      }
-    }
-  });
 
-  // ---- greedy element colouring (one 64-bit colour mask per node) ----
-  {
-    std::vector<uint64_t>& used = P.s_used;
-    used.assign(nnode, 0);
-    std::vector<int>& color = P.s_color;
-    color.resize(nelem);
-    int maxc = 0;
-    for (int e = 0; e < nelem; ++e) {
-      const int* ce = conn + (long long)e * nnpe;
-      uint64_t m = 0;
-      for (int a = 0; a < nnpe; ++a) m |= used[ce[a]];
-      if (m == ~0ULL) return "build_pattern: more than 64 element colours";
-      int c = __builtin_ctzll(~m);
-      color[e] = c;
-      maxc = std::max(maxc, c + 1);
-      for (int a = 0; a < nnpe; ++a) used[ce[a]] |= (1ULL << c);
-    }
-    P.ncolor = maxc;
-    P.color_ptr.assign(maxc + 1, 0);
-    for (int e = 0; e < nelem; ++e) P.color_ptr[color[e] + 1]++;
-    for (int c = 0; c < maxc; ++c) P.color_ptr[c + 1] += P.color_ptr[c];
-    P.elem_by_color.resize(nelem);
-    std::vector<int> fill(P.color_ptr.begin(), P.color_ptr.end() - 1);
-    for (int e = 0; e < nelem; ++e) P.elem_by_color[fill[color[e]]++] = e;
-  }
-
-  // ---- node-block sliced ELL ------------------------------------------
+  // ---- node-block sliced ELL: slice widths from the row lengths -------
   P.nslice = (nnode + 31) / 32;
   P.bsoff.assign(P.nslice + 1, 0);
   for (int s = 0; s < P.nslice; ++s) {
@@ -192,57 +180,88 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   }
   P.nchunk = P.bsoff[P.nslice];
   if (P.nchunk * 32LL * ndpn * ndpn > 2000000000LL) return "build_pattern: block layout exceeds 2^31 entries";
-  P.bcol.assign((size_t)P.nchunk * 32, 0);
-  parallel_for(P.nslice, [&](long long lo, long long hi) {
-    for (long long s = lo; s < hi; ++s) {
-      int w = P.bsoff[s + 1] - P.bsoff[s];
-      for (int lane = 0; lane < 32; ++lane) {
-        int i = (int)s * 32 + lane;
-        int len = i < nnode ? P.nrp[i + 1] - P.nrp[i] : 0;
-        for (int k = 0; k < w; ++k)
-          P.bcol[(size_t)(P.bsoff[s] + k) * 32 + lane] =
-              k < len ? P.ncol[P.nrp[i] + k] : (i < nnode ? i : 0);
-      }
+
+  // free dofs per node, for the reference's lower-triangle count below
+  std::vector<int>& ufree = P.s_ufree;
+  ufree.resize(nnode);
+  parallel_for(nnode, [&](long long lo, long long hi) {
+    for (long long I = lo; I < hi; ++I) {
+      int f = 0;
+      for (int j = 0; j < ndpn; ++j) f += rest[ndpn * I + j] ? 0 : 1;
+      ufree[I] = f;
     }
   });
 
-  // ---- the reference's lower-triangle count --------------------------
-  // A free row r = I*ndpn + i holds the free dofs c <= r of its node row: all
-  // free dofs of the neighbours J < I (the row is sorted, so those before the
-  // diagonal) and the free dofs j <= i of I itself; a restrained row holds its
-  // diagonal only.
-  {
-    std::vector<int>& ufree = P.s_ufree;
-    ufree.assign(nnode, 0);
-    for (int I = 0; I < nnode; ++I)
-      for (int j = 0; j < ndpn; ++j) ufree[I] += rest[ndpn * I + j] ? 0 : 1;
-    unsigned hw = std::thread::hardware_concurrency();
-    const int nt = (int)std::max(1u, std::min(hw ? hw : 1u, 64u));
-    std::vector<long long> part(nt, 0);
-    std::vector<std::thread> th;
-    for (int t = 0; t < nt; ++t)
-      th.emplace_back([&, t]() {
-        long long acc = 0;
-        for (long long I = (long long)nnode * t / nt; I < (long long)nnode * (t + 1) / nt; ++I) {
-          long long below = 0;
-          for (int k = P.nrp[I]; k < P.nrp[I] + P.ndiag[I]; ++k) below += ufree[P.ncol[k]];
-          int own = 0;
-          for (int i = 0; i < ndpn; ++i) {
-            const long long r = I * ndpn + i;
-            if (rest[r]) {
-              acc += 1;
-            } else {
-              ++own;
-              acc += below + own;
-            }
-          }
+  // The fill pass writes, per node row i (sorted):
+  //   * the row into ncol, and ndiag;
+  //   * the element -> node-pair block map: with pos[J] = J's position in
+  //     row i, each incident element (e, a) with conn[e][a] == i gets
+  //     slot[e][a][b] = pos[conn[e][b]] (every node of the element is in the
+  //     row); each (e, a) belongs to one row, so the writes do not overlap;
+  //   * the row's lane of its slice in the node-block sliced ELL, padded to
+  //     the slice width with the row's own node;
+  //   * the reference's lower-triangle count of its dof rows: a free row
+  //     r = I*ndpn + i holds the free dofs c <= r of its node row (all free
+  //     dofs of the neighbours J < I -- those before the diagonal -- and the
+  //     free dofs j <= i of I itself); a restrained row holds its diagonal.
+  // Each row is read once.
+  P.ncol.resize(P.nblk);
+  P.ndiag.resize(nnode);
+  const int npair = nnpe * nnpe;
+  P.slot.resize((size_t)nelem * npair);
+  P.bcol.resize((size_t)P.nchunk * 32);
+  std::vector<long long> lower(nck, 0);
+  parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
+    std::vector<int> buf;
+    std::vector<int>& mark = P.s_mark[ck];
+    std::vector<int>& pos = P.s_mark[nck + ck];
+    if ((long long)pos.size() < nnode) pos.resize(nnode);
+    long long acc = 0;
+    for (long long i = lo; i < hi; ++i) {
+      collect((int)i, buf, mark, nnode + (int)i + 1, true);
+      const int len = (int)buf.size();
+      std::copy(buf.begin(), buf.end(), P.ncol.begin() + P.nrp[i]);
+      const int d = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
+      P.ndiag[i] = d;
+      for (int k = 0; k < len; ++k) pos[buf[k]] = k;
+      for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
+        const long long e = inc[k];
+        const int* ce = conn + e * nnpe;
+        for (int a = 0; a < nnpe; ++a) {
+          if (ce[a] != (int)i) continue;
+          uint16_t* sl = P.slot.data() + e * npair + a * nnpe;
+          for (int b = 0; b < nnpe; ++b) sl[b] = (uint16_t)pos[ce[b]];
         }
-        part[t] = acc;
-      });
-    for (auto& x : th) x.join();
-    P.nnz_lower = 0;
-    for (long long v : part) P.nnz_lower += v;
+      }
+      const long long s = i / 32;
+      const int w = P.bsoff[s + 1] - P.bsoff[s];
+      int* bc = P.bcol.data() + (size_t)P.bsoff[s] * 32 + (i % 32);
+      for (int k = 0; k < len; ++k) bc[(size_t)k * 32] = buf[k];
+      for (int k = len; k < w; ++k) bc[(size_t)k * 32] = (int)i;
+      long long below = 0;
+      for (int k = 0; k < d; ++k) below += ufree[buf[k]];
+      int own = 0;
+      for (int j = 0; j < ndpn; ++j) {
+        if (rest[i * ndpn + j]) {
+          acc += 1;
+        } else {
+          ++own;
+          acc += below + own;
+        }
+      }
+    }
+    lower[ck] = acc;
+  });
+  // lanes past the last node in the last slice
+  for (int i = nnode; i < P.nslice * 32; ++i) {
+    const int s = i / 32, w = P.bsoff[s + 1] - P.bsoff[s];
+    for (int k = 0; k < w; ++k) P.bcol[(size_t)(P.bsoff[s] + k) * 32 + (i % 32)] = 0;
   }
+  P.nnz_lower = 0;
+  for (long long v : lower) P.nnz_lower += v;
+
+  if (colouring.t.joinable()) colouring.t.join();
+  if (!colour_err.empty()) return colour_err;
   if (!with_scalar) {
     release_scratch(P);
     return "";

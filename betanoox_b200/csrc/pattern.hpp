@@ -17,17 +17,45 @@
 //     sparse.cpp:482-495), exported for the bit-exact structure check.
 #pragma once
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace betagpu {
+
+// Allocator whose resize() leaves new elements default-initialised (no zero
+// fill) for the large outputs the build writes in full in parallel; a
+// single-threaded zero fill before that would touch every page twice.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using FillVec = std::vector<T, NoInitAlloc<T>>;
 
 struct HostPattern {
   int nnode = 0, nelem = 0, nnpe = 0, ndpn = 0, ndof = 0;
 
   // node graph (CSR over nodes, columns ascending, self included)
   std::vector<int> nrp;       // nnode+1
-  std::vector<int> ncol;      // nblk
+  FillVec<int> ncol;          // nblk
   std::vector<int> ndiag;     // position of node i in its own row
   long long nblk = 0;
 
@@ -37,12 +65,12 @@ struct HostPattern {
   std::vector<int> elem_by_color; // nelem
 
   // element -> position of node J in node I's row, nelem * nnpe * nnpe
-  std::vector<uint16_t> slot;
+  FillVec<uint16_t> slot;
 
   // node-block sliced ELL: slice s covers nodes [32s, 32s+32)
   int nslice = 0;
   std::vector<int> bsoff;     // nslice+1, in chunks (one chunk = 32 blocks)
-  std::vector<int> bcol;      // nchunk*32, padding points at the row's own node
+  FillVec<int> bcol;          // nchunk*32, padding points at the row's own node
   long long nchunk = 0;
 
   // scalar sliced ELL over dofs (restrained rows: diagonal only; restrained

@@ -4,7 +4,8 @@
 // kinds are built one after another into one reused pattern: hex8 grids
 // with 3 and 1 dofs per node, natural and shuffled node numberings, and a
 // quad4 plate with an unused node and a degenerate element (a repeated
-// node).  Exit code 0 when every build matches.
+// node).  Each mesh is also built single-threaded, which must give the same
+// result.  Exit code 0 when every build matches.
 #include "../../betanoox_b200/csrc/pattern.hpp"
 
 #include <algorithm>
@@ -99,8 +100,15 @@ int main() {
                                                   M.rest.data(), fresh, true);
     const std::string e2 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, M.conn.data(), fd.data(),
                                                   M.rest.data(), reused, true);
-    const bool ok = e1.empty() && e2.empty() && equal(fresh, reused) && fresh.s_mark.empty() &&
-                    !reused.s_mark.empty();
+    // the same build on one thread (as the batch engine runs it) must agree:
+    // nothing may depend on the thread count or on the concurrent colouring
+    HostPattern serial;
+    betagpu::pattern_serial_on_this_thread(true);
+    const std::string e3 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, M.conn.data(), fd.data(),
+                                                  M.rest.data(), serial, true);
+    betagpu::pattern_serial_on_this_thread(false);
+    const bool ok = e1.empty() && e2.empty() && e3.empty() && equal(fresh, reused) && equal(fresh, serial) &&
+                    fresh.s_mark.empty() && !reused.s_mark.empty();
     std::printf("%-60s %s\n", M.name.c_str(), ok ? "equal" : "DIFFERENT");
     bad += ok ? 0 : 1;
   }

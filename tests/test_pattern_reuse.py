@@ -1,6 +1,6 @@
 """Host structure build reused by a solver context (HostPattern::keep_scratch):
 a pattern rebuilt into the memory of an earlier, different mesh equals a
-fresh build in every field (tests/cpp/pattern_reuse_check.cpp, compiled
+fresh build in every field, and so does a single-threaded build (tests/cpp/pattern_reuse_check.cpp, compiled
 here against the host sources; no GPU needed)."""
 import os
 import subprocess
