@@ -60,11 +60,21 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
                           const int* first_dof, const unsigned char* rest, HostPattern& P, bool with_scalar) {
   if (nnode <= 0 || nelem <= 0 || nnpe <= 0 || nnpe > 8 || ndpn < 1 || ndpn > 3)
     return "build_pattern: bad sizes";
-  for (int i = 0; i < nnode; ++i)
-    if (first_dof[i] != ndpn * i)
-      return "build_pattern: first_dof must be the uniform node-major numbering ndpn*node";
-  for (long long k = 0; k < (long long)nelem * nnpe; ++k)
-    if (conn[k] < 0 || conn[k] >= nnode) return "build_pattern: connectivity out of range";
+  {
+    bool bad_dof = false, bad_conn = false;  // each set only to true, by any thread
+    parallel_for(nnode, [&](long long lo, long long hi) {
+      bool bad = false;
+      for (long long i = lo; i < hi; ++i) bad |= first_dof[i] != ndpn * (int)i;
+      if (bad) __atomic_store_n(&bad_dof, true, __ATOMIC_RELAXED);
+    });
+    parallel_for((long long)nelem * nnpe, [&](long long lo, long long hi) {
+      bool bad = false;
+      for (long long k = lo; k < hi; ++k) bad |= conn[k] < 0 || conn[k] >= nnode;
+      if (bad) __atomic_store_n(&bad_conn, true, __ATOMIC_RELAXED);
+    });
+    if (bad_dof) return "build_pattern: first_dof must be the uniform node-major numbering ndpn*node";
+    if (bad_conn) return "build_pattern: connectivity out of range";
+  }
   reset_keep(P);
   P.nnode = nnode; P.nelem = nelem; P.nnpe = nnpe; P.ndpn = ndpn; P.ndof = nnode * ndpn;
 

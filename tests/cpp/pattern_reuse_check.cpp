@@ -112,5 +112,24 @@ int main() {
     std::printf("%-60s %s\n", M.name.c_str(), ok ? "equal" : "DIFFERENT");
     bad += ok ? 0 : 1;
   }
+  // invalid input is refused with its message, on any thread count
+  {
+    Mesh M = hex8(30, 3, false, 0);
+    std::vector<int> fd(M.nnode);
+    for (int i = 0; i < M.nnode; ++i) fd[i] = M.nd * i;
+    HostPattern Q;
+    std::vector<int> bad_conn = M.conn;
+    bad_conn[bad_conn.size() - 3] = M.nnode;  // one node index past the end, near the end of the list
+    const std::string e1 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, bad_conn.data(), fd.data(),
+                                                  M.rest.data(), Q, false);
+    std::vector<int> bad_fd = fd;
+    bad_fd[M.nnode / 2] += 1;
+    const std::string e2 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, M.conn.data(), bad_fd.data(),
+                                                  M.rest.data(), Q, false);
+    const bool ok = e1 == "build_pattern: connectivity out of range" &&
+                    e2 == "build_pattern: first_dof must be the uniform node-major numbering ndpn*node";
+    std::printf("%-60s %s\n", "invalid connectivity and numbering", ok ? "refused" : "NOT REFUSED");
+    bad += ok ? 0 : 1;
+  }
   return bad ? 1 : 0;
 }

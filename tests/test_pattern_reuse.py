@@ -16,3 +16,4 @@ def test_reused_pattern_equals_fresh_build(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count("equal") == 7
+    assert "NOT REFUSED" not in r.stdout and r.stdout.count("refused") == 1
