@@ -507,10 +507,20 @@ class RefEquations:
         self.lib.ref_equations_assemble.argtypes = [I, I, I, I, _ipc, _dp, C.c_void_p, _u8, _dp, _dp, D, I, C.c_void_p,
                                                     _lp, _ipc, _dp, C.c_longlong, C.POINTER(C.c_longlong), _dp, _dp,
                                                     C.c_void_p, _dp]
+        self.lib.ref_equations_resultant.argtypes = [I, I, I, _ipc, _dp, _u8, _dp]
 
     @staticmethod
     def available():
         return os.path.exists(REF_EQUATIONS_LIB)
+
+    def resultant(self, n, maps, Fe, restrained):
+        """Equations::assembleResultantVector of element force vectors Fe
+        (nelem x nde) with the restraint mask: the global internal force."""
+        maps = np.ascontiguousarray(maps, dtype=np.int32)
+        out = np.zeros(n)
+        self.lib.ref_equations_resultant(n, maps.shape[0], maps.shape[1], maps.reshape(-1),
+                                         _f64(Fe).reshape(-1).copy(), np.ascontiguousarray(restrained, np.uint8), out)
+        return out
 
     def assemble(self, n, maps, Ke, restrained, prescribed, load, solve=False, eps=1e-4, maxit=10000, Fe=None,
                  x0=None, timings=None, parcg=False):

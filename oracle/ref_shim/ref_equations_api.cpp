@@ -64,6 +64,23 @@ struct QuietStreams {
 }  // namespace
 
 extern "C" {
+// The global internal force as the reference sums it for a residual
+// (BasicModel::CalculateResidual): restraints set, setupStorage(Sparse, n),
+// then Equations::assembleResultantVector per element with its force vector
+// Fe (nelem x nde); out gets the resultant vector (restrained rows skipped).
+int ref_equations_resultant(int n, int nelem, int nde, const int* maps, const double* Fe,
+                            const unsigned char* restrained, double* out) {
+  QuietStreams quiet;
+  Equations eq;
+  for (int i = 0; i < n; ++i)
+    if (restrained[i]) eq.setRestraint(i, true);
+  eq.setupStorage(Sparse, n);
+  for (int e = 0; e < nelem; ++e)
+    eq.assembleResultantVector(maps + (size_t)e * nde, nde, Fe + (size_t)e * nde);
+  for (int i = 0; i < n; ++i) out[i] = eq.resultantVector[i];
+  return 0;
+}
+
 // n unknowns; nelem elements of nde dofs each, maps (nelem x nde) their
 // equation numbers and Ke (nelem x nde x nde, row-major, upper triangle read)
 // their matrices, Fe (nelem x nde, may be null) their force vectors;

@@ -46,6 +46,11 @@ the compiled reference leaf library (``make -C oracle``):
   322-347): per element its formK_s / formF_s_new
   (HeatTransferElement3DTransient.cpp) on the oracle's element K and M, the
   Equations addMatrix of Mbar_e with Fbar_e, and solve from u_s.
+* ``ref_internal_force.json`` -- the global internal force of a renumbered
+  hex8 cube under a random displacement: element forces from the
+  reference's ElasticityElement3D (derivativesOfFields, calculateStrain,
+  addToFe) summed by its Equations::assembleResultantVector with the
+  restraint mask.
 * ``ref_matrix_kat.json`` -- the known answers written in the reference's
   DEBUG_MATRIX_CLASS main (beta/math/matrix.cpp:679-696).
 * ``oracle_small.json`` -- small end-to-end cases from the oracle (element
@@ -347,6 +352,32 @@ def ref_heat_steps():
     return out
 
 
+
+def internal_force_case():
+    m = W.renumbered(W.cube_hex8(4, seed=5), 3)
+    u = np.random.default_rng(1).normal(size=m.ndof)
+    return m, u
+
+
+def ref_internal_force():
+    leaf, req = bo.RefLeaf(), bo.RefEquations()
+    m, u = internal_force_case()
+    maps = element_maps(m)
+    xi, eta, zeta, w = leaf.hex_points(m.order)
+    Fe = np.zeros((m.nelem, 24))
+    for e in range(m.nelem):
+        X, C6 = m.xyz[m.conn[e]], bo.cmat_ortho3d(m.params[e])
+        K, F = np.zeros((24, 24)), np.zeros(24)
+        for a, b, c, wt in zip(xi, eta, zeta, w):
+            S, d0, d1, d2 = leaf.shape_hex8(a, b, c)
+            J = np.array([d0 @ X, d1 @ X, d2 @ X])
+            g = np.linalg.solve(J, np.array([d0, d1, d2]))
+            K, F, _ = leaf.elastic_point(C6, g[0], g[1], g[2], np.linalg.det(J) * wt, K, u=u[maps[e]], Fe=F)
+        Fe[e] = F
+    return {"source": "reference ElasticityElement3D addToFe + equation.cpp assembleResultantVector compiled "
+                      "unmodified (oracle/_ref)", "f": req.resultant(m.ndof, maps, Fe, m.restrained).tolist()}
+
+
 if __name__ == "__main__":
     with open(os.path.join(OUT, "ref_quadrature.json"), "w") as f:
         json.dump(ref_quadrature(), f)
@@ -360,6 +391,8 @@ if __name__ == "__main__":
         json.dump(ref_equations(), f)
     with open(os.path.join(OUT, "ref_heat_steps.json"), "w") as f:
         json.dump(ref_heat_steps(), f)
+    with open(os.path.join(OUT, "ref_internal_force.json"), "w") as f:
+        json.dump(ref_internal_force(), f)
     with open(os.path.join(OUT, "ref_matrix_kat.json"), "w") as f:
         json.dump(matrix_kat(), f, indent=1)
     with open(os.path.join(OUT, "oracle_small.json"), "w") as f:

@@ -493,3 +493,22 @@ def test_parcg_solves_like_the_oracle(oracle):
                            m.load, solve=True, eps=1e-10, maxit=100000, parcg=True)
         x = _oracle_system(oracle, m, True, 1e-10)[4]
         assert np.abs(got[5] - x).max() <= 1e-11 * np.abs(x).max()
+
+
+def test_internal_force_equals_the_reference_resultant(oracle):
+    """The oracle's global internal force (restrained rows skipped) against
+    the reference's: element forces from ElasticityElement3D's own
+    derivativesOfFields / calculateStrain / addToFe summed by
+    Equations::assembleResultantVector (compiled unmodified), on a renumbered
+    cube under a random displacement; live, the oracle's element forces
+    through the reference's assembleResultantVector are bit-identical."""
+    gen = _gen_golden()
+    m, u = gen.internal_force_case()
+    f = oracle.internal_force_hex8(m, m.params, m.order, u, m.restrained)
+    ref = np.array(_load("ref_internal_force.json")["f"])
+    assert np.abs(f - ref).max() <= 1e-14 * np.abs(ref).max()
+    if oracle.RefEquations.available():
+        maps = gen.element_maps(m)
+        Fe = np.stack([oracle.fe_hex8(m.xyz[m.conn[e]], oracle.cmat_ortho3d(m.params[e]), u[maps[e]], m.order)
+                       for e in range(m.nelem)])
+        np.testing.assert_array_equal(oracle.RefEquations().resultant(m.ndof, maps, Fe, m.restrained), f)
