@@ -508,6 +508,10 @@ void* oracle_sys_create(int n) {
 
 void oracle_sys_destroy(void* h) { delete (OracleSystem*)h; }
 
+// The zero-diagonal replacement value (Equations::setReplaceZeroDiagonal_Option
+// passed on to LargeMatrix; 0 = none, a zero diagonal is then an error).
+void oracle_sys_set_zero_diag(void* h, double v) { ((OracleSystem*)h)->zeroDiagReplacement = v; }
+
 // Restraints and prescribed values: Equations::setRestraint / setSolution
 // (equation.cpp:306-341).  Loads: Equations::addLoadToEqn (:851-868) -- a
 // nonzero load on a restrained dof is a fatal error in the reference.

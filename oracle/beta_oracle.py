@@ -68,6 +68,7 @@ def _load():
         "oracle_fe_hex8": (I, [_dp, _dp, I, _dp, _dp]),
         "oracle_sys_create": (V, [I]),
         "oracle_sys_destroy": (None, [V]),
+        "oracle_sys_set_zero_diag": (None, [V, D]),
         "oracle_sys_set_bc": (I, [V, _up, _dp, _dp]),
         "oracle_sys_specify": (None, [V, _ip, I]),
         "oracle_sys_allocate": (None, [V]),
@@ -270,6 +271,11 @@ class System:
         y = np.zeros(self.n)
         lib().oracle_sys_vector_product(self.h, _f64(x), y)
         return y
+
+    def set_zero_diag(self, value):
+        """Replacement for zero diagonals at the solve (0: a zero diagonal is
+        an error, as in the reference without ReplaceZeroDiagonal)."""
+        lib().oracle_sys_set_zero_diag(self.h, float(value))
 
     def solve(self, eps=1e-4, maxit=10000, init_guess=None):
         out = np.zeros(self.n)
@@ -506,7 +512,7 @@ class RefEquations:
         I, D = C.c_int, C.c_double
         self.lib.ref_equations_assemble.argtypes = [I, I, I, I, _ipc, _dp, C.c_void_p, _u8, _dp, _dp, D, I, C.c_void_p,
                                                     _lp, _ipc, _dp, C.c_longlong, C.POINTER(C.c_longlong), _dp, _dp,
-                                                    C.c_void_p, _dp]
+                                                    C.c_void_p, _dp, D]
         self.lib.ref_equations_resultant.argtypes = [I, I, I, _ipc, _dp, _u8, _dp]
 
     @staticmethod
@@ -523,13 +529,15 @@ class RefEquations:
         return out
 
     def assemble(self, n, maps, Ke, restrained, prescribed, load, solve=False, eps=1e-4, maxit=10000, Fe=None,
-                 x0=None, timings=None, parcg=False):
+                 x0=None, timings=None, parcg=False, zero_diag=0.0):
         """Element matrices Ke (and force vectors Fe) through the reference's
         Equations; solve from the initial guess x0 when asked.  Returns
         (rowptr, col, val, pseudo_load, load_vector, x or None); a list given
         as timings receives the seconds of structure, scatter and solve.
         parcg selects the reference's two-thread ParCG storage and solver
-        instead of the default serial SymmetricSparseMatrix."""
+        instead of the default serial SymmetricSparseMatrix; zero_diag is the
+        ReplaceZeroDiagonal option (0: none -- the reference then exits on a
+        zero diagonal, so give one whenever a row can be empty)."""
         maps = np.ascontiguousarray(maps, dtype=np.int32)
         nelem, nde = maps.shape
         Ke = np.ascontiguousarray(Ke, dtype=float).reshape(-1)
@@ -546,7 +554,7 @@ class RefEquations:
                                              np.ascontiguousarray(restrained, dtype=np.uint8), _f64(prescribed),
                                              _f64(load), float(eps), int(maxit), None if g is None else g.ctypes.data,
                                              rp, col, val, cap, C.byref(nnz), pseudo, lv,
-                                             None if x is None else x.ctypes.data, secs)
+                                             None if x is None else x.ctypes.data, secs, float(zero_diag))
         if rc:
             raise ValueError("ref_equations_assemble returned %d" % rc)
         k = nnz.value

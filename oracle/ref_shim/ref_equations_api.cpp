@@ -98,13 +98,16 @@ int ref_equations_resultant(int n, int nelem, int nde, const int* maps, const do
 // entries, *nnz the count), the pseudo-load vector, the load vector, x, and
 // (when non-null) seconds[3]: wall time of the structure (setup, pattern,
 // allocate), of the element scatter (addMatrix, loads) and of the solve.
+// zero_diag is the ReplaceZeroDiagonal option the storage gets (0: none;
+// the reference's solve then exits on a zero diagonal).
 // Returns 0; 1 when cap is too small; 2 when a load sits on a restrained
 // unknown (the reference stops there with "Cannot add load to a restrained
 // degree of freedom").
 int ref_equations_assemble(int parcg, int n, int nelem, int nde, const int* maps, const double* Ke,
                            const double* Fe, const unsigned char* restrained, const double* prescribed,
                            const double* load, double eps, int maxit, const double* x0, long long* rp, int* col, double* val, long long cap,
-                           long long* nnz, double* pseudo, double* loadvec, double* x, double* seconds) {
+                           long long* nnz, double* pseudo, double* loadvec, double* x, double* seconds,
+                           double zero_diag) {
   for (int i = 0; i < n; ++i)
     if (restrained[i] && load[i] != 0.0) return 2;
   QuietStreams quiet;
@@ -113,6 +116,7 @@ int ref_equations_assemble(int parcg, int n, int nelem, int nde, const int* maps
   Equations eq;
   eq.setMaxIterations(maxit);
   eq.setSOLUTION_EPSILON(eps);
+  eq.setReplaceZeroDiagonal_Option(zero_diag);
   for (int i = 0; i < n; ++i)
     if (restrained[i]) eq.setRestraint(i, true);
   eq.setupStorage(parcg ? ParCG : Sparse, n);

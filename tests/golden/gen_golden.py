@@ -38,7 +38,8 @@ the compiled reference leaf library (``make -C oracle``):
   matrix.cpp, compiled unmodified into oracle/_ref/libbeta_ref_equations.so)
   on small meshes -- renumbered, with nonzero prescribed values, an unused
   node -- given the oracle's element matrices: the lower triangle (CSR), the
-  pseudo-load vector and the solution.
+  pseudo-load vector and the solution; and a solve whose unused free node
+  leaves zero-diagonal rows, with the ReplaceZeroDiagonal option set.
 * ``ref_heat_steps.json`` -- backward-Euler steps of a small hex8 slab
   (with and without a heat input) and a quad4 plate with a heat input
   (the 2D element), alpha 1 and 0.5, composed from the
@@ -287,6 +288,15 @@ EQUATION_CASES = {
 }
 
 
+def zero_diag_case():
+    """A renumbered plate with one node no element uses, its dofs left free:
+    their rows hold only a zero diagonal (ReplaceZeroDiagonal territory)."""
+    m = W.renumbered(W.plate_quad4(4), 2, unused_node=True)
+    r = m.restrained.copy()
+    r[-m.ndpn:] = 0
+    return dataclasses.replace(m, restrained=r)
+
+
 def ref_equations():
     r = bo.RefEquations()
     out = {"source": "reference equation.cpp + addeqn.cpp + sparse.cpp + largeMatrix.cpp + matrix.cpp compiled "
@@ -301,6 +311,12 @@ def ref_equations():
         out["cases"][name] = {"rowptr": rp.tolist(), "col": col.tolist(), "val": val.tolist(),
                               "pseudo": pseudo.tolist(), "load": lv.tolist(),
                               "x": None if x is None else x.tolist()}
+    m = zero_diag_case()
+    nd = m.nnpe * m.ndpn
+    st, Ke = bo.element_matrices_threaded(m, m.params, m.order, 0, m.nelem)
+    x = r.assemble(m.ndof, element_maps(m), Ke.reshape(m.nelem, nd, nd), m.restrained, m.prescribed, m.load,
+                   solve=True, eps=1e-10, zero_diag=2.5)[5]
+    out["zero_diag"] = {"value": 2.5, "x": x.tolist()}
     return out
 
 

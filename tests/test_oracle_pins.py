@@ -512,3 +512,23 @@ def test_internal_force_equals_the_reference_resultant(oracle):
         Fe = np.stack([oracle.fe_hex8(m.xyz[m.conn[e]], oracle.cmat_ortho3d(m.params[e]), u[maps[e]], m.order)
                        for e in range(m.nelem)])
         np.testing.assert_array_equal(oracle.RefEquations().resultant(m.ndof, maps, Fe, m.restrained), f)
+
+
+def test_zero_diagonal_replacement_equals_the_reference(oracle):
+    """LargeMatrix::CheckAndFixZeroDiagonal (largeMatrix.cpp:43-79) through
+    the solve: rows of an unused free node hold only a zero diagonal.
+    Without a replacement value the oracle refuses (the reference exits);
+    with ReplaceZeroDiagonal set, its solution is bit-identical to the
+    reference's Equations solve."""
+    gen = _gen_golden()
+    m = gen.zero_diag_case()
+    g = _load("ref_equations.json")["zero_diag"]
+    s = oracle.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    s.assemble(m.params, m.order)
+    assert s.solve(eps=1e-10, maxit=10000)[0] == oracle.ERR_ZERO_DIAG
+    s.set_zero_diag(g["value"])
+    rc, x, st = s.solve(eps=1e-10, maxit=10000)
+    assert rc == 0
+    np.testing.assert_array_equal(x, np.array(g["x"]))
