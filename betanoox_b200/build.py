@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
@@ -48,7 +49,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB + ".tmp", *[os.path.join(SRC, s) for s in SOURCES]]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
+    started = time.time()
     subprocess.run(cmd, check=True)
+    # the library carries the time its build started: a source edited while
+    # nvcc ran (possibly after it had compiled that file) then reads as newer
+    # and the next build() compiles everything again, instead of leaving
+    # objects built from two versions of a shared header in one library
+    os.utime(LIB + ".tmp", (started, started))
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

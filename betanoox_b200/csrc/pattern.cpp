@@ -50,6 +50,7 @@ static void release_scratch(HostPattern& P) {
   if (P.keep_scratch) return;
   std::vector<int>().swap(P.s_icnt);
   std::vector<int>().swap(P.s_inc);
+  std::vector<int>().swap(P.s_ccnt);
   std::vector<int>().swap(P.s_color);
   std::vector<int>().swap(P.s_ufree);
   std::vector<uint64_t>().swap(P.s_used);
@@ -122,25 +123,42 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     colour();
 
   // ---- node -> element incidence -------------------------------------
-  // Counted and filled by all threads with atomic adds; the order of a
-  // node's elements is then arbitrary, which nothing downstream sees (rows
-  // are sorted, slots are looked up, the colouring walks elements in order).
+  // A counting sort by node with one count array per element chunk (no
+  // atomics): chunk t counts its entries per node, the counts become
+  // per-chunk offsets within each node's list, and chunk t fills its part in
+  // element order, so every node's elements come out ascending.
   std::vector<int>& icnt = P.s_icnt;
   icnt.assign(nnode + 1, 0);
-  const long long nent = (long long)nelem * nnpe;
-  parallel_for(nent, [&](long long lo, long long hi) {
-    for (long long k = lo; k < hi; ++k) __atomic_fetch_add(&icnt[conn[k] + 1], 1, __ATOMIC_RELAXED);
+  const int nec = chunk_count(nelem);
+  std::vector<int>& ccnt = P.s_ccnt;
+  ccnt.resize((size_t)nec * nnode);
+  parallel_chunks(nelem, [&](int t, long long e0, long long e1) {
+    int* c = ccnt.data() + (size_t)t * nnode;
+    std::fill(c, c + nnode, 0);
+    for (long long k = e0 * nnpe; k < e1 * nnpe; ++k) ++c[conn[k]];
+  });
+  parallel_for(nnode, [&](long long lo, long long hi) {
+    for (long long i = lo; i < hi; ++i) {
+      int s = 0;
+      for (int t = 0; t < nec; ++t) {
+        int& c = ccnt[(size_t)t * nnode + i];
+        const int v = c;
+        c = s;
+        s += v;
+      }
+      icnt[i + 1] = s;
+    }
   });
   for (int i = 0; i < nnode; ++i) icnt[i + 1] += icnt[i];
   std::vector<int>& inc = P.s_inc;
   inc.resize(icnt[nnode]);
-  {
-    std::vector<int> fill(icnt.begin(), icnt.end() - 1);
-    parallel_for(nent, [&](long long lo, long long hi) {
-      for (long long k = lo; k < hi; ++k)
-        inc[__atomic_fetch_add(&fill[conn[k]], 1, __ATOMIC_RELAXED)] = (int)(k / nnpe);
-    });
-  }
+  parallel_chunks(nelem, [&](int t, long long e0, long long e1) {
+    int* c = ccnt.data() + (size_t)t * nnode;
+    for (long long k = e0 * nnpe; k < e1 * nnpe; ++k) {
+      const int i = conn[k];
+      inc[icnt[i] + c[i]++] = (int)(k / nnpe);
+    }
+  });
 
   // ---- node graph (two passes: count, then fill) ---------------------
   // Neighbours of node i are deduplicated with a per-thread marker array

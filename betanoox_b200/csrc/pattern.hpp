@@ -93,7 +93,7 @@ struct HostPattern {
   // rebuild writes to resident pages instead of faulting fresh ones in;
   // otherwise the scratch is released when the build ends.
   bool keep_scratch = false;
-  std::vector<int> s_icnt, s_inc, s_color, s_ufree;
+  std::vector<int> s_icnt, s_inc, s_color, s_ufree, s_ccnt;
   std::vector<uint64_t> s_used;
   std::vector<std::vector<int>> s_mark;  // one marker array per build thread
 };
