@@ -19,13 +19,17 @@ static int chunk_count(long long n) {
   return (t_serial || n < 20000 || t <= 1) ? 1 : t;
 }
 
-// body(chunk, lo, hi) over chunk_count(n) contiguous ranges, one thread each.
-static void parallel_chunks(long long n, const std::function<void(int, long long, long long)>& body) {
-  const int t = chunk_count(n);
-  if (t == 1) { body(0, 0, n); return; }
+// body(chunk, lo, hi) over t contiguous ranges of [0, n), one thread each.
+static void parallel_chunks_n(int t, long long n, const std::function<void(int, long long, long long)>& body) {
+  if (t <= 1) { body(0, 0, n); return; }
   std::vector<std::thread> th;
   for (int k = 0; k < t; ++k) th.emplace_back(body, k, n * k / t, n * (k + 1) / t);
   for (auto& x : th) x.join();
+}
+
+// body(chunk, lo, hi) over chunk_count(n) contiguous ranges, one thread each.
+static void parallel_chunks(long long n, const std::function<void(int, long long, long long)>& body) {
+  parallel_chunks_n(chunk_count(n), n, body);
 }
 
 static void parallel_for(long long n, const std::function<void(long long, long long)>& body) {
@@ -126,13 +130,15 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   // A counting sort by node with one count array per element chunk (no
   // atomics): chunk t counts its entries per node, the counts become
   // per-chunk offsets within each node's list, and chunk t fills its part in
-  // element order, so every node's elements come out ascending.
+  // element order, so every node's elements come out ascending.  The
+  // chunks are at most the mean entries per node, so the count arrays never
+  // outgrow the incidence list itself.
   std::vector<int>& icnt = P.s_icnt;
   icnt.assign(nnode + 1, 0);
-  const int nec = chunk_count(nelem);
+  const int nec = (int)std::max(1LL, std::min<long long>(chunk_count(nelem), (long long)nelem * nnpe / nnode));
   std::vector<int>& ccnt = P.s_ccnt;
   ccnt.resize((size_t)nec * nnode);
-  parallel_chunks(nelem, [&](int t, long long e0, long long e1) {
+  parallel_chunks_n(nec, nelem, [&](int t, long long e0, long long e1) {
     int* c = ccnt.data() + (size_t)t * nnode;
     std::fill(c, c + nnode, 0);
     for (long long k = e0 * nnpe; k < e1 * nnpe; ++k) ++c[conn[k]];
@@ -152,7 +158,7 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   for (int i = 0; i < nnode; ++i) icnt[i + 1] += icnt[i];
   std::vector<int>& inc = P.s_inc;
   inc.resize(icnt[nnode]);
-  parallel_chunks(nelem, [&](int t, long long e0, long long e1) {
+  parallel_chunks_n(nec, nelem, [&](int t, long long e0, long long e1) {
     int* c = ccnt.data() + (size_t)t * nnode;
     for (long long k = e0 * nnpe; k < e1 * nnpe; ++k) {
       const int i = conn[k];
