@@ -843,8 +843,6 @@ int oracle_sys_assemble_mesh(void* h, int kind, int nelem, int nnpe, int ndpn, i
 int oracle_internal_force_hex8(int nelem, const int* conn, const double* xyz,
                                const int* first_dof, const double* params, int order,
                                const unsigned char* restrained, const double* u, double* fint) {
-  int ndof_max = 0;
-  (void)ndof_max;
   double xe[24], ue[24], Fe[24], C36[36];
   int map[24];
   for (int e = 0; e < nelem; ++e) {
