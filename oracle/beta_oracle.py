@@ -461,6 +461,7 @@ class RefMaterial:
         self.lib.ref_cmat_ortho3d.argtypes = [_dp, _dp, C.c_void_p]
         self.lib.ref_cmat_plane_stress.argtypes = [_dp, _dp]
         self.lib.ref_elastic_stress.argtypes = [_dp, _dp, _dp]
+        self.lib.ref_heat_conductivity.argtypes = [_dp, _dp, _dp, _dp]
 
     @staticmethod
     def available():
@@ -487,6 +488,14 @@ class RefMaterial:
         if self.lib.ref_cmat_plane_stress(_f64(np.asarray(m4, dtype=float)[:4]), Cm):
             raise ValueError("PlaneStress::read failed")
         return Cm.reshape(3, 3)
+
+    def heat_conductivity(self, k3, grad):
+        """HeatTransferMaterial read of readConductivity (k11, k22, k33) and
+        calculateFlux at the temperature gradient grad: (k 3 x 3, flux)."""
+        Cm, flux = np.zeros(9), np.zeros(3)
+        if self.lib.ref_heat_conductivity(_f64(k3), _f64(grad), Cm, flux):
+            raise ValueError("HeatTransferMaterial::read failed")
+        return Cm.reshape(3, 3), flux
 
     def elastic_stress(self, m9, strain):
         """ElasticMaterial::calculateStress at zero temperature and moisture."""

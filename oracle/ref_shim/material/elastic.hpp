@@ -21,6 +21,7 @@ class Rotation {
     for (int i = 0; i < 6; ++i) g[i] = l[i];
   }
   void rotate_Cmat_from_local_to_global(const Matrix& local, Matrix& global) const { global = local; }
+  void rotate_3D_2nd_Order_Tensor_from_local_to_global(const Matrix& local, Matrix& global) const { global = local; }
 };
 
 enum { clear = 0, haveS = 1, haveC = 2 };

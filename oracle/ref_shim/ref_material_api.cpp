@@ -1,6 +1,7 @@
 // C entry points over the reference's own matrix.cpp (dense LU inverse),
 // elastic.cpp (ElasticMaterial: readModuli fills the compliance, the
-// stiffness is its inverse) and pStress.cpp (PlaneStress), compiled
+// stiffness is its inverse), pStress.cpp (PlaneStress) and
+// heatTransferMaterial.cpp (readConductivity, the flux), compiled
 // unmodified into oracle/_ref/libbeta_ref_material.so.  Test infrastructure:
 // used only to pin the oracle's constitutive matrices against the
 // reference's code.  The materials read their constants from an input
@@ -12,6 +13,7 @@
 #include <strings.h>
 
 #include "elastic.hpp"
+#include "heatTransferMaterial.hpp"
 #include "pStress.hpp"
 
 int verboseFlag = 0;
@@ -99,6 +101,28 @@ int ref_cmat_plane_stress(const double* m4, double* C9) {
   if (!p.read(&in)) return 1;
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) C9[i * 3 + j] = (*p.cMat)(i, j);
+  return 0;
+}
+
+// HeatTransferMaterial::initialize + read of a readConductivity block
+// (k11, k22, k33): C9 gets its conductivity tensor (row-major 3 x 3) and,
+// for the temperature gradient grad, flux = calculateFlux (-k grad T).
+int ref_heat_conductivity(const double* k3, const double* grad, double* C9, double* flux) {
+  QuietCout q;
+  HeatTransferMaterial mat;
+  mat.initialize();
+  char deck[256];
+  std::snprintf(deck, sizeof deck, "readConductivity\n%.17g %.17g %.17g\nexitHeatTransferMaterial\n", k3[0],
+                k3[1], k3[2]);
+  std::istringstream in(deck);
+  if (!mat.read(&in)) return 1;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) C9[i * 3 + j] = (*mat.cMat)(i, j);
+  InterpAndSolDerivatives id;
+  id.p_u1_x1 = grad[0];
+  id.p_u1_x2 = grad[1];
+  id.p_u1_x3 = grad[2];
+  mat.calculateFlux(flux, &id);
   return 0;
 }
 

@@ -28,7 +28,9 @@ the compiled reference leaf library (``make -C oracle``):
   assembled lower triangle of a small RVE.
 * ``ref_materials.json`` -- constitutive matrices built by the reference's
   own material code (beta/materials/3D/elastic.cpp ElasticMaterial::read of
-  a readModuli block, beta/materials/2D/pStress.cpp PlaneStress::read) and
+  a readModuli block, beta/materials/2D/pStress.cpp PlaneStress::read,
+  beta_ext/diffusion/material/heatTransferMaterial.cpp readConductivity and
+  calculateFlux) and
   inverses by its own Matrix::invert (beta/math/matrix.cpp), compiled
   unmodified into oracle/_ref/libbeta_ref_material.so.
 * ``ref_equations.json`` -- the reference's own global assembly
@@ -268,10 +270,15 @@ def ref_materials():
     for n in (3, 6, 9):
         A = rng.normal(size=(n, n)) + n * np.eye(n)
         inv.append({"A": A.tolist(), "inverse": r.invert(A).tolist()})
-    return {"source": "reference elastic.cpp + pStress.cpp + matrix.cpp compiled unmodified (oracle/_ref)",
+    cond = []
+    for k3, grad in (([2.5, 1.5, 0.7], [0.1, -0.2, 0.3]), ([1.0, 1.0, 1.0], [3.0, 0.5, -1.25])):
+        C9, flux = r.heat_conductivity(k3, grad)
+        cond.append({"k3": k3, "grad": grad, "C": C9.tolist(), "flux": flux.tolist()})
+    return {"source": "reference elastic.cpp + pStress.cpp + heatTransferMaterial.cpp + matrix.cpp compiled "
+                      "unmodified (oracle/_ref)",
             "ortho3d": [{"m9": m, "C": r.cmat_ortho3d(m).tolist()} for m in ortho],
             "plane_stress": [{"m4": m, "C": r.cmat_plane_stress(m).tolist()} for m in pstress],
-            "invert": inv}
+            "invert": inv, "conductivity": cond}
 
 
 

@@ -532,3 +532,20 @@ def test_zero_diagonal_replacement_equals_the_reference(oracle):
     rc, x, st = s.solve(eps=1e-10, maxit=10000)
     assert rc == 0
     np.testing.assert_array_equal(x, np.array(g["x"]))
+
+
+def test_conductivity_equals_the_reference_material(oracle):
+    """HeatTransferMaterial::read of a readConductivity block (the reference's
+    own heatTransferMaterial.cpp, compiled unmodified) builds diag(k11, k22,
+    k33), the tensor the oracle's diffusion elements take from the same three
+    parameters: element matrices from either are bit-identical; its flux is
+    -k grad T."""
+    xyz = _unit_hex((0.9, 1.1, 0.8), 0.04)
+    for case in _load("ref_materials.json")["conductivity"]:
+        C9 = np.array(case["C"])
+        np.testing.assert_array_equal(C9, np.diag(case["k3"]))
+        np.testing.assert_array_equal(np.array(case["flux"]), -(C9 @ np.array(case["grad"])))
+        a = oracle.km_hex8_heat(xyz, case["k3"], 1.3, order=2)
+        b = oracle.km_hex8_heat(xyz, C9, 1.3, order=2)
+        np.testing.assert_array_equal(a[1], b[1])
+        np.testing.assert_array_equal(a[2], b[2])
