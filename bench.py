@@ -779,6 +779,50 @@ def cpu_full_solves(models, tol, budget_s, threads):
     return done, dofs, secs
 
 
+def reference_full_solves(models, tol, budget_s, threads):
+    """Whole systems, in list order until budget_s seconds are spent, solved by
+    the reference's own code (oracle/_ref): element matrices through
+    ElasticityElement3D's B and addToKe, the Equations pattern, addMatrix and
+    its two-thread ParCG solve (stop rule sqrt(r.r/x.x) < tol).  Each system
+    is first solved by the oracle's threaded port, which proves convergence
+    (the reference's solve exits otherwise) and gives the port's time on the
+    same systems.  Returns (systems, dofs, reference seconds, port seconds), or
+    None when oracle/_ref is absent."""
+    from oracle import beta_oracle as bo
+    if not (bo.RefLeaf.available() and bo.RefEquations.available()):
+        return None
+    leaf, req = bo.RefLeaf(), bo.RefEquations()
+    done, dofs, t_ref, t_port = 0, 0, 0.0, 0.0
+    for m in models:
+        t0 = time.perf_counter()
+        s = bo.System(m)
+        s.set_bc(m.restrained, m.prescribed, m.load)
+        s.build_pattern()
+        s.assemble(m.params, m.order)
+        rc, _, _ = s.solve_threaded(s.rhs(), tol, maxit=200000, threads=threads)
+        t_port += time.perf_counter() - t0
+        del s
+        if rc != 0:
+            break
+        # one constitutive matrix per material phase (the reference's material
+        # objects are per group), built before the clock starts
+        rows, inv = np.unique(m.params, axis=0, return_inverse=True)
+        C = np.stack([bo.cmat_ortho3d(r) for r in rows])[np.asarray(inv).reshape(-1)]
+        nd = m.nnpe * m.ndpn
+        maps = (m.first_dof[m.conn][:, :, None] + np.arange(m.ndpn)[None, None, :]).reshape(m.nelem, nd)
+        xe = np.ascontiguousarray(m.xyz[m.conn])
+        t0 = time.perf_counter()
+        Ke = leaf.elastic_hex8_ke(xe, C, m.order)
+        req.assemble(m.ndof, maps, Ke, m.restrained, m.prescribed, m.load, solve=True, eps=tol, maxit=200000,
+                     parcg=True)
+        t_ref += time.perf_counter() - t0
+        done += 1
+        dofs += m.ndof
+        if t_ref + t_port >= budget_s:
+            break
+    return done, dofs, t_ref, t_port
+
+
 def run_batch(args):
     import torch
     from betanoox_b200 import Batch, Solver, _abi, opts
@@ -936,6 +980,38 @@ def run_batch_reference(args):
     ndof_tot = sum(m.ndof for m in models)
     th = os.cpu_count() or 1
     vals, last = [], None
+    ref, rvals, pvals = None, [], []
+    try:
+        for k in range(max(1, args.warmup and 1) + args.steps):
+            ref = reference_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
+            if ref is None or ref[0] == 0:
+                ref = None
+                break
+            if k >= 1:
+                rvals.append(ref[1] / ref[2])
+                pvals.append(ref[1] / ref[3])
+    except OSError as e:  # oracle/_ref present but not loadable on this host
+        print(f"reference code unavailable ({e}); timing the port", file=sys.stderr)
+        ref = None
+    if ref is not None and rvals:
+        n, d, t_ref, t_port = ref
+        v = statistics.median(rvals)
+        return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * ndof_tot / v, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded generator)",
+                "impl": "reference",
+                "config": {"workload": f"{len(models)} two-phase RVE hex8 cubes n~U{{8..40}}, {ndof_tot} dofs total",
+                           "ndof_total": ndof_tot},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": 2, "kind": "reference",
+                                 "sample": f"first {n} RVEs solved whole ({d} dofs, {t_ref:.1f} s) by the "
+                                           f"reference's own code compiled from its sources (oracle/_ref): "
+                                           f"element B/addToKe, Equations pattern + addMatrix, ParCG solve, "
+                                           f"one system at a time",
+                                 "port_all_cores": {"value": statistics.median(pvals), "unit": UNIT, "cores": th,
+                                                    "kind": "port",
+                                                    "sample": f"the same {n} RVEs, FP64 assembly + threaded "
+                                                              f"Jacobi-PCG ({t_port:.1f} s)"}},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     for k in range(max(1, args.warmup and 1) + args.steps):
         n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
         if k >= 1:

@@ -45,3 +45,15 @@ def test_reference_arm_prints_one_json_line():
     assert cb["kind"] in ("reference", "port")
     if cb["kind"] == "reference":
         assert cb["port_all_cores"]["kind"] == "port"
+
+
+def test_reference_full_solves_run_the_reference(oracle):
+    """The batch arm's sampler: whole RVEs solved by the reference's own code
+    after the port, both timed on the same systems."""
+    if not (oracle.RefLeaf.available() and oracle.RefEquations.available()):
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    sys.path.insert(0, ROOT)
+    import bench
+    models = [W.rve_hex8(4, seed=3), W.rve_hex8(5, seed=4)]
+    n, d, t_ref, t_port = bench.reference_full_solves(models, 1e-8, 1e9, 2)
+    assert n == 2 and d == sum(m.ndof for m in models) and t_ref > 0 and t_port > 0
