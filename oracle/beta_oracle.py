@@ -597,6 +597,7 @@ class RefLeaf:
         self.lib.ref_heat_step_terms.argtypes = [I, _dp, _dp, _dp, D, D, D, _dp, _dp]
         self.lib.ref_elastic_point.argtypes = [I, I, _dp, _dp, _dp, C.c_void_p, C.c_void_p, D, _dp, _dp, _dp]
         self.lib.ref_elastic_hex8_ke.argtypes = [I, _dp, _dp, I, _dp]
+        self.lib.ref_heat_hex8_step_terms.argtypes = [I, _dp, _dp, _dp, I, _dp, D, D, D, _dp, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
         self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
                                           C.c_void_p, C.c_void_p]
@@ -712,6 +713,20 @@ class RefLeaf:
         if rc:
             raise ValueError("ref_elastic_hex8_ke: non-positive Jacobian")
         return Ke.reshape(nel, 24, 24)
+
+    def heat_hex8_step_terms(self, xyz, k3, cap, order, u_e, a1, a2, dt):
+        """Per hex8 diffusion element (xyz nel x 8 x 3, k3 nel x 3, cap nel,
+        nodal u_e nel x 8): the reference's K, M (addToKe, addToMe) and step
+        terms (formK_s, formF_s_new) -> (Mbar nel x 8 x 8, F nel x 8)."""
+        xyz = _f64(xyz).reshape(-1, 24)
+        nel = xyz.shape[0]
+        Mb, F = np.zeros(nel * 64), np.zeros(nel * 8)
+        rc = self.lib.ref_heat_hex8_step_terms(nel, xyz.reshape(-1).copy(), _f64(k3).reshape(-1).copy(),
+                                               _f64(cap).reshape(-1).copy(), int(order),
+                                               _f64(u_e).reshape(-1).copy(), float(a1), float(a2), float(dt), Mb, F)
+        if rc:
+            raise ValueError("ref_heat_hex8_step_terms: non-positive Jacobian")
+        return Mb.reshape(nel, 8, 8), F.reshape(nel, 8)
 
     def print_lower(self, path, fmt, row_ptr, col, val):
         """The reference's printMatrixAddressFormat (fmt 1), ...Upper (2) or

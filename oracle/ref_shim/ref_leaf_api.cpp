@@ -322,6 +322,86 @@ int ref_elastic_hex8_ke(int nel, const double* xyz, const double* C36, int order
   return 0;
 }
 
+// The element side of DiffusionModel's step for nel hex8 diffusion elements,
+// as the reference forms it: per element K (addToKe, diagonal conductivity
+// k3) and M (addToMe, capacity cap) over its own HexQuadPoints rule and
+// shapeHex8/derivHex8 with the Jacobian restated as in ref_elastic_hex8_ke,
+// then formK_s (Mbar = (a1 K + M)/dt) and formF_s_new (F = -(a1+a2)/dt K u_s).
+// xyz nel x 8 x 3, k3 nel x 3, cap nel, u_s nel x 8 (the element's nodal
+// values); Mbar nel x 8 x 8 (upper triangles), F nel x 8.  A serial loop.
+int ref_heat_hex8_step_terms(int nel, const double* xyz, const double* k3, const double* cap, int order,
+                             const double* u_s, double a1, double a2, double dt, double* Mbar, double* F) {
+  QuietStdout quiet;
+  double *gx, *gy, *gz, *gw;
+  HexQuadPoints::getQuadraturePointsForHex(order, &gx, &gy, &gz, &gw);
+  const int nip = order * order * order;
+  HeatTransferElement3Dtransient e;
+  Matrix K(8, 8), M(8, 8), Kb(8, 8), c(3, 3);
+  HeatTransferMaterial mat;
+  InterpAndSolDerivatives id(8, 8);
+  id.allocate();
+  id.numberOfInterp = 8;
+  std::vector<double> fe(8), us(8);
+  int dofs[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+  e.material = &mat;
+  e.Ke = &K;
+  e.Me = &M;
+  e.Ke_orig = &Kb;
+  e.Fe = fe.data();
+  e.dofList = dofs;
+  e.numDof = 8;
+  Array<double> ap(2);
+  ap[0] = a1;
+  ap[1] = a2;
+  double S[8], d0[8], d1[8], d2[8];
+  for (int el = 0; el < nel; ++el) {
+    const double* X = xyz + (size_t)el * 24;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) c(i, j) = i == j ? k3[(size_t)el * 3 + i] : 0.0;
+    mat.saturation = cap[el];
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) K(i, j) = M(i, j) = Kb(i, j) = 0.0;
+    for (int ip = 0; ip < nip; ++ip) {
+      shapeHex8(S, gx[ip], gy[ip], gz[ip]);
+      derivHex8(d0, d1, d2, gx[ip], gy[ip], gz[ip]);
+      double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int a = 0; a < 8; ++a)
+        for (int k = 0; k < 3; ++k) {
+          J[0][k] += d0[a] * X[a * 3 + k];
+          J[1][k] += d1[a] * X[a * 3 + k];
+          J[2][k] += d2[a] * X[a * 3 + k];
+        }
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
+                   c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      if (!(det > 0.0)) return 2;
+      const double inv[3][3] = {
+          {c00 / det, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det, (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det},
+          {c01 / det, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det, (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det},
+          {c02 / det, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det, (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det}};
+      for (int a = 0; a < 8; ++a) {
+        id.S[a] = S[a];
+        id.p_S_x1[a] = inv[0][0] * d0[a] + inv[0][1] * d1[a] + inv[0][2] * d2[a];
+        id.p_S_x2[a] = inv[1][0] * d0[a] + inv[1][1] * d1[a] + inv[1][2] * d2[a];
+        id.p_S_x3[a] = inv[2][0] * d0[a] + inv[2][1] * d1[a] + inv[2][2] * d2[a];
+      }
+      e.addToKe(&c, &id, det * gw[ip]);
+      e.addToMe(nullptr, &id, det * gw[ip]);
+    }
+    for (int i = 0; i < 8; ++i) {
+      us[i] = u_s[(size_t)el * 8 + i];
+      fe[i] = 0.0;
+    }
+    e.formK_s(ap, dt);
+    e.formF_s_new(ap, us.data(), nullptr, nullptr, dt);
+    for (int i = 0; i < 8; ++i) {
+      F[(size_t)el * 8 + i] = fe[i];
+      for (int j = 0; j < 8; ++j) Mbar[(size_t)el * 64 + i * 8 + j] = Kb(i, j);
+    }
+  }
+  return 0;
+}
+
 // The element side of one backward-Euler step (DiffusionModel with a1, a2):
 // formK_s gives Mbar = (a1 K + M)/dt, formF_s_new F = -(a1+a2)/dt K u_s, from
 // the element's K and M (upper triangles, n x n row-major) and its nodal u_s.

@@ -57,3 +57,15 @@ def test_reference_full_solves_run_the_reference(oracle):
     models = [W.rve_hex8(4, seed=3), W.rve_hex8(5, seed=4)]
     n, d, t_ref, t_port = bench.reference_full_solves(models, 1e-8, 1e9, 2)
     assert n == 2 and d == sum(m.ndof for m in models) and t_ref > 0 and t_port > 0
+
+
+def test_reference_heat_baseline_runs_the_reference(oracle):
+    """The heat arm's sampler: transient steps by the reference's own element
+    step terms, Equations scatter and solve, after the oracle's step."""
+    if not (oracle.RefLeaf.available() and oracle.RefEquations.available()):
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    sys.path.insert(0, ROOT)
+    import bench
+    args = SimpleNamespace(cpu_heat_nx=8, heat_nz=4, heat_nx=16, dt=1e-3, heat_tol=1e-10)
+    cb = bench.reference_heat_baseline(args, W.heat_slab(16, 16, 4, order=2))
+    assert cb["kind"] == "reference" and cb["value"] > 0 and cb["port_single_thread"]["value"] > 0
