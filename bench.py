@@ -842,9 +842,11 @@ def cpu_full_solves(models, tol, budget_s, threads):
 
 def reference_full_solves(models, tol, budget_s, threads):
     """Whole systems, in list order until budget_s seconds are spent, solved by
-    the reference's own code (oracle/_ref): element matrices through
-    ElasticityElement3D's B and addToKe, the Equations pattern, addMatrix and
-    its two-thread ParCG solve (stop rule sqrt(r.r/x.x) < tol).  Each system
+    the reference's own code (oracle/_ref): element matrices through its
+    elements (ElasticityElement3D / ElasticityElement2D B and addToKe, or
+    HeatTransferElement3Dtransient addToKe for steady diffusion), the
+    Equations pattern, addMatrix and its two-thread ParCG solve (stop rule
+    sqrt(r.r/x.x) < tol).  Each system
     is first solved by the oracle's threaded port, which proves convergence
     (the reference's solve exits otherwise) and gives the port's time on the
     same systems.  Returns (systems, dofs, reference seconds, port seconds), or
@@ -865,15 +867,26 @@ def reference_full_solves(models, tol, budget_s, threads):
         del s
         if rc != 0:
             break
-        # one constitutive matrix per material phase (the reference's material
-        # objects are per group), built before the clock starts
+        # one material matrix per distinct parameter row (the reference's
+        # material objects are per group), built before the clock starts
         rows, inv = np.unique(m.params, axis=0, return_inverse=True)
-        C = np.stack([bo.cmat_ortho3d(r) for r in rows])[np.asarray(inv).reshape(-1)]
+        inv = np.asarray(inv).reshape(-1)
         nd = m.nnpe * m.ndpn
         maps = (m.first_dof[m.conn][:, :, None] + np.arange(m.ndpn)[None, None, :]).reshape(m.nelem, nd)
         xe = np.ascontiguousarray(m.xyz[m.conn])
+        if m.kind == 2:    # hex8 elasticity
+            C = np.stack([bo.cmat_ortho3d(r) for r in rows])[inv]
+            element = lambda: leaf.elastic_hex8_ke(xe, C, m.order)  # noqa: E731
+        elif m.kind == 1:  # quad4 plane stress
+            C = np.stack([bo.cmat_plane_stress(r[:4]) for r in rows])[inv]
+            element = lambda: leaf.elastic_quad4_ke(xe, C, m.order)  # noqa: E731
+        elif m.kind == 3:  # hex8 diffusion, steady
+            k3 = np.ascontiguousarray(m.params[:, :3])
+            element = lambda: leaf.heat_hex8_k(xe, k3, m.order)  # noqa: E731
+        else:
+            break
         t0 = time.perf_counter()
-        Ke = leaf.elastic_hex8_ke(xe, C, m.order)
+        Ke = element()
         req.assemble(m.ndof, maps, Ke, m.restrained, m.prescribed, m.load, solve=True, eps=tol, maxit=200000,
                      parcg=True)
         t_ref += time.perf_counter() - t0
@@ -1249,6 +1262,34 @@ def run_serve_reference(args):
     models = [W.serve_request(args.seed, j) for j in range(pool_n)]
     th = os.cpu_count() or 1
     vals, last = [], None
+    ref, rvals, pvals = None, [], []
+    try:
+        for k in range(1 + args.steps):
+            ref = reference_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
+            if ref is None or ref[0] == 0:
+                ref = None
+                break
+            if k >= 1:
+                rvals.append(ref[1] / ref[2])
+                pvals.append(ref[1] / ref[3])
+    except OSError as e:  # oracle/_ref present but not loadable on this host
+        print(f"reference code unavailable ({e}); timing the port", file=sys.stderr)
+        ref = None
+    if ref is not None and rvals:
+        n, d, t_ref, t_port = ref
+        v = statistics.median(rvals)
+        return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * d / v, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
+                "config": {"workload": f"stream of {args.requests} requests (quad4 / hex8 elasticity / hex8 "
+                                       f"diffusion, log-uniform 1e3-5e5 dofs), solved one at a time"},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": 2, "kind": "reference",
+                                 "sample": f"first {n} requests solved whole per step ({d} dofs, {t_ref:.1f} s) by "
+                                           f"the reference's own code compiled from its sources (oracle/_ref): "
+                                           f"its elements, Equations pattern + addMatrix, ParCG solve",
+                                 "port_all_cores": {"value": statistics.median(pvals), "unit": UNIT, "cores": th,
+                                                    "kind": "port", "sample": f"the same {n} requests ({t_port:.1f} s)"}},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     for k in range(1 + args.steps):
         n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
         if k >= 1:

@@ -598,6 +598,8 @@ class RefLeaf:
         self.lib.ref_elastic_point.argtypes = [I, I, _dp, _dp, _dp, C.c_void_p, C.c_void_p, D, _dp, _dp, _dp]
         self.lib.ref_elastic_hex8_ke.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_heat_hex8_step_terms.argtypes = [I, _dp, _dp, _dp, I, _dp, D, D, D, _dp, _dp]
+        self.lib.ref_elastic_quad4_ke.argtypes = [I, _dp, _dp, I, _dp]
+        self.lib.ref_heat_hex8_k.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
         self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
                                           C.c_void_p, C.c_void_p]
@@ -713,6 +715,26 @@ class RefLeaf:
         if rc:
             raise ValueError("ref_elastic_hex8_ke: non-positive Jacobian")
         return Ke.reshape(nel, 24, 24)
+
+    def elastic_quad4_ke(self, xy, C9, order):
+        """Quad4 plane stiffness (nel x 8 x 8 upper triangles) through the
+        reference's Gauss rule, shape functions and ElasticityElement2D."""
+        xy = _f64(xy).reshape(-1, 8)
+        nel = xy.shape[0]
+        Ke = np.zeros(nel * 64)
+        if self.lib.ref_elastic_quad4_ke(nel, xy.reshape(-1).copy(), _f64(C9).reshape(-1).copy(), int(order), Ke):
+            raise ValueError("ref_elastic_quad4_ke: non-positive Jacobian")
+        return Ke.reshape(nel, 8, 8)
+
+    def heat_hex8_k(self, xyz, k3, order):
+        """Hex8 conductivity matrices (nel x 8 x 8 upper triangles) through the
+        reference's HeatTransferElement3Dtransient::addToKe."""
+        xyz = _f64(xyz).reshape(-1, 24)
+        nel = xyz.shape[0]
+        K = np.zeros(nel * 64)
+        if self.lib.ref_heat_hex8_k(nel, xyz.reshape(-1).copy(), _f64(k3).reshape(-1).copy(), int(order), K):
+            raise ValueError("ref_heat_hex8_k: non-positive Jacobian")
+        return K.reshape(nel, 8, 8)
 
     def heat_hex8_step_terms(self, xyz, k3, cap, order, u_e, a1, a2, dt):
         """Per hex8 diffusion element (xyz nel x 8 x 3, k3 nel x 3, cap nel,

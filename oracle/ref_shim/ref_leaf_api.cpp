@@ -76,6 +76,61 @@ struct QuietStdout {
   }
 };
 
+// Shape functions and global gradients of a hex8 at one of the reference's
+// Gauss points (shapeHex8 / derivHex8), with the Jacobian J (rows d/dxi,
+// d/deta, d/dzeta of the coordinates X, 8 x 3), its determinant and inverse
+// by cofactors -- IsoElement::jacobian (isoElement.cpp:250-389) restated,
+// that file does not compile here.  Returns det J (<= 0: a bad element).
+double hex8_point(const double* X, double xi, double eta, double zeta, InterpAndSolDerivatives& id) {
+  double S[8], d0[8], d1[8], d2[8];
+  shapeHex8(S, xi, eta, zeta);
+  derivHex8(d0, d1, d2, xi, eta, zeta);
+  double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int a = 0; a < 8; ++a)
+    for (int k = 0; k < 3; ++k) {
+      J[0][k] += d0[a] * X[a * 3 + k];
+      J[1][k] += d1[a] * X[a * 3 + k];
+      J[2][k] += d2[a] * X[a * 3 + k];
+    }
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
+               c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  if (!(det > 0.0)) return det;
+  const double inv[3][3] = {
+      {c00 / det, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det, (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det},
+      {c01 / det, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det, (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det},
+      {c02 / det, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det, (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det}};
+  for (int a = 0; a < 8; ++a) {
+    id.S[a] = S[a];
+    id.p_S_x1[a] = inv[0][0] * d0[a] + inv[0][1] * d1[a] + inv[0][2] * d2[a];
+    id.p_S_x2[a] = inv[1][0] * d0[a] + inv[1][1] * d1[a] + inv[1][2] * d2[a];
+    id.p_S_x3[a] = inv[2][0] * d0[a] + inv[2][1] * d1[a] + inv[2][2] * d2[a];
+  }
+  return det;
+}
+
+// The same for a quad4 (shapeQuad4 / derivQuad4, 2 x 2 Jacobian).
+double quad4_point(const double* X, double xi, double eta, InterpAndSolDerivatives& id) {
+  double S[4], d0[4], d1[4];
+  shapeQuad4(S, xi, eta);
+  derivQuad4(d0, d1, xi, eta);
+  double J[2][2] = {{0, 0}, {0, 0}};
+  for (int a = 0; a < 4; ++a)
+    for (int k = 0; k < 2; ++k) {
+      J[0][k] += d0[a] * X[a * 2 + k];
+      J[1][k] += d1[a] * X[a * 2 + k];
+    }
+  const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  if (!(det > 0.0)) return det;
+  const double i00 = J[1][1] / det, i01 = -J[0][1] / det, i10 = -J[1][0] / det, i11 = J[0][0] / det;
+  for (int a = 0; a < 4; ++a) {
+    id.S[a] = S[a];
+    id.p_S_x1[a] = i00 * d0[a] + i01 * d1[a];
+    id.p_S_x2[a] = i10 * d0[a] + i11 * d1[a];
+  }
+  return det;
+}
+
 // One integration point of the reference's own elasticity element E
 // (ElasticityElement3D or ElasticityElement2D): calculateBmatrix + addToKe
 // into Ke (ndof x ndof row-major, upper triangle) and, when u is given,
@@ -281,7 +336,7 @@ int ref_elastic_hex8_ke(int nel, const double* xyz, const double* C36, int order
   e.b = rows;
   e.Ke = &K;
   e.numDof = 24;
-  double S[8], d0[8], d1[8], d2[8], stress[6] = {0, 0, 0, 0, 0, 0};
+  double stress[6] = {0, 0, 0, 0, 0, 0};
   for (int el = 0; el < nel; ++el) {
     const double* X = xyz + (size_t)el * 24;
     for (int i = 0; i < 6; ++i)
@@ -289,35 +344,87 @@ int ref_elastic_hex8_ke(int nel, const double* xyz, const double* C36, int order
     for (int i = 0; i < 24; ++i)
       for (int j = 0; j < 24; ++j) K(i, j) = 0.0;
     for (int ip = 0; ip < nip; ++ip) {
-      shapeHex8(S, gx[ip], gy[ip], gz[ip]);
-      derivHex8(d0, d1, d2, gx[ip], gy[ip], gz[ip]);
-      double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-      for (int a = 0; a < 8; ++a)
-        for (int k = 0; k < 3; ++k) {
-          J[0][k] += d0[a] * X[a * 3 + k];
-          J[1][k] += d1[a] * X[a * 3 + k];
-          J[2][k] += d2[a] * X[a * 3 + k];
-        }
-      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
-                   c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-      const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      const double det = hex8_point(X, gx[ip], gy[ip], gz[ip], id);
       if (!(det > 0.0)) return 2;
-      const double inv[3][3] = {
-          {c00 / det, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det, (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det},
-          {c01 / det, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det, (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det},
-          {c02 / det, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det, (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det}};
-      for (int a = 0; a < 8; ++a) {
-        id.S[a] = S[a];
-        id.p_S_x1[a] = inv[0][0] * d0[a] + inv[0][1] * d1[a] + inv[0][2] * d2[a];
-        id.p_S_x2[a] = inv[1][0] * d0[a] + inv[1][1] * d1[a] + inv[1][2] * d2[a];
-        id.p_S_x3[a] = inv[2][0] * d0[a] + inv[2][1] * d1[a] + inv[2][2] * d2[a];
-      }
       e.calculateBmatrix(&id, rows);
       e.addToKe(&c, &id, det * gw[ip], stress);
     }
     double* out = Ke + (size_t)el * 576;
     for (int i = 0; i < 24; ++i)
       for (int j = 0; j < 24; ++j) out[i * 24 + j] = K(i, j);
+  }
+  return 0;
+}
+
+// Quad4 plane stiffness of nel elements the way the reference forms it: its
+// QuadQuadPoints rule, shapeQuad4/derivQuad4, the 2 x 2 Jacobian restated,
+// then ElasticityElement2D::calculateBmatrix + addToKe.  xy nel x 4 x 2, C9
+// nel x 3 x 3, Ke nel x 8 x 8 (upper triangles).  A serial loop.
+int ref_elastic_quad4_ke(int nel, const double* xy, const double* C9, int order, double* Ke) {
+  QuietStdout quiet;
+  double *gx, *gy, *gw;
+  QuadQuadPoints::getQuadraturePointsForQuad(order, &gx, &gy, &gw);
+  const int nip = order * order;
+  ElasticityElement2D e;
+  std::vector<double> brows(6 * 8, 0.0);
+  double* rows[6];
+  for (int r = 0; r < 6; ++r) rows[r] = brows.data() + r * 8;
+  Matrix K(8, 8), c(3, 3);
+  InterpAndSolDerivatives id(4, 4);
+  id.allocate();
+  id.numberOfInterp = 4;
+  e.b = rows;
+  e.Ke = &K;
+  e.numDof = 8;
+  double stress[6] = {0, 0, 0, 0, 0, 0};
+  for (int el = 0; el < nel; ++el) {
+    const double* X = xy + (size_t)el * 8;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) c(i, j) = C9[(size_t)el * 9 + i * 3 + j];
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) K(i, j) = 0.0;
+    for (int ip = 0; ip < nip; ++ip) {
+      const double det = quad4_point(X, gx[ip], gy[ip], id);
+      if (!(det > 0.0)) return 2;
+      e.calculateBmatrix(&id, rows);
+      e.addToKe(&c, &id, det * gw[ip], stress);
+    }
+    double* out = Ke + (size_t)el * 64;
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) out[i * 8 + j] = K(i, j);
+  }
+  return 0;
+}
+
+// Hex8 diffusion conductivity of nel elements (steady analyses): addToKe of
+// HeatTransferElement3Dtransient with the diagonal conductivity k3 over the
+// reference's Gauss rule.  K nel x 8 x 8 (upper triangles).  A serial loop.
+int ref_heat_hex8_k(int nel, const double* xyz, const double* k3, int order, double* Kout) {
+  QuietStdout quiet;
+  double *gx, *gy, *gz, *gw;
+  HexQuadPoints::getQuadraturePointsForHex(order, &gx, &gy, &gz, &gw);
+  const int nip = order * order * order;
+  HeatTransferElement3Dtransient e;
+  Matrix K(8, 8), c(3, 3);
+  InterpAndSolDerivatives id(8, 8);
+  id.allocate();
+  id.numberOfInterp = 8;
+  e.Ke = &K;
+  e.numDof = 8;
+  for (int el = 0; el < nel; ++el) {
+    const double* X = xyz + (size_t)el * 24;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) c(i, j) = i == j ? k3[(size_t)el * 3 + i] : 0.0;
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) K(i, j) = 0.0;
+    for (int ip = 0; ip < nip; ++ip) {
+      const double det = hex8_point(X, gx[ip], gy[ip], gz[ip], id);
+      if (!(det > 0.0)) return 2;
+      e.addToKe(&c, &id, det * gw[ip]);
+    }
+    double* out = Kout + (size_t)el * 64;
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) out[i * 8 + j] = K(i, j);
   }
   return 0;
 }
@@ -353,7 +460,6 @@ int ref_heat_hex8_step_terms(int nel, const double* xyz, const double* k3, const
   Array<double> ap(2);
   ap[0] = a1;
   ap[1] = a2;
-  double S[8], d0[8], d1[8], d2[8];
   for (int el = 0; el < nel; ++el) {
     const double* X = xyz + (size_t)el * 24;
     for (int i = 0; i < 3; ++i)
@@ -362,29 +468,8 @@ int ref_heat_hex8_step_terms(int nel, const double* xyz, const double* k3, const
     for (int i = 0; i < 8; ++i)
       for (int j = 0; j < 8; ++j) K(i, j) = M(i, j) = Kb(i, j) = 0.0;
     for (int ip = 0; ip < nip; ++ip) {
-      shapeHex8(S, gx[ip], gy[ip], gz[ip]);
-      derivHex8(d0, d1, d2, gx[ip], gy[ip], gz[ip]);
-      double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-      for (int a = 0; a < 8; ++a)
-        for (int k = 0; k < 3; ++k) {
-          J[0][k] += d0[a] * X[a * 3 + k];
-          J[1][k] += d1[a] * X[a * 3 + k];
-          J[2][k] += d2[a] * X[a * 3 + k];
-        }
-      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
-                   c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-      const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      const double det = hex8_point(X, gx[ip], gy[ip], gz[ip], id);
       if (!(det > 0.0)) return 2;
-      const double inv[3][3] = {
-          {c00 / det, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det, (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det},
-          {c01 / det, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det, (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det},
-          {c02 / det, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det, (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det}};
-      for (int a = 0; a < 8; ++a) {
-        id.S[a] = S[a];
-        id.p_S_x1[a] = inv[0][0] * d0[a] + inv[0][1] * d1[a] + inv[0][2] * d2[a];
-        id.p_S_x2[a] = inv[1][0] * d0[a] + inv[1][1] * d1[a] + inv[1][2] * d2[a];
-        id.p_S_x3[a] = inv[2][0] * d0[a] + inv[2][1] * d1[a] + inv[2][2] * d2[a];
-      }
       e.addToKe(&c, &id, det * gw[ip]);
       e.addToMe(nullptr, &id, det * gw[ip]);
     }

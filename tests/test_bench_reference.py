@@ -69,3 +69,22 @@ def test_reference_heat_baseline_runs_the_reference(oracle):
     args = SimpleNamespace(cpu_heat_nx=8, heat_nz=4, heat_nx=16, dt=1e-3, heat_tol=1e-10)
     cb = bench.reference_heat_baseline(args, W.heat_slab(16, 16, 4, order=2))
     assert cb["kind"] == "reference" and cb["value"] > 0 and cb["port_single_thread"]["value"] > 0
+
+
+def test_reference_full_solves_cover_the_serve_kinds(oracle):
+    """The sampler on one small request of each serving kind (quad4 plane
+    stress, hex8 elasticity, hex8 steady diffusion)."""
+    if not (oracle.RefLeaf.available() and oracle.RefEquations.available()):
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    sys.path.insert(0, ROOT)
+    import bench
+    picked = {}
+    for j in range(60):
+        m = W.serve_request(11, j, dof_lo=300.0, dof_hi=3000.0)
+        picked.setdefault(m.kind, m)
+        if len(picked) == 3:
+            break
+    assert sorted(picked) == [1, 2, 3]
+    models = list(picked.values())
+    n, d, t_ref, t_port = bench.reference_full_solves(models, 1e-8, 1e9, 2)
+    assert n == 3 and d == sum(m.ndof for m in models)
