@@ -599,6 +599,8 @@ class RefLeaf:
         self.lib.ref_elastic_hex8_ke.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_heat_hex8_step_terms.argtypes = [I, _dp, _dp, _dp, I, _dp, D, D, D, _dp, _dp]
         self.lib.ref_elastic_quad4_ke.argtypes = [I, _dp, _dp, I, _dp]
+        self.lib.ref_elastic_update.argtypes = [I, I, _dp, _dp, I, C.c_void_p, C.c_char_p, _dp, _dp, _dp]
+        self.lib.ref_elastic_vol_avg.argtypes = [I, I, _dp, _dp, I, _dp, _dp]
         self.lib.ref_heat_hex8_k.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
         self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
@@ -715,6 +717,32 @@ class RefLeaf:
         if rc:
             raise ValueError("ref_elastic_hex8_ke: non-positive Jacobian")
         return Ke.reshape(nel, 24, 24)
+
+    def elastic_update(self, X, C_mat, order, action, u=None):
+        """The reference's own element driver update(action, u) of
+        ElasticityElement3D (X: 8 x 3) or ElasticityElement2D (X: 4 x 2):
+        (Ke upper triangle, Fe, integrals of strain, stress, energy (6 each))."""
+        X = _f64(X)
+        dim, nnode = X.shape[1], X.shape[0]
+        n = dim * nnode
+        Ke, Fe, sums = np.zeros(n * n), np.zeros(n), np.zeros(18)
+        uv = None if u is None else _f64(u).reshape(-1).copy()
+        rc = self.lib.ref_elastic_update(dim, nnode, X.reshape(-1).copy(), _f64(C_mat).reshape(-1).copy(), int(order),
+                                         None if uv is None else uv.ctypes.data, action.encode(), Ke, Fe, sums)
+        if rc:
+            raise ValueError("ref_elastic_update refused the element")
+        return Ke.reshape(n, n), Fe, sums.reshape(3, 6)
+
+    def elastic_vol_avg(self, X, C_mat, order, u):
+        """getVolAvgValues: [volume, stress integral (6), strain integral (6),
+        SED (3)]."""
+        X = _f64(X)
+        out = np.zeros(16)
+        rc = self.lib.ref_elastic_vol_avg(X.shape[1], X.shape[0], X.reshape(-1).copy(), _f64(C_mat).reshape(-1).copy(),
+                                          int(order), _f64(u).reshape(-1).copy(), out)
+        if rc:
+            raise ValueError("ref_elastic_vol_avg refused the element")
+        return out
 
     def elastic_quad4_ke(self, xy, C9, order):
         """Quad4 plane stiffness (nel x 8 x 8 upper triangles) through the

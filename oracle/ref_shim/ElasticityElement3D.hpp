@@ -1,6 +1,9 @@
 // Shim: ElasticityElement3D (and the elastic material it calls) as
 // ElasticityElement3D.cpp defines and uses them (the reference ships no
 // headers): the member functions that file defines and the members it reads.
+// The members ElasticityElement2D specialises are virtual, so that the 3D
+// element's driver (update, loopOverIntegrationPoints) reaches the plane
+// element's versions.
 #pragma once
 #include "element_shim_common.hpp"
 
@@ -36,9 +39,9 @@ class ElasticityElement3D : public IsoElement {
   ElasticityElement3D(void);
   ~ElasticityElement3D(void);
   void addToFe(int numDof, int numStrains, double** b, double* stress, double integrationFactor, double* force);
-  void calculateBmatrix(InterpAndSolDerivatives* id_ptr, double** b);
-  void calculateStrain(InterpAndSolDerivatives* id_ptr, double* strain);
-  void derivativesOfFields(InterpAndSolDerivatives* id_ptr);
+  virtual void calculateBmatrix(InterpAndSolDerivatives* id_ptr, double** b);
+  virtual void calculateStrain(InterpAndSolDerivatives* id_ptr, double* strain);
+  virtual void derivativesOfFields(InterpAndSolDerivatives* id_ptr);
   void printNodalStressesInLCS(std::ostream& stressout);
   void printNodalStressesInGCS(std::ostream& stressout);
   void printNodalStrainsInLCS(std::ostream& strainout);
@@ -46,8 +49,8 @@ class ElasticityElement3D : public IsoElement {
   void printQuadStrains(int totalNumIPs, std::ostream& SO);
   void printQuadStresses(int totalNumIPs, std::ostream& SO);
   void printNodalForcesByElement(std::ostream& forcesout);
-  void getVolAvgValues(double* uGlobal, double* volAvgStress, double* volAvgStrain, double* SED, double* volume);
-  void addToKe(Matrix* cMat, InterpAndSolDerivatives* id_ptr, double integrationFactor, double* stress);
+  virtual void getVolAvgValues(double* uGlobal, double* volAvgStress, double* volAvgStrain, double* SED, double* volume);
+  virtual void addToKe(Matrix* cMat, InterpAndSolDerivatives* id_ptr, double integrationFactor, double* stress);
   void initializeArrays();
   bool geometryCheck();
   void setPointers(ElementWorkspace* s);

@@ -15,6 +15,8 @@
 #include <string>
 #include <vector>
 
+#include "hexQuadPoint.hpp"
+#include "quadQuadPoint.hpp"
 #include "utility/excepts.hpp"
 #include "utility/utility_defines.h"
 
@@ -84,6 +86,7 @@ class Matrix {
 
 struct GaussPointList {
   int totalNumIPs = 0;
+  double *xiList = nullptr, *etaList = nullptr, *zetaList = nullptr;
   double* weightList = nullptr;
 };
 
@@ -188,18 +191,105 @@ class BasicElement {
   ElementWorkspace* bag = nullptr;
 };
 
+// The reference's own Gauss rules and shape functions (gauss.cpp, shape.cpp,
+// compiled into the same library).
+void shapeHex8(double* S, double xi, double eta, double zeta);
+void derivHex8(double* Sxi, double* Seta, double* Szeta, double xi, double eta, double zeta);
+void shapeQuad4(double* S, double zeta, double eta);
+void derivQuad4(double* Szeta, double* Seta, double zeta, double eta);
+
+// IsoElement's services, written for this build because isoElement.cpp and
+// BasicElement.cpp do not compile here: the reference's tensor Gauss rules
+// and shape functions for hex8 / quad4 (numberOfIntegrationDirections 3 /
+// 2), the Jacobian, its determinant and the global shape-function gradients
+// at a point (the algebra of IsoElement::jacobian, isoElement.cpp:250-389),
+// and the element's nodal coordinates and solution from tables a test
+// attaches (coords: nnpe x 3; edofs: nnpe x dofs-per-node global numbers).
+// Orientation is the identity.
 class IsoElement : public BasicElement {
  public:
   void readSpecialCommand(std::istream&, ElementGroup*, int, char*) {}
-  void interpolation(int, GaussPointList&, InterpAndSolDerivatives*) {}
-  void jacobian(InterpAndSolDerivatives*) {}
+  void getQuadraturePoints(GaussPointList& g) {
+    if (numberOfIntegrationDirections == 3) {
+      HexQuadPoints::getQuadraturePointsForHex(integrationOrder, &g.xiList, &g.etaList, &g.zetaList, &g.weightList);
+      g.totalNumIPs = integrationOrder * integrationOrder * integrationOrder;
+    } else {
+      QuadQuadPoints::getQuadraturePointsForQuad(integrationOrder, &g.xiList, &g.etaList, &g.weightList);
+      g.totalNumIPs = integrationOrder * integrationOrder;
+    }
+  }
+  void interpolation(int ip, GaussPointList& g, InterpAndSolDerivatives* id) {
+    id->numberOfInterp = numNodesPerElement;
+    if (numberOfIntegrationDirections == 3) {
+      shapeHex8(id->S, g.xiList[ip], g.etaList[ip], g.zetaList[ip]);
+      derivHex8(id->p_S_Lx1, id->p_S_Lx2, id->p_S_Lx3, g.xiList[ip], g.etaList[ip], g.zetaList[ip]);
+    } else {
+      shapeQuad4(id->S, g.xiList[ip], g.etaList[ip]);
+      derivQuad4(id->p_S_Lx1, id->p_S_Lx2, g.xiList[ip], g.etaList[ip]);
+    }
+  }
+  void jacobian(InterpAndSolDerivatives* id) {
+    const int n = id->numberOfInterp;
+    const double *L1 = id->p_S_Lx1, *L2 = id->p_S_Lx2, *L3 = id->p_S_Lx3;
+    const double *x = id->xCoor, *y = id->yCoor, *z = id->zCoor;
+    if (numberOfIntegrationDirections == 3) {
+      double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int a = 0; a < n; ++a) {
+        const double L[3] = {L1[a], L2[a], L3[a]};
+        for (int r = 0; r < 3; ++r) {
+          J[r][0] += L[r] * x[a];
+          J[r][1] += L[r] * y[a];
+          J[r][2] += L[r] * z[a];
+        }
+      }
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
+                   c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      id->detJ = det;
+      const double inv[3][3] = {
+          {c00 / det, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det, (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det},
+          {c01 / det, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det, (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det},
+          {c02 / det, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det, (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det}};
+      for (int a = 0; a < n; ++a) {
+        id->p_S_x1[a] = inv[0][0] * L1[a] + inv[0][1] * L2[a] + inv[0][2] * L3[a];
+        id->p_S_x2[a] = inv[1][0] * L1[a] + inv[1][1] * L2[a] + inv[1][2] * L3[a];
+        id->p_S_x3[a] = inv[2][0] * L1[a] + inv[2][1] * L2[a] + inv[2][2] * L3[a];
+      }
+    } else {
+      double J[2][2] = {{0, 0}, {0, 0}};
+      for (int a = 0; a < n; ++a) {
+        J[0][0] += L1[a] * x[a];
+        J[0][1] += L1[a] * y[a];
+        J[1][0] += L2[a] * x[a];
+        J[1][1] += L2[a] * y[a];
+      }
+      const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+      id->detJ = det;
+      for (int a = 0; a < n; ++a) {
+        id->p_S_x1[a] = (J[1][1] * L1[a] - J[0][1] * L2[a]) / det;
+        id->p_S_x2[a] = (-J[1][0] * L1[a] + J[0][0] * L2[a]) / det;
+      }
+    }
+  }
   double getIntegrationFactor() { return 1.0; }
   void calculateElementVolume(IntegrationDataType&) {}
-  void extractNodalCoordinates(double*, double*, double*) {}
-  void extractSolution(double*, double**) {}
-  void getQuadraturePoints(GaussPointList&) {}
+  void extractNodalCoordinates(double* x, double* y, double* z) {
+    for (int a = 0; a < numNodesPerElement; ++a) {
+      x[a] = coords[a * 3];
+      y[a] = coords[a * 3 + 1];
+      z[a] = coords[a * 3 + 2];
+    }
+  }
+  void extractSolution(double* u, double** d) {
+    const int nd = numDof / numNodesPerElement;
+    for (int a = 0; a < numNodesPerElement; ++a)
+      for (int c = 0; c < nd; ++c) d[c][a] = u[edofs[a * nd + c]];
+  }
   void AllocateRotations() {}
   void extrapolateQuadValuesToNodes(double**, int, double**) {}
-  Rotation* OrientationAtIP = nullptr;
+  const double* coords = nullptr;
+  const int* edofs = nullptr;
+  Rotation own_rotation;
+  Rotation* OrientationAtIP = &own_rotation;
   void* ElementNodeRotations = nullptr;
 };

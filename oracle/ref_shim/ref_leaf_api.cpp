@@ -184,9 +184,126 @@ int elastic_point(int dim, int nnode, const double* C, const double* dx, const d
   }
   return 0;
 }
+// The ElementWorkspace arrays an elasticity element with nip points reads and
+// writes: per point stresses, strains and their rotated copies; per element
+// and total strain, stress, energy and local-stress integrals.
+struct ElasticBag {
+  ElementWorkspace w;
+  std::vector<double> pts, sums;
+  std::vector<double*> rows;
+  explicit ElasticBag(int nip) : pts((size_t)4 * nip * 6, 0.0), sums(8 * 6, 0.0), rows((size_t)4 * nip) {
+    for (int k = 0; k < 4 * nip; ++k) rows[k] = pts.data() + (size_t)k * 6;
+    w.quadPointStresses = rows.data();
+    w.quadPointStrains = rows.data() + nip;
+    w.rotatedStresses = rows.data() + 2 * nip;
+    w.rotatedStrains = rows.data() + 3 * nip;
+    double* t = sums.data();
+    w.strainVolume_element = t;
+    w.stressVolume_element = t + 6;
+    w.energyVolume_element = t + 12;
+    w.localStressVolume_element = t + 18;
+    w.strainVolume_total = t + 24;
+    w.stressVolume_total = t + 30;
+    w.energyVolume_total = t + 36;
+    w.localStressVolume_total = t + 42;
+  }
+};
+
+// One elasticity element E (ElasticityElement3D or ElasticityElement2D) set up
+// as the reference's model would hand it over: nnode nodes at X (nnode x dim),
+// local dof numbers 0..ndof-1, the constitutive matrix C, the integration
+// order, its workspace, stiffness and force buffers.  run(e) then calls the
+// reference's own member functions on it.
+template <class E, class F>
+int with_elastic(int dim, int nnode, const double* X, const double* C, int order, F run) {
+  QuietStdout quiet;
+  E e;
+  const int ndof = dim * nnode, ns = e.numStrains;
+  if (ndof > (dim == 3 ? 96 : 36)) return 1;
+  const int nip = dim == 3 ? order * order * order : order * order;
+  e.numNodesPerElement = nnode;
+  e.numDof = ndof;
+  e.setIntegrationOrder(order);
+  std::vector<double> coords((size_t)nnode * 3, 0.0);
+  for (int a = 0; a < nnode; ++a)
+    for (int k = 0; k < dim; ++k) coords[a * 3 + k] = X[a * dim + k];
+  std::vector<int> dofs(ndof);
+  for (int i = 0; i < ndof; ++i) dofs[i] = i;
+  e.coords = coords.data();
+  e.edofs = dofs.data();
+  std::vector<double> brows((size_t)6 * ndof, 0.0);
+  double* rows[6];
+  for (int r = 0; r < 6; ++r) rows[r] = brows.data() + (size_t)r * ndof;
+  ElasticBag bag(nip);
+  bag.w.b = rows;
+  e.setPointers(&bag.w);
+  Matrix K(ndof, ndof);
+  std::vector<double> fe(ndof, 0.0), ife(ndof, 0.0);
+  e.Ke = &K;
+  e.Fe = fe.data();
+  e.initialFe = ife.data();
+  ElasticMaterial mat;
+  mat.numStrains = ns;
+  mat.cmat = Matrix(ns, ns);
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j < ns; ++j) mat.cmat(i, j) = C[i * ns + j];
+  e.material = &mat;
+  e.isv.assign(nip, nullptr);
+  return run(e, K, fe, bag);
+}
 }  // namespace
 
 extern "C" {
+// The reference's own element driver: ElasticityElement3D (dim 3, hex8) or
+// ElasticityElement2D (dim 2, quad4) update(action, u) -> its
+// loopOverIntegrationPoints and processActionCode ("K" stiffness, "F"
+// internal force with the stresses it needs, "S" stresses), over the
+// reference's Gauss rule.  u (element dofs, interleaved) may be null.  Ke
+// (ndof x ndof, upper triangle), Fe (ndof) and sums (18: the element's
+// strain, stress and energy integrals, 6 each, as loopOverIntegrationPoints
+// adds them to the workspace totals).
+int ref_elastic_update(int dim, int nnode, const double* X, const double* C, int order, const double* u,
+                       const char* action, double* Ke, double* Fe, double* sums) {
+  auto run = [&](auto& e, Matrix& K, std::vector<double>& fe, ElasticBag& bag) {
+    std::vector<double> uu;
+    if (u) uu.assign(u, u + e.numDof);
+    std::string act(action);
+    e.update(&act[0], u ? uu.data() : nullptr);
+    const int n = e.numDof;
+    for (int i = 0; i < n; ++i) {
+      Fe[i] = fe[i];
+      for (int j = 0; j < n; ++j) Ke[i * n + j] = K(i, j);
+    }
+    for (int k = 0; k < 18; ++k) sums[k] = bag.sums[24 + k];
+    return 0;
+  };
+  if (dim == 3) return with_elastic<ElasticityElement3D>(3, nnode, X, C, order, run);
+  if (dim == 2) return with_elastic<ElasticityElement2D>(2, nnode, X, C, order, run);
+  return 1;
+}
+
+// ElasticityElement3D / ElasticityElement2D::getVolAvgValues, the reference's
+// post-solve element outputs: out = [volume, stress integral (6), strain
+// integral (6), SED (3)] for the element's displacement u (element dofs).
+int ref_elastic_vol_avg(int dim, int nnode, const double* X, const double* C, int order, const double* u,
+                        double* out) {
+  auto run = [&](auto& e, Matrix&, std::vector<double>&, ElasticBag&) {
+    std::vector<double> uu(u, u + e.numDof);
+    double stress[6] = {0, 0, 0, 0, 0, 0}, strain[6] = {0, 0, 0, 0, 0, 0}, sed[3] = {0, 0, 0}, vol = 0.0;
+    e.getVolAvgValues(uu.data(), stress, strain, sed, &vol);
+    out[0] = vol;
+    for (int k = 0; k < 6; ++k) {
+      out[1 + k] = stress[k];
+      out[7 + k] = strain[k];
+    }
+    for (int k = 0; k < 3; ++k) out[13 + k] = sed[k];
+    return 0;
+  };
+  if (dim == 3) return with_elastic<ElasticityElement3D>(3, nnode, X, C, order, run);
+  if (dim == 2) return with_elastic<ElasticityElement2D>(2, nnode, X, C, order, run);
+  return 1;
+}
+
 int ref_gauss_1d(int k, double* x, double* w) {
   GAUSS g(k);
   for (int i = 0; i < k; ++i) { x[i] = g.getCoord(i); w[i] = g.getWeight(i); }

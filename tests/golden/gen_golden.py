@@ -16,7 +16,8 @@ the compiled reference leaf library (``make -C oracle``):
   and the step terms formK_s / formF_s_new; for a distorted hex8 and quad4,
   the elasticity elements' stiffness (calculateBmatrix + addToKe) and, for
   the hex8, the internal force (derivativesOfFields + calculateStrain +
-  addToFe) for a general constitutive matrix.
+  addToFe) for a general constitutive matrix; the element driver
+  update("KF") and getVolAvgValues of both elasticity elements.
   These are outputs of the reference code itself (oracle/_ref).
 * ``ref_cg.json`` -- the reference's own Jacobi-PCG (sparse.cpp
   SymmetricSparseMatrix::solve, compiled unmodified with largeMatrix.cpp)
@@ -167,8 +168,37 @@ def ref_quadrature():
             K, _, _ = r.elastic_point(C3, g[0], g[1], None, np.linalg.det(J) * wt, K)
         e2["orders"][str(order)] = {"K": K.tolist()}
     out["elastic2d"] = e2
+    out["elastic_driver"] = elastic_driver_case(r)
     out["source"] = ("reference gauss.cpp + shape.cpp + HeatTransfer{2D,3D}Transient and Elasticity{2D,3D} "
                      "element files compiled unmodified (oracle/_ref)")
+    return out
+
+
+def elastic_driver_inputs():
+    rng = np.random.default_rng(31)
+    X = (np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], float)
+         * np.array([1.2, 0.9, 1.1]) + rng.uniform(-0.08, 0.08, (8, 3)))
+    m9 = [150.0, 12.0, 9.0, 0.25, 0.32, 0.28, 5.0, 3.5, 4.2]
+    u = rng.normal(size=24)
+    X2 = np.array([[0.0, 0.0], [1.2, 0.1], [1.1, 0.9], [-0.05, 1.0]])
+    m4 = [140.0, 10.0, 0.3, 5.0]
+    u2 = rng.normal(size=8)
+    return X, m9, u, X2, m4, u2
+
+
+def elastic_driver_case(r):
+    """The reference's element driver update("KF") and getVolAvgValues on one
+    hex8 and one quad4 with material constants."""
+    X, m9, u, X2, m4, u2 = elastic_driver_inputs()
+    C6, C3 = bo.cmat_ortho3d(m9), bo.cmat_plane_stress(m4)
+    out = {"hex8": {}, "quad4": {}}
+    for order in (2, 3):
+        K, F, sums = r.elastic_update(X, C6, order, "KF", u)
+        out["hex8"][str(order)] = {"K": K.tolist(), "F": F.tolist(), "vol_avg": r.elastic_vol_avg(X, C6, order, u).tolist()}
+    K, F, sums = r.elastic_update(X2, C3, 2, "K")
+    va = r.elastic_vol_avg(X2, C3, 2, u2)
+    # the plane element's getVolAvgValues fills 3 stress / strain components
+    out["quad4"]["2"] = {"K": K.tolist(), "volume": float(va[0]), "stress": va[1:4].tolist(), "strain": va[7:10].tolist()}
     return out
 
 

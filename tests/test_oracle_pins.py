@@ -549,3 +549,45 @@ def test_conductivity_equals_the_reference_material(oracle):
         b = oracle.km_hex8_heat(xyz, C9, 1.3, order=2)
         np.testing.assert_array_equal(a[1], b[1])
         np.testing.assert_array_equal(a[2], b[2])
+
+
+def _one_element_model(kind, X, params):
+    nnpe, ndim = X.shape
+    ndpn = 3 if kind == 2 else 2
+    n = nnpe * ndpn
+    return W.Model("one element", kind, ndim, np.ascontiguousarray(X, float), np.arange(nnpe, dtype=np.int32)[None, :],
+                   ndpn, np.asarray(params, float)[None, :], np.zeros(n, np.uint8), np.zeros(n), np.zeros(n), 2)
+
+
+def test_element_driver_and_outputs_equal_the_reference(oracle):
+    """The reference's own element driver and post-solve outputs (compiled
+    unmodified; isoElement.cpp's interpolation and Jacobian supplied by the
+    shim): ElasticityElement3D::update("KF") -- loopOverIntegrationPoints,
+    processActionCode, calculateStress / calculateFe / calculateKe -- against
+    the oracle's hex8 stiffness and internal force, ElasticityElement2D
+    through the same driver against the quad4 stiffness, and getVolAvgValues
+    against the oracle's element outputs (volume, stress and strain
+    integrals, strain energy)."""
+    gen = _gen_golden()
+    X, m9, u, X2, m4, u2 = gen.elastic_driver_inputs()
+    g = _load("ref_quadrature.json")["elastic_driver"]
+    C6, C3 = oracle.cmat_ortho3d(m9), oracle.cmat_plane_stress(m4)
+    iu = np.triu_indices(24)
+    for order, ref in g["hex8"].items():
+        o = int(order)
+        Kr, Fr, va = np.array(ref["K"]), np.array(ref["F"]), np.array(ref["vol_avg"])
+        K = oracle.ke_hex8(X, C6, o)[1]
+        assert np.abs(K[iu] - Kr[iu]).max() <= 1e-14 * np.abs(Kr).max()
+        F = oracle.fe_hex8(X, C6, u, o)
+        assert np.abs(F - Fr).max() <= 1e-14 * np.abs(Fr).max()
+        out = oracle.element_outputs(_one_element_model(2, X, m9), np.asarray(m9)[None, :], o, u)[0]
+        ref_row = np.concatenate([va[:13], va[13:14]])  # volume, stress (6), strain (6), SED
+        np.testing.assert_allclose(out, ref_row, rtol=1e-13, atol=1e-14 * np.abs(ref_row).max())
+    ref = g["quad4"]["2"]
+    Kr = np.array(ref["K"])
+    iu = np.triu_indices(8)
+    K = oracle.ke_quad4(X2, C3, 2)[1]
+    assert np.abs(K[iu] - Kr[iu]).max() <= 1e-14 * np.abs(Kr).max()
+    out = oracle.element_outputs(_one_element_model(1, X2, m4), np.asarray(m4)[None, :], 2, u2)[0]
+    np.testing.assert_allclose(out[:7], np.concatenate([[ref["volume"]], ref["stress"], ref["strain"]]),
+                               rtol=1e-13, atol=1e-14)
