@@ -601,6 +601,7 @@ class RefLeaf:
         self.lib.ref_elastic_quad4_ke.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_elastic_update.argtypes = [I, I, _dp, _dp, I, C.c_void_p, C.c_char_p, _dp, _dp, _dp]
         self.lib.ref_elastic_vol_avg.argtypes = [I, I, _dp, _dp, I, _dp, _dp]
+        self.lib.ref_heat_update.argtypes = [I, I, _dp, _dp, D, I, C.c_void_p, C.c_char_p, _dp, _dp]
         self.lib.ref_heat_hex8_k.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_write_csr.argtypes = [C.c_char_p, I, I, I, _ipc, _ipc, _dp]
         self.lib.ref_read_csr.argtypes = [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
@@ -732,6 +733,22 @@ class RefLeaf:
         if rc:
             raise ValueError("ref_elastic_update refused the element")
         return Ke.reshape(n, n), Fe, sums.reshape(3, 6)
+
+    def heat_update(self, X, k3, cap, order, action="KM", u=None):
+        """The reference's own diffusion driver update(action, u) of
+        HeatTransferElement3Dtransient (X: 8 x 3) or ...2Dtransient (X: 4 x 2):
+        (K, M) upper triangles."""
+        X = _f64(X)
+        n = X.shape[0]
+        K, M = np.zeros(n * n), np.zeros(n * n)
+        uv = None if u is None else _f64(u).reshape(-1).copy()
+        k = np.zeros(3)
+        k[:len(k3)] = k3
+        rc = self.lib.ref_heat_update(X.shape[1], n, X.reshape(-1).copy(), k, float(cap), int(order),
+                                      None if uv is None else uv.ctypes.data, action.encode(), K, M)
+        if rc:
+            raise ValueError("ref_heat_update refused the element")
+        return K.reshape(n, n), M.reshape(n, n)
 
     def elastic_vol_avg(self, X, C_mat, order, u):
         """getVolAvgValues: [volume, stress integral (6), strain integral (6),

@@ -1,6 +1,8 @@
 // Shim: HeatTransferElement3Dtransient as HeatTransferElement3DTransient.cpp
 // defines it (the reference ships no headers): its members and the element
-// matrices and vectors it fills.
+// matrices and vectors it fills.  The members the 2D element specialises are
+// virtual, so that this element's driver (update, loopOverIntegrationPoints)
+// reaches the 2D versions.
 #pragma once
 #include "element_shim_common.hpp"
 
@@ -13,14 +15,14 @@ class HeatTransferElement3Dtransient : public IsoElement {
  public:
   HeatTransferElement3Dtransient(void);
   ~HeatTransferElement3Dtransient(void);
-  void addToFe(int numDof, int numStrains, InterpAndSolDerivatives* id_ptr, double* flux, double integrationFactor,
-               double* force);
+  virtual void addToFe(int numDof, int numStrains, InterpAndSolDerivatives* id_ptr, double* flux,
+                       double integrationFactor, double* force);
   void addToMe(Matrix* cMat, InterpAndSolDerivatives* id_ptr, double integrationFactor);
-  void gradientsOfFieldVariables(InterpAndSolDerivatives* id_ptr);
+  virtual void gradientsOfFieldVariables(InterpAndSolDerivatives* id_ptr);
   double pointValueOfFieldVariables(InterpAndSolDerivatives* id_ptr, double* nodeValue);
   void printNodalFluxesInLCS(std::ostream& outstream);
   void printNodalFluxesInGCS(std::ostream& outstream);
-  void addToKe(Matrix* cMat, InterpAndSolDerivatives* id_ptr, double integrationFactor);
+  virtual void addToKe(Matrix* cMat, InterpAndSolDerivatives* id_ptr, double integrationFactor);
   void readSpecialCommand(std::istream& inStream, ElementGroup* element, int numElements, char* command);
   void initializeArrays();
   void setPointers(ElementWorkspace* s);

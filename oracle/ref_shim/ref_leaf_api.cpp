@@ -282,6 +282,67 @@ int ref_elastic_update(int dim, int nnode, const double* X, const double* C, int
   return 1;
 }
 
+// The reference's own diffusion element driver: HeatTransferElement3Dtransient
+// (dim 3, hex8) or HeatTransferElement2Dtransient (dim 2, quad4)
+// update(action, u) -> loopOverIntegrationPoints and processActionCode ("K"
+// conductivity, "M" capacity) over the reference's Gauss rule, with the
+// diagonal conductivity k3 (k11, k22, k33) and capacity cap.  K and M: nnode x
+// nnode, upper triangles.  u (nodal values) may be null.
+int ref_heat_update(int dim, int nnode, const double* X, const double* k3, double cap, int order, const double* u,
+                    const char* action, double* Kout, double* Mout) {
+  QuietStdout quiet;
+  auto run = [&](auto& e) {
+    e.numNodesPerElement = nnode;
+    e.numDof = nnode;
+    e.setIntegrationOrder(order);
+    std::vector<double> coords((size_t)nnode * 3, 0.0);
+    for (int a = 0; a < nnode; ++a)
+      for (int k = 0; k < dim; ++k) coords[a * 3 + k] = X[a * dim + k];
+    std::vector<int> dofs(nnode);
+    for (int i = 0; i < nnode; ++i) dofs[i] = i;
+    e.coords = coords.data();
+    e.edofs = dofs.data();
+    TransientElementWorkspace bag;
+    double flux_el[3] = {0, 0, 0}, grad_el[3] = {0, 0, 0}, flux_tot[3] = {0, 0, 0}, grad_tot[3] = {0, 0, 0};
+    bag.fluxVolume_element = flux_el;
+    bag.gradientVolume_element = grad_el;
+    bag.fluxVolume_total = flux_tot;
+    bag.gradientVolume_total = grad_tot;
+    e.bag = &bag;
+    Matrix K(nnode, nnode), Ko(nnode, nnode), M(nnode, nnode);
+    std::vector<double> fe(nnode, 0.0), fo(nnode, 0.0);
+    e.Ke = &K;
+    e.Ke_orig = &Ko;
+    e.Me = &M;
+    e.Fe = fe.data();
+    e.F_orig = fo.data();
+    HeatTransferMaterial mat;
+    mat.saturation = cap;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) mat.cmat(i, j) = i == j ? k3[i] : 0.0;
+    e.material = &mat;
+    std::vector<double> uu;
+    if (u) uu.assign(u, u + nnode);
+    std::string act(action);
+    e.update(&act[0], u ? uu.data() : nullptr);
+    for (int i = 0; i < nnode; ++i)
+      for (int j = 0; j < nnode; ++j) {
+        Kout[i * nnode + j] = K(i, j);
+        Mout[i * nnode + j] = M(i, j);
+      }
+    return 0;
+  };
+  if (dim == 3 && nnode == 8) {
+    HeatTransferElement3Dtransient e;
+    return run(e);
+  }
+  if (dim == 2 && nnode == 4) {
+    HeatTransferElement2Dtransient e;
+    return run(e);
+  }
+  return 1;
+}
+
 // ElasticityElement3D / ElasticityElement2D::getVolAvgValues, the reference's
 // post-solve element outputs: out = [volume, stress integral (6), strain
 // integral (6), SED (3)] for the element's displacement u (element dofs).

@@ -17,7 +17,8 @@ the compiled reference leaf library (``make -C oracle``):
   the elasticity elements' stiffness (calculateBmatrix + addToKe) and, for
   the hex8, the internal force (derivativesOfFields + calculateStrain +
   addToFe) for a general constitutive matrix; the element driver
-  update("KF") and getVolAvgValues of both elasticity elements.
+  update("KF") and getVolAvgValues of both elasticity elements, and the
+  diffusion elements' driver update("KM").
   These are outputs of the reference code itself (oracle/_ref).
 * ``ref_cg.json`` -- the reference's own Jacobi-PCG (sparse.cpp
   SymmetricSparseMatrix::solve, compiled unmodified with largeMatrix.cpp)
@@ -169,8 +170,30 @@ def ref_quadrature():
         e2["orders"][str(order)] = {"K": K.tolist()}
     out["elastic2d"] = e2
     out["elastic_driver"] = elastic_driver_case(r)
+    out["heat_driver"] = heat_driver_case(r)
     out["source"] = ("reference gauss.cpp + shape.cpp + HeatTransfer{2D,3D}Transient and Elasticity{2D,3D} "
                      "element files compiled unmodified (oracle/_ref)")
+    return out
+
+
+def heat_driver_inputs():
+    rng = np.random.default_rng(41)
+    X = (np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], float)
+         * np.array([1.2, 0.9, 1.1]) + rng.uniform(-0.08, 0.08, (8, 3)))
+    X2 = np.array([[0.0, 0.0], [1.2, 0.1], [1.1, 0.9], [-0.05, 1.0]])
+    return X, [2.0, 1.5, 0.8], 1.7, X2, [2.0, 1.5], 1.3
+
+
+def heat_driver_case(r):
+    """The reference's diffusion element driver update("KM") on one hex8 and
+    one quad4 (the 2D element through the 3D element's driver)."""
+    X, k3, c3, X2, k2, c2 = heat_driver_inputs()
+    out = {"hex8": {}, "quad4": {}}
+    for order in (2, 3):
+        K, M = r.heat_update(X, k3, c3, order)
+        out["hex8"][str(order)] = {"K": K.tolist(), "M": M.tolist()}
+        K, M = r.heat_update(X2, k2, c2, order)
+        out["quad4"][str(order)] = {"K": K.tolist(), "M": M.tolist()}
     return out
 
 

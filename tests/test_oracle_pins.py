@@ -591,3 +591,20 @@ def test_element_driver_and_outputs_equal_the_reference(oracle):
     out = oracle.element_outputs(_one_element_model(1, X2, m4), np.asarray(m4)[None, :], 2, u2)[0]
     np.testing.assert_allclose(out[:7], np.concatenate([[ref["volume"]], ref["stress"], ref["strain"]]),
                                rtol=1e-13, atol=1e-14)
+
+
+def test_diffusion_driver_equals_the_reference(oracle):
+    """The reference's own diffusion element driver (compiled unmodified):
+    HeatTransferElement3Dtransient::update("KM") -- loopOverIntegrationPoints,
+    processActionCode, calculateKe / calculateMe -- and the 2D element
+    through the same driver, against the oracle's K and M."""
+    X, k3, c3, X2, k2, c2 = _gen_golden().heat_driver_inputs()
+    g = _load("ref_quadrature.json")["heat_driver"]
+    for order in ("2", "3"):
+        for key, (st, K, M) in (("hex8", oracle.km_hex8_heat(X, k3, c3, order=int(order))),
+                                ("quad4", oracle.km_quad4_heat(X2, k2, c2, order=int(order)))):
+            ref = g[key][order]
+            Kr, Mr = np.array(ref["K"]), np.array(ref["M"])
+            iu = np.triu_indices(Kr.shape[0])
+            assert np.abs(K[iu] - Kr[iu]).max() <= 1e-14 * np.abs(Kr).max()
+            assert np.abs(M[iu] - Mr[iu]).max() <= 1e-14 * np.abs(Mr).max()
