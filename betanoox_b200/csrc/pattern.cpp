@@ -39,8 +39,9 @@ static void parallel_for(long long n, const std::function<void(long long, long l
 // Empties every output of P but keeps the memory of its vectors.
 static void reset_keep(HostPattern& P) {
   P.nnode = P.nelem = P.nnpe = P.ndpn = P.ndof = 0;
-  for (auto* v : {&P.nrp, &P.ndiag, &P.color_ptr, &P.elem_by_color, &P.bsoff, &P.scol, &P.soff, &P.srowlen})
+  for (auto* v : {&P.nrp, &P.ndiag, &P.color_ptr, &P.elem_by_color, &P.bsoff, &P.soff, &P.srowlen})
     v->clear();
+  P.scol.clear();
   P.ncol.clear();
   P.bcol.clear();
   P.slot.clear();
@@ -334,7 +335,7 @@ std::string build_scalar(HostPattern& P, const unsigned char* rest) {
     P.ssoff[s + 1] = P.ssoff[s] + (long long)w * 32;
   }
   if (P.ssoff[P.nsslice] > 2000000000LL) return "build_pattern: scalar layout exceeds 2^31 entries";
-  P.scol.assign(P.ssoff[P.nsslice], 0);
+  P.scol.resize(P.ssoff[P.nsslice]);  // every lane is written below, padding included
   P.sdiag.assign(ndof, 0);
   parallel_for(P.nsslice, [&](long long lo, long long hi) {
     for (long long s = lo; s < hi; ++s) {

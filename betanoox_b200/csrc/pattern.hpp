@@ -77,7 +77,7 @@ struct HostPattern {
   // columns removed), slice s covers rows [32s, 32s+32)
   int nsslice = 0;
   std::vector<long long> ssoff;   // nsslice+1, in entries
-  std::vector<int> scol;          // ssoff.back()
+  FillVec<int> scol;              // ssoff.back()
   std::vector<int> soff;          // per node-pair block: column offset of node J's
                                   // first free dof within rows of node I
   std::vector<int> srowlen;       // per dof
