@@ -322,18 +322,28 @@ std::string build_scalar(HostPattern& P, const unsigned char* rest) {
     }
   });
   P.srowlen.resize(ndof);
-  P.nnz_full = 0;
-  for (int r = 0; r < ndof; ++r) {
-    P.srowlen[r] = rest[r] ? 1 : nodelen[r / ndpn];
-    P.nnz_full += P.srowlen[r];
-  }
   P.nsslice = (ndof + 31) / 32;
   P.ssoff.assign(P.nsslice + 1, 0);
-  for (int s = 0; s < P.nsslice; ++s) {
-    int w = 0;
-    for (int r = s * 32; r < std::min(ndof, s * 32 + 32); ++r) w = std::max(w, P.srowlen[r]);
-    P.ssoff[s + 1] = P.ssoff[s] + (long long)w * 32;
-  }
+  // row lengths, per-slice widths (in ssoff[s+1]) and the nonzero count, by
+  // slices on all threads; then the prefix over slices
+  std::vector<long long> part(chunk_count(P.nsslice), 0);
+  parallel_chunks(P.nsslice, [&](int ck, long long lo, long long hi) {
+    long long acc = 0;
+    for (long long s = lo; s < hi; ++s) {
+      int w = 0;
+      for (int r = (int)s * 32; r < std::min(ndof, (int)s * 32 + 32); ++r) {
+        const int len = rest[r] ? 1 : nodelen[r / ndpn];
+        P.srowlen[r] = len;
+        acc += len;
+        w = std::max(w, len);
+      }
+      P.ssoff[s + 1] = (long long)w * 32;
+    }
+    part[ck] = acc;
+  });
+  P.nnz_full = 0;
+  for (long long v : part) P.nnz_full += v;
+  for (int s = 0; s < P.nsslice; ++s) P.ssoff[s + 1] += P.ssoff[s];
   if (P.ssoff[P.nsslice] > 2000000000LL) return "build_pattern: scalar layout exceeds 2^31 entries";
   P.scol.resize(P.ssoff[P.nsslice]);  // every lane is written below, padding included
   P.sdiag.assign(ndof, 0);
