@@ -462,6 +462,9 @@ class RefMaterial:
         self.lib.ref_cmat_plane_stress.argtypes = [_dp, _dp]
         self.lib.ref_elastic_stress.argtypes = [_dp, _dp, _dp]
         self.lib.ref_heat_conductivity.argtypes = [_dp, _dp, _dp, _dp]
+        _ip32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+        self.lib.ref_set_num_dof.argtypes = [C.c_int, C.c_char_p, _ip32, _ip32, C.POINTER(C.c_int)]
+        self.lib.ref_node_records.argtypes = [C.c_int, _ip32, _dp, C.c_char_p, _ip32, _dp]
 
     @staticmethod
     def available():
@@ -488,6 +491,23 @@ class RefMaterial:
         if self.lib.ref_cmat_plane_stress(_f64(np.asarray(m4, dtype=float)[:4]), Cm):
             raise ValueError("PlaneStress::read failed")
         return Cm.reshape(3, 3)
+
+    def set_num_dof(self, nnode, deck):
+        """Node::setNumDofPerNode on nnode nodes reading deck: (numDof,
+        firstDof, total)."""
+        nd, fd, tot = np.zeros(nnode, np.int32), np.zeros(nnode, np.int32), C.c_int(0)
+        self.lib.ref_set_num_dof(int(nnode), deck.encode(), nd, fd, C.byref(tot))
+        return nd, fd, tot.value
+
+    def node_records(self, nums, xyz, path):
+        """Node::writeBinary of each node to path, then Node::readBinary of
+        them back: (numbers, coordinates) as read."""
+        nums = np.ascontiguousarray(nums, np.int32)
+        xyz = _f64(xyz).reshape(-1, 3).copy()
+        nb, xb = np.zeros_like(nums), np.zeros_like(xyz)
+        if self.lib.ref_node_records(len(nums), nums, xyz.reshape(-1), str(path).encode(), nb, xb.reshape(-1)):
+            raise OSError("ref_node_records could not write " + str(path))
+        return nb, xb
 
     def heat_conductivity(self, k3, grad):
         """HeatTransferMaterial read of readConductivity (k11, k22, k33) and

@@ -1,7 +1,8 @@
 // C entry points over the reference's own matrix.cpp (dense LU inverse),
 // elastic.cpp (ElasticMaterial: readModuli fills the compliance, the
 // stiffness is its inverse), pStress.cpp (PlaneStress) and
-// heatTransferMaterial.cpp (readConductivity, the flux), compiled
+// heatTransferMaterial.cpp (readConductivity, the flux) and node.cpp
+// (setNumDofPerNode, the node records), compiled
 // unmodified into oracle/_ref/libbeta_ref_material.so.  Test infrastructure:
 // used only to pin the oracle's constitutive matrices against the
 // reference's code.  The materials read their constants from an input
@@ -14,6 +15,7 @@
 
 #include "elastic.hpp"
 #include "heatTransferMaterial.hpp"
+#include "node.hpp"
 #include "pStress.hpp"
 
 int verboseFlag = 0;
@@ -123,6 +125,51 @@ int ref_heat_conductivity(const double* k3, const double* grad, double* C9, doub
   id.p_u1_x2 = grad[1];
   id.p_u1_x3 = grad[2];
   mat.calculateFlux(flux, &id);
+  return 0;
+}
+
+// Node::setNumDofPerNode over numNodes nodes reading the block deck (lines
+// "n all" or "n first last increment", ended by "end"): numDof and firstDof
+// per node and the total.  Returns 0.
+int ref_set_num_dof(int numNodes, const char* deck, int* numDof, int* firstDof, int* total) {
+  QuietCout q;
+  NodeGroup nodes(numNodes);
+  for (int i = 0; i < numNodes; ++i) nodes[i].nodeNum = i;
+  std::istringstream in(deck);
+  std::ostringstream out;
+  int tot = 0;
+  Node::setNumDofPerNode(&in, &out, numNodes, &nodes, tot);
+  for (int i = 0; i < numNodes; ++i) {
+    numDof[i] = nodes[i].getNumDof();
+    firstDof[i] = nodes[i].getFirstDof();
+  }
+  *total = tot;
+  return 0;
+}
+
+// Node::writeBinary of nodes (numbers nums, coordinates xyz n x 3) to path,
+// one record after another, and Node::readBinary of them back into
+// nums_back / xyz_back.
+int ref_node_records(int n, const int* nums, const double* xyz, const char* path, int* nums_back,
+                     double* xyz_back) {
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return 1;
+  for (int i = 0; i < n; ++i) {
+    Node nd(nums[i], xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    nd.writeBinary(f);
+  }
+  std::fclose(f);
+  f = std::fopen(path, "rb");
+  if (!f) return 1;
+  for (int i = 0; i < n; ++i) {
+    Node nd;
+    nd.readBinary(f);
+    nums_back[i] = nd.nodeNum;
+    xyz_back[3 * i] = nd.x;
+    xyz_back[3 * i + 1] = nd.y;
+    xyz_back[3 * i + 2] = nd.z;
+  }
+  std::fclose(f);
   return 0;
 }
 

@@ -608,3 +608,33 @@ def test_diffusion_driver_equals_the_reference(oracle):
             iu = np.triu_indices(Kr.shape[0])
             assert np.abs(K[iu] - Kr[iu]).max() <= 1e-14 * np.abs(Kr).max()
             assert np.abs(M[iu] - Mr[iu]).max() <= 1e-14 * np.abs(Mr).max()
+
+
+def test_dof_numbering_and_node_records_equal_the_reference(oracle, abi, tmp_path):
+    """Node::setNumDofPerNode (node.cpp, compiled unmodified): a uniform
+    "n all" block numbers dofs node-major, firstDof = n * node -- the
+    numbering the library and the workloads use -- and mixed blocks give the
+    running sum; the node records of the library's binary mesh writer are
+    byte-identical to Node::writeBinary's, and Node::readBinary reads them."""
+    if not oracle.RefMaterial.available():
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    r = oracle.RefMaterial()
+    m = W.cube_hex8(3, seed=1)
+    nd, fd, tot = r.set_num_dof(m.nnode, "3 all\nend\n")
+    assert (nd == 3).all() and tot == m.ndof
+    np.testing.assert_array_equal(fd, m.first_dof)
+    nd, fd, tot = r.set_num_dof(10, "2 0 9 1\n3 1 9 2\nend\n")
+    np.testing.assert_array_equal(nd, [2, 3, 2, 3, 2, 3, 2, 3, 2, 3])
+    np.testing.assert_array_equal(fd, np.concatenate([[0], np.cumsum(nd)[:-1]]))
+    assert tot == nd.sum()
+    xyz = np.ascontiguousarray(m.xyz, dtype=np.float64)
+    conn = np.ascontiguousarray(m.conn, dtype=np.int32)
+    path = tmp_path / "mesh.bin"
+    assert abi.beta_gpu_write_mesh(str(path).encode(), 1, 3, m.nnode, xyz.ctypes.data, m.nelem, 8,
+                                   conn.ctypes.data, 1) == 0
+    nums = np.arange(1, m.nnode + 1, dtype=np.int32)
+    nb, xb = r.node_records(nums, xyz, tmp_path / "nodes.bin")
+    np.testing.assert_array_equal(nb, nums)
+    np.testing.assert_array_equal(xb, xyz)
+    ours = path.read_bytes()[12:12 + 28 * m.nnode]  # after the three-int header
+    assert ours == (tmp_path / "nodes.bin").read_bytes()
