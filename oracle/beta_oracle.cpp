@@ -239,6 +239,16 @@ int oracle_cmat_ortho3d(const double* m9, double* C36) {
   return OR_OK;
 }
 
+// oracle_cmat_ortho3d for n materials (m9: n x 9, C36: n x 36); 0 or the first
+// failing status.
+int oracle_cmat_ortho3d_many(int n, const double* m9, double* C36) {
+  for (int e = 0; e < n; ++e) {
+    const int st = oracle_cmat_ortho3d(m9 + (size_t)e * 9, C36 + (size_t)e * 36);
+    if (st) return st;
+  }
+  return 0;
+}
+
 // Plane-stress C from (E11,E22,nu12,G12) (beta/materials/2D/pStress.cpp:68-85).
 void oracle_cmat_plane_stress(const double* m4, double* C9) {
   double s11 = 1 / m4[0], s12 = -m4[2] / m4[0], s22 = 1. / m4[1], s66 = 1. / m4[3];
@@ -837,6 +847,43 @@ int oracle_sys_assemble_mesh(void* h, int kind, int nelem, int nnpe, int ndpn, i
   return OR_OK;
 }
 
+// oracle_sys_assemble_mesh with the element matrices of each block of
+// elements computed on all threads first; they are then added in element
+// order, so the assembled system is bit-identical to the serial one.
+int oracle_sys_assemble_mesh_threaded(void* h, int kind, int nelem, int nnpe, int ndpn, int ndim,
+                                      const int* conn, const double* xyz, const int* first_dof,
+                                      const double* params, int nparams, int order, int threads) {
+  g_threads = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
+  if (g_threads > 256) g_threads = 256;
+  const int nd = nnpe * ndpn;
+  const int block = std::max(1, std::min(nelem, 16384));
+  std::vector<double> K((size_t)block * nd * nd);
+  oracle_sys_zero(h);
+  for (int e0 = 0; e0 < nelem; e0 += block) {
+    const int e1 = std::min(nelem, e0 + block);
+    std::vector<int> err(256, 0);
+    par_for(e1 - e0, [&](int lo, int hi, int t) {
+      double xe[24], Me[64];
+      for (int k = lo; k < hi; ++k) {
+        const int e = e0 + k;
+        gather_xyz(nnpe, ndim, conn + (size_t)e * nnpe, xyz, xe);
+        const int st = oracle_element_matrix(kind, xe, params + (size_t)e * nparams, order,
+                                             K.data() + (size_t)k * nd * nd, Me);
+        if (st && !err[t]) err[t] = st;
+      }
+    });
+    for (int v : err)
+      if (v) return v;
+    int map[64];
+    for (int e = e0; e < e1; ++e) {
+      elem_dofs(nnpe, ndpn, conn + (size_t)e * nnpe, first_dof, map);
+      const int st = oracle_sys_add_matrix(h, K.data() + (size_t)(e - e0) * nd * nd, map, nd, nullptr);
+      if (st) return st;
+    }
+  }
+  return OR_OK;
+}
+
 // Global internal force f_int = sum_e Fe(u_e) (BasicModel::CalculateResidual,
 // BasicModel.cpp:1035-1061; Equations::assembleResultantVector,
 // equation.cpp:790-807, which skips restrained rows).  hex8 elasticity only.
@@ -1014,8 +1061,45 @@ void* oracle_csr_from_sys(void* h) {
 
 void oracle_csr_destroy(void* c) { delete (OracleCsr*)c; }
 
+// The full (both-triangle) CSR of a lower triangle given as 0-based CSR rows
+// (rp n+1, col, val), as SymmetricSparseMatrix stores it (sparse.cpp:479-495).
+void* oracle_csr_from_lower(int n, const long long* rp, const int* col, const double* val) {
+  auto* c = new OracleCsr();
+  c->n = n;
+  std::vector<long long> cnt(n + 1, 0);
+  for (int i = 0; i < n; ++i)
+    for (long long k = rp[i]; k < rp[i + 1]; ++k) {
+      cnt[i]++;
+      if (col[k] != i) cnt[col[k]]++;
+    }
+  c->rp.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) c->rp[i + 1] = c->rp[i] + cnt[i];
+  c->ci.resize(c->rp[n]);
+  c->v.resize(c->rp[n]);
+  std::vector<long long> fill(c->rp.begin(), c->rp.end() - 1);
+  for (int i = 0; i < n; ++i)
+    for (long long k = rp[i]; k < rp[i + 1]; ++k) {
+      const int j = col[k];
+      c->ci[fill[i]] = j; c->v[fill[i]++] = val[k];
+      if (j != i) { c->ci[fill[j]] = i; c->v[fill[j]++] = val[k]; }
+    }
+  return c;
+}
+
+// The threaded Jacobi-PCG with a choice of stop rule: rule 0 is the
+// reference's sqrt(r.r / x.x) < eps (sparse.cpp:223), rule 1 is
+// sqrt(r.r / b.b) < eps.  trace (may be null) receives the reference rule's
+// quantity sqrt(r.r / x.x) after each of the first trace_len iterations.
+int oracle_csr_pcg_threaded_rule(void* hc, const double* b, double* x, double eps, int maxit, int threads,
+                                 int rule, double* trace, int trace_len, OracleSolveStats* st);
+
 int oracle_csr_pcg_threaded(void* hc, const double* b, double* x, double eps, int maxit,
                             int threads, OracleSolveStats* st) {
+  return oracle_csr_pcg_threaded_rule(hc, b, x, eps, maxit, threads, 0, nullptr, 0, st);
+}
+
+int oracle_csr_pcg_threaded_rule(void* hc, const double* b, double* x, double eps, int maxit, int threads,
+                                 int rule, double* trace, int trace_len, OracleSolveStats* st) {
   auto* c = (OracleCsr*)hc;
   const int n = c->n;
   g_threads = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
@@ -1044,6 +1128,8 @@ int oracle_csr_pcg_threaded(void* hc, const double* b, double* x, double eps, in
     part[4 * t] = acc;
   });
   double rq = sum_parts(0);
+  double bb = 0;
+  for (int i = 0; i < n; ++i) bb += b[i] * b[i];
   int it = 0;
   bool conv = false;
   double lastnorm = 0;
@@ -1079,8 +1165,9 @@ int oracle_csr_pcg_threaded(void* hc, const double* b, double* x, double eps, in
     par_for(n, [&](int lo, int hi, int) {
       for (int i = lo; i < hi; ++i) p[i] = q[i] + bk * p[i];
     });
+    if (trace && it < trace_len) trace[it] = std::sqrt(rn / xn);
     ++it;
-    lastnorm = std::sqrt(rn / xn);
+    lastnorm = rule == 1 ? (bb > 0 ? std::sqrt(rn / bb) : std::sqrt(rn)) : std::sqrt(rn / xn);
     if (lastnorm < eps) conv = true;
   }
   if (st) { st->iterations = it; st->last_norm = lastnorm; st->status = conv ? OR_OK : OR_ERR_MAXIT; }

@@ -82,12 +82,16 @@ def _load():
         "oracle_sys_rhs": (None, [V, _dp]),
         "oracle_sys_specify_mesh": (None, [V, I, I, I, _ip, _ip]),
         "oracle_sys_assemble_mesh": (I, [V, I, I, I, I, I, _ip, _dp, _ip, _dp, I, I]),
+        "oracle_sys_assemble_mesh_threaded": (I, [V, I, I, I, I, I, _ip, _dp, _ip, _dp, I, I, I]),
         "oracle_internal_force_hex8": (I, [I, _ip, _dp, _ip, _dp, I, P, _dp, _dp]),
         "oracle_element_outputs": (I, [I, I, _ip, _dp, _ip, _dp, I, _dp, _dp]),
         "oracle_heat_step": (I, [V, I, I, _ip, _dp, _ip, _dp, I, D, D, _dp, D, I, C.POINTER(SolveStats)]),
         "oracle_csr_from_sys": (V, [V]),
         "oracle_csr_destroy": (None, [V]),
         "oracle_csr_pcg_threaded": (I, [V, _dp, _dp, D, I, I, C.POINTER(SolveStats)]),
+        "oracle_csr_pcg_threaded_rule": (I, [V, _dp, _dp, D, I, I, I, P, I, C.POINTER(SolveStats)]),
+        "oracle_csr_from_lower": (V, [I, _lp, _ip, _dp]),
+        "oracle_cmat_ortho3d_many": (I, [I, _dp, _dp]),
         "oracle_element_matrices_threaded": (I, [I, I, I, I, I, _ip, _dp, _dp, I, I, I, _dp, I]),
     }
     for name, (res, args) in sig.items():
@@ -161,6 +165,14 @@ def cmat_ortho3d(m9):
     C36 = np.zeros(36)
     assert lib().oracle_cmat_ortho3d(_f64(m9), C36) == 0
     return C36.reshape(6, 6)
+
+
+def cmat_ortho3d_many(params):
+    """cmat_ortho3d for every row of params (n x 9): n x 6 x 6."""
+    params = _f64(params)
+    out = np.zeros((params.shape[0], 36))
+    assert lib().oracle_cmat_ortho3d_many(params.shape[0], params.reshape(-1), out.reshape(-1)) == 0
+    return out.reshape(-1, 6, 6)
 
 
 def cmat_plane_stress(m4):
@@ -249,6 +261,20 @@ class System:
             self.h, m.kind, m.nelem, m.nnpe, m.ndpn, m.ndim, _i32(m.conn).reshape(-1),
             _f64(m.xyz).reshape(-1), _i32(m.first_dof), params.reshape(-1), params.shape[1], order)
 
+    def assemble_threaded(self, params, order, threads=0):
+        """assemble() with the element matrices computed on all threads and
+        added in element order: the same system, bit for bit."""
+        m = self.mesh
+        params = _f64(params)
+        return lib().oracle_sys_assemble_mesh_threaded(
+            self.h, m.kind, m.nelem, m.nnpe, m.ndpn, m.ndim, _i32(m.conn).reshape(-1),
+            _f64(m.xyz).reshape(-1), _i32(m.first_dof), params.reshape(-1), params.shape[1], order, int(threads))
+
+    def csr(self):
+        """The threaded solver's full CSR of this system."""
+        rp, col, val = self.export_lower()
+        return Csr(self.n, rp, col, val)
+
     def export_lower(self):
         nnz = int(lib().oracle_sys_nnz(self.h))
         rp = np.zeros(self.n + 1, dtype=np.int64)
@@ -332,6 +358,36 @@ def element_matrices_threaded(mesh, params, order, e0, e1, threads=0):
                                                 _i32(mesh.conn).reshape(-1), _f64(mesh.xyz).reshape(-1),
                                                 params.reshape(-1), params.shape[1], order, nd, out, threads)
     return st, out
+
+
+class Csr:
+    """The threaded Jacobi-PCG's full CSR built from a lower triangle (0-based
+    CSR rows, as SymmetricSparseMatrix stores it)."""
+
+    RULE_REF, RULE_RB = 0, 1
+
+    def __init__(self, n, rp, col, val):
+        self.n = int(n)
+        self.h = lib().oracle_csr_from_lower(self.n, np.ascontiguousarray(rp, np.int64), _i32(col), _f64(val))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().oracle_csr_destroy(self.h)
+        except Exception:
+            pass
+
+    def pcg(self, b, eps, maxit=100000, threads=0, rule=0, x0=None, trace_len=0):
+        """Jacobi-PCG from x0 (zero) to sqrt(r.r/x.x) < eps (rule 0, the
+        reference's) or sqrt(r.r/b.b) < eps (rule 1).  Returns (rc, x, stats,
+        trace): trace holds the reference rule's quantity after each of the
+        first trace_len iterations."""
+        x = np.zeros(self.n) if x0 is None else _f64(x0).copy()
+        st = SolveStats()
+        tr = np.zeros(max(1, trace_len))
+        rc = lib().oracle_csr_pcg_threaded_rule(self.h, _f64(b), x, float(eps), int(maxit), int(threads), int(rule),
+                                                tr.ctypes.data if trace_len else None, int(trace_len), C.byref(st))
+        return rc, x, st, tr[:min(trace_len, st.iterations)]
 
 
 # -- setElementMaterial block of an input deck ----------------------------------
@@ -590,6 +646,83 @@ class RefEquations:
         if timings is not None:
             timings[:] = secs.tolist()
         return rp, col[:k].copy(), val[:k].copy(), pseudo, lv, x
+
+
+class RefSystem:
+    """One full system held in the reference's own Equations (equation.cpp over
+    SymmetricSparseMatrix, or ParCGMatrix when parcg), built in the
+    reference's order by the calls below and solved repeatedly by
+    Equations::solve: what the bench's reference arm times."""
+
+    def __init__(self, n, restrained, prescribed, parcg=False, maxit=1000000):
+        if not os.path.exists(REF_EQUATIONS_LIB):
+            raise FileNotFoundError(REF_EQUATIONS_LIB)
+        self.lib = C.CDLL(REF_EQUATIONS_LIB)
+        L, V, I, D = self.lib, C.c_void_p, C.c_int, C.c_double
+        _ipc = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+        _u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+        for name, res, args in (
+                ("ref_eqsys_create", V, [I, I, _u8, _dp, I]),
+                ("ref_eqsys_pattern", I, [V, I, I, _ipc]),
+                ("ref_eqsys_allocate", I, [V]),
+                ("ref_eqsys_add", I, [V, I, I, _ipc, _dp]),
+                ("ref_eqsys_loads", I, [V, _dp]),
+                ("ref_eqsys_nnz", C.c_longlong, [V]),
+                ("ref_eqsys_export", I, [V, _lp, _ipc, _dp, _dp]),
+                ("ref_eqsys_solve", I, [V, D, V, V, C.POINTER(C.c_double)]),
+                ("ref_eqsys_destroy", None, [V])):
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        self.n = int(n)
+        self.h = L.ref_eqsys_create(int(bool(parcg)), self.n, np.ascontiguousarray(restrained, np.uint8),
+                                    _f64(prescribed), int(maxit))
+
+    def close(self):
+        if self.h:
+            self.lib.ref_eqsys_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pattern(self, maps):
+        maps = np.ascontiguousarray(maps, np.int32)
+        self.lib.ref_eqsys_pattern(self.h, maps.shape[0], maps.shape[1], maps.reshape(-1))
+
+    def allocate(self):
+        self.lib.ref_eqsys_allocate(self.h)
+
+    def add(self, maps, Ke):
+        maps = np.ascontiguousarray(maps, np.int32)
+        self.lib.ref_eqsys_add(self.h, maps.shape[0], maps.shape[1], maps.reshape(-1), _f64(Ke).reshape(-1))
+
+    def loads(self, load):
+        if self.lib.ref_eqsys_loads(self.h, _f64(load)):
+            raise ValueError("a load sits on a restrained unknown")
+
+    def nnz(self):
+        return int(self.lib.ref_eqsys_nnz(self.h))
+
+    def export(self):
+        """(rp, col, val) of the lower triangle and the right-hand side b."""
+        k = self.nnz()
+        rp, col, val, b = np.zeros(self.n + 1, np.int64), np.zeros(k, np.int32), np.zeros(k), np.zeros(self.n)
+        self.lib.ref_eqsys_export(self.h, rp, col, val, b)
+        return rp, col, val, b
+
+    def solve(self, eps, x0=None, want_x=False):
+        """Equations::solve with stop tolerance eps from x0; returns (seconds,
+        x or None).  The reference exits the process when its iteration
+        limit is reached: choose eps so that it converges."""
+        g = None if x0 is None else _f64(x0).copy()
+        x = np.zeros(self.n) if want_x else None
+        sec = C.c_double(0.0)
+        self.lib.ref_eqsys_solve(self.h, float(eps), None if g is None else g.ctypes.data,
+                                 None if x is None else x.ctypes.data, C.byref(sec))
+        return sec.value, x
 
 
 class RefLeaf:

@@ -168,4 +168,124 @@ int ref_equations_assemble(int parcg, int n, int nelem, int nde, const int* maps
   }
   return 0;
 }
+
+// ---- one persistent system, for timing the reference's own path ------------
+// The bench's reference arm builds the full system once with these calls, in
+// the reference's order (setRestraint, setupStorage, setSolution,
+// specifyNonZeroLocation per element, allocate, zeroMatrix, addMatrix per
+// element, addLoadToEqn), then times Equations::solve on it repeatedly.
+struct RefEqSystem {
+  Equations eq;
+  int n = 0;
+  int parcg = 0;
+};
+
+void* ref_eqsys_create(int parcg, int n, const unsigned char* restrained, const double* prescribed, int maxit) {
+  QuietStreams quiet;
+  auto* h = new RefEqSystem();
+  h->n = n;
+  h->parcg = parcg;
+  h->eq.setMaxIterations(maxit);
+  for (int i = 0; i < n; ++i)
+    if (restrained[i]) h->eq.setRestraint(i, true);
+  h->eq.setupStorage(parcg ? ParCG : Sparse, n);
+  for (int i = 0; i < n; ++i)
+    if (restrained[i]) h->eq.setSolution(prescribed[i], i);
+  return h;
+}
+
+// specifyNonZeroLocation for nelem elements of nde dofs (maps nelem x nde)
+int ref_eqsys_pattern(void* hp, int nelem, int nde, const int* maps) {
+  auto* h = (RefEqSystem*)hp;
+  QuietStreams quiet;
+  for (int e = 0; e < nelem; ++e) h->eq.specifyNonZeroLocation(maps + (size_t)e * nde, nde);
+  return 0;
+}
+
+int ref_eqsys_allocate(void* hp) {
+  auto* h = (RefEqSystem*)hp;
+  QuietStreams quiet;
+  h->eq.allocate();
+  h->eq.zeroMatrix();
+  return 0;
+}
+
+// addMatrix of nelem element matrices Ke (nelem x nde x nde, row-major, upper
+// triangle read) at their maps
+int ref_eqsys_add(void* hp, int nelem, int nde, const int* maps, const double* Ke) {
+  auto* h = (RefEqSystem*)hp;
+  QuietStreams quiet;
+  Matrix K(nde, nde);
+  for (int e = 0; e < nelem; ++e) {
+    const double* ke = Ke + (size_t)e * nde * nde;
+    for (int i = 0; i < nde; ++i)
+      for (int j = 0; j < nde; ++j) K(i, j) = ke[i * nde + j];
+    h->eq.addMatrix(K, maps + (size_t)e * nde, nde, 0, 0);
+  }
+  return 0;
+}
+
+// addLoadToEqn per nonzero load; 2 when a load sits on a restrained unknown
+int ref_eqsys_loads(void* hp, const double* load) {
+  auto* h = (RefEqSystem*)hp;
+  for (int i = 0; i < h->n; ++i)
+    if (load[i] != 0.0 && h->eq.restraint[i]) return 2;
+  QuietStreams quiet;
+  for (int i = 0; i < h->n; ++i)
+    if (load[i] != 0.0) h->eq.addLoadToEqn(load[i], i, false);
+  return 0;
+}
+
+long long ref_eqsys_nnz(void* hp) {
+  auto* h = (RefEqSystem*)hp;
+  SymmetricSparseMatrix& A = *static_cast<SymmetricSparseMatrix*>(h->eq.a);
+  long long k = 0;
+  for (int i = 0; i < h->n; ++i) k += A.row[i].getNum();
+  return k;
+}
+
+// The assembled lower triangle as 0-based CSR (rp n+1, col/val nnz) and the
+// right-hand side Equations::solve forms from it (equation.cpp:1320-1322:
+// load + pseudo-load on free rows, the prescribed value on restrained rows).
+int ref_eqsys_export(void* hp, long long* rp, int* col, double* val, double* b) {
+  auto* h = (RefEqSystem*)hp;
+  SymmetricSparseMatrix& A = *static_cast<SymmetricSparseMatrix*>(h->eq.a);
+  long long k = 0;
+  rp[0] = 0;
+  for (int i = 0; i < h->n; ++i) {
+    const int m = A.row[i].getNum();
+    for (int t = 0; t < m; ++t, ++k) {
+      col[k] = A.row[i][t];
+      val[k] = A.mat[i][t];
+    }
+    rp[i + 1] = k;
+  }
+  for (int i = 0; i < h->n; ++i)
+    b[i] = h->eq.restraint[i] ? h->eq.solution[i] : h->eq.loadVector[i] + h->eq.pseudoLoadVector[i];
+  return 0;
+}
+
+// Equations::solve from the initial guess x0 (null: the reference's last
+// solution) with the storage's stop tolerance set to eps; x (may be null)
+// gets the solution, *seconds the solve's wall time.  The reference exits the
+// process when a solve reaches its iteration limit, so the caller picks eps
+// from the oracle's trace of the same iterates.
+int ref_eqsys_solve(void* hp, double eps, const double* x0, double* x, double* seconds) {
+  auto* h = (RefEqSystem*)hp;
+  static_cast<SymmetricSparseMatrix*>(h->eq.a)->setSOLUTION_EPSILON(eps);
+  QuietStreams quiet;
+  std::vector<double> guess;
+  if (x0) guess.assign(x0, x0 + h->n);
+  const auto t0 = std::chrono::steady_clock::now();
+  const double* u = h->eq.solve(x0 ? guess.data() : 0);
+  if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (x)
+    for (int i = 0; i < h->n; ++i) x[i] = u[i];
+  return 0;
+}
+
+void ref_eqsys_destroy(void* hp) {
+  QuietStreams quiet;
+  delete (RefEqSystem*)hp;
+}
 }
