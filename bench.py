@@ -202,6 +202,35 @@ def whole_job_rate(units_per_rank, seconds, dev=0):
     return ws * units_per_rank / tmax, tmax
 
 
+def _sub_args(args, which):
+    """The arguments of a sub-record run inside the default line: bounded so
+    the whole line stays within minutes (stated in each record's config)."""
+    a = argparse.Namespace(**vars(args))
+    a.skip_cpu = True
+    a.steps, a.warmup = args.sub_steps, max(3, args.sub_warmup)
+    if which == "batch":
+        a.fp64_stride = args.sub_fp64_stride
+        a.e2e_steps = 1
+    else:
+        a.requests = args.sub_requests
+        a.capacity_requests = min(args.capacity_requests, args.sub_requests)
+        a.serve_pool = min(args.serve_pool, args.sub_requests)
+        a.warmup = 1
+    return a
+
+
+_SUB_KEYS = ("value", "unit", "steps", "warmup", "ms_per_step", "config", "latency_ms", "per_step_ms", "fp64_plain",
+             "mixed_over_fp64", "capacity_over_fp64", "roofline", "rel_err_vs_fp64_reference", "e2e",
+             "gpu_launches", "clocks", "batch", "serve")
+
+
+def _sub_record(out):
+    """The keys of a configuration's own line kept in the default line."""
+    if out is None:
+        return None
+    return {k: out[k] for k in _SUB_KEYS if k in out}
+
+
 def run_ours(args):
     import torch
     from betanoox_b200 import Solver, _abi, opts
@@ -269,17 +298,6 @@ def run_ours(args):
         ms_64, st_64, _ = timed(step_64, max(1, min(args.steps, 2)), 1)
         u_64 = g.download()
         fp64 = {"ms": ms_64, "stats": [s.as_dict() for s in st_64], "u": u_64}
-    # accuracy: error of both against a tight FP64 reference solution
-    err = None
-    if not args.skip_accuracy:
-        g.assemble(_abi.FP64)
-        g.solve(opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=1e-13))
-        u_t = g.download()
-        nt = np.linalg.norm(u_t)
-        err = {"mixed": float(np.linalg.norm(u_mp - u_t) / nt)}
-        if fp64:
-            err["fp64"] = float(np.linalg.norm(fp64["u"] - u_t) / nt)
-
     # -- end to end through the C ABI from pinned host buffers --
     e2e = None
     if not args.skip_e2e:
@@ -323,12 +341,19 @@ def run_ours(args):
     value, tot_s = whole_job_rate(m.ndof * args.steps, sum(ms_mp) / 1e3, dev)
     tot_ms = tot_s * 1e3
     ms_step = tot_ms / args.steps
+    spmv_ms = statistics.median([s.ms_spmv_avg for s in st_mp])
+    g.close()
+
+    # -- the batched and served forms, as sub-records of this line (all ranks) --
+    subs = {}
+    if not args.skip_batch:
+        subs["batch"] = _sub_record(run_batch(_sub_args(args, "batch"), nested=True))
+    if not args.skip_serve:
+        subs["serve"] = _sub_record(run_serve(_sub_args(args, "serve"), nested=True))
 
     out = None
     if rank == 0:
         peak, peak_kind = _peaks()
-        nblk = int(g.nnz_blocks) if hasattr(g, "nnz_blocks") else None
-        spmv_ms = statistics.median([s.ms_spmv_avg for s in st_mp])
         alg = spmv_algorithmic_bytes(_nblk(m), m.nnode, m.ndpn)
         achieved = alg / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
         tr = _traffic()
@@ -343,12 +368,8 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32 inner / fp64 outer", "data": "synthetic (seeded generator)",
-            "config": {"workload": f"hex8 elasticity cube {m.meta['n']}^3, {m.ndof} dofs, lognormal E, "
-                                   f"2x2x2 Gauss, z=0 clamped, p=1 on z=1",
-                       "global_batch": ws, "ndof": m.ndof, "nelem": m.nelem, "parallelism": f"replicas x{ws}",
-                       "tol": tol, "stop_rule": "||b-Au||/||b||", "replace_delta": args.inner_tol,
-                       "l2": "inputs larger than L2 (FP32 matrix ~1 GB per replica)"},
-            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "config": cube_config(m, args, ws),
+            "per_step_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "mixed": {"iterations": [s.iterations for s in st_mp], "outer": [s.outer_iterations for s in st_mp],
                       "true_rel_residual": [s.true_rel_residual for s in st_mp], "ms_steps": ms_mp},
             "e2e": e2e, "gpu_launches": cnt_mp[0], "roofline": roof,
@@ -360,11 +381,24 @@ def run_ours(args):
                                  "iterations": [s["iterations"] for s in fp64["stats"]],
                                  "ms_spmv_avg": [s["ms_spmv_avg"] for s in fp64["stats"]]}
             out["mixed_over_fp64"] = value / (ws * v64)
-        if err:
-            out["rel_err_vs_fp64_reference"] = err
-        if not args.skip_cpu:
-            out["cpu_baseline"] = cpu_baseline(m, args, st_64_iters=out.get("fp64_plain", {}).get("iterations"))
-    g.close()
+        out.update(subs)
+        # the oracle at full size (host, rank 0, after all GPU timing and
+        # collectives): its FP64 solution is the accuracy reference, and its
+        # own full solve is the CPU baseline
+        truth = None
+        if not (args.skip_accuracy and args.skip_cpu):
+            truth = oracle_cube_truth(m, args)
+        if truth is not None:
+            ut = truth["u"]
+            nt = np.linalg.norm(ut)
+            if not args.skip_accuracy:
+                err = {"mixed": float(np.linalg.norm(u_mp - ut) / nt),
+                       "oracle": truth["how"], "oracle_iterations": truth["iterations_tight"]}
+                if fp64:
+                    err["fp64"] = float(np.linalg.norm(fp64["u"] - ut) / nt)
+                out["rel_err_vs_oracle"] = err
+            if not args.skip_cpu:
+                out["cpu_baseline"] = truth["cpu_baseline"]
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -386,169 +420,212 @@ def _nblk(m):
     return 2 * nnz.value - m.nnode
 
 
-# ---- CPU baseline (oracle restatement, test infrastructure) ---------------
-def cpu_baseline(m, args, st_64_iters=None, steps=1):
-    """Bounded sample of the workload on the host cores, extrapolated:
-      * element matrices: a contiguous slice of the mesh, all host threads
-        (the compute half of ESA_Assembler::assembleK);
-      * PCG: a fixed number of iterations of the threaded CSR Jacobi-PCG on
-        the same generator at a smaller size, scaled per stored entry;
-      * iteration count of the full solve: the plain FP64 GPU PCG's (same
-        algorithm and stop rule) when measured, else estimated.
-    """
+def cube_config(m, args, ws):
+    """The cube workload's config record, the same in both arms."""
+    return {"workload": f"hex8 elasticity cube {m.meta['n']}^3, {m.ndof} dofs, lognormal E, "
+                        f"2x2x2 Gauss, z=0 clamped, p=1 on z=1",
+            "global_batch": ws, "ndof": m.ndof, "nelem": m.nelem, "parallelism": f"replicas x{ws}",
+            "tol": args.tol, "stop_rule": "||b-Au||/||b||", "replace_delta": args.inner_tol,
+            "l2": "inputs larger than L2 (FP32 matrix ~1 GB per replica)"}
+
+
+# ---- the oracle at full size (test infrastructure) -------------------------
+def oracle_cube_truth(m, args):
+    """The oracle on the whole workload, on all host threads, after the GPU
+    timing: its FP64 assembly (element matrices on all threads, added in
+    element order: bit-identical to the serial restatement of the
+    reference's assembly) and its threaded Jacobi-PCG from the same initial
+    guess, first to the bench's own stop rule ||r||/||b|| <= tol (a full
+    solve, timed: the CPU baseline, nothing extrapolated) and then on to
+    ||r||/||b|| <= args.oracle_tol (the accuracy reference)."""
     from oracle import beta_oracle as bo
-    from betanoox_b200 import workloads as W
-    threads = os.cpu_count() or 1
-    ne_s = min(m.nelem, args.cpu_elems)
+    th = os.cpu_count() or 1
+    s = bo.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
     t0 = time.perf_counter()
-    st, _ = bo.element_matrices_threaded(m, m.params, m.order, 0, ne_s, threads)
-    t_el = (time.perf_counter() - t0) / ne_s
-    ms = W.cube_hex8(args.cpu_n)
-    s = bo.System(ms)
-    s.set_bc(ms.restrained, ms.prescribed, ms.load)
     s.build_pattern()
-    s.assemble(ms.params, ms.order)
+    t_struct = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rc = s.assemble_threaded(m.params, m.order, th)
+    t_asm = time.perf_counter() - t0
+    if rc:
+        raise RuntimeError(f"oracle assembly failed ({rc})")
+    csr = s.csr()
     b = s.rhs()
-    nnz_s = 2 * bo.lib().oracle_sys_nnz(s.h) - ms.ndof
-    s.solve_threaded(b, 1e-30, maxit=2, threads=threads)  # builds the CSR copy
+    del s
+    x0 = np.where(np.asarray(m.restrained, bool), m.prescribed, 0.0)
     t0 = time.perf_counter()
-    rc, x, sst = s.solve_threaded(b, 1e-30, maxit=args.cpu_iters, threads=threads)
-    t_it = (time.perf_counter() - t0) / max(1, sst.iterations)
-    nnz_full = 2 * _lower_nnz(m) - m.ndof
-    t_it_full = t_it * nnz_full / nnz_s
-    iters = int(statistics.median(st_64_iters)) if st_64_iters else None
-    if iters is None:
-        iters = int(args.cpu_assumed_iters)
-    t_total = t_el * m.nelem + iters * t_it_full
-    return {"value": m.ndof / t_total, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": (f"extrapolated: element matrices of {ne_s} of {m.nelem} elements "
-                       f"({t_el * 1e6:.2f} us/elem on {threads} threads) + {sst.iterations} threaded Jacobi-PCG "
-                       f"iterations on the {args.cpu_n}^3 cube ({t_it * 1e3:.2f} ms/iter, scaled by stored "
-                       f"entries {nnz_full}/{nnz_s}) x {iters} iterations (plain FP64 GPU PCG count, same stop rule)"),
-            "seconds_full_solve_est": t_total}
+    rc, x, st, _ = csr.pcg(b, args.tol, maxit=200000, threads=th, rule=bo.Csr.RULE_RB, x0=x0)
+    t_solve = time.perf_counter() - t0
+    if rc:
+        raise RuntimeError(f"oracle solve failed ({rc})")
+    rc, xt, st2, _ = csr.pcg(b, args.oracle_tol, maxit=200000, threads=th, rule=bo.Csr.RULE_RB, x0=x)
+    cb = {"value": m.ndof / (t_asm + t_solve), "unit": UNIT, "cores": th, "kind": "port",
+          "sample": (f"the whole workload, measured (not extrapolated): the oracle's FP64 assembly of all "
+                     f"{m.nelem} elements on {th} threads ({t_asm:.2f} s) + its threaded Jacobi-PCG from zero to "
+                     f"||r||/||b|| <= {args.tol:g}, {st.iterations} iterations ({t_solve:.1f} s); the structure "
+                     f"({t_struct:.2f} s) is built once, untimed, as on the GPU"),
+          "seconds": t_asm + t_solve, "iterations": st.iterations}
+    return {"u": xt, "cpu_baseline": cb, "iterations_tight": st.iterations + st2.iterations,
+            "how": (f"the oracle's FP64 solution: its own assembly, threaded Jacobi-PCG to ||r||/||b|| <= "
+                    f"{args.oracle_tol:g}")}
 
 
-def reference_code_baseline(m, args, iters_full):
-    """The reference's own code (oracle/_ref, compiled from its sources), run
-    serially as its default SerialAssembler + SymmetricSparseMatrix::solve
-    path runs, on a bounded sample of the workload, extrapolated:
-      * element matrices: ElasticityElement3D calculateBmatrix + addToKe with
-        the reference's Gauss rule and shape functions on a slice of the mesh;
-      * structure and scatter: Equations specifyNonZeroLocation / allocate and
-        addMatrix on a smaller cube of the same generator, per element;
-      * solve: SymmetricSparseMatrix::solve (its Jacobi-PCG and stop rule) and
-        ParCGMatrix::solve (the same PCG on two OpenMP threads) on that cube,
-        the faster per iteration, scaled by stored lower-triangle entries,
-        times the full solve's iteration count.
-    Returns None when oracle/_ref is absent (the reference tree was not
-    present where the repository was built)."""
+# ---- the reference arm: the reference's own code (oracle/_ref) ---------------
+def _eps_after(trace, k, margin=1e-6):
+    """A stop tolerance under which the reference rule's quantity (trace[i]
+    after iteration i+1) first falls at iteration k' >= k: the smallest such
+    k' whose value lies below every earlier one by the margin.  Returns
+    (k', eps) or None."""
+    for kk in range(max(1, k), len(trace) + 1):
+        v = trace[kk - 1] * (1.0 + margin)
+        if all(trace[i] > v for i in range(kk - 1)):
+            return kk, v
+    return None
+
+
+def reference_cube_setup(m, args):
+    """The whole workload built once by the reference's own code compiled
+    from its sources (oracle/_ref): per element its Gauss rule, shape
+    functions and ElasticityElement3D B / addToKe (serially, as
+    SerialAssembler, the reference's default), Equations
+    specifyNonZeroLocation / allocate and addMatrix with the restraint
+    elimination, addLoadToEqn; storage ParCGMatrix (its two-thread OpenMP
+    solver) or SymmetricSparseMatrix (serial).  The element matrices and the
+    scatter are timed in full; the structure is timed apart (built once per
+    analysis by the reference, as it is on the GPU).
+
+    The full solve's iteration count to the bench's stop rule
+    ||r||/||b|| <= tol comes from the oracle's threaded Jacobi-PCG on the
+    reference's own assembled matrix and right-hand side (the same
+    recurrence as the reference's solver, step for step); its trace of the
+    reference rule sqrt(r.r/x.x) gives the tolerances at which the
+    reference's solve stops after a chosen number of iterations."""
     from oracle import beta_oracle as bo
-    from betanoox_b200 import workloads as W
-    if not (bo.RefLeaf.available() and bo.RefEquations.available()):
-        return None
-    leaf, req = bo.RefLeaf(), bo.RefEquations()
-    ne_s = min(m.nelem, args.cpu_elems)
-    C_s = np.stack([bo.cmat_ortho3d(p) for p in m.params[:ne_s]])
-    xe = np.ascontiguousarray(m.xyz[m.conn[:ne_s]])
+    th = os.cpu_count() or 1
+    leaf = bo.RefLeaf()
+    Cs = bo.cmat_ortho3d_many(m.params)  # the materials as read: one per element, untimed
+    nd = m.nnpe * m.ndpn
+    maps = np.ascontiguousarray(
+        (m.first_dof[m.conn][:, :, None] + np.arange(m.ndpn)[None, None, :]).reshape(m.nelem, nd), np.int32)
+    rs = bo.RefSystem(m.ndof, m.restrained, m.prescribed, parcg=args.ref_solver == "parcg")
     t0 = time.perf_counter()
-    leaf.elastic_hex8_ke(xe, C_s, m.order)
-    t_el = (time.perf_counter() - t0) / ne_s
-    ms = W.cube_hex8(args.cpu_ref_n)
-    Ke = leaf.elastic_hex8_ke(ms.xyz[ms.conn], np.stack([bo.cmat_ortho3d(p) for p in ms.params]), ms.order)
-    nd = ms.nnpe * ms.ndpn
-    maps = (ms.first_dof[ms.conn][:, :, None] + np.arange(ms.ndpn)[None, None, :]).reshape(ms.nelem, nd)
-    # the oracle's serial PCG is the reference's step for step: its count is the
-    # reference's, and it proves convergence first (the reference exits otherwise)
-    s = bo.System(ms)
-    s.set_bc(ms.restrained, ms.prescribed, ms.load)
-    s.build_pattern()
-    s.assemble(ms.params, ms.order)
-    rc, _, sst = s.solve(eps=args.cpu_ref_eps, maxit=100000)
-    if rc != 0:
-        return None
-    # both of the reference's own solvers on the same system: the default serial
-    # SymmetricSparseMatrix::solve and ParCG's two-thread OpenMP solve; the
-    # faster one is the reference's figure
-    solvers = {}
-    for name, parcg in (("SymmetricSparseMatrix::solve (serial)", False), ("ParCGMatrix::solve (2 threads)", True)):
-        secs = []
-        rp, _, _, _, _, _ = req.assemble(ms.ndof, maps, Ke, ms.restrained, ms.prescribed, ms.load, solve=True,
-                                         eps=args.cpu_ref_eps, maxit=100000, timings=secs, parcg=parcg)
-        solvers[name] = (secs, 2 if parcg else 1)
-    best = min(solvers, key=lambda k: solvers[k][0][2])
-    (t_struct, t_scatter, t_solve), cores = solvers[best]
-    t_it = t_solve / max(1, sst.iterations)
-    nnz_s, nnz_full = int(rp[-1]), _lower_nnz(m)
-    t_it_full = t_it * nnz_full / nnz_s
-    per_elem = t_el + (t_struct + t_scatter) / ms.nelem
-    t_total = per_elem * m.nelem + iters_full * t_it_full
-    per_iter = ", ".join(f"{k} {v[0][2] / max(1, sst.iterations) * 1e3:.2f} ms/iter" for k, v in solvers.items())
-    return {"value": m.ndof / t_total, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": (f"extrapolated, the reference's own code compiled from its sources (oracle/_ref): "
-                       f"element matrices of {ne_s} of {m.nelem} elements, serial ({t_el * 1e6:.2f} us/elem); "
-                       f"Equations pattern + addMatrix on the {args.cpu_ref_n}^3 cube "
-                       f"({(t_struct + t_scatter) / ms.nelem * 1e6:.2f} us/elem); its solvers there, "
-                       f"{sst.iterations} iterations at eps {args.cpu_ref_eps:g} ({per_iter}), the faster, "
-                       f"{best}, scaled by lower-triangle entries {nnz_full}/{nnz_s} x {iters_full} iterations"),
-            "solver": best, "seconds_full_solve_est": t_total}
+    rs.pattern(maps)
+    rs.allocate()
+    t_struct = time.perf_counter() - t0
+    t_el = t_add = 0.0
+    for e0 in range(0, m.nelem, 32768):
+        e1 = min(m.nelem, e0 + 32768)
+        xe = np.ascontiguousarray(m.xyz[m.conn[e0:e1]])
+        t0 = time.perf_counter()
+        Ke = leaf.elastic_hex8_ke(xe, Cs[e0:e1], m.order)
+        t_el += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rs.add(maps[e0:e1], Ke)
+        t_add += time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rs.loads(m.load)
+    t_add += time.perf_counter() - t0
+    del Cs, maps
+    rp, col, val, b = rs.export()
+    csr = bo.Csr(m.ndof, rp, col, val)
+    del rp, col, val
+    ka, kb = args.ref_iters_a, args.ref_iters_b
+    x0 = np.where(np.asarray(m.restrained, bool), m.prescribed, 0.0)
+    t0 = time.perf_counter()
+    rc, _, st, trace = csr.pcg(b, args.tol, maxit=200000, threads=th, rule=bo.Csr.RULE_RB, x0=x0,
+                               trace_len=kb + 64)
+    t_port = time.perf_counter() - t0
+    if rc:
+        raise RuntimeError("the oracle's solve of the reference's system did not converge")
+    pa, pb = _eps_after(trace, ka), _eps_after(trace, kb)
+    if pa is None or pb is None or pb[0] <= pa[0]:
+        raise RuntimeError("no stop tolerances for the bounded solves")
+    (ka, eps_a), (kb, eps_b) = pa, pb
+    # the reference's solve at eps_b must stop after exactly kb iterations:
+    # its iterate equals the oracle's kb-th (the neighbouring iterates differ
+    # by far more than rounding)
+    zero = np.zeros(m.ndof)
+    _, xr = rs.solve(eps_b, x0=zero, want_x=True)
+    _, xo, _, _ = csr.pcg(b, 0.0, maxit=kb, threads=th, rule=bo.Csr.RULE_REF, x0=x0)
+    chk = float(np.linalg.norm(xr - xo) / np.linalg.norm(xo))
+    if not chk <= 1e-9:
+        raise RuntimeError(f"the reference's bounded solve is not the oracle's {kb}-th iterate ({chk:.2e})")
+    return {"rs": rs, "iters_full": st.iterations, "t_el": t_el, "t_add": t_add, "t_struct": t_struct,
+            "ka": ka, "kb": kb, "eps_a": eps_a, "eps_b": eps_b, "check": chk, "t_port_solve": t_port,
+            "threads": th}
 
 
-def _lower_nnz(m):
-    from betanoox_b200 import _abi
-    lib = _abi.load()
-    conn = np.ascontiguousarray(m.conn, np.int32)
-    fd = np.ascontiguousarray(m.first_dof, np.int32)
-    r = np.ascontiguousarray(m.restrained, np.uint8)
-    nnz = C.c_longlong()
-    lib.beta_gpu_pattern_lower_host(m.nnode, m.nelem, m.nnpe, m.ndpn, conn.ctypes.data, fd.ctypes.data,
-                                    r.ctypes.data, C.byref(nnz), None, None)
-    return nnz.value
+def reference_cube_step(R, ndof):
+    """One bounded sample: two of the reference's Equations::solve calls on the
+    full system from zero, stopped after ka and kb iterations by their
+    tolerances.  Per-iteration time = the difference / (kb - ka); the solve's
+    fixed cost = the ka solve minus ka iterations.  Returns (DOF/s of the
+    whole workload, wall seconds of the sample, seconds per iteration)."""
+    zero = np.zeros(ndof)
+    ta, _ = R["rs"].solve(R["eps_a"], x0=zero)
+    tb, _ = R["rs"].solve(R["eps_b"], x0=zero)
+    t_it = max(1e-12, (tb - ta) / (R["kb"] - R["ka"]))
+    t_fix = max(0.0, ta - R["ka"] * t_it)
+    total = R["t_el"] + R["t_add"] + t_fix + R["iters_full"] * t_it
+    return ndof / total, ta + tb, t_it, t_fix
+
+
+def _unavailable(why):
+    return {"impl": "reference", "unavailable": why}
 
 
 def run_reference(args):
-    """The reference's own code when oracle/_ref was built (its serial
-    assembly and the faster of its serial and two-thread solvers), else the
-    oracle's all-core port; the port's figure is reported beside the
-    reference's either way."""
+    """The reference's own CPU path (oracle/_ref) on the cube: assembly measured
+    in full once, each step a bounded sample of its solve on the full system
+    (the only extrapolation: iterations x measured full-size time per
+    iteration).  Rank 0 alone works under torchrun."""
     ws, rank, local = _dist()
     if rank != 0:
         return None
+    from oracle import beta_oracle as bo
+    if not (bo.RefLeaf.available() and bo.RefEquations.available()):
+        return _unavailable("oracle/_ref (the reference's sources compiled here) is absent")
     m = make_model(args.config, args.n)
-    iters = args.cpu_assumed_iters
-    vals = []
-    cb = None
-    port = cpu_baseline(m, args, None)
-
-    def ref_code():
-        try:
-            return reference_code_baseline(m, args, iters)
-        except OSError as e:  # oracle/_ref present but not loadable on this host
-            print(f"reference code unavailable ({e}); timing the port", file=sys.stderr)
-            return None
-
-    if args.warmup:
-        ref_code()
-    for _ in range(args.steps):
-        cb = ref_code()
-        if cb is None:
-            break
-        vals.append(cb["value"])
-    if cb is None:
-        vals = []
-        for _ in range(args.steps):
-            cb = cpu_baseline(m, args, None)
-            vals.append(cb["value"])
-    else:
-        cb["port_all_cores"] = {k: port[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    try:
+        R = reference_cube_setup(m, args)
+    except OSError as e:
+        return _unavailable(f"oracle/_ref does not load on this host: {e}")
+    vals, walls, its, fixes = [], [], [], []
+    for k in range(args.warmup + args.steps):
+        v, wall, t_it, t_fix = reference_cube_step(R, m.ndof)
+        if k >= args.warmup:
+            vals.append(v)
+            walls.append(wall)
+            its.append(t_it)
+            fixes.append(t_fix)
+    R["rs"].close()
     v = statistics.median(vals)
-    cb["value"] = v
+    solver = ("ParCGMatrix::solve (ParCG.cpp, 2 OpenMP threads)" if args.ref_solver == "parcg"
+              else "SymmetricSparseMatrix::solve (sparse.cpp, serial)")
+    cores = 2 if args.ref_solver == "parcg" else 1
+    t_it = statistics.median(its)
+    cb = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "solver": solver,
+          "sample": (f"the reference's own code compiled from its sources (oracle/_ref) on the whole "
+                     f"{m.ndof}-dof system: element matrices (ElasticityElement3D B/addToKe, serial) "
+                     f"{R['t_el']:.2f} s and Equations::addMatrix {R['t_add']:.2f} s, measured in full once; "
+                     f"each step runs Equations::solve ({solver}) twice on the full system, stopped after "
+                     f"{R['ka']} and {R['kb']} iterations by tolerance (checked against the oracle's iterate, "
+                     f"{R['check']:.1e}): {t_it * 1e3:.1f} ms per iteration, {statistics.median(fixes) * 1e3:.1f} ms "
+                     f"fixed; the full solve = fixed + {R['iters_full']} iterations x per-iteration time, the "
+                     f"count from the oracle's threaded Jacobi-PCG on the reference's own matrix to "
+                     f"||r||/||b|| <= {args.tol:g} (the only extrapolated quantity); structure "
+                     f"{R['t_struct']:.2f} s untimed, as on the GPU"),
+          "iterations_full_solve": R["iters_full"], "seconds_per_iteration": t_it,
+          "seconds_assembly": R["t_el"] + R["t_add"],
+          "port_all_cores": {"unit": UNIT, "cores": R["threads"], "kind": "port",
+                             "seconds_full_solve": R["t_port_solve"],
+                             "sample": "the oracle's threaded Jacobi-PCG, the same full solve (measured)"}}
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * m.ndof / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
-            "config": {"workload": f"hex8 elasticity cube {m.meta['n']}^3, {m.ndof} dofs", "ndof": m.ndof,
-                       "assumed_iterations": iters},
-            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-
+            "ms_per_step": 1e3 * statistics.median(walls), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": cube_config(m, args, ws), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 # ---- transient diffusion (backward Euler) ------------------------------------
@@ -588,12 +665,15 @@ def run_heat(args):
         return list(a)
 
     def march(prec, o, nsteps):
+        # k is linear, so C/dt + K is the same every step: assembled once, in the
+        # first step's time (--heat-reassemble: every step, as the reference does)
         stats, ms = [], []
         with torch.cuda.stream(stream):
-            for _ in range(nsteps):
+            for k in range(nsteps):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                g.assemble(prec, _abi.ASM_MBAR, dt, 1.0)
+                if k == 0 or args.heat_reassemble:
+                    g.assemble(prec, _abi.ASM_MBAR, dt, 1.0)
                 st, _ = g.heat_run(dt, 1, o)
                 e1.record(stream)
                 stats.append(st)
@@ -643,8 +723,9 @@ def run_heat(args):
             ge.load_model(pm)
             ge.build_pattern()
             ge.lib.beta_gpu_heat_set_state(ge.h, u0p.ctypes.data_as(C.c_void_p))
-            for _ in range(args.heat_steps):
-                ge.assemble(_abi.FP32, _abi.ASM_MBAR, dt, 1.0)
+            for k in range(args.heat_steps):
+                if k == 0 or args.heat_reassemble:
+                    ge.assemble(_abi.FP32, _abi.ASM_MBAR, dt, 1.0)
                 ge.heat_run(dt, 1, o_mp)
             ge.lib.beta_gpu_heat_get_state(ge.h, u_host.ctypes.data_as(C.c_void_p))
             torch.cuda.synchronize()
@@ -677,7 +758,7 @@ def run_heat(args):
                                    f"Gaussian bump; each step assembles C/dt+K (FP32) and solves it",
                        "ndof": m.ndof, "time_steps": args.heat_steps, "tol": tol,
                        "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (matrix ~1 GB)"},
-            "latency_ms": {"p50": float(np.percentile(ms_mp, 50)), "p99": float(np.percentile(ms_mp, 99))},
+            "per_step_ms": {"p50": float(np.percentile(ms_mp, 50)), "p99": float(np.percentile(ms_mp, 99))},
             "heat": {"iterations_per_step": [min(its), int(statistics.median(its)), max(its)],
                      "refinements_per_step_median": int(statistics.median([s.outer_iterations for s in st_mp]))},
             "e2e": e2e, "gpu_launches": c1[0] - c0[0], "roofline": roof, "clocks": clk.summary(),
@@ -770,29 +851,34 @@ def reference_heat_baseline(args, m):
 
 
 def run_heat_reference(args):
+    """The reference's own transient step (oracle/_ref) on a bounded sample
+    slab; each bench step is one such sample.  Prints the unavailable line
+    where oracle/_ref is absent or does not load."""
     ws, rank, _ = _dist()
     if rank != 0:
         return None
+    from oracle import beta_oracle as bo
+    if not (bo.RefLeaf.available() and bo.RefEquations.available()):
+        return _unavailable("oracle/_ref (the reference's sources compiled here) is absent")
     m = heat_model(args)
-    cb, vals = None, []
+    vals, walls, cb = [], [], None
     try:
-        for k in range(max(1, args.warmup and 1) + max(1, args.steps)):
+        for k in range(args.warmup + max(1, args.steps)):
+            t0 = time.perf_counter()
             cb = reference_heat_baseline(args, m)
+            wall = time.perf_counter() - t0
             if cb is None:
-                break
-            if k >= 1:
+                return _unavailable("the oracle's transient step did not converge on the sample slab")
+            if k >= args.warmup:
                 vals.append(cb["value"])
-    except OSError as e:  # oracle/_ref present but not loadable on this host
-        print(f"reference code unavailable ({e}); timing the port", file=sys.stderr)
-        cb = None
-    if cb is None or not vals:
-        vals = [heat_cpu_baseline(args, m)["value"] for _ in range(max(1, args.steps))]
-        cb = heat_cpu_baseline(args, m)
+                walls.append(wall)
+    except OSError as e:
+        return _unavailable(f"oracle/_ref does not load on this host: {e}")
     v = statistics.median(vals)
     cb["value"] = v
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * m.ndof / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
+            "ms_per_step": 1e3 * statistics.median(walls), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
             "config": {"workload": f"transient diffusion hex8 {args.heat_nx}x{args.heat_nx}x{args.heat_nz}, "
                                    f"{m.ndof} dofs, backward Euler dt={args.dt}", "ndof": m.ndof},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -897,12 +983,15 @@ def reference_full_solves(models, tol, budget_s, threads):
     return done, dofs, t_ref, t_port
 
 
-def run_batch(args):
+def run_batch(args, nested=False):
+    """The batch configuration.  nested: a sub-record of the default line (the
+    process group already exists and stays up; no CPU baseline)."""
     import torch
     from betanoox_b200 import Batch, Solver, _abi, opts
     from betanoox_b200 import workloads as W
     ws, rank, dev = _dist()
-    _init_dist(dev)
+    if not nested:
+        _init_dist(dev)
     t0 = time.perf_counter()
     models = W.rve_batch(count=args.count, seed=args.seed)
     t_gen = time.perf_counter() - t0
@@ -949,7 +1038,7 @@ def run_batch(args):
         stream = torch.cuda.Stream(device=dev)
         for k, (sid, m) in enumerate(zip(ids, models)):
             want_acc = k % args.check_every == 0
-            want_64 = k < args.fp64_sample
+            want_64 = k % args.fp64_stride == 0 and k // args.fp64_stride < args.fp64_sample
             if not (want_acc or want_64):
                 continue
             g = Solver(dev)
@@ -1017,7 +1106,7 @@ def run_batch(args):
                        "launch_shape": {"threads": threads, "gang_boost": boost, "gangs": ginfo["gangs"],
                                         "gang_ctas": ginfo["gang_ctas"]},
                        "l2": f"inputs larger than L2 (pool {b.info()['used'] / 2**30:.1f} GiB)"},
-            "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+            "per_step_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
             "batch": {"ms_steps": ms, "iterations_total": int(sum(iters)), "iterations_max": int(max(iters)),
                       "not_converged": bad[:5], "n_not_converged": len(bad), "setup_s": {"generate": t_gen,
                       "add_many": t_add, "autotune": t_tune}},
@@ -1027,80 +1116,71 @@ def run_batch(args):
             out["rel_err_vs_fp64_reference"] = {"max": max(errs), "n_checked": len(errs)}
         if fp64_dofs:
             v64 = fp64_dofs / (fp64_ms / 1e3)
-            out["fp64_plain"] = {"value": ws * v64, "systems": min(args.fp64_sample, len(models)),
-                                 "how": "sequential per-system plain FP64 Jacobi-PCG (FP64 assembly + solve, "
-                                        "CUDA events), same stop rule and tol",
+            out["fp64_plain"] = {"value": ws * v64, "systems": len(fp64_iters),
+                                 "how": f"sequential per-system plain FP64 Jacobi-PCG (FP64 assembly + solve, "
+                                        f"CUDA events), same stop rule and tol, on every {args.fp64_stride}-th "
+                                        f"system of the batch",
                                  "iterations_median": int(statistics.median(fp64_iters))}
             out["mixed_over_fp64"] = value / (ws * v64)
-        if not args.skip_cpu:
+        if not args.skip_cpu and not nested:
             th = os.cpu_count() or 1
             n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s, th)
             out["cpu_baseline"] = {"value": d / sec, "unit": UNIT, "cores": th, "kind": "port",
                                    "sample": f"first {n} of {len(models)} RVEs solved whole on the host "
                                              f"({d} dofs in {sec:.1f} s): FP64 assembly + threaded Jacobi-PCG"}
     b.close()
-    if ws > 1:
+    if ws > 1 and not nested:
         import torch.distributed as dist
         dist.destroy_process_group()
     return out
 
 
 def run_batch_reference(args):
+    """Whole RVEs of the batch, in list order within a time budget per step,
+    solved by the reference's own code (oracle/_ref) one system at a time;
+    each bench step is one such sample.  Prints the unavailable line where
+    oracle/_ref is absent or does not load."""
     ws, rank, _ = _dist()
     if rank != 0:
         return None
+    from oracle import beta_oracle as bo
+    if not (bo.RefLeaf.available() and bo.RefEquations.available()):
+        return _unavailable("oracle/_ref (the reference's sources compiled here) is absent")
     from betanoox_b200 import workloads as W
     models = W.rve_batch(count=args.count, seed=args.seed)
     ndof_tot = sum(m.ndof for m in models)
     th = os.cpu_count() or 1
-    vals, last = [], None
-    ref, rvals, pvals = None, [], []
+    rvals, pvals, walls, ref = [], [], [], None
     try:
-        for k in range(max(1, args.warmup and 1) + args.steps):
+        for k in range(args.warmup + max(1, args.steps)):
+            t0 = time.perf_counter()
             ref = reference_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
+            wall = time.perf_counter() - t0
             if ref is None or ref[0] == 0:
-                ref = None
-                break
-            if k >= 1:
+                return _unavailable("no RVE was solved by the reference's code within the step's budget")
+            if k >= args.warmup:
                 rvals.append(ref[1] / ref[2])
                 pvals.append(ref[1] / ref[3])
-    except OSError as e:  # oracle/_ref present but not loadable on this host
-        print(f"reference code unavailable ({e}); timing the port", file=sys.stderr)
-        ref = None
-    if ref is not None and rvals:
-        n, d, t_ref, t_port = ref
-        v = statistics.median(rvals)
-        return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * ndof_tot / v, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded generator)",
-                "impl": "reference",
-                "config": {"workload": f"{len(models)} two-phase RVE hex8 cubes n~U{{8..40}}, {ndof_tot} dofs total",
-                           "ndof_total": ndof_tot},
-                "cpu_baseline": {"value": v, "unit": UNIT, "cores": 2, "kind": "reference",
-                                 "sample": f"first {n} RVEs solved whole ({d} dofs, {t_ref:.1f} s) by the "
-                                           f"reference's own code compiled from its sources (oracle/_ref): "
-                                           f"element B/addToKe, Equations pattern + addMatrix, ParCG solve, "
-                                           f"one system at a time",
-                                 "port_all_cores": {"value": statistics.median(pvals), "unit": UNIT, "cores": th,
-                                                    "kind": "port",
-                                                    "sample": f"the same {n} RVEs, FP64 assembly + threaded "
-                                                              f"Jacobi-PCG ({t_port:.1f} s)"}},
-                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    for k in range(max(1, args.warmup and 1) + args.steps):
-        n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
-        if k >= 1:
-            vals.append(d / sec)
-            last = (n, d, sec)
-    v = statistics.median(vals)
-    n, d, sec = last
-    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * ndof_tot / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
+                walls.append(wall)
+    except OSError as e:
+        return _unavailable(f"oracle/_ref does not load on this host: {e}")
+    n, d, t_ref, t_port = ref
+    v = statistics.median(rvals)
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(walls), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded generator)",
+            "impl": "reference",
             "config": {"workload": f"{len(models)} two-phase RVE hex8 cubes n~U{{8..40}}, {ndof_tot} dofs total",
                        "ndof_total": ndof_tot},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port",
-                             "sample": f"first {n} RVEs solved whole per step ({d} dofs, {sec:.1f} s): "
-                                       f"FP64 assembly + threaded Jacobi-PCG, one system at a time"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 2, "kind": "reference",
+                             "sample": f"first {n} RVEs solved whole per step ({d} dofs, {t_ref:.1f} s) by the "
+                                       f"reference's own code compiled from its sources (oracle/_ref): "
+                                       f"element B/addToKe, Equations pattern + addMatrix, ParCG solve, "
+                                       f"one system at a time; the rate applies to the whole batch",
+                             "port_all_cores": {"value": statistics.median(pvals), "unit": UNIT, "cores": th,
+                                                "kind": "port",
+                                                "sample": f"the same {n} RVEs, FP64 assembly + threaded "
+                                                          f"Jacobi-PCG ({t_port:.1f} s)"}},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -1150,12 +1230,15 @@ def _serve_stream(server, models, arrivals, threads):
     return out, t_end - arrivals[0]
 
 
-def run_serve(args):
+def run_serve(args, nested=False):
+    """The serving configuration.  nested: a sub-record of the default line
+    (the process group already exists and stays up; no CPU baseline)."""
     import torch
     from betanoox_b200 import Server, _abi, opts
     from betanoox_b200 import workloads as W
     ws, rank, dev = _dist()
-    _init_dist(dev)
+    if not nested:
+        _init_dist(dev)
     t0 = time.perf_counter()
     pool_n = min(args.requests, args.serve_pool)
     models = [W.serve_request(args.seed + 1000 * rank, j) for j in range(pool_n)]
@@ -1240,70 +1323,62 @@ def run_serve(args):
             out["fp64_plain"] = fp64
             out["mixed_over_fp64"] = value / fp64["value"]
             out["capacity_over_fp64"] = cap_dofs / fp64["value"]
-        if not args.skip_cpu:
+        if not args.skip_cpu and not nested:
             thc = os.cpu_count() or 1
             n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s, thc)
             out["cpu_baseline"] = {"value": d / sec, "unit": UNIT, "cores": thc, "kind": "port",
                                    "sample": f"first {n} requests solved whole on the host, one at a time "
                                              f"({d} dofs in {sec:.1f} s): FP64 assembly + threaded Jacobi-PCG"}
     srv.close()
-    if ws > 1:
+    if ws > 1 and not nested:
         import torch.distributed as dist
         dist.destroy_process_group()
     return out
 
 
 def run_serve_reference(args):
+    """The request stream's first requests solved whole, one at a time, by the
+    reference's own code (oracle/_ref) within a time budget per step; each
+    bench step is one such sample.  Prints the unavailable line where
+    oracle/_ref is absent or does not load."""
     ws, rank, _ = _dist()
     if rank != 0:
         return None
+    from oracle import beta_oracle as bo
+    if not (bo.RefLeaf.available() and bo.RefEquations.available()):
+        return _unavailable("oracle/_ref (the reference's sources compiled here) is absent")
     from betanoox_b200 import workloads as W
     pool_n = min(args.requests, args.serve_pool)
     models = [W.serve_request(args.seed, j) for j in range(pool_n)]
     th = os.cpu_count() or 1
-    vals, last = [], None
-    ref, rvals, pvals = None, [], []
+    rvals, pvals, walls, ref = [], [], [], None
     try:
-        for k in range(1 + args.steps):
+        for k in range(args.warmup + max(1, args.steps)):
+            t0 = time.perf_counter()
             ref = reference_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
+            wall = time.perf_counter() - t0
             if ref is None or ref[0] == 0:
-                ref = None
-                break
-            if k >= 1:
+                return _unavailable("no request was solved by the reference's code within the step's budget")
+            if k >= args.warmup:
                 rvals.append(ref[1] / ref[2])
                 pvals.append(ref[1] / ref[3])
-    except OSError as e:  # oracle/_ref present but not loadable on this host
-        print(f"reference code unavailable ({e}); timing the port", file=sys.stderr)
-        ref = None
-    if ref is not None and rvals:
-        n, d, t_ref, t_port = ref
-        v = statistics.median(rvals)
-        return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * d / v, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
-                "config": {"workload": f"stream of {args.requests} requests (quad4 / hex8 elasticity / hex8 "
-                                       f"diffusion, log-uniform 1e3-5e5 dofs), solved one at a time"},
-                "cpu_baseline": {"value": v, "unit": UNIT, "cores": 2, "kind": "reference",
-                                 "sample": f"first {n} requests solved whole per step ({d} dofs, {t_ref:.1f} s) by "
-                                           f"the reference's own code compiled from its sources (oracle/_ref): "
-                                           f"its elements, Equations pattern + addMatrix, ParCG solve",
-                                 "port_all_cores": {"value": statistics.median(pvals), "unit": UNIT, "cores": th,
-                                                    "kind": "port", "sample": f"the same {n} requests ({t_port:.1f} s)"}},
-                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    for k in range(1 + args.steps):
-        n, d, sec = cpu_full_solves(models, args.tol, args.cpu_budget_s / max(1, args.steps), th)
-        if k >= 1:
-            vals.append(d / sec)
-            last = (n, d, sec)
-    v = statistics.median(vals)
-    n, d, sec = last
-    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * d / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp64", "data": "synthetic (seeded generator)", "impl": "reference",
-            "config": {"workload": f"stream of {args.requests} requests (quad4 / hex8 elasticity / hex8 diffusion, "
-                                   f"log-uniform 1e3-5e5 dofs), solved one at a time"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port",
-                             "sample": f"first {n} requests solved whole per step ({d} dofs, {sec:.1f} s)"},
+                walls.append(wall)
+    except OSError as e:
+        return _unavailable(f"oracle/_ref does not load on this host: {e}")
+    n, d, t_ref, t_port = ref
+    v = statistics.median(rvals)
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(walls), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded generator)",
+            "impl": "reference",
+            "config": {"workload": f"stream of {args.requests} requests (quad4 / hex8 elasticity / hex8 "
+                                   f"diffusion, log-uniform 1e3-5e5 dofs), solved one at a time"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 2, "kind": "reference",
+                             "sample": f"first {n} requests solved whole per step ({d} dofs, {t_ref:.1f} s) by "
+                                       f"the reference's own code compiled from its sources (oracle/_ref): "
+                                       f"its elements, Equations pattern + addMatrix, ParCG solve",
+                             "port_all_cores": {"value": statistics.median(pvals), "unit": UNIT, "cores": th,
+                                                "kind": "port", "sample": f"the same {n} requests ({t_port:.1f} s)"}},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -1322,14 +1397,13 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
-    ap.add_argument("--cpu-elems", type=int, default=100000)
-    ap.add_argument("--cpu-n", type=int, default=30)
-    ap.add_argument("--cpu-iters", type=int, default=30)
-    ap.add_argument("--cpu-assumed-iters", type=int, default=2000)
-    # the reference-code solve sample: a cube as large as the port's (its matrix
-    # out of cache), a loose stop rule only to bound the sample's iterations
-    ap.add_argument("--cpu-ref-n", type=int, default=30)
-    ap.add_argument("--cpu-ref-eps", type=float, default=1e-3)
+    # the oracle's accuracy reference: ||r||/||b|| of its FP64 solution
+    ap.add_argument("--oracle-tol", type=float, default=1e-12)
+    # the reference arm's bounded solves: iteration counts of the two samples
+    # per step, and the reference's solver (ParCG: its two-thread OpenMP one)
+    ap.add_argument("--ref-iters-a", type=int, default=2)
+    ap.add_argument("--ref-iters-b", type=int, default=6)
+    ap.add_argument("--ref-solver", default="parcg", choices=["parcg", "serial"])
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     # batch / serve
     ap.add_argument("--count", type=int, default=512)
@@ -1339,6 +1413,14 @@ def main():
     ap.add_argument("--check-every", type=int, default=32)
     ap.add_argument("--shape", default="", help="threads,gang_boost: skip the autotuner")
     ap.add_argument("--fp64-sample", type=int, default=512)
+    ap.add_argument("--fp64-stride", type=int, default=1, help="batch: plain FP64 on every k-th system")
+    # the batched and served forms inside the default (cube) line
+    ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--skip-serve", action="store_true")
+    ap.add_argument("--sub-steps", type=int, default=3)
+    ap.add_argument("--sub-warmup", type=int, default=3)
+    ap.add_argument("--sub-fp64-stride", type=int, default=4)
+    ap.add_argument("--sub-requests", type=int, default=1000)
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--serve-pool", type=int, default=1000)
     ap.add_argument("--capacity-requests", type=int, default=1000)
@@ -1355,6 +1437,7 @@ def main():
     ap.add_argument("--heat-steps", type=int, default=100)
     ap.add_argument("--dt", type=float, default=1e-3)
     ap.add_argument("--heat-tol", type=float, default=1e-9)
+    ap.add_argument("--heat-reassemble", action="store_true", help="assemble C/dt + K every step")
     ap.add_argument("--cpu-heat-nx", type=int, default=48)
     args = ap.parse_args()
     if args.warmup < 3:

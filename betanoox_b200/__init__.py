@@ -125,6 +125,11 @@ class Solver:
         self._check(self.lib.beta_gpu_matrix_lower_values(self.h, precision, _ptr(vals), _ptr(pl)), "lower_values")
         return vals, pl
 
+    def set_zero_diagonal(self, value):
+        """ReplaceZeroDiagonal: 0 refuses a zero global diagonal at the solve;
+        another value replaces every zero diagonal by it."""
+        self._check(self.lib.beta_gpu_set_zero_diagonal(self.h, float(value)), "set_zero_diagonal")
+
     def solve(self, o=None, raise_on_error=True):
         o = o or opts()
         st = SolveStats()

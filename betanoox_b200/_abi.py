@@ -108,6 +108,7 @@ SIGNATURES = {
     "beta_gpu_last_error": (C.c_char_p, [_P]),
     "beta_gpu_version": (_I, []),
     "beta_gpu_set_stream": (_I, [_P, _P]),
+    "beta_gpu_set_zero_diagonal": (_I, [_P, _D]),
     "beta_gpu_counters": (_I, [_P, C.POINTER(C.c_longlong), _I]),
     "beta_gpu_mesh_upload": (_I, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _I, _I]),
     "beta_gpu_materials_upload": (_I, [_P, _I, _I, _P, _P]),

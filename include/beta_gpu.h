@@ -195,6 +195,17 @@ BETA_GPU_API int beta_gpu_assemble(beta_gpu_ctx* ctx, int what, int precision, d
 BETA_GPU_API int beta_gpu_matrix_lower_values(beta_gpu_ctx* ctx, int precision, double* vals,
                                  double* pseudo_load);
 
+/* Equations::setReplaceZeroDiagonal_Option, the ReplaceZeroDiagonal command
+ * (equation.cpp:1819-1823), as LargeMatrix::CheckAndFixZeroDiagonal applies
+ * it when a solve starts (largeMatrix.cpp:43-79, sparse.cpp:127): with value
+ * 0 (the default) a zero global diagonal is refused (BETA_GPU_ERR_ZERODIAG,
+ * where the reference exits); with any other value every zero diagonal of
+ * the assembled matrix the solve uses (FP64, or FP32 for mixed precision,
+ * whose FP64 residual operator gets the same entry) becomes value before the
+ * solve, and stays so until the next assembly.  A negative diagonal below the
+ * first zero one is refused either way (BETA_GPU_ERR_NEGDIAG). */
+BETA_GPU_API int beta_gpu_set_zero_diagonal(beta_gpu_ctx* ctx, double value);
+
 /* ---- solve --------------------------------------------------------------- */
 /* Equations::solve: right-hand side = load + pseudo-load on free dofs,
  * prescribed values on restrained dofs; then PCG per opts.  The solution stays
@@ -506,9 +517,11 @@ BETA_GPU_API int beta_gpu_server_stats(beta_gpu_server* server, long long* out, 
  * Same arguments, algorithm and results as beta_gpu_csr_pcg_device, except:
  *   - n may not exceed BETA_GPU_NOALLOC_MAX_ROWS; larger systems return
  *     BETA_GPU_ERR_TOO_LARGE before any device work;
- *   - the first call on a device looks up the array's device address for that
- *     device (make that device current first, and make the first call before
- *     any stream capture);
+ *   - the first call on a device sets the array up there (loads the library's
+ *     module on that device and looks up the array's device address): make
+ *     that device current first, and make the first call before any stream
+ *     capture.  Every call looks the address up again (cheap after the first),
+ *     so a cudaDeviceReset between calls leaves no stale address behind;
  *   - all calls share the one array: calls that overlap on the GPU (other
  *     streams, other host threads) race and corrupt each other -- serialize them;
  *   - stats->ms_solve is not measured (0).

@@ -1,12 +1,15 @@
 """The bench's reference arm on the host: where the reference's own code was
-compiled (oracle/_ref), the cube's reference figure comes from it -- element
-B/addToKe, Equations pattern and addMatrix, and the faster of
-SymmetricSparseMatrix::solve and the two-thread ParCG solve -- with the
-oracle's all-core port beside it."""
+compiled (oracle/_ref), the cube's reference figure comes from it -- the
+whole system assembled once by its element code and Equations, and each step
+two of its Equations::solve calls on that full system, stopped after a known
+number of iterations -- and the product library is never loaded."""
+import json
 import os
+import subprocess
 import sys
 from types import SimpleNamespace
 
+import numpy as np
 import pytest
 
 from betanoox_b200 import workloads as W
@@ -14,37 +17,69 @@ from betanoox_b200 import workloads as W
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def test_reference_code_baseline_times_the_reference(oracle):
+def _need_ref(oracle):
     if not (oracle.RefLeaf.available() and oracle.RefEquations.available()):
         pytest.skip("oracle/_ref not built (reference tree absent)")
+
+
+def test_eps_after_picks_a_first_crossing():
     sys.path.insert(0, ROOT)
     import bench
-    m = W.cube_hex8(6, seed=2)
-    args = SimpleNamespace(cpu_elems=64, cpu_ref_n=4, cpu_ref_eps=1e-6)
-    cb = bench.reference_code_baseline(m, args, 100)
-    assert cb["kind"] == "reference" and cb["cores"] in (1, 2)
-    assert cb["value"] > 0 and cb["seconds_full_solve_est"] > 0
-    assert "SymmetricSparseMatrix::solve" in cb["sample"] and "ParCGMatrix::solve" in cb["sample"]
+    tr = [10.0, 5.0, 6.0, 4.0, 3.0, 3.0, 1.0]
+    assert bench._eps_after(tr, 2)[0] == 2
+    assert bench._eps_after(tr, 3)[0] == 4          # 6.0 is not below 5.0
+    assert bench._eps_after(tr, 6)[0] == 7          # 3.0 repeats: not below the earlier 3.0
+    assert bench._eps_after(tr, 8) is None
+    k, eps = bench._eps_after(tr, 4)
+    assert all(v > eps for v in tr[:k - 1]) and tr[k - 1] < eps
 
 
-def test_reference_arm_prints_one_json_line():
+@pytest.mark.parametrize("solver", ["parcg", "serial"])
+def test_reference_cube_setup_and_step(oracle, solver):
+    """The setup's bounded solve is checked against the oracle's iterate; a
+    step gives a positive rate whose full solve covers the measured count."""
+    _need_ref(oracle)
+    sys.path.insert(0, ROOT)
+    import bench
+    m = W.cube_hex8(8, seed=2)
+    args = SimpleNamespace(tol=1e-10, ref_iters_a=2, ref_iters_b=6, ref_solver=solver)
+    R = bench.reference_cube_setup(m, args)
+    assert R["check"] <= 1e-9 and R["kb"] > R["ka"] >= 2
+    # the count is the oracle's full solve of the same system to ||r||/||b|| <= tol
+    s = oracle.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    s.assemble(m.params, m.order)
+    rc, x, st, _ = s.csr().pcg(s.rhs(), 1e-10, rule=oracle.Csr.RULE_RB, threads=2)
+    assert rc == 0 and abs(st.iterations - R["iters_full"]) <= 2
+    v, wall, t_it, t_fix = bench.reference_cube_step(R, m.ndof)
+    R["rs"].close()
+    assert v > 0 and wall > 0 and t_it > 0 and t_fix >= 0
+
+
+def test_reference_arm_prints_one_json_line_without_the_product(oracle):
     """bench.py --impl reference on a small cube: standard output is exactly
     one JSON line (the reference code's own messages are kept off it), with
-    the reference's figure and, where oracle/_ref exists, the port beside it."""
-    import json
-    import subprocess
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0", "--n", "12", "--cpu-elems", "500", "--cpu-ref-n", "6", "--cpu-n", "8",
-                        "--cpu-iters", "5"], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    the same config record as the GPU arm, and libbeta_gpu.so is never mapped
+    into the process."""
+    _need_ref(oracle)
+    code = ("import sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '2', '--warmup', '1', "
+            "'--n', '10']; import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "sys.stderr.write('PRODUCT_MAPPED=%d\\n' % ('libbeta_gpu' in maps))")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT)
     assert r.returncode == 0, r.stderr
     lines = r.stdout.strip().splitlines()
     assert len(lines) == 1, r.stdout
+    assert "PRODUCT_MAPPED=0" in r.stderr
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["value"] == d["value"]
-    cb = d["cpu_baseline"]
-    assert cb["kind"] in ("reference", "port")
-    if cb["kind"] == "reference":
-        assert cb["port_all_cores"]["kind"] == "port"
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] == 2
+    sys.path.insert(0, ROOT)
+    import bench
+    args = SimpleNamespace(tol=1e-10, inner_tol=0.01)
+    assert d["config"] == json.loads(json.dumps(bench.cube_config(W.cube_hex8(10), args, 1)))
+    assert d["ms_per_step"] * d["steps"] < 60e3
 
 
 def test_reference_full_solves_run_the_reference(oracle):

@@ -68,6 +68,44 @@ def test_noalloc_matches_allocating_solver_twice(oracle):
             assert st.true_rel_residual <= 1e-11
 
 
+def test_noalloc_larger_then_smaller_system(oracle):
+    """A smaller system right after a larger one: the shared array still holds
+    the larger system's vectors past the smaller one's n, and a different grid
+    size leaves other reduction partials behind.  Both answers must equal the
+    allocating solver's."""
+    lib = _abi.load()
+    big, small = W.cube_hex8(8, seed=5), W.plate_quad4(10)
+    nb, tb = _device_system(oracle, big)
+    ns, ts = _device_system(oracle, small)
+    assert nb > 4 * ns
+    ref = {}
+    for key, (n, t) in (("big", (nb, tb)), ("small", (ns, ts))):
+        rc0, x0, st0 = _solve(lib.beta_gpu_csr_pcg_device, n, t)
+        assert rc0 == _abi.OK
+        ref[key] = (x0, st0.iterations)
+    # no allocating call between the two allocation-free ones
+    got = {}
+    for key, (n, t) in (("big", (nb, tb)), ("small", (ns, ts))):
+        rc, x, st = _solve(lib.beta_gpu_csr_pcg_device_noalloc, n, t)
+        assert rc == _abi.OK, st.as_dict()
+        got[key] = (x, st.iterations)
+    for key in ("big", "small"):
+        x0, it0 = ref[key]
+        x, it = got[key]
+        assert np.linalg.norm(x - x0) <= 1e-12 * np.linalg.norm(x0), key
+        assert it == it0, key
+
+
+def test_noalloc_bad_arguments_report_status():
+    lib = _abi.load()
+    st = _abi.SolveStats()
+    st.status = 12345
+    rc = lib.beta_gpu_csr_pcg_device_noalloc(0, None, None, None, None, None, _abi.STOP_RB, 1e-10, 10, None,
+                                             C.byref(st))
+    assert rc == _abi.ERR_ARG
+    assert st.status == _abi.ERR_ARG
+
+
 def test_noalloc_rejects_oversized_systems():
     import torch
     lib = _abi.load()
