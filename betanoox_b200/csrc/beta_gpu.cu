@@ -424,6 +424,14 @@ struct ProfAcc {
 
 // Runs PCG iterations in chunks until the device state says done.  kind 0:
 // scalar FP64; kind ND (1..3): node-block FP32.
+// With profiling on, the SpMV launches at k = kProfEvery/2, 3 kProfEvery/2, ...
+// of each chunk are bracketed by events (a sample: an event pair around every
+// launch costs the iteration a few microseconds).
+constexpr int kProfEvery = 16;
+inline bool prof_sample(int k, int ce) {
+  return ce < kProfEvery ? k == ce / 2 : k % kProfEvery == kProfEvery / 2;
+}
+
 template <int ND>
 int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
   const int ce = std::max(1, check_every);
@@ -431,7 +439,8 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
   if (prof && prof->on && (rc = ensure_events(c, 2 * ce)) != BETA_GPU_OK) return rc;
   for (;;) {
     for (int k = 0; k < ce; ++k) {
-      if (prof && prof->on) CK(cudaEventRecord(c->evs[2 * k], c->stream));
+      const bool sample = prof && prof->on && prof_sample(k, ce);
+      if (sample) CK(cudaEventRecord(c->evs[2 * k], c->stream));
       if constexpr (ND == 0) {
         ScalarMat A{c->ndof, c->P.nsslice, c->ssoff.p, c->scol.p, c->sval.p};
         launch(c, k_spmv_dot_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, 
@@ -441,7 +450,7 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
         launch(c, k_spmv_dot_b<ND>, grid_for(c, (long long)c->P.nslice * 32, 256), 256, 0,
             A, (const float*)c->v32[2].p, c->v32[3].p, c->st.p, c->partials.p);
       }
-      if (prof && prof->on) CK(cudaEventRecord(c->evs[2 * k + 1], c->stream));
+      if (sample) CK(cudaEventRecord(c->evs[2 * k + 1], c->stream));
       if constexpr (ND == 0) {
         launch(c, k_update_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->x64.p, c->r64.p, c->p64.p,
                                                                      c->q64.p, c->d64.p, c->st.p, c->partials.p);
@@ -461,6 +470,7 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
     if (prof && prof->on) {
       int real = std::min(ce, std::max(0, s.iter - before) + (s.done && s.status == kStatusBreakdown ? 1 : 0));
       for (int k = 0; k < real; ++k) {
+        if (!prof_sample(k, ce)) continue;
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->evs[2 * k], c->evs[2 * k + 1]));
         prof->ms += ms;
@@ -1287,6 +1297,9 @@ int beta_gpu_solve(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, beta_gpu_solve
     if (stats && (status == BETA_GPU_OK || status == BETA_GPU_MAXIT)) {
       // true FP64 residual of the returned iterate
       if ((rc = mf_apply(c, 1.0, c->x64.p, 0.0, nullptr, 0.0, c->y64.p))) return rc;
+      if (c->zrep_on)
+        launch(c, k_zdiag_apply, grid_for(c, n, 256), 256, 0, n, (const unsigned char*)c->zrep.p, c->zdiag,
+               (const double*)c->x64.p, c->y64.p);
       launch(c, k_residual64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->load.p, c->y64.p, c->x64.p,
                                                               c->r64.p, c->sums.p, c->partials.p, c->ticket.p);
       double s2[2];

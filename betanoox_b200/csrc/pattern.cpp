@@ -39,7 +39,7 @@ static void parallel_for(long long n, const std::function<void(long long, long l
 // Empties every output of P but keeps the memory of its vectors.
 static void reset_keep(HostPattern& P) {
   P.nnode = P.nelem = P.nnpe = P.ndpn = P.ndof = 0;
-  for (auto* v : {&P.nrp, &P.ndiag, &P.color_ptr, &P.elem_by_color, &P.bsoff, &P.soff, &P.srowlen})
+  for (auto* v : {&P.nrp, &P.ndiag, &P.color_ptr, &P.elem_by_color, &P.bsoff, &P.soff, &P.srowlen, &P.unused})
     v->clear();
   P.scol.clear();
   P.ncol.clear();
@@ -167,6 +167,10 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     }
   });
 
+  P.unused.clear();
+  for (int i = 0; i < nnode; ++i)
+    if (icnt[i] == icnt[i + 1]) P.unused.push_back(i);
+
   // ---- node graph (two passes: count, then fill) ---------------------
   // Neighbours of node i are deduplicated with a per-thread marker array
   // (mark[J] == stamp once J is taken; the stamps of the two passes differ),
@@ -273,6 +277,10 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
       int* bc = P.bcol.data() + (size_t)P.bsoff[s] * 32 + (i % 32);
       for (int k = 0; k < len; ++k) bc[(size_t)k * 32] = buf[k];
       for (int k = len; k < w; ++k) bc[(size_t)k * 32] = (int)i;
+      if (icnt[i] == icnt[i + 1]) {  // a node in no element: its rows hold the diagonal alone
+        acc += ndpn;
+        continue;
+      }
       long long below = 0;
       for (int k = 0; k < d; ++k) below += ufree[buf[k]];
       int own = 0;
@@ -306,6 +314,10 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   return msg;
 }
 
+static bool node_unused(const HostPattern& P, int I) {
+  return !P.unused.empty() && std::binary_search(P.unused.begin(), P.unused.end(), I);
+}
+
 std::string build_scalar(HostPattern& P, const unsigned char* rest) {
   const int nnode = P.nnode, ndpn = P.ndpn;
   const int ndof = P.ndof;
@@ -332,7 +344,7 @@ std::string build_scalar(HostPattern& P, const unsigned char* rest) {
     for (long long s = lo; s < hi; ++s) {
       int w = 0;
       for (int r = (int)s * 32; r < std::min(ndof, (int)s * 32 + 32); ++r) {
-        const int len = rest[r] ? 1 : nodelen[r / ndpn];
+        const int len = (rest[r] || node_unused(P, r / ndpn)) ? 1 : nodelen[r / ndpn];
         P.srowlen[r] = len;
         acc += len;
         w = std::max(w, len);
@@ -355,7 +367,7 @@ std::string build_scalar(HostPattern& P, const unsigned char* rest) {
         long long base = P.ssoff[s] + lane;
         int k = 0;
         if (r < ndof) {
-          if (rest[r]) {
+          if (rest[r] || node_unused(P, r / ndpn)) {
             P.scol[base] = r;
             P.sdiag[r] = base;
             k = 1;
@@ -386,7 +398,7 @@ void export_lower_pattern(const HostPattern& P, const unsigned char* rest, long 
   const int nd = P.ndpn;
   for (int r = 0; r < P.ndof; ++r) {
     row_ptr[r] = p;
-    if (rest[r]) { col[p++] = r; continue; }
+    if (rest[r] || node_unused(P, r / nd)) { col[p++] = r; continue; }
     int I = r / nd;
     long long start = p;
     for (int k = P.nrp[I]; k < P.nrp[I + 1]; ++k) {
@@ -407,7 +419,7 @@ void export_lower_values_scalar(const HostPattern& P, const unsigned char* rest,
   const int nd = P.ndpn;
   for (int r = 0; r < P.ndof; ++r) {
     long long base = P.ssoff[r / 32] + (r % 32);
-    if (rest[r]) { out[p++] = sval[P.sdiag[r]]; continue; }
+    if (rest[r] || node_unused(P, r / nd)) { out[p++] = sval[P.sdiag[r]]; continue; }
     int I = r / nd;
     int k = 0;
     for (int q = P.nrp[I]; q < P.nrp[I + 1]; ++q) {
@@ -430,7 +442,7 @@ void export_lower_values_block(const HostPattern& P, const unsigned char* rest, 
     int I = r / nd, i = r % nd;
     long long chunk0 = P.bsoff[I / 32];
     int lane = I % 32;
-    if (rest[r]) {
+    if (rest[r] || node_unused(P, I)) {
       long long ch = chunk0 + P.ndiag[I];
       out[p++] = bval[ch * 32 * bb + (long long)(i * nd + i) * 32 + lane];
       continue;

@@ -58,6 +58,10 @@ struct HostPattern {
   FillVec<int> ncol;          // nblk
   std::vector<int> ndiag;     // position of node i in its own row
   long long nblk = 0;
+  // nodes that no element uses, ascending: their rows are the diagonal alone
+  // in the reference's pattern (Equations gives an empty row its diagonal),
+  // while the node graph keeps their (zero) diagonal block
+  std::vector<int> unused;
 
   // element colouring
   int ncolor = 0;

@@ -78,6 +78,27 @@ def test_host_pattern_ragged_restraints(abi, oracle):
     np.testing.assert_array_equal(col, col2)
 
 
+@pytest.mark.parametrize("make", [lambda: W.plate_quad4(4), lambda: W.cube_hex8(3, seed=7),
+                                  lambda: W.heat_slab(4, 3, 3)])
+def test_host_pattern_unused_free_node(abi, oracle, make):
+    """A node no element uses, its dofs left free: Equations gives each of its
+    (empty) rows the diagonal alone -- no entries between its own dofs."""
+    import dataclasses
+    m = W.renumbered(make(), 2, unused_node=True)
+    r = m.restrained.copy()
+    r[-m.ndpn:] = 0
+    m = dataclasses.replace(m, restrained=r)
+    s = oracle.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    rp, col, _ = s.export_lower()
+    rp2, col2 = _host_pattern(abi, m)
+    np.testing.assert_array_equal(rp, rp2)
+    np.testing.assert_array_equal(col, col2)
+    for r in range(m.ndof - m.ndpn, m.ndof):
+        assert list(col2[rp2[r]:rp2[r + 1]]) == [r]
+
+
 def test_host_pattern_rejects_bad_numbering(abi):
     m = W.cube_hex8(2)
     conn = np.ascontiguousarray(m.conn, np.int32)

@@ -59,7 +59,9 @@ def test_zero_diagonal_refused_then_replaced(oracle, base):
     # the matrix keeps the replacement (SymmetricSparseMatrix after the solve)
     vals, _ = g.lower_values(_abi.FP64)
     rp, col, val = s.export_lower()
-    np.testing.assert_allclose(vals[rp[1:] - 1], val[rp[1:] - 1], rtol=1e-12, atol=0)
+    dg, do = vals[rp[1:] - 1], val[rp[1:] - 1]
+    bad = np.nonzero(np.abs(dg - do) > 1e-12 * np.abs(do))[0]
+    assert len(bad) == 0, [(int(i), float(dg[i]), float(do[i]), int(m.restrained[i])) for i in bad[:8]]
     # mixed precision: FP32 matrix replaced, FP64 residual operator with the same entry
     g.assemble(_abi.FP32)
     rc, st = g.solve(opts(mode=_abi.MODE_MPIR, tol=1e-12))
