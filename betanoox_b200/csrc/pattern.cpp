@@ -13,6 +13,13 @@ static thread_local bool t_serial = false;
 void pattern_serial_on_this_thread(bool on) { t_serial = on; }
 
 // Number of contiguous chunks parallel_chunks splits n items into.
+// Bytes the node-sized marker arrays of the node-graph passes may take in all
+// (a test build sets 0 to run the bandwidth-sized form on every mesh, and
+// BETA_PATTERN_SPAN_CAP=0 as well to sort and deduplicate every row).
+#ifndef BETA_PATTERN_MARK_BUDGET
+#define BETA_PATTERN_MARK_BUDGET (512LL << 20)
+#endif
+
 static int chunk_count(long long n) {
   unsigned hw = std::thread::hardware_concurrency();
   int t = (int)std::min<unsigned>(hw ? hw : 1, 64);
@@ -172,33 +179,75 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     if (icnt[i] == icnt[i + 1]) P.unused.push_back(i);
 
   // ---- node graph (two passes: count, then fill) ---------------------
-  // Neighbours of node i are deduplicated with a per-thread marker array
-  // (mark[J] == stamp once J is taken; the stamps of the two passes differ),
-  // so only the distinct ones are sorted.
-  auto collect = [&](int i, std::vector<int>& buf, std::vector<int>& mark, int stamp, bool sorted) {
+  // Neighbours of node i are deduplicated with a marker array (mark[J - lo]
+  // == stamp once J is taken; the stamps of the two passes differ), so only
+  // the distinct ones are sorted.  Each chunk of rows has its own marker and
+  // position arrays: node-sized ones (kept between builds of a solver
+  // context) while all of them fit in kMarkBudget bytes; beyond that each
+  // chunk marks within the span of node ids its rows reach, which follows
+  // the numbering's bandwidth, and a chunk whose span is still wider than
+  // kSpanCap sorts and deduplicates each row instead.
+  struct Span { int lo = 0, hi = -1; };
+  const int nck = chunk_count(nnode);
+  constexpr long long kMarkBudget = BETA_PATTERN_MARK_BUDGET;
+  const bool node_sized = 2LL * nck * nnode * (long long)sizeof(int) <= kMarkBudget;
+#ifdef BETA_PATTERN_SPAN_CAP
+  const long long kSpanCap = BETA_PATTERN_SPAN_CAP;  // a test build: 0 sorts every row
+#else
+  const long long kSpanCap = 4LL * ((nnode + nck - 1) / nck) + 65536;
+#endif
+  std::vector<Span> span(nck);
+  if (node_sized) {
+    P.s_mark.resize(2 * nck);  // per chunk: the marker, and the positions of the current row
+  } else {
+    std::vector<std::vector<int>>().swap(P.s_mark);
+  }
+  auto collect = [&](int i, std::vector<int>& buf, int* mark, int lo, int stamp) {
     buf.clear();
     for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
       const int* ce = conn + (long long)inc[k] * nnpe;
-      for (int a = 0; a < nnpe; ++a) {
-        const int J = ce[a];
-        if (mark[J] != stamp) {
-          mark[J] = stamp;
-          buf.push_back(J);
+      if (mark) {
+        for (int a = 0; a < nnpe; ++a) {
+          const int J = ce[a];
+          if (mark[J - lo] != stamp) {
+            mark[J - lo] = stamp;
+            buf.push_back(J);
+          }
         }
+      } else {
+        buf.insert(buf.end(), ce, ce + nnpe);
       }
     }
     if (buf.empty()) buf.push_back(i);  // a node in no element keeps its diagonal
-    if (sorted) std::sort(buf.begin(), buf.end());
+    std::sort(buf.begin(), buf.end());
+    if (!mark) buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
   };
-  const int nck = chunk_count(nnode);
-  P.s_mark.resize(2 * nck);  // per chunk: the marker, and the positions of the current row
   P.nrp.assign(nnode + 1, 0);
   parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
-    std::vector<int> buf;
-    std::vector<int>& mark = P.s_mark[ck];
-    mark.assign(nnode, 0);
+    std::vector<int> buf, local;
+    int* mark = nullptr;
+    Span sp{0, nnode - 1};
+    if (node_sized) {
+      P.s_mark[ck].assign(nnode, 0);
+      mark = P.s_mark[ck].data();
+    } else {
+      sp = Span{(int)lo, (int)hi - 1};
+      for (long long i = lo; i < hi; ++i)
+        for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
+          const int* ce = conn + (long long)inc[k] * nnpe;
+          for (int a = 0; a < nnpe; ++a) {
+            sp.lo = std::min(sp.lo, ce[a]);
+            sp.hi = std::max(sp.hi, ce[a]);
+          }
+        }
+      if ((long long)sp.hi - sp.lo + 1 <= kSpanCap) {
+        local.assign((size_t)(sp.hi - sp.lo + 1), 0);
+        mark = local.data();
+      }
+    }
+    span[ck] = sp;
     for (long long i = lo; i < hi; ++i) {
-      collect((int)i, buf, mark, (int)i + 1, false);
+      collect((int)i, buf, mark, sp.lo, (int)i + 1);
       P.nrp[i + 1] = (int)buf.size();
     }
   });
@@ -251,25 +300,38 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   P.bcol.resize((size_t)P.nchunk * 32);
   std::vector<long long> lower(nck, 0);
   parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
-    std::vector<int> buf;
-    std::vector<int>& mark = P.s_mark[ck];
-    std::vector<int>& pos = P.s_mark[nck + ck];
-    if ((long long)pos.size() < nnode) pos.resize(nnode);
+    const Span sp = span[ck];
+    std::vector<int> buf, local_mark, local_pos;
+    int *mark = nullptr, *pos = nullptr;
+    if (node_sized) {
+      std::vector<int>& pv = P.s_mark[nck + ck];
+      if ((long long)pv.size() < nnode) pv.resize(nnode);
+      mark = P.s_mark[ck].data();
+      pos = pv.data();
+    } else if ((long long)sp.hi - sp.lo + 1 <= kSpanCap) {
+      local_mark.assign((size_t)(sp.hi - sp.lo + 1), 0);
+      local_pos.resize((size_t)(sp.hi - sp.lo + 1));
+      mark = local_mark.data();
+      pos = local_pos.data();
+    }
     long long acc = 0;
     for (long long i = lo; i < hi; ++i) {
-      collect((int)i, buf, mark, nnode + (int)i + 1, true);
+      collect((int)i, buf, mark, sp.lo, nnode + (int)i + 1);
       const int len = (int)buf.size();
       std::copy(buf.begin(), buf.end(), P.ncol.begin() + P.nrp[i]);
       const int d = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
       P.ndiag[i] = d;
-      for (int k = 0; k < len; ++k) pos[buf[k]] = k;
+      if (pos)
+        for (int k = 0; k < len; ++k) pos[buf[k] - sp.lo] = k;
       for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
         const long long e = inc[k];
         const int* ce = conn + e * nnpe;
         for (int a = 0; a < nnpe; ++a) {
           if (ce[a] != (int)i) continue;
           uint16_t* sl = P.slot.data() + e * npair + a * nnpe;
-          for (int b = 0; b < nnpe; ++b) sl[b] = (uint16_t)pos[ce[b]];
+          for (int b = 0; b < nnpe; ++b)  // J's position in the sorted row
+            sl[b] = (uint16_t)(pos ? pos[ce[b] - sp.lo]
+                                   : std::lower_bound(buf.begin(), buf.end(), ce[b]) - buf.begin());
         }
       }
       const long long s = i / 32;

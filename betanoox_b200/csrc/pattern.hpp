@@ -99,7 +99,7 @@ struct HostPattern {
   bool keep_scratch = false;
   std::vector<int> s_icnt, s_inc, s_color, s_ufree, s_ccnt;
   std::vector<uint64_t> s_used;
-  std::vector<std::vector<int>> s_mark;  // one marker array per build thread
+  std::vector<std::vector<int>> s_mark;  // node-sized marker and position arrays per chunk (within a budget)
 };
 
 // Builds everything above.  conn: nelem*nnpe; restrained: ndof (0/1).

@@ -5,7 +5,9 @@
 // with 3 and 1 dofs per node, natural and shuffled node numberings, and a
 // quad4 plate with an unused node and a degenerate element (a repeated
 // node).  Each mesh is also built single-threaded, which must give the same
-// result.  Exit code 0 when every build matches.
+// result, and a hash of every field is printed, so that a build compiled with
+// BETA_PATTERN_MARK_BUDGET=0 (the bandwidth-sized marker form on every mesh)
+// can be compared with the default one.  Exit code 0 when every build matches.
 #include "../../betanoox_b200/csrc/pattern.hpp"
 
 #include <algorithm>
@@ -28,6 +30,16 @@ static bool equal(const HostPattern& P, const HostPattern& Q) {
          P.nchunk == Q.nchunk && P.nsslice == Q.nsslice && same(P.ssoff, Q.ssoff) && same(P.scol, Q.scol) &&
          same(P.soff, Q.soff) && same(P.srowlen, Q.srowlen) && same(P.sdiag, Q.sdiag) &&
          P.nnz_full == Q.nnz_full && P.nnz_lower == Q.nnz_lower;
+}
+
+static unsigned long long hash_of(const HostPattern& P) {
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&](long long v) { h ^= (unsigned long long)v; h *= 1099511628211ull; };
+  auto all = [&](const auto& a) { mix((long long)a.size()); for (size_t i = 0; i < a.size(); ++i) mix(a[i]); };
+  all(P.nrp); all(P.ncol); all(P.ndiag); all(P.color_ptr); all(P.elem_by_color); all(P.slot); all(P.bsoff);
+  all(P.bcol); all(P.ssoff); all(P.scol); all(P.soff); all(P.srowlen); all(P.sdiag); all(P.unused);
+  mix(P.nblk); mix(P.ncolor); mix(P.nchunk); mix(P.nnz_full); mix(P.nnz_lower);
+  return h;
 }
 
 struct Mesh {
@@ -107,9 +119,16 @@ int main() {
     const std::string e3 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, M.conn.data(), fd.data(),
                                                   M.rest.data(), serial, true);
     betagpu::pattern_serial_on_this_thread(false);
+#if defined(BETA_PATTERN_MARK_BUDGET) && BETA_PATTERN_MARK_BUDGET == 0
+    const bool marks_kept = reused.s_mark.empty();  // nothing node-sized is held
+#else
+    const bool marks_kept = !reused.s_mark.empty();
+#endif
     const bool ok = e1.empty() && e2.empty() && e3.empty() && equal(fresh, reused) && equal(fresh, serial) &&
-                    fresh.s_mark.empty() && !reused.s_mark.empty();
+                    same(fresh.unused, reused.unused) && same(fresh.unused, serial.unused) &&
+                    fresh.s_mark.empty() && marks_kept;
     std::printf("%-60s %s\n", M.name.c_str(), ok ? "equal" : "DIFFERENT");
+    std::printf("hash %-55s %016llx\n", M.name.c_str(), hash_of(fresh));
     bad += ok ? 0 : 1;
   }
   // invalid input is refused with its message, on any thread count

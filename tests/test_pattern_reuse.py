@@ -8,12 +8,25 @@ import subprocess
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def test_reused_pattern_equals_fresh_build(tmp_path):
-    exe = os.path.join(str(tmp_path), "pattern_reuse_check")
-    subprocess.run(["g++", "-std=c++17", "-O2", "-pthread", "-Wall",
+def _run(tmp_path, name, extra):
+    exe = os.path.join(str(tmp_path), name)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-pthread", "-Wall", *extra,
                     os.path.join(ROOT, "tests", "cpp", "pattern_reuse_check.cpp"),
                     os.path.join(ROOT, "betanoox_b200", "csrc", "pattern.cpp"), "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count("equal") == 7
+    assert r.stdout.count(" equal") == 7
     assert "NOT REFUSED" not in r.stdout and r.stdout.count("refused") == 1
+    return [line for line in r.stdout.splitlines() if line.startswith("hash ")]
+
+
+def test_reused_pattern_equals_fresh_build(tmp_path):
+    """Also: the node-graph passes' bandwidth-sized marker form (used when
+    node-sized markers would exceed their memory budget) and their
+    sort-per-row form (a span too wide even for that) build the same pattern,
+    field for field, as the node-sized form."""
+    default = _run(tmp_path, "pattern_reuse_check", [])
+    bounded = _run(tmp_path, "pattern_reuse_check_bounded", ["-DBETA_PATTERN_MARK_BUDGET=0"])
+    sorted_rows = _run(tmp_path, "pattern_reuse_check_sorted", ["-DBETA_PATTERN_MARK_BUDGET=0",
+                                                                  "-DBETA_PATTERN_SPAN_CAP=0"])
+    assert len(default) == 7 and default == bounded == sorted_rows
