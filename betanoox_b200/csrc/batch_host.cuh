@@ -197,7 +197,7 @@ cudaLaunchConfig_t batch_cfg(beta_gpu_batch* b, int grid, cudaLaunchAttribute* a
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid, 1, 1);
   cfg.blockDim = dim3(T, 1, 1);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = stage_bytes<T>();
   cfg.stream = b->stream;
   attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: gang barriers can complete
   attr[0].val.cooperative = 1;
@@ -210,7 +210,13 @@ cudaLaunchConfig_t batch_cfg(beta_gpu_batch* b, int grid, cudaLaunchAttribute* a
 template <int T>
 int batch_ctas_raw(beta_gpu_batch* b) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve<T>, T, 0) != cudaSuccess) {
+  // the matrix staging ring is dynamic shared memory beyond the default 48 KB
+  if (cudaFuncSetAttribute(k_batch_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes<T>()) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve<T>, T, stage_bytes<T>()) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }

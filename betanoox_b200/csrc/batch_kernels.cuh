@@ -334,80 +334,113 @@ __device__ __forceinline__ bool b_rz(const BSys& S, const Grp& g, double* part, 
 // the differences of a smooth p carry no cancellation.  Padding entries hold
 // zeros, so their column does not matter.
 
-// One 32-node slice of q = A p_new in FP32 with the direction update folded
-// into the gather: p_new[J] = fmaf(bt, p_old[J], z[J]) for every column J --
-// the same arithmetic, and so the same bits, as updating p in a separate
-// pass.  Saves a pass over the vectors and a group barrier per iteration.
-// pI receives p_new of the lane's own node.  RS: the matrix is in row-sum
-// form (else the plain assembled one).
-template <int ND, bool RS>
-__device__ __forceinline__ void spmv_row_fused(const BlockMat& A, int s, int lane, const float* pold,
-                                               const float* z, float bt, float* acc, float* pI) {
+// ---- matrix chunks staged in shared memory --------------------------------
+// A warp multiplies its slice chunk by chunk; chunk k's 32 column indices and
+// 32*ND*ND values (contiguous in the sliced layout, 256-byte aligned pool
+// regions) are copied into a per-warp ring of kDepth chunks with 16-byte
+// cp.async.cg, kDepth-1 chunks ahead of the one being multiplied.  The copies
+// in flight live in shared memory, not registers, so a warp keeps several
+// chunks of HBM traffic in flight with few warps per SM (loads into registers,
+// two chunks ahead, left the one-CTA-per-SM kernel at about half of HBM).
+// The arithmetic and its order are unchanged by the staging.  cp.async.cg reads
+// through L2, where the matrix written earlier in the launch (assembly, row
+// sums) is visible after the group barrier.
+constexpr int kStageFloats = 32 * (1 + 9);  // one chunk of the widest (3 dofs per node) layout
+
+template <int T>
+__host__ __device__ constexpr int stage_depth() { return T >= 1024 ? 3 : 4; }
+
+template <int T>
+__host__ __device__ constexpr size_t stage_bytes() {
+  return (size_t)(T / 32) * stage_depth<T>() * kStageFloats * sizeof(float);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Chunk (cols: 32 ints, vals: 32*ND*ND floats) into dst: cols first, then vals.
+template <int ND>
+__device__ __forceinline__ void stage_chunk(float* dst, const int* cols, const float* vals, int lane) {
+  constexpr int kPieces = 8 + 8 * ND * ND;  // 16-byte pieces
+  for (int q = lane; q < kPieces; q += 32) {
+    const void* src = q < 8 ? (const void*)(cols + 4 * q) : (const void*)(vals + 4 * (q - 8));
+    cp_async16(dst + 4 * q, src);
+  }
+}
+
+// One 32-node slice of q = A p in FP32.  FUSED: the direction update is
+// folded into the gather, p_new[J] = fmaf(bt, p_old[J], z[J]) for every
+// column J -- the same arithmetic, and so the same bits, as updating p in a
+// separate pass; pI receives p_new of the lane's own node.  Otherwise p was
+// written before the pass and pI receives p[I].  RS: the matrix is in
+// row-sum form (else the plain assembled one).  ring: this warp's
+// kDepth * kStageFloats floats.
+template <int ND, bool RS, bool FUSED, int D>
+__device__ __forceinline__ void spmv_row_staged(const BlockMat& A, int s, int lane, const float* p, const float* z,
+                                                float bt, float* acc, float* pI, float* ring) {
   constexpr int BB = ND * ND;
   const int I = 32 * s + lane;
   const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
-  const int* cp = A.bcol + (long long)c0 * 32 + lane;
-  const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
+  const int* cb = A.bcol + (long long)c0 * 32;
+  const float* vb = A.bval + (long long)c0 * 32 * BB;
 #pragma unroll
   for (int i = 0; i < ND; ++i) { acc[i] = 0.f; pI[i] = 0.f; }
   if (I < A.nnode) {
-    float po[ND], zv[ND];
-    PVec<ND>::ld(pold, I, po);
-    PVec<ND>::ld(z, I, zv);
+    if constexpr (FUSED) {
+      float po[ND], zv[ND];
+      PVec<ND>::ld(p, I, po);
+      PVec<ND>::ld(z, I, zv);
 #pragma unroll
-    for (int i = 0; i < ND; ++i) pI[i] = fmaf(bt, po[i], zv[i]);
+      for (int i = 0; i < ND; ++i) pI[i] = fmaf(bt, po[i], zv[i]);
+    } else {
+      PVec<ND>::ld(p, I, pI);
+    }
   }
-#pragma unroll 2
+#pragma unroll
+  for (int k = 0; k < D - 1; ++k) {
+    if (k < w) stage_chunk<ND>(ring + k * kStageFloats, cb + k * 32, vb + (long long)k * 32 * BB, lane);
+    cp_async_commit();  // empty groups keep the count uniform
+  }
   for (int k = 0; k < w; ++k) {
-    const int J = __ldcs(cp + k * 32);
-    float po[ND], zv[ND];
-    PVec<ND>::ld(pold, J, po);
-    PVec<ND>::ld(z, J, zv);
+    const int kn = k + D - 1;
+    if (kn < w) stage_chunk<ND>(ring + (kn % D) * kStageFloats, cb + kn * 32, vb + (long long)kn * 32 * BB, lane);
+    cp_async_commit();
+    cp_async_wait<D - 1>();  // chunk k's copies of this lane have landed
+    __syncwarp();            // ... and every lane's
+    const float* st = ring + (k % D) * kStageFloats;
+    const int J = reinterpret_cast<const int*>(st)[lane];
     float v[BB];
 #pragma unroll
-    for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);
+    for (int t = 0; t < BB; ++t) v[t] = st[32 + t * 32 + lane];
     float d[ND];
+    if constexpr (FUSED) {
+      float po[ND], zv[ND];
+      PVec<ND>::ld(p, J, po);
+      PVec<ND>::ld(z, J, zv);
 #pragma unroll
-    for (int j = 0; j < ND; ++j) {
-      const float pj = fmaf(bt, po[j], zv[j]);
-      if constexpr (RS) d[j] = J == I ? pI[j] : pj - pI[j];
-      else d[j] = pj;
+      for (int j = 0; j < ND; ++j) {
+        const float pj = fmaf(bt, po[j], zv[j]);
+        if constexpr (RS) d[j] = J == I ? pI[j] : pj - pI[j];
+        else d[j] = pj;
+      }
+    } else {
+      float pj[ND];
+      PVec<ND>::ld(p, J, pj);
+#pragma unroll
+      for (int j = 0; j < ND; ++j) d[j] = J == I ? pI[j] : pj[j] - pI[j];
     }
 #pragma unroll
     for (int i = 0; i < ND; ++i)
 #pragma unroll
       for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], d[j], acc[i]);
+    __syncwarp();  // every lane has read this stage before it is refilled
   }
-}
-
-// One 32-node slice of q = A p in FP32 (p written before the pass).
-template <int ND>
-__device__ __forceinline__ void spmv_row_rs(const BlockMat& A, int s, int lane, const float* p, float* acc,
-                                            float* pI) {
-  constexpr int BB = ND * ND;
-  const int I = 32 * s + lane;
-  const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
-  const int* cp = A.bcol + (long long)c0 * 32 + lane;
-  const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
-#pragma unroll
-  for (int i = 0; i < ND; ++i) { acc[i] = 0.f; pI[i] = 0.f; }
-  if (I < A.nnode) PVec<ND>::ld(p, I, pI);
-#pragma unroll 2
-  for (int k = 0; k < w; ++k) {
-    const int J = __ldcs(cp + k * 32);
-    float pj[ND];
-    PVec<ND>::ld(p, J, pj);
-    float v[BB];
-#pragma unroll
-    for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);
-    float d[ND];
-#pragma unroll
-    for (int j = 0; j < ND; ++j) d[j] = J == I ? pI[j] : pj[j] - pI[j];
-#pragma unroll
-    for (int i = 0; i < ND; ++i)
-#pragma unroll
-      for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], d[j], acc[i]);
-  }
+  cp_async_wait<0>();  // only empty groups can remain; none is left pending
 }
 
 // One 32-node slice of q = A p with FP64 vectors and arithmetic on the FP32
@@ -494,9 +527,10 @@ __device__ __forceinline__ bool b_rz64(const BSys& S, const Grp& g, double* part
   return group_sum<2>(g, part, S.nslice, out);
 }
 
-template <int ND>
+template <int ND, int D>
 __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const double* s_dN, const double* s_N,
-                        const double* s_w, const float* s_dNf, const float* s_Nf, const float* s_wf) {
+                        const double* s_w, const float* s_dNf, const float* s_Nf, const float* s_wf, float* s_ring) {
+  float* const ring = s_ring + (threadIdx.x >> 5) * D * kStageFloats;
   constexpr int SM = ND * (ND + 1) / 2;
   const int tid = g.rank * blockDim.x + threadIdx.x, nt = g.size * blockDim.x;
   const int lane = threadIdx.x & 31, nwc = blockDim.x >> 5;
@@ -801,9 +835,9 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     for (int s = wid; s < nsl; s += nw) {
       float acc[ND], pv[ND];
       if constexpr (kFused) {
-        spmv_row_fused<ND, kRowSum0>(A, s, lane, pold, S.z32, bt0, acc, pv);
+        spmv_row_staged<ND, kRowSum0, true, D>(A, s, lane, pold, S.z32, bt0, acc, pv, ring);
       } else {
-        spmv_row_rs<ND>(A, s, lane, pnew, acc, pv);
+        spmv_row_staged<ND, true, false, D>(A, s, lane, pnew, nullptr, 0.f, acc, pv, ring);
       }
       const int I = s * 32 + lane;
       double v[1] = {0.0};
@@ -920,6 +954,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restri
   __shared__ double s_dN[kMaxIP * 24], s_N[kMaxIP * 8], s_w[kMaxIP];
   __shared__ float s_dNf[kMaxIP * 24], s_Nf[kMaxIP * 8], s_wf[kMaxIP];
   __shared__ long long s_t0;
+  extern __shared__ __align__(16) float s_ring[];  // stage_bytes<THREADS>() of matrix staging
   const BParams P = *prm;
   const BPlan pl = plan[blockIdx.x];
   if (threadIdx.x == 0) {
@@ -934,9 +969,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restri
     b_stage<double>(S.gt, S.nip, nn, ndir, s_dN, s_N, s_w);
     b_stage<float>(S.gt, S.nip, nn, ndir, s_dNf, s_Nf, s_wf);
     __syncthreads();
-    if (S.ndpn == 3) b_solve<3>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf);
-    else if (S.ndpn == 2) b_solve<2>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf);
-    else b_solve<1>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf);
+    constexpr int D = stage_depth<THREADS>();
+    if (S.ndpn == 3) b_solve<3, D>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf, s_ring);
+    else if (S.ndpn == 2) b_solve<2, D>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf, s_ring);
+    else b_solve<1, D>(S, P, g, s_dN, s_N, s_w, s_dNf, s_Nf, s_wf, s_ring);
   };
   if (pl.k >= 0 && pl.k < P.nbig) {
     const Grp gang{pl.rank, pl.size, bar + pl.bar, &gs, gabort, P.spin_ns, nullptr, t0};
