@@ -156,6 +156,34 @@ class Solver:
         return f
 
     # -- transient diffusion -------------------------------------------------
+    def set_solution(self, u):
+        """The current solution (a Newton loop's starting point, the tangent's displacement)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self._check(self.lib.beta_gpu_set_solution(self.h, _ptr(u)), "set_solution")
+
+    def internal_force_nonlinear(self, u):
+        """The geometric-nonlinear internal force f(u) (hex8 elasticity)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        f = np.zeros_like(u)
+        self._check(self.lib.beta_gpu_internal_force_nonlinear(self.h, _ptr(u), _ptr(f)), "internal_force_nonlinear")
+        return f
+
+    def newton(self, solve=None, max_residual=1e-10, max_newton=400, use_last_solution=False,
+               raise_on_error=True):
+        """BasicModel::iterate with the geometric-nonlinear hex8 element:
+        returns (rc, stats, history of max |R| per iteration)."""
+        o = _abi.NewtonOpts()
+        o.max_residual = max_residual
+        o.max_newton = max_newton
+        o.use_last_solution = int(bool(use_last_solution))
+        o.solve = solve or opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_REF, tol=1e-10, maxit=100000)
+        st = _abi.NewtonStats()
+        hist = np.zeros(max_newton + 1)
+        rc = self.lib.beta_gpu_newton(self.h, C.byref(o), C.byref(st), _ptr(hist))
+        if raise_on_error and rc not in (_abi.OK,):
+            self._check(rc, "newton")
+        return rc, st, hist[:st.iterations + 1]
+
     def heat_set_state(self, u0):
         u0 = np.ascontiguousarray(u0, dtype=np.float64)
         self._check(self.lib.beta_gpu_heat_set_state(self.h, _ptr(u0)), "heat_set_state")

@@ -51,6 +51,7 @@ QUAD4_HEAT = 4
 
 ASM_K = 1
 ASM_MBAR = 2
+ASM_TANGENT = 3
 
 FP64 = 0
 FP32 = 1
@@ -83,6 +84,19 @@ class SolveStats(C.Structure):
         ("final_norm", C.c_double), ("true_rel_residual", C.c_double), ("ms_solve", C.c_double),
         ("ms_spmv_avg", C.c_double),
     ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
+class NewtonOpts(C.Structure):
+    _fields_ = [("max_residual", C.c_double), ("max_newton", C.c_int), ("use_last_solution", C.c_int),
+                ("solve", SolveOpts)]
+
+
+class NewtonStats(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("linear_iterations", C.c_int),
+                ("reserved", C.c_int), ("max_residual", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
@@ -132,6 +146,9 @@ SIGNATURES = {
     "beta_gpu_download": (_I, [_P, _P]),
     "beta_gpu_matvec": (_I, [_P, _I, _P, _P]),
     "beta_gpu_internal_force": (_I, [_P, _P, _P]),
+    "beta_gpu_internal_force_nonlinear": (_I, [_P, _P, _P]),
+    "beta_gpu_set_solution": (_I, [_P, _P]),
+    "beta_gpu_newton": (_I, [_P, C.POINTER(NewtonOpts), C.POINTER(NewtonStats), _P]),
     "beta_gpu_heat_set_state": (_I, [_P, _P]),
     "beta_gpu_heat_run": (_I, [_P, _D, _D, _I, C.POINTER(SolveOpts), C.POINTER(SolveStats), C.POINTER(_I)]),
     "beta_gpu_heat_get_state": (_I, [_P, _P]),

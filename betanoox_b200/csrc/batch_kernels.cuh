@@ -527,10 +527,10 @@ __device__ __forceinline__ bool b_rz64(const BSys& S, const Grp& g, double* part
   return group_sum<2>(g, part, S.nslice, out);
 }
 
-template <int ND, int D>
+template <int ND, int SD>
 __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const double* s_dN, const double* s_N,
                         const double* s_w, const float* s_dNf, const float* s_Nf, const float* s_wf, float* s_ring) {
-  float* const ring = s_ring + (threadIdx.x >> 5) * D * kStageFloats;
+  float* const ring = s_ring + (threadIdx.x >> 5) * SD * kStageFloats;
   constexpr int SM = ND * (ND + 1) / 2;
   const int tid = g.rank * blockDim.x + threadIdx.x, nt = g.size * blockDim.x;
   const int lane = threadIdx.x & 31, nwc = blockDim.x >> 5;
@@ -835,9 +835,9 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     for (int s = wid; s < nsl; s += nw) {
       float acc[ND], pv[ND];
       if constexpr (kFused) {
-        spmv_row_staged<ND, kRowSum0, true, D>(A, s, lane, pold, S.z32, bt0, acc, pv, ring);
+        spmv_row_staged<ND, kRowSum0, true, SD>(A, s, lane, pold, S.z32, bt0, acc, pv, ring);
       } else {
-        spmv_row_staged<ND, true, false, D>(A, s, lane, pnew, nullptr, 0.f, acc, pv, ring);
+        spmv_row_staged<ND, true, false, SD>(A, s, lane, pnew, nullptr, 0.f, acc, pv, ring);
       }
       const int I = s * 32 + lane;
       double v[1] = {0.0};

@@ -175,6 +175,7 @@ struct beta_gpu_ctx {
   DBuf<unsigned char> zrep;
   bool zrep_on = false;
   DBuf<int> dfirst;
+  DBuf<unsigned long long> dmax;  // Newton: bits of the largest |residual|
   // solution / transient state
   DBuf<double> u, us;
   bool have_u = false, have_us = false;
@@ -316,14 +317,19 @@ ElemArgs elem_args(beta_gpu_ctx* c) {
   return A;
 }
 
+// ugnl: the displacement of a geometric-nonlinear tangent (hex8 elasticity),
+// null for the linear element.
 template <typename T>
-int launch_assembly(beta_gpu_ctx* c, const ElemArgs& A) {
+int launch_assembly(beta_gpu_ctx* c, const ElemArgs& A, const double* ugnl = nullptr) {
   const int nip = c->h_gt.nip;
   for (int col = 0; col < c->P.ncolor; ++col) {
     const int beg = c->P.color_ptr[col], nel = c->P.color_ptr[col + 1] - beg;
     if (nel == 0) continue;
     const int* el = c->elems.p + beg;
-    if (c->kind == BETA_GPU_HEX8_ELASTIC) {
+    if (ugnl) {
+      size_t sm = (size_t)nip * 33 * sizeof(T);
+      launch(c, k_asm_hex8_gnl<T>, grid_for(c, nel, 8), 256, sm, A, el, nel, ugnl);
+    } else if (c->kind == BETA_GPU_HEX8_ELASTIC) {
       size_t sm = (size_t)nip * 33 * sizeof(T);
       launch(c, k_asm_hex8_elastic<T>, grid_for(c, nel, 8), 256, sm, A, el, nel);
     } else if (c->kind == BETA_GPU_HEX8_HEAT) {
@@ -371,6 +377,30 @@ int mf_apply(beta_gpu_ctx* c, double c1, const double* w1, double c2, const doub
     else
       launch(c, k_mf_quad4_pstress, grid_for(c, nel, 64), 256, 0, A, el, nel, w1, w2, y);
     CKL("matrix-free kernel launch");
+  }
+  return BETA_GPU_OK;
+}
+
+// y = geometric-nonlinear internal force at displacement u (FP64), y zeroed
+// first; hex8 elasticity.
+int fint_apply(beta_gpu_ctx* c, const double* u, double* y) {
+  MfArgs A;
+  A.xyz = c->xyz.p;
+  A.conn = c->conn.p;
+  A.gparams = c->gparams.p;
+  A.egroup = c->have_egroup ? c->egroup.p : nullptr;
+  A.nparams = c->nparams;
+  A.nip = c->h_gt.nip;
+  A.gt = c->gt.p;
+  A.c1 = 1.0;
+  A.c2 = 0.0;
+  A.cm = 0.0;
+  CK(cudaMemsetAsync(y, 0, sizeof(double) * c->ndof, c->stream));
+  for (int col = 0; col < c->P.ncolor; ++col) {
+    const int beg = c->P.color_ptr[col], nel = c->P.color_ptr[col + 1] - beg;
+    if (nel == 0) continue;
+    launch(c, k_fint_hex8_gnl, grid_for(c, nel, 32), 256, 0, A, (const int*)c->elems.p + beg, nel, u, y);
+    CKL("k_fint_hex8_gnl launch");
   }
   return BETA_GPU_OK;
 }
@@ -675,6 +705,33 @@ int mpir_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c
     stats->final_norm = q;
   }
   return status;
+}
+
+// One inexact Newton step in FP32: the residual r64 (FP64) rounded to FP32,
+// block-Jacobi PCG on the FP32 tangent from zero until the FP32 recursive
+// residual has fallen by o->inner_tol (default 1e-3); the correction is left
+// in v32[0].
+template <int ND>
+int newton_step32(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, int* iterations) {
+  int rc;
+  if ((rc = compute_minv<ND>(c, o->precond)) != BETA_GPU_OK) return rc;
+  const int n = c->ndof;
+  const double delta = (o->inner_tol > 0 && o->inner_tol < 1) ? o->inner_tol : 1e-3;
+  const int ce = o->check_every > 0 ? o->check_every : std::max(8, std::min(64, c->ndof / 20000));
+  launch(c, k_to32, grid_for(c, n, 256), 256, 0, (long long)n, (const double*)c->r64.p, 1.0, c->v32[1].p);
+  if ((rc = init_state(c, kRuleReliable, 1.0, o->maxit > 0 ? o->maxit : 10000)) != BETA_GPU_OK) return rc;
+  c->h_st->delta2 = delta * delta;
+  c->h_st->tolabs2 = 0.0;
+  CK(h2d(c, (char*)c->st.p + offsetof(PcgState, delta2), &c->h_st->delta2, sizeof(double)));
+  CK(h2d(c, (char*)c->st.p + offsetof(PcgState, tolabs2), &c->h_st->tolabs2, sizeof(double)));
+  launch(c, k_start_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->v32[0].p, (const float*)c->v32[1].p,
+         c->v32[2].p, (const float*)c->minv.p, c->st.p, c->partials.p);
+  CKL("k_start_b");
+  PcgState s;
+  if ((rc = pcg_loop<ND>(c, ce, nullptr, &s)) != BETA_GPU_OK) return rc;
+  *iterations = s.iter;
+  if (s.status == kStatusBreakdown) return fail(c, BETA_GPU_BREAKDOWN, "PCG breakdown in a Newton step");
+  return BETA_GPU_OK;
 }
 
 int mpir_dispatch(beta_gpu_ctx* c, bool start_from_rhs, const beta_gpu_solve_opts* o, double c1, double c2,
@@ -1168,7 +1225,13 @@ int beta_gpu_assemble(beta_gpu_ctx* c, int what, int precision, double dt, doubl
   if (!c->have_pattern || !c->have_mat) return fail(c, BETA_GPU_ERR_STATE, "pattern and materials required");
   cudaSetDevice(c->device);
   double ks = 1.0, ms = 0.0;
-  if (what == BETA_GPU_ASM_MBAR) {
+  const double* ugnl = nullptr;
+  if (what == BETA_GPU_ASM_TANGENT) {
+    if (c->kind != BETA_GPU_HEX8_ELASTIC)
+      return fail(c, BETA_GPU_ERR_UNSUPPORTED, "the geometric-nonlinear tangent is for hex8 elasticity");
+    if (!c->have_u) return fail(c, BETA_GPU_ERR_STATE, "the tangent needs a current solution");
+    ugnl = c->u.p;
+  } else if (what == BETA_GPU_ASM_MBAR) {
     if (!is_diffusion(c->kind)) return fail(c, BETA_GPU_ERR_UNSUPPORTED, "Mbar assembly is for diffusion elements");
     if (!(dt > 0)) return fail(c, BETA_GPU_ERR_ARG, "dt must be positive");
     ks = alpha * dt / dt;  // (a1 K + M)/dt with a1 = alpha*dt (formK_s, HeatTransferElement3DTransient.cpp:341)
@@ -1201,7 +1264,7 @@ int beta_gpu_assemble(beta_gpu_ctx* c, int what, int precision, double dt, doubl
     CK(cudaMemsetAsync(c->pseudo.p, 0, sizeof(double) * c->ndof, c->stream));
     A.sval = c->sval.p;
     A.pseudo = c->pseudo.p;
-    if ((rc = launch_assembly<double>(c, A))) return rc;
+    if ((rc = launch_assembly<double>(c, A, ugnl))) return rc;
     launch(c, k_set_restrained_diag64, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->rest.p, c->sdiag.p,
                                                                               c->sval.p);
     CKL("k_set_restrained_diag64");
@@ -1214,7 +1277,7 @@ int beta_gpu_assemble(beta_gpu_ctx* c, int what, int precision, double dt, doubl
     CK(c->bval.alloc(nv));
     CK(cudaMemsetAsync(c->bval.p, 0, sizeof(float) * nv, c->stream));
     A.bval = c->bval.p;
-    if ((rc = launch_assembly<float>(c, A))) return rc;
+    if ((rc = launch_assembly<float>(c, A, ugnl))) return rc;
     const int g = grid_for(c, c->nnode, 256);
     if (c->ndpn == 3) launch(c, k_set_restrained_diag32<3>, g, 256, 0, c->nnode, c->rest.p, c->bsoff.p, c->ndiag.p, c->bval.p);
     else if (c->ndpn == 2) launch(c, k_set_restrained_diag32<2>, g, 256, 0, c->nnode, c->rest.p, c->bsoff.p, c->ndiag.p, c->bval.p);
@@ -1561,6 +1624,119 @@ int beta_gpu_heat_run(beta_gpu_ctx* c, double dt, double alpha, int nsteps, cons
   if (stats) *stats = s;
   if (total_iterations) *total_iterations = total;
   return BETA_GPU_OK;
+}
+
+int beta_gpu_set_solution(beta_gpu_ctx* c, const double* u) {
+  if (!c || !u) return BETA_GPU_ERR_ARG;
+  if (!c->have_pattern) return fail(c, BETA_GPU_ERR_STATE, "mesh and pattern required");
+  if (!all_finite(u, c->ndof)) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite solution");
+  cudaSetDevice(c->device);
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  CK(h2d(c, c->u.p, u, sizeof(double) * c->ndof));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_u = true;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_internal_force_nonlinear(beta_gpu_ctx* c, const double* u, double* f) {
+  if (!c || !u || !f) return BETA_GPU_ERR_ARG;
+  if (!c->have_pattern || !c->have_mat) return fail(c, BETA_GPU_ERR_STATE, "pattern and materials required");
+  if (c->kind != BETA_GPU_HEX8_ELASTIC)
+    return fail(c, BETA_GPU_ERR_UNSUPPORTED, "the geometric-nonlinear internal force is for hex8 elasticity");
+  cudaSetDevice(c->device);
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  CK(h2d(c, c->t64.p, u, sizeof(double) * c->ndof));
+  if ((rc = fint_apply(c, c->t64.p, c->y64.p))) return rc;
+  CK(d2h(c, f, c->y64.p, sizeof(double) * c->ndof));
+  CK(cudaStreamSynchronize(c->stream));
+  return BETA_GPU_OK;
+}
+
+// BasicModel::iterate (BasicModel.cpp:1244-1381) with the hex8 element in its
+// geometric-nonlinear form.  Each iteration: the internal force f(u) in FP64
+// (getGlobalForces), R = load - f on free dofs (0 on restrained ones), stop
+// once max |R| < opts->max_residual; the tangent K_T(u) (assembleK at the
+// current solution); K_T d = R; u += d on free dofs
+// (incrementalSolutionUsingResidual + addIncrementalDisplacements,
+// equation.cpp:1638-1720).  FP64 steps solve with the FP64 tangent and the
+// reference's PCG from the current solution as initial guess, as the
+// reference passes it; mixed steps assemble the tangent in FP32 and reduce
+// the FP32 residual by opts->solve.inner_tol with block-Jacobi PCG -- the
+// FP64 residual of the next iteration refines each step (an inexact Newton).
+int beta_gpu_newton(beta_gpu_ctx* c, const beta_gpu_newton_opts* o, beta_gpu_newton_stats* stats,
+                    double* history) {
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (!c || !o) return BETA_GPU_ERR_ARG;
+  if (c->kind != BETA_GPU_HEX8_ELASTIC)
+    return fail(c, BETA_GPU_ERR_UNSUPPORTED, "the geometric-nonlinear Newton loop is for hex8 elasticity");
+  if (!c->have_pattern || !c->have_mat || !c->have_bc)
+    return fail(c, BETA_GPU_ERR_STATE, "mesh, pattern, materials and boundary conditions required");
+  cudaSetDevice(c->device);
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  CK(c->dmax.alloc(1));
+  const int n = c->ndof;
+  const int max_newton = o->max_newton > 0 ? o->max_newton : 400;
+  const double tol = o->max_residual > 0 ? o->max_residual : 1e-10;
+  const bool mixed = o->solve.mode == BETA_GPU_MODE_MPIR;
+  if (!(o->use_last_solution && c->have_u)) {
+    launch(c, k_ext64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->presc.p, (const double*)nullptr, c->u.p);
+    CKL("k_ext64");
+  }
+  c->have_u = true;
+  int status = BETA_GPU_OK, it = 0;
+  long long lin = 0;
+  double maxr = 0.0;
+  for (;; ++it) {
+    if ((rc = fint_apply(c, c->u.p, c->y64.p))) return rc;
+    CK(cudaMemsetAsync(c->dmax.p, 0, sizeof(unsigned long long), c->stream));
+    launch(c, k_newton_residual, grid_for(c, n, 256), 256, 0, n, c->rest.p, (const double*)c->load.p,
+           (const double*)c->y64.p, c->r64.p, c->dmax.p);
+    CKL("k_newton_residual");
+    unsigned long long bits = 0;
+    CK(d2h(c, c->h_sums, c->dmax.p, sizeof(bits)));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(&bits, c->h_sums, sizeof(bits));
+    std::memcpy(&maxr, &bits, sizeof(maxr));
+    if (history) history[it] = maxr;
+    if (!(maxr < 1e300)) { status = BETA_GPU_BREAKDOWN; break; }
+    if (maxr < tol) break;
+    if (it >= max_newton) { status = BETA_GPU_MAXIT; break; }
+    if ((rc = beta_gpu_assemble(c, BETA_GPU_ASM_TANGENT, mixed ? BETA_GPU_FP32 : BETA_GPU_FP64, 0.0, 1.0)) !=
+        BETA_GPU_OK) {
+      status = rc;
+      break;
+    }
+    if (!mixed) {
+      CK(cudaMemcpyAsync(c->b64.p, c->r64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->x64.p, c->u.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+      beta_gpu_solve_stats ls;
+      std::memset(&ls, 0, sizeof(ls));
+      rc = fp64_core(c, &o->solve, &ls, nullptr);
+      lin += ls.iterations;
+      if (rc != BETA_GPU_OK && rc != BETA_GPU_MAXIT) { status = rc; break; }
+      launch(c, k_add_free64, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->u.p, (const double*)c->x64.p);
+    } else {
+      int its = 0;
+      rc = newton_step32<3>(c, &o->solve, &its);
+      lin += its;
+      if (rc != BETA_GPU_OK) { status = rc; break; }
+      launch(c, k_add_free_from32, grid_for(c, n, 256), 256, 0, n, c->rest.p, c->u.p,
+             (const float*)c->v32[0].p);
+    }
+    CKL("Newton update");
+  }
+  if (stats) {
+    stats->status = status;
+    stats->iterations = it;
+    stats->linear_iterations = (int)std::min<long long>(lin, 2000000000LL);
+    stats->max_residual = maxr;
+  }
+  if (status == BETA_GPU_MAXIT) c->err = "Newton iterations exhausted before max |residual| < max_residual";
+  if (status == BETA_GPU_BREAKDOWN) c->err = "non-finite residual in the Newton loop";
+  return status;
 }
 
 // Jacobi-PCG on caller-owned device CSR; scratch from cudaMalloc, freed on return.

@@ -213,6 +213,141 @@ __global__ void __launch_bounds__(256) k_asm_hex8_elastic(ElemArgs A, const int*
     asm_hex8_elastic_warp<T>(A, elems, nel, w, s_dN, s_N, s_w);
 }
 
+// ---- hex8 geometric-nonlinear tangent (ElasticityElement3D with analysisType
+// GEOMETRIC_NONLINEAR, ElasticityElement3D.cpp:84-119, 124-160, 560-641) ----
+// At displacement u the strain-displacement rows of node a are those of the
+// linear element applied to F^T, F = I + grad u (calculateBmatrix adds
+// grad u * dN to every row), so the material block of a node pair is
+// F K^L_ab F^T with K^L_ab the linear element's block above; the
+// initial-stress term adds (dN_a . S dN_b) I, S = C E with E the
+// Green-Lagrange strain (engineering shear) -- the stress the reference
+// computes before addToKe when analysisType is GEOMETRIC_NONLINEAR.
+template <typename T>
+__device__ __forceinline__ void asm_hex8_gnl_warp(const ElemArgs& A, const int* __restrict__ elems, int nel, int w,
+                                                  const double* __restrict__ u, const T* s_dN, const T* s_w) {
+  const int lane = threadIdx.x & 31;
+  const int b = lane & 7, a0 = lane >> 3, a1 = a0 + 4;
+  const int e = elems[w];
+  const int* ce = A.conn + (long long)e * 8;
+  const int J = ce[b];
+  const int n0 = ce[0];
+  T xr[3], ub[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    xr[c] = (T)(A.xyz[3LL * J + c] - A.xyz[3LL * n0 + c]);
+    ub[c] = (T)u[3LL * J + c];
+  }
+  double nn[6], gg[3];
+  ortho_c(A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams, nn, gg);
+  const T N00 = nn[0], N01 = nn[1], N02 = nn[2], N11 = nn[3], N12 = nn[4], N22 = nn[5];
+  const T G4 = gg[0], G5 = gg[1], G6 = gg[2];
+  T K0[9], K1[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) K0[k] = K1[k] = T(0);
+  for (int ip = 0; ip < A.nip; ++ip) {
+    const T* dn = s_dN + ip * 24;
+    const T d0 = dn[b], d1 = dn[8 + b], d2 = dn[16 + b];
+    T M[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      M[c] = group_sum<8>(d0 * xr[c]);
+      M[3 + c] = group_sum<8>(d1 * xr[c]);
+      M[6 + c] = group_sum<8>(d2 * xr[c]);
+    }
+    T Mi[9];
+    const T det = inv3<T>(M, Mi);
+    const T f = det * s_w[ip];
+    const T g0 = Mi[0] * d0 + Mi[1] * d1 + Mi[2] * d2;
+    const T g1 = Mi[3] * d0 + Mi[4] * d1 + Mi[5] * d2;
+    const T g2 = Mi[6] * d0 + Mi[7] * d1 + Mi[8] * d2;
+    // F[k][j] = delta_kj + du_k/dx_j
+    T F[9];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      F[3 * k] = group_sum<8>(ub[k] * g0);
+      F[3 * k + 1] = group_sum<8>(ub[k] * g1);
+      F[3 * k + 2] = group_sum<8>(ub[k] * g2);
+    }
+    // Green-Lagrange strain (engineering shear) from H = F - I, then S = C E
+    const T E0 = F[0] + T(0.5) * (F[0] * F[0] + F[3] * F[3] + F[6] * F[6]);
+    const T E1 = F[4] + T(0.5) * (F[1] * F[1] + F[4] * F[4] + F[7] * F[7]);
+    const T E2 = F[8] + T(0.5) * (F[2] * F[2] + F[5] * F[5] + F[8] * F[8]);
+    const T E3 = F[1] + F[3] + F[0] * F[1] + F[3] * F[4] + F[6] * F[7];
+    const T E4 = F[5] + F[7] + F[1] * F[2] + F[4] * F[5] + F[7] * F[8];
+    const T E5 = F[2] + F[6] + F[0] * F[2] + F[3] * F[5] + F[6] * F[8];
+    const T S0 = N00 * E0 + N01 * E1 + N02 * E2, S1 = N01 * E0 + N11 * E1 + N12 * E2;
+    const T S2 = N02 * E0 + N12 * E1 + N22 * E2, S3 = G4 * E3, S4 = G5 * E4, S5 = G6 * E5;
+    F[0] += T(1);
+    F[4] += T(1);
+    F[8] += T(1);
+    // S dN_b (the initial-stress term of every pair with this lane's node)
+    const T sg0 = S0 * g0 + S3 * g1 + S5 * g2;
+    const T sg1 = S3 * g0 + S1 * g1 + S4 * g2;
+    const T sg2 = S5 * g0 + S4 * g1 + S2 * g2;
+    T h[2][3];
+    h[0][0] = __shfl_sync(0xffffffffu, g0, a0);
+    h[0][1] = __shfl_sync(0xffffffffu, g1, a0);
+    h[0][2] = __shfl_sync(0xffffffffu, g2, a0);
+    h[1][0] = __shfl_sync(0xffffffffu, g0, a1);
+    h[1][1] = __shfl_sync(0xffffffffu, g1, a1);
+    h[1][2] = __shfl_sync(0xffffffffu, g2, a1);
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      T* K = p ? K1 : K0;
+      const T x0 = h[p][0] * f, x1 = h[p][1] * f, x2 = h[p][2] * f;
+      T L[9];  // the linear block K^L_ab (as in asm_hex8_elastic_warp)
+      L[0] = x0 * N00 * g0 + x1 * G4 * g1 + x2 * G6 * g2;
+      L[1] = x0 * N01 * g1 + x1 * G4 * g0;
+      L[2] = x0 * N02 * g2 + x2 * G6 * g0;
+      L[3] = x1 * N01 * g0 + x0 * G4 * g1;
+      L[4] = x1 * N11 * g1 + x0 * G4 * g0 + x2 * G5 * g2;
+      L[5] = x1 * N12 * g2 + x2 * G5 * g1;
+      L[6] = x2 * N02 * g0 + x0 * G6 * g2;
+      L[7] = x2 * N12 * g1 + x1 * G5 * g2;
+      L[8] = x2 * N22 * g2 + x1 * G5 * g1 + x0 * G6 * g0;
+      T FL[9];  // F L
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) FL[3 * k + m] = F[3 * k] * L[m] + F[3 * k + 1] * L[3 + m] + F[3 * k + 2] * L[6 + m];
+      const T ks = x0 * sg0 + x1 * sg1 + x2 * sg2;
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l)
+          K[3 * k + l] += FL[3 * k] * F[3 * l] + FL[3 * k + 1] * F[3 * l + 1] + FL[3 * k + 2] * F[3 * l + 2] +
+                          (k == l ? ks : T(0));
+    }
+  }
+  if ((b == a0 && !(K0[0] > 0 && K0[4] > 0 && K0[8] > 0)) ||
+      (b == a1 && !(K1[0] > 0 && K1[4] > 0 && K1[8] > 0)))
+    atomicOr(A.flags, kFlagNegDiag);
+  const int I0 = __shfl_sync(0xffffffffu, J, a0);
+  const int I1 = __shfl_sync(0xffffffffu, J, a1);
+  const uint16_t* sl = A.slot + (long long)e * 64;
+  if constexpr (sizeof(T) == 4) {
+    scatter_block32<3>(A, I0, J, sl[a0 * 8 + b], K0);
+    scatter_block32<3>(A, I1, J, sl[a1 * 8 + b], K1);
+  } else {
+    double pl0[3], pl1[3];  // the pseudo-load of prescribed values: a Newton step does not use it
+    scatter_block64<3>(A, I0, J, sl[a0 * 8 + b], K0, pl0);
+    scatter_block64<3>(A, I1, J, sl[a1 * 8 + b], K1, pl1);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_asm_hex8_gnl(ElemArgs A, const int* __restrict__ elems, int nel,
+                                                      const double* __restrict__ u) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_dN = reinterpret_cast<T*>(smem_raw);
+  T* s_N = s_dN + A.nip * 24;
+  T* s_w = s_N + A.nip * 8;
+  stage_gauss<T, 8, 3>(A.gt, A.nip, s_dN, s_N, s_w);
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < nel; w += gridDim.x * wpb)
+    asm_hex8_gnl_warp<T>(A, elems, nel, w, u, s_dN, s_w);
+}
+
 // ---- quad4 plane stress, two elements per warp ---------------------------
 // lane = 16*sub + 4*a + b handles pair (a,b) of element 2*warp+sub.
 template <typename T>

@@ -99,6 +99,88 @@ __global__ void __launch_bounds__(256) k_mf_hex8_elastic(MfArgs A, const int* __
     mf_hex8_elastic_warp(A, elems, nel, w, w1, w2, y, s_dN, s_w);
 }
 
+// Geometric-nonlinear internal force of hex8 elasticity at displacement u
+// (ElasticityElement3D with analysisType GEOMETRIC_NONLINEAR, update("F")):
+// per Gauss point F = I + grad u, the Green-Lagrange strain E (engineering
+// shear, calculateStrain :124-160), S = C E, and Fe_b = B_b^T S = F (S dN_b)
+// (the nonlinear B of calculateBmatrix :84-119 in addToFe :41-55); y += Fe.
+// 8 lanes per element, 4 elements per warp, as mf_hex8_elastic_warp.
+__device__ __forceinline__ void fint_hex8_gnl_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
+                                                   const double* u, double* y, const double* s_dN, const double* s_w) {
+  const int lane = threadIdx.x & 31, b = lane & 7;
+  const int idx = 4 * w + (lane >> 3);
+  const bool valid = idx < nel;
+  const int e = elems[valid ? idx : nel - 1];
+  const int* ce = A.conn + (long long)e * 8;
+  const int J = ce[b], n0 = ce[0];
+  double xr[3], ub[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    xr[c] = A.xyz[3LL * J + c] - A.xyz[3LL * n0 + c];
+    ub[c] = u[3LL * J + c];
+  }
+  double nn[6], gg[3];
+  ortho_c(A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams, nn, gg);
+  double f0 = 0, f1 = 0, f2 = 0;
+  for (int ip = 0; ip < A.nip; ++ip) {
+    const double d0 = s_dN[ip * 24 + b], d1 = s_dN[ip * 24 + 8 + b], d2 = s_dN[ip * 24 + 16 + b];
+    double M[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      M[c] = group_sum<8>(d0 * xr[c]);
+      M[3 + c] = group_sum<8>(d1 * xr[c]);
+      M[6 + c] = group_sum<8>(d2 * xr[c]);
+    }
+    double Mi[9];
+    const double det = inv3<double>(M, Mi);
+    const double g0 = Mi[0] * d0 + Mi[1] * d1 + Mi[2] * d2;
+    const double g1 = Mi[3] * d0 + Mi[4] * d1 + Mi[5] * d2;
+    const double g2 = Mi[6] * d0 + Mi[7] * d1 + Mi[8] * d2;
+    double H[9];  // du_k/dx_j
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      H[3 * k] = group_sum<8>(ub[k] * g0);
+      H[3 * k + 1] = group_sum<8>(ub[k] * g1);
+      H[3 * k + 2] = group_sum<8>(ub[k] * g2);
+    }
+    const double E0 = H[0] + 0.5 * (H[0] * H[0] + H[3] * H[3] + H[6] * H[6]);
+    const double E1 = H[4] + 0.5 * (H[1] * H[1] + H[4] * H[4] + H[7] * H[7]);
+    const double E2 = H[8] + 0.5 * (H[2] * H[2] + H[5] * H[5] + H[8] * H[8]);
+    const double E3 = H[1] + H[3] + H[0] * H[1] + H[3] * H[4] + H[6] * H[7];
+    const double E4 = H[5] + H[7] + H[1] * H[2] + H[4] * H[5] + H[7] * H[8];
+    const double E5 = H[2] + H[6] + H[0] * H[2] + H[3] * H[5] + H[6] * H[8];
+    const double S0 = nn[0] * E0 + nn[1] * E1 + nn[2] * E2;
+    const double S1 = nn[1] * E0 + nn[3] * E1 + nn[4] * E2;
+    const double S2 = nn[2] * E0 + nn[4] * E1 + nn[5] * E2;
+    const double S3 = gg[0] * E3, S4 = gg[1] * E4, S5 = gg[2] * E5;
+    const double sg0 = S0 * g0 + S3 * g1 + S5 * g2;
+    const double sg1 = S3 * g0 + S1 * g1 + S4 * g2;
+    const double sg2 = S5 * g0 + S4 * g1 + S2 * g2;
+    const double fw = det * s_w[ip];
+    f0 += fw * ((1.0 + H[0]) * sg0 + H[1] * sg1 + H[2] * sg2);
+    f1 += fw * (H[3] * sg0 + (1.0 + H[4]) * sg1 + H[5] * sg2);
+    f2 += fw * (H[6] * sg0 + H[7] * sg1 + (1.0 + H[8]) * sg2);
+  }
+  if (valid) {
+    y[3LL * J] += f0;
+    y[3LL * J + 1] += f1;
+    y[3LL * J + 2] += f2;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_fint_hex8_gnl(MfArgs A, const int* __restrict__ elems, int nel,
+                                                       const double* __restrict__ u, double* __restrict__ y) {
+  __shared__ double s_dN[kMaxIP * 24];
+  __shared__ double s_w[kMaxIP];
+  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
+    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
+  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
+  __syncthreads();
+  const int wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); 4 * w < nel; w += gridDim.x * wpb)
+    fint_hex8_gnl_warp(A, elems, nel, w, u, y, s_dN, s_w);
+}
+
 // quad4 plane stress: 4 lanes per element, 8 elements per warp.
 __device__ __forceinline__ void mf_quad4_pstress_warp(const MfArgs& A, const int* __restrict__ elems, int nel, int w,
     const double* w1, const double* w2, double* y, const double* s_dN, const double* s_w) {

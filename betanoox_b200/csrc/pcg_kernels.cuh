@@ -772,6 +772,41 @@ __global__ void __launch_bounds__(256) k_rhs_elim64(int n, const unsigned char* 
   if (reduce_last<1>(acc, partials, ticket, out) && threadIdx.x == 0) sums[0] = out[0];
 }
 
+// Newton residual r = rest ? 0 : load - y, and the largest |r| (bits of a
+// non-negative double: integer order is IEEE order, so atomicMax is exact and
+// order-free; a NaN ranks above every number).
+__global__ void __launch_bounds__(256) k_newton_residual(int n, const unsigned char* __restrict__ rest,
+                                                         const double* __restrict__ load,
+                                                         const double* __restrict__ y, double* __restrict__ r,
+                                                         unsigned long long* maxbits) {
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ri = rest[i] ? 0.0 : (load ? load[i] : 0.0) - y[i];
+    r[i] = ri;
+    const double a = fabs(ri);
+    if (a > m || a != a) m = a;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double t = __shfl_xor_sync(0xffffffffu, m, o);
+    if (t > m || t != t) m = t;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(m));
+}
+
+// u += d on free dofs
+__global__ void k_add_free64(int n, const unsigned char* __restrict__ rest, double* __restrict__ u,
+                             const double* __restrict__ d) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (!rest[i]) u[i] += d[i];
+}
+
+__global__ void k_add_free_from32(int n, const unsigned char* __restrict__ rest, double* __restrict__ u,
+                                  const float* __restrict__ d) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (!rest[i]) u[i] += (double)d[i];
+}
+
 // y += a x
 __global__ void k_axpy64(int n, double* __restrict__ y, double a, const double* __restrict__ x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];

@@ -211,6 +211,30 @@ def cube_hex8(n=100, seed=2024, pressure=1.0, order=2, sigma=0.5, nu_lo=0.20, nu
                  {"n": n, "seed": seed})
 
 
+# ---- a cantilever for the geometric-nonlinear Newton loop --------------------
+def cantilever_hex8(nx=20, ny=2, nz=2, length=10.0, width=1.0, height=1.0, load=6.0, E=1e4, nu=0.3, order=2):
+    """A beam [0,length] x [0,width] x [0,height], nx x ny x nz hex8, clamped at
+    x = 0, a total transverse load `load` in -z shared equally by the nodes of
+    the end face x = length; isotropic E, nu.  At the default load the linear
+    tip deflection is about a quarter of the length, so the deflected shape
+    rotates by tens of degrees and the geometric-nonlinear solution departs
+    from the linear one."""
+    xyz, conn = grid_hex8(nx, ny, nz, length, width, height)
+    nnode = xyz.shape[0]
+    ne = conn.shape[0]
+    params = iso3d_params(np.full(ne, float(E)), np.full(ne, float(nu)))
+    ndof = 3 * nnode
+    rest = np.zeros(ndof, np.uint8)
+    root = np.where(np.isclose(xyz[:, 0], 0.0))[0]
+    for c in range(3):
+        rest[3 * root + c] = 1
+    tip = np.where(np.isclose(xyz[:, 0], length))[0]
+    f = np.zeros(ndof)
+    f[3 * tip + 2] = -load / len(tip)
+    return Model(f"hex8_cantilever_{nx}x{ny}x{nz}", _abi.HEX8_ELASTIC, 3, xyz, conn, 3, params, rest, np.zeros(ndof),
+                 f, order, {"load": load, "length": length})
+
+
 # ---- configuration 3: transient diffusion slab ------------------------------
 def heat_slab(nx=256, ny=256, nz=64, seed=7, order=3, lx=1.0, ly=1.0):
     """[0,lx]x[0,ly]x[0,lz] with lz = lx*nz/nx (cubic cells); k_e = exp(N(0,1)),

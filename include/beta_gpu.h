@@ -77,7 +77,9 @@ enum {
 /* ---- what to assemble (Element::update action letters) ------------------ */
 enum {
   BETA_GPU_ASM_K = 1,      /* "K": stiffness / conductivity                           */
-  BETA_GPU_ASM_MBAR = 2    /* "KM" + formK_s: Mbar = (a1*K + M)/dt (DiffusionModel.cpp:322-347) */
+  BETA_GPU_ASM_MBAR = 2,   /* "KM" + formK_s: Mbar = (a1*K + M)/dt (DiffusionModel.cpp:322-347) */
+  BETA_GPU_ASM_TANGENT = 3 /* "K" with analysisType GEOMETRIC_NONLINEAR at the current solution
+                              (hex8 elasticity; ElasticityElement3D.cpp:84-119, 560-641)          */
 };
 
 /* ---- precision of the assembled matrix ---------------------------------- */
@@ -499,6 +501,44 @@ BETA_GPU_API int beta_gpu_server_cancel(beta_gpu_server* server, long long reque
  * bytes, [10] microseconds the worker spent in launches, [11] bytes
  * host->device, [12] bytes device->host; n <= 13. */
 BETA_GPU_API int beta_gpu_server_stats(beta_gpu_server* server, long long* out, int n);
+
+/* ---- geometric-nonlinear Newton loop (hex8 elasticity) ------------------- */
+/* BasicModel::iterate (BasicModel.cpp:1244-1381) with the element in its
+ * GEOMETRIC_NONLINEAR form: Green-Lagrange strain, B with the
+ * displacement-gradient terms, the initial-stress term in the tangent
+ * (ElasticityElement3D.cpp:84-160, 560-641). */
+typedef struct beta_gpu_newton_opts {
+  double max_residual;       /* stop when max |load - f_int| over free dofs < this (the reference's
+                                maxAllowableResidual; 0: its default 1e-10)                       */
+  int max_newton;            /* Newton solves at most (0: the reference's 400)                    */
+  int use_last_solution;     /* start from the context's solution, else from the prescribed values */
+  beta_gpu_solve_opts solve; /* each step: MODE_FP64 -- FP64 tangent, the reference's PCG from the
+                                current solution as initial guess (solve.stop_rule, tol, maxit);
+                                MODE_MPIR -- FP32 tangent, block-Jacobi PCG reducing the FP32
+                                residual by solve.inner_tol (0: 1e-3), refined by the next FP64
+                                residual (an inexact Newton)                                       */
+} beta_gpu_newton_opts;
+
+typedef struct beta_gpu_newton_stats {
+  int status;            /* BETA_GPU_OK, MAXIT, BREAKDOWN or a linear solve's error      */
+  int iterations;        /* Newton solves done                                            */
+  int linear_iterations; /* PCG iterations in all                                         */
+  int reserved;
+  double max_residual;   /* max |R| over free dofs at exit                                */
+} beta_gpu_newton_stats;
+
+/* Runs the loop; the solution stays on the device (beta_gpu_download).
+ * history (may be NULL): max |R| at each iteration, max_newton + 1 entries. */
+BETA_GPU_API int beta_gpu_newton(beta_gpu_ctx* ctx, const beta_gpu_newton_opts* opts,
+                                 beta_gpu_newton_stats* stats, double* history);
+/* The context's current solution from host memory (BasicModel::
+ * readDisplacementsIntoCurrentSolution, BasicModel.cpp:1230-1242: a Newton
+ * loop restarted from saved displacements); the tangent assembly and a
+ * Newton loop with use_last_solution start from it. */
+BETA_GPU_API int beta_gpu_set_solution(beta_gpu_ctx* ctx, const double* u);
+/* The geometric-nonlinear internal force f(u) (getGlobalForces with "F",
+ * BasicModel.cpp:1063-1110, without the restraint mapping); host vectors. */
+BETA_GPU_API int beta_gpu_internal_force_nonlinear(beta_gpu_ctx* ctx, const double* u, double* f);
 
 /* ---- allocation-free variant of beta_gpu_csr_pcg_device ------------------ */
 /* No counterpart in the reference (BETA's solvers allocate their work vectors

@@ -482,6 +482,105 @@ int oracle_fe_hex8(const double* xyz24, const double* C36, int order, const doub
 }
 
 // ---------------------------------------------------------------------------
+// Geometric-nonlinear hex8: ElasticityElement3D with analysisType
+// GEOMETRIC_NONLINEAR, the element of BasicModel::iterate.  At each
+// integration point: the displacement gradient H_kj = sum_a dN_a/dx_j u_a,k
+// (derivativesOfFields, ElasticityElement3D.cpp:162-207); B with the
+// displacement-gradient terms added to the linear rows (calculateBmatrix
+// :84-119); the Green-Lagrange strain in engineering shear (calculateStrain
+// :124-160); stress = C strain (no hygrothermal strain); the tangent Ke +=
+// (C B)^T B f with the initial-stress term K_sigma (addToKe :560-641, upper
+// triangle) and Fe += B^T stress f (addToFe :41-55); f = detJ * w.  Either
+// output may be null.  Same operation order as the reference's code.
+int oracle_gnl_hex8(const double* xyz24, const double* C36, int order, const double* ue, double* Ke, double* Fe) {
+  double xi[64], eta[64], zeta[64], w[64];
+  if (order < 1 || order > 4) return OR_ERR_ARG;
+  oracle_hex_points(order, xi, eta, zeta, w);
+  if (Ke)
+    for (int i = 0; i < 24; ++i)
+      for (int j = i; j < 24; ++j) Ke[i * 24 + j] = 0.;
+  if (Fe)
+    for (int i = 0; i < 24; ++i) Fe[i] = 0.;
+  const int nip = order * order * order;
+  for (int ip = 0; ip < nip; ++ip) {
+    double d0[8], d1[8], d2[8], g[3][8], B[6][24];
+    oracle_shape_hex8(xi[ip], eta[ip], zeta[ip], nullptr, d0, d1, d2);
+    const double f = jac3(xyz24, d0, d1, d2, g) * w[ip];
+    // H[k][j] = du_k/dx_j
+    double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int a = 0; a < 8; ++a)
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) H[k][j] += g[j][a] * ue[3 * a + k];
+    bmat3(g, B);
+    for (int a = 0; a < 8; ++a) {
+      const double dg1 = g[0][a], dg2 = g[1][a], dg3 = g[2][a];
+      for (int k = 0; k < 3; ++k) {
+        const int c = 3 * a + k;
+        B[0][c] += H[k][0] * dg1;
+        B[1][c] += H[k][1] * dg2;
+        B[2][c] += H[k][2] * dg3;
+        B[3][c] += H[k][0] * dg2 + H[k][1] * dg1;
+        B[4][c] += H[k][1] * dg3 + H[k][2] * dg2;
+        B[5][c] += H[k][0] * dg3 + H[k][2] * dg1;
+      }
+    }
+    double eps[6];
+    eps[0] = H[0][0];
+    eps[1] = H[1][1];
+    eps[2] = H[2][2];
+    eps[3] = H[0][1] + H[1][0];
+    eps[4] = H[1][2] + H[2][1];
+    eps[5] = H[0][2] + H[2][0];
+    eps[0] += .5 * (H[0][0] * H[0][0] + H[1][0] * H[1][0] + H[2][0] * H[2][0]);
+    eps[1] += .5 * (H[0][1] * H[0][1] + H[1][1] * H[1][1] + H[2][1] * H[2][1]);
+    eps[2] += .5 * (H[0][2] * H[0][2] + H[1][2] * H[1][2] + H[2][2] * H[2][2]);
+    eps[3] += H[0][0] * H[0][1] + H[1][0] * H[1][1] + H[2][0] * H[2][1];
+    eps[4] += H[0][1] * H[0][2] + H[1][1] * H[1][2] + H[2][1] * H[2][2];
+    eps[5] += H[0][0] * H[0][2] + H[1][0] * H[1][2] + H[2][0] * H[2][2];
+    double sig[6];
+    for (int k = 0; k < 6; ++k) {
+      double s = 0;
+      for (int m = 0; m < 6; ++m) s += C36[k * 6 + m] * eps[m];
+      sig[k] = s;
+    }
+    if (Ke) {
+      double CB[6][24];
+      for (int ii = 0; ii < 24; ++ii)
+        for (int k = 0; k < 6; ++k) {
+          double s = 0;
+          for (int m = 0; m < 6; ++m) s += B[m][ii] * C36[m * 6 + k];
+          CB[k][ii] = s;
+        }
+      for (int ii = 0; ii < 24; ++ii)
+        for (int jj = ii; jj < 24; ++jj) {
+          double s = 0;
+          for (int k = 0; k < 6; ++k) s += CB[k][ii] * B[k][jj];
+          Ke[ii * 24 + jj] += s * f;
+        }
+      for (int a = 0; a < 8; ++a)
+        for (int b = a; b < 8; ++b) {
+          const double b11 = sig[0] * g[0][a] * g[0][b] + sig[1] * g[1][a] * g[1][b] + sig[2] * g[2][a] * g[2][b] +
+                             sig[3] * (g[0][a] * g[1][b] + g[1][a] * g[0][b]) +
+                             sig[4] * (g[1][a] * g[2][b] + g[2][a] * g[1][b]) +
+                             sig[5] * (g[0][a] * g[2][b] + g[2][a] * g[0][b]);
+          const double v = b11 * f;
+          for (int k = 0; k < 3; ++k) Ke[(3 * a + k) * 24 + 3 * b + k] += v;
+        }
+    }
+    if (Fe)
+      for (int i = 0; i < 24; ++i) {
+        double s = 0.;
+        for (int k = 0; k < 6; ++k) s += B[k][i] * sig[k];
+        Fe[i] += s * f;
+      }
+  }
+  if (Ke)
+    for (int i = 0; i < 24; ++i)
+      if (Ke[i * 24 + i] <= 0) return OR_ERR_NEG_DIAG;
+  return OR_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Equations + SymmetricSparseMatrix (default storage "SPARSE").
 // Storage: per row a sorted column list of J <= I (SortedList<int>), values in
 // the same order; the diagonal is the last entry of each row
@@ -882,6 +981,126 @@ int oracle_sys_assemble_mesh_threaded(void* h, int kind, int nelem, int nnpe, in
     }
   }
   return OR_OK;
+}
+
+// The geometric-nonlinear tangent at total displacement u assembled through
+// addMatrix (BasicModel::assembleK(currentSolution) with analysisType
+// GEOMETRIC_NONLINEAR).
+int oracle_sys_assemble_gnl(void* h, int nelem, const int* conn, const double* xyz, const int* first_dof,
+                            const double* params, int order, const double* u) {
+  double xe[24], ue[24], Ke[24 * 24], C36[36];
+  int map[24];
+  oracle_sys_zero(h);
+  for (int e = 0; e < nelem; ++e) {
+    const int* ce = conn + (size_t)e * 8;
+    gather_xyz(8, 3, ce, xyz, xe);
+    elem_dofs(8, 3, ce, first_dof, map);
+    for (int i = 0; i < 24; ++i) ue[i] = u[map[i]];
+    int st = oracle_cmat_ortho3d(params + (size_t)e * 9, C36);
+    if (st) return st;
+    st = oracle_gnl_hex8(xe, C36, order, ue, Ke, nullptr);
+    if (st) return st;
+    st = oracle_sys_add_matrix(h, Ke, map, 24, nullptr);
+    if (st) return st;
+  }
+  return OR_OK;
+}
+
+// The geometric-nonlinear internal force sum_e Fe(u) over all rows (the
+// restraint mapping left to the caller).
+int oracle_fint_gnl(int nelem, const int* conn, const double* xyz, const int* first_dof, const double* params,
+                    int order, const double* u, double* f, int n) {
+  double xe[24], ue[24], Fe[24], C36[36];
+  int map[24];
+  for (int i = 0; i < n; ++i) f[i] = 0.0;
+  for (int e = 0; e < nelem; ++e) {
+    const int* ce = conn + (size_t)e * 8;
+    gather_xyz(8, 3, ce, xyz, xe);
+    elem_dofs(8, 3, ce, first_dof, map);
+    for (int i = 0; i < 24; ++i) ue[i] = u[map[i]];
+    int st = oracle_cmat_ortho3d(params + (size_t)e * 9, C36);
+    if (st) return st;
+    oracle_gnl_hex8(xe, C36, order, ue, nullptr, Fe);
+    for (int i = 0; i < 24; ++i) f[map[i]] += Fe[i];
+  }
+  return OR_OK;
+}
+
+// BasicModel::iterate (BasicModel.cpp:1244-1381) for hex8 elasticity with
+// analysisType GEOMETRIC_NONLINEAR, on a system whose restraints and loads are
+// set: from the total displacement u (restrained entries hold their
+// prescribed values), each Newton iteration
+//   * sums the element forces Fe(u) into the resultant (getGlobalForces,
+//     BasicModel.cpp:1063-1110; assembleResultantVector skips restrained
+//     rows) and forms the residual R = load - resultant on free rows, 0 on
+//     restrained ones (calculateResidualNorm, equation.cpp:1516-1529);
+//   * stops once max |R| < max_residual (BasicModel.cpp:1292);
+//   * assembles the tangent Ke(u) through addMatrix (assembleK(currentSolution));
+//   * solves K d = R with the reference's PCG and stop rule from the initial
+//     guess u itself, restrained entries their prescribed values
+//     (incrementalSolutionUsingResidual, equation.cpp:1638-1703);
+//   * adds d to the free entries of u (addIncrementalDisplacements :1707-1720).
+// history[it] = max |R| of iteration it (up to max_newton + 1 entries);
+// *iters = Newton solves done; *lin_iters = PCG iterations in all.
+int oracle_newton_hex8(void* h, int nelem, const int* conn, const double* xyz, const int* first_dof,
+                       const double* params, int order, double* u, double max_residual, int max_newton, double eps,
+                       int maxit, double* history, int* iters, int* lin_iters) {
+  auto* s = (OracleSystem*)h;
+  const int L = s->n;
+  std::vector<double> res(L), R(L), guess(L);
+  double xe[24], ue[24], Ke[24 * 24], Fe[24], C36[36];
+  int map[24];
+  int total_lin = 0, it = 0;
+  bool conv = false;
+  for (;; ++it) {
+    std::fill(res.begin(), res.end(), 0.0);
+    for (int e = 0; e < nelem; ++e) {
+      const int* ce = conn + (size_t)e * 8;
+      gather_xyz(8, 3, ce, xyz, xe);
+      elem_dofs(8, 3, ce, first_dof, map);
+      for (int i = 0; i < 24; ++i) ue[i] = u[map[i]];
+      int st = oracle_cmat_ortho3d(params + (size_t)e * 9, C36);
+      if (st) return st;
+      oracle_gnl_hex8(xe, C36, order, ue, nullptr, Fe);
+      for (int i = 0; i < 24; ++i)
+        if (!s->rest[map[i]]) res[map[i]] += Fe[i];
+    }
+    double mx = 0.0;
+    for (int i = 0; i < L; ++i) {
+      R[i] = s->rest[i] ? 0.0 : s->loadVector[i] - res[i];
+      if (std::fabs(R[i]) > mx) mx = std::fabs(R[i]);
+    }
+    if (history) history[it] = mx;
+    conv = mx < max_residual;
+    if (conv || it >= max_newton) break;
+    oracle_sys_zero(h);
+    for (int e = 0; e < nelem; ++e) {
+      const int* ce = conn + (size_t)e * 8;
+      gather_xyz(8, 3, ce, xyz, xe);
+      elem_dofs(8, 3, ce, first_dof, map);
+      for (int i = 0; i < 24; ++i) ue[i] = u[map[i]];
+      oracle_cmat_ortho3d(params + (size_t)e * 9, C36);
+      int st = oracle_gnl_hex8(xe, C36, order, ue, Ke, nullptr);
+      if (st) return st;
+      st = oracle_sys_add_matrix(h, Ke, map, 24, nullptr);
+      if (st) return st;
+    }
+    for (int i = 0; i < L; ++i) guess[i] = u[i];
+    OracleSolveStats ls;
+    std::memset(&ls, 0, sizeof(ls));
+    int rc = pcg_ref(s, R.data(), guess.data(), eps, maxit, &ls);
+    total_lin += ls.iterations;
+    if (rc != OR_OK) {
+      if (iters) *iters = it;
+      if (lin_iters) *lin_iters = total_lin;
+      return rc;
+    }
+    for (int i = 0; i < L; ++i)
+      if (!s->rest[i]) u[i] += R[i];
+  }
+  if (iters) *iters = it;
+  if (lin_iters) *lin_iters = total_lin;
+  return conv ? OR_OK : OR_ERR_MAXIT;
 }
 
 // Global internal force f_int = sum_e Fe(u_e) (BasicModel::CalculateResidual,

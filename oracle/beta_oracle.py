@@ -66,6 +66,11 @@ def _load():
         "oracle_km_hex8_heat": (I, [_dp, _dp, D, I, _dp, _dp]),
         "oracle_km_quad4_heat": (I, [_dp, _dp, D, I, _dp, _dp]),
         "oracle_fe_hex8": (I, [_dp, _dp, I, _dp, _dp]),
+        "oracle_gnl_hex8": (I, [_dp, _dp, I, _dp, P, P]),
+        "oracle_sys_assemble_gnl": (I, [V, I, _ip, _dp, _ip, _dp, I, _dp]),
+        "oracle_fint_gnl": (I, [I, _ip, _dp, _ip, _dp, I, _dp, _dp, I]),
+        "oracle_newton_hex8": (I, [V, I, _ip, _dp, _ip, _dp, I, _dp, D, I, D, I, _dp, C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int)]),
         "oracle_sys_create": (V, [I]),
         "oracle_sys_destroy": (None, [V]),
         "oracle_sys_set_zero_diag": (None, [V, D]),
@@ -319,6 +324,26 @@ class System:
         rc = lib().oracle_csr_pcg_threaded(self._csr, _f64(b), x, eps, maxit, threads, C.byref(st))
         return rc, x, st
 
+    def assemble_gnl(self, params, order, u):
+        """The geometric-nonlinear tangent at total displacement u (hex8)."""
+        m = self.mesh
+        return lib().oracle_sys_assemble_gnl(self.h, m.nelem, _i32(m.conn).reshape(-1), _f64(m.xyz).reshape(-1),
+                                             _i32(m.first_dof), _f64(params).reshape(-1), int(order), _f64(u))
+
+    def newton(self, params, order, u0, max_residual=1e-10, max_newton=400, eps=1e-10, maxit=100000):
+        """BasicModel::iterate for hex8 elasticity (geometric nonlinear) from
+        the total displacement u0: (rc, u, history of max |R| per iteration,
+        Newton solves, PCG iterations in all)."""
+        m = self.mesh
+        u = _f64(u0).copy()
+        hist = np.zeros(max_newton + 1)
+        its, lin = C.c_int(0), C.c_int(0)
+        rc = lib().oracle_newton_hex8(self.h, m.nelem, _i32(m.conn).reshape(-1), _f64(m.xyz).reshape(-1),
+                                      _i32(m.first_dof), _f64(params).reshape(-1), int(order), u,
+                                      float(max_residual), int(max_newton), float(eps), int(maxit), hist,
+                                      C.byref(its), C.byref(lin))
+        return rc, u, hist[:its.value + 1], its.value, lin.value
+
     def heat_step(self, params, order, dt, u_s, alpha=1.0, eps=1e-10, maxit=10000):
         m = self.mesh
         st = SolveStats()
@@ -327,6 +352,27 @@ class System:
                                     _i32(m.first_dof), _f64(params).reshape(-1), order, dt, alpha, u,
                                     eps, maxit, C.byref(st))
         return rc, u, st
+
+
+def gnl_hex8(xyz, C36, ue, order=2):
+    """Geometric-nonlinear hex8 at nodal displacements ue (24): (tangent Ke
+    24 x 24 upper triangle, Fe 24) -- ElasticityElement3D with analysisType
+    GEOMETRIC_NONLINEAR."""
+    Ke, Fe = np.zeros(576), np.zeros(24)
+    st = lib().oracle_gnl_hex8(_f64(xyz).reshape(-1), _f64(C36).reshape(-1), int(order), _f64(ue).reshape(-1),
+                               Ke.ctypes.data, Fe.ctypes.data)
+    if st:
+        raise ArithmeticError(f"gnl_hex8 status {st}")
+    return Ke.reshape(24, 24), Fe
+
+
+def internal_force_gnl_hex8(mesh, params, order, u):
+    """sum_e Fe(u) of the geometric-nonlinear hex8 element over all rows."""
+    f = np.zeros(mesh.ndof)
+    st = lib().oracle_fint_gnl(mesh.nelem, _i32(mesh.conn).reshape(-1), _f64(mesh.xyz).reshape(-1),
+                               _i32(mesh.first_dof), _f64(params).reshape(-1), int(order), _f64(u), f, mesh.ndof)
+    assert st == 0
+    return f
 
 
 def internal_force_hex8(mesh, params, order, u, restrained=None):
@@ -753,6 +799,8 @@ class RefLeaf:
         self.lib.ref_heat_hex8_step_terms.argtypes = [I, _dp, _dp, _dp, I, _dp, D, D, D, _dp, _dp]
         self.lib.ref_elastic_quad4_ke.argtypes = [I, _dp, _dp, I, _dp]
         self.lib.ref_elastic_update.argtypes = [I, I, _dp, _dp, I, C.c_void_p, C.c_char_p, _dp, _dp, _dp]
+        self.lib.ref_elastic_update_analysis.argtypes = [I, I, _dp, _dp, I, C.c_void_p, C.c_char_p, I, _dp, _dp,
+                                                         _dp]
         self.lib.ref_elastic_vol_avg.argtypes = [I, I, _dp, _dp, I, _dp, _dp]
         self.lib.ref_heat_update.argtypes = [I, I, _dp, _dp, D, I, C.c_void_p, C.c_char_p, _dp, _dp]
         self.lib.ref_heat_hex8_k.argtypes = [I, _dp, _dp, I, _dp]
@@ -871,6 +919,20 @@ class RefLeaf:
         if rc:
             raise ValueError("ref_elastic_hex8_ke: non-positive Jacobian")
         return Ke.reshape(nel, 24, 24)
+
+    def elastic_update_gnl(self, X, C_mat, order, action, u):
+        """elastic_update with analysisType GEOMETRIC_NONLINEAR (the element of
+        BasicModel::iterate): (Ke upper triangle, Fe, integrals)."""
+        X = _f64(X)
+        dim, nnode = X.shape[1], X.shape[0]
+        n = dim * nnode
+        Ke, Fe, sums = np.zeros(n * n), np.zeros(n), np.zeros(18)
+        uv = _f64(u).reshape(-1).copy()
+        rc = self.lib.ref_elastic_update_analysis(dim, nnode, X.reshape(-1).copy(), _f64(C_mat).reshape(-1).copy(),
+                                                  int(order), uv.ctypes.data, action.encode(), 1, Ke, Fe, sums)
+        if rc:
+            raise ValueError("ref_elastic_update_analysis refused the element")
+        return Ke.reshape(n, n), Fe, sums.reshape(3, 6)
 
     def elastic_update(self, X, C_mat, order, action, u=None):
         """The reference's own element driver update(action, u) of

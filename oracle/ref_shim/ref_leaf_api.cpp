@@ -262,12 +262,14 @@ extern "C" {
 // (ndof x ndof, upper triangle), Fe (ndof) and sums (18: the element's
 // strain, stress and energy integrals, 6 each, as loopOverIntegrationPoints
 // adds them to the workspace totals).
-int ref_elastic_update(int dim, int nnode, const double* X, const double* C, int order, const double* u,
-                       const char* action, double* Ke, double* Fe, double* sums) {
+// analysis: BasicElement::analysisType (LINEAR 0, GEOMETRIC_NONLINEAR 1).
+int ref_elastic_update_analysis(int dim, int nnode, const double* X, const double* C, int order, const double* u,
+                                const char* action, int analysis, double* Ke, double* Fe, double* sums) {
   auto run = [&](auto& e, Matrix& K, std::vector<double>& fe, ElasticBag& bag) {
     std::vector<double> uu;
     if (u) uu.assign(u, u + e.numDof);
     std::string act(action);
+    e.analysisType = analysis;
     e.update(&act[0], u ? uu.data() : nullptr);
     const int n = e.numDof;
     for (int i = 0; i < n; ++i) {
@@ -280,6 +282,11 @@ int ref_elastic_update(int dim, int nnode, const double* X, const double* C, int
   if (dim == 3) return with_elastic<ElasticityElement3D>(3, nnode, X, C, order, run);
   if (dim == 2) return with_elastic<ElasticityElement2D>(2, nnode, X, C, order, run);
   return 1;
+}
+
+int ref_elastic_update(int dim, int nnode, const double* X, const double* C, int order, const double* u,
+                       const char* action, double* Ke, double* Fe, double* sums) {
+  return ref_elastic_update_analysis(dim, nnode, X, C, order, u, action, LINEAR, Ke, Fe, sums);
 }
 
 // The reference's own diffusion element driver: HeatTransferElement3Dtransient

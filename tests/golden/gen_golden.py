@@ -20,6 +20,11 @@ the compiled reference leaf library (``make -C oracle``):
   update("KF") and getVolAvgValues of both elasticity elements, and the
   diffusion elements' driver update("KM").
   These are outputs of the reference code itself (oracle/_ref).
+* ``ref_gnl.json`` -- the reference's own ElasticityElement3D with
+  analysisType GEOMETRIC_NONLINEAR (the element of BasicModel::iterate):
+  tangent and internal force of distorted hex8 elements at given
+  displacements (``python tests/golden/gen_golden.py gnl`` writes this file
+  alone).
 * ``ref_cg.json`` -- the reference's own Jacobi-PCG (sparse.cpp
   SymmetricSparseMatrix::solve, compiled unmodified with largeMatrix.cpp)
   on small assembled systems read by its own readMatrixAddressFormat from
@@ -222,6 +227,38 @@ def elastic_driver_case(r):
     va = r.elastic_vol_avg(X2, C3, 2, u2)
     # the plane element's getVolAvgValues fills 3 stress / strain components
     out["quad4"]["2"] = {"K": K.tolist(), "volume": float(va[0]), "stress": va[1:4].tolist(), "strain": va[7:10].tolist()}
+    return out
+
+
+def gnl_inputs():
+    """Distorted hex8 elements with general orthotropic constants and
+    displacements large enough for the nonlinear terms to matter."""
+    rng = np.random.default_rng(47)
+    cases = []
+    for k in range(3):
+        X = (np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], float)
+             * np.array([1.3, 0.8, 1.0]) + rng.uniform(-0.07, 0.07, (8, 3)))
+        m9 = [100.0 + 20 * k, 80.0, 120.0, 0.28, 0.31, 0.25, 30.0, 40.0, 35.0]
+        u = 0.1 * rng.normal(size=24)
+        cases.append((X, m9, u))
+    return cases
+
+
+def ref_gnl():
+    """The reference's own ElasticityElement3D with analysisType
+    GEOMETRIC_NONLINEAR (update "K" and "F" at displacements u): tangent
+    (upper triangle) and internal force, orders 2 and 3."""
+    r = bo.RefLeaf()
+    out = {"source": "reference ElasticityElement3D.cpp update('K'/'F') with analysisType GEOMETRIC_NONLINEAR "
+                     "(oracle/_ref)", "cases": []}
+    for X, m9, u in gnl_inputs():
+        C6 = bo.cmat_ortho3d(m9)
+        case = {"X": X.tolist(), "m9": m9, "u": u.tolist()}
+        for order in (2, 3):
+            K, _, _ = r.elastic_update_gnl(X, C6, order, "K", u)
+            _, F, _ = r.elastic_update_gnl(X, C6, order, "F", u)
+            case[str(order)] = {"K": np.triu(K).tolist(), "F": F.tolist()}
+        out["cases"].append(case)
     return out
 
 
@@ -455,6 +492,12 @@ def ref_internal_force():
 
 
 if __name__ == "__main__":
+    if sys.argv[1:] == ["gnl"]:  # only the geometric-nonlinear element's fixture
+        with open(os.path.join(OUT, "ref_gnl.json"), "w") as f:
+            json.dump(ref_gnl(), f)
+        sys.exit(0)
+    with open(os.path.join(OUT, "ref_gnl.json"), "w") as f:
+        json.dump(ref_gnl(), f)
     with open(os.path.join(OUT, "ref_quadrature.json"), "w") as f:
         json.dump(ref_quadrature(), f)
     with open(os.path.join(OUT, "ref_cg.json"), "w") as f:

@@ -638,3 +638,76 @@ def test_dof_numbering_and_node_records_equal_the_reference(oracle, abi, tmp_pat
     np.testing.assert_array_equal(xb, xyz)
     ours = path.read_bytes()[12:12 + 28 * m.nnode]  # after the three-int header
     assert ours == (tmp_path / "nodes.bin").read_bytes()
+
+
+def test_geometric_nonlinear_element_equals_the_reference(oracle):
+    """ElasticityElement3D with analysisType GEOMETRIC_NONLINEAR (the element of
+    BasicModel::iterate): B with the displacement-gradient terms, Green-Lagrange
+    strain, the initial-stress term (ElasticityElement3D.cpp:84-160, 560-641).
+    The oracle's tangent and internal force equal the reference's own code's
+    on distorted elements at large displacements (golden, and live where
+    oracle/_ref is built)."""
+    g = _load("ref_gnl.json")
+    live = oracle.RefLeaf() if oracle.RefLeaf.available() else None
+    for case in g["cases"]:
+        X, C6, u = np.array(case["X"]), oracle.cmat_ortho3d(case["m9"]), np.array(case["u"])
+        for order in (2, 3):
+            K, F = oracle.gnl_hex8(X, C6, u, order)
+            Kr, Fr = np.array(case[str(order)]["K"]), np.array(case[str(order)]["F"])
+            assert np.abs(np.triu(K) - Kr).max() <= 1e-15 * np.abs(Kr).max()
+            assert np.abs(F - Fr).max() <= 1e-15 * np.abs(Fr).max()
+            if live is not None:
+                Kl, _, _ = live.elastic_update_gnl(X, C6, order, "K", u)
+                _, Fl, _ = live.elastic_update_gnl(X, C6, order, "F", u)
+                np.testing.assert_array_equal(np.triu(Kl), Kr)
+                np.testing.assert_array_equal(Fl, Fr)
+
+
+def test_geometric_nonlinear_tangent_is_the_derivative_of_the_force(oracle):
+    """The tangent (material + initial-stress terms) is the derivative of the
+    internal force: central differences agree to the step's truncation."""
+    rng = np.random.default_rng(5)
+    X = np.array([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1], [1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], float)
+    X = X + 0.05 * rng.normal(size=X.shape)
+    C6 = oracle.cmat_ortho3d([100, 90, 110, 0.3, 0.25, 0.28, 40, 35, 45])
+    u = 0.1 * rng.normal(size=24)
+    K, _ = oracle.gnl_hex8(X, C6, u)
+    Kf = np.triu(K) + np.triu(K, 1).T
+    h = 1e-6
+    J = np.zeros((24, 24))
+    for j in range(24):
+        e = np.zeros(24)
+        e[j] = h
+        J[:, j] = (oracle.gnl_hex8(X, C6, u + e)[1] - oracle.gnl_hex8(X, C6, u - e)[1]) / (2 * h)
+    assert np.abs(J - Kf).max() <= 1e-8 * np.abs(Kf).max()
+    K0, F0 = oracle.gnl_hex8(X, C6, np.zeros(24))
+    _, KL = oracle.ke_hex8(X, C6)
+    np.testing.assert_allclose(np.triu(K0), np.triu(KL), rtol=0, atol=1e-13 * np.abs(KL).max())
+    assert np.abs(F0).max() == 0.0
+
+
+def test_newton_converges_quadratically_on_a_cantilever(oracle):
+    """BasicModel::iterate restated: from zero the first step is the linear
+    solution; the loop stops once max |R| < 1e-10, the last steps square the
+    residual, and a load 1000x smaller gives the linear answer."""
+    m = W.cantilever_hex8(nx=12, ny=2, nz=2, load=6.0)
+    s = oracle.System(m)
+    s.set_bc(m.restrained, m.prescribed, m.load)
+    s.build_pattern()
+    rc, u, hist, its, lin = s.newton(m.params, m.order, np.zeros(m.ndof), max_residual=1e-10, max_newton=40,
+                                     eps=1e-13)
+    assert rc == 0 and hist[-1] < 1e-10 and 3 <= its <= 20
+    assert hist[-2] < 1e-3 and hist[-1] < 10 * hist[-2] ** 1.5
+    ms = W.cantilever_hex8(nx=12, ny=2, nz=2, load=6e-3)
+    s2 = oracle.System(ms)
+    s2.set_bc(ms.restrained, ms.prescribed, ms.load)
+    s2.build_pattern()
+    rc, u2, _, _, _ = s2.newton(ms.params, ms.order, np.zeros(ms.ndof), max_residual=1e-14, max_newton=40, eps=1e-14)
+    s3 = oracle.System(ms)
+    s3.set_bc(ms.restrained, ms.prescribed, ms.load)
+    s3.build_pattern()
+    s3.assemble(ms.params, ms.order)
+    _, ulin, _ = s3.solve(eps=1e-14, maxit=100000)
+    assert np.linalg.norm(u2 - ulin) <= 2e-3 * np.linalg.norm(ulin)
+    tip = np.isclose(m.xyz[:, 0], m.meta["length"])
+    assert u[3 * np.nonzero(tip)[0] + 2].mean() > 1e3 * u2[3 * np.nonzero(tip)[0] + 2].mean()  # both negative
