@@ -93,6 +93,20 @@ class Solver:
         self.nnz_lower = int(nnz.value)
         return self.nnz_lower
 
+    def set_block_runs(self, run):
+        """Column runs of the FP32 block matrix: 3 (default) stores one column
+        index per run of up to three consecutive node columns where that
+        shrinks the matrix by 5 % or more, 1 one index per block.  Applies at
+        the next build_pattern."""
+        self._check(self.lib.beta_gpu_set_block_runs(self.h, int(run)), "set_block_runs")
+
+    def block_layout(self):
+        """(run length, value chunks, column chunks, bytes) of the FP32 block
+        matrix as built."""
+        out = (C.c_longlong * 4)()
+        self._check(self.lib.beta_gpu_block_layout(self.h, out, 4), "block_layout")
+        return tuple(int(v) for v in out)
+
     def pattern_lower(self):
         n = self.model.ndof
         rp = np.zeros(n + 1, dtype=np.int64)

@@ -621,7 +621,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     ElemArgs E;
     E.xyz = S.xyz; E.conn = S.conn; E.gparams = S.gparams; E.egroup = S.egroup; E.nparams = S.nparams;
     E.nip = S.nip; E.gt = S.gt; E.slot = S.slot; E.nrp = S.nrp; E.rest = S.rest; E.presc = S.presc;
-    E.bsoff = S.bsoff; E.bval = S.bval; E.soff = nullptr; E.ssoff = nullptr; E.sval = nullptr; E.pseudo = nullptr;
+    E.bsoff = S.bsoff; E.vpos = nullptr; E.bval = S.bval; E.soff = nullptr; E.ssoff = nullptr; E.sval = nullptr; E.pseudo = nullptr;
     E.kscale = 1.0; E.mscale = 0.0; E.flags = S.gflag;
     while (st.phase == kPhaseNew) {
       const int k = st.sub;

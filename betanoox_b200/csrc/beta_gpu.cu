@@ -150,7 +150,7 @@ struct beta_gpu_ctx {
   bool have_scalar = false;  // scalar FP64 layout built and uploaded
   HostPattern P;
   DBuf<int> elems, nrp, bsoff, bcol, ndiag, soff, scol;
-  DBuf<uint16_t> slot;
+  DBuf<uint16_t> slot, vpos;
   DBuf<long long> ssoff, sdiag;
   // matrices
   DBuf<double> sval, pseudo;
@@ -306,6 +306,7 @@ ElemArgs elem_args(beta_gpu_ctx* c) {
   A.rest = c->rest.p;
   A.presc = c->presc.p;
   A.bsoff = c->bsoff.p;
+  A.vpos = c->P.run > 1 ? c->vpos.p : nullptr;
   A.bval = c->bval.p;
   A.soff = c->soff.p;
   A.ssoff = c->ssoff.p;
@@ -477,8 +478,12 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
             A, c->p64.p, c->q64.p, c->st.p, c->partials.p);
       } else {
         BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p};
-        launch(c, k_spmv_dot_b<ND>, grid_for(c, (long long)c->P.nslice * 32, 256), 256, 0,
-            A, (const float*)c->v32[2].p, c->v32[3].p, c->st.p, c->partials.p);
+        if (c->P.run == 3)
+          launch(c, k_spmv_dot_b<ND, 3>, grid_for(c, (long long)c->P.nslice * 32, 256), 256, 0,
+              A, (const float*)c->v32[2].p, c->v32[3].p, c->st.p, c->partials.p);
+        else
+          launch(c, k_spmv_dot_b<ND, 1>, grid_for(c, (long long)c->P.nslice * 32, 256), 256, 0,
+              A, (const float*)c->v32[2].p, c->v32[3].p, c->st.p, c->partials.p);
       }
       if (sample) CK(cudaEventRecord(c->evs[2 * k + 1], c->stream));
       if constexpr (ND == 0) {
@@ -995,6 +1000,7 @@ int beta_gpu_create(beta_gpu_ctx** out, int device) {
   std::unique_ptr<beta_gpu_ctx> c(new beta_gpu_ctx());
   c->device = device;
   c->P.keep_scratch = true;  // a context rebuilds its structure into the same memory
+  c->P.run_request = 3;      // column runs where they shrink the FP32 matrix
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) { cudaGetLastError(); return BETA_GPU_ERR_CUDA; }
   beta_gpu_ctx* cp = c.get();
@@ -1048,6 +1054,28 @@ int beta_gpu_set_zero_diagonal(beta_gpu_ctx* c, double value) {
   if (!c) return BETA_GPU_ERR_ARG;
   if (!std::isfinite(value)) return fail(c, BETA_GPU_ERR_ARG, "the zero-diagonal replacement must be finite");
   c->zdiag = value;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_set_block_runs(beta_gpu_ctx* c, int run) {
+  if (!c) return BETA_GPU_ERR_ARG;
+  if (run != 1 && run != 3) return fail(c, BETA_GPU_ERR_ARG, "the column run length must be 1 or 3");
+  if (c->P.run_request != run && c->have_pattern) {
+    c->have_pattern = false;  // the next build_pattern lays the columns out anew
+    invalidate_matrices(c);
+  }
+  c->P.run_request = run;
+  return BETA_GPU_OK;
+}
+
+int beta_gpu_block_layout(const beta_gpu_ctx* c, long long* out, int n) {
+  if (!c || !out || n < 0 || n > 4) return BETA_GPU_ERR_ARG;
+  if (!c->have_pattern) return BETA_GPU_ERR_STATE;
+  const HostPattern& P = c->P;
+  const long long bb = (long long)P.ndpn * P.ndpn;
+  const long long v[4] = {P.run, P.nchunk, (long long)P.bcol.size() / 32,
+                          P.nchunk * 32 * bb * 4 + (long long)P.bcol.size() * 4};
+  for (int i = 0; i < n; ++i) out[i] = v[i];
   return BETA_GPU_OK;
 }
 
@@ -1177,6 +1205,7 @@ int beta_gpu_build_pattern(beta_gpu_ctx* c, long long* nnz_lower) {
   if ((rc = upload(c, c->bsoff, P.bsoff.data(), P.bsoff.size()))) return rc;
   if ((rc = upload(c, c->bcol, P.bcol.data(), P.bcol.size()))) return rc;
   if ((rc = upload(c, c->ndiag, P.ndiag.data(), P.ndiag.size()))) return rc;
+  if (P.run > 1 && (rc = upload(c, c->vpos, P.vpos.data(), P.vpos.size()))) return rc;
   CK(cudaStreamSynchronize(c->stream));
   c->have_pattern = true;
   c->have_scalar = false;
@@ -1457,9 +1486,17 @@ int beta_gpu_matvec(beta_gpu_ctx* c, int precision, const double* x, double* y) 
     BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p};
     const int g = grid_for(c, (long long)c->P.nslice * 32, 256), gn = grid_for(c, n, 256);
     launch(c, k_to32, gn, 256, 0, (long long)n, (const double*)c->t64.p, 1.0, c->v32[0].p);
-    if (c->ndpn == 3) launch(c, k_spmv_b<3>, g, 256, 0, A, (const float*)c->v32[0].p, c->v32[1].p);
-    else if (c->ndpn == 2) launch(c, k_spmv_b<2>, g, 256, 0, A, (const float*)c->v32[0].p, c->v32[1].p);
-    else launch(c, k_spmv_b<1>, g, 256, 0, A, (const float*)c->v32[0].p, c->v32[1].p);
+    const float* xv = c->v32[0].p;
+    float* yv = c->v32[1].p;
+    if (c->P.run == 3) {
+      if (c->ndpn == 3) launch(c, k_spmv_b<3, 3>, g, 256, 0, A, xv, yv);
+      else if (c->ndpn == 2) launch(c, k_spmv_b<2, 3>, g, 256, 0, A, xv, yv);
+      else launch(c, k_spmv_b<1, 3>, g, 256, 0, A, xv, yv);
+    } else {
+      if (c->ndpn == 3) launch(c, k_spmv_b<3>, g, 256, 0, A, xv, yv);
+      else if (c->ndpn == 2) launch(c, k_spmv_b<2>, g, 256, 0, A, xv, yv);
+      else launch(c, k_spmv_b<1>, g, 256, 0, A, xv, yv);
+    }
     CK(cudaMemsetAsync(c->y64.p, 0, sizeof(double) * n, c->stream));
     launch(c, k_axpy_from32, gn, 256, 0, (long long)n, c->y64.p, 1.0, (const float*)c->v32[1].p);
   }

@@ -33,8 +33,10 @@ struct ElemArgs {
   const int* nrp;             // node graph row pointers
   const unsigned char* rest;  // ndof
   const double* presc;        // ndof
-  // FP32 node-block sliced ELL target
+  // FP32 node-block sliced ELL target; vpos: the block's virtual position
+  // in its row for a layout of column runs (null: the graph position)
   const int* bsoff;
+  const uint16_t* vpos;
   float* bval;
   // FP64 scalar sliced ELL target (+ pseudo load)
   const int* soff;
@@ -59,13 +61,15 @@ __device__ __forceinline__ void stage_gauss(const GaussTable* gt, int nip, T* s_
 }
 
 // ---- scatter of one ND x ND block K (row-major) for the node pair (I,J) --
-// FP32 node-block layout: block (I, pos) lives in chunk bsoff[I/32] + pos,
-// entry (i,j) at chunk*32*ND*ND + (i*ND+j)*32 + I%32.  Restrained rows and
+// FP32 node-block layout: block (I, pos) lives in chunk bsoff[I/32] + v,
+// v = pos (one column per block) or vpos[nrp[I] + pos] (column runs), entry
+// (i,j) at chunk*32*ND*ND + (i*ND+j)*32 + I%32.  Restrained rows and
 // columns stay zero; their diagonal is set to 1 afterwards (equation.cpp:500).
 template <int ND>
 __device__ __forceinline__ void scatter_block32(const ElemArgs& A, int I, int J, int pos,
                                                 const float* K) {
-  const long long chunk = (long long)A.bsoff[I >> 5] + pos;
+  const int v = A.vpos ? (int)A.vpos[A.nrp[I] + pos] : pos;
+  const long long chunk = (long long)A.bsoff[I >> 5] + v;
   float* base = A.bval + chunk * (32 * ND * ND) + (I & 31);
 #pragma unroll
   for (int i = 0; i < ND; ++i) {

@@ -51,6 +51,8 @@ static void reset_keep(HostPattern& P) {
   P.scol.clear();
   P.ncol.clear();
   P.bcol.clear();
+  P.vpos.clear();
+  P.run = 1;
   P.slot.clear();
   P.ssoff.clear();
   P.sdiag.clear();
@@ -67,6 +69,102 @@ static void release_scratch(HostPattern& P) {
   std::vector<int>().swap(P.s_ufree);
   std::vector<uint64_t>().swap(P.s_used);
   std::vector<std::vector<int>>().swap(P.s_mark);
+}
+
+// Column storage of the node-block layout for a caller that accepts runs
+// (P.run_request = R > 1): one column index per run of up to R consecutive
+// node columns when that makes the FP32 matrix (values + columns) at least
+// 5 % smaller than one index per block, else one per block.  The rows are
+// in ncol; ndiag holds graph positions on entry and virtual ones on exit.
+// A row's runs are formed greedily over its ascending columns: a run starts
+// at the first column not yet covered (moved back to nnode - R at the end of
+// the node range, so its R gathers stay in bounds) and covers every column
+// below its start + R.  The runs of a row ascend, so the SpMV visits the
+// non-zero blocks in the same column order as the one-index layout and
+// adds exact zeros between them.
+static void build_columns(HostPattern& P) {
+  const int nnode = P.nnode, R = P.run_request, bb = P.ndpn * P.ndpn;
+  P.run = 1;
+  P.vpos.clear();
+  auto runs_of = [&](long long i, auto&& emit) {
+    const int q0 = P.nrp[i], len = P.nrp[i + 1] - q0;
+    const int* c = P.ncol.data() + q0;
+    int m = 0;
+    for (int k = 0; k < len; ++m) {
+      const int s0 = std::min(c[k], nnode - R);
+      emit(m, s0);
+      for (; k < len && c[k] < s0 + R; ++k) P.vpos[q0 + k] = (uint16_t)(R * m + (c[k] - s0));
+    }
+    return m;
+  };
+  std::vector<int> wr(P.nslice, 0);
+  if (nnode >= R) {
+    parallel_for(P.nslice, [&](long long lo, long long hi) {
+      for (long long s = lo; s < hi; ++s) {
+        int w = 0;
+        for (long long i = s * 32; i < std::min<long long>(nnode, s * 32 + 32); ++i) {
+          const int q0 = P.nrp[i], len = P.nrp[i + 1] - q0;
+          const int* c = P.ncol.data() + q0;
+          int m = 0;
+          for (int k = 0; k < len; ++m) {
+            const int s0 = std::min(c[k], nnode - R);
+            while (k < len && c[k] < s0 + R) ++k;
+          }
+          w = std::max(w, m);
+        }
+        wr[s] = w;
+      }
+    });
+  }
+  long long nrc = 0;
+  int wmax = 0;
+  for (int w : wr) {
+    nrc += w;
+    wmax = std::max(wmax, w);
+  }
+  const double run_bytes = (double)nrc * 32 * (4.0 + 4.0 * R * bb);
+  const double ell_bytes = (double)P.nchunk * 32 * (4.0 + 4.0 * bb);
+  const bool use_runs = nnode >= R && (long long)R * wmax <= 65535 && R * nrc * 32LL * bb <= 2000000000LL &&
+                        run_bytes <= 0.95 * ell_bytes;
+  if (!use_runs) {
+    P.bcol.resize((size_t)P.nchunk * 32);
+    parallel_for(P.nslice, [&](long long lo, long long hi) {
+      for (long long s = lo; s < hi; ++s) {
+        const int w = P.bsoff[s + 1] - P.bsoff[s];
+        for (int l = 0; l < 32; ++l) {
+          const long long i = s * 32 + l;
+          int* bc = P.bcol.data() + (size_t)P.bsoff[s] * 32 + l;
+          int k = 0;
+          if (i < nnode)
+            for (int q = P.nrp[i]; q < P.nrp[i + 1]; ++q, ++k) bc[(size_t)k * 32] = P.ncol[q];
+          for (; k < w; ++k) bc[(size_t)k * 32] = i < nnode ? (int)i : 0;
+        }
+      }
+    });
+    return;
+  }
+  P.run = R;
+  for (int s = 0; s < P.nslice; ++s) P.bsoff[s + 1] = P.bsoff[s] + R * wr[s];
+  P.nchunk = P.bsoff[P.nslice];
+  P.bcol.resize((size_t)nrc * 32);
+  P.vpos.resize((size_t)P.nblk);
+  parallel_for(P.nslice, [&](long long lo, long long hi) {
+    for (long long s = lo; s < hi; ++s) {
+      const long long r0 = P.bsoff[s] / R;
+      const int w = wr[s];
+      for (int l = 0; l < 32; ++l) {
+        const long long i = s * 32 + l;
+        int* bc = P.bcol.data() + (size_t)r0 * 32 + l;
+        int m = 0;
+        if (i < nnode) {
+          m = runs_of(i, [&](int k, int s0) { bc[(size_t)k * 32] = s0; });
+          P.ndiag[i] = P.vpos[P.nrp[i] + P.ndiag[i]];
+        }
+        const int pad = i < nnode ? std::min((int)i, nnode - R) : 0;
+        for (; m < w; ++m) bc[(size_t)m * 32] = pad;
+      }
+    }
+  });
 }
 
 std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* conn,
@@ -297,7 +395,9 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   P.ndiag.resize(nnode);
   const int npair = nnpe * nnpe;
   P.slot.resize((size_t)nelem * npair);
-  P.bcol.resize((size_t)P.nchunk * 32);
+  // with runs requested the columns are laid out after the fill (build_columns)
+  const bool ell_now = P.run_request <= 1;
+  if (ell_now) P.bcol.resize((size_t)P.nchunk * 32);
   std::vector<long long> lower(nck, 0);
   parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
     const Span sp = span[ck];
@@ -334,11 +434,13 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
                                    : std::lower_bound(buf.begin(), buf.end(), ce[b]) - buf.begin());
         }
       }
-      const long long s = i / 32;
-      const int w = P.bsoff[s + 1] - P.bsoff[s];
-      int* bc = P.bcol.data() + (size_t)P.bsoff[s] * 32 + (i % 32);
-      for (int k = 0; k < len; ++k) bc[(size_t)k * 32] = buf[k];
-      for (int k = len; k < w; ++k) bc[(size_t)k * 32] = (int)i;
+      if (ell_now) {
+        const long long s = i / 32;
+        const int w = P.bsoff[s + 1] - P.bsoff[s];
+        int* bc = P.bcol.data() + (size_t)P.bsoff[s] * 32 + (i % 32);
+        for (int k = 0; k < len; ++k) bc[(size_t)k * 32] = buf[k];
+        for (int k = len; k < w; ++k) bc[(size_t)k * 32] = (int)i;
+      }
       if (icnt[i] == icnt[i + 1]) {  // a node in no element: its rows hold the diagonal alone
         acc += ndpn;
         continue;
@@ -358,9 +460,13 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     lower[ck] = acc;
   });
   // lanes past the last node in the last slice
-  for (int i = nnode; i < P.nslice * 32; ++i) {
-    const int s = i / 32, w = P.bsoff[s + 1] - P.bsoff[s];
-    for (int k = 0; k < w; ++k) P.bcol[(size_t)(P.bsoff[s] + k) * 32 + (i % 32)] = 0;
+  if (ell_now) {
+    for (int i = nnode; i < P.nslice * 32; ++i) {
+      const int s = i / 32, w = P.bsoff[s + 1] - P.bsoff[s];
+      for (int k = 0; k < w; ++k) P.bcol[(size_t)(P.bsoff[s] + k) * 32 + (i % 32)] = 0;
+    }
+  } else {
+    build_columns(P);
   }
   P.nnz_lower = 0;
   for (long long v : lower) P.nnz_lower += v;
@@ -511,7 +617,7 @@ void export_lower_values_block(const HostPattern& P, const unsigned char* rest, 
     }
     for (int q = P.nrp[I]; q < P.nrp[I + 1]; ++q) {
       int J = P.ncol[q];
-      long long ch = chunk0 + (q - P.nrp[I]);
+      long long ch = chunk0 + (P.run > 1 ? (int)P.vpos[q] : q - P.nrp[I]);
       for (int j = 0; j < nd; ++j) {
         int c = J * nd + j;
         if (rest[c] || c > r) continue;

@@ -56,7 +56,7 @@ struct HostPattern {
   // node graph (CSR over nodes, columns ascending, self included)
   std::vector<int> nrp;       // nnode+1
   FillVec<int> ncol;          // nblk
-  std::vector<int> ndiag;     // position of node i in its own row
+  std::vector<int> ndiag;     // virtual position of node i's diagonal block in its row
   long long nblk = 0;
   // nodes that no element uses, ascending: their rows are the diagonal alone
   // in the reference's pattern (Equations gives an empty row its diagonal),
@@ -71,11 +71,22 @@ struct HostPattern {
   // element -> position of node J in node I's row, nelem * nnpe * nnpe
   FillVec<uint16_t> slot;
 
-  // node-block sliced ELL: slice s covers nodes [32s, 32s+32)
+  // node-block sliced ELL: slice s covers nodes [32s, 32s+32).  Values:
+  // block (I, virtual position v) at chunk bsoff[I/32] + v, entry t at
+  // (chunk*ND*ND + t)*32 + I%32.  Columns: with run == 1 one per block
+  // (virtual position = graph position); with run == R > 1 one per run of R
+  // consecutive node columns J0..J0+R-1 (chunks bsoff[s] + R*k .. + R*k+R-1
+  // share the column bcol[(bsoff[s]/R + k)*32 + lane] = J0), so a row of a
+  // lexicographically numbered hex mesh stores 9 column indices instead of
+  // 27; block (I, graph position q) sits at virtual position
+  // vpos[nrp[I] + q] = R*k + (J - J0), and the run's other slots are zero.
+  int run_request = 1;        // input: the largest run the caller accepts (1 or 3)
+  int run = 1;                // the run length built
   int nslice = 0;
-  std::vector<int> bsoff;     // nslice+1, in chunks (one chunk = 32 blocks)
-  FillVec<int> bcol;          // nchunk*32, padding points at the row's own node
-  long long nchunk = 0;
+  std::vector<int> bsoff;     // nslice+1, in (virtual) chunks of 32 blocks
+  FillVec<int> bcol;          // nchunk/run*32, padding points at the row's own node
+  FillVec<uint16_t> vpos;     // run > 1: nblk virtual positions (empty otherwise)
+  long long nchunk = 0;       // virtual chunks (value storage = nchunk*32*ND*ND floats)
 
   // scalar sliced ELL over dofs (restrained rows: diagonal only; restrained
   // columns removed), slice s covers rows [32s, 32s+32)

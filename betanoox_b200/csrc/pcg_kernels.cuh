@@ -357,61 +357,81 @@ struct BlockMat {
 
 // NC: gather x through the read-only cache (only when x is not written
 // during the kernel).
-// U: chunks whose loads are issued together (more bytes in flight per warp
-// for kernels with few warps per SM).
-template <int ND, bool PADDED, bool NC = true, int U = 2>
+// U: column chunks whose loads are issued together (more bytes in flight per
+// warp for kernels with few warps per SM).
+// R: the layout's run length: each column index J0 serves R consecutive
+// value chunks, for node columns J0 .. J0+R-1 (R = 1: one index per block).
+// The blocks are visited in ascending column order for every R, and a run's
+// empty slots hold zeros, so both layouts give the same sums.
+template <int ND, bool PADDED, bool NC = true, int U = 2, int R = 1>
 __device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane, const float* x, float* acc) {
   constexpr int BB = ND * ND;
-  const int c0 = A.bsoff[s], w = A.bsoff[s + 1] - c0;
-  const int* cp = A.bcol + (long long)c0 * 32 + lane;
+  const int c0 = A.bsoff[s], w = (A.bsoff[s + 1] - c0) / R;
+  const int* cp = A.bcol + (long long)(c0 / R) * 32 + lane;
   const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
 #pragma unroll
   for (int i = 0; i < ND; ++i) acc[i] = 0.f;
 #pragma unroll U
   for (int k = 0; k < w; ++k) {
-    const int J = __ldcs(cp + k * 32);
-    float xv[ND];
-    if constexpr (PADDED) {
-      if constexpr (NC) PVec<ND>::ldg(x, J, xv);
-      else PVec<ND>::ld(x, J, xv);
-    } else {
-      if constexpr (NC) NodeIO<ND>::ldg(x, J, xv);
-      else NodeIO<ND>::ld(x, J, xv);
+    const int J0 = __ldcs(cp + k * 32);
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int J = J0 + j;
+      float xv[ND];
+      if constexpr (PADDED) {
+        if constexpr (NC) PVec<ND>::ldg(x, J, xv);
+        else PVec<ND>::ld(x, J, xv);
+      } else {
+        if constexpr (NC) NodeIO<ND>::ldg(x, J, xv);
+        else NodeIO<ND>::ld(x, J, xv);
+      }
+      float v[BB];
+#pragma unroll
+      for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + ((long long)(k * R + j) * BB + t) * 32);
+#pragma unroll
+      for (int i = 0; i < ND; ++i)
+#pragma unroll
+        for (int jj = 0; jj < ND; ++jj) acc[i] = fmaf(v[i * ND + jj], xv[jj], acc[i]);
     }
-    float v[BB];
-#pragma unroll
-    for (int t = 0; t < BB; ++t) v[t] = __ldcs(vp + (long long)k * 32 * BB + t * 32);
-#pragma unroll
-    for (int i = 0; i < ND; ++i)
-#pragma unroll
-      for (int j = 0; j < ND; ++j) acc[i] = fmaf(v[i * ND + j], xv[j], acc[i]);
   }
 }
 
-template <int ND>
+// Loads in flight and resident blocks of the inner SpMV per layout, from
+// measurements on the 100^3 cube (ND 3) and the 256x256x64 slab (ND 1):
+// one column per block: four chunks per lane, 4 x 256 threads per SM;
+// runs of 3 (ND 3): one run (27 values, 3 gathers) per lane, 4 blocks per SM;
+// runs of 3 (ND 1): two runs per lane, 8 blocks per SM.
+template <int ND, int R>
+struct SpmvShape {
+  static constexpr int U = R == 1 ? 4 : (ND == 3 ? 1 : 2);
+  static constexpr int MINB = (R > 1 && ND == 1) ? 8 : 4;
+};
+
+template <int ND, int R = 1>
 __global__ void __launch_bounds__(256) k_spmv_b(BlockMat A, const float* __restrict__ x, float* __restrict__ y) {
   const int lane = threadIdx.x & 31;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslice; s += (gridDim.x * blockDim.x) >> 5) {
     float acc[ND];
-    spmv_row_b<ND, false>(A, s, lane, x, acc);
+    spmv_row_b<ND, false, true, 2, R>(A, s, lane, x, acc);
     const int I = s * 32 + lane;
     if (I < A.nnode) NodeIO<ND>::st(y, I, acc);
   }
 }
 
 // q = A p, alpha = rho / (p.q)
-// Four chunks' loads in flight per lane (1024 threads per SM at up to 64
-// registers): 6 % faster than two at eight 256-thread blocks per SM on the
-// 100^3 cube, bit-identical (the same sums in the same order).
-template <int ND>
-__global__ void __launch_bounds__(256, 4) k_spmv_dot_b(BlockMat A, const float* __restrict__ p,
+// One column per block: four chunks' loads in flight per lane (1024 threads
+// per SM at up to 64 registers), 6 % faster than two at eight 256-thread
+// blocks per SM on the 100^3 cube, bit-identical (the same sums in the same
+// order).  Runs of 3 columns: 10 % (ND 3) and 30 % (ND 1) faster again.
+template <int ND, int R = 1>
+__global__ void __launch_bounds__(256, SpmvShape<ND, R>::MINB) k_spmv_dot_b(BlockMat A, const float* __restrict__ p,
                                                        float* __restrict__ q, PcgState* st, double* partials) {
   if (st->done) return;
   const int lane = threadIdx.x & 31;
   double acc_d[1] = {0.0};
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslice; s += (gridDim.x * blockDim.x) >> 5) {
     float acc[ND];
-    spmv_row_b<ND, true, true, 4>(A, s, lane, p, acc);
+    spmv_row_b<ND, true, true, SpmvShape<ND, R>::U, R>(A, s, lane, p, acc);
     const int I = s * 32 + lane;
     if (I < A.nnode) {
       NodeIO<ND>::st(q, I, acc);

@@ -7,7 +7,10 @@
 // node).  Each mesh is also built single-threaded, which must give the same
 // result, and a hash of every field is printed, so that a build compiled with
 // BETA_PATTERN_MARK_BUDGET=0 (the bandwidth-sized marker form on every mesh)
-// can be compared with the default one.  Exit code 0 when every build matches.
+// can be compared with the default one.  Every mesh is built a second time
+// with column runs allowed (run_request 3, fresh and into a second reused
+// pattern), which must keep every field but the column layout and place
+// every block where its run says.  Exit code 0 when every build matches.
 #include "../../betanoox_b200/csrc/pattern.hpp"
 
 #include <algorithm>
@@ -29,7 +32,40 @@ static bool equal(const HostPattern& P, const HostPattern& Q) {
          same(P.slot, Q.slot) && P.nslice == Q.nslice && same(P.bsoff, Q.bsoff) && same(P.bcol, Q.bcol) &&
          P.nchunk == Q.nchunk && P.nsslice == Q.nsslice && same(P.ssoff, Q.ssoff) && same(P.scol, Q.scol) &&
          same(P.soff, Q.soff) && same(P.srowlen, Q.srowlen) && same(P.sdiag, Q.sdiag) &&
-         P.nnz_full == Q.nnz_full && P.nnz_lower == Q.nnz_lower;
+         P.nnz_full == Q.nnz_full && P.nnz_lower == Q.nnz_lower && P.run == Q.run && same(P.vpos, Q.vpos);
+}
+
+// A build with runs allowed (R) against the one-column-per-block build E of
+// the same mesh: the same graph, colouring, slot map and scalar layout; and,
+// when runs were chosen, every block (I, q) at a distinct virtual position of
+// its row whose run column + offset is its column, the diagonal remapped,
+// every run inside the node range.  Prints the run length chosen.
+static bool runs_valid(const HostPattern& P, const HostPattern& E, const char* name) {
+  bool ok = same(P.nrp, E.nrp) && same(P.ncol, E.ncol) && same(P.slot, E.slot) && same(P.color_ptr, E.color_ptr) &&
+            same(P.elem_by_color, E.elem_by_color) && same(P.ssoff, E.ssoff) && same(P.scol, E.scol) &&
+            same(P.soff, E.soff) && same(P.sdiag, E.sdiag) && P.nnz_lower == E.nnz_lower && P.nslice == E.nslice;
+  if (P.run == 1) {
+    ok = ok && equal(P, E);
+  } else {
+    const int R = P.run;
+    ok = ok && (long long)P.vpos.size() == P.nblk && P.nchunk == P.bsoff[P.nslice] &&
+         (long long)P.bcol.size() * R == P.nchunk * 32;
+    for (int s = 0; ok && s <= P.nslice; ++s) ok = P.bsoff[s] % R == 0;
+    for (size_t k = 0; ok && k < P.bcol.size(); ++k) ok = P.bcol[k] >= 0 && P.bcol[k] <= P.nnode - R;
+    std::vector<char> seen;
+    for (int I = 0; ok && I < P.nnode; ++I) {
+      const int s = I / 32, lane = I % 32, w = P.bsoff[s + 1] - P.bsoff[s];
+      seen.assign(w, 0);
+      for (int q = P.nrp[I]; ok && q < P.nrp[I + 1]; ++q) {
+        const int v = P.vpos[q];
+        ok = v < w && !seen[v] && P.bcol[((size_t)P.bsoff[s] / R + v / R) * 32 + lane] + v % R == P.ncol[q];
+        if (ok) seen[v] = 1;
+      }
+      ok = ok && P.ndiag[I] == P.vpos[P.nrp[I] + E.ndiag[I]];
+    }
+  }
+  std::printf("runs %-55s run=%d %s\n", name, P.run, ok ? "valid" : "INVALID");
+  return ok;
 }
 
 static unsigned long long hash_of(const HostPattern& P) {
@@ -37,7 +73,8 @@ static unsigned long long hash_of(const HostPattern& P) {
   auto mix = [&](long long v) { h ^= (unsigned long long)v; h *= 1099511628211ull; };
   auto all = [&](const auto& a) { mix((long long)a.size()); for (size_t i = 0; i < a.size(); ++i) mix(a[i]); };
   all(P.nrp); all(P.ncol); all(P.ndiag); all(P.color_ptr); all(P.elem_by_color); all(P.slot); all(P.bsoff);
-  all(P.bcol); all(P.ssoff); all(P.scol); all(P.soff); all(P.srowlen); all(P.sdiag); all(P.unused);
+  all(P.bcol); all(P.ssoff); all(P.scol); all(P.soff); all(P.srowlen); all(P.sdiag); all(P.unused); all(P.vpos);
+  mix(P.run);
   mix(P.nblk); mix(P.ncolor); mix(P.nchunk); mix(P.nnz_full); mix(P.nnz_lower);
   return h;
 }
@@ -101,8 +138,10 @@ int main() {
   std::vector<Mesh> meshes = {hex8(6, 3, false, 0),  hex8(24, 3, false, 0), hex8(24, 1, true, 3),
                               quad4_with_extras(150, 90), hex8(40, 3, true, 5), hex8(5, 1, false, 0),
                               hex8(24, 3, false, 0)};
-  HostPattern reused;
+  HostPattern reused, reused_runs;
   reused.keep_scratch = true;
+  reused_runs.keep_scratch = true;
+  reused_runs.run_request = 3;
   int bad = 0;
   for (const Mesh& M : meshes) {
     std::vector<int> fd(M.nnode);
@@ -130,6 +169,16 @@ int main() {
     std::printf("%-60s %s\n", M.name.c_str(), ok ? "equal" : "DIFFERENT");
     std::printf("hash %-55s %016llx\n", M.name.c_str(), hash_of(fresh));
     bad += ok ? 0 : 1;
+    // the column-run layout, fresh and rebuilt into reused memory
+    HostPattern runs;
+    runs.run_request = 3;
+    const std::string e4 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, M.conn.data(), fd.data(),
+                                                  M.rest.data(), runs, true);
+    const std::string e5 = betagpu::build_pattern(M.nnode, M.nelem, M.nnpe, M.nd, M.conn.data(), fd.data(),
+                                                  M.rest.data(), reused_runs, true);
+    const bool rok = e4.empty() && e5.empty() && runs_valid(runs, fresh, M.name.c_str()) && equal(runs, reused_runs);
+    std::printf("hash runs %-50s %016llx\n", M.name.c_str(), hash_of(runs));
+    bad += rok ? 0 : 1;
   }
   // invalid input is refused with its message, on any thread count
   {

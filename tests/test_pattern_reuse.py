@@ -1,7 +1,9 @@
 """Host structure build reused by a solver context (HostPattern::keep_scratch):
 a pattern rebuilt into the memory of an earlier, different mesh equals a
-fresh build in every field, and so does a single-threaded build (tests/cpp/pattern_reuse_check.cpp, compiled
-here against the host sources; no GPU needed)."""
+fresh build in every field, and so does a single-threaded build; the
+column-run layout of the FP32 block matrix places every block in its run
+(tests/cpp/pattern_reuse_check.cpp, compiled here against the host sources;
+no GPU needed)."""
 import os
 import subprocess
 
@@ -16,6 +18,13 @@ def _run(tmp_path, name, extra):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count(" equal") == 7
+    assert r.stdout.count(" valid") == 7 and "INVALID" not in r.stdout
+    # lexicographic hex8 grids and the quad4 plate take runs of 3; the
+    # shuffled numberings keep one column per block
+    runs = dict(line[5:].rsplit(" run=", 1) for line in r.stdout.splitlines() if line.startswith("runs "))
+    for name, tail in runs.items():
+        want = "1" if "shuffled" in name else "3"
+        assert tail.split()[0] == want, (name, tail)
     assert "NOT REFUSED" not in r.stdout and r.stdout.count("refused") == 1
     return [line for line in r.stdout.splitlines() if line.startswith("hash ")]
 
@@ -29,4 +38,4 @@ def test_reused_pattern_equals_fresh_build(tmp_path):
     bounded = _run(tmp_path, "pattern_reuse_check_bounded", ["-DBETA_PATTERN_MARK_BUDGET=0"])
     sorted_rows = _run(tmp_path, "pattern_reuse_check_sorted", ["-DBETA_PATTERN_MARK_BUDGET=0",
                                                                   "-DBETA_PATTERN_SPAN_CAP=0"])
-    assert len(default) == 7 and default == bounded == sorted_rows
+    assert len(default) == 14 and default == bounded == sorted_rows
