@@ -75,11 +75,16 @@ class Solver:
         fd = np.ascontiguousarray(m.first_dof, dtype=np.int32)
         self._check(self.lib.beta_gpu_mesh_upload(self.h, m.kind, m.ndim, m.nnode, _ptr(xyz), m.nelem, m.nnpe,
                                                   _ptr(conn), _ptr(fd), m.ndpn, m.order), "mesh_upload")
-        p = np.ascontiguousarray(m.params if params is None else params, dtype=np.float64)
+        self.load_materials(m.params if params is None else params, elem_group)
+        self.set_bc(m.restrained, m.prescribed, m.load)
+
+    def load_materials(self, params, elem_group=None):
+        """Material parameters per group (one group per element without
+        elem_group); the assembled matrices are rebuilt at their next use."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
         eg = None if elem_group is None else np.ascontiguousarray(elem_group, dtype=np.int32)
         self._check(self.lib.beta_gpu_materials_upload(self.h, p.shape[0], p.shape[1], _ptr(p), _ptr(eg)),
                     "materials_upload")
-        self.set_bc(m.restrained, m.prescribed, m.load)
 
     def set_bc(self, restrained, prescribed, load):
         r = np.ascontiguousarray(restrained, dtype=np.uint8)
@@ -99,6 +104,12 @@ class Solver:
         shrinks the matrix by 5 % or more, 1 one index per block.  Applies at
         the next build_pattern."""
         self._check(self.lib.beta_gpu_set_block_runs(self.h, int(run)), "set_block_runs")
+
+    def set_operator_cache(self, on):
+        """Keep the FP64 element matrices of a hex8 diffusion mesh on the
+        device for the FP64 operator (True, the default) or integrate them at
+        every use (False)."""
+        self._check(self.lib.beta_gpu_set_operator_cache(self.h, 1 if on else 0), "set_operator_cache")
 
     def block_layout(self):
         """(run length, value chunks, column chunks, bytes) of the FP32 block

@@ -130,6 +130,7 @@ SIGNATURES = {
     "beta_gpu_build_pattern": (_I, [_P, C.POINTER(C.c_longlong)]),
     "beta_gpu_set_block_runs": (_I, [_P, _I]),
     "beta_gpu_block_layout": (_I, [_P, C.POINTER(C.c_longlong), _I]),
+    "beta_gpu_set_operator_cache": (_I, [_P, _I]),
     "beta_gpu_pattern_lower": (_I, [_P, _P, _P]),
     "beta_gpu_pattern_lower_host": (_I, [_I, _I, _I, _I, _P, _P, _P, C.POINTER(C.c_longlong), _P, _P]),
     "beta_gpu_assemble": (_I, [_P, _I, _I, _D, _D]),

@@ -138,6 +138,13 @@ struct beta_gpu_ctx {
   // materials
   int ngroups = 0, nparams = 0;
   DBuf<double> gparams;
+  // cached FP64 element matrices of the operator (hex8 diffusion): built at
+  // the first operator use after the mesh, materials or element order change
+  DBuf<double> mfc;
+  bool mfc_on = true, mfc_valid = false;
+  // per-iteration log rate of the last PCG loop's stop quantity (0: unknown),
+  // for sizing the first chunk of the next loop
+  double lnrate = 0.0;
   DBuf<int> egroup;
   bool have_egroup = false, have_mat = false;
   // boundary conditions
@@ -289,6 +296,7 @@ bool all_finite(const double* a, size_t n) {
 void invalidate_matrices(beta_gpu_ctx* c) {
   c->have64 = c->have32 = false;
   c->minv_kind = -1;
+  c->lnrate = 0.0;
 }
 
 // ---- element launches (colour by colour) ----------------------------------
@@ -351,6 +359,28 @@ int launch_assembly(beta_gpu_ctx* c, const ElemArgs& A, const double* ugnl = nul
 bool is_diffusion(int kind) { return kind == BETA_GPU_HEX8_HEAT || kind == BETA_GPU_QUAD4_HEAT; }
 
 // y = K (c1 w1 + c2 w2) + cm M w1 (FP64, matrix-free), y zeroed first.
+// Builds the cached element matrices of a hex8 diffusion mesh when they are
+// enabled, not yet built and fit in a quarter of the free device memory
+// (otherwise the operator keeps integrating on the fly).
+int ensure_mfc(beta_gpu_ctx* c, const MfArgs& A) {
+  if (c->mfc_valid || !c->mfc_on || c->kind != BETA_GPU_HEX8_HEAT) return BETA_GPU_OK;
+  const size_t vals = (size_t)((c->nelem + 31) / 32) * 32 * kMfcHeat;
+  if (c->mfc.n != vals) {
+    c->mfc.release();
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    if (vals * sizeof(double) > fr / 4) return BETA_GPU_OK;
+    CK(c->mfc.alloc(vals));
+  }
+  launch(c, k_mfc_build_hex8_heat<0>, grid_for(c, c->nelem, 256), 256, 0, A, (const int*)c->elems.p, c->nelem,
+         c->mfc.p);
+  launch(c, k_mfc_build_hex8_heat<1>, grid_for(c, c->nelem, 256), 256, 0, A, (const int*)c->elems.p, c->nelem,
+         c->mfc.p);
+  CKL("k_mfc_build_hex8_heat");
+  c->mfc_valid = true;
+  return BETA_GPU_OK;
+}
+
 int mf_apply(beta_gpu_ctx* c, double c1, const double* w1, double c2, const double* w2, double cm,
              double* y) {
   MfArgs A;
@@ -364,7 +394,19 @@ int mf_apply(beta_gpu_ctx* c, double c1, const double* w1, double c2, const doub
   A.c1 = c1;
   A.c2 = c2;
   A.cm = cm;
+  int rc;
+  if ((rc = ensure_mfc(c, A)) != BETA_GPU_OK) return rc;
   CK(cudaMemsetAsync(y, 0, sizeof(double) * c->ndof, c->stream));
+  if (c->mfc_valid) {
+    for (int col = 0; col < c->P.ncolor; ++col) {
+      const int beg = c->P.color_ptr[col], nel = c->P.color_ptr[col + 1] - beg;
+      if (nel == 0) continue;
+      launch(c, k_mfc_apply_hex8_heat, grid_for(c, nel, 256), 256, 0, (const int*)c->conn.p,
+             (const int*)c->elems.p, beg, nel, (const double*)c->mfc.p, c1, c2, cm, w1, w2, y);
+      CKL("k_mfc_apply_hex8_heat launch");
+    }
+    return BETA_GPU_OK;
+  }
   for (int col = 0; col < c->P.ncolor; ++col) {
     const int beg = c->P.color_ptr[col], nel = c->P.color_ptr[col + 1] - beg;
     if (nel == 0) continue;
@@ -463,14 +505,38 @@ inline bool prof_sample(int k, int ce) {
   return ce < kProfEvery ? k == ce / 2 : k % kProfEvery == kProfEvery / 2;
 }
 
+// Host polling of the device-side PCG: a chunk of iterations is launched, the
+// state read back, and so on until the state says done.  The iterations of a
+// chunk that follow the one that ends the loop cost a few microseconds per
+// launch for nothing (each kernel returns at once), and a chunk that ends
+// short costs a host round trip; so a chunk is sized to end a little past
+// the predicted end, from the rate at which the loop's stop quantity has
+// been falling (log-linear between the first poll and the latest one; for
+// the first chunk, the rate of the context's previous loop), within
+// [kMinChunk, check_every].
+constexpr int kMinChunk = 4;
+
+inline double stop_quantity(const PcgState& s) {
+  return s.rule == kRuleReliable ? s.rr : s.last * s.last;
+}
+inline double stop_target(const PcgState& s) {
+  return s.rule == kRuleReliable ? std::max(s.tolabs2, s.delta2 * s.maxrr) : s.tol2;
+}
+
 template <int ND>
 int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
   const int ce = std::max(1, check_every);
   int rc;
   if (prof && prof->on && (rc = ensure_events(c, 2 * ce)) != BETA_GPU_OK) return rc;
+  int n = ce;
+  // a reliable-update loop ends when r.r has fallen by delta2 from its start
+  if (c->h_st->rule == kRuleReliable && c->lnrate < 0.0 && c->h_st->delta2 > 0.0)
+    n = std::min(ce, std::max(kMinChunk, (int)(0.85 * std::log(c->h_st->delta2) / c->lnrate)));
+  double g0 = -1.0;
+  int it0 = 0;
   for (;;) {
-    for (int k = 0; k < ce; ++k) {
-      const bool sample = prof && prof->on && prof_sample(k, ce);
+    for (int k = 0; k < n; ++k) {
+      const bool sample = prof && prof->on && prof_sample(k, n);
       if (sample) CK(cudaEventRecord(c->evs[2 * k], c->stream));
       if constexpr (ND == 0) {
         ScalarMat A{c->ndof, c->P.nsslice, c->ssoff.p, c->scol.p, c->sval.p};
@@ -503,18 +569,34 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
     PcgState s;
     if ((rc = read_state(c, &s)) != BETA_GPU_OK) return rc;
     if (prof && prof->on) {
-      int real = std::min(ce, std::max(0, s.iter - before) + (s.done && s.status == kStatusBreakdown ? 1 : 0));
+      int real = std::min(n, std::max(0, s.iter - before) + (s.done && s.status == kStatusBreakdown ? 1 : 0));
       for (int k = 0; k < real; ++k) {
-        if (!prof_sample(k, ce)) continue;
+        if (!prof_sample(k, n)) continue;
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->evs[2 * k], c->evs[2 * k + 1]));
         prof->ms += ms;
         prof->launches += 1;
       }
     }
+    const double g = stop_quantity(s);
+    const bool measured = g0 > 0.0 && g > 0.0 && s.iter > it0;
+    const double lr = measured ? std::log(g / g0) / (s.iter - it0) : c->lnrate;
     if (s.done) {
+      if (measured && lr < 0.0 && std::isfinite(lr)) c->lnrate = lr;
       *out = s;
       return BETA_GPU_OK;
+    }
+    if (g0 <= 0.0 && g > 0.0) {
+      g0 = g;
+      it0 = s.iter;
+    }
+    const double target = stop_target(s);
+    n = ce;
+    if (lr < 0.0 && std::isfinite(lr) && target > 0.0 && g > target) {
+      const double left = std::log(target / g) / lr;
+      if (left < ce) n = std::min(ce, std::max(kMinChunk, (int)std::ceil(left) + 2));
+    } else if (target > 0.0 && g <= target) {
+      n = kMinChunk;
     }
   }
 }
@@ -1068,6 +1150,14 @@ int beta_gpu_set_block_runs(beta_gpu_ctx* c, int run) {
   return BETA_GPU_OK;
 }
 
+int beta_gpu_set_operator_cache(beta_gpu_ctx* c, int on) {
+  if (!c || (on != 0 && on != 1)) return BETA_GPU_ERR_ARG;
+  c->mfc_on = on != 0;
+  c->mfc_valid = false;
+  if (!on) c->mfc.release();
+  return BETA_GPU_OK;
+}
+
 int beta_gpu_block_layout(const beta_gpu_ctx* c, long long* out, int n) {
   if (!c || !out || n < 0 || n > 4) return BETA_GPU_ERR_ARG;
   if (!c->have_pattern) return BETA_GPU_ERR_STATE;
@@ -1129,6 +1219,7 @@ int beta_gpu_mesh_upload(beta_gpu_ctx* c, int kind, int ndim, int nnode, const d
   c->have_bc = false;
   c->have_mat = false;
   c->have_u = c->have_us = false;
+  c->mfc_valid = false;
   invalidate_matrices(c);
   return BETA_GPU_OK;
 }
@@ -1153,6 +1244,7 @@ int beta_gpu_materials_upload(beta_gpu_ctx* c, int ngroups, int nparams, const d
   c->ngroups = ngroups;
   c->nparams = nparams;
   c->have_mat = true;
+  c->mfc_valid = false;
   invalidate_matrices(c);
   return BETA_GPU_OK;
 }
@@ -1209,6 +1301,7 @@ int beta_gpu_build_pattern(beta_gpu_ctx* c, long long* nnz_lower) {
   CK(cudaStreamSynchronize(c->stream));
   c->have_pattern = true;
   c->have_scalar = false;
+  c->mfc_valid = false;  // the cache follows the colour order of the elements
   invalidate_matrices(c);
   if (nnz_lower) *nnz_lower = P.nnz_lower;
   return BETA_GPU_OK;

@@ -393,4 +393,121 @@ __global__ void __launch_bounds__(256) k_mf_hex8_heat_t(MfArgs A, const int* __r
     mf_hex8_heat_elem(A, elems[i], w1, w2, y, s_dN, s_N, s_w);
 }
 
+// ---- cached FP64 element matrices of the hex8 diffusion operator ----------
+// For a mesh whose conductivity and capacity do not change between applies
+// (linear k, the transient steps and repeated solves), the element integrals
+// K_e = int k grad N grad N^T and M_e = int c N N^T are computed once and the
+// operator y = K (c1 w1 + c2 w2) + cm M w1 reads them instead of
+// re-integrating: 72 FP64 values per element (the upper triangles, 36 + 36)
+// against about 2,400 FP64 multiply-adds at 2x2x2 Gauss points.  Layout:
+// element k of the colour-ordered list holds value t at
+// (k/32)*72*32 + t*32 + k%32, so a warp of consecutive threads reads 256
+// contiguous bytes per value.  Upper-triangle index of (a, b), a <= b:
+// a*8 - a*(a-1)/2 + (b - a).
+constexpr int kMfcHeat = 72;
+
+__device__ __forceinline__ int tri8(int a, int b) { return a * 8 - (a * (a - 1)) / 2 + (b - a); }
+
+// One thread per element; KM = 0 integrates K_e, KM = 1 M_e (two passes keep
+// the accumulators and the Gauss-point gradients in registers).
+template <int KM>
+__global__ void __launch_bounds__(256) k_mfc_build_hex8_heat(MfArgs A, const int* __restrict__ elems, int nel,
+                                                              double* __restrict__ cache) {
+  __shared__ double s_dN[kMaxIP * 24];
+  __shared__ double s_N[kMaxIP * 8];
+  __shared__ double s_w[kMaxIP];
+  for (int i = threadIdx.x; i < A.nip * 24; i += blockDim.x)
+    s_dN[i] = A.gt->dN[i / 24][(i / 8) % 3][i % 8];
+  for (int i = threadIdx.x; i < A.nip * 8; i += blockDim.x) s_N[i] = A.gt->N[i / 8][i % 8];
+  for (int i = threadIdx.x; i < A.nip; i += blockDim.x) s_w[i] = A.gt->w[i];
+  __syncthreads();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nel; k += gridDim.x * blockDim.x) {
+    const int e = elems[k];
+    const int* ce = A.conn + (long long)e * 8;
+    double x[8][3];
+    const int n0 = ce[0];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) x[a][c] = A.xyz[3LL * ce[a] + c] - A.xyz[3LL * n0 + c];
+    const double* pm = A.gparams + (long long)(A.egroup ? A.egroup[e] : e) * A.nparams;
+    const double k0 = pm[0], k1 = pm[1], k2 = pm[2], cap = pm[3];
+    double acc[36];
+#pragma unroll
+    for (int t = 0; t < 36; ++t) acc[t] = 0.0;
+    for (int ip = 0; ip < A.nip; ++ip) {
+      const double* d = s_dN + ip * 24;
+      const double* N = s_N + ip * 8;
+      double M[9];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          double t = 0.0;
+#pragma unroll
+          for (int a = 0; a < 8; ++a) t += d[r * 8 + a] * x[a][c];
+          M[r * 3 + c] = t;
+        }
+      double Mi[9];
+      const double fw = inv3<double>(M, Mi) * s_w[ip];
+      if constexpr (KM == 0) {
+        double g[3][8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+          g[0][a] = Mi[0] * d[a] + Mi[1] * d[8 + a] + Mi[2] * d[16 + a];
+          g[1][a] = Mi[3] * d[a] + Mi[4] * d[8 + a] + Mi[5] * d[16 + a];
+          g[2][a] = Mi[6] * d[a] + Mi[7] * d[8 + a] + Mi[8] * d[16 + a];
+        }
+        const double w0 = fw * k0, w1 = fw * k1, w2 = fw * k2;
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+          for (int b = a; b < 8; ++b)
+            acc[tri8(a, b)] += w0 * g[0][a] * g[0][b] + w1 * g[1][a] * g[1][b] + w2 * g[2][a] * g[2][b];
+      } else {
+        const double wm = fw * cap;
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+          for (int b = a; b < 8; ++b) acc[tri8(a, b)] += wm * N[a] * N[b];
+      }
+    }
+    double* out = cache + (long long)(k >> 5) * kMfcHeat * 32 + KM * 36 * 32 + (k & 31);
+#pragma unroll
+    for (int t = 0; t < 36; ++t) out[t * 32] = acc[t];
+  }
+}
+
+// y += K_e (c1 w1 + c2 w2) + cm M_e w1 over the elements [beg, beg+nel) of
+// the colour-ordered list (one colour: no two elements share a node).
+__global__ void __launch_bounds__(256) k_mfc_apply_hex8_heat(const int* __restrict__ conn,
+    const int* __restrict__ elems, int beg, int nel, const double* __restrict__ cache, double c1, double c2,
+    double cm, const double* __restrict__ w1, const double* __restrict__ w2, double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nel; i += gridDim.x * blockDim.x) {
+    const int k = beg + i;
+    const int* ce = conn + (long long)elems[k] * 8;
+    int nd[8];
+    double vk[8], vm[8], f[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      nd[a] = ce[a];
+      vm[a] = w1[nd[a]];
+      vk[a] = c1 * vm[a] + (w2 ? c2 * w2[nd[a]] : 0.0);
+      f[a] = 0.0;
+    }
+    const double* Kc = cache + (long long)(k >> 5) * kMfcHeat * 32 + (k & 31);
+    const double* Mc = Kc + 36 * 32;
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+      for (int b = a; b < 8; ++b) {
+        const double kv = __ldcs(Kc + tri8(a, b) * 32), mv = cm * __ldcs(Mc + tri8(a, b) * 32);
+        f[a] += kv * vk[b] + mv * vm[b];
+        if (b != a) f[b] += kv * vk[a] + mv * vm[a];
+      }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) y[nd[a]] += f[a];
+  }
+}
+
 }  // namespace betagpu

@@ -182,6 +182,15 @@ BETA_GPU_API int beta_gpu_build_pattern(beta_gpu_ctx* ctx, long long* nnz_lower)
  * the same either way.  Takes effect at the next beta_gpu_build_pattern (a
  * built pattern is dropped when the value changes). */
 BETA_GPU_API int beta_gpu_set_block_runs(beta_gpu_ctx* ctx, int run);
+/* FP64 element matrices of the hex8 diffusion operator kept on the device (no
+ * counterpart in the reference, which integrates its elements at every
+ * assembly).  With on = 1 (the default) the first FP64 operator use after a
+ * mesh, material or pattern change integrates K_e and M_e of every element
+ * once (72 doubles per element, built only when they fit in a quarter of the
+ * free device memory), and the FP64 residuals of mixed-precision solves and
+ * the transient right-hand sides read them instead of integrating again;
+ * on = 0 integrates at every use.  Results agree to rounding. */
+BETA_GPU_API int beta_gpu_set_operator_cache(beta_gpu_ctx* ctx, int on);
 /* The layout built: out[0] run length (1 or 3), out[1] value chunks of 32
  * blocks, out[2] column chunks of 32 indices, out[3] bytes of values and
  * columns.  n <= 4.  BETA_GPU_ERR_STATE before the pattern is built. */
