@@ -148,6 +148,19 @@ def _pinned_copy(a):
     return t.numpy()
 
 
+def _phase_shares(d, d0=None):
+    """Shares of the systems' group device time (kernel timers): setup
+    (assembly, factors, first residual), reliable updates (FP64 residual
+    replacements) and inner iterations."""
+    g = lambda k: d[k] - (d0[k] if d0 else 0)
+    busy = g("sys_busy_ns")
+    if busy <= 0:
+        return None
+    setup, repl = g("sys_setup_ns"), g("sys_repl_ns")
+    return {"setup": setup / busy, "reliable_updates": repl / busy, "iterations": (busy - setup - repl) / busy,
+            "group_s": busy / 1e9}
+
+
 def spmv_algorithmic_bytes(nblk, nnode, nd, ncols=None):
     """Per launch of the FP32 node-block SpMV: the nd*nd FP32 values of every
     non-zero block once, the layout's 4-byte column indices once (ncols: one
@@ -1124,7 +1137,12 @@ def run_batch(args, nested=False):
             "per_step_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
             "batch": {"ms_steps": ms, "iterations_total": int(sum(iters)), "iterations_max": int(max(iters)),
                       "not_converged": bad[:5], "n_not_converged": len(bad), "setup_s": {"generate": t_gen,
-                      "add_many": t_add, "autotune": t_tune}},
+                      "add_many": t_add, "autotune": t_tune},
+                      "group_time_share": _phase_shares(b.info()),
+                      # the systems whose groups ran longest in the last launch, against the launch
+                      "longest_systems": [{"n": models[k].meta["n"], "iterations": res[k][2].iterations,
+                                           "group_ms": round(res[k][2].ms_solve, 2)}
+                                          for k in sorted(range(len(res)), key=lambda k: -res[k][2].ms_solve)[:4]]},
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clk.summary(),
         }
         if errs:
@@ -1267,7 +1285,10 @@ def run_serve(args, nested=False):
     cap_n = min(args.capacity_requests, pool_n)
     for _ in range(args.warmup):
         _serve_stream(srv, models[:min(cap_n, 32)], np.zeros(min(cap_n, 32)), th)
+    sc0 = srv.stats()
     res_cap, wall_cap = _serve_stream(srv, models[:cap_n], np.zeros(cap_n), th)
+    sc1 = srv.stats()
+    cap_busy = (sc1["busy_us"] - sc0["busy_us"]) / 1e6 / wall_cap
     cap_rps = cap_n / wall_cap
     cap_dofs = sum(r[1] for r in res_cap) / wall_cap
     lam = args.load * cap_rps
@@ -1292,20 +1313,33 @@ def run_serve(args, nested=False):
         if args.serve_fp64_sample:
             from betanoox_b200 import Solver
             tw, d64 = 0.0, 0
+            # one context for every request, as a single-system server would
+            # keep it (its buffers are reused; a context per request would add
+            # its creation and teardown to each request)
+            g = Solver(dev)
+            ph = np.zeros(5)
+            o64 = opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=args.tol)
             for m in models[:args.serve_fp64_sample]:
-                t1 = time.perf_counter()
-                g = Solver(dev)
+                t = [time.perf_counter()]
                 g.load_model(m)
+                t.append(time.perf_counter())
                 g.build_pattern()
+                t.append(time.perf_counter())
                 g.assemble(_abi.FP64)
-                g.solve(opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=args.tol))
+                t.append(time.perf_counter())
+                g.solve(o64)
+                t.append(time.perf_counter())
                 g.download()
-                g.close()
-                tw += time.perf_counter() - t1
+                t.append(time.perf_counter())
+                ph += np.diff(t)
+                tw += t[-1] - t[0]
                 d64 += m.ndof
+            g.close()
             fp64 = {"value": ws * d64 / tw, "requests": min(args.serve_fp64_sample, len(models)),
-                    "how": "sequential requests through the single-system API, plain FP64 Jacobi-PCG, "
-                           "host structure build + upload + assembly + solve + download"}
+                    "phases_s": dict(zip(["upload", "structure", "assembly", "solve", "download"],
+                                         [round(float(v), 4) for v in ph])),
+                    "how": "sequential requests through the single-system API on one reused context, plain "
+                           "FP64 Jacobi-PCG: host structure build + upload + assembly + solve + download"}
         fams = {}
         for j in range(len(res)):
             f = models[j % len(models)].meta["family"]
@@ -1328,7 +1362,9 @@ def run_serve(args, nested=False):
                       "max_final_norm": float(max(r[4] for r in res)), "launches": s1["launches"] - s0["launches"],
                       "busy_frac": (s1["busy_us"] - s0["busy_us"]) / 1e6 / wall, "wall_s": wall,
                       "generate_s": t_gen,
-                      "capacity_burst": {"requests": cap_n, "wall_s": wall_cap, "dofs_per_s": cap_dofs}},
+                      "capacity_burst": {"requests": cap_n, "wall_s": wall_cap, "dofs_per_s": cap_dofs,
+                                         "busy_frac": cap_busy, "group_time_share": _phase_shares(sc1, sc0)},
+                      "group_time_share": _phase_shares(s1, s0)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": s1["h2d"] - s0["h2d"],
                     "d2h_bytes_per_step": s1["d2h"] - s0["d2h"],
                     "includes": "arrival to result on host: structure build, admission, solve, download"},

@@ -459,7 +459,7 @@ class Batch:
             raise self._err(st, "batch_reset")
 
     INFO = ["live", "used", "pool", "launches", "h2d", "d2h", "last_launch_ns", "gangs", "gang_ctas", "threads",
-            "gang_boost"]
+            "gang_boost", "sys_busy_ns", "sys_setup_ns", "sys_repl_ns", "iterations"]
 
     def info(self):
         a = (C.c_longlong * len(self.INFO))()
@@ -474,7 +474,8 @@ class Server:
     retires each as soon as it converges."""
 
     STATS = ["submitted", "done", "rejected", "failed", "cancelled", "queued", "running", "launches",
-             "pool_used", "pool_bytes", "busy_us", "h2d", "d2h"]
+             "pool_used", "pool_bytes", "busy_us", "h2d", "d2h", "sys_busy_ns", "sys_setup_ns", "sys_repl_ns",
+             "iterations"]
 
     def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, max_systems: int = 4096, o=None,
                  iters_per_launch: int = 200, threads: int = 0, gang_boost: int = -1, slice_us: int = 0):

@@ -11,6 +11,15 @@ struct beta_gpu_batch {
   int device = 0;
   int nsm = 148;
   cudaStream_t stream = nullptr;
+  // uploads of admitted systems and downloads of results, which may overlap
+  // a launch on `stream`; a launch waits for ev_copy when uploads are pending
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev_copy = nullptr;
+  bool copy_pending = false;
+  // set during a sliced launch to end its slice early (batch_preempt), after
+  // at least min_slice_ns; zeroed before every launch
+  int* d_preempt = nullptr;
+  long long min_slice_ns = 2000000LL;
   std::string err;
   // pool
   unsigned char* pool = nullptr;
@@ -24,6 +33,8 @@ struct beta_gpu_batch {
     long long work = 0;  // stored FP32 matrix values
     int nslice = 0;
     long long served = 0;  // last launch in which the system made progress
+    int last_iters = 0;    // inner iterations of its last completed solve (0: none yet)
+    bool fresh = false;    // admitted after the launch in flight was issued: not in it
     BSys desc;
     BState st;
   };
@@ -61,6 +72,9 @@ struct beta_gpu_batch {
   int last_ngang = 0, last_gang_ctas = 0;
   std::map<int, cudaGraphExec_t> graphs;
   long long n_launch = 0, n_h2d = 0, n_d2h = 0;
+  // group device time of removed systems: in all, in setup, in reliable
+  // updates; and their inner iterations (live systems are added on query)
+  long long rm_busy_ns = 0, rm_setup_ns = 0, rm_repl_ns = 0, rm_iters = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket the last launch on `stream`
   float last_ms = 0.f;
   static constexpr int kMaxCtas = 4096;
@@ -165,10 +179,10 @@ SysLayout layout_for(int ndim, int nnode, int nelem, int nnpe, int ndpn, int ngr
   return L;
 }
 
-int batch_h2d(beta_gpu_batch* b, void* dst, const void* src, size_t bytes) {
+int batch_h2d(beta_gpu_batch* b, void* dst, const void* src, size_t bytes, cudaStream_t st = nullptr) {
   if (!bytes) return BETA_GPU_OK;
   b->n_h2d += (long long)bytes;
-  BCK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st ? st : b->stream));
   return BETA_GPU_OK;
 }
 
@@ -314,12 +328,30 @@ int gang_plan(int na, const long long* work, const int* nslice, int nctas, int w
   return ngang;
 }
 
-// Gang plan of one launch over act[0..na) (sorted largest first) into h_plan.
+// Expected remaining cost of a system, the weight of the gang plan: its stored
+// matrix values x the inner iterations it still needs.  The iterations are
+// those of its last completed solve when it has one (a repeat solve after a
+// reset), else an estimate that grows like the number of nodes along one side
+// of the mesh, nnode^(1/ndim) (CG iterations on these elliptic systems grow
+// with the elements along a side), less the iterations already done (at least
+// a tenth is kept).  Weighting by size alone gave every system about its
+// share of the CTAs by size, so the largest, which also need the most
+// iterations, held the launch long after the others had finished (64 RVEs:
+// the launch took exactly as long as its slowest system).
+long long plan_weight(const beta_gpu_batch::Sys& S) {
+  double it = S.last_iters > 0 ? (double)S.last_iters
+                                : std::pow((double)std::max(1, S.nnode), 1.0 / (double)std::max(1, S.ndim));
+  it = std::max(0.1 * it, it - (double)S.st.iter);
+  return std::max(1LL, (long long)((double)S.work * it));
+}
+
+// Gang plan of one launch over act[0..na) (sorted by plan weight, largest
+// first) into h_plan.
 int batch_plan(beta_gpu_batch* b, const int* act, int na, int nctas) {
   std::vector<long long> work(na);
   std::vector<int> nsl(na), g(std::max(1, na));
   for (int i = 0; i < na; ++i) {
-    work[i] = b->sys[act[i]].work;
+    work[i] = plan_weight(b->sys[act[i]]);
     nsl[i] = b->sys[act[i]].nslice;
   }
   const int ngang = gang_plan(na, work.data(), nsl.data(), nctas, b->threads / 32, b->gang_boost, g.data());
@@ -338,10 +370,15 @@ int batch_plan(beta_gpu_batch* b, const int* act, int na, int nctas) {
 // Uploads descriptors of live systems, the active list (unfinished, largest
 // first) and the parameters; returns the number of active systems.
 int batch_prepare(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, int* nactive) {
+  if (b->copy_pending) {  // systems admitted since the last launch: their uploads first
+    BCK(cudaStreamWaitEvent(b->stream, b->ev_copy, 0));
+    b->copy_pending = false;
+  }
+  for (auto& S : b->sys) S.fresh = false;
   int na = 0;
   std::vector<std::pair<long long, int>> order;
   for (int i = 0; i < (int)b->sys.size(); ++i)
-    if (b->sys[i].live && b->sys[i].st.phase != kPhaseDone) order.push_back({-b->sys[i].work, i});
+    if (b->sys[i].live && b->sys[i].st.phase != kPhaseDone) order.push_back({-plan_weight(b->sys[i]), i});
   std::sort(order.begin(), order.end());
   for (auto& w : order) b->h_active[na++] = w.second;
   for (int i = 0; i < (int)b->sys.size(); ++i)
@@ -364,6 +401,9 @@ int batch_prepare(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int budget, i
   P.spin_ns = b->spin_ns;  // default 2 s at one barrier: far beyond any phase of a resident gang
   P.switch_iters = b->switch_iters;
   P.slice_ns = b->slice_ns;
+  P.preempt = b->d_preempt;
+  P.min_slice_ns = b->min_slice_ns;
+
   int rc;
   if (!b->sys.empty() && (rc = batch_h2d(b, b->d_sys, b->h_sys, sizeof(BSys) * b->sys.size()))) return rc;
   if ((rc = batch_h2d(b, b->d_active, b->h_active, sizeof(int) * std::max(1, na)))) return rc;
@@ -382,7 +422,7 @@ int batch_pull_states(beta_gpu_batch* b) {
   BCK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   for (size_t i = 0; i < n; ++i) {
-    if (!b->sys[i].live) continue;
+    if (!b->sys[i].live || b->sys[i].fresh) continue;  // a fresh system keeps its initial state
     const BState& s = b->h_states[i];
     if (s.iter != b->sys[i].st.iter || s.phase != b->sys[i].st.phase) b->sys[i].served = b->n_launch;
     b->sys[i].st = s;
@@ -394,6 +434,9 @@ int batch_pull_states(beta_gpu_batch* b) {
 int batch_reset_states(beta_gpu_batch* b) {
   if (b->sys.empty()) return BETA_GPU_OK;
   for (size_t i = 0; i < b->sys.size(); ++i) {
+    const BState& o = b->sys[i].st;
+    if (b->sys[i].live && o.phase == kPhaseDone && o.status == kBConverged && o.iter > 0)
+      b->sys[i].last_iters = o.iter;
     BState s;
     std::memset(&s, 0, sizeof(s));
     s.phase = b->sys[i].live ? kPhaseNew : kPhaseDone;

@@ -46,6 +46,8 @@ struct BState {
   float bt;    // FP32 mode: beta of the direction update the next SpMV applies
   int pb;      // FP32 mode: which direction buffer holds the current p (0: p32, 1: p32b)
   long long busy_ns;  // device time spent on the system (its group's, summed over launches)
+  long long setup_ns; // of which in the setup (assembly, factors, row sums, first residual)
+  long long repl_ns;  // of which in reliable updates (FP64 matrix-free residual and restart)
   int sub;            // setup: the next step (kPhaseNew)
 };
 
@@ -94,7 +96,16 @@ struct BParams {
   long long spin_ns;            // longest wait at a gang barrier before the launch gives up
   int switch_iters;             // FP32 cycle longer than this: continue in FP64 (0: never)
   long long slice_ns;           // time slice: systems stop after the iteration in which it ends (0: none)
+  // With a time slice, the slice also ends once *preempt is non-zero (the
+  // server sets it when it has admitted new work) and min_slice_ns have passed.
+  const int* preempt;
+  long long min_slice_ns;
 };
+
+// The slice is over early: new work is waiting for the next launch.
+__device__ __forceinline__ bool slice_preempted(const BParams& P, long long elapsed) {
+  return P.preempt != nullptr && elapsed >= P.min_slice_ns && *(const volatile int*)P.preempt != 0;
+}
 
 // Per CTA: the gang it belongs to for this launch.
 struct BPlan {
@@ -111,6 +122,7 @@ struct GangShared {
   // time-slice bookkeeping of the system being solved (thread 0 only; kept
   // here rather than in registers, which the SpMV loop needs)
   long long t_in, t_mark;
+  long long t_repl;  // start of the reliable update in progress (0: none)
   int stop_sent;
   double wred[2][8];
   double red[2];
@@ -576,7 +588,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
       const long long now = globaltimer_ns();
       const long long t_step = now - g.gs->t_mark;
       g.gs->t_mark = now;
-      if (now + t_step - g.t0 >= P.slice_ns) {
+      if (now + t_step - g.t0 >= P.slice_ns || slice_preempted(P, now - g.t0)) {
         *stop_at = (unsigned)(st.iter + 1);
         g.gs->stop_sent = 1;
       }
@@ -704,7 +716,8 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
         if (a2[1] == 0.0 || st.rn <= P.tol * st.bn) { st.phase = kPhaseDone; st.status = kBConverged; }
         break;
       }
-      if (P.slice_ns > 0 && tid == 0 && !g.gs->stop_sent && globaltimer_ns() - g.t0 >= P.slice_ns) {
+      if (P.slice_ns > 0 && tid == 0 && !g.gs->stop_sent &&
+          (globaltimer_ns() - g.t0 >= P.slice_ns || slice_preempted(P, globaltimer_ns() - g.t0))) {
         *stop_step = (unsigned)k;
         g.gs->stop_sent = 1;
       }
@@ -715,12 +728,18 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
         break;
       }
     }
+    if (tid == 0) st.setup_ns += globaltimer_ns() - g.gs->t_in;
   }
 
   const double tolabs2 = (0.5 * P.tol * st.bn) * (0.5 * P.tol * st.bn);
   const double delta2 = P.delta * P.delta;
   int spent = 0;
+  if (threadIdx.x == 0) g.gs->t_repl = 0;
   while (st.phase == kPhaseIter && (P.budget <= 0 || spent < P.budget) && !slice_end) {
+    if (tid == 0 && g.gs->t_repl) {
+      st.repl_ns += globaltimer_ns() - g.gs->t_repl;
+      g.gs->t_repl = 0;
+    }
     if (st.mode == 1) {
       // ---- FP64 vectors and arithmetic on the FP32 row-sum matrix, with the
       // same reliable updates (restrained dofs stay fixed)
@@ -777,6 +796,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
       if (a2[1] > st.maxrr) st.maxrr = a2[1];
       double beta;
       if (a2[1] < tolabs2 || a2[1] < delta2 * st.maxrr || st.iter >= P.maxit) {
+        if (tid == 0) g.gs->t_repl = globaltimer_ns();
         // reliable update: fold the correction into x (x changes only here,
         // so its rounding does not pile up over the iterations), r64 = the
         // FP64 matrix-free true residual
@@ -892,6 +912,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     if (a2[1] > st.maxrr) st.maxrr = a2[1];
     const bool long_cycle = P.switch_iters > 0 && st.iter - st.cycle0 >= P.switch_iters;
     if (a2[1] < tolabs2 || a2[1] < delta2 * st.maxrr || st.iter >= P.maxit || long_cycle) {
+      if (tid == 0) g.gs->t_repl = globaltimer_ns();
       // reliable update: fold y into x, replace r by the FP64 true residual
       for (int i = tid; i < n; i += nt) { S.x64[i] += (double)S.y32[i]; S.y32[i] = 0.f; }
       if (!gsync(g)) return aborted();
@@ -933,6 +954,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     st.bt = (float)beta;  // applied by the next SpMV's gather
   }
   if (tid == 0) {
+    if (g.gs->t_repl) st.repl_ns += globaltimer_ns() - g.gs->t_repl;
     st.busy_ns += globaltimer_ns() - g.gs->t_in;
     *S.st = st;
   }
@@ -985,7 +1007,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_batch_solve(const BSys* __restri
       // past the time slice no CTA starts another system, and an assembly,
       // which is not cut short, starts only in the first half of it
       const long long el = globaltimer_ns() - t0;
-      const bool over = P.slice_ns > 0 && el >= P.slice_ns;
+      const bool over = P.slice_ns > 0 && (el >= P.slice_ns || slice_preempted(P, el));
       const int k = (*(volatile int*)gabort || over) ? P.nactive : P.nbig + atomicAdd(counter, 1);
       gs.skip = k < P.nactive && P.slice_ns > 0 && 2 * el > P.slice_ns && sys[active[k]].st->phase == kPhaseNew;
       gs.idx = k;

@@ -965,7 +965,12 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   unsigned char* base = b->pool + off;
   const GaussTable* gt = batch_gauss(b, Q.ndim, Q.order);
   int rc = gt ? BETA_GPU_OK : BETA_GPU_ERR_CUDA;
-  auto up = [&](size_t o, const void* src, size_t bytes) { if (!rc) rc = batch_h2d(b, base + o, src, bytes); };
+  // on the copy stream: a launch may be running on b->stream meanwhile (the
+  // memory is free pool space that no running system uses); the next launch
+  // waits for these copies (batch_prepare)
+  auto up = [&](size_t o, const void* src, size_t bytes) {
+    if (!rc) rc = batch_h2d(b, base + o, src, bytes, b->copy);
+  };
   up(L.o_xyz, Q.xyz.data(), sizeof(double) * Q.xyz.size());
   up(L.o_conn, Q.conn.data(), sizeof(int) * Q.conn.size());
   up(L.o_gp, Q.gp.data(), sizeof(double) * Q.gp.size());
@@ -980,15 +985,17 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   up(L.o_ndiag, P.ndiag.data(), sizeof(int) * P.ndiag.size());
   up(L.o_bsoff, P.bsoff.data(), sizeof(int) * P.bsoff.size());
   up(L.o_bcol, P.bcol.data(), sizeof(int) * P.bcol.size());
-  if (rc == BETA_GPU_OK && cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); rc = BETA_GPU_ERR_CUDA; }
   beta_gpu_batch::Sys& S = b->sys[id];
   if (rc != BETA_GPU_OK) {
+    cudaStreamSynchronize(b->copy);
+    cudaGetLastError();
     pool_free(b, off, L.total);
     S.live = false;
     b->free_ids.push_back(id);
     return bfail(b, rc, "upload of the system failed");
   }
   S.live = true;
+  S.last_iters = 0;
   S.kind = Q.kind; S.ndim = Q.ndim; S.nnode = Q.nnode; S.nelem = Q.nelem; S.nnpe = Q.nnpe; S.ndpn = Q.ndpn;
   S.ndof = (int)ndof; S.order = Q.order; S.off = (size_t)off; S.bytes = L.total;
   S.work = (long long)P.nchunk * 32 * Q.ndpn * Q.ndpn;
@@ -1038,9 +1045,63 @@ int admit_system(beta_gpu_batch* b, const PreparedSys& Q, int* sys_id) {
   s0.status = kBRunning;
   S.st = s0;
   b->h_states[id] = s0;
-  if ((rc = batch_h2d(b, b->d_states + id, b->h_states + id, sizeof(BState)))) return rc;
-  BCK(cudaStreamSynchronize(b->stream));
+  S.fresh = true;
+  // from s0 itself (pageable: staged before the call returns), not from the
+  // pinned h_states, which the next state read-back may overwrite first
+  if ((rc = batch_h2d(b, b->d_states + id, &s0, sizeof(BState), b->copy))) return rc;
+  BCK(cudaEventRecord(b->ev_copy, b->copy));
+  b->copy_pending = true;
   *sys_id = id;
+  return BETA_GPU_OK;
+}
+
+// A launch in two halves, so that a caller (the server) can do host work and
+// copies on the copy stream while the launch runs: batch_start issues it
+// (nothing to do: *launched = false), batch_finish waits for it and reads the
+// states back.
+int batch_start(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int iters_per_launch, bool* launched) {
+  int na = 0, rc;
+  *launched = false;
+  if ((rc = batch_prepare(b, o, iters_per_launch, &na))) return rc;
+  if (na > 0) {
+    BCK(cudaMemsetAsync(b->d_preempt, 0, sizeof(int), b->stream));
+    BCK(cudaEventRecord(b->ev0, b->stream));
+    if ((rc = batch_launch_graph(b))) return rc;
+    BCK(cudaEventRecord(b->ev1, b->stream));
+    *launched = true;
+  }
+  return BETA_GPU_OK;
+}
+
+// Ends the slice of the launch in flight early (the copy stream writes the
+// flag while the launch runs; the kernel reads it at its slice checks).
+int batch_preempt(beta_gpu_batch* b) {
+  static const int one = 1;
+  BCK(cudaMemcpyAsync(b->d_preempt, &one, sizeof(int), cudaMemcpyHostToDevice, b->copy));
+  // the next launch zeroes the flag only after this write (batch_prepare waits)
+  BCK(cudaEventRecord(b->ev_copy, b->copy));
+  b->copy_pending = true;
+  return BETA_GPU_OK;
+}
+
+int batch_finish(beta_gpu_batch* b) {
+  const int rc = batch_pull_states(b);
+  if (rc == BETA_GPU_TIMEOUT) {
+    // the launch stopped mid-iteration: unfinished systems restart from scratch next time
+    const std::string msg = b->err;
+    for (size_t i = 0; i < b->sys.size(); ++i)
+      if (b->sys[i].live && b->sys[i].st.phase != kPhaseDone) {
+        std::memset(&b->sys[i].st, 0, sizeof(BState));
+        b->sys[i].st.phase = kPhaseNew;
+        b->sys[i].st.status = kBRunning;
+      }
+    for (size_t i = 0; i < b->sys.size(); ++i) b->h_states[i] = b->sys[i].st;
+    if (!b->sys.empty() && batch_h2d(b, b->d_states, b->h_states, sizeof(BState) * b->sys.size()) == BETA_GPU_OK)
+      cudaStreamSynchronize(b->stream);
+    b->err = msg;
+  }
+  if (rc != BETA_GPU_OK) return rc;
+  BCK(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
   return BETA_GPU_OK;
 }
 
@@ -2054,6 +2115,8 @@ int beta_gpu_batch_create(beta_gpu_batch** out, int device, long long budget, in
   if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return BETA_GPU_ERR_CUDA; }
   BCK(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device));
   BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  BCK(cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking));
+  BCK(cudaEventCreateWithFlags(&b->ev_copy, cudaEventDisableTiming));
   BCK(cudaEventCreate(&b->ev0));
   BCK(cudaEventCreate(&b->ev1));
   BCK(cudaMalloc(&b->pool, (size_t)budget));
@@ -2066,6 +2129,8 @@ int beta_gpu_batch_create(beta_gpu_batch** out, int device, long long budget, in
   BCK(cudaMalloc(&b->d_params, sizeof(BParams)));
   BCK(cudaMalloc(&b->d_plan, sizeof(BPlan) * beta_gpu_batch::kMaxCtas));
   BCK(cudaMalloc(&b->d_ctl, sizeof(int) * (2 + beta_gpu_batch::kMaxCtas)));
+  BCK(cudaMalloc(&b->d_preempt, 256));
+  BCK(cudaMemset(b->d_preempt, 0, 256));
   BCK(cudaMallocHost(&b->h_plan, sizeof(BPlan) * beta_gpu_batch::kMaxCtas));
   BCK(cudaMallocHost(&b->h_ctl, sizeof(int) * 2));
   BCK(cudaMallocHost(&b->h_sys, sizeof(BSys) * max_systems));
@@ -2080,6 +2145,7 @@ int beta_gpu_batch_destroy(beta_gpu_batch* b) {
   if (!b) return BETA_GPU_OK;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->copy) cudaStreamSynchronize(b->copy);
   for (auto& g : b->graphs) cudaGraphExecDestroy(g.second);
   for (auto& t : b->gts) cudaFree(t.second);
   cudaFree(b->pool);
@@ -2089,6 +2155,7 @@ int beta_gpu_batch_destroy(beta_gpu_batch* b) {
   cudaFree(b->d_params);
   cudaFree(b->d_plan);
   cudaFree(b->d_ctl);
+  cudaFree(b->d_preempt);
   cudaFreeHost(b->h_plan);
   cudaFreeHost(b->h_ctl);
   cudaFreeHost(b->h_sys);
@@ -2097,6 +2164,8 @@ int beta_gpu_batch_destroy(beta_gpu_batch* b) {
   cudaFreeHost(b->h_params);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->ev_copy) cudaEventDestroy(b->ev_copy);
+  if (b->copy) cudaStreamDestroy(b->copy);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return BETA_GPU_OK;
@@ -2159,31 +2228,10 @@ int beta_gpu_batch_add_many(beta_gpu_batch* b, int count, const beta_gpu_system*
 int beta_gpu_batch_run(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int iters_per_launch, int* n_unfinished) {
   if (!b || !o) return BETA_GPU_ERR_ARG;
   cudaSetDevice(b->device);
-  int na = 0, rc;
-  if ((rc = batch_prepare(b, o, iters_per_launch, &na))) return rc;
-  if (na > 0) {
-    BCK(cudaEventRecord(b->ev0, b->stream));
-    if ((rc = batch_launch_graph(b))) return rc;
-    BCK(cudaEventRecord(b->ev1, b->stream));
-    if ((rc = batch_pull_states(b))) {
-      if (rc == BETA_GPU_TIMEOUT) {
-        // the launch stopped mid-iteration: unfinished systems restart from scratch next time
-        const std::string msg = b->err;
-        for (size_t i = 0; i < b->sys.size(); ++i)
-          if (b->sys[i].live && b->sys[i].st.phase != kPhaseDone) {
-            std::memset(&b->sys[i].st, 0, sizeof(BState));
-            b->sys[i].st.phase = kPhaseNew;
-            b->sys[i].st.status = kBRunning;
-          }
-        for (size_t i = 0; i < b->sys.size(); ++i) b->h_states[i] = b->sys[i].st;
-        if (!b->sys.empty() && batch_h2d(b, b->d_states, b->h_states, sizeof(BState) * b->sys.size()) == BETA_GPU_OK)
-          cudaStreamSynchronize(b->stream);
-        b->err = msg;
-      }
-      return rc;
-    }
-    BCK(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
-  }
+  bool launched = false;
+  int rc;
+  if ((rc = batch_start(b, o, iters_per_launch, &launched))) return rc;
+  if (launched && (rc = batch_finish(b))) return rc;
   int left = 0;
   for (auto& S : b->sys)
     if (S.live && S.st.phase != kPhaseDone) ++left;
@@ -2214,9 +2262,11 @@ int beta_gpu_batch_result(beta_gpu_batch* b, int id, double* u, beta_gpu_solve_s
     st->ms_solve = 1e-6 * (double)S.st.busy_ns;
   }
   if (u) {
+    // on the copy stream: a finished system is in no launch, so its
+    // solution can be read while another launch runs
     b->n_d2h += (long long)(sizeof(double) * S.ndof);
-    BCK(cudaMemcpyAsync(u, S.desc.x64, sizeof(double) * S.ndof, cudaMemcpyDeviceToHost, b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
+    BCK(cudaMemcpyAsync(u, S.desc.x64, sizeof(double) * S.ndof, cudaMemcpyDeviceToHost, b->copy));
+    BCK(cudaStreamSynchronize(b->copy));
   }
   return status;
 }
@@ -2224,6 +2274,10 @@ int beta_gpu_batch_result(beta_gpu_batch* b, int id, double* u, beta_gpu_solve_s
 int beta_gpu_batch_remove(beta_gpu_batch* b, int id) {
   if (!b || id < 0 || id >= (int)b->sys.size() || !b->sys[id].live) return BETA_GPU_ERR_ARG;
   beta_gpu_batch::Sys& S = b->sys[id];
+  b->rm_busy_ns += S.st.busy_ns;
+  b->rm_setup_ns += S.st.setup_ns;
+  b->rm_repl_ns += S.st.repl_ns;
+  b->rm_iters += S.st.iter;
   pool_free(b, S.off, S.bytes);
   S.live = false;
   S.st.phase = kPhaseDone;
@@ -2331,12 +2385,19 @@ int beta_gpu_batch_reset(beta_gpu_batch* b) {
 }
 
 int beta_gpu_batch_info(const beta_gpu_batch* b, long long* out, int n) {
-  if (!b || !out || n < 0 || n > 11) return BETA_GPU_ERR_ARG;
-  long long live = 0;
-  for (auto& S : b->sys) live += S.live ? 1 : 0;
-  const long long v[11] = {live, (long long)b->used, (long long)b->pool_bytes, b->n_launch, b->n_h2d, b->n_d2h,
+  if (!b || !out || n < 0 || n > 15) return BETA_GPU_ERR_ARG;
+  long long live = 0, busy = b->rm_busy_ns, setup = b->rm_setup_ns, repl = b->rm_repl_ns, its = b->rm_iters;
+  for (auto& S : b->sys) {
+    if (!S.live) continue;
+    ++live;
+    busy += S.st.busy_ns;
+    setup += S.st.setup_ns;
+    repl += S.st.repl_ns;
+    its += S.st.iter;
+  }
+  const long long v[15] = {live, (long long)b->used, (long long)b->pool_bytes, b->n_launch, b->n_h2d, b->n_d2h,
                            (long long)((double)b->last_ms * 1e6), b->last_ngang, b->last_gang_ctas, b->threads,
-                           b->gang_boost};
+                           b->gang_boost, busy, setup, repl, its};
   for (int i = 0; i < n; ++i) out[i] = v[i];
   return BETA_GPU_OK;
 }
@@ -2455,11 +2516,12 @@ int beta_gpu_server_cancel(beta_gpu_server* S, long long id) {
 }
 
 int beta_gpu_server_stats(beta_gpu_server* S, long long* out, int n) {
-  if (!S || !out || n < 0 || n > 13) return BETA_GPU_ERR_ARG;
+  if (!S || !out || n < 0 || n > 17) return BETA_GPU_ERR_ARG;
   std::lock_guard<std::mutex> lk(S->mu);
-  const long long v[13] = {S->n_submitted, S->n_done,      S->n_rejected,          S->n_failed,
+  const long long v[17] = {S->n_submitted, S->n_done,      S->n_rejected,          S->n_failed,
                            S->n_cancelled, (long long)S->queue.size(), S->n_running, S->n_launches,
-                           S->pool_used,   S->pool_bytes, (long long)(S->busy_ms * 1000.0), S->h2d, S->d2h};
+                           S->pool_used,   S->pool_bytes, (long long)(S->busy_ms * 1000.0), S->h2d, S->d2h,
+                           S->sys_busy_ns, S->sys_setup_ns, S->sys_repl_ns, S->sys_iters};
   for (int i = 0; i < n; ++i) out[i] = v[i];
   return BETA_GPU_OK;
 }

@@ -471,7 +471,11 @@ BETA_GPU_API int beta_gpu_batch_reset(beta_gpu_batch* batch);
  * launches, out[4] bytes host->device, out[5] bytes device->host, out[6]
  * device time of the last launch in ns (CUDA events on the batch's stream),
  * out[7] gangs and out[8] CTAs in gangs in the last launch, out[9] threads
- * per CTA, out[10] gang boost; n <= 11. */
+ * per CTA, out[10] gang boost, out[11] device time the systems' groups spent
+ * on them (ns, summed over systems, removed ones included), out[12] of which
+ * in setup (assembly, factors, first residual), out[13] of which in reliable
+ * updates (FP64 residual replacements), out[14] inner iterations in all;
+ * n <= 15. */
 BETA_GPU_API int beta_gpu_batch_info(const beta_gpu_batch* batch, long long* out, int n);
 
 /* ---- continuous-batching server ------------------------------------------ */
@@ -522,8 +526,11 @@ BETA_GPU_API int beta_gpu_server_set_slice(beta_gpu_server* server, long long sl
 BETA_GPU_API int beta_gpu_server_cancel(beta_gpu_server* server, long long request_id);
 /* out[0] submitted, [1] done, [2] rejected, [3] failed, [4] cancelled,
  * [5] queued, [6] running, [7] launches, [8] pool bytes in use, [9] pool
- * bytes, [10] microseconds the worker spent in launches, [11] bytes
- * host->device, [12] bytes device->host; n <= 13. */
+ * bytes, [10] device microseconds of the launches (CUDA events), [11] bytes
+ * host->device, [12] bytes device->host, [13] device time the retired
+ * systems' groups spent on them (ns, summed over systems), [14] of which in
+ * setup, [15] of which in reliable updates, [16] their inner iterations;
+ * n <= 17. */
 BETA_GPU_API int beta_gpu_server_stats(beta_gpu_server* server, long long* out, int n);
 
 /* ---- geometric-nonlinear Newton loop (hex8 elasticity) ------------------- */
