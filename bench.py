@@ -682,7 +682,7 @@ def run_heat(args):
     # right-hand side; the metric's bar is the solution error (<= 1e-8), which
     # is measured below against a tightly converged FP64 march.
     tol = args.heat_tol
-    o_mp = opts(mode=_abi.MODE_MPIR, tol=tol, inner_tol=args.inner_tol, profile=True)
+    o_mp = opts(mode=_abi.MODE_MPIR, tol=tol, inner_tol=args.heat_inner_tol, profile=True)
     o_64 = opts(mode=_abi.MODE_FP64, stop_rule=_abi.STOP_RB, tol=tol, profile=True)
 
     def counters():
@@ -1498,6 +1498,11 @@ def main():
     ap.add_argument("--heat-steps", type=int, default=100)
     ap.add_argument("--dt", type=float, default=1e-3)
     ap.add_argument("--heat-tol", type=float, default=1e-9)
+    # residual replacement after a 1e3 fall of the FP32 residual: the mass
+    # term keeps the step's system well conditioned, so two replacements per
+    # step reach the tolerance in the same 164 inner iterations as four at 1e-2
+    # (33.5 against 35.5 ms per step, solution error 2.3e-9)
+    ap.add_argument("--heat-inner-tol", type=float, default=1e-3)
     ap.add_argument("--heat-reassemble", action="store_true", help="assemble C/dt + K every step")
     ap.add_argument("--cpu-heat-nx", type=int, default=48)
     args = ap.parse_args()

@@ -513,7 +513,9 @@ inline bool prof_sample(int k, int ce) {
 // the predicted end, from the rate at which the loop's stop quantity has
 // been falling (log-linear between the first poll and the latest one; for
 // the first chunk, the rate of the context's previous loop), within
-// [kMinChunk, check_every].
+// [kMinChunk, check_every].  rr0 > 0: r.r when the loop starts (known to the
+// caller of a reliable-update loop from its FP64 residual), which makes the
+// first poll's prediction a measured one too.
 constexpr int kMinChunk = 4;
 
 inline double stop_quantity(const PcgState& s) {
@@ -524,16 +526,22 @@ inline double stop_target(const PcgState& s) {
 }
 
 template <int ND>
-int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
+int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out, double rr0 = -1.0) {
   const int ce = std::max(1, check_every);
   int rc;
   if (prof && prof->on && (rc = ensure_events(c, 2 * ce)) != BETA_GPU_OK) return rc;
   int n = ce;
-  // a reliable-update loop ends when r.r has fallen by delta2 from its start
-  if (c->h_st->rule == kRuleReliable && c->lnrate < 0.0 && c->h_st->delta2 > 0.0)
-    n = std::min(ce, std::max(kMinChunk, (int)(0.85 * std::log(c->h_st->delta2) / c->lnrate)));
-  double g0 = -1.0;
-  int it0 = 0;
+  const int it_start = c->h_st->iter;
+  const bool rel = c->h_st->rule == kRuleReliable;
+  // a reliable-update loop ends when r.r has fallen by delta2 from its start,
+  // or below tolabs2
+  if (rel && c->lnrate < 0.0 && c->h_st->delta2 > 0.0) {
+    double fall = c->h_st->delta2;
+    if (rr0 > 0.0 && c->h_st->tolabs2 > 0.0) fall = std::max(fall, c->h_st->tolabs2 / rr0);
+    n = std::min(ce, std::max(kMinChunk, (int)(0.85 * std::log(fall) / c->lnrate)));
+  }
+  double g0 = rel && rr0 > 0.0 ? rr0 : -1.0;
+  int it0 = it_start;
   for (;;) {
     for (int k = 0; k < n; ++k) {
       const bool sample = prof && prof->on && prof_sample(k, n);
@@ -582,7 +590,14 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out) {
     const bool measured = g0 > 0.0 && g > 0.0 && s.iter > it0;
     const double lr = measured ? std::log(g / g0) / (s.iter - it0) : c->lnrate;
     if (s.done) {
-      if (measured && lr < 0.0 && std::isfinite(lr)) c->lnrate = lr;
+      double lr_end = measured ? lr : 0.0;
+      // a loop that ended at its first poll: a reliable-update loop has cut
+      // r.r from its largest value since the last replacement to s.rr in
+      // the loop's own iterations
+      if (!measured && s.rule == kRuleReliable && s.status == kStatusReplace && s.rr > 0.0 && s.maxrr > s.rr &&
+          s.iter > it_start)
+        lr_end = std::log(s.rr / s.maxrr) / (s.iter - it_start);
+      if (lr_end < 0.0 && std::isfinite(lr_end)) c->lnrate = lr_end;
       *out = s;
       return BETA_GPU_OK;
     }
@@ -763,7 +778,7 @@ int mpir_core(beta_gpu_ctx* c, const beta_gpu_solve_opts* o, double c1, double c
     CKL("k_start_b");
     for (;;) {
       PcgState s;
-      if ((rc = pcg_loop<ND>(c, ce, prof, &s)) != BETA_GPU_OK) return rc;
+      if ((rc = pcg_loop<ND>(c, ce, prof, &s, rn * rn)) != BETA_GPU_OK) return rc;
       iters = s.iter;
       if (s.status == kStatusBreakdown) { status = BETA_GPU_BREAKDOWN; break; }
       // fold the FP32 correction into the FP64 iterate, then measure the truth

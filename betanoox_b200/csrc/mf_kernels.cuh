@@ -497,14 +497,28 @@ __global__ void __launch_bounds__(256) k_mfc_apply_hex8_heat(const int* __restri
     }
     const double* Kc = cache + (long long)(k >> 5) * kMfcHeat * 32 + (k & 31);
     const double* Mc = Kc + 36 * 32;
+    // a term whose scale is zero is not read (the step scale needs M alone,
+    // the FP64 right-hand side K alone): half the bytes
+    if (c1 != 0.0 || c2 != 0.0) {
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+      for (int a = 0; a < 8; ++a)
 #pragma unroll
-      for (int b = a; b < 8; ++b) {
-        const double kv = __ldcs(Kc + tri8(a, b) * 32), mv = cm * __ldcs(Mc + tri8(a, b) * 32);
-        f[a] += kv * vk[b] + mv * vm[b];
-        if (b != a) f[b] += kv * vk[a] + mv * vm[a];
-      }
+        for (int b = a; b < 8; ++b) {
+          const double kv = __ldcs(Kc + tri8(a, b) * 32);
+          f[a] += kv * vk[b];
+          if (b != a) f[b] += kv * vk[a];
+        }
+    }
+    if (cm != 0.0) {
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = a; b < 8; ++b) {
+          const double mv = cm * __ldcs(Mc + tri8(a, b) * 32);
+          f[a] += mv * vm[b];
+          if (b != a) f[b] += mv * vm[a];
+        }
+    }
 #pragma unroll
     for (int a = 0; a < 8; ++a) y[nd[a]] += f[a];
   }
