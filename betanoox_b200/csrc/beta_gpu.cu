@@ -287,10 +287,36 @@ int upload(beta_gpu_ctx* c, DBuf<T>& d, const T* h, size_t n) {
   return BETA_GPU_OK;
 }
 
+// Runs body(lo, hi) over [0, n) on the host's threads when n is large (the
+// input checks of a million-element mesh are otherwise tens of ms on one core).
+template <class F>
+void host_parallel(size_t n, F&& body) {
+  constexpr size_t kGrain = 1 << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>(std::min<size_t>(hw, 32), (n + kGrain - 1) / kGrain);
+  if (nt <= 1) {
+    body(size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t step = (n + nt - 1) / nt;
+  for (size_t t = 0; t < nt; ++t) {
+    const size_t lo = t * step, hi = std::min(n, lo + step);
+    if (lo < hi) th.emplace_back([&body, lo, hi] { body(lo, hi); });
+  }
+  for (auto& x : th) x.join();
+}
+
 bool all_finite(const double* a, size_t n) {
-  for (size_t i = 0; i < n; ++i)
-    if (!std::isfinite(a[i])) return false;
-  return true;
+  std::atomic<bool> ok{true};
+  host_parallel(n, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i)
+      if (!std::isfinite(a[i])) {
+        ok = false;
+        return;
+      }
+  });
+  return ok;
 }
 
 void invalidate_matrices(beta_gpu_ctx* c) {
@@ -1273,8 +1299,17 @@ int beta_gpu_mesh_upload(beta_gpu_ctx* c, int kind, int ndim, int nnode, const d
   if (order < 1 || order > 4) return fail(c, BETA_GPU_ERR_ARG, "integration order must be 1..4");
   if ((long long)nnode * ndpn > 2000000000LL) return fail(c, BETA_GPU_ERR_ARG, "too many dofs");
   if (!all_finite(xyz, (size_t)nnode * ndim)) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite coordinates");
-  for (long long k = 0; k < (long long)nelem * nnpe; ++k)
-    if (conn[k] < 0 || conn[k] >= nnode) return fail(c, BETA_GPU_ERR_ARG, "connectivity out of range");
+  {
+    std::atomic<bool> in_range{true};
+    host_parallel((size_t)nelem * nnpe, [&](size_t lo, size_t hi) {
+      for (size_t k = lo; k < hi; ++k)
+        if (conn[k] < 0 || conn[k] >= nnode) {
+          in_range = false;
+          return;
+        }
+    });
+    if (!in_range) return fail(c, BETA_GPU_ERR_ARG, "connectivity out of range");
+  }
   c->kind = kind; c->ndim = ndim; c->nnode = nnode; c->nelem = nelem; c->nnpe = nnpe; c->ndpn = ndpn;
   c->ndof = nnode * ndpn; c->order = order;
   TRACE("validated");
@@ -1332,15 +1367,30 @@ int beta_gpu_bc_upload(beta_gpu_ctx* c, const unsigned char* restrained, const d
   cudaSetDevice(c->device);
   const size_t n = c->ndof;
   std::vector<unsigned char> r(n, 0);
-  if (restrained)
-    for (size_t i = 0; i < n; ++i) r[i] = restrained[i] ? 1 : 0;
-  std::vector<double> pz(n, 0.0), lz(n, 0.0);
+  std::vector<double> pz, lz;  // zeros stand in for a missing array
+  if (!prescribed) pz.assign(n, 0.0);
+  if (!load) lz.assign(n, 0.0);
   const double* p = prescribed ? prescribed : pz.data();
   const double* l = load ? load : lz.data();
-  if (!all_finite(p, n) || !all_finite(l, n)) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite boundary data");
-  for (size_t i = 0; i < n; ++i)
-    if (r[i] && l[i] != 0.0)
-      return fail(c, BETA_GPU_ERR_LOAD_ON_RESTRAINED, "Cannot add load to a restrained degree of freedom.");
+  // one pass: 0/1 restraints, finite values, no load on a restrained dof
+  std::atomic<int> bad{0};  // 1 non-finite, 2 load on a restrained dof
+  host_parallel(n, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) {
+      const unsigned char ri = restrained && restrained[i] ? 1 : 0;
+      r[i] = ri;
+      if (!std::isfinite(p[i]) || !std::isfinite(l[i])) {
+        bad = 1;
+        return;
+      }
+      if (ri && l[i] != 0.0) {
+        int z = 0;
+        bad.compare_exchange_strong(z, 2);
+      }
+    }
+  });
+  if (bad == 1) return fail(c, BETA_GPU_ERR_NOT_FINITE, "non-finite boundary data");
+  if (bad == 2)
+    return fail(c, BETA_GPU_ERR_LOAD_ON_RESTRAINED, "Cannot add load to a restrained degree of freedom.");
   if (c->have_pattern && r != c->h_rest) {
     c->have_pattern = false;
     invalidate_matrices(c);
