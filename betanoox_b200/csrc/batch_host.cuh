@@ -58,7 +58,9 @@ struct beta_gpu_batch {
   // launch shape: threads per CTA; gang sizing: a system gets about
   // gang_boost x (its share of the batch's matrix values) of the CTAs, and a
   // gang when that is at least 2 (0: every system on one CTA)
-  int threads = 512, gang_boost = 4;
+  // (1024 threads: 32 warps per SM at 64 registers; faster than 512 at 128
+  // registers on the RVE batches and the serving mix)
+  int threads = 1024, gang_boost = 4;
   // a system whose FP32 inner solve needs more than this many iterations for
   // one residual-replacement cycle continues in FP64, matrix-free (0: never)
   int switch_iters = 500;

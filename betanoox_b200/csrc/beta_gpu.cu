@@ -2369,8 +2369,8 @@ int beta_gpu_batch_autotune(beta_gpu_batch* b, const beta_gpu_solve_opts* o, int
   if (!b || !o || budget < 0) return BETA_GPU_ERR_ARG;
   cudaSetDevice(b->device);
   // (threads per CTA, gang boost)
-  const int shapes[][2] = {{512, 0}, {512, 1}, {512, 2}, {512, 4}, {512, 8}, {512, 16},
-                           {256, 4}, {256, 16}, {1024, 4}};
+  const int shapes[][2] = {{1024, 2}, {1024, 4}, {1024, 8}, {1024, 16}, {512, 1}, {512, 2}, {512, 4},
+                           {512, 16}, {256, 4}};
   double best = 1e300;
   int bt = b->threads, bg = b->gang_boost, rc = BETA_GPU_OK;
   const long long slice = b->slice_ns;

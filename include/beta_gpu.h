@@ -418,10 +418,11 @@ BETA_GPU_API int beta_gpu_batch_run(beta_gpu_batch* batch, const beta_gpu_solve_
 BETA_GPU_API int beta_gpu_batch_result(beta_gpu_batch* batch, int sys_id, double* u,
                                        beta_gpu_solve_stats* stats);
 BETA_GPU_API int beta_gpu_batch_remove(beta_gpu_batch* batch, int sys_id);
-/* Launch shape: threads per CTA (256, 512 or 1024; one CTA per SM) and gang
- * sizing.  A system gets about gang_boost x (its share of the batch's FP32
- * matrix values) of the CTAs, as one gang, when that is at least 2; the other
- * systems are solved by single CTAs.  gang_boost 0: every system on one CTA.
+/* Launch shape: threads per CTA (256, 512 or 1024 (the default); one CTA per
+ * SM) and gang sizing.  A system gets about gang_boost x (its share of the
+ * batch's work: FP32 matrix values x expected iterations) of the CTAs, as one
+ * gang, when that is at least 2; the other systems are solved by single CTAs.
+ * gang_boost 0: every system on one CTA.
  * The result of a system does not depend on either choice. */
 BETA_GPU_API int beta_gpu_batch_tune(beta_gpu_batch* batch, int threads_per_cta, int gang_boost);
 /* Times every launch shape (threads per CTA, gang boost) on the current
