@@ -103,3 +103,26 @@ def test_cancel_and_bad_input():
             s.poll(10 ** 9)
     assert states[:3] == [_abi.REQ_DONE] * 3
     assert states[3] in (_abi.REQ_CANCELLED, _abi.REQ_DONE)
+
+
+def test_arrival_ends_the_running_slice():
+    """Continuous batching under a long time slice: a small request that
+    arrives while a big one is being solved is admitted during the running
+    launch, which then ends its slice early (after at most one iteration past
+    the 2 ms minimum), so the small request finishes long before the big one
+    instead of waiting for the launch -- here, for the big solve -- to end."""
+    big = W.cube_hex8(80, seed=3)  # 1.6 M dofs: a solve of a few hundred ms
+    small = W.plate_quad4(8)
+    with Server(hbm_budget=4 << 30, o=opts(tol=1e-10), iters_per_launch=10 ** 6, slice_us=20_000_000) as s:
+        rb = s.submit(big)
+        t_end = time.monotonic() + 60
+        while s.poll(rb)[0] != _abi.REQ_RUNNING and time.monotonic() < t_end:
+            time.sleep(0.002)
+        time.sleep(0.02)  # the big system's launch is under way
+        rs = s.submit(small)
+        st_s, _, ss, lat_s = s.wait(rs)
+        st_b, _, sb, lat_b = s.wait(rb)
+        launches = s.stats()["launches"]
+    assert st_s == st_b == _abi.REQ_DONE and ss.status == sb.status == _abi.OK
+    assert lat_s < 0.5 * lat_b, (lat_s, lat_b)
+    assert launches >= 2
