@@ -98,8 +98,12 @@ struct BParams {
   long long slice_ns;           // time slice: systems stop after the iteration in which it ends (0: none)
   // With a time slice, the slice also ends once *preempt is non-zero (the
   // server sets it when it has admitted new work) and min_slice_ns have passed.
-  const int* preempt;
+  int* preempt;
   long long min_slice_ns;
+  // A system that finishes sets *preempt itself, so the launch ends soon and
+  // its result can be collected (the server asks for this when no request
+  // waits; with a backlog the slice runs out, and launches stay long).
+  int end_on_done;
 };
 
 // The slice is over early: new work is waiting for the next launch.
@@ -961,6 +965,7 @@ __device__ void b_solve(const BSys& S, const BParams& P, const Grp& g, const dou
     if (g.gs->t_repl) st.repl_ns += globaltimer_ns() - g.gs->t_repl;
     st.busy_ns += globaltimer_ns() - g.gs->t_in;
     *S.st = st;
+    if (P.end_on_done && st.phase == kPhaseDone && P.preempt) *(volatile int*)P.preempt = 1;
   }
   gsync(g);
 }

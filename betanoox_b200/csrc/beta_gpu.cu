@@ -2483,6 +2483,7 @@ int beta_gpu_server_create(beta_gpu_server** out, int device, long long budget, 
   }
   std::unique_ptr<beta_gpu_server> S(new beta_gpu_server());
   S->batch = b;
+  b->keep_singles = true;  // small requests start next to big ones
   S->opts = *o;
   S->iters_per_launch = iters_per_launch;
   S->pool_bytes = (long long)b->pool_bytes;

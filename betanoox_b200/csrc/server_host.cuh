@@ -233,6 +233,9 @@ void server_loop(beta_gpu_server* S) {
       {
         std::lock_guard<std::mutex> lk(S->mu);
         S->launch_done = false;
+        // nothing waits: end the launch once a request finishes, so its
+        // result goes out at once (with a backlog the slice runs out)
+        b->end_on_done = S->queue.empty() ? 1 : 0;
       }
       rc = batch_start(b, &S->opts, S->iters_per_launch, &launched);
       if (launched && cudaLaunchHostFunc(b->stream, server_launch_done, S) != cudaSuccess) {
