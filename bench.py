@@ -173,6 +173,8 @@ def spmv_algorithmic_bytes(nblk, nnode, nd, ncols=None):
 def _layout_label(layout, nd):
     run = layout[0] if layout else 1
     cols = "one column per block" if run == 1 else f"one column per run of {run} node columns"
+    if layout and len(layout) > 4 and layout[4]:
+        cols += ", compact"
     return f"k_spmv_dot_b<{nd},{run}> (FP32 node-block sliced ELL, {cols}, + p.Ap)"
 
 
@@ -391,13 +393,14 @@ def run_ours(args):
     out = None
     if rank == 0:
         peak, peak_kind = _peaks()
-        alg = spmv_algorithmic_bytes(_nblk(m), m.nnode, m.ndpn, 32 * layout[2])
+        alg = spmv_algorithmic_bytes(_nblk(m), m.nnode, m.ndpn, layout[2])
         achieved = alg / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
         tr = _traffic()
         kern = _layout_label(layout, m.ndpn)
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
-                "traffic": tr.get("bytes_per_launch") if tr and tr.get("kernel") == kern.split(" ")[0] else None,
+                "traffic": (round(tr["traffic_over_algorithmic"] * alg)
+                            if tr and tr.get("kernel") == kern.split(" ")[0] else None),
                 "kernel": kern,
                 "algorithmic_bytes_per_launch": alg, "ms_per_launch": spmv_ms,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
@@ -779,7 +782,7 @@ def run_heat(args):
         peak, peak_kind = _peaks()
         spmv_ms = statistics.median([s.ms_spmv_avg for s in st_mp])
         layout = g.block_layout()
-        alg = spmv_algorithmic_bytes(_nblk(m), m.nnode, 1, 32 * layout[2])
+        alg = spmv_algorithmic_bytes(_nblk(m), m.nnode, 1, layout[2])
         achieved = alg / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": None,

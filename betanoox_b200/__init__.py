@@ -112,10 +112,10 @@ class Solver:
         self._check(self.lib.beta_gpu_set_operator_cache(self.h, 1 if on else 0), "set_operator_cache")
 
     def block_layout(self):
-        """(run length, value chunks, column chunks, bytes) of the FP32 block
-        matrix as built."""
-        out = (C.c_longlong * 4)()
-        self._check(self.lib.beta_gpu_block_layout(self.h, out, 4), "block_layout")
+        """(run length, value chunks, column indices read, bytes, compact) of
+        the FP32 block matrix as built."""
+        out = (C.c_longlong * 5)()
+        self._check(self.lib.beta_gpu_block_layout(self.h, out, 5), "block_layout")
         return tuple(int(v) for v in out)
 
     def pattern_lower(self):

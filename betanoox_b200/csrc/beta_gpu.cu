@@ -156,7 +156,7 @@ struct beta_gpu_ctx {
   bool have_pattern = false;
   bool have_scalar = false;  // scalar FP64 layout built and uploaded
   HostPattern P;
-  DBuf<int> elems, nrp, bsoff, bcol, ndiag, soff, scol;
+  DBuf<int> elems, nrp, bsoff, bcol, ndiag, soff, scol, cptr;
   DBuf<uint16_t> slot, vpos;
   DBuf<long long> ssoff, sdiag;
   // matrices
@@ -577,7 +577,7 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out, dou
         launch(c, k_spmv_dot_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, 
             A, c->p64.p, c->q64.p, c->st.p, c->partials.p);
       } else {
-        BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p};
+        BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p, c->P.compact ? c->cptr.p : nullptr};
         if (c->P.run == 3)
           launch(c, k_spmv_dot_b<ND, 3>, grid_for(c, (long long)c->P.nslice * 32, 256), 256, 0,
               A, (const float*)c->v32[2].p, c->v32[3].p, c->st.p, c->partials.p);
@@ -1261,12 +1261,12 @@ int beta_gpu_set_operator_cache(beta_gpu_ctx* c, int on) {
 }
 
 int beta_gpu_block_layout(const beta_gpu_ctx* c, long long* out, int n) {
-  if (!c || !out || n < 0 || n > 4) return BETA_GPU_ERR_ARG;
+  if (!c || !out || n < 0 || n > 5) return BETA_GPU_ERR_ARG;
   if (!c->have_pattern) return BETA_GPU_ERR_STATE;
   const HostPattern& P = c->P;
   const long long bb = (long long)P.ndpn * P.ndpn;
-  const long long v[4] = {P.run, P.nchunk, (long long)P.bcol.size() / 32,
-                          P.nchunk * 32 * bb * 4 + (long long)P.bcol.size() * 4};
+  const long long cols = P.compact ? (long long)(P.ccol.size() + P.cptr.size()) : (long long)P.bcol.size();
+  const long long v[5] = {P.run, P.nchunk, cols, P.nchunk * 32 * bb * 4 + cols * 4, P.compact ? 1 : 0};
   for (int i = 0; i < n; ++i) out[i] = v[i];
   return BETA_GPU_OK;
 }
@@ -1421,7 +1421,12 @@ int beta_gpu_build_pattern(beta_gpu_ctx* c, long long* nnz_lower) {
   if ((rc = upload(c, c->slot, P.slot.data(), P.slot.size()))) return rc;
   if ((rc = upload(c, c->nrp, P.nrp.data(), P.nrp.size()))) return rc;
   if ((rc = upload(c, c->bsoff, P.bsoff.data(), P.bsoff.size()))) return rc;
-  if ((rc = upload(c, c->bcol, P.bcol.data(), P.bcol.size()))) return rc;
+  if (P.compact) {  // the SpMV reads the compact columns; the full ones stay on the host
+    if ((rc = upload(c, c->bcol, P.ccol.data(), P.ccol.size()))) return rc;
+    if ((rc = upload(c, c->cptr, P.cptr.data(), P.cptr.size()))) return rc;
+  } else if ((rc = upload(c, c->bcol, P.bcol.data(), P.bcol.size()))) {
+    return rc;
+  }
   if ((rc = upload(c, c->ndiag, P.ndiag.data(), P.ndiag.size()))) return rc;
   if (P.run > 1 && (rc = upload(c, c->vpos, P.vpos.data(), P.vpos.size()))) return rc;
   CK(cudaStreamSynchronize(c->stream));
@@ -1702,7 +1707,7 @@ int beta_gpu_matvec(beta_gpu_ctx* c, int precision, const double* x, double* y) 
     launch(c, k_spmv_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, A, c->t64.p, c->y64.p, nullptr);
   } else {
     if (!c->have32) return fail(c, BETA_GPU_ERR_STATE, "no FP32 matrix");
-    BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p};
+    BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p, c->P.compact ? c->cptr.p : nullptr};
     const int g = grid_for(c, (long long)c->P.nslice * 32, 256), gn = grid_for(c, n, 256);
     launch(c, k_to32, gn, 256, 0, (long long)n, (const double*)c->t64.p, 1.0, c->v32[0].p);
     const float* xv = c->v32[0].p;

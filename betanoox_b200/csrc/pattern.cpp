@@ -53,6 +53,9 @@ static void reset_keep(HostPattern& P) {
   P.bcol.clear();
   P.vpos.clear();
   P.run = 1;
+  P.compact = false;
+  P.cptr.clear();
+  P.ccol.clear();
   P.slot.clear();
   P.ssoff.clear();
   P.sdiag.clear();
@@ -144,6 +147,9 @@ static void build_columns(HostPattern& P) {
     return;
   }
   P.run = R;
+  P.compact = false;
+  P.cptr.clear();
+  P.ccol.clear();
   for (int s = 0; s < P.nslice; ++s) P.bsoff[s + 1] = P.bsoff[s] + R * wr[s];
   P.nchunk = P.bsoff[P.nslice];
   P.bcol.resize((size_t)nrc * 32);
@@ -165,6 +171,49 @@ static void build_columns(HostPattern& P) {
       }
     }
   });
+  if (!P.compact_request) return;
+  // the compact form: slices whose every run sits at one offset from the row
+  std::vector<char> uni(P.nslice, 0);
+  parallel_for(P.nslice, [&](long long lo, long long hi) {
+    for (long long s = lo; s < hi; ++s) {
+      if ((s + 1) * 32 > nnode) continue;  // a partial last slice keeps its columns
+      const int* c = P.bcol.data() + (size_t)(P.bsoff[s] / R) * 32;
+      bool u = true;
+      for (int k = 0; k < wr[s] && u; ++k) {
+        const int off = c[(size_t)k * 32] - (int)(s * 32);
+        for (int l = 1; l < 32; ++l)
+          if (c[(size_t)k * 32 + l] - (int)(s * 32 + l) != off) {
+            u = false;
+            break;
+          }
+      }
+      uni[s] = u ? 1 : 0;
+    }
+  });
+  long long full = 0, small = 0;
+  for (int s = 0; s < P.nslice; ++s) (uni[s] ? small : full) += wr[s];
+  const double before = (double)nrc * 32 * 4, after = (double)(full * 32 + small + P.nslice) * 4;
+  const double values = (double)P.nchunk * 32 * 4.0 * bb;
+  if (before - after < 0.02 * (values + before) || full * 32 + small > 2000000000LL) return;
+  P.cptr.resize(P.nslice);
+  long long at = 0;
+  for (int s = 0; s < P.nslice; ++s) {
+    P.cptr[s] = uni[s] ? ~(int)at : (int)at;
+    at += uni[s] ? wr[s] : 32LL * wr[s];
+  }
+  P.ccol.resize((size_t)at);
+  parallel_for(P.nslice, [&](long long lo, long long hi) {
+    for (long long s = lo; s < hi; ++s) {
+      const int* c = P.bcol.data() + (size_t)(P.bsoff[s] / R) * 32;
+      if (P.cptr[s] < 0) {
+        int* d = P.ccol.data() + ~P.cptr[s];
+        for (int k = 0; k < wr[s]; ++k) d[k] = c[(size_t)k * 32] - (int)(s * 32);
+      } else {
+        std::copy(c, c + (size_t)wr[s] * 32, P.ccol.begin() + P.cptr[s]);
+      }
+    }
+  });
+  P.compact = true;
 }
 
 std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* conn,

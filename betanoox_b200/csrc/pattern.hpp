@@ -81,12 +81,23 @@ struct HostPattern {
   // 27; block (I, graph position q) sits at virtual position
   // vpos[nrp[I] + q] = R*k + (J - J0), and the run's other slots are zero.
   int run_request = 1;        // input: the largest run the caller accepts (1 or 3)
+  bool compact_request = true; // input: allow the compact form of column runs
   int run = 1;                // the run length built
   int nslice = 0;
   std::vector<int> bsoff;     // nslice+1, in (virtual) chunks of 32 blocks
   FillVec<int> bcol;          // nchunk/run*32, padding points at the row's own node
   FillVec<uint16_t> vpos;     // run > 1: nblk virtual positions (empty otherwise)
   long long nchunk = 0;       // virtual chunks (value storage = nchunk*32*ND*ND floats)
+  // Column runs, compact form (when it makes the matrix at least 2 % smaller):
+  // a slice whose 32 rows all have their runs at the same offsets from the
+  // row (J0 - I equal across the lanes for every run: a slice inside one
+  // x-row of a structured mesh) stores those w offsets once instead of 32 x w
+  // columns.  cptr[s] >= 0: the slice's columns at ccol[cptr[s] + k*32 + lane];
+  // cptr[s] < 0: its offsets at ccol[~cptr[s] + k], J0 = I + offset.  bcol
+  // keeps the full columns (host only).
+  bool compact = false;
+  std::vector<int> cptr;      // nslice
+  FillVec<int> ccol;
 
   // scalar sliced ELL over dofs (restrained rows: diagonal only; restrained
   // columns removed), slice s covers rows [32s, 32s+32)

@@ -353,6 +353,10 @@ struct BlockMat {
   const int* bsoff;  // nslice+1 (chunks)
   const int* bcol;
   const float* bval;
+  // compact column runs (nullptr: none): cptr[s] >= 0, the slice's columns at
+  // bcol[cptr[s] + k*32 + lane]; cptr[s] < 0, its run offsets from the row at
+  // bcol[~cptr[s] + k]
+  const int* cptr = nullptr;
 };
 
 // NC: gather x through the read-only cache (only when x is not written
@@ -367,13 +371,28 @@ template <int ND, bool PADDED, bool NC = true, int U = 2, int R = 1>
 __device__ __forceinline__ void spmv_row_b(const BlockMat& A, int s, int lane, const float* x, float* acc) {
   constexpr int BB = ND * ND;
   const int c0 = A.bsoff[s], w = (A.bsoff[s + 1] - c0) / R;
+  // run k's column: J0 = base + cp[k * stride] (a compact slice: the row plus
+  // one offset that every lane reads; otherwise the lane's own column)
   const int* cp = A.bcol + (long long)(c0 / R) * 32 + lane;
+  int stride = 32, base = 0;
+  if constexpr (R > 1) {
+    if (A.cptr) {
+      const int p = A.cptr[s];
+      if (p < 0) {
+        cp = A.bcol + ~p;
+        stride = 1;
+        base = s * 32 + lane;
+      } else {
+        cp = A.bcol + p + lane;
+      }
+    }
+  }
   const float* vp = A.bval + (long long)c0 * 32 * BB + lane;
 #pragma unroll
   for (int i = 0; i < ND; ++i) acc[i] = 0.f;
 #pragma unroll U
   for (int k = 0; k < w; ++k) {
-    const int J0 = __ldcs(cp + k * 32);
+    const int J0 = R > 1 ? base + __ldg(cp + k * stride) : __ldcs(cp + k * 32);
 #pragma unroll
     for (int j = 0; j < R; ++j) {
       const int J = J0 + j;

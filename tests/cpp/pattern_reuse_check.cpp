@@ -32,7 +32,8 @@ static bool equal(const HostPattern& P, const HostPattern& Q) {
          same(P.slot, Q.slot) && P.nslice == Q.nslice && same(P.bsoff, Q.bsoff) && same(P.bcol, Q.bcol) &&
          P.nchunk == Q.nchunk && P.nsslice == Q.nsslice && same(P.ssoff, Q.ssoff) && same(P.scol, Q.scol) &&
          same(P.soff, Q.soff) && same(P.srowlen, Q.srowlen) && same(P.sdiag, Q.sdiag) &&
-         P.nnz_full == Q.nnz_full && P.nnz_lower == Q.nnz_lower && P.run == Q.run && same(P.vpos, Q.vpos);
+         P.nnz_full == Q.nnz_full && P.nnz_lower == Q.nnz_lower && P.run == Q.run && same(P.vpos, Q.vpos) &&
+         P.compact == Q.compact && same(P.cptr, Q.cptr) && same(P.ccol, Q.ccol);
 }
 
 // A build with runs allowed (R) against the one-column-per-block build E of
@@ -63,8 +64,21 @@ static bool runs_valid(const HostPattern& P, const HostPattern& E, const char* n
       }
       ok = ok && P.ndiag[I] == P.vpos[P.nrp[I] + E.ndiag[I]];
     }
+    // the compact form gives every lane of every slice the same run columns
+    if (ok && P.compact) {
+      ok = (int)P.cptr.size() == P.nslice;
+      for (int s = 0; ok && s < P.nslice; ++s) {
+        const int w = (P.bsoff[s + 1] - P.bsoff[s]) / R;
+        for (int k = 0; ok && k < w; ++k)
+          for (int lane = 0; ok && lane < 32; ++lane) {
+            const int c = P.cptr[s];
+            const int j0 = c < 0 ? 32 * s + lane + P.ccol[(size_t)~c + k] : P.ccol[(size_t)c + (size_t)k * 32 + lane];
+            ok = j0 == P.bcol[((size_t)P.bsoff[s] / R + k) * 32 + lane];
+          }
+      }
+    }
   }
-  std::printf("runs %-55s run=%d %s\n", name, P.run, ok ? "valid" : "INVALID");
+  std::printf("runs %-55s run=%d compact=%d %s\n", name, P.run, P.compact ? 1 : 0, ok ? "valid" : "INVALID");
   return ok;
 }
 
@@ -74,7 +88,9 @@ static unsigned long long hash_of(const HostPattern& P) {
   auto all = [&](const auto& a) { mix((long long)a.size()); for (size_t i = 0; i < a.size(); ++i) mix(a[i]); };
   all(P.nrp); all(P.ncol); all(P.ndiag); all(P.color_ptr); all(P.elem_by_color); all(P.slot); all(P.bsoff);
   all(P.bcol); all(P.ssoff); all(P.scol); all(P.soff); all(P.srowlen); all(P.sdiag); all(P.unused); all(P.vpos);
+  all(P.cptr); all(P.ccol);
   mix(P.run);
+  mix(P.compact);
   mix(P.nblk); mix(P.ncolor); mix(P.nchunk); mix(P.nnz_full); mix(P.nnz_lower);
   return h;
 }
@@ -137,7 +153,7 @@ static Mesh quad4_with_extras(int nx, int ny) {
 int main() {
   std::vector<Mesh> meshes = {hex8(6, 3, false, 0),  hex8(24, 3, false, 0), hex8(24, 1, true, 3),
                               quad4_with_extras(150, 90), hex8(40, 3, true, 5), hex8(5, 1, false, 0),
-                              hex8(24, 3, false, 0)};
+                              hex8(24, 3, false, 0),  hex8(70, 1, false, 0)};
   HostPattern reused, reused_runs;
   reused.keep_scratch = true;
   reused_runs.keep_scratch = true;

@@ -22,6 +22,9 @@ MODELS = {
     "quad4": lambda: W.plate_quad4(40),               # 2 dofs per node
     "heat": lambda: W.heat_slab(12, 10, 6, order=3),  # 1 dof per node
     "rve": lambda: W.rve_hex8(9, 4),
+    # x-rows of 97 nodes: most 32-node slices lie inside one row, so the runs
+    # take their compact form (one offset per run for such a slice)
+    "heat_long": lambda: W.heat_slab(96, 10, 6, order=3),
 }
 
 
@@ -42,7 +45,9 @@ def test_runs_equal_one_column_per_block(name):
     g1, g3 = _pair(m)
     l1, l3 = g1.block_layout(), g3.block_layout()
     assert l1[0] == 1 and l3[0] == 3
-    assert l3[3] <= 0.95 * l1[3] and l3[1] == 3 * l3[2]
+    assert l3[3] <= 0.95 * l1[3]
+    if name == "heat_long":
+        assert l3[4] == 1 and l3[3] <= 0.9 * l1[3]
     g1.assemble(_abi.FP32)
     g3.assemble(_abi.FP32)
     v1, _ = g1.lower_values(_abi.FP32)

@@ -17,8 +17,10 @@ def _run(tmp_path, name, extra):
                     os.path.join(ROOT, "betanoox_b200", "csrc", "pattern.cpp"), "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count(" equal") == 7
-    assert r.stdout.count(" valid") == 7 and "INVALID" not in r.stdout
+    assert r.stdout.count(" equal") == 8
+    assert r.stdout.count(" valid") == 8 and "INVALID" not in r.stdout
+    # the 70^3 grid with one dof per node takes the compact form of its runs
+    assert any("hex8 n=70 nd=1" in line and "compact=1" in line for line in r.stdout.splitlines())
     # lexicographic hex8 grids and the quad4 plate take runs of 3; the
     # shuffled numberings keep one column per block
     runs = dict(line[5:].rsplit(" run=", 1) for line in r.stdout.splitlines() if line.startswith("runs "))
@@ -38,4 +40,4 @@ def test_reused_pattern_equals_fresh_build(tmp_path):
     bounded = _run(tmp_path, "pattern_reuse_check_bounded", ["-DBETA_PATTERN_MARK_BUDGET=0"])
     sorted_rows = _run(tmp_path, "pattern_reuse_check_sorted", ["-DBETA_PATTERN_MARK_BUDGET=0",
                                                                   "-DBETA_PATTERN_SPAN_CAP=0"])
-    assert len(default) == 14 and default == bounded == sorted_rows
+    assert len(default) == 16 and default == bounded == sorted_rows
