@@ -511,6 +511,150 @@ __global__ void __launch_bounds__(256) k_update_b(int nnode, float* __restrict__
   if (reduce_last<3>(acc, partials, &st->ticket, out) && threadIdx.x == 0) finish_update(st, out[0], out[1], out[2]);
 }
 
+// ---- the same two vector passes, four consecutive nodes per thread --------
+// Four nodes' ND components are 4*ND floats, the padded direction 4*PVec::W
+// and the packed block-Jacobi factors 4*ND(ND+1)/2: whole float4s, so a
+// thread moves them with 16-byte loads and stores instead of ND 4-byte ones
+// per node (the one-node update reached 0.73 of HBM on the slab).  Per node
+// the arithmetic is the same; the FP64 partial sums add the nodes in another
+// grouping.  The last nnode % 4 nodes go one per thread.  Used for one dof per
+// node (with three, 80 registers a thread cost more than they gain).
+template <int NF>
+__device__ __forceinline__ void ld4(const float* v, long long i4, float (&o)[4 * NF]) {
+  const float4* q = reinterpret_cast<const float4*>(v) + i4 * NF;
+#pragma unroll
+  for (int k = 0; k < NF; ++k) {
+    const float4 t = q[k];
+    o[4 * k] = t.x; o[4 * k + 1] = t.y; o[4 * k + 2] = t.z; o[4 * k + 3] = t.w;
+  }
+}
+template <int NF>
+__device__ __forceinline__ void st4(float* v, long long i4, const float (&a)[4 * NF]) {
+  float4* q = reinterpret_cast<float4*>(v) + i4 * NF;
+#pragma unroll
+  for (int k = 0; k < NF; ++k) q[k] = make_float4(a[4 * k], a[4 * k + 1], a[4 * k + 2], a[4 * k + 3]);
+}
+
+template <int ND>
+__device__ __forceinline__ void prec_packed(const float* a, const float* r, float* z) {
+  if constexpr (ND == 1) {
+    z[0] = a[0] * r[0];
+  } else if constexpr (ND == 2) {
+    z[0] = fmaf(a[0], r[0], a[1] * r[1]);
+    z[1] = fmaf(a[1], r[0], a[2] * r[1]);
+  } else {
+    z[0] = fmaf(a[0], r[0], fmaf(a[1], r[1], a[2] * r[2]));
+    z[1] = fmaf(a[1], r[0], fmaf(a[3], r[1], a[4] * r[2]));
+    z[2] = fmaf(a[2], r[0], fmaf(a[4], r[1], a[5] * r[2]));
+  }
+}
+
+// x += alpha p; r -= alpha q; z = M r; (r.z, r.r, x.x) in FP64
+template <int ND>
+__global__ void __launch_bounds__(256) k_update_b4(int nnode, float* __restrict__ x, float* __restrict__ r,
+                                                   const float* __restrict__ p, const float* __restrict__ q,
+                                                   const float* __restrict__ minv, PcgState* st,
+                                                   double* partials) {
+  if (st->done) return;
+  constexpr int S = ND * (ND + 1) / 2, W = PVec<ND>::W;
+  const float a = (float)st->alpha;
+  double acc[3] = {0.0, 0.0, 0.0};
+  const long long n4 = nnode / 4;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nt = (long long)gridDim.x * blockDim.x;
+  for (long long i4 = tid; i4 < n4; i4 += nt) {
+    float xv[4 * ND], rv[4 * ND], qv[4 * ND], pv[4 * W], mv[4 * S];
+    ld4<ND>(x, i4, xv);
+    ld4<ND>(r, i4, rv);
+    ld4<W>(p, i4, pv);
+    ld4<ND>(q, i4, qv);
+    ld4<S>(minv, i4, mv);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        xv[ND * j + i] = fmaf(a, pv[W * j + i], xv[ND * j + i]);
+        rv[ND * j + i] = fmaf(-a, qv[ND * j + i], rv[ND * j + i]);
+      }
+      float z[ND];
+      prec_packed<ND>(mv + S * j, rv + ND * j, z);
+      float rz = 0.f, r2 = 0.f, x2 = 0.f;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        rz = fmaf(rv[ND * j + i], z[i], rz);
+        r2 = fmaf(rv[ND * j + i], rv[ND * j + i], r2);
+        x2 = fmaf(xv[ND * j + i], xv[ND * j + i], x2);
+      }
+      acc[0] += rz;
+      acc[1] += r2;
+      acc[2] += x2;
+    }
+    st4<ND>(x, i4, xv);
+    st4<ND>(r, i4, rv);
+  }
+  for (long long I = 4 * n4 + tid; I < nnode; I += nt) {  // the last nnode % 4 nodes
+    float xv[ND], rv[ND], pv[ND], qv[ND], z[ND];
+    NodeIO<ND>::ld(x, I, xv);
+    NodeIO<ND>::ld(r, I, rv);
+    PVec<ND>::ld(p, I, pv);
+    NodeIO<ND>::ld(q, I, qv);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      xv[i] = fmaf(a, pv[i], xv[i]);
+      rv[i] = fmaf(-a, qv[i], rv[i]);
+    }
+    NodeIO<ND>::st(x, I, xv);
+    NodeIO<ND>::st(r, I, rv);
+    NodeIO<ND>::prec(minv, I, rv, z);
+    float rz = 0.f, r2 = 0.f, x2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      rz = fmaf(rv[i], z[i], rz);
+      r2 = fmaf(rv[i], rv[i], r2);
+      x2 = fmaf(xv[i], xv[i], x2);
+    }
+    acc[0] += rz;
+    acc[1] += r2;
+    acc[2] += x2;
+  }
+  double out[3];
+  if (reduce_last<3>(acc, partials, &st->ticket, out) && threadIdx.x == 0) finish_update(st, out[0], out[1], out[2]);
+}
+
+// p = M r + beta p
+template <int ND>
+__global__ void __launch_bounds__(256) k_pupd_b4(int nnode, float* __restrict__ p, const float* __restrict__ r,
+                                                 const float* __restrict__ minv, const PcgState* st) {
+  if (st->done) return;
+  constexpr int S = ND * (ND + 1) / 2, W = PVec<ND>::W;
+  const float bt = (float)st->beta;
+  const long long n4 = nnode / 4;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nt = (long long)gridDim.x * blockDim.x;
+  for (long long i4 = tid; i4 < n4; i4 += nt) {
+    float rv[4 * ND], pv[4 * W], mv[4 * S];
+    ld4<ND>(r, i4, rv);
+    ld4<W>(p, i4, pv);
+    ld4<S>(minv, i4, mv);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float z[ND];
+      prec_packed<ND>(mv + S * j, rv + ND * j, z);
+#pragma unroll
+      for (int i = 0; i < ND; ++i) pv[W * j + i] = fmaf(bt, pv[W * j + i], z[i]);
+      if constexpr (W > ND) pv[W * j + ND] = 0.f;  // the padding lane of a padded node
+    }
+    st4<W>(p, i4, pv);
+  }
+  for (long long I = 4 * n4 + tid; I < nnode; I += nt) {
+    float rv[ND], pv[ND], z[ND];
+    NodeIO<ND>::ld(r, I, rv);
+    PVec<ND>::ld(p, I, pv);
+    NodeIO<ND>::prec(minv, I, rv, z);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) pv[i] = fmaf(bt, pv[i], z[i]);
+    PVec<ND>::st(p, I, pv);
+  }
+}
+
 // p = M r + beta p
 template <int ND>
 __global__ void __launch_bounds__(256) k_pupd_b(int nnode, float* __restrict__ p, const float* __restrict__ r,
