@@ -526,7 +526,14 @@ BETA_GPU_API int beta_gpu_server_poll(beta_gpu_server* server, long long request
                                       int* ndof, double* u, beta_gpu_solve_stats* stats, double* latency_ms,
                                       int release);
 /* Time slice of each launch, as beta_gpu_batch_set_slice (0, the default:
- * iters_per_launch alone bounds a launch); takes effect at the next launch. */
+ * iters_per_launch alone bounds a launch); takes effect at the next launch.
+ * With a slice, a running launch ends it early (after at least 2 ms) when
+ * requests that arrived meanwhile have all been admitted, or -- for a launch
+ * issued while no request waited -- when one of its requests finishes, so new
+ * work and finished results wait about one iteration, not the rest of the
+ * slice; with a backlog the slice runs out.  Gang plans keep a few CTAs (the
+ * small systems' share of the work, 1 to 1/8 of the CTAs) for systems solved
+ * by one CTA, so a small request next to big ones starts at once. */
 BETA_GPU_API int beta_gpu_server_set_slice(beta_gpu_server* server, long long slice_us);
 /* Queued requests end CANCELLED before admission, running ones after the current launch. */
 BETA_GPU_API int beta_gpu_server_cancel(beta_gpu_server* server, long long request_id);
