@@ -591,24 +591,14 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out, dou
                                                                      c->q64.p, c->d64.p, c->st.p, c->partials.p);
         launch(c, k_pupd_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->p64.p, c->r64.p, c->d64.p, c->st.p);
       } else {
-        if constexpr (ND == 1) {
-          // one dof per node: four nodes per thread, 16-byte accesses (heat
-          // slab step 30.4 -> 29.6 ms); with three the 80 registers of the
-          // four-node pass cost more occupancy than the wide accesses gain
-          // (cube step 411 -> 421 ms), so the one-node passes stay
-          const long long quads = c->nnode / 4 + 1;
-          launch(c, k_update_b4<ND>, grid_for(c, quads, 256), 256, 0, c->nnode, c->v32[0].p, c->v32[1].p,
-                 (const float*)c->v32[2].p, (const float*)c->v32[3].p, (const float*)c->minv.p, c->st.p,
-                 c->partials.p);
-          launch(c, k_pupd_b4<ND>, grid_for(c, quads, 256), 256, 0, c->nnode, c->v32[2].p,
-                 (const float*)c->v32[1].p, (const float*)c->minv.p, (const PcgState*)c->st.p);
-        } else {
-          launch(c, k_update_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->v32[0].p, c->v32[1].p,
-                 (const float*)c->v32[2].p, (const float*)c->v32[3].p, (const float*)c->minv.p, c->st.p,
-                 c->partials.p);
-          launch(c, k_pupd_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->v32[2].p,
-                 (const float*)c->v32[1].p, (const float*)c->minv.p, (const PcgState*)c->st.p);
-        }
+        // several nodes per thread with wide accesses where that pays (one
+        // dof per node: four)
+        const long long blocks = c->nnode / PassNodes<ND>::N + 1;
+        launch(c, k_update_bn<ND>, grid_for(c, blocks, 256), 256, 0, c->nnode, c->v32[0].p, c->v32[1].p,
+               (const float*)c->v32[2].p, (const float*)c->v32[3].p, (const float*)c->minv.p, c->st.p,
+               c->partials.p);
+        launch(c, k_pupd_bn<ND>, grid_for(c, blocks, 256), 256, 0, c->nnode, c->v32[2].p,
+               (const float*)c->v32[1].p, (const float*)c->minv.p, (const PcgState*)c->st.p);
       }
     }
     CKL("pcg launch");

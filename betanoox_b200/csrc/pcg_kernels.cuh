@@ -474,65 +474,53 @@ __global__ void __launch_bounds__(256, SpmvShape<ND, R>::MINB) k_spmv_dot_b(Bloc
   }
 }
 
-// x += alpha p; r -= alpha q; z = M r; (r.z, r.r, x.x) in FP64
-template <int ND>
-__global__ void __launch_bounds__(256) k_update_b(int nnode, float* __restrict__ x, float* __restrict__ r,
-                                                  const float* __restrict__ p, const float* __restrict__ q,
-                                                  const float* __restrict__ minv, PcgState* st, double* partials) {
-  if (st->done) return;
-  const float a = (float)st->alpha;
-  double acc[3] = {0.0, 0.0, 0.0};
-  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
-    float xv[ND], rv[ND], pv[ND], qv[ND], z[ND];
-    NodeIO<ND>::ld(x, I, xv);
-    NodeIO<ND>::ld(r, I, rv);
-    PVec<ND>::ld(p, I, pv);
-    NodeIO<ND>::ld(q, I, qv);
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      xv[i] = fmaf(a, pv[i], xv[i]);
-      rv[i] = fmaf(-a, qv[i], rv[i]);
-    }
-    NodeIO<ND>::st(x, I, xv);
-    NodeIO<ND>::st(r, I, rv);
-    NodeIO<ND>::prec(minv, I, rv, z);
-    float rz = 0.f, r2 = 0.f, x2 = 0.f;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      rz = fmaf(rv[i], z[i], rz);
-      r2 = fmaf(rv[i], rv[i], r2);
-      x2 = fmaf(xv[i], xv[i], x2);
-    }
-    acc[0] += rz;
-    acc[1] += r2;
-    acc[2] += x2;
-  }
-  double out[3];
-  if (reduce_last<3>(acc, partials, &st->ticket, out) && threadIdx.x == 0) finish_update(st, out[0], out[1], out[2]);
-}
 
-// ---- the same two vector passes, four consecutive nodes per thread --------
-// Four nodes' ND components are 4*ND floats, the padded direction 4*PVec::W
-// and the packed block-Jacobi factors 4*ND(ND+1)/2: whole float4s, so a
-// thread moves them with 16-byte loads and stores instead of ND 4-byte ones
-// per node (the one-node update reached 0.73 of HBM on the slab).  Per node
-// the arithmetic is the same; the FP64 partial sums add the nodes in another
-// grouping.  The last nnode % 4 nodes go one per thread.  Used for one dof per
-// node (with three, 80 registers a thread cost more than they gain).
-template <int NF>
-__device__ __forceinline__ void ld4(const float* v, long long i4, float (&o)[4 * NF]) {
-  const float4* q = reinterpret_cast<const float4*>(v) + i4 * NF;
+// ---- the same two vector passes, several consecutive nodes per thread -----
+// NPT consecutive nodes' ND components are NPT*ND floats, the padded
+// direction NPT*PVec::W and the packed block-Jacobi factors NPT*ND(ND+1)/2:
+// a thread moves them with the widest aligned accesses those counts allow
+// (16 or 8 bytes) instead of ND 4-byte ones per node.  Per node the arithmetic
+// is the same; the FP64 partial sums add the nodes in another grouping.  The
+// last nnode % NPT nodes go one per thread.  One dof per node: four nodes
+// (16-byte accesses; the one-node update reached 0.73 of HBM on the slab:
+// transient step 30.4 -> 29.7 ms).  Three: one node (two nodes with 8- and
+// 16-byte accesses measured the same cube step, four nodes at 80 registers
+// slower).
+template <int N>
+__device__ __forceinline__ void ldn(const float* v, long long blk, float (&o)[N]) {
+  if constexpr (N % 4 == 0) {
+    const float4* q = reinterpret_cast<const float4*>(v) + blk * (N / 4);
 #pragma unroll
-  for (int k = 0; k < NF; ++k) {
-    const float4 t = q[k];
-    o[4 * k] = t.x; o[4 * k + 1] = t.y; o[4 * k + 2] = t.z; o[4 * k + 3] = t.w;
+    for (int k = 0; k < N / 4; ++k) {
+      const float4 t = q[k];
+      o[4 * k] = t.x; o[4 * k + 1] = t.y; o[4 * k + 2] = t.z; o[4 * k + 3] = t.w;
+    }
+  } else if constexpr (N % 2 == 0) {
+    const float2* q = reinterpret_cast<const float2*>(v) + blk * (N / 2);
+#pragma unroll
+    for (int k = 0; k < N / 2; ++k) {
+      const float2 t = q[k];
+      o[2 * k] = t.x; o[2 * k + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) o[k] = v[blk * N + k];
   }
 }
-template <int NF>
-__device__ __forceinline__ void st4(float* v, long long i4, const float (&a)[4 * NF]) {
-  float4* q = reinterpret_cast<float4*>(v) + i4 * NF;
+template <int N>
+__device__ __forceinline__ void stn(float* v, long long blk, const float (&a)[N]) {
+  if constexpr (N % 4 == 0) {
+    float4* q = reinterpret_cast<float4*>(v) + blk * (N / 4);
 #pragma unroll
-  for (int k = 0; k < NF; ++k) q[k] = make_float4(a[4 * k], a[4 * k + 1], a[4 * k + 2], a[4 * k + 3]);
+    for (int k = 0; k < N / 4; ++k) q[k] = make_float4(a[4 * k], a[4 * k + 1], a[4 * k + 2], a[4 * k + 3]);
+  } else if constexpr (N % 2 == 0) {
+    float2* q = reinterpret_cast<float2*>(v) + blk * (N / 2);
+#pragma unroll
+    for (int k = 0; k < N / 2; ++k) q[k] = make_float2(a[2 * k], a[2 * k + 1]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[blk * N + k] = a[k];
+  }
 }
 
 template <int ND>
@@ -549,27 +537,32 @@ __device__ __forceinline__ void prec_packed(const float* a, const float* r, floa
   }
 }
 
+template <int ND>
+struct PassNodes {
+  static constexpr int N = ND == 1 ? 4 : 1;  // nodes per thread
+};
+
 // x += alpha p; r -= alpha q; z = M r; (r.z, r.r, x.x) in FP64
 template <int ND>
-__global__ void __launch_bounds__(256) k_update_b4(int nnode, float* __restrict__ x, float* __restrict__ r,
+__global__ void __launch_bounds__(256) k_update_bn(int nnode, float* __restrict__ x, float* __restrict__ r,
                                                    const float* __restrict__ p, const float* __restrict__ q,
                                                    const float* __restrict__ minv, PcgState* st,
                                                    double* partials) {
   if (st->done) return;
-  constexpr int S = ND * (ND + 1) / 2, W = PVec<ND>::W;
+  constexpr int S = ND * (ND + 1) / 2, W = PVec<ND>::W, NP = PassNodes<ND>::N;
   const float a = (float)st->alpha;
   double acc[3] = {0.0, 0.0, 0.0};
-  const long long n4 = nnode / 4;
+  const long long nb = nnode / NP;
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nt = (long long)gridDim.x * blockDim.x;
-  for (long long i4 = tid; i4 < n4; i4 += nt) {
-    float xv[4 * ND], rv[4 * ND], qv[4 * ND], pv[4 * W], mv[4 * S];
-    ld4<ND>(x, i4, xv);
-    ld4<ND>(r, i4, rv);
-    ld4<W>(p, i4, pv);
-    ld4<ND>(q, i4, qv);
-    ld4<S>(minv, i4, mv);
+  for (long long ib = tid; ib < nb; ib += nt) {
+    float xv[NP * ND], rv[NP * ND], qv[NP * ND], pv[NP * W], mv[NP * S];
+    ldn<NP * ND>(x, ib, xv);
+    ldn<NP * ND>(r, ib, rv);
+    ldn<NP * W>(p, ib, pv);
+    ldn<NP * ND>(q, ib, qv);
+    ldn<NP * S>(minv, ib, mv);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < NP; ++j) {
 #pragma unroll
       for (int i = 0; i < ND; ++i) {
         xv[ND * j + i] = fmaf(a, pv[W * j + i], xv[ND * j + i]);
@@ -588,10 +581,10 @@ __global__ void __launch_bounds__(256) k_update_b4(int nnode, float* __restrict_
       acc[1] += r2;
       acc[2] += x2;
     }
-    st4<ND>(x, i4, xv);
-    st4<ND>(r, i4, rv);
+    stn<NP * ND>(x, ib, xv);
+    stn<NP * ND>(r, ib, rv);
   }
-  for (long long I = 4 * n4 + tid; I < nnode; I += nt) {  // the last nnode % 4 nodes
+  for (long long I = NP * nb + tid; I < nnode; I += nt) {  // the last nnode % NP nodes
     float xv[ND], rv[ND], pv[ND], qv[ND], z[ND];
     NodeIO<ND>::ld(x, I, xv);
     NodeIO<ND>::ld(r, I, rv);
@@ -622,29 +615,29 @@ __global__ void __launch_bounds__(256) k_update_b4(int nnode, float* __restrict_
 
 // p = M r + beta p
 template <int ND>
-__global__ void __launch_bounds__(256) k_pupd_b4(int nnode, float* __restrict__ p, const float* __restrict__ r,
+__global__ void __launch_bounds__(256) k_pupd_bn(int nnode, float* __restrict__ p, const float* __restrict__ r,
                                                  const float* __restrict__ minv, const PcgState* st) {
   if (st->done) return;
-  constexpr int S = ND * (ND + 1) / 2, W = PVec<ND>::W;
+  constexpr int S = ND * (ND + 1) / 2, W = PVec<ND>::W, NP = PassNodes<ND>::N;
   const float bt = (float)st->beta;
-  const long long n4 = nnode / 4;
+  const long long nb = nnode / NP;
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nt = (long long)gridDim.x * blockDim.x;
-  for (long long i4 = tid; i4 < n4; i4 += nt) {
-    float rv[4 * ND], pv[4 * W], mv[4 * S];
-    ld4<ND>(r, i4, rv);
-    ld4<W>(p, i4, pv);
-    ld4<S>(minv, i4, mv);
+  for (long long ib = tid; ib < nb; ib += nt) {
+    float rv[NP * ND], pv[NP * W], mv[NP * S];
+    ldn<NP * ND>(r, ib, rv);
+    ldn<NP * W>(p, ib, pv);
+    ldn<NP * S>(minv, ib, mv);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < NP; ++j) {
       float z[ND];
       prec_packed<ND>(mv + S * j, rv + ND * j, z);
 #pragma unroll
       for (int i = 0; i < ND; ++i) pv[W * j + i] = fmaf(bt, pv[W * j + i], z[i]);
       if constexpr (W > ND) pv[W * j + ND] = 0.f;  // the padding lane of a padded node
     }
-    st4<W>(p, i4, pv);
+    stn<NP * W>(p, ib, pv);
   }
-  for (long long I = 4 * n4 + tid; I < nnode; I += nt) {
+  for (long long I = NP * nb + tid; I < nnode; I += nt) {
     float rv[ND], pv[ND], z[ND];
     NodeIO<ND>::ld(r, I, rv);
     PVec<ND>::ld(p, I, pv);
