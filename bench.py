@@ -125,8 +125,8 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic():
-    p = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+def _traffic(name="spmv_traffic.json"):
+    p = os.path.join(ROOT, "profiles", name)
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f)
@@ -784,9 +784,13 @@ def run_heat(args):
         layout = g.block_layout()
         alg = spmv_algorithmic_bytes(_nblk(m), m.nnode, 1, layout[2])
         achieved = alg / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
+        tr = _traffic("spmv_traffic_heat.json")
+        kern = _layout_label(layout, 1)
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
-                "kernel": _layout_label(layout, 1) + ", one dof per node",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": (round(tr["traffic_over_algorithmic"] * alg)
+                            if tr and tr.get("kernel") == kern.split(" ")[0] else None),
+                "kernel": kern + ", one dof per node",
                 "algorithmic_bytes_per_launch": alg, "ms_per_launch": spmv_ms,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s"}
