@@ -1141,6 +1141,7 @@ def run_batch(args, nested=False):
                 "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_launch,
                 "note": "inner-iteration bytes only (assembly and FP64 residual replacements excluded); "
                         "small systems re-read their matrix from L2",
+                "ncu_dram": _traffic("batch_dram.json"),
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s"}
         sizes = sorted(m.meta["n"] for m in models)
