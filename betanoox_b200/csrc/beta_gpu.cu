@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstddef>
@@ -171,6 +172,8 @@ struct beta_gpu_ctx {
   DBuf<unsigned> flags, ticket;
   PcgState* h_st = nullptr;   // pinned
   double* h_sums = nullptr;   // pinned
+  char* h_stage = nullptr;    // pinned staging of large pageable uploads (two halves)
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   DBuf<double> b64, x64, r64, p64, q64, d64, y64, t64;
   DBuf<float> v32[5];         // node-layout float vectors: x(d), r, p, q, spare
   DBuf<float> minv;
@@ -207,9 +210,13 @@ bool trace_on() {
   }
   return on == 1;
 }
-#define TRACE(msg)                                                         \
-  do {                                                                     \
-    if (trace_on()) std::fprintf(stderr, "[beta_gpu] %s:%d %s\n", __func__, __LINE__, msg); \
+// milliseconds on the host's steady clock, for the traced steps
+double trace_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+#define TRACE(msg)                                                                                      \
+  do {                                                                                                  \
+    if (trace_on()) std::fprintf(stderr, "[beta_gpu] %.3f %s:%d %s\n", trace_ms(), __func__, __LINE__, msg); \
   } while (0)
 
 int fail(beta_gpu_ctx* c, int code, const std::string& msg) {
@@ -260,8 +267,69 @@ void launch(beta_gpu_ctx* c, void (*k)(KArgs...), int grid, int block, size_t sm
   ++c->n_launch;
 }
 
+// Runs body(lo, hi) over [0, n) on the host's threads when n is large (the
+// input checks of a million-element mesh are otherwise tens of ms on one core).
+template <class F>
+void host_parallel(size_t n, F&& body) {
+  constexpr size_t kGrain = 1 << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>(std::min<size_t>(hw, 32), (n + kGrain - 1) / kGrain);
+  if (nt <= 1) {
+    body(size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t step = (n + nt - 1) / nt;
+  for (size_t t = 0; t < nt; ++t) {
+    const size_t lo = t * step, hi = std::min(n, lo + step);
+    if (lo < hi) th.emplace_back([&body, lo, hi] { body(lo, hi); });
+  }
+  for (auto& x : th) x.join();
+}
+
+// Uploads of at least kStageMin bytes from pageable host memory go through
+// the context's pinned staging buffer: all host threads copy one half while
+// the DMA of the other half runs, instead of the driver's single-threaded
+// staging of a pageable copy.  Like a pageable copy, the source may be
+// reused as soon as the call returns.
+constexpr size_t kStageHalf = size_t(32) << 20;
+constexpr size_t kStageMin = size_t(4) << 20;
+
+bool pageable(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
+cudaError_t h2d_staged(beta_gpu_ctx* c, char* dst, const char* src, size_t bytes) {
+  cudaError_t e;
+  if (!c->h_stage) {
+    if (cudaHostAlloc((void**)&c->h_stage, 2 * kStageHalf, cudaHostAllocDefault) != cudaSuccess) {
+      c->h_stage = nullptr;
+      cudaGetLastError();
+      return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+    }
+    for (auto& ev : c->stage_ev)
+      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+  }
+  for (size_t off = 0, k = 0; off < bytes; off += kStageHalf, ++k) {
+    const size_t n = std::min(kStageHalf, bytes - off);
+    const int h = (int)(k & 1);
+    char* st = c->h_stage + h * kStageHalf;
+    if ((e = cudaEventSynchronize(c->stage_ev[h])) != cudaSuccess) return e;  // its last copy has finished
+    host_parallel(n, [&](size_t lo, size_t hi) { std::memcpy(st + lo, src + off + lo, hi - lo); });
+    if ((e = cudaMemcpyAsync(dst + off, st, n, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(c->stage_ev[h], c->stream)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t h2d(beta_gpu_ctx* c, void* dst, const void* src, size_t bytes) {
   c->n_h2d += (long long)bytes;
+  if (bytes >= kStageMin && pageable(src)) return h2d_staged(c, (char*)dst, (const char*)src, bytes);
   return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
 }
 
@@ -285,26 +353,6 @@ int upload(beta_gpu_ctx* c, DBuf<T>& d, const T* h, size_t n) {
   if (n) CK(h2d(c, d.p, h, n * sizeof(T)));
   TRACE("copy queued");
   return BETA_GPU_OK;
-}
-
-// Runs body(lo, hi) over [0, n) on the host's threads when n is large (the
-// input checks of a million-element mesh are otherwise tens of ms on one core).
-template <class F>
-void host_parallel(size_t n, F&& body) {
-  constexpr size_t kGrain = 1 << 20;
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t nt = std::min<size_t>(std::min<size_t>(hw, 32), (n + kGrain - 1) / kGrain);
-  if (nt <= 1) {
-    body(size_t(0), n);
-    return;
-  }
-  std::vector<std::thread> th;
-  const size_t step = (n + nt - 1) / nt;
-  for (size_t t = 0; t < nt; ++t) {
-    const size_t lo = t * step, hi = std::min(n, lo + step);
-    if (lo < hi) th.emplace_back([&body, lo, hi] { body(lo, hi); });
-  }
-  for (auto& x : th) x.join();
 }
 
 bool all_finite(const double* a, size_t n) {
@@ -1223,6 +1271,9 @@ int beta_gpu_destroy(beta_gpu_ctx* c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->h_st) cudaFreeHost(c->h_st);
   if (c->h_sums) cudaFreeHost(c->h_sums);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  for (auto e : c->stage_ev)
+    if (e) cudaEventDestroy(e);
   cudaStream_t s = c->own_stream;
   delete c;  // DBuf destructors free device memory
   if (s) cudaStreamDestroy(s);
@@ -1316,7 +1367,10 @@ int beta_gpu_mesh_upload(beta_gpu_ctx* c, int kind, int ndim, int nnode, const d
   c->kind = kind; c->ndim = ndim; c->nnode = nnode; c->nelem = nelem; c->nnpe = nnpe; c->ndpn = ndpn;
   c->ndof = nnode * ndpn; c->order = order;
   TRACE("validated");
-  c->h_conn.assign(conn, conn + (size_t)nelem * nnpe);
+  c->h_conn.resize((size_t)nelem * nnpe);
+  host_parallel(c->h_conn.size(), [&](size_t lo, size_t hi) {
+    std::memcpy(c->h_conn.data() + lo, conn + lo, (hi - lo) * sizeof(int));
+  });
   c->h_first_dof.assign(first_dof, first_dof + nnode);
   int rc;
   if ((rc = upload(c, c->xyz, xyz, (size_t)nnode * ndim))) return rc;
@@ -1415,9 +1469,11 @@ int beta_gpu_build_pattern(beta_gpu_ctx* c, long long* nnz_lower) {
   cudaSetDevice(c->device);
   // node-level structure only: the scalar FP64 layout is built the first
   // time an FP64 assembly needs it (ensure_scalar)
+  TRACE("enter");
   std::string msg = build_pattern(c->nnode, c->nelem, c->nnpe, c->ndpn, c->h_conn.data(), c->h_first_dof.data(),
                                   c->h_rest.data(), c->P, false);
   if (!msg.empty()) return fail(c, BETA_GPU_ERR_UNSUPPORTED, msg);
+  TRACE("host structure built");
   const HostPattern& P = c->P;
   int rc;
   if ((rc = upload(c, c->elems, P.elem_by_color.data(), P.elem_by_color.size()))) return rc;
@@ -1432,7 +1488,9 @@ int beta_gpu_build_pattern(beta_gpu_ctx* c, long long* nnz_lower) {
   }
   if ((rc = upload(c, c->ndiag, P.ndiag.data(), P.ndiag.size()))) return rc;
   if (P.run > 1 && (rc = upload(c, c->vpos, P.vpos.data(), P.vpos.size()))) return rc;
+  TRACE("uploads queued");
   CK(cudaStreamSynchronize(c->stream));
+  TRACE("uploads done");
   c->have_pattern = true;
   c->have_scalar = false;
   c->mfc_valid = false;  // the cache follows the colour order of the elements

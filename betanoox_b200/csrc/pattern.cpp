@@ -72,6 +72,7 @@ static void release_scratch(HostPattern& P) {
   std::vector<int>().swap(P.s_ufree);
   std::vector<uint64_t>().swap(P.s_used);
   std::vector<std::vector<int>>().swap(P.s_mark);
+  std::vector<FillVec<int>>().swap(P.s_rows);
 }
 
 // Column storage of the node-block layout for a caller that accepts runs
@@ -325,15 +326,26 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   for (int i = 0; i < nnode; ++i)
     if (icnt[i] == icnt[i + 1]) P.unused.push_back(i);
 
-  // ---- node graph (two passes: count, then fill) ---------------------
+  // free dofs per node, for the reference's lower-triangle count below
+  std::vector<int>& ufree = P.s_ufree;
+  ufree.resize(nnode);
+  parallel_for(nnode, [&](long long lo, long long hi) {
+    for (long long I = lo; I < hi; ++I) {
+      int f = 0;
+      for (int j = 0; j < ndpn; ++j) f += rest[ndpn * I + j] ? 0 : 1;
+      ufree[I] = f;
+    }
+  });
+
+  // ---- node graph: one pass over the rows, then their columns placed ----
   // Neighbours of node i are deduplicated with a marker array (mark[J - lo]
-  // == stamp once J is taken; the stamps of the two passes differ), so only
-  // the distinct ones are sorted.  Each chunk of rows has its own marker and
-  // position arrays: node-sized ones (kept between builds of a solver
-  // context) while all of them fit in kMarkBudget bytes; beyond that each
-  // chunk marks within the span of node ids its rows reach, which follows
-  // the numbering's bandwidth, and a chunk whose span is still wider than
-  // kSpanCap sorts and deduplicates each row instead.
+  // == i + 1 once J is taken), so only the distinct ones are sorted.  Each
+  // chunk of rows has its own marker and position arrays: node-sized ones
+  // (kept between builds of a solver context) while all of them fit in
+  // kMarkBudget bytes; beyond that each chunk marks within the span of node
+  // ids its rows reach, which follows the numbering's bandwidth, and a chunk
+  // whose span is still wider than kSpanCap sorts and deduplicates each row
+  // instead.
   struct Span { int lo = 0, hi = -1; };
   const int nck = chunk_count(nnode);
   constexpr long long kMarkBudget = BETA_PATTERN_MARK_BUDGET;
@@ -343,7 +355,6 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
 #else
   const long long kSpanCap = 4LL * ((nnode + nck - 1) / nck) + 65536;
 #endif
-  std::vector<Span> span(nck);
   if (node_sized) {
     P.s_mark.resize(2 * nck);  // per chunk: the marker, and the positions of the current row
   } else {
@@ -369,14 +380,41 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
     std::sort(buf.begin(), buf.end());
     if (!mark) buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
   };
+
+  // The row pass collects each node row i (sorted) once, keeps it in its
+  // chunk's buffer P.s_rows[ck] (rows lo..hi back to back) and writes from it:
+  //   * the row length into nrp[i + 1], and ndiag;
+  //   * the element -> node-pair block map: with pos[J] = J's position in
+  //     row i, each incident element (e, a) with conn[e][a] == i gets
+  //     slot[e][a][b] = pos[conn[e][b]] (every node of the element is in the
+  //     row); each (e, a) belongs to one row, so the writes do not overlap;
+  //   * the reference's lower-triangle count of its dof rows: a free row
+  //     r = I*ndpn + i holds the free dofs c <= r of its node row (all free
+  //     dofs of the neighbours J < I -- those before the diagonal -- and the
+  //     free dofs j <= i of I itself); a restrained row holds its diagonal.
+  // After the prefix over nrp the place pass copies each chunk's rows into
+  // ncol (one contiguous range per chunk; both passes split the rows into
+  // the same chunks) and, with one column per block, each row into its lane
+  // of the node-block sliced ELL, padded to the slice width with the row's
+  // own node.
   P.nrp.assign(nnode + 1, 0);
+  P.ndiag.resize(nnode);
+  const int npair = nnpe * nnpe;
+  P.slot.resize((size_t)nelem * npair);
+  if ((int)P.s_rows.size() < nck) P.s_rows.resize(nck);
+  std::vector<long long> lower(nck, 0);
   parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
-    std::vector<int> buf, local;
-    int* mark = nullptr;
+    std::vector<int> buf, local, local_pos;
+    FillVec<int>& rows = P.s_rows[ck];
+    rows.clear();
+    int *mark = nullptr, *pos = nullptr;
     Span sp{0, nnode - 1};
     if (node_sized) {
       P.s_mark[ck].assign(nnode, 0);
+      std::vector<int>& pv = P.s_mark[nck + ck];
+      if ((long long)pv.size() < nnode) pv.resize(nnode);
       mark = P.s_mark[ck].data();
+      pos = pv.data();
     } else {
       sp = Span{(int)lo, (int)hi - 1};
       for (long long i = lo; i < hi; ++i)
@@ -389,14 +427,49 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
         }
       if ((long long)sp.hi - sp.lo + 1 <= kSpanCap) {
         local.assign((size_t)(sp.hi - sp.lo + 1), 0);
+        local_pos.resize((size_t)(sp.hi - sp.lo + 1));
         mark = local.data();
+        pos = local_pos.data();
       }
     }
-    span[ck] = sp;
+    long long acc = 0;
     for (long long i = lo; i < hi; ++i) {
       collect((int)i, buf, mark, sp.lo, (int)i + 1);
-      P.nrp[i + 1] = (int)buf.size();
+      const int len = (int)buf.size();
+      rows.insert(rows.end(), buf.begin(), buf.end());
+      P.nrp[i + 1] = len;
+      const int d = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
+      P.ndiag[i] = d;
+      if (pos)
+        for (int k = 0; k < len; ++k) pos[buf[k] - sp.lo] = k;
+      for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
+        const long long e = inc[k];
+        const int* ce = conn + e * nnpe;
+        for (int a = 0; a < nnpe; ++a) {
+          if (ce[a] != (int)i) continue;
+          uint16_t* sl = P.slot.data() + e * npair + a * nnpe;
+          for (int b = 0; b < nnpe; ++b)  // J's position in the sorted row
+            sl[b] = (uint16_t)(pos ? pos[ce[b] - sp.lo]
+                                   : std::lower_bound(buf.begin(), buf.end(), ce[b]) - buf.begin());
+        }
+      }
+      if (icnt[i] == icnt[i + 1]) {  // a node in no element: its rows hold the diagonal alone
+        acc += ndpn;
+        continue;
+      }
+      long long below = 0;
+      for (int k = 0; k < d; ++k) below += ufree[buf[k]];
+      int own = 0;
+      for (int j = 0; j < ndpn; ++j) {
+        if (rest[i * ndpn + j]) {
+          acc += 1;
+        } else {
+          ++own;
+          acc += below + own;
+        }
+      }
     }
+    lower[ck] = acc;
   });
   for (int i = 0; i < nnode; ++i) {
     if (P.nrp[i + 1] > 65535) return "build_pattern: a node with more than 65535 neighbours";
@@ -416,97 +489,24 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
   P.nchunk = P.bsoff[P.nslice];
   if (P.nchunk * 32LL * ndpn * ndpn > 2000000000LL) return "build_pattern: block layout exceeds 2^31 entries";
 
-  // free dofs per node, for the reference's lower-triangle count below
-  std::vector<int>& ufree = P.s_ufree;
-  ufree.resize(nnode);
-  parallel_for(nnode, [&](long long lo, long long hi) {
-    for (long long I = lo; I < hi; ++I) {
-      int f = 0;
-      for (int j = 0; j < ndpn; ++j) f += rest[ndpn * I + j] ? 0 : 1;
-      ufree[I] = f;
-    }
-  });
-
-  // The fill pass writes, per node row i (sorted):
-  //   * the row into ncol, and ndiag;
-  //   * the element -> node-pair block map: with pos[J] = J's position in
-  //     row i, each incident element (e, a) with conn[e][a] == i gets
-  //     slot[e][a][b] = pos[conn[e][b]] (every node of the element is in the
-  //     row); each (e, a) belongs to one row, so the writes do not overlap;
-  //   * the row's lane of its slice in the node-block sliced ELL, padded to
-  //     the slice width with the row's own node;
-  //   * the reference's lower-triangle count of its dof rows: a free row
-  //     r = I*ndpn + i holds the free dofs c <= r of its node row (all free
-  //     dofs of the neighbours J < I -- those before the diagonal -- and the
-  //     free dofs j <= i of I itself); a restrained row holds its diagonal.
-  // Each row is read once.
+  // ---- place pass --------------------------------------------------------
   P.ncol.resize(P.nblk);
-  P.ndiag.resize(nnode);
-  const int npair = nnpe * nnpe;
-  P.slot.resize((size_t)nelem * npair);
-  // with runs requested the columns are laid out after the fill (build_columns)
+  // with runs requested the columns are laid out after this pass (build_columns)
   const bool ell_now = P.run_request <= 1;
   if (ell_now) P.bcol.resize((size_t)P.nchunk * 32);
-  std::vector<long long> lower(nck, 0);
   parallel_chunks(nnode, [&](int ck, long long lo, long long hi) {
-    const Span sp = span[ck];
-    std::vector<int> buf, local_mark, local_pos;
-    int *mark = nullptr, *pos = nullptr;
-    if (node_sized) {
-      std::vector<int>& pv = P.s_mark[nck + ck];
-      if ((long long)pv.size() < nnode) pv.resize(nnode);
-      mark = P.s_mark[ck].data();
-      pos = pv.data();
-    } else if ((long long)sp.hi - sp.lo + 1 <= kSpanCap) {
-      local_mark.assign((size_t)(sp.hi - sp.lo + 1), 0);
-      local_pos.resize((size_t)(sp.hi - sp.lo + 1));
-      mark = local_mark.data();
-      pos = local_pos.data();
-    }
-    long long acc = 0;
+    const int* row = P.s_rows[ck].data();
+    std::copy(row, row + (P.nrp[hi] - P.nrp[lo]), P.ncol.begin() + P.nrp[lo]);
+    if (!ell_now) return;
     for (long long i = lo; i < hi; ++i) {
-      collect((int)i, buf, mark, sp.lo, nnode + (int)i + 1);
-      const int len = (int)buf.size();
-      std::copy(buf.begin(), buf.end(), P.ncol.begin() + P.nrp[i]);
-      const int d = (int)(std::lower_bound(buf.begin(), buf.end(), (int)i) - buf.begin());
-      P.ndiag[i] = d;
-      if (pos)
-        for (int k = 0; k < len; ++k) pos[buf[k] - sp.lo] = k;
-      for (int k = icnt[i]; k < icnt[i + 1]; ++k) {
-        const long long e = inc[k];
-        const int* ce = conn + e * nnpe;
-        for (int a = 0; a < nnpe; ++a) {
-          if (ce[a] != (int)i) continue;
-          uint16_t* sl = P.slot.data() + e * npair + a * nnpe;
-          for (int b = 0; b < nnpe; ++b)  // J's position in the sorted row
-            sl[b] = (uint16_t)(pos ? pos[ce[b] - sp.lo]
-                                   : std::lower_bound(buf.begin(), buf.end(), ce[b]) - buf.begin());
-        }
-      }
-      if (ell_now) {
-        const long long s = i / 32;
-        const int w = P.bsoff[s + 1] - P.bsoff[s];
-        int* bc = P.bcol.data() + (size_t)P.bsoff[s] * 32 + (i % 32);
-        for (int k = 0; k < len; ++k) bc[(size_t)k * 32] = buf[k];
-        for (int k = len; k < w; ++k) bc[(size_t)k * 32] = (int)i;
-      }
-      if (icnt[i] == icnt[i + 1]) {  // a node in no element: its rows hold the diagonal alone
-        acc += ndpn;
-        continue;
-      }
-      long long below = 0;
-      for (int k = 0; k < d; ++k) below += ufree[buf[k]];
-      int own = 0;
-      for (int j = 0; j < ndpn; ++j) {
-        if (rest[i * ndpn + j]) {
-          acc += 1;
-        } else {
-          ++own;
-          acc += below + own;
-        }
-      }
+      const int len = P.nrp[i + 1] - P.nrp[i];
+      const int* r = row + (P.nrp[i] - P.nrp[lo]);
+      const long long s = i / 32;
+      const int w = P.bsoff[s + 1] - P.bsoff[s];
+      int* bc = P.bcol.data() + (size_t)P.bsoff[s] * 32 + (i % 32);
+      for (int k = 0; k < len; ++k) bc[(size_t)k * 32] = r[k];
+      for (int k = len; k < w; ++k) bc[(size_t)k * 32] = (int)i;
     }
-    lower[ck] = acc;
   });
   // lanes past the last node in the last slice
   if (ell_now) {
