@@ -1,8 +1,8 @@
-"""Uploads of 4 MB or more from pageable host memory go through the solver
-context's pinned staging buffer in 32 MB halves (a threaded host copy into
-one half while the DMA of the other runs).  An 80^3 hex8 cube has a 65.5 MB
-slot map (three halves, the first one refilled after its copy), a 37 MB
-material array (two halves) and 13-16 MB mesh and load arrays, so every
+"""Uploads of 4 MiB or more from pageable host memory go through the solver
+context's pinned staging buffer in 32 MiB halves (a threaded host copy into
+one half while the DMA of the other runs).  An 84^3 hex8 cube has a 72 MiB
+slot map (three halves, the first one refilled after its copy), a 41 MiB
+material array (two halves) and 14-18 MiB mesh and load arrays, so every
 structure and mesh array of a build takes that path.  The operators
 assembled from the staged structure must equal the FP64 matrix-free element
 operator, which reads only the mesh, on the free dofs; and the same mesh,
@@ -27,7 +27,7 @@ def _pinned(a):
 
 
 def test_staged_structure_and_mesh_uploads():
-    m = W.cube_hex8(80, seed=4)
+    m = W.cube_hex8(84, seed=4)
     assert m.nelem * m.nnpe * m.nnpe * 2 > 2 * (32 << 20)  # the slot map spans three halves
     free = m.restrained == 0
     u = np.random.default_rng(5).standard_normal(m.ndof)
