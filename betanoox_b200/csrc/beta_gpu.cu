@@ -172,8 +172,6 @@ struct beta_gpu_ctx {
   DBuf<unsigned> flags, ticket;
   PcgState* h_st = nullptr;   // pinned
   double* h_sums = nullptr;   // pinned
-  char* h_stage = nullptr;    // pinned staging of large pageable uploads (two halves)
-  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   DBuf<double> b64, x64, r64, p64, q64, d64, y64, t64;
   DBuf<float> v32[5];         // node-layout float vectors: x(d), r, p, q, spare
   DBuf<float> minv;
@@ -287,13 +285,26 @@ void host_parallel(size_t n, F&& body) {
   for (auto& x : th) x.join();
 }
 
-// Uploads of at least kStageMin bytes from pageable host memory go through
-// the context's pinned staging buffer: all host threads copy one half while
-// the DMA of the other half runs, instead of the driver's single-threaded
-// staging of a pageable copy.  Like a pageable copy, the source may be
-// reused as soon as the call returns.
+// Uploads of at least kStageMin bytes from pageable host memory go through a
+// pinned staging buffer: all host threads copy one half while the DMA of the
+// other half runs, instead of the driver's single-threaded staging of a
+// pageable copy.  Like a pageable copy, the source may be reused as soon as
+// the call returns.  There is one buffer per device for the whole process,
+// allocated at the first such upload and kept until the process ends (so a
+// short-lived context pays no pinned allocation), shared by the contexts on
+// that device under a mutex; each half has an event recorded on the stream
+// of the copy that last read it, and a refill waits for that event.
 constexpr size_t kStageHalf = size_t(32) << 20;
 constexpr size_t kStageMin = size_t(4) << 20;
+constexpr int kStageDevices = 64;
+
+struct Stage {
+  std::mutex mu;
+  char* buf = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool failed = false;  // no pinned memory to be had: plain pageable copies
+};
+Stage g_stage[kStageDevices];
 
 bool pageable(const void* p) {
   cudaPointerAttributes a;
@@ -304,25 +315,39 @@ bool pageable(const void* p) {
   return a.type == cudaMemoryTypeUnregistered;
 }
 
-cudaError_t h2d_staged(beta_gpu_ctx* c, char* dst, const char* src, size_t bytes) {
-  cudaError_t e;
-  if (!c->h_stage) {
-    if (cudaHostAlloc((void**)&c->h_stage, 2 * kStageHalf, cudaHostAllocDefault) != cudaSuccess) {
-      c->h_stage = nullptr;
-      cudaGetLastError();
-      return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
-    }
-    for (auto& ev : c->stage_ev)
-      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+// S.mu held; false: use a plain copy
+bool stage_ready(Stage& S) {
+  if (S.buf) return true;
+  if (S.failed) return false;
+  bool ok = cudaHostAlloc((void**)&S.buf, 2 * kStageHalf, cudaHostAllocDefault) == cudaSuccess;
+  for (auto& ev : S.ev) ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    for (auto& ev : S.ev)
+      if (ev) cudaEventDestroy(ev);
+    if (S.buf) cudaFreeHost(S.buf);
+    S.buf = nullptr;
+    S.ev[0] = S.ev[1] = nullptr;
+    S.failed = true;
   }
+  return ok;
+}
+
+cudaError_t h2d_staged(beta_gpu_ctx* c, char* dst, const char* src, size_t bytes) {
+  if (c->device < 0 || c->device >= kStageDevices)
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+  Stage& S = g_stage[c->device];
+  std::lock_guard<std::mutex> lock(S.mu);
+  if (!stage_ready(S)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+  cudaError_t e;
   for (size_t off = 0, k = 0; off < bytes; off += kStageHalf, ++k) {
     const size_t n = std::min(kStageHalf, bytes - off);
     const int h = (int)(k & 1);
-    char* st = c->h_stage + h * kStageHalf;
-    if ((e = cudaEventSynchronize(c->stage_ev[h])) != cudaSuccess) return e;  // its last copy has finished
+    char* st = S.buf + h * kStageHalf;
+    if ((e = cudaEventSynchronize(S.ev[h])) != cudaSuccess) return e;  // its last copy has finished
     host_parallel(n, [&](size_t lo, size_t hi) { std::memcpy(st + lo, src + off + lo, hi - lo); });
     if ((e = cudaMemcpyAsync(dst + off, st, n, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess) return e;
-    if ((e = cudaEventRecord(c->stage_ev[h], c->stream)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(S.ev[h], c->stream)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
@@ -1271,9 +1296,6 @@ int beta_gpu_destroy(beta_gpu_ctx* c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->h_st) cudaFreeHost(c->h_st);
   if (c->h_sums) cudaFreeHost(c->h_sums);
-  if (c->h_stage) cudaFreeHost(c->h_stage);
-  for (auto e : c->stage_ev)
-    if (e) cudaEventDestroy(e);
   cudaStream_t s = c->own_stream;
   delete c;  // DBuf destructors free device memory
   if (s) cudaStreamDestroy(s);
