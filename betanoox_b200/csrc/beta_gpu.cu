@@ -663,9 +663,14 @@ int pcg_loop(beta_gpu_ctx* c, int check_every, ProfAcc* prof, PcgState* out, dou
         launch(c, k_update_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->x64.p, c->r64.p, c->p64.p,
                                                                      c->q64.p, c->d64.p, c->st.p, c->partials.p);
         launch(c, k_pupd_s, grid_for(c, c->ndof, 256), 256, 0, c->ndof, c->p64.p, c->r64.p, c->d64.p, c->st.p);
+      } else if constexpr (PassNodes<ND>::N == 1) {  // two and three dofs per node
+        launch(c, k_update_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->v32[0].p, c->v32[1].p,
+               (const float*)c->v32[2].p, (const float*)c->v32[3].p, (const float*)c->minv.p, c->st.p,
+               c->partials.p);
+        launch(c, k_pupd_b<ND>, grid_for(c, c->nnode, 256), 256, 0, c->nnode, c->v32[2].p,
+               (const float*)c->v32[1].p, (const float*)c->minv.p, (const PcgState*)c->st.p);
       } else {
-        // several nodes per thread with wide accesses where that pays (one
-        // dof per node: four)
+        // several nodes per thread with 16-byte accesses (one dof per node: four)
         const long long blocks = c->nnode / PassNodes<ND>::N + 1;
         launch(c, k_update_bn<ND>, grid_for(c, blocks, 256), 256, 0, c->nnode, c->v32[0].p, c->v32[1].p,
                (const float*)c->v32[2].p, (const float*)c->v32[3].p, (const float*)c->minv.p, c->st.p,

@@ -475,17 +475,56 @@ __global__ void __launch_bounds__(256, SpmvShape<ND, R>::MINB) k_spmv_dot_b(Bloc
 }
 
 
+// x += alpha p; r -= alpha q; z = M r; (r.z, r.r, x.x) in FP64
+template <int ND>
+__global__ void __launch_bounds__(256) k_update_b(int nnode, float* __restrict__ x, float* __restrict__ r,
+                                                  const float* __restrict__ p, const float* __restrict__ q,
+                                                  const float* __restrict__ minv, PcgState* st, double* partials) {
+  if (st->done) return;
+  const float a = (float)st->alpha;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nnode; I += gridDim.x * blockDim.x) {
+    float xv[ND], rv[ND], pv[ND], qv[ND], z[ND];
+    NodeIO<ND>::ld(x, I, xv);
+    NodeIO<ND>::ld(r, I, rv);
+    PVec<ND>::ld(p, I, pv);
+    NodeIO<ND>::ld(q, I, qv);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      xv[i] = fmaf(a, pv[i], xv[i]);
+      rv[i] = fmaf(-a, qv[i], rv[i]);
+    }
+    NodeIO<ND>::st(x, I, xv);
+    NodeIO<ND>::st(r, I, rv);
+    NodeIO<ND>::prec(minv, I, rv, z);
+    float rz = 0.f, r2 = 0.f, x2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      rz = fmaf(rv[i], z[i], rz);
+      r2 = fmaf(rv[i], rv[i], r2);
+      x2 = fmaf(xv[i], xv[i], x2);
+    }
+    acc[0] += rz;
+    acc[1] += r2;
+    acc[2] += x2;
+  }
+  double out[3];
+  if (reduce_last<3>(acc, partials, &st->ticket, out) && threadIdx.x == 0) finish_update(st, out[0], out[1], out[2]);
+}
+
 // ---- the same two vector passes, several consecutive nodes per thread -----
 // NPT consecutive nodes' ND components are NPT*ND floats, the padded
 // direction NPT*PVec::W and the packed block-Jacobi factors NPT*ND(ND+1)/2:
 // a thread moves them with the widest aligned accesses those counts allow
 // (16 or 8 bytes) instead of ND 4-byte ones per node.  Per node the arithmetic
 // is the same; the FP64 partial sums add the nodes in another grouping.  The
-// last nnode % NPT nodes go one per thread.  One dof per node: four nodes
-// (16-byte accesses; the one-node update reached 0.73 of HBM on the slab:
-// transient step 30.4 -> 29.7 ms).  Three: one node (two nodes with 8- and
-// 16-byte accesses measured the same cube step, four nodes at 80 registers
-// slower).
+// last nnode % NPT nodes go one per thread.  Used for one dof per node, four
+// nodes (16-byte accesses; the one-node update reached 0.73 of HBM on the
+// slab: transient step 30.4 -> 29.7 ms).  Two and three dofs per node keep
+// the one-node kernels k_update_b and k_pupd_b: at three, this form with one
+// node per thread took 32 us a cold update launch on the 100^3 cube against
+// 27 (64-bit indexing, every load issued before the stores), two nodes
+// measured the same cube step, four nodes at 80 registers slower.
 template <int N>
 __device__ __forceinline__ void ldn(const float* v, long long blk, float (&o)[N]) {
   if constexpr (N % 4 == 0) {
