@@ -508,6 +508,10 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
       for (int k = len; k < w; ++k) bc[(size_t)k * 32] = (int)i;
     }
   });
+  // the row buffers (nblk ints in all) stay for the next build of a solver
+  // context only within the marker budget
+  if (!P.keep_scratch || (long long)P.nblk * (long long)sizeof(int) > kMarkBudget)
+    std::vector<FillVec<int>>().swap(P.s_rows);
   // lanes past the last node in the last slice
   if (ell_now) {
     for (int i = nnode; i < P.nslice * 32; ++i) {

@@ -122,7 +122,8 @@ struct HostPattern {
   std::vector<int> s_icnt, s_inc, s_color, s_ufree, s_ccnt;
   std::vector<uint64_t> s_used;
   std::vector<std::vector<int>> s_mark;  // node-sized marker and position arrays per chunk (within a budget)
-  std::vector<FillVec<int>> s_rows;      // per row chunk: its rows' sorted columns, from the count pass to the fill pass
+  std::vector<FillVec<int>> s_rows;      // per row chunk: its rows' sorted columns, from the row pass to the place
+                                         // pass (kept with keep_scratch only within the marker budget)
 };
 
 // Builds everything above.  conn: nelem*nnpe; restrained: ndof (0/1).
