@@ -145,6 +145,10 @@ BETA_GPU_API int beta_gpu_set_stream(beta_gpu_ctx* ctx, void* stream);
 BETA_GPU_API int beta_gpu_counters(const beta_gpu_ctx* ctx, long long* out, int n);
 
 /* ---- model upload (BasicMesh::ReadMesh / SetElementProperty / loads) ----- */
+/* Every upload copies its host input before it returns (the caller may reuse
+ * the buffer at once): pinned inputs directly, pageable ones of 4 MiB or more
+ * through a 64 MiB pinned staging buffer allocated once per device and kept
+ * for the process, shared by the contexts on that device. */
 /* Mesh: ndim 2|3, xyz[nnode*ndim] (node-major), conn[nelem*nnpe] in BETA
  * local node order (BasicElement.cpp:464-467, 518-525), first_dof[nnode].
  * `kind` fixes the element formulation; `integration_order` is the Gauss order
