@@ -1747,6 +1747,7 @@ int beta_gpu_solve_rhs(beta_gpu_ctx* c, const double* b, const double* x0, const
     CK(h2d(c, c->u.p, x0, sizeof(double) * n));
     c->have_u = true;
   }
+  CK(cudaStreamSynchronize(c->stream));  // b and x0 read before any way out (pinned inputs copy asynchronously)
   beta_gpu_solve_opts o2 = *o;
   o2.use_last_solution = x0 ? 1 : 0;
   if (o->mode == BETA_GPU_MODE_FP64) {
@@ -1786,15 +1787,15 @@ int beta_gpu_matvec(beta_gpu_ctx* c, int precision, const double* x, double* y) 
   if (!c || !x || !y) return BETA_GPU_ERR_ARG;
   cudaSetDevice(c->device);
   int rc;
+  if (precision == BETA_GPU_FP64 ? !c->have64 : !c->have32)  // checked before x is queued for copying
+    return fail(c, BETA_GPU_ERR_STATE, precision == BETA_GPU_FP64 ? "no FP64 matrix" : "no FP32 matrix");
   if ((rc = ensure_workspace(c))) return rc;
   const int n = c->ndof;
   CK(h2d(c, c->t64.p, x, sizeof(double) * n));
   if (precision == BETA_GPU_FP64) {
-    if (!c->have64) return fail(c, BETA_GPU_ERR_STATE, "no FP64 matrix");
     ScalarMat A{n, c->P.nsslice, c->ssoff.p, c->scol.p, c->sval.p};
     launch(c, k_spmv_s, grid_for(c, (long long)c->P.nsslice * 32, 256), 256, 0, A, c->t64.p, c->y64.p, nullptr);
   } else {
-    if (!c->have32) return fail(c, BETA_GPU_ERR_STATE, "no FP32 matrix");
     BlockMat A{c->nnode, c->P.nslice, c->bsoff.p, c->bcol.p, c->bval.p, c->P.compact ? c->cptr.p : nullptr};
     const int g = grid_for(c, (long long)c->P.nslice * 32, 256), gn = grid_for(c, n, 256);
     launch(c, k_to32, gn, 256, 0, (long long)n, (const double*)c->t64.p, 1.0, c->v32[0].p);
