@@ -150,6 +150,38 @@ static Mesh quad4_with_extras(int nx, int ny) {
   return M;
 }
 
+// The node graph and slot map against their definition, built here the
+// plain way (per node: its elements' nodes, sorted and deduplicated): row I
+// holds exactly the nodes that share an element with I (I alone for a node
+// in no element), ascending; ndiag is I's position in its row (one column per
+// block); and slot[e][a][b] is the position of conn[e][b] in row conn[e][a].
+static bool graph_semantics(const HostPattern& P, const Mesh& M) {
+  std::vector<std::vector<int>> elems(M.nnode);
+  for (int e = 0; e < M.nelem; ++e)
+    for (int a = 0; a < M.nnpe; ++a) elems[M.conn[(size_t)e * M.nnpe + a]].push_back(e);
+  std::vector<int> row;
+  for (int I = 0; I < M.nnode; ++I) {
+    row.clear();
+    for (int e : elems[I])
+      row.insert(row.end(), M.conn.begin() + (size_t)e * M.nnpe, M.conn.begin() + (size_t)(e + 1) * M.nnpe);
+    if (row.empty()) row.push_back(I);
+    std::sort(row.begin(), row.end());
+    row.erase(std::unique(row.begin(), row.end()), row.end());
+    if ((int)row.size() != P.nrp[I + 1] - P.nrp[I] || !std::equal(row.begin(), row.end(), P.ncol.begin() + P.nrp[I]))
+      return false;
+    if (P.run == 1 && P.ncol[P.nrp[I] + P.ndiag[I]] != I) return false;
+  }
+  const int np = M.nnpe * M.nnpe;
+  for (int e = 0; e < M.nelem; ++e)
+    for (int a = 0; a < M.nnpe; ++a)
+      for (int b = 0; b < M.nnpe; ++b) {
+        const int I = M.conn[(size_t)e * M.nnpe + a], J = M.conn[(size_t)e * M.nnpe + b];
+        const int q = P.slot[(size_t)e * np + a * M.nnpe + b];
+        if (q >= P.nrp[I + 1] - P.nrp[I] || P.ncol[P.nrp[I] + q] != J) return false;
+      }
+  return true;
+}
+
 int main() {
   std::vector<Mesh> meshes = {hex8(6, 3, false, 0),  hex8(24, 3, false, 0), hex8(24, 1, true, 3),
                               quad4_with_extras(150, 90), hex8(40, 3, true, 5), hex8(5, 1, false, 0),
@@ -183,6 +215,9 @@ int main() {
                     same(fresh.unused, reused.unused) && same(fresh.unused, serial.unused) &&
                     fresh.s_mark.empty() && marks_kept;
     std::printf("%-60s %s\n", M.name.c_str(), ok ? "equal" : "DIFFERENT");
+    const bool gok = ok && graph_semantics(fresh, M);
+    std::printf("graph %-54s %s\n", M.name.c_str(), gok ? "as defined" : "NOT AS DEFINED");
+    bad += gok || !ok ? 0 : 1;
     std::printf("hash %-55s %016llx\n", M.name.c_str(), hash_of(fresh));
     bad += ok ? 0 : 1;
     // the column-run layout, fresh and rebuilt into reused memory

@@ -1,6 +1,7 @@
 """Host structure build reused by a solver context (HostPattern::keep_scratch):
 a pattern rebuilt into the memory of an earlier, different mesh equals a
-fresh build in every field, and so does a single-threaded build; the
+fresh build in every field, and so does a single-threaded build; the node
+rows and the element slot map equal their definition built the plain way; the
 column-run layout of the FP32 block matrix places every block in its run
 (tests/cpp/pattern_reuse_check.cpp, compiled here against the host sources;
 no GPU needed)."""
@@ -18,6 +19,8 @@ def _run(tmp_path, name, extra):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count(" equal") == 8
+    # rows and slot map against their definition, built the plain way
+    assert r.stdout.count(" as defined") == 8 and "NOT AS DEFINED" not in r.stdout
     assert r.stdout.count(" valid") == 8 and "INVALID" not in r.stdout
     # the 70^3 grid with one dof per node takes the compact form of its runs
     assert any("hex8 n=70 nd=1" in line and "compact=1" in line for line in r.stdout.splitlines())
